@@ -1,0 +1,290 @@
+/*
+ * ba_cuda.h — C ABI of the B200-native bundle-adjustment solver.
+ *
+ * This header is the drop-in boundary for openmvg-ba's bundle-adjustment
+ * hot path. Every entry point takes plain pointers and sizes; no C++ or
+ * torch types cross it. All input buffers are caller-owned and read-only;
+ * all output buffers are caller-allocated with the shapes stated below.
+ *
+ * Reference interfaces this boundary replaces (paths inside openmvg-rs):
+ *   - BundleAdjuster::solve          crates/openmvg-ba/src/solver.rs:1562-1573
+ *   - BundleProblem (+ builder)      crates/openmvg-ba/src/problem.rs:447-577
+ *   - SolveConfig / validate         crates/openmvg-ba/src/solver.rs:74-155
+ *   - SolveReport / SolveDiagnostics crates/openmvg-ba/src/solver.rs:294-624
+ *   - Solution                       crates/openmvg-ba/src/solver.rs:788-1314
+ *   - SolveError                     crates/openmvg-ba/src/solver.rs:1474-1493
+ *   - ProblemError                   crates/openmvg-ba/src/problem.rs:731-779
+ *
+ * Return codes map one to one onto SolveError / ProblemError variants; the
+ * UTF-8 message is written into omvgba_error.message.
+ */
+#ifndef OMVGBA_BA_CUDA_H
+#define OMVGBA_BA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OMVGBA_ABI_VERSION 1u
+
+/* ---- return codes (SolveError, solver.rs:1474-1493; ProblemError, problem.rs:731) ---- */
+enum omvgba_code {
+  OMVGBA_OK = 0,
+  OMVGBA_INVALID_CONFIG = 1,      /* SolveError::InvalidConfig */
+  OMVGBA_UNSUPPORTED = 2,         /* SolveError::Unsupported: hand the problem on unchanged */
+  OMVGBA_RESOURCE_EXHAUSTED = 3,  /* SolveError::ResourceExhausted */
+  OMVGBA_NUMERICAL = 4,           /* SolveError::Numerical */
+  OMVGBA_INTERNAL = 5,            /* SolveError::Internal */
+  OMVGBA_INVALID_PROBLEM = 6,     /* ProblemError (BundleProblemBuilder::build) */
+  OMVGBA_INVALID_ARGUMENT = 7,    /* null pointer, short output buffer, bad enum */
+  OMVGBA_CUDA_ERROR = 8           /* a CUDA runtime call failed (reported as Internal upstream) */
+};
+
+typedef struct omvgba_error {
+  int32_t code;
+  int32_t detail; /* ProblemError variant index or offending element index, -1 if none */
+  char message[480];
+} omvgba_error;
+
+/* ---- camera models (openmvg-core camera::Camera, brown_conrady.rs, distortion.rs) ---- */
+enum omvgba_camera_model {
+  OMVGBA_CAMERA_PINHOLE = 0,
+  OMVGBA_CAMERA_BROWN_CONRADY = 1,
+  OMVGBA_CAMERA_FISHEYE = 2,   /* accepted by the contract, rejected as Unsupported for pixel BA */
+  OMVGBA_CAMERA_SPHERICAL = 3  /* idem */
+};
+/* RadialDistortion discriminant: None, K1, K1K2, K1K2K3 (distortion.rs:183-241) */
+enum omvgba_radial_kind { OMVGBA_RADIAL_NONE = 0, OMVGBA_RADIAL_K1 = 1, OMVGBA_RADIAL_K1K2 = 2, OMVGBA_RADIAL_K1K2K3 = 3 };
+/* TangentialDistortion discriminant: None, P1, P1P2 (distortion.rs:459-527) */
+enum omvgba_tangential_kind { OMVGBA_TANGENTIAL_NONE = 0, OMVGBA_TANGENTIAL_P1 = 1, OMVGBA_TANGENTIAL_P1P2 = 2 };
+
+/* IntrinsicVariables bits (problem.rs:42-70) */
+#define OMVGBA_INTRINSIC_FOCAL (1u << 0)
+#define OMVGBA_INTRINSIC_PRINCIPAL_POINT (1u << 1)
+#define OMVGBA_INTRINSIC_RADIAL (1u << 2)
+#define OMVGBA_INTRINSIC_TANGENTIAL (1u << 3)
+/* PoseVariables bits (problem.rs:15-40) */
+#define OMVGBA_POSE_ROTATION (1u << 0)
+#define OMVGBA_POSE_TRANSLATION (1u << 1)
+#define OMVGBA_POSE_FREE (OMVGBA_POSE_ROTATION | OMVGBA_POSE_TRANSLATION)
+
+/* BundlePose: WorldToCameraPose (rotation R world->camera, row-major; center C) + variables. */
+typedef struct omvgba_pose {
+  double rotation[9];
+  double center[3];
+  uint32_t variables;
+  uint32_t reserved;
+} omvgba_pose;
+
+/* BundleIntrinsic: CameraIntrinsics + IntrinsicVariables + IntrinsicCertification. */
+typedef struct omvgba_intrinsic {
+  int32_t model;            /* omvgba_camera_model */
+  int32_t radial_kind;      /* omvgba_radial_kind (Brown-Conrady only) */
+  int32_t tangential_kind;  /* omvgba_tangential_kind (Brown-Conrady only) */
+  uint32_t variables;       /* OMVGBA_INTRINSIC_* bits */
+  int32_t certification;    /* 0 Required, 1 Waived */
+  int32_t fixed_model;      /* CameraIntrinsics::is_fixed(): 1 forbids variable coordinates */
+  double fx, fy, cx, cy;
+  double k1, k2, k3, p1, p2;
+  uint32_t width, height;
+} omvgba_intrinsic;
+
+enum omvgba_residual_space { OMVGBA_RESIDUAL_PIXELS = 0, OMVGBA_RESIDUAL_ANGULAR = 1 };
+/* RobustLoss (problem.rs:267-300). The scale carries its own residual space. */
+enum omvgba_loss_kind { OMVGBA_LOSS_SQUARED = 0, OMVGBA_LOSS_HUBER = 1, OMVGBA_LOSS_CAUCHY = 2 };
+/* Gauge (problem.rs:302-312) */
+enum omvgba_gauge_kind { OMVGBA_GAUGE_FREE = 0, OMVGBA_GAUGE_FIXED_BASELINE = 1 };
+
+/* BundleProblem (problem.rs:447-577) as structure-of-arrays. */
+typedef struct omvgba_problem {
+  uint64_t pose_count;
+  const omvgba_pose* poses;
+  uint64_t intrinsic_count;
+  const omvgba_intrinsic* intrinsics;
+  uint64_t point_count;
+  const double* points;        /* point_count x 3, interleaved xyz */
+  const uint8_t* point_fixed;  /* point_count flags, or NULL for all free */
+  uint64_t observation_count;
+  const uint32_t* observation_pose;
+  const uint32_t* observation_intrinsic;
+  const uint32_t* observation_point;
+  const double* observation_pixel; /* observation_count x 2, interleaved */
+  int32_t residual_space;      /* omvgba_residual_space */
+  int32_t loss_kind;           /* omvgba_loss_kind */
+  double loss_scale;           /* delta (Huber) or scale (Cauchy), in loss_scale_space units */
+  int32_t loss_scale_space;    /* omvgba_residual_space of the loss scale */
+  int32_t gauge_kind;          /* omvgba_gauge_kind */
+  uint64_t gauge_first, gauge_second;
+  double gauge_distance;
+} omvgba_problem;
+
+/* LinearSolver (solver.rs:11-18) */
+enum omvgba_linear_solver { OMVGBA_SOLVER_AUTO = 0, OMVGBA_SOLVER_DIRECT = 1, OMVGBA_SOLVER_ITERATIVE = 2 };
+/* Build-private precision policy (not in the reference API). */
+enum omvgba_precision {
+  OMVGBA_PRECISION_FP64 = 0,  /* every kernel in FP64 */
+  OMVGBA_PRECISION_MIXED = 1  /* FP32 Jacobians and matvecs; FP64 point inverses, factorizations,
+                                 dot products, cost and LM test; FP64 refinement of the step */
+};
+/* Build-private reduced-camera-system operator. */
+enum omvgba_matvec { OMVGBA_MATVEC_AUTO = 0, OMVGBA_MATVEC_EXPLICIT = 1, OMVGBA_MATVEC_IMPLICIT = 2 };
+
+/* SolveConfig (solver.rs:74-155) plus build-private execution options. */
+typedef struct omvgba_config {
+  uint64_t max_iterations;        /* default 50 */
+  double function_tolerance;      /* default 1e-6 */
+  double gradient_tolerance;      /* default 1e-10 */
+  double parameter_tolerance;     /* default 1e-8 */
+  int32_t linear_solver;          /* omvgba_linear_solver, default Auto */
+  int32_t has_workspace_budget;   /* 0: None */
+  uint64_t workspace_budget_bytes;
+  /* build-private */
+  int32_t precision;              /* omvgba_precision */
+  int32_t matvec;                 /* omvgba_matvec */
+  double pcg_relative_tolerance;  /* 0: native default 1e-1 (native/mod.rs:597-603) */
+  uint32_t pcg_max_iterations;    /* 0: 600 (sparse/api.rs:395) */
+  int32_t device;                 /* CUDA device ordinal */
+  void* stream;                   /* cudaStream_t or NULL for a context-owned stream */
+} omvgba_config;
+
+/* Fill *config with SolveConfig::default() and the build-private defaults. */
+void omvgba_config_default(omvgba_config* config);
+
+/* SolveStatus / ConvergenceReason (solver.rs:87-105) */
+enum omvgba_solve_status {
+  OMVGBA_STATUS_CONVERGED = 0,
+  OMVGBA_STATUS_MAX_ITERATIONS = 1,
+  OMVGBA_STATUS_STALLED = 2,
+  OMVGBA_STATUS_DEGENERATE = 3,
+  OMVGBA_STATUS_SKIPPED = 4
+};
+enum omvgba_convergence_reason { OMVGBA_REASON_NONE = -1, OMVGBA_REASON_OBJECTIVE = 0, OMVGBA_REASON_GRADIENT = 1, OMVGBA_REASON_STEP = 2 };
+/* Observability (solver.rs:107-115) */
+enum omvgba_observability {
+  OMVGBA_OBS_FULL_RANK = 0,
+  OMVGBA_OBS_ONLY_EXPECTED_GAUGE = 1,
+  OMVGBA_OBS_RANK_DEFICIENT = 2,
+  OMVGBA_OBS_NOT_ASSESSED = 3
+};
+
+/* SolveReport + SolveDiagnostics (solver.rs:294-624). Optional fields carry a has_ flag. */
+typedef struct omvgba_report {
+  int32_t status;                 /* omvgba_solve_status */
+  int32_t convergence_reason;     /* omvgba_convergence_reason */
+  uint64_t iteration_count;
+  double initial_objective, final_objective;
+  double initial_rmse, final_rmse;
+  uint64_t accepted_step_count, rejected_step_count;
+  uint64_t rejected_linearization, rejected_step_solve, rejected_candidate, rejected_insufficient_reduction;
+  int32_t has_stationarity;
+  double scaled_gradient_inf_norm;
+  int32_t observability;          /* omvgba_observability */
+  int32_t has_weak_point_count;
+  uint64_t weak_point_count;
+  uint64_t quarantined_point_count;
+  int32_t has_noninvertible_observation_count;
+  uint64_t noninvertible_observation_count;
+  int32_t has_observability_details;
+  uint64_t details_pose_rank, details_pose_dimension, details_weak_point_count;
+  int32_t has_linear_solver;
+  int32_t linear_solver;          /* omvgba_linear_solver actually used */
+  int32_t has_observation_count;
+  uint64_t observation_count;
+  int32_t has_inlier_count;
+  uint64_t inlier_count;
+  int32_t has_final_inlier_rmse;
+  double final_inlier_rmse;
+  uint64_t unconstrained_intrinsic_count; /* indices in omvgba_solution.unconstrained_intrinsics */
+  /* build telemetry (not part of the reference report) */
+  uint64_t pcg_iteration_count;
+  uint64_t reduced_dimension;
+  double final_damping;
+  double solve_seconds;           /* wall time inside omvgba_solve */
+  double upload_seconds;          /* host->device problem upload inside that time */
+} omvgba_report;
+
+/* Solution (solver.rs:788-1314). Every array is caller-allocated. */
+typedef struct omvgba_solution {
+  omvgba_pose* poses;              /* pose_count */
+  omvgba_intrinsic* intrinsics;    /* intrinsic_count */
+  double* points;                  /* point_count x 3 */
+  uint64_t* quarantined_points;    /* capacity point_count; count = report.quarantined_point_count */
+  uint64_t* unconstrained_intrinsics; /* capacity intrinsic_count */
+  omvgba_report report;
+} omvgba_solution;
+
+/* One solver context per thread or stream: device workspaces, streams, no global state. */
+typedef struct omvgba_context omvgba_context;
+
+omvgba_context* omvgba_context_create(int32_t device, omvgba_error* error);
+void omvgba_context_destroy(omvgba_context* context);
+uint32_t omvgba_abi_version(void);
+
+/* BundleAdjuster::solve (solver.rs:1562-1573) on the GPU. Never mutates the problem. */
+int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                     omvgba_solution* solution, omvgba_error* error);
+
+/* BundleAdjuster::name (solver.rs:1566). */
+const char* omvgba_adjuster_name(void);
+
+/*
+ * First linearization of the lowered problem, per observation in the solver's
+ * point-major order (observations stably sorted by point, native/calibrated.rs:371-375).
+ * Outputs: residual (n x 2, prediction minus pixel), sqrt_weight (n), point Jacobian
+ * J_proj * R * s (n x 6, row-major 2x3), camera Jacobian (n x 2 x 9, row-major; columns
+ * beyond the camera's free dimension are zero), source_index (n, the input observation).
+ * Reference: schur/point.rs:176-355, kernel/projection.rs:47-87, self_calibration/model.rs:26-324.
+ */
+int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* problem,
+                               const omvgba_config* config, double* residual, double* sqrt_weight,
+                               double* point_jacobian, double* camera_jacobian, uint64_t* source_index,
+                               omvgba_error* error);
+
+/*
+ * Reprojection residual of the centred radial model (self_calibration/model.rs:26-129) over an
+ * unsorted observation list, and its vector-Jacobian product. Camera j has rotation vector
+ * rotvec[3j..3j+3] (R = exp(rotvec)), translation t[3j..], intrinsics intr[3j..] = (f, k1, k2);
+ * residual_i = f (1 + k1 r^2 + k2 r^4) n_i - pixel_i with n_i the normalized camera point.
+ * Inadmissible observations produce NaN residuals and zero gradients.
+ * The VJP accumulates into grad_* (caller zeroes them): for each input the adjoint sum over
+ * observations of J^T grad_residual, in a fixed order (deterministic run to run).
+ * Pointers are DEVICE pointers; stream is a cudaStream_t (NULL = legacy default stream).
+ */
+int32_t omvgba_residual_forward_f32(void* stream, uint64_t observation_count, const uint32_t* camera_index,
+                                    const uint32_t* point_index, const float* pixel, uint64_t camera_count,
+                                    const float* rotvec, const float* translation, const float* intrinsics,
+                                    uint64_t point_count, const float* points, float* residual,
+                                    omvgba_error* error);
+int32_t omvgba_residual_vjp_f32(void* stream, uint64_t observation_count, const uint32_t* camera_index,
+                                const uint32_t* point_index, const float* pixel, uint64_t camera_count,
+                                const float* rotvec, const float* translation, const float* intrinsics,
+                                uint64_t point_count, const float* points, const float* grad_residual,
+                                float* grad_rotvec, float* grad_translation, float* grad_intrinsics,
+                                float* grad_points, void* workspace, uint64_t workspace_bytes,
+                                omvgba_error* error);
+/* Bytes of device workspace omvgba_residual_vjp_f32 needs for these sizes. */
+uint64_t omvgba_residual_vjp_workspace_bytes(uint64_t observation_count, uint64_t camera_count,
+                                             uint64_t point_count);
+int32_t omvgba_residual_forward_f64(void* stream, uint64_t observation_count, const uint32_t* camera_index,
+                                    const uint32_t* point_index, const double* pixel, uint64_t camera_count,
+                                    const double* rotvec, const double* translation, const double* intrinsics,
+                                    uint64_t point_count, const double* points, double* residual,
+                                    omvgba_error* error);
+
+/*
+ * Many independent problems (local-BA windows) solved together: one persistent launch per LM
+ * phase over all windows, per-window convergence masks, graph-captured. Each window follows
+ * omvgba_solve's contract; solutions[i] receives window i. No reference counterpart: the
+ * reference solves one problem per call (crates/openmvg-ba/src/solver.rs:1562).
+ */
+int32_t omvgba_solve_batched(omvgba_context* context, uint64_t window_count, const omvgba_problem* windows,
+                             const omvgba_config* config, omvgba_solution* solutions, omvgba_error* error);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OMVGBA_BA_CUDA_H */

@@ -1,0 +1,2363 @@
+// gpu_solver.cu — B200 (sm_100a) Levenberg–Marquardt bundle adjustment.
+//
+// Hot path (reference paths relative to the openmvg-rs root):
+//   K1  k_linearize ........ per-observation projection, robust weight, analytic point / camera
+//                            Jacobians and the per-point 3x3 Gram + FP64 damped inverse
+//                            (schur/point.rs:176-448, schur/assembly.rs:893-1040, point_block.rs:78-184)
+//   K2  k_block_chunks ..... camera-side deterministic segmented reductions: U blocks, g, reduced g,
+//                            damping diagonal, pose/intrinsic edges, diagonal point coupling
+//       k_pairs ............ explicit Schur blocks S_bb' -= W V^-1 W^T (schur/assembly.rs:999-1038)
+//   K3  k_dense_cholesky ... dense FP64 Cholesky for small reduced systems (stands in for faer LLT)
+//       k_mv_points/blocks . matrix-free reduced-camera-system product S x (retained/operator.rs:137-227)
+//       block-Jacobi PCG ... sparse/pcg.rs:23-119, retained/mod.rs:682-934, retained/block.rs:148-246
+//   K4  k_retract, k_candidate_points: step cap, retraction, back-substitution and candidate rule
+//                            (optimizer.rs:376-702, sparse/calibrated/candidate.rs:23-333,
+//                            schur/point.rs:537-728, point_geometry.rs:110-130)
+// Every reduction runs in a fixed order (fixed grid, fixed shuffle trees, fixed chunk order), so a
+// solve is bitwise reproducible run to run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "gpu_solver.hpp"
+
+namespace omvgba {
+
+#define CUDA_OK(expr)                                                                                 \
+  do {                                                                                                \
+    cudaError_t _e = (expr);                                                                          \
+    if (_e != cudaSuccess)                                                                            \
+      throw SolveFailure{8, std::string("CUDA error: ") + cudaGetErrorString(_e) + " at " #expr};     \
+  } while (0)
+
+constexpr int kChunk = 256;     // entities per block chunk
+constexpr int kReduceThreads = 256;
+
+// ----------------------------------------------------------------------------------------------
+// Context
+// ----------------------------------------------------------------------------------------------
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double* pinned = nullptr;  // scalar readback
+  size_t pinned_count = 0;
+};
+
+Context* context_create(int device, std::string* error) {
+  Context* c = new Context();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->pinned, sizeof(double) * 64);
+  if (e != cudaSuccess) {
+    if (error) *error = cudaGetErrorString(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return nullptr;
+  }
+  c->pinned_count = 64;
+  return c;
+}
+
+void context_destroy(Context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+// Device buffer owned for one solve (stream-ordered allocation).
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  void alloc(size_t count, cudaStream_t stream) {
+    release();
+    s = stream;
+    n = count;
+    if (count) CUDA_OK(cudaMallocAsync((void**)&p, sizeof(T) * count, stream));
+  }
+  void upload(const T* host, size_t count, cudaStream_t stream) {
+    alloc(count, stream);
+    if (count) CUDA_OK(cudaMemcpyAsync(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, stream));
+  }
+  void zero() {
+    if (n) CUDA_OK(cudaMemsetAsync(p, 0, sizeof(T) * n, s));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+// ----------------------------------------------------------------------------------------------
+// Device problem view
+// ----------------------------------------------------------------------------------------------
+struct Gauge {
+  int fixed_cam;
+  double baseline, scene;
+  double dir[3], b0[3], b1[3];
+};
+
+struct DevView {
+  int P, ncam, self_cal, pixel_model;
+  const uint32_t* pt_off;      // P+1
+  const uint32_t* obs_cam;     // N
+  const double* obs_px;        // N x 2
+  const uint32_t* obs_model;   // N (calibrated)
+  const FixedCameraDev* models;
+  const uint32_t* cam_group;   // ncam
+  const int* pose_off;         // ncam
+  const int* pose_dim;         // ncam
+  const int* intr_off;         // ng
+  const int* intr_dim;         // ng
+  const uint8_t* fixed_points; // P
+};
+
+struct DevState {
+  double* pose;    // ncam x 12: R (9) then t (3)
+  double* points;  // P x 3
+  double* groups;  // ng x 3 (focal, k1, k2)
+};
+
+__device__ __forceinline__ RadialDev make_radial(const double* g) {
+  RadialDev c;
+  c.focal = g[0];
+  c.k1 = g[1];
+  c.k2 = g[2];
+  double t;
+  c.has_turn = first_radial_turn_squared(c.k1, c.k2, &t) ? 1 : 0;
+  c.turn = t;
+  return c;
+}
+
+// Projection of observation o for camera point xc; Ji is filled for self-calibration.
+__device__ __forceinline__ bool project_obs(const DevView& v, const double* groups, int o, const double xc[3],
+                                            double r[2], double J[2][3], double Ji[2][3]) {
+  double ox = v.obs_px[2 * o], oy = v.obs_px[2 * o + 1];
+  if (v.self_cal) {
+    RadialDev c = make_radial(groups + 3 * v.cam_group[v.obs_cam[o]]);
+    return radial_linearize(c, xc[0], xc[1], xc[2], ox, oy, r, J, Ji);
+  }
+  const FixedCameraDev& m = v.models[v.obs_model[o]];
+  if (v.pixel_model) return pixel_linearize(m, xc[0], xc[1], xc[2], ox, oy, r, J);
+  return m.linearize(xc[0], xc[1], xc[2], ox, oy, r, J);
+}
+
+// ----------------------------------------------------------------------------------------------
+// Deterministic reductions
+// ----------------------------------------------------------------------------------------------
+template <int NV>
+struct RedVec {
+  double v[NV];
+};
+
+// Per-point linearization summary reduced over points: sums (cost, sq, point_red) and extrema.
+struct PointSummary {
+  double cost, sq, point_red, grad_norm, min_rcond;
+  double invalid, weak, pad;
+};
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  return x;
+}
+__device__ __forceinline__ double warp_max(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+  return x;
+}
+__device__ __forceinline__ double warp_min(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+  return x;
+}
+
+// Reduce an array of PointSummary (one per point) into per-block partials; fixed order.
+__global__ void k_reduce_summary(const PointSummary* in, int n, PointSummary* out) {
+  __shared__ PointSummary sh[kReduceThreads / 32];
+  int tid = threadIdx.x;
+  PointSummary acc{0, 0, 0, 0, 1.0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + tid; i < n; i += gridDim.x * blockDim.x) {
+    PointSummary s = in[i];
+    acc.cost += s.cost;
+    acc.sq += s.sq;
+    acc.point_red += s.point_red;
+    acc.grad_norm = fmax(acc.grad_norm, s.grad_norm);
+    acc.min_rcond = fmin(acc.min_rcond, s.min_rcond);
+    acc.invalid += s.invalid;
+    acc.weak += s.weak;
+  }
+  acc.cost = warp_sum(acc.cost);
+  acc.sq = warp_sum(acc.sq);
+  acc.point_red = warp_sum(acc.point_red);
+  acc.grad_norm = warp_max(acc.grad_norm);
+  acc.min_rcond = warp_min(acc.min_rcond);
+  acc.invalid = warp_sum(acc.invalid);
+  acc.weak = warp_sum(acc.weak);
+  if ((tid & 31) == 0) sh[tid >> 5] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    PointSummary t = sh[0];
+    for (int w = 1; w < (int)(blockDim.x / 32); ++w) {
+      t.cost += sh[w].cost;
+      t.sq += sh[w].sq;
+      t.point_red += sh[w].point_red;
+      t.grad_norm = fmax(t.grad_norm, sh[w].grad_norm);
+      t.min_rcond = fmin(t.min_rcond, sh[w].min_rcond);
+      t.invalid += sh[w].invalid;
+      t.weak += sh[w].weak;
+    }
+    out[blockIdx.x] = t;
+  }
+}
+
+// Sum of NV-component records (e.g. dot products) with a fixed grid: per block partial, then the
+// final pass over partials in index order.
+template <int NV>
+__global__ void k_reduce_vec(const RedVec<NV>* in, int n, RedVec<NV>* out) {
+  __shared__ double sh[kReduceThreads / 32][NV];
+  int tid = threadIdx.x;
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + tid; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += in[i].v[k];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = warp_sum(acc[k]);
+  if ((tid & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[tid >> 5][k] = acc[k];
+  __syncthreads();
+  if (tid == 0) {
+    RedVec<NV> t;
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += sh[w][k];
+      t.v[k] = s;
+    }
+    out[blockIdx.x] = t;
+  }
+}
+
+// Dot products of D-vectors: out[k] = sum_i a_k[i] * b_k[i], fixed order.
+struct DotArgs {
+  const double* a[4];
+  const double* b[4];
+  int count;
+};
+__global__ void k_dots(DotArgs args, int n, double* out) {
+  // single block of 1024 threads: strided partials, fixed shuffle tree, fixed warp order
+  __shared__ double sh[32][4];
+  int tid = threadIdx.x;
+  double acc[4] = {0, 0, 0, 0};
+  for (int i = tid; i < n; i += blockDim.x)
+    for (int k = 0; k < args.count; ++k) acc[k] += args.a[k][i] * args.b[k][i];
+  for (int k = 0; k < 4; ++k) acc[k] = warp_sum(acc[k]);
+  if ((tid & 31) == 0)
+    for (int k = 0; k < 4; ++k) sh[tid >> 5][k] = acc[k];
+  __syncthreads();
+  if (tid < args.count) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += sh[w][tid];
+    out[tid] = s;
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// K1: per-point linearization (+ point-block factorization)
+// ----------------------------------------------------------------------------------------------
+template <typename T>
+struct LinOut {
+  T* jc;           // N x 18 (2 rows x 9 columns: pose | intrinsics), sqrt-weighted
+  T* jp;           // N x 6, sqrt-weighted
+  double* rw;      // N x 2, sqrt-weighted residual
+  double* vinv;    // P x 6: damped point-block inverse (zero for fixed points)
+  double* ig;      // P x 3: Vhat^-1 g_p (zero for fixed points)
+  double* gp;      // P x 3: point gradient
+  double* ddiag;   // P x 3: damping diagonal
+  PointSummary* summary;  // P
+  double* sw;      // optional N: sqrt weight per observation (debug linearization only)
+};
+
+// pose_motion (schur/point.rs:730-762) applied to the projection Jacobian: J * [-[RX]x | s I]
+__device__ __forceinline__ void pose_jacobian(const double J[2][3], const double rot[3], int cam, const Gauge& g,
+                                              double out[2][6]) {
+  double m[3][6] = {{0.0, rot[2], -rot[1], 0, 0, 0}, {-rot[2], 0.0, rot[0], 0, 0, 0}, {rot[1], -rot[0], 0.0, 0, 0, 0}};
+  if (cam == g.fixed_cam) {
+    for (int c = 0; c < 3; ++c) {
+      m[c][3] = g.baseline * g.b0[c];
+      m[c][4] = g.baseline * g.b1[c];
+    }
+  } else {
+    m[0][3] = g.scene;
+    m[1][4] = g.scene;
+    m[2][5] = g.scene;
+  }
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 6; ++c) out[r][c] = J[r][0] * m[0][c] + J[r][1] * m[1][c] + J[r][2] * m[2][c];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge g, LossDev loss, double lambda,
+                                                   LinOut<T> out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= v.P) return;
+  const double X0 = s.points[3 * p], X1 = s.points[3 * p + 1], X2 = s.points[3 * p + 2];
+  double V[6] = {0, 0, 0, 0, 0, 0}, gp[3] = {0, 0, 0};
+  double cost = 0.0, sq = 0.0;
+  bool ok = true;
+  uint32_t o0 = v.pt_off[p], o1 = v.pt_off[p + 1];
+  for (uint32_t o = o0; o < o1; ++o) {
+    int cam = v.obs_cam[o];
+    const double* P = s.pose + 12 * cam;
+    double rot[3] = {P[0] * X0 + P[1] * X1 + P[2] * X2, P[3] * X0 + P[4] * X1 + P[5] * X2,
+                     P[6] * X0 + P[7] * X1 + P[8] * X2};
+    double xc[3] = {rot[0] + P[9], rot[1] + P[10], rot[2] + P[11]};
+    double r[2], J[2][3], Ji[2][3];
+    if (!project_obs(v, s.groups, o, xc, r, J, Ji)) {
+      ok = false;
+      for (int k = 0; k < 18; ++k) out.jc[(size_t)18 * o + k] = T(0);
+      for (int k = 0; k < 6; ++k) out.jp[(size_t)6 * o + k] = T(0);
+      out.rw[2 * o] = 0.0;
+      out.rw[2 * o + 1] = 0.0;
+      continue;
+    }
+    double rn = sqrt(r[0] * r[0] + r[1] * r[1]);
+    double sw = loss.sqrt_weight(rn);
+    cost += loss.cost(rn);
+    sq += rn * rn;
+    double jp[2][3];
+    for (int a = 0; a < 2; ++a)
+      for (int c = 0; c < 3; ++c) jp[a][c] = (J[a][0] * P[c] + J[a][1] * P[3 + c] + J[a][2] * P[6 + c]) * g.scene;
+    for (int a = 0; a < 2; ++a) {
+      double wr = sw * r[a];
+      double w0 = sw * jp[a][0], w1 = sw * jp[a][1], w2 = sw * jp[a][2];
+      gp[0] += w0 * wr;
+      gp[1] += w1 * wr;
+      gp[2] += w2 * wr;
+      V[0] += w0 * w0;
+      V[1] += w1 * w0;
+      V[2] += w1 * w1;
+      V[3] += w2 * w0;
+      V[4] += w2 * w1;
+      V[5] += w2 * w2;
+    }
+    double jc[2][9];
+    for (int a = 0; a < 2; ++a)
+      for (int k = 0; k < 9; ++k) jc[a][k] = 0.0;
+    int pd = v.pose_dim[cam];
+    if (pd > 0) {
+      double pj[2][6];
+      pose_jacobian(J, rot, cam, g, pj);
+      for (int a = 0; a < 2; ++a)
+        for (int k = 0; k < pd; ++k) jc[a][k] = pj[a][k];
+    }
+    if (v.self_cal) {
+      int id = v.intr_dim[v.cam_group[cam]];
+      for (int a = 0; a < 2; ++a)
+        for (int k = 0; k < id; ++k) jc[a][pd + k] = Ji[a][k];
+    }
+    T* jco = out.jc + (size_t)18 * o;
+    for (int a = 0; a < 2; ++a)
+      for (int k = 0; k < 9; ++k) jco[9 * a + k] = T(sw * jc[a][k]);
+    T* jpo = out.jp + (size_t)6 * o;
+    for (int a = 0; a < 2; ++a)
+      for (int c = 0; c < 3; ++c) jpo[3 * a + c] = T(sw * jp[a][c]);
+    out.rw[2 * o] = sw * r[0];
+    out.rw[2 * o + 1] = sw * r[1];
+    if (out.sw) out.sw[o] = sw;
+  }
+  PointSummary sm{0, 0, 0, 0, 1.0, 0, 0, 0};
+  double zero6[6] = {0, 0, 0, 0, 0, 0};
+  double* vi = out.vinv + 6 * (size_t)p;
+  double* ig = out.ig + 3 * (size_t)p;
+  for (int k = 0; k < 6; ++k) vi[k] = 0.0;
+  ig[0] = ig[1] = ig[2] = 0.0;
+  out.gp[3 * (size_t)p] = gp[0];
+  out.gp[3 * (size_t)p + 1] = gp[1];
+  out.gp[3 * (size_t)p + 2] = gp[2];
+  (void)zero6;
+  if (!ok) {
+    sm.invalid = 1;
+    out.summary[p] = sm;
+    return;
+  }
+  sm.cost = cost;
+  sm.sq = sq;
+  if (v.fixed_points[p]) {
+    out.summary[p] = sm;
+    return;
+  }
+  // scaled_gradient_inf_norm (schur/assembly.rs:1071-1090)
+  {
+    double scale = fmax(fmax(fmax(0.0, V[0]), V[2]), V[5]);
+    double gn;
+    if (!(isfinite(scale) && scale > 0.0)) {
+      gn = (gp[0] == 0.0 && gp[1] == 0.0 && gp[2] == 0.0) ? 0.0 : INFINITY;
+    } else {
+      double fl = 64.0 * kEps * scale;
+      gn = fmax(fmax(fabs(gp[0]) / sqrt(fmax(V[0], fl)), fabs(gp[1]) / sqrt(fmax(V[2], fl))),
+                fabs(gp[2]) / sqrt(fmax(V[5], fl)));
+    }
+    sm.grad_norm = gn;
+  }
+  double damped[6], inv[6];
+  if (!point_factor(V, lambda, damped, inv)) {
+    sm.invalid = 1;
+    if (lambda == 0.0) {
+      sm.weak = 1;
+      sm.min_rcond = 0.0;
+    }
+    out.summary[p] = sm;
+    return;
+  }
+  double dd[3];
+  point_damping_diagonal(V, dd);
+  out.ddiag[3 * (size_t)p] = dd[0];
+  out.ddiag[3 * (size_t)p + 1] = dd[1];
+  out.ddiag[3 * (size_t)p + 2] = dd[2];
+  if (lambda == 0.0) {
+    double rc = point_rcond(V, inv);
+    sm.min_rcond = rc;
+    if (rc <= 64.0 * kEps * 3.0) sm.weak = 1;
+  }
+  double igv[3];
+  sym3_apply(inv, gp, igv);
+  sm.point_red = 0.5 * (gp[0] * igv[0] + gp[1] * igv[1] + gp[2] * igv[2]);
+  for (int k = 0; k < 6; ++k) vi[k] = inv[k];
+  ig[0] = igv[0];
+  ig[1] = igv[1];
+  ig[2] = igv[2];
+  out.summary[p] = sm;
+}
+
+// ----------------------------------------------------------------------------------------------
+// K2: camera-side block reductions (deterministic chunked segmented sums)
+// ----------------------------------------------------------------------------------------------
+// An entity is (observation, segment): segment 0 = pose columns, 1 = intrinsic columns.
+struct BlockTables {
+  int nblocks;
+  const int* blk_off;        // parameter offset of each block
+  const int* blk_dim;        // dimension of each block
+  const int* blk_col;        // column of the block inside an observation's 9-column Jacobian (0 or pose dim)
+  const int* blk_edge;       // pose blocks: intrinsic block index of the camera's group with dim > 0, else -1
+  const uint32_t* ent;       // entity list, block-major: obs * 2 + seg
+  const uint32_t* ent_point; // point of each entity (same order)
+  int nchunks;
+  const int* chunk_block;    // block of each chunk
+  const int* chunk_col;      // Jacobian column of the block's segment for every entity of the chunk
+  const uint32_t* chunk_begin;  // into ent
+  const uint32_t* chunk_end;
+  const int* blk_chunk_begin;   // per block: first chunk
+  const int* blk_chunk_end;
+};
+
+// Assembly record per chunk: U lower (21), g (6), reduced g (6), diag (6), edge (18), coupling lower (21)
+constexpr int kAsmRec = 21 + 6 + 6 + 6 + 18 + 21;
+
+template <typename T>
+__global__ void __launch_bounds__(32) k_block_chunks(BlockTables bt, LinOut<T> lin, const int* obs_intr_col,
+                                                     double* chunk_out) {
+  int c = blockIdx.x;
+  if (c >= bt.nchunks) return;
+  int lane = threadIdx.x;
+  int b = bt.chunk_block[c];
+  int d = bt.blk_dim[b];
+  int col = bt.chunk_col[c];
+  bool has_edge = bt.blk_edge[b] >= 0;
+  double U[21], gfull[6], gred[6], dg[6], E[18], Cpl[21];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) {
+    U[k] = 0.0;
+    Cpl[k] = 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) gfull[k] = gred[k] = dg[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 18; ++k) E[k] = 0.0;
+  for (uint32_t i = bt.chunk_begin[c] + lane; i < bt.chunk_end[c]; i += 32) {
+    uint32_t e = bt.ent[i];
+    uint32_t o = e >> 1;
+    uint32_t p = bt.ent_point[i];
+    const T* jc = lin.jc + (size_t)18 * o;
+    double a0[6], a1[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      a0[k] = k < d ? (double)jc[col + k] : 0.0;
+      a1[k] = k < d ? (double)jc[9 + col + k] : 0.0;
+    }
+    double r0 = lin.rw[2 * o], r1 = lin.rw[2 * o + 1];
+    const T* jp = lin.jp + (size_t)6 * o;
+    double p0[3] = {(double)jp[0], (double)jp[1], (double)jp[2]};
+    double p1[3] = {(double)jp[3], (double)jp[4], (double)jp[5]};
+    const double* ig = lin.ig + 3 * (size_t)p;
+    // reduced residual: r_w - Jp (Vhat^-1 g_p)
+    double q0 = r0 - (p0[0] * ig[0] + p0[1] * ig[1] + p0[2] * ig[2]);
+    double q1 = r1 - (p1[0] * ig[0] + p1[1] * ig[1] + p1[2] * ig[2]);
+    // A = Jp Vhat^-1 Jp^T (2x2)
+    const double* vi = lin.vinv + 6 * (size_t)p;
+    double t0[3], t1[3];
+    sym3_apply(vi, p0, t0);
+    sym3_apply(vi, p1, t1);
+    double A00 = p0[0] * t0[0] + p0[1] * t0[1] + p0[2] * t0[2];
+    double A01 = p0[0] * t1[0] + p0[1] * t1[1] + p0[2] * t1[2];
+    double A11 = p1[0] * t1[0] + p1[1] * t1[1] + p1[2] * t1[2];
+    int idx = 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      gfull[r] += a0[r] * r0 + a1[r] * r1;
+      gred[r] += a0[r] * q0 + a1[r] * q1;
+      dg[r] += a0[r] * a0[r] + a1[r] * a1[r];
+      // (A a)_r terms for coupling: c_r = [a0_r a1_r] A
+      double c0 = a0[r] * A00 + a1[r] * A01;
+      double c1 = a0[r] * A01 + a1[r] * A11;
+#pragma unroll
+      for (int s2 = 0; s2 <= r; ++s2) {
+        U[idx] += a0[r] * a0[s2] + a1[r] * a1[s2];
+        Cpl[idx] += c0 * a0[s2] + c1 * a1[s2];
+        ++idx;
+      }
+    }
+    if (has_edge) {
+      int icol = obs_intr_col[o];  // column of the intrinsic segment (pose dim), idim in upper bits
+      int id = icol >> 8;
+      icol &= 0xff;
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          if (k < id) E[3 * r + k] += a0[r] * (double)jc[icol + k] + a1[r] * (double)jc[9 + icol + k];
+    }
+  }
+  double* rec = chunk_out + (size_t)kAsmRec * c;
+#pragma unroll
+  for (int k = 0; k < 21; ++k) {
+    double s = warp_sum(U[k]);
+    double t = warp_sum(Cpl[k]);
+    if (lane == 0) {
+      rec[k] = s;
+      rec[57 + k] = t;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double a = warp_sum(gfull[k]), bb = warp_sum(gred[k]), cc = warp_sum(dg[k]);
+    if (lane == 0) {
+      rec[21 + k] = a;
+      rec[27 + k] = bb;
+      rec[33 + k] = cc;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 18; ++k) {
+    double s = warp_sum(E[k]);
+    if (lane == 0) rec[39 + k] = s;
+  }
+}
+
+// Per block: sum its chunk records in chunk order -> block assembly record.
+__global__ void k_block_finalize(BlockTables bt, const double* chunk_out, double* blk_out) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.nblocks) return;
+  double acc[kAsmRec];
+  for (int k = 0; k < kAsmRec; ++k) acc[k] = 0.0;
+  for (int c = bt.blk_chunk_begin[b]; c < bt.blk_chunk_end[b]; ++c) {
+    const double* rec = chunk_out + (size_t)kAsmRec * c;
+    for (int k = 0; k < kAsmRec; ++k) acc[k] += rec[k];
+  }
+  double* out = blk_out + (size_t)kAsmRec * b;
+  for (int k = 0; k < kAsmRec; ++k) out[k] = acc[k];
+}
+
+// Scatter block records into the D-vectors (g, reduced g, diag) — one thread per block.
+__global__ void k_block_vectors(BlockTables bt, const double* blk_out, double* gfull, double* gred, double* diag,
+                                int* clamp_count, double* diag_minmax) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.nblocks) return;
+  const double* rec = blk_out + (size_t)kAsmRec * b;
+  int o = bt.blk_off[b], d = bt.blk_dim[b];
+  double s = 0.0;
+  for (int k = 0; k < d; ++k) {
+    gfull[o + k] = rec[21 + k];
+    gred[o + k] = rec[27 + k];
+    s = fmax(s, rec[33 + k]);
+  }
+  // raw diagonal extrema before clamping (finalize_assembly, schur/assembly.rs:701-712)
+  double mn = INFINITY, mx = 0.0;
+  for (int k = 0; k < d; ++k) {
+    mn = fmin(mn, rec[33 + k]);
+    mx = fmax(mx, rec[33 + k]);
+  }
+  diag_minmax[2 * b] = mn;
+  diag_minmax[2 * b + 1] = mx;
+  // clamp_damping_block (schur/assembly.rs:744-766)
+  double fl = s > 0.0 ? 64.0 * kEps * s : 1.0;
+  int cl = 0;
+  for (int k = 0; k < d; ++k) {
+    double v = rec[33 + k];
+    if (v < fl) {
+      v = fl;
+      ++cl;
+    }
+    diag[o + k] = v;
+  }
+  clamp_count[b] = cl;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Explicit Schur blocks via pair lists (Direct / dense S and cross-pair preconditioner terms)
+// ----------------------------------------------------------------------------------------------
+struct PairTables {
+  int ngroups;
+  const int* grp_row;        // row block
+  const int* grp_col;        // column block
+  const uint32_t* grp_begin; // into pairs
+  const uint32_t* grp_end;
+  const uint32_t* pair_a;    // entity (obs*2+seg) on the row side
+  const uint32_t* pair_b;    // entity on the column side
+  const uint32_t* pair_p;    // point
+};
+
+// out[g] (36 values, row-major d_row x d_col) = sum over pairs of Jc_a^T (Jp_a Vhat^-1 Jp_b^T) Jc_b
+template <typename T>
+__global__ void __launch_bounds__(32) k_pairs(PairTables pt, BlockTables bt, LinOut<T> lin, const int* seg_col,
+                                              double* out) {
+  int gidx = blockIdx.x;
+  if (gidx >= pt.ngroups) return;
+  int lane = threadIdx.x;
+  int rb = pt.grp_row[gidx], cb = pt.grp_col[gidx];
+  int dr = bt.blk_dim[rb], dc = bt.blk_dim[cb];
+  double acc[36];
+#pragma unroll
+  for (int k = 0; k < 36; ++k) acc[k] = 0.0;
+  for (uint32_t i = pt.grp_begin[gidx] + lane; i < pt.grp_end[gidx]; i += 32) {
+    uint32_t ea = pt.pair_a[i], eb = pt.pair_b[i], p = pt.pair_p[i];
+    uint32_t oa = ea >> 1, ob = eb >> 1;
+    int ca = seg_col[ea], cbcol = seg_col[eb];
+    const T* jpa = lin.jp + (size_t)6 * oa;
+    const T* jpb = lin.jp + (size_t)6 * ob;
+    const double* vi = lin.vinv + 6 * (size_t)p;
+    double pa0[3] = {(double)jpa[0], (double)jpa[1], (double)jpa[2]}, pa1[3] = {(double)jpa[3], (double)jpa[4], (double)jpa[5]};
+    double pb0[3] = {(double)jpb[0], (double)jpb[1], (double)jpb[2]}, pb1[3] = {(double)jpb[3], (double)jpb[4], (double)jpb[5]};
+    double t0[3], t1[3];
+    sym3_apply(vi, pb0, t0);
+    sym3_apply(vi, pb1, t1);
+    double A00 = pa0[0] * t0[0] + pa0[1] * t0[1] + pa0[2] * t0[2];
+    double A01 = pa0[0] * t1[0] + pa0[1] * t1[1] + pa0[2] * t1[2];
+    double A10 = pa1[0] * t0[0] + pa1[1] * t0[1] + pa1[2] * t0[2];
+    double A11 = pa1[0] * t1[0] + pa1[1] * t1[1] + pa1[2] * t1[2];
+    const T* ja = lin.jc + (size_t)18 * oa;
+    const T* jb = lin.jc + (size_t)18 * ob;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r >= dr) break;
+      double a0 = (double)ja[ca + r], a1 = (double)ja[9 + ca + r];
+      double c0 = a0 * A00 + a1 * A10, c1 = a0 * A01 + a1 * A11;
+#pragma unroll
+      for (int s2 = 0; s2 < 6; ++s2) {
+        if (s2 >= dc) break;
+        acc[6 * r + s2] += c0 * (double)jb[cbcol + s2] + c1 * (double)jb[9 + cbcol + s2];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 36; ++k) {
+    double s = warp_sum(acc[k]);
+    if (lane == 0) out[(size_t)36 * gidx + k] = s;
+  }
+}
+
+// Dense S = U blocks + edges - pair sums + lambda * diag  (row-major D x D, both triangles)
+__global__ void k_dense_from_blocks(BlockTables bt, const double* blk_out, int D, double* S) {
+  int b = blockIdx.x;
+  if (b >= bt.nblocks) return;
+  const double* rec = blk_out + (size_t)kAsmRec * b;
+  int o = bt.blk_off[b], d = bt.blk_dim[b];
+  if (threadIdx.x == 0) {
+    int idx = 0;
+    for (int r = 0; r < 6; ++r)
+      for (int c = 0; c <= r; ++c, ++idx) {
+        if (r >= d || c >= d) continue;
+        S[(size_t)(o + r) * D + (o + c)] += rec[idx];
+        if (r != c) S[(size_t)(o + c) * D + (o + r)] += rec[idx];
+      }
+    int eb = bt.blk_edge[b];
+    if (eb >= 0) {
+      int io = bt.blk_off[eb], id = bt.blk_dim[eb];
+      for (int r = 0; r < d; ++r)
+        for (int k = 0; k < id; ++k) {
+          double v = rec[39 + 3 * r + k];
+          S[(size_t)(o + r) * D + (io + k)] += v;
+          S[(size_t)(io + k) * D + (o + r)] += v;
+        }
+    }
+  }
+}
+
+__global__ void k_dense_pairs(PairTables pt, BlockTables bt, const double* pair_out, int D, double* S) {
+  int gidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gidx >= pt.ngroups) return;
+  int rb = pt.grp_row[gidx], cb = pt.grp_col[gidx];
+  int ro = bt.blk_off[rb], co = bt.blk_off[cb], dr = bt.blk_dim[rb], dc = bt.blk_dim[cb];
+  const double* v = pair_out + (size_t)36 * gidx;
+  // groups are unique per (row, col) with row >= col; diagonal groups hold both orientations
+  for (int r = 0; r < dr; ++r)
+    for (int c = 0; c < dc; ++c) {
+      double x = v[6 * r + c];
+      if (rb == cb) {
+        S[(size_t)(ro + r) * D + (co + c)] -= x;
+      } else {
+        S[(size_t)(ro + r) * D + (co + c)] -= x;
+        S[(size_t)(co + c) * D + (ro + r)] -= x;
+      }
+    }
+}
+
+__global__ void k_dense_add_diag(int D, const double* diag, double lambda, double* S) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < D) S[(size_t)i * D + i] += lambda * diag[i];
+}
+
+// Dense Cholesky (lower, in place) by one CTA, left-looking: every entry L[i][j] is one thread's
+// sequential dot over k < j, so the factor does not depend on the launch shape. status[0] = 1 on
+// success (every pivot finite and positive).
+__global__ void __launch_bounds__(1024) k_dense_cholesky(int D, double* A, int* status) {
+  __shared__ int ok;
+  __shared__ double piv;
+  if (threadIdx.x == 0) ok = 1;
+  __syncthreads();
+  for (int j = 0; j < D; ++j) {
+    if (threadIdx.x == 0) {
+      double s = A[(size_t)j * D + j];
+      for (int k = 0; k < j; ++k) s -= A[(size_t)j * D + k] * A[(size_t)j * D + k];
+      if (!(isfinite(s) && s > 0.0)) {
+        ok = 0;
+      } else {
+        piv = sqrt(s);
+        A[(size_t)j * D + j] = piv;
+      }
+    }
+    __syncthreads();
+    if (!ok) break;
+    double d = piv;
+    for (int i = j + 1 + threadIdx.x; i < D; i += blockDim.x) {
+      double v = A[(size_t)i * D + j];
+      for (int k = 0; k < j; ++k) v -= A[(size_t)i * D + k] * A[(size_t)j * D + k];
+      A[(size_t)i * D + j] = v / d;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) status[0] = ok;
+}
+
+// Solve L L^T x = b in place: row-oriented forward and backward substitution, one thread, so the
+// summation order is the textbook sequential one.
+__global__ void k_dense_solve(int D, const double* L, double* x) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i < D; ++i) {
+    double v = x[i];
+    for (int k = 0; k < i; ++k) v -= L[(size_t)i * D + k] * x[k];
+    x[i] = v / L[(size_t)i * D + i];
+  }
+  for (int i = D - 1; i >= 0; --i) {
+    double v = x[i];
+    for (int k = i + 1; k < D; ++k) v -= L[(size_t)k * D + i] * x[k];
+    x[i] = v / L[(size_t)i * D + i];
+  }
+}
+
+// y = S x for dense S (one warp per row), deterministic per-row order
+__global__ void k_dense_matvec(int D, const double* S, const double* x, double* y) {
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (row >= D) return;
+  double s = 0.0;
+  for (int c = lane; c < D; c += 32) s += S[(size_t)row * D + c] * x[c];
+  s = warp_sum(s);
+  if (lane == 0) y[row] = s;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Matrix-free reduced camera system product (implicit Schur)
+// ----------------------------------------------------------------------------------------------
+// Pass 1 (point-major): e_o = Jc_o x_o; z_p = Vhat^-1 sum_o Jp_o^T e_o; f_o = e_o - Jp_o z_p
+template <typename T>
+__global__ void __launch_bounds__(128) k_mv_points(DevView v, LinOut<T> lin, const double* x, T* f) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= v.P) return;
+  uint32_t o0 = v.pt_off[p], o1 = v.pt_off[p + 1];
+  T b0 = 0, b1 = 0, b2 = 0;
+  // first pass: accumulate b
+  for (uint32_t o = o0; o < o1; ++o) {
+    int cam = v.obs_cam[o];
+    int pd = v.pose_dim[cam], po = v.pose_off[cam];
+    const T* jc = lin.jc + (size_t)18 * o;
+    T e0 = 0, e1 = 0;
+    for (int k = 0; k < pd; ++k) {
+      T xv = (T)x[po + k];
+      e0 += jc[k] * xv;
+      e1 += jc[9 + k] * xv;
+    }
+    if (v.self_cal) {
+      int g = v.cam_group[cam];
+      int id = v.intr_dim[g], io = v.intr_off[g];
+      for (int k = 0; k < id; ++k) {
+        T xv = (T)x[io + k];
+        e0 += jc[pd + k] * xv;
+        e1 += jc[9 + pd + k] * xv;
+      }
+    }
+    const T* jp = lin.jp + (size_t)6 * o;
+    b0 += jp[0] * e0 + jp[3] * e1;
+    b1 += jp[1] * e0 + jp[4] * e1;
+    b2 += jp[2] * e0 + jp[5] * e1;
+    f[2 * o] = e0;
+    f[2 * o + 1] = e1;
+  }
+  const double* vi = lin.vinv + 6 * (size_t)p;
+  T z0 = (T)vi[0] * b0 + (T)vi[1] * b1 + (T)vi[3] * b2;
+  T z1 = (T)vi[1] * b0 + (T)vi[2] * b1 + (T)vi[4] * b2;
+  T z2 = (T)vi[3] * b0 + (T)vi[4] * b1 + (T)vi[5] * b2;
+  for (uint32_t o = o0; o < o1; ++o) {
+    const T* jp = lin.jp + (size_t)6 * o;
+    f[2 * o] -= jp[0] * z0 + jp[1] * z1 + jp[2] * z2;
+    f[2 * o + 1] -= jp[3] * z0 + jp[4] * z1 + jp[5] * z2;
+  }
+}
+
+// Pass 2 (block chunks): partial y_b = sum_e Jc_e^T f_o
+template <typename T>
+__global__ void __launch_bounds__(32) k_mv_chunks(BlockTables bt, LinOut<T> lin, const T* f, double* chunk_y) {
+  int c = blockIdx.x;
+  if (c >= bt.nchunks) return;
+  int lane = threadIdx.x;
+  int b = bt.chunk_block[c];
+  int d = bt.blk_dim[b];
+  int col = bt.chunk_col[c];
+  T acc[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t i = bt.chunk_begin[c] + lane; i < bt.chunk_end[c]; i += 32) {
+    uint32_t o = bt.ent[i] >> 1;
+    const T* jc = lin.jc + (size_t)18 * o;
+    T f0 = f[2 * o], f1 = f[2 * o + 1];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (k < d) acc[k] += jc[col + k] * f0 + jc[9 + col + k] * f1;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double s = warp_sum((double)acc[k]);
+    if (lane == 0) chunk_y[(size_t)6 * c + k] = s;
+  }
+}
+
+// y_b = sum of chunk partials (chunk order) + lambda * diag_b x_b
+__global__ void k_mv_finalize(BlockTables bt, const double* chunk_y, const double* diag, double lambda,
+                              const double* x, double* y) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.nblocks) return;
+  int o = bt.blk_off[b], d = bt.blk_dim[b];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = bt.blk_chunk_begin[b]; c < bt.blk_chunk_end[b]; ++c)
+    for (int k = 0; k < d; ++k) acc[k] += chunk_y[(size_t)6 * c + k];
+  for (int k = 0; k < d; ++k) y[o + k] = acc[k] + lambda * diag[o + k] * x[o + k];
+}
+
+// ----------------------------------------------------------------------------------------------
+// Block-Jacobi preconditioner (FP64): P_b = U_bb + lambda D_b - C_b - cross pairs
+// ----------------------------------------------------------------------------------------------
+__global__ void k_block_factor(BlockTables bt, const double* blk_out, const double* diag, double lambda,
+                               const double* cross, const int* blk_cross_begin, const int* blk_cross_end,
+                               double* factor, int* fail) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.nblocks) return;
+  int d = bt.blk_dim[b], o = bt.blk_off[b];
+  const double* rec = blk_out + (size_t)kAsmRec * b;
+  double m[6][6];
+  int idx = 0;
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c <= r; ++c, ++idx) {
+      double v = rec[idx] - rec[57 + idx];
+      m[r][c] = v;
+      m[c][r] = v;
+    }
+  for (int g = blk_cross_begin[b]; g < blk_cross_end[b]; ++g) {
+    const double* cv = cross + (size_t)36 * g;
+    // a diagonal pair group holds each ordered cross pair once: add both orientations
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c) m[r][c] -= cv[6 * r + c] + cv[6 * c + r];
+  }
+  for (int k = 0; k < d; ++k) m[k][k] += lambda * diag[o + k];
+  // PackedCameraBlockFactor::factor (retained/block.rs:171-218)
+  double* F = factor + 42 * (size_t)b;  // 36 lower + 6 scale
+  double ds = 0.0;
+  for (int i = 0; i < d; ++i) ds = fmax(ds, m[i][i]);
+  if (!(isfinite(ds) && ds > 0.0)) {
+    fail[b] = 1;
+    return;
+  }
+  double fl = 64.0 * kEps * ds;
+  double sc[6];
+  for (int i = 0; i < d; ++i) sc[i] = sqrt(fmax(m[i][i], fl));
+  double L[6][6];
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c <= r; ++c) {
+      double v = m[r][c] / (sc[r] * sc[c]);
+      for (int k = 0; k < c; ++k) v -= L[r][k] * L[c][k];
+      if (r == c) {
+        if (!(isfinite(v) && v > 64.0 * kEps)) {
+          fail[b] = 1;
+          return;
+        }
+        L[r][c] = sqrt(v);
+      } else {
+        L[r][c] = v / L[c][c];
+      }
+    }
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 6; ++c) F[6 * r + c] = (r < d && c <= r) ? L[r][c] : 0.0;
+  for (int i = 0; i < 6; ++i) F[36 + i] = i < d ? sc[i] : 1.0;
+  fail[b] = 0;
+}
+
+__global__ void k_block_precond(BlockTables bt, const double* factor, const double* r, double* z) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.nblocks) return;
+  int d = bt.blk_dim[b], o = bt.blk_off[b];
+  const double* F = factor + 42 * (size_t)b;
+  double s[6];
+  for (int i = 0; i < d; ++i) {
+    double v = r[o + i] / F[36 + i];
+    for (int k = 0; k < i; ++k) v -= F[6 * i + k] * s[k];
+    s[i] = v / F[6 * i + i];
+  }
+  for (int i = d - 1; i >= 0; --i) {
+    double v = s[i];
+    for (int k = i + 1; k < d; ++k) v -= F[6 * k + i] * s[k];
+    s[i] = v / F[6 * i + i];
+  }
+  for (int i = 0; i < d; ++i) z[o + i] = s[i] / F[36 + i];
+}
+
+__global__ void k_axpy2(int n, double alpha, const double* d, const double* q, double* x, double* r) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    x[i] += alpha * d[i];
+    r[i] -= alpha * q[i];
+  }
+}
+__global__ void k_xpby(int n, const double* z, double beta, double* d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = z[i] + beta * d[i];
+}
+__global__ void k_neg_copy(int n, const double* a, double* b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = -a[i];
+}
+__global__ void k_residual_update(int n, const double* g, const double* q, double* r) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = -g[i] - q[i];
+}
+__global__ void k_scale(int n, double s, double* x) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= s;
+}
+
+// ----------------------------------------------------------------------------------------------
+// K4: step cap, retraction, candidate points
+// ----------------------------------------------------------------------------------------------
+// Per camera: max of the rotation-part norm and the rest (limit_camera_step, optimizer.rs:677-702)
+__global__ void k_step_block_norm(int ncam, const int* pose_off, const int* pose_dim, const double* step,
+                                  double* out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncam) return;
+  int d = pose_dim[c], o = pose_off[c];
+  if (d == 0) {
+    out[c] = 0.0;
+    return;
+  }
+  int fd = d < 3 ? d : 3;
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = 0; k < fd; ++k) s1 += step[o + k] * step[o + k];
+  for (int k = fd; k < d; ++k) s2 += step[o + k] * step[o + k];
+  out[c] = fmax(sqrt(s1), sqrt(s2));
+}
+
+__device__ __forceinline__ void exp_so3_dev(const double w[3], double R[9]) {
+  // numerics/manifold/so3.rs:254-265 with matrix_polynomial (:420-423)
+  double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  double th = sqrt(th2);
+  double a[3], lin, quad;
+  if (th < 1e-10) {
+    a[0] = w[0];
+    a[1] = w[1];
+    a[2] = w[2];
+    lin = 1.0;
+    quad = 0.5;
+  } else {
+    a[0] = w[0] / th;
+    a[1] = w[1] / th;
+    a[2] = w[2] / th;
+    lin = sin(th);
+    quad = 1.0 - cos(th);
+  }
+  double K[3][3] = {{0.0, -a[2], a[1]}, {a[2], 0.0, -a[0]}, {-a[1], a[0], 0.0}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double k2 = K[i][0] * K[0][j] + K[i][1] * K[1][j] + K[i][2] * K[2][j];
+      R[3 * i + j] = (i == j ? 1.0 : 0.0) + K[i][j] * lin + k2 * quad;
+    }
+}
+
+// retract_poses (optimizer.rs:376-424) and retract_cameras (self_calibration/optimizer.rs:565-587)
+__global__ void k_retract(DevView v, int ng, const double* step, Gauge g, const double* cur_pose,
+                          const double* cur_groups, double* cand_pose, double* cand_groups) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < v.ncam) {
+    const double* P = cur_pose + 12 * c;
+    double* Q = cand_pose + 12 * c;
+    int d = v.pose_dim[c], o = v.pose_off[c];
+    if (d == 0) {
+      for (int k = 0; k < 12; ++k) Q[k] = P[k];
+    } else {
+      double w[3] = {step[o], step[o + 1], step[o + 2]};
+      double U[9];
+      exp_so3_dev(w, U);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += U[3 * i + k] * P[3 * k + j];
+          Q[3 * i + j] = s;
+        }
+      if (c == g.fixed_cam) {
+        // retract_s2 (numerics/manifold.rs:133-147)
+        double d0 = step[o + 3], d1 = step[o + 4];
+        double vv[3] = {g.b0[0] * d0 + g.b1[0] * d1, g.b0[1] * d0 + g.b1[1] * d1, g.b0[2] * d0 + g.b1[2] * d1};
+        double th = sqrt(vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]);
+        double tn = sqrt(g.dir[0] * g.dir[0] + g.dir[1] * g.dir[1] + g.dir[2] * g.dir[2]);
+        double tv[3] = {g.dir[0] / tn, g.dir[1] / tn, g.dir[2] / tn};
+        double out[3];
+        if (th < 1e-10) {
+          double s[3] = {tv[0] + vv[0], tv[1] + vv[1], tv[2] + vv[2]};
+          double n = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+          out[0] = s[0] / n;
+          out[1] = s[1] / n;
+          out[2] = s[2] / n;
+        } else {
+          double cs = cos(th), sn = sin(th) / th;
+          for (int k = 0; k < 3; ++k) out[k] = tv[k] * cs + vv[k] * sn;
+        }
+        for (int k = 0; k < 3; ++k) Q[9 + k] = g.baseline * out[k];
+      } else {
+        for (int k = 0; k < 3; ++k) Q[9 + k] = P[9 + k] + g.scene * step[o + 3 + k];
+      }
+    }
+  }
+  if (v.self_cal && c < ng) {
+    const double* G = cur_groups + 3 * c;
+    double* H = cand_groups + 3 * c;
+    int d = v.intr_dim[c], o = v.intr_off[c];
+    double dl[3] = {0, 0, 0};
+    for (int k = 0; k < d; ++k) dl[k] = step[o + k];
+    if (d == 0) {
+      H[0] = G[0];
+      H[1] = G[1];
+      H[2] = G[2];
+    } else {
+      H[0] = G[0] * exp(dl[0]);
+      H[1] = G[1] + dl[1];
+      H[2] = G[2] + dl[2];
+    }
+  }
+}
+
+// Admitted track cost (schur/point.rs:705-728): returns false when a projection fails or the
+// geometry is not admitted.
+__device__ bool admitted_cost(const DevView& v, const double* pose, const double* groups, const double X[3], int p,
+                              const LossDev& loss, double scene, int admission, double* cost) {
+  TrackGeometryDev geo;
+  geo.init(scene);
+  double total = 0.0;
+  for (uint32_t o = v.pt_off[p]; o < v.pt_off[p + 1]; ++o) {
+    int cam = v.obs_cam[o];
+    const double* P = pose + 12 * cam;
+    double xc[3];
+    for (int i = 0; i < 3; ++i) xc[i] = P[3 * i] * X[0] + P[3 * i + 1] * X[1] + P[3 * i + 2] * X[2] + P[9 + i];
+    double r[2], J[2][3], Ji[2][3];
+    if (!project_obs(v, groups, o, xc, r, J, Ji)) return false;
+    // rotate_transposed(R, camera point)
+    double off[3];
+    for (int j = 0; j < 3; ++j) off[j] = P[j] * xc[0] + P[3 + j] * xc[1] + P[6 + j] * xc[2];
+    geo.push(off[0], off[1], off[2]);
+    total += loss.cost(sqrt(r[0] * r[0] + r[1] * r[1]));
+  }
+  bool ok = admission == 0 ? true : (admission == 1 ? !geo.collapsed() : !geo.degenerate());
+  if (!ok) return false;
+  *cost = total;
+  return true;
+}
+
+struct CandidateOut {
+  double cost, step_sq, damping, failed;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_candidate_points(DevView v, LinOut<T> lin, const double* step,
+                                                          DevState cur, DevState cand, Gauge g, LossDev loss,
+                                                          RedVec<4>* out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= v.P) return;
+  double X[3] = {cur.points[3 * p], cur.points[3 * p + 1], cur.points[3 * p + 2]};
+  RedVec<4> res;
+  res.v[0] = res.v[1] = res.v[2] = res.v[3] = 0.0;
+  if (v.fixed_points[p]) {
+    double c;
+    cand.points[3 * p] = X[0];
+    cand.points[3 * p + 1] = X[1];
+    cand.points[3 * p + 2] = X[2];
+    if (!admitted_cost(v, cand.pose, cand.groups, X, p, loss, 0.0, 0, &c))
+      res.v[3] = 1.0;
+    else
+      res.v[0] = c;
+    out[p] = res;
+    return;
+  }
+  // back-substitution: dp = -(Vhat^-1 g_p + Vhat^-1 sum_o Jp_o^T Jc_o dc_o)  (schur/point.rs:537-596)
+  double b0 = 0, b1 = 0, b2 = 0;
+  for (uint32_t o = v.pt_off[p]; o < v.pt_off[p + 1]; ++o) {
+    int cam = v.obs_cam[o];
+    int pd = v.pose_dim[cam], po = v.pose_off[cam];
+    const T* jc = lin.jc + (size_t)18 * o;
+    double e0 = 0, e1 = 0;
+    for (int k = 0; k < pd; ++k) {
+      e0 += (double)jc[k] * step[po + k];
+      e1 += (double)jc[9 + k] * step[po + k];
+    }
+    if (v.self_cal) {
+      int gi = v.cam_group[cam];
+      int id = v.intr_dim[gi], io = v.intr_off[gi];
+      for (int k = 0; k < id; ++k) {
+        e0 += (double)jc[pd + k] * step[io + k];
+        e1 += (double)jc[9 + pd + k] * step[io + k];
+      }
+    }
+    const T* jp = lin.jp + (size_t)6 * o;
+    b0 += (double)jp[0] * e0 + (double)jp[3] * e1;
+    b1 += (double)jp[1] * e0 + (double)jp[4] * e1;
+    b2 += (double)jp[2] * e0 + (double)jp[5] * e1;
+  }
+  const double* vi = lin.vinv + 6 * (size_t)p;
+  const double* ig = lin.ig + 3 * (size_t)p;
+  double bb[3] = {b0, b1, b2}, z[3];
+  sym3_apply(vi, bb, z);
+  double sp[3] = {-(ig[0] + z[0]), -(ig[1] + z[1]), -(ig[2] + z[2])};
+  double st[3] = {X[0] + g.scene * sp[0], X[1] + g.scene * sp[1], X[2] + g.scene * sp[2]};
+  // candidate_rule (point_geometry.rs:110-130)
+  double c;
+  bool moved = false, have = false;
+  if (admitted_cost(v, cand.pose, cand.groups, st, p, loss, g.scene, 2, &c)) {
+    moved = true;
+    have = true;
+  } else if (admitted_cost(v, cand.pose, cand.groups, X, p, loss, g.scene, 1, &c)) {
+    have = true;
+  } else {
+    double c2;
+    if (!admitted_cost(v, cur.pose, cur.groups, X, p, loss, g.scene, 1, &c2)) {
+      if (admitted_cost(v, cand.pose, cand.groups, X, p, loss, g.scene, 0, &c)) have = true;
+    }
+  }
+  if (!have) {
+    res.v[3] = 1.0;
+    out[p] = res;
+    return;
+  }
+  const double* P = moved ? st : X;
+  cand.points[3 * p] = P[0];
+  cand.points[3 * p + 1] = P[1];
+  cand.points[3 * p + 2] = P[2];
+  res.v[0] = c;
+  if (moved) {
+    res.v[1] = sp[0] * sp[0] + sp[1] * sp[1] + sp[2] * sp[2];
+    const double* dd = lin.ddiag + 3 * (size_t)p;
+    res.v[2] = dd[0] * sp[0] * sp[0] + dd[1] * sp[1] * sp[1] + dd[2] * sp[2] * sp[2];
+  }
+  out[p] = res;
+}
+
+// Track-cost metrics at the current state (schur/diagnostics.rs:18-44), per point: cost, squared residual.
+__global__ void k_metrics(DevView v, DevState s, LossDev loss, RedVec<3>* out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= v.P) return;
+  RedVec<3> r;
+  r.v[0] = r.v[1] = r.v[2] = 0.0;
+  double X[3] = {s.points[3 * p], s.points[3 * p + 1], s.points[3 * p + 2]};
+  for (uint32_t o = v.pt_off[p]; o < v.pt_off[p + 1]; ++o) {
+    const double* P = s.pose + 12 * v.obs_cam[o];
+    double xc[3];
+    for (int i = 0; i < 3; ++i) xc[i] = P[3 * i] * X[0] + P[3 * i + 1] * X[1] + P[3 * i + 2] * X[2] + P[9 + i];
+    double rr[2], J[2][3], Ji[2][3];
+    if (!project_obs(v, s.groups, o, xc, rr, J, Ji)) {
+      r.v[2] = 1.0;
+      continue;
+    }
+    double rn = sqrt(rr[0] * rr[0] + rr[1] * rr[1]);
+    r.v[0] += loss.cost(rn);
+    r.v[1] += rn * rn;
+  }
+  out[p] = r;
+}
+
+// Observations whose measurement cannot be inverted (kernel/multi_view/model.rs:350-364).
+__global__ void k_noninvertible(DevView v, int N, const double* groups, RedVec<1>* out) {
+  int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= N) return;
+  double bad = 0.0;
+  double mx = v.obs_px[2 * o], my = v.obs_px[2 * o + 1];
+  if (v.self_cal) {
+    RadialDev c = make_radial(groups + 3 * v.cam_group[v.obs_cam[o]]);
+    bad = radial_bearing_ok(c, mx, my) ? 0.0 : 1.0;
+  } else if (!v.pixel_model) {
+    const FixedCameraDev& m = v.models[v.obs_model[o]];
+    bad = m.remove_distortion((mx - m.cx) / m.fx, (my - m.cy) / m.fy) ? 0.0 : 1.0;
+  }
+  out[o].v[0] = bad;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Host driver
+// ----------------------------------------------------------------------------------------------
+static inline int grid_for(size_t n, int threads) { return (int)std::max<size_t>(1, (n + threads - 1) / threads); }
+
+struct Setup {
+  // block tables (host copies)
+  std::vector<int> blk_off, blk_dim, blk_col, blk_edge;
+  std::vector<uint32_t> ent, ent_point;
+  std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
+  std::vector<uint32_t> chunk_begin, chunk_end;
+  std::vector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment
+  std::vector<int> seg_col;       // per entity id (obs*2+seg): column
+  // pair tables
+  std::vector<int> grp_row, grp_col;
+  std::vector<uint32_t> grp_begin, grp_end, pair_a, pair_b, pair_p;
+  // cross same-block pairs (preconditioner)
+  std::vector<int> xgrp_row, xgrp_col;
+  std::vector<uint32_t> xgrp_begin, xgrp_end, xpair_a, xpair_b, xpair_p;
+  std::vector<int> blk_cross_begin, blk_cross_end;
+};
+
+struct Layout {
+  int D = 0;
+  std::vector<int> pose_off, pose_dim, intr_off, intr_dim;
+  std::vector<int> cam_pose_block, group_block;  // block index or -1
+};
+
+static Layout make_layout(const NativeProblem& n) {
+  Layout L;
+  L.pose_off.resize(n.ncam);
+  L.pose_dim.resize(n.ncam);
+  int off = 0;
+  for (int c = 0; c < n.ncam; ++c) {
+    int d = (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+    L.pose_off[c] = off;
+    L.pose_dim[c] = d;
+    off += d;
+  }
+  size_t ng = n.self_cal ? n.group_dim.size() : 0;
+  L.intr_off.assign(std::max<size_t>(ng, 1), 0);
+  L.intr_dim.assign(std::max<size_t>(ng, 1), 0);
+  for (size_t g = 0; g < ng; ++g) {
+    L.intr_off[g] = off;
+    L.intr_dim[g] = n.group_dim[g];
+    off += n.group_dim[g];
+  }
+  L.D = off;
+  return L;
+}
+
+static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_pairs, Setup& S) {
+  size_t N = n.obs_cam.size(), P = n.points.size() / 3;
+  // blocks: pose blocks (camera order) then intrinsic blocks (group order)
+  std::vector<int> cam_block(n.ncam, -1), grp_block(L.intr_dim.size(), -1);
+  for (int c = 0; c < n.ncam; ++c)
+    if (L.pose_dim[c] > 0) {
+      cam_block[c] = (int)S.blk_off.size();
+      S.blk_off.push_back(L.pose_off[c]);
+      S.blk_dim.push_back(L.pose_dim[c]);
+      S.blk_col.push_back(0);
+      S.blk_edge.push_back(-1);
+    }
+  if (n.self_cal)
+    for (size_t g = 0; g < n.group_dim.size(); ++g)
+      if (L.intr_dim[g] > 0) {
+        grp_block[g] = (int)S.blk_off.size();
+        S.blk_off.push_back(L.intr_off[g]);
+        S.blk_dim.push_back(L.intr_dim[g]);
+        S.blk_col.push_back(-1);  // column depends on the observation's camera pose dim
+        S.blk_edge.push_back(-1);
+      }
+  if (n.self_cal)
+    for (int c = 0; c < n.ncam; ++c)
+      if (cam_block[c] >= 0 && grp_block[n.cam_group[c]] >= 0) S.blk_edge[cam_block[c]] = grp_block[n.cam_group[c]];
+  int nb = (int)S.blk_off.size();
+  // entity lists per block (stable in observation order)
+  S.seg_col.assign(2 * N, 0);
+  S.obs_intr_col.assign(N, 0);
+  std::vector<int> ent_block(2 * N, -1);
+  std::vector<uint32_t> counts(nb + 1, 0);
+  for (size_t o = 0; o < N; ++o) {
+    int c = n.obs_cam[o];
+    int pd = L.pose_dim[c];
+    if (cam_block[c] >= 0) {
+      ent_block[2 * o] = cam_block[c];
+      S.seg_col[2 * o] = 0;
+      counts[cam_block[c] + 1]++;
+    }
+    if (n.self_cal) {
+      int g = n.cam_group[c];
+      S.obs_intr_col[o] = (L.intr_dim[g] << 8) | pd;
+      if (grp_block[g] >= 0) {
+        ent_block[2 * o + 1] = grp_block[g];
+        S.seg_col[2 * o + 1] = pd;
+        counts[grp_block[g] + 1]++;
+      }
+    }
+  }
+  for (int b = 0; b < nb; ++b) counts[b + 1] += counts[b];
+  S.ent.assign(counts[nb], 0);
+  S.ent_point.assign(counts[nb], 0);
+  std::vector<uint32_t> fill(counts.begin(), counts.end() - 1);
+  std::vector<uint32_t> obs_point(N);
+  for (size_t p = 0; p < P; ++p)
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) obs_point[o] = (uint32_t)p;
+  for (size_t e = 0; e < 2 * N; ++e) {
+    int b = ent_block[e];
+    if (b < 0) continue;
+    uint32_t at = fill[b]++;
+    S.ent[at] = (uint32_t)e;
+    S.ent_point[at] = obs_point[e >> 1];
+  }
+  // intrinsic blocks have a per-observation column: stored via seg_col; blk_col = -1 means "use seg"
+  // For kernels that take blk_col, intrinsic blocks read their column from obs_intr_col. To keep the
+  // chunk kernel simple, split entity lists so every chunk has one column: intrinsic entities of
+  // cameras with different pose dims (0, 5, 6) are grouped by column inside the block.
+  for (int b = 0; b < nb; ++b) {
+    if (S.blk_col[b] >= 0) continue;
+    std::stable_sort(S.ent.begin() + counts[b], S.ent.begin() + counts[b + 1],
+                     [&](uint32_t a, uint32_t c) { return S.seg_col[a] < S.seg_col[c]; });
+    for (uint32_t i = counts[b]; i < counts[b + 1]; ++i) S.ent_point[i] = obs_point[S.ent[i] >> 1];
+  }
+  // chunks (never mixing columns)
+  S.blk_chunk_begin.assign(nb, 0);
+  S.blk_chunk_end.assign(nb, 0);
+  for (int b = 0; b < nb; ++b) {
+    S.blk_chunk_begin[b] = (int)S.chunk_block.size();
+    uint32_t i = counts[b];
+    while (i < counts[b + 1]) {
+      int col = S.seg_col[S.ent[i]];
+      uint32_t j = i;
+      while (j < counts[b + 1] && j - i < (uint32_t)kChunk && S.seg_col[S.ent[j]] == col) ++j;
+      S.chunk_block.push_back(b);
+      S.chunk_col.push_back(col);
+      S.chunk_begin.push_back(i);
+      S.chunk_end.push_back(j);
+      i = j;
+    }
+    S.blk_chunk_end[b] = (int)S.chunk_block.size();
+  }
+  // pair lists
+  S.blk_cross_begin.assign(nb, 0);
+  S.blk_cross_end.assign(nb, 0);
+  struct Pair {
+    int rb, cb;
+    uint32_t p, a, b;
+  };
+  std::vector<Pair> pairs, xpairs;
+  std::vector<uint32_t> ents;
+  for (size_t p = 0; p < P; ++p) {
+    if (n.fixed_points[p]) continue;
+    ents.clear();
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o)
+      for (int sgm = 0; sgm < 2; ++sgm)
+        if (ent_block[2 * o + sgm] >= 0) ents.push_back((uint32_t)(2 * o + sgm));
+    for (size_t i = 0; i < ents.size(); ++i)
+      for (size_t j = 0; j <= i; ++j) {
+        uint32_t a = ents[i], b = ents[j];
+        int ba = ent_block[a], bb = ent_block[b];
+        if (ba < bb) {
+          std::swap(a, b);
+          std::swap(ba, bb);
+        }
+        if (want_all_pairs) {
+          pairs.push_back({ba, bb, (uint32_t)p, a, b});
+          // a diagonal-block pair with distinct entities contributes both orientations
+          if (ba == bb && a != b) pairs.push_back({ba, bb, (uint32_t)p, b, a});
+        }
+        if (ba == bb && a != b) xpairs.push_back({ba, bb, (uint32_t)p, a, b});
+      }
+  }
+  auto build = [&](std::vector<Pair>& v, std::vector<int>& gr, std::vector<int>& gc, std::vector<uint32_t>& gb,
+                   std::vector<uint32_t>& ge, std::vector<uint32_t>& pa, std::vector<uint32_t>& pbv,
+                   std::vector<uint32_t>& pp) {
+    std::stable_sort(v.begin(), v.end(), [](const Pair& x, const Pair& y) {
+      return x.rb != y.rb ? x.rb < y.rb : (x.cb != y.cb ? x.cb < y.cb : false);
+    });
+    size_t i = 0;
+    while (i < v.size()) {
+      size_t j = i;
+      while (j < v.size() && v[j].rb == v[i].rb && v[j].cb == v[i].cb) ++j;
+      gr.push_back(v[i].rb);
+      gc.push_back(v[i].cb);
+      gb.push_back((uint32_t)i);
+      ge.push_back((uint32_t)j);
+      i = j;
+    }
+    pa.resize(v.size());
+    pbv.resize(v.size());
+    pp.resize(v.size());
+    for (size_t k = 0; k < v.size(); ++k) {
+      pa[k] = v[k].a;
+      pbv[k] = v[k].b;
+      pp[k] = v[k].p;
+    }
+  };
+  if (want_all_pairs) build(pairs, S.grp_row, S.grp_col, S.grp_begin, S.grp_end, S.pair_a, S.pair_b, S.pair_p);
+  build(xpairs, S.xgrp_row, S.xgrp_col, S.xgrp_begin, S.xgrp_end, S.xpair_a, S.xpair_b, S.xpair_p);
+  for (size_t gidx = 0; gidx < S.xgrp_row.size(); ++gidx) {
+    int b = S.xgrp_row[gidx];
+    if (S.blk_cross_end[b] == 0 && S.blk_cross_begin[b] == 0) S.blk_cross_begin[b] = (int)gidx;
+    S.blk_cross_end[b] = (int)gidx + 1;
+  }
+  for (int b = 0; b < nb; ++b)
+    if (S.blk_cross_end[b] == 0) S.blk_cross_begin[b] = 0;
+}
+
+template <typename T>
+struct Solver {
+  Context* ctx;
+  cudaStream_t st;
+  const NativeProblem& n;
+  LmOptions opt;
+  Layout L;
+  Setup S;
+  int N, P, D, nb, ng;
+  bool direct;
+  // device data
+  DBuf<uint32_t> d_pt_off, d_obs_cam, d_obs_model, d_cam_group;
+  DBuf<double> d_obs_px;
+  DBuf<FixedCameraDev> d_models;
+  DBuf<int> d_pose_off, d_pose_dim, d_intr_off, d_intr_dim;
+  DBuf<uint8_t> d_fixed_points;
+  DBuf<double> d_pose[2], d_points[2], d_groups[2];
+  int cur = 0;
+  DBuf<T> d_jc, d_jp, d_f;
+  DBuf<double> d_rw, d_vinv, d_ig, d_gp, d_ddiag;
+  DBuf<PointSummary> d_summary, d_summary_part;
+  DBuf<int> d_blk_off, d_blk_dim, d_blk_col, d_blk_edge, d_chunk_block, d_chunk_col, d_blk_chunk_begin, d_blk_chunk_end;
+  DBuf<uint32_t> d_ent, d_ent_point, d_chunk_begin, d_chunk_end;
+  DBuf<int> d_obs_intr_col, d_seg_col;
+  DBuf<double> d_chunk_out, d_blk_out;
+  DBuf<double> d_gfull, d_gred, d_diag, d_diag_minmax;
+  DBuf<int> d_clamp;
+  // pairs
+  DBuf<int> d_grp_row, d_grp_col, d_xgrp_row, d_xgrp_col, d_blk_cross_begin, d_blk_cross_end;
+  DBuf<uint32_t> d_grp_begin, d_grp_end, d_pair_a, d_pair_b, d_pair_p;
+  DBuf<uint32_t> d_xgrp_begin, d_xgrp_end, d_xpair_a, d_xpair_b, d_xpair_p;
+  DBuf<double> d_pair_out, d_xpair_out;
+  DBuf<double> d_S, d_Lf;
+  DBuf<int> d_status;
+  // PCG vectors
+  DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_chunk_y, d_factor, d_tmp;
+  DBuf<int> d_fail;
+  DBuf<double> d_scalars, d_cam_norm;
+  DBuf<RedVec<4>> d_cand, d_cand_part;
+  DBuf<RedVec<3>> d_met, d_met_part;
+  DBuf<RedVec<1>> d_one, d_one_part;
+  DBuf<RedVec<1>> d_norm_part;
+  int red_blocks;
+
+  Solver(Context* c, const NativeProblem& prob, const LmOptions& o) : ctx(c), st(c->stream), n(prob), opt(o) {
+    L = make_layout(n);
+    N = (int)n.obs_cam.size();
+    P = (int)(n.points.size() / 3);
+    D = L.D;
+    ng = n.self_cal ? (int)n.group_dim.size() : 0;
+    direct = !opt.iterative;
+    build_tables(n, L, direct || D <= opt.dense_rank_limit, S);
+    nb = (int)S.blk_off.size();
+    red_blocks = std::min(1024, grid_for(std::max(P, N), kReduceThreads));
+    upload();
+  }
+
+  DevView view() const {
+    DevView v;
+    v.P = P;
+    v.ncam = n.ncam;
+    v.self_cal = n.self_cal ? 1 : 0;
+    v.pixel_model = n.pixel_model ? 1 : 0;
+    v.pt_off = d_pt_off.p;
+    v.obs_cam = d_obs_cam.p;
+    v.obs_px = d_obs_px.p;
+    v.obs_model = d_obs_model.p;
+    v.models = d_models.p;
+    v.cam_group = d_cam_group.p;
+    v.pose_off = d_pose_off.p;
+    v.pose_dim = d_pose_dim.p;
+    v.intr_off = d_intr_off.p;
+    v.intr_dim = d_intr_dim.p;
+    v.fixed_points = d_fixed_points.p;
+    return v;
+  }
+  DevState state(int which) const { return {d_pose[which].p, d_points[which].p, d_groups[which].p}; }
+  LinOut<T> lin() const {
+    return {d_jc.p, d_jp.p, d_rw.p, d_vinv.p, d_ig.p, d_gp.p, d_ddiag.p, d_summary.p, nullptr};
+  }
+  BlockTables tables() const {
+    BlockTables b;
+    b.nblocks = nb;
+    b.blk_off = d_blk_off.p;
+    b.blk_dim = d_blk_dim.p;
+    b.blk_col = d_blk_col.p;
+    b.blk_edge = d_blk_edge.p;
+    b.ent = d_ent.p;
+    b.ent_point = d_ent_point.p;
+    b.nchunks = (int)S.chunk_block.size();
+    b.chunk_block = d_chunk_block.p;
+    b.chunk_col = d_chunk_col.p;
+    b.chunk_begin = d_chunk_begin.p;
+    b.chunk_end = d_chunk_end.p;
+    b.blk_chunk_begin = d_blk_chunk_begin.p;
+    b.blk_chunk_end = d_blk_chunk_end.p;
+    return b;
+  }
+  PairTables pairs(bool cross) const {
+    PairTables t;
+    if (cross) {
+      t.ngroups = (int)S.xgrp_row.size();
+      t.grp_row = d_xgrp_row.p;
+      t.grp_col = d_xgrp_col.p;
+      t.grp_begin = d_xgrp_begin.p;
+      t.grp_end = d_xgrp_end.p;
+      t.pair_a = d_xpair_a.p;
+      t.pair_b = d_xpair_b.p;
+      t.pair_p = d_xpair_p.p;
+    } else {
+      t.ngroups = (int)S.grp_row.size();
+      t.grp_row = d_grp_row.p;
+      t.grp_col = d_grp_col.p;
+      t.grp_begin = d_grp_begin.p;
+      t.grp_end = d_grp_end.p;
+      t.pair_a = d_pair_a.p;
+      t.pair_b = d_pair_b.p;
+      t.pair_p = d_pair_p.p;
+    }
+    return t;
+  }
+
+  void upload() {
+    std::vector<uint32_t> pt_off(n.pt_off.begin(), n.pt_off.end());
+    d_pt_off.upload(pt_off.data(), pt_off.size(), st);
+    d_obs_cam.upload(n.obs_cam.data(), n.obs_cam.size(), st);
+    d_obs_px.upload(n.obs_px.data(), n.obs_px.size(), st);
+    std::vector<uint32_t> om = n.obs_model;
+    if (om.empty()) om.assign(1, 0);
+    d_obs_model.upload(om.data(), om.size(), st);
+    std::vector<FixedCameraDev> models = n.models;
+    if (models.empty()) models.resize(1);
+    d_models.upload(models.data(), models.size(), st);
+    std::vector<uint32_t> cg = n.cam_group;
+    if (cg.empty()) cg.assign(n.ncam, 0);
+    d_cam_group.upload(cg.data(), cg.size(), st);
+    d_pose_off.upload(L.pose_off.data(), L.pose_off.size(), st);
+    d_pose_dim.upload(L.pose_dim.data(), L.pose_dim.size(), st);
+    d_intr_off.upload(L.intr_off.data(), L.intr_off.size(), st);
+    d_intr_dim.upload(L.intr_dim.data(), L.intr_dim.size(), st);
+    d_fixed_points.upload(n.fixed_points.data(), n.fixed_points.size(), st);
+    std::vector<double> pose(12 * (size_t)n.ncam);
+    for (int c = 0; c < n.ncam; ++c) {
+      for (int k = 0; k < 9; ++k) pose[12 * c + k] = n.rotation[9 * c + k];
+      for (int k = 0; k < 3; ++k) pose[12 * c + 9 + k] = n.translation[3 * c + k];
+    }
+    for (int w = 0; w < 2; ++w) {
+      d_pose[w].upload(pose.data(), pose.size(), st);
+      d_points[w].upload(n.points.data(), n.points.size(), st);
+      std::vector<double> gr = n.groups;
+      if (gr.empty()) gr.assign(3, 0.0);
+      d_groups[w].upload(gr.data(), gr.size(), st);
+    }
+    d_jc.alloc((size_t)18 * N, st);
+    d_jp.alloc((size_t)6 * N, st);
+    d_f.alloc((size_t)2 * N, st);
+    d_rw.alloc((size_t)2 * N, st);
+    d_vinv.alloc((size_t)6 * P, st);
+    d_ig.alloc((size_t)3 * P, st);
+    d_gp.alloc((size_t)3 * P, st);
+    d_ddiag.alloc((size_t)3 * P, st);
+    d_ddiag.zero();
+    d_summary.alloc(P, st);
+    d_summary_part.alloc(red_blocks, st);
+    auto up_i = [&](DBuf<int>& b, const std::vector<int>& v) {
+      std::vector<int> t = v;
+      if (t.empty()) t.push_back(0);
+      b.upload(t.data(), t.size(), st);
+    };
+    auto up_u = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) {
+      std::vector<uint32_t> t = v;
+      if (t.empty()) t.push_back(0);
+      b.upload(t.data(), t.size(), st);
+    };
+    up_i(d_blk_off, S.blk_off);
+    up_i(d_blk_dim, S.blk_dim);
+    std::vector<int> col = S.blk_col;
+    for (auto& c : col) c = std::max(c, 0);
+    up_i(d_blk_col, col);
+    up_i(d_blk_edge, S.blk_edge);
+    up_u(d_ent, S.ent);
+    up_u(d_ent_point, S.ent_point);
+    up_i(d_chunk_block, S.chunk_block);
+    up_i(d_chunk_col, S.chunk_col);
+    up_u(d_chunk_begin, S.chunk_begin);
+    up_u(d_chunk_end, S.chunk_end);
+    up_i(d_blk_chunk_begin, S.blk_chunk_begin);
+    up_i(d_blk_chunk_end, S.blk_chunk_end);
+    up_i(d_obs_intr_col, S.obs_intr_col);
+    up_i(d_seg_col, S.seg_col);
+    up_i(d_grp_row, S.grp_row);
+    up_i(d_grp_col, S.grp_col);
+    up_u(d_grp_begin, S.grp_begin);
+    up_u(d_grp_end, S.grp_end);
+    up_u(d_pair_a, S.pair_a);
+    up_u(d_pair_b, S.pair_b);
+    up_u(d_pair_p, S.pair_p);
+    up_i(d_xgrp_row, S.xgrp_row);
+    up_i(d_xgrp_col, S.xgrp_col);
+    up_u(d_xgrp_begin, S.xgrp_begin);
+    up_u(d_xgrp_end, S.xgrp_end);
+    up_u(d_xpair_a, S.xpair_a);
+    up_u(d_xpair_b, S.xpair_b);
+    up_u(d_xpair_p, S.xpair_p);
+    up_i(d_blk_cross_begin, S.blk_cross_begin);
+    up_i(d_blk_cross_end, S.blk_cross_end);
+    d_chunk_out.alloc((size_t)kAsmRec * std::max<size_t>(1, S.chunk_block.size()), st);
+    d_blk_out.alloc((size_t)kAsmRec * std::max(1, nb), st);
+    d_gfull.alloc(std::max(1, D), st);
+    d_gred.alloc(std::max(1, D), st);
+    d_diag.alloc(std::max(1, D), st);
+    d_diag_minmax.alloc(2 * std::max(1, nb), st);
+    d_clamp.alloc(std::max(1, nb), st);
+    d_pair_out.alloc((size_t)36 * std::max<size_t>(1, S.grp_row.size()), st);
+    d_xpair_out.alloc((size_t)36 * std::max<size_t>(1, S.xgrp_row.size()), st);
+    if (!S.grp_row.empty() || direct) {
+      d_S.alloc((size_t)std::max(1, D) * std::max(1, D), st);
+      d_Lf.alloc((size_t)std::max(1, D) * std::max(1, D), st);
+    }
+    d_status.alloc(4, st);
+    for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp}) b->alloc(std::max(1, D), st);
+    d_chunk_y.alloc((size_t)6 * std::max<size_t>(1, S.chunk_block.size()), st);
+    d_factor.alloc((size_t)42 * std::max(1, nb), st);
+    d_fail.alloc(std::max(1, nb), st);
+    d_scalars.alloc(16, st);
+    d_cam_norm.alloc(std::max(1, n.ncam), st);
+    d_cand.alloc(P, st);
+    d_cand_part.alloc(red_blocks, st);
+    d_met.alloc(P, st);
+    d_met_part.alloc(red_blocks, st);
+    d_one.alloc(std::max(N, n.ncam), st);
+    d_one_part.alloc(red_blocks, st);
+  }
+
+  void sync() { CUDA_OK(cudaStreamSynchronize(st)); }
+  void check_launch() { CUDA_OK(cudaGetLastError()); }
+
+  template <int NV>
+  RedVec<NV> reduce(const RedVec<NV>* in, int count, DBuf<RedVec<NV>>& part) {
+    k_reduce_vec<NV><<<red_blocks, kReduceThreads, 0, st>>>(in, count, part.p);
+    k_reduce_vec<NV><<<1, kReduceThreads, 0, st>>>(part.p, red_blocks, part.p + 0);
+    check_launch();
+    RedVec<NV> h;
+    CUDA_OK(cudaMemcpyAsync(&h, part.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    sync();
+    return h;
+  }
+
+  Gauge gauge_for(int which, double scene) {
+    Gauge g{};
+    g.fixed_cam = n.gauge_cam;
+    g.scene = scene;
+    if (n.gauge_cam >= 0) {
+      double t[3];
+      CUDA_OK(cudaMemcpyAsync(t, d_pose[which].p + 12 * n.gauge_cam + 9, sizeof(t), cudaMemcpyDeviceToHost, st));
+      sync();
+      g.baseline = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      for (int k = 0; k < 3; ++k) g.dir[k] = t[k] / g.baseline;
+      // s2_tangent_basis (numerics/manifold.rs:118-131)
+      double nv = std::sqrt(g.dir[0] * g.dir[0] + g.dir[1] * g.dir[1] + g.dir[2] * g.dir[2]);
+      double tv[3] = {g.dir[0] / nv, g.dir[1] / nv, g.dir[2] / nv};
+      double ref[3] = {0, 0, 0};
+      if (std::fabs(tv[0]) <= std::fabs(tv[1]) && std::fabs(tv[0]) <= std::fabs(tv[2]))
+        ref[0] = 1;
+      else if (std::fabs(tv[1]) <= std::fabs(tv[2]))
+        ref[1] = 1;
+      else
+        ref[2] = 1;
+      auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1];
+        c[1] = a[2] * b[0] - a[0] * b[2];
+        c[2] = a[0] * b[1] - a[1] * b[0];
+      };
+      double b0[3], b1[3];
+      cross(tv, ref, b0);
+      double n0 = std::sqrt(b0[0] * b0[0] + b0[1] * b0[1] + b0[2] * b0[2]);
+      for (int k = 0; k < 3; ++k) b0[k] /= n0;
+      cross(tv, b0, b1);
+      double n1 = std::sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
+      for (int k = 0; k < 3; ++k) {
+        g.b0[k] = b0[k];
+        g.b1[k] = b1[k] / n1;
+      }
+    }
+    return g;
+  }
+
+  struct Assembly {
+    bool valid;
+    double cost, sq, point_red, grad_norm, min_rcond;
+    uint64_t weak;
+    double min_diag, max_diag;
+    int clamp;
+  };
+
+  // Full linearization + camera-side reductions at the given damping.
+  Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_dense) {
+    DevView v = view();
+    k_linearize<T><<<grid_for(P, 128), 128, 0, st>>>(v, state(which), g, loss, lambda, lin());
+    check_launch();
+    k_reduce_summary<<<red_blocks, kReduceThreads, 0, st>>>(d_summary.p, P, d_summary_part.p);
+    k_reduce_summary<<<1, kReduceThreads, 0, st>>>(d_summary_part.p, red_blocks, d_summary_part.p);
+    check_launch();
+    BlockTables bt = tables();
+    if (bt.nchunks > 0) {
+      k_block_chunks<T><<<bt.nchunks, 32, 0, st>>>(bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
+      k_block_finalize<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_chunk_out.p, d_blk_out.p);
+      CUDA_OK(cudaMemsetAsync(d_gfull.p, 0, sizeof(double) * std::max(1, D), st));
+      CUDA_OK(cudaMemsetAsync(d_gred.p, 0, sizeof(double) * std::max(1, D), st));
+      CUDA_OK(cudaMemsetAsync(d_diag.p, 0, sizeof(double) * std::max(1, D), st));
+      k_block_vectors<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_blk_out.p, d_gfull.p, d_gred.p, d_diag.p, d_clamp.p,
+                                                     d_diag_minmax.p);
+      check_launch();
+    }
+    if (build_dense && D > 0) {
+      PairTables pt = pairs(false);
+      if (pt.ngroups > 0) k_pairs<T><<<pt.ngroups, 32, 0, st>>>(pt, bt, lin(), d_seg_col.p, d_pair_out.p);
+      CUDA_OK(cudaMemsetAsync(d_S.p, 0, sizeof(double) * (size_t)D * D, st));
+      k_dense_from_blocks<<<nb, 32, 0, st>>>(bt, d_blk_out.p, D, d_S.p);
+      if (pt.ngroups > 0) k_dense_pairs<<<grid_for(pt.ngroups, 64), 64, 0, st>>>(pt, bt, d_pair_out.p, D, d_S.p);
+      k_dense_add_diag<<<grid_for(D, 128), 128, 0, st>>>(D, d_diag.p, lambda, d_S.p);
+      check_launch();
+    }
+    PointSummary ps;
+    CUDA_OK(cudaMemcpyAsync(&ps, d_summary_part.p, sizeof(ps), cudaMemcpyDeviceToHost, st));
+    std::vector<double> mm(2 * std::max(nb, 1));
+    std::vector<int> cl(std::max(nb, 1));
+    std::vector<double> gvals(std::max(D, 1)), dvals(std::max(D, 1));
+    if (nb > 0) {
+      CUDA_OK(cudaMemcpyAsync(mm.data(), d_diag_minmax.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(cl.data(), d_clamp.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    }
+    if (D > 0) {
+      CUDA_OK(cudaMemcpyAsync(gvals.data(), d_gfull.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(dvals.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+    }
+    std::vector<double> gr(std::max(D, 1));
+    if (D > 0) CUDA_OK(cudaMemcpyAsync(gr.data(), d_gred.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+    sync();
+    Assembly a;
+    a.valid = ps.invalid == 0.0;
+    a.cost = ps.cost;
+    a.sq = ps.sq;
+    a.point_red = ps.point_red;
+    a.grad_norm = ps.grad_norm;
+    a.min_rcond = ps.min_rcond;
+    a.weak = (uint64_t)ps.weak;
+    double mn = INFINITY, mx = 0.0;
+    a.clamp = 0;
+    for (int b = 0; b < nb; ++b) {
+      mn = std::min(mn, mm[2 * b]);
+      mx = std::max(mx, mm[2 * b + 1]);
+      a.clamp += cl[b];
+    }
+    a.min_diag = D == 0 ? 0.0 : mn;
+    a.max_diag = mx;
+    // scaled_gradient_inf_norm_prepared over the unreduced camera gradient (schur/assembly.rs:1092-1107)
+    double gn = 0.0;
+    bool finite = true;
+    for (int i = 0; i < D; ++i) {
+      double cv = dvals[i], val = gvals[i];
+      double t = (std::isfinite(cv) && cv > 0.0) ? std::fabs(val) / std::sqrt(cv) : (val == 0.0 ? 0.0 : INFINITY);
+      gn = std::max(gn, t);
+      finite = finite && std::isfinite(gr[i]);
+    }
+    a.grad_norm = std::max(a.grad_norm, gn);
+    a.valid = a.valid && finite && std::isfinite(a.cost);
+    if (build_dense && D > 0 && a.valid) {
+      // the dense S must be finite (hessian.is_finite)
+    }
+    return a;
+  }
+
+  // ---- camera step ----
+  bool direct_step() {
+    CUDA_OK(cudaMemcpyAsync(d_Lf.p, d_S.p, sizeof(double) * (size_t)D * D, cudaMemcpyDeviceToDevice, st));
+    k_dense_cholesky<<<1, 1024, 0, st>>>(D, d_Lf.p, d_status.p);
+    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_step.p);
+    check_launch();
+    int ok = 0;
+    CUDA_OK(cudaMemcpyAsync(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (!ok) return false;
+    k_dense_solve<<<1, 32, 0, st>>>(D, d_Lf.p, d_step.p);
+    check_launch();
+    return true;
+  }
+
+  void dots(std::initializer_list<std::pair<const double*, const double*>> pairs, double* out) {
+    DotArgs a{};
+    int k = 0;
+    for (auto& pr : pairs) {
+      a.a[k] = pr.first;
+      a.b[k] = pr.second;
+      ++k;
+    }
+    a.count = k;
+    k_dots<<<1, 1024, 0, st>>>(a, D, d_scalars.p);
+    check_launch();
+    CUDA_OK(cudaMemcpyAsync(out, d_scalars.p, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+    sync();
+  }
+
+  // y = S_lambda x (implicit, matrix-free)
+  void matvec(const double* x, double* y, double lambda) {
+    if (direct || !d_S.p || false) {
+    }
+    DevView v = view();
+    k_mv_points<T><<<grid_for(P, 128), 128, 0, st>>>(v, lin(), x, d_f.p);
+    BlockTables bt = tables();
+    if (bt.nchunks > 0) k_mv_chunks<T><<<bt.nchunks, 32, 0, st>>>(bt, lin(), d_f.p, d_chunk_y.p);
+    k_mv_finalize<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_chunk_y.p, d_diag.p, lambda, x, y);
+    check_launch();
+  }
+
+  bool factor_preconditioner(double lambda) {
+    BlockTables bt = tables();
+    PairTables xt = pairs(true);
+    if (xt.ngroups > 0) k_pairs<T><<<xt.ngroups, 32, 0, st>>>(xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
+    k_block_factor<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
+                                                   d_blk_cross_begin.p, d_blk_cross_end.p, d_factor.p, d_fail.p);
+    check_launch();
+    std::vector<int> fail(std::max(nb, 1));
+    if (nb > 0) CUDA_OK(cudaMemcpyAsync(fail.data(), d_fail.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    sync();
+    for (int b = 0; b < nb; ++b)
+      if (fail[b]) return false;
+    return true;
+  }
+  void precond(const double* r, double* z) {
+    k_block_precond<<<grid_for(nb, 64), 64, 0, st>>>(tables(), d_factor.p, r, z);
+    check_launch();
+  }
+
+  struct PcgResult {
+    bool accepted = false;
+    uint64_t terms = 0;
+    double rel = NAN;
+  };
+  // pcg::solve (sparse/pcg.rs:23-119), require_bounded_residual
+  PcgResult pcg(double lambda, uint64_t max_it, double tol) {
+    PcgResult res;
+    CUDA_OK(cudaMemsetAsync(d_step.p, 0, sizeof(double) * D, st));
+    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_r.p);
+    double h[4];
+    dots({{d_r.p, d_r.p}}, h);
+    double n0 = std::sqrt(h[0]);
+    if (!std::isfinite(n0)) return res;
+    if (n0 == 0.0) {
+      res.accepted = true;
+      res.rel = 0.0;
+      return res;
+    }
+    precond(d_r.p, d_z.p);
+    CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    dots({{d_r.p, d_z.p}}, h);
+    double rho = h[0];
+    if (!(std::isfinite(rho) && rho > 0.0)) return res;
+    auto recompute = [&]() {
+      matvec(d_step.p, d_q.p, lambda);
+      k_residual_update<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_q.p, d_r.p);
+      check_launch();
+    };
+    for (uint64_t it = 1; it <= max_it; ++it) {
+      matvec(d_dir.p, d_q.p, lambda);
+      dots({{d_dir.p, d_q.p}}, h);
+      double curv = h[0];
+      if (!(std::isfinite(curv) && curv > 0.0)) {
+        res.terms = it - 1;
+        return res;
+      }
+      double alpha = rho / curv;
+      if (!std::isfinite(alpha)) {
+        res.terms = it - 1;
+        return res;
+      }
+      k_axpy2<<<grid_for(D, 256), 256, 0, st>>>(D, alpha, d_dir.p, d_q.p, d_step.p, d_r.p);
+      precond(d_r.p, d_z.p);
+      dots({{d_r.p, d_r.p}, {d_r.p, d_z.p}}, h);
+      double ratio = std::sqrt(h[0]) / n0;
+      if (!std::isfinite(ratio)) {
+        res.terms = it;
+        return res;
+      }
+      if (ratio <= tol) {
+        recompute();
+        dots({{d_r.p, d_r.p}}, h);
+        double tr = std::sqrt(h[0]) / n0;
+        if (std::isfinite(tr) && tr <= tol) {
+          res.accepted = true;
+          res.terms = it;
+          res.rel = tr;
+          return res;
+        }
+        if (!std::isfinite(tr)) {
+          res.terms = it;
+          return res;
+        }
+        precond(d_r.p, d_z.p);
+        CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+        dots({{d_r.p, d_z.p}}, h);
+        rho = h[0];
+        if (!(std::isfinite(rho) && rho > 0.0)) {
+          res.terms = it;
+          res.rel = tr;
+          return res;
+        }
+        continue;
+      }
+      double nrho = h[1];
+      if (!(std::isfinite(nrho) && nrho > 0.0)) {
+        res.terms = it;
+        return res;
+      }
+      double beta = nrho / rho;
+      if (!std::isfinite(beta)) {
+        res.terms = it;
+        return res;
+      }
+      k_xpby<<<grid_for(D, 256), 256, 0, st>>>(D, d_z.p, beta, d_dir.p);
+      check_launch();
+      rho = nrho;
+    }
+    recompute();
+    dots({{d_r.p, d_r.p}}, h);
+    res.terms = max_it;
+    res.rel = std::sqrt(h[0]) / n0;
+    return res;
+  }
+
+  double scene_scale_host() {
+    // observed_scene_scale (optimizer.rs:630-675) for calibrated, scene_scale (:620-628) for self-cal
+    if (n.gauge_cam >= 0) {
+      const double* t = &n.translation[3 * n.gauge_cam];
+      return std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    }
+    if (n.self_cal) {
+      double s = 0.0;
+      for (size_t i = 0; i < n.points.size(); ++i) s += n.points[i] * n.points[i];
+      return std::max(std::sqrt(s / double(P)), kMinPositive);
+    }
+    double scale = 0.0, sq = 1.0;
+    size_t count = 0;
+    for (int p = 0; p < P; ++p) {
+      if (n.pt_off[p] == n.pt_off[p + 1]) continue;
+      count++;
+      for (int k = 0; k < 3; ++k) {
+        double m = std::fabs(n.points[3 * p + k]);
+        if (m == 0.0) continue;
+        if (scale < m) {
+          double r = scale / m;
+          sq = 1.0 + sq * r * r;
+          scale = m;
+        } else {
+          double r = m / scale;
+          sq += r * r;
+        }
+      }
+    }
+    if (scale == 0.0 || count == 0) return kMinPositive;
+    double rms = scale * std::sqrt(sq / double(count));
+    return std::isfinite(rms) ? std::max(rms, kMinPositive) : scale;
+  }
+
+  void metrics(int which, const LossDev& loss, double* cost, double* rmse) {
+    k_metrics<<<grid_for(P, 128), 128, 0, st>>>(view(), state(which), loss, d_met.p);
+    check_launch();
+    RedVec<3> r = reduce<3>(d_met.p, P, d_met_part);
+    if (r.v[2] > 0.0) {
+      *cost = INFINITY;
+      *rmse = INFINITY;
+      return;
+    }
+    *cost = r.v[0];
+    *rmse = std::sqrt(r.v[1] / double(2 * (size_t)N));
+  }
+
+  NativeReport refine(std::vector<double>& rotation, std::vector<double>& translation, std::vector<double>& points,
+                      std::vector<double>& groups) {
+    NativeReport rep;
+    double scene = scene_scale_host();
+    // stages (continuation.rs:18-74)
+    struct Stage {
+      LossDev loss;
+      uint64_t iters;
+    } stages[3];
+    const LossDev l2{kLossL2, 0.0};
+    if (opt.loss.kind == kLossCauchy) {
+      uint64_t w = std::min<uint64_t>(opt.max_iterations / 4, 5);
+      stages[0] = {l2, w};
+      stages[1] = {opt.loss, opt.max_iterations - w};
+      stages[2] = {l2, 0};
+    } else {
+      stages[0] = {opt.loss, opt.max_iterations};
+      stages[1] = {l2, 0};
+      stages[2] = {l2, 0};
+    }
+    int target = 0;
+    for (int i = 2; i >= 0; --i)
+      if (stages[i].iters > 0) {
+        target = i;
+        break;
+      }
+    bool reuse = false;
+    for (auto& s : stages)
+      if (s.iters > 0) {
+        reuse = s.loss.kind == opt.loss.kind && s.loss.scale == opt.loss.scale;
+        break;
+      }
+    bool have_initial = false;
+    double init_cost = INFINITY, init_rmse = INFINITY;
+    if (!reuse) {
+      metrics(cur, opt.loss, &init_cost, &init_rmse);
+      have_initial = true;
+    }
+    // Nielsen controller (numerics/refine/nonlinear/controller.rs:6-91) and run state (run_state.rs)
+    double lambda = direct ? 1e-4 : 1e-1, nu = 2.0;
+    auto increase = [&]() {
+      lambda = std::min(lambda * nu, 1e12);
+      nu = std::min(nu * 2.0, 1e12);
+    };
+    uint64_t iterations = 0, accepted = 0, target_accepted = 0, rej[4] = {0, 0, 0, 0};
+    int convergence = -1;
+    uint64_t pcg_terms = 0;
+    double iter_tol = std::min(std::sqrt(opt.relative_cost_tolerance), 1e-6);
+    bool done = false;
+    int cand = 1 - cur;
+    size_t free_points = 0;
+    for (int p = 0; p < P; ++p) free_points += n.fixed_points[p] ? 0 : 1;
+    for (int si = 0; si < 3 && !done; ++si) {
+      bool confirm = false;
+      for (uint64_t it = 0; it < stages[si].iters; ++it) {
+        iterations++;
+        Gauge g = gauge_for(cur, scene);
+        Assembly a = assemble(cur, g, stages[si].loss, lambda, direct);
+        if (!have_initial && std::isfinite(a.cost) && std::isfinite(a.sq) && N > 0) {
+          init_cost = a.cost;
+          init_rmse = std::sqrt(a.sq / double(2 * (size_t)N));
+          have_initial = true;
+        }
+        if (!a.valid) {
+          rej[0]++;
+          increase();
+          continue;
+        }
+        double current = a.cost;
+        if (si == target && convergence < 0 && std::isfinite(a.grad_norm) && a.grad_norm >= 0.0 &&
+            std::isfinite(current) && a.grad_norm <= opt.gradient_tolerance * (1.0 + std::fabs(current))) {
+          convergence = 1;
+          done = true;
+          break;
+        }
+        bool iterative_step = false;
+        double rel_res = 0.0;
+        if (direct) {
+          if (D > 0 && !direct_step()) {
+            rej[1]++;
+            increase();
+            continue;
+          }
+        } else {
+          if (!factor_preconditioner(lambda)) {
+            rej[1]++;
+            increase();
+            continue;
+          }
+          double tol = confirm ? std::min(opt.pcg_tolerance, iter_tol) : opt.pcg_tolerance;
+          uint64_t limit = confirm ? opt.pcg_max_iterations : std::min<uint64_t>(opt.pcg_max_iterations, (uint64_t)D);
+          PcgResult r = pcg(lambda, limit, tol);
+          pcg_terms += r.terms;
+          if (!r.accepted) {
+            rej[1]++;
+            increase();
+            continue;
+          }
+          iterative_step = true;
+          rel_res = r.rel;
+        }
+        // step cap (calibrated only)
+        if (!n.self_cal && D > 0) {
+          k_step_block_norm<<<grid_for(n.ncam, 128), 128, 0, st>>>(n.ncam, d_pose_off.p, d_pose_dim.p, d_step.p,
+                                                                   d_cam_norm.p);
+          check_launch();
+          std::vector<double> norms(n.ncam);
+          CUDA_OK(cudaMemcpyAsync(norms.data(), d_cam_norm.p, sizeof(double) * n.ncam, cudaMemcpyDeviceToHost, st));
+          sync();
+          double largest = 0.0;
+          for (double x : norms) largest = std::max(largest, x);
+          if (largest > 0.5) {
+            k_scale<<<grid_for(D, 256), 256, 0, st>>>(D, 0.5 / largest, d_step.p);
+            check_launch();
+          }
+        }
+        DevView v = view();
+        k_retract<<<grid_for(std::max(n.ncam, ng), 128), 128, 0, st>>>(v, ng, d_step.p, g, d_pose[cur].p,
+                                                                        d_groups[cur].p, d_pose[cand].p,
+                                                                        d_groups[cand].p);
+        k_candidate_points<T><<<grid_for(P, 128), 128, 0, st>>>(v, lin(), d_step.p, state(cur), state(cand), g,
+                                                                stages[si].loss, d_cand.p);
+        check_launch();
+        RedVec<4> cr = reduce<4>(d_cand.p, P, d_cand_part);
+        if (cr.v[3] > 0.0) {
+          rej[2]++;
+          increase();
+          continue;
+        }
+        double point_rms =
+            std::sqrt(cr.v[1] / double(n.self_cal ? std::max(P, 1) : std::max<size_t>(free_points, 1)));
+        // model reduction (camera_step.rs:44-81, optimizer.rs:590-618, retained/mod.rs:742-800)
+        double damped;
+        if (!iterative_step) {
+          if (D > 0)
+            k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, st>>>(D, d_S.p, d_step.p, d_q.p);
+          else
+            CUDA_OK(cudaMemsetAsync(d_q.p, 0, sizeof(double), st));
+          check_launch();
+        } else {
+          matvec(d_step.p, d_q.p, lambda);
+        }
+        double h[4] = {0, 0, 0, 0};
+        if (D > 0) dots({{d_gred.p, d_step.p}, {d_step.p, d_q.p}}, h);
+        if (!iterative_step) {
+          damped = a.point_red - h[0] - 0.5 * h[1];
+        } else {
+          damped = a.point_red + (-h[0] - 0.5 * h[1]);
+          if (!(std::isfinite(damped) && damped > 0.0)) damped = NAN;
+        }
+        // camera damping norm: sum diag * step^2
+        CUDA_OK(cudaMemcpyAsync(d_tmp.p, d_step.p, sizeof(double) * std::max(D, 1), cudaMemcpyDeviceToDevice, st));
+        double cd[1] = {0.0};
+        if (D > 0) {
+          std::vector<double> hs(D), hd(D);
+          CUDA_OK(cudaMemcpyAsync(hs.data(), d_step.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+          CUDA_OK(cudaMemcpyAsync(hd.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+          sync();
+          for (int i = 0; i < D; ++i) cd[0] += hd[i] * hs[i] * hs[i];
+          double ss = 0.0;
+          for (int i = 0; i < D; ++i) ss += hs[i] * hs[i];
+          h[2] = ss;
+        }
+        double predicted = damped + 0.5 * lambda * (cd[0] + cr.v[2]);
+        double reduction = current - cr.v[0];
+        // NielsenController::accept
+        double gain = (std::isfinite(reduction) && std::isfinite(predicted) && predicted > 0.0) ? reduction / predicted
+                                                                                              : NAN;
+        if (!(std::isfinite(gain) && gain > 0.0)) {
+          increase();
+          rej[3]++;
+          continue;
+        }
+        double c2 = 2.0 * gain - 1.0;
+        lambda = std::max(lambda * std::max(1.0 - c2 * c2 * c2, 1.0 / 3.0), 1e-12);
+        nu = 2.0;
+        std::swap(cur, cand);
+        accepted++;
+        double crms = std::sqrt(h[2] / double(std::max(D, 1)));
+        double sn = std::sqrt(crms * crms + point_rms * point_rms);
+        if (si == target) {
+          target_accepted++;
+          double relc = reduction / (1.0 + std::fabs(current));
+          int cc = sn <= opt.step_tolerance ? 2 : (relc <= opt.relative_cost_tolerance ? 0 : -1);
+          if (iterative_step && cc >= 0 && rel_res > iter_tol) {
+            confirm = true;
+            convergence = -1;
+          } else {
+            confirm = false;
+            convergence = cc;
+            if (cc >= 0) {
+              done = true;
+              break;
+            }
+          }
+        }
+      }
+    }
+    // final undamped assembly and certificate
+    Gauge g = gauge_for(cur, scene);
+    bool dense_rank = D <= opt.dense_rank_limit && !S.grp_row.empty();
+    Assembly fa = assemble(cur, g, opt.loss, 0.0, dense_rank);
+    rep.rank = 3;
+    if (dense_rank || D == 0) {
+      if (!fa.valid)
+        rep.rank = 2;
+      else if (D == 0)
+        rep.rank = 0;
+      else
+        rep.rank = rank_full() ? 0 : 2;
+    }
+    bool well = rep.rank != 2 && fa.weak == 0;
+    if (!well)
+      rep.status = 3;
+    else if (convergence >= 0)
+      rep.status = 0;
+    else if (iterations > 0 && target_accepted == 0)
+      rep.status = 2;
+    else
+      rep.status = 1;
+    rep.reason = convergence;
+    if (fa.valid) {
+      rep.final_cost = fa.cost;
+      rep.final_rmse = std::sqrt(fa.sq / double(2 * (size_t)N));
+    } else {
+      metrics(cur, opt.loss, &rep.final_cost, &rep.final_rmse);
+    }
+    rep.gradient_inf_norm = fa.grad_norm;
+    rep.initial_cost = init_cost;
+    rep.initial_rmse = init_rmse;
+    rep.iterations = iterations;
+    rep.accepted = accepted;
+    for (int k = 0; k < 4; ++k) rep.rej[k] = rej[k];
+    rep.rejected = rej[0] + rej[1] + rej[2] + rej[3];
+    rep.weak = fa.weak;
+    {
+      k_noninvertible<<<grid_for(N, 256), 256, 0, st>>>(view(), N, d_groups[cur].p, d_one.p);
+      check_launch();
+      RedVec<1> r = reduce<1>(d_one.p, N, d_one_part);
+      rep.noninvertible = (uint64_t)r.v[0];
+    }
+    rep.pcg_terms = pcg_terms;
+    rep.final_damping = lambda;
+    rep.D = D;
+    // download state
+    std::vector<double> pose(12 * (size_t)n.ncam);
+    CUDA_OK(cudaMemcpyAsync(pose.data(), d_pose[cur].p, sizeof(double) * pose.size(), cudaMemcpyDeviceToHost, st));
+    points.resize(n.points.size());
+    CUDA_OK(cudaMemcpyAsync(points.data(), d_points[cur].p, sizeof(double) * points.size(), cudaMemcpyDeviceToHost, st));
+    groups.assign(n.groups.size(), 0.0);
+    if (!groups.empty())
+      CUDA_OK(cudaMemcpyAsync(groups.data(), d_groups[cur].p, sizeof(double) * groups.size(), cudaMemcpyDeviceToHost, st));
+    sync();
+    rotation.resize(9 * (size_t)n.ncam);
+    translation.resize(3 * (size_t)n.ncam);
+    for (int c = 0; c < n.ncam; ++c) {
+      for (int k = 0; k < 9; ++k) rotation[9 * c + k] = pose[12 * c + k];
+      for (int k = 0; k < 3; ++k) translation[3 * c + k] = pose[12 * c + 9 + k];
+    }
+    return rep;
+  }
+
+  // Rank certificate on the final undamped dense S: Jacobi-equilibrated Cholesky with a pivot floor
+  // of 64 eps D (the equilibrated spectrum is bounded by D).
+  bool rank_full() {
+    std::vector<double> Sh((size_t)D * D);
+    CUDA_OK(cudaMemcpyAsync(Sh.data(), d_S.p, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost, st));
+    sync();
+    double ds = 0.0;
+    for (int i = 0; i < D; ++i) ds = std::max(ds, std::fabs(Sh[(size_t)i * D + i]));
+    if (!(std::isfinite(ds) && ds > 0.0)) return false;
+    double fl = 64.0 * kEps * ds;
+    std::vector<double> sc(D);
+    for (int i = 0; i < D; ++i) sc[i] = 1.0 / std::sqrt(std::max(Sh[(size_t)i * D + i], fl));
+    for (int i = 0; i < D; ++i)
+      for (int j = 0; j < D; ++j) Sh[(size_t)i * D + j] *= sc[i] * sc[j];
+    CUDA_OK(cudaMemcpyAsync(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
+    k_dense_cholesky<<<1, 1024, 0, st>>>(D, d_Lf.p, d_status.p);
+    check_launch();
+    int ok = 0;
+    CUDA_OK(cudaMemcpyAsync(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    std::vector<double> Lh((size_t)D * D);
+    CUDA_OK(cudaMemcpyAsync(Lh.data(), d_Lf.p, sizeof(double) * Lh.size(), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (!ok) return false;
+    double tol = 64.0 * kEps * D * D;
+    for (int i = 0; i < D; ++i) {
+      double pv = Lh[(size_t)i * D + i];
+      if (!(pv * pv > tol)) return false;
+    }
+    return true;
+  }
+};
+
+NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOptions& options,
+                        std::vector<double>& rotation, std::vector<double>& translation, std::vector<double>& points,
+                        std::vector<double>& groups) {
+  CUDA_OK(cudaSetDevice(ctx->device));
+  if (problem.obs_cam.size() >= (1ull << 31)) throw SolveFailure{3, "observation count exceeds 2^31"};
+  if (options.precision == 1) {
+    Solver<float> s(ctx, problem, options);
+    return s.refine(rotation, translation, points, groups);
+  }
+  Solver<double> s(ctx, problem, options);
+  return s.refine(rotation, translation, points, groups);
+}
+
+void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOptions& options, double* residual,
+                         double* sqrt_weight, double* point_jacobian, double* camera_jacobian) {
+  CUDA_OK(cudaSetDevice(ctx->device));
+  Solver<double> s(ctx, problem, options);
+  double scene = s.scene_scale_host();
+  Gauge g = s.gauge_for(s.cur, scene);
+  size_t N = problem.obs_cam.size();
+  DBuf<double> d_sw;
+  d_sw.alloc(std::max<size_t>(N, 1), s.st);
+  LinOut<double> lo = s.lin();
+  lo.sw = d_sw.p;
+  k_linearize<double><<<grid_for(s.P, 128), 128, 0, s.st>>>(s.view(), s.state(s.cur), g, options.loss, 0.0, lo);
+  s.check_launch();
+  std::vector<double> jc(18 * N), jp(6 * N), rw(2 * N), sw(N);
+  CUDA_OK(cudaMemcpyAsync(jc.data(), s.d_jc.p, sizeof(double) * jc.size(), cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(cudaMemcpyAsync(jp.data(), s.d_jp.p, sizeof(double) * jp.size(), cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(cudaMemcpyAsync(rw.data(), s.d_rw.p, sizeof(double) * rw.size(), cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(cudaMemcpyAsync(sw.data(), d_sw.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s.st));
+  s.sync();
+  // the kernel stores sqrt-weighted rows; divide the weight back out
+  for (size_t o = 0; o < N; ++o) {
+    double w = sw[o];
+    sqrt_weight[o] = w;
+    for (int k = 0; k < 2; ++k) residual[2 * o + k] = rw[2 * o + k] / w;
+    for (int k = 0; k < 6; ++k) point_jacobian[6 * o + k] = jp[6 * o + k] / w;
+    for (int k = 0; k < 18; ++k) camera_jacobian[18 * o + k] = jc[18 * o + k] / w;
+  }
+}
+
+}  // namespace omvgba

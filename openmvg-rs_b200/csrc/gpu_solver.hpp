@@ -1,0 +1,93 @@
+// gpu_solver.hpp — interface between the host-side lowering (host.cpp) and the GPU
+// Levenberg–Marquardt driver (gpu_solver.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ba_device.cuh"
+
+namespace omvgba {
+
+// Failure carrying an omvgba_code.
+struct SolveFailure {
+  int code;
+  std::string message;
+};
+
+// The problem after native lowering (anchor frame, point-major observations, native camera order).
+struct NativeProblem {
+  bool self_cal = false;
+  int ncam = 0;
+  std::vector<double> rotation;     // ncam x 9 (row-major, world -> camera in the anchor frame)
+  std::vector<double> translation;  // ncam x 3
+  std::vector<double> points;       // P x 3
+  std::vector<uint8_t> fixed_points;
+  std::vector<uint8_t> fixed_poses;
+  std::vector<uint32_t> obs_cam;    // native camera per observation (point-major order)
+  std::vector<double> obs_px;       // N x 2 (self-calibration: centred at the principal point)
+  std::vector<uint64_t> obs_src;    // input observation index
+  std::vector<uint32_t> obs_model;  // calibrated: fixed camera model per observation
+  std::vector<uint64_t> pt_off;     // P + 1
+  bool pixel_model = true;          // pinhole pixel projection (no distortion anywhere)
+  std::vector<FixedCameraDev> models;
+  std::vector<double> groups;       // self-calibration: ng x 3 (focal, k1, k2)
+  std::vector<uint32_t> cam_group;  // per native camera
+  std::vector<int> group_dim;       // free (log f, k1, k2) prefix per group, 0 when fixed
+  int gauge_cam = -1;               // FixedBaseline camera on the S^2 chart, -1 when free
+};
+
+struct LmOptions {
+  uint64_t max_iterations = 50;
+  LossDev loss{kLossL2, 0.0};
+  double gradient_tolerance = 1e-10, step_tolerance = 1e-8, relative_cost_tolerance = 1e-6;
+  bool iterative = false;
+  double pcg_tolerance = 1e-1;
+  uint64_t pcg_max_iterations = 600;
+  int precision = 0;  // 0 FP64, 1 mixed
+  int matvec = 0;     // 0 auto, 1 explicit, 2 implicit
+  int dense_rank_limit = 2048;
+};
+
+struct NativeReport {
+  int status = 1;      // 0 converged, 1 max iterations, 2 stalled, 3 degenerate
+  int reason = -1;     // 0 cost, 1 gradient, 2 step
+  uint64_t iterations = 0, accepted = 0, rejected = 0;
+  uint64_t rej[4] = {0, 0, 0, 0};
+  double initial_cost = 0, initial_rmse = 0, final_cost = 0, final_rmse = 0;
+  double gradient_inf_norm = 0;
+  int rank = 3;        // 0 full, 2 deficient, 3 not assessed
+  uint64_t weak = 0;
+  uint64_t noninvertible = 0;
+  uint64_t pcg_terms = 0;
+  double final_damping = 0;
+  int D = 0;
+};
+
+struct Context;  // device, stream, pinned scratch
+
+Context* context_create(int device, std::string* error);
+void context_destroy(Context* ctx);
+
+// Runs the LM refinement on the GPU; on return points/rotation/translation/groups hold the refined
+// native state. Throws SolveFailure.
+NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOptions& options,
+                        std::vector<double>& rotation, std::vector<double>& translation,
+                        std::vector<double>& points, std::vector<double>& groups);
+
+// First linearization, per observation (point-major): see omvgba_debug_linearize.
+void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOptions& options, double* residual,
+                         double* sqrt_weight, double* point_jacobian, double* camera_jacobian);
+
+// Residual norms of an input problem's observations with a world-frame state, for the Solution
+// metrics (solver.rs:1052-1131). active: per point flag. Returns false when a projection fails.
+struct WorldMetrics {
+  double cost = 0, rmse = 0;
+  uint64_t count = 0;
+  uint64_t inliers = 0;
+  double inlier_sq = 0;
+  bool ok = false;
+};
+
+}  // namespace omvgba

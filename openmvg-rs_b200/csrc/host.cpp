@@ -1,0 +1,1204 @@
+// host.cpp — C ABI (include/ba_cuda.h) of the B200 bundle-adjustment solver: problem validation,
+// native lowering, quarantine re-solves, report and Solution construction around the GPU LM loop.
+//
+// Reference (paths relative to the openmvg-rs root):
+//   NativeBundleAdjuster::solve ...... native/mod.rs:235-367 (routing, quarantine)
+//   problem / config checks .......... problem.rs:492-577, solver.rs:122-141
+//   gauge plans ...................... native/gauge.rs:9-330
+//   world rebase ..................... native/world_rebase.rs:19-87
+//   calibrated lowering .............. native/calibrated.rs:200-460
+//   self-calibrating lowering ........ native/self_calibration.rs:47-198, 442-512
+//   report mapping ................... native/reporting.rs:24-141
+//   Solution metrics ................. solver.rs:803-1131; weak points solver.rs:1149-1226
+//   quarantine ....................... quarantine.rs:34-96
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/ba_cuda.h"
+#include "gpu_solver.hpp"
+
+namespace omvgba {
+namespace {
+
+using Mat3 = std::array<std::array<double, 3>, 3>;
+using Vec3 = std::array<double, 3>;
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw SolveFailure{code, msg}; }
+
+Mat3 pose_R(const omvgba_pose& p) {
+  Mat3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r[i][j] = p.rotation[i * 3 + j];
+  return r;
+}
+Vec3 pose_C(const omvgba_pose& p) { return {p.center[0], p.center[1], p.center[2]}; }
+Vec3 point_at(const omvgba_problem& pr, size_t i) { return {pr.points[3 * i], pr.points[3 * i + 1], pr.points[3 * i + 2]}; }
+bool point_fixed(const omvgba_problem& pr, size_t i) { return pr.point_fixed && pr.point_fixed[i]; }
+bool all_finite(const double* v, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+Mat3 mat_mul(const Mat3& a, const Mat3& b) {
+  Mat3 c{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) c[i][j] += a[i][k] * b[k][j];
+  return c;
+}
+Vec3 rotate(const Mat3& r, const Vec3& x) {
+  return {r[0][0] * x[0] + r[0][1] * x[1] + r[0][2] * x[2], r[1][0] * x[0] + r[1][1] * x[1] + r[1][2] * x[2],
+          r[2][0] * x[0] + r[2][1] * x[1] + r[2][2] * x[2]};
+}
+Vec3 rotate_t(const Mat3& r, const Vec3& v) {
+  return {r[0][0] * v[0] + r[1][0] * v[1] + r[2][0] * v[2], r[0][1] * v[0] + r[1][1] * v[1] + r[2][1] * v[2],
+          r[0][2] * v[0] + r[1][2] * v[1] + r[2][2] * v[2]};
+}
+double sqdist(const Vec3& a, const Vec3& b) {
+  double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return dx * dx + dy * dy + dz * dz;
+}
+
+FixedCameraDev make_fixed_camera(const omvgba_intrinsic& in) {
+  FixedCameraDev m{};
+  m.fx = in.fx;
+  m.fy = in.fy;
+  m.cx = in.cx;
+  m.cy = in.cy;
+  if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+    m.radial_kind = in.radial_kind;
+    m.tangential_kind = in.tangential_kind;
+    m.k1 = in.radial_kind >= 1 ? in.k1 : 0.0;
+    m.k2 = in.radial_kind >= 2 ? in.k2 : 0.0;
+    m.k3 = in.radial_kind >= 3 ? in.k3 : 0.0;
+    m.p1 = in.tangential_kind >= 1 ? in.p1 : 0.0;
+    m.p2 = in.tangential_kind >= 2 ? in.p2 : 0.0;
+    double t;
+    m.has_turn = first_radial_turn_squared(m.k1, m.k2, &t) ? 1 : 0;
+    m.turn_squared = m.has_turn ? t : INFINITY;
+  } else {
+    m.radial_kind = 0;
+    m.tangential_kind = 0;
+    m.has_turn = 0;
+    m.turn_squared = INFINITY;
+  }
+  return m;
+}
+
+LossDev problem_loss(const omvgba_problem& pr) {
+  if (pr.loss_kind == OMVGBA_LOSS_HUBER) return {kLossHuber, pr.loss_scale};
+  if (pr.loss_kind == OMVGBA_LOSS_CAUCHY) return {kLossCauchy, pr.loss_scale / std::sqrt(2.0)};
+  return {kLossL2, 0.0};
+}
+
+// ---- validation ----------------------------------------------------------------------------
+void validate_problem(const omvgba_problem& pr) {
+  if (pr.pose_count == 0) fail(OMVGBA_INVALID_PROBLEM, "bundle adjustment requires at least one pose");
+  if (pr.intrinsic_count == 0) fail(OMVGBA_INVALID_PROBLEM, "bundle adjustment requires at least one intrinsic");
+  if (pr.point_count == 0) fail(OMVGBA_INVALID_PROBLEM, "bundle adjustment requires at least one point");
+  if (pr.observation_count == 0) fail(OMVGBA_INVALID_PROBLEM, "bundle adjustment requires at least one observation");
+  if (!pr.poses || !pr.intrinsics || !pr.points || !pr.observation_pose || !pr.observation_intrinsic ||
+      !pr.observation_point || !pr.observation_pixel)
+    fail(OMVGBA_INVALID_ARGUMENT, "problem arrays must not be null");
+  for (size_t i = 0; i < pr.pose_count; ++i) {
+    Mat3 R = pose_R(pr.poses[i]);
+    bool ok = all_finite(pr.poses[i].rotation, 9) && all_finite(pr.poses[i].center, 3);
+    for (int a = 0; a < 3 && ok; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double s = R[0][a] * R[0][b] + R[1][a] * R[1][b] + R[2][a] * R[2][b];
+        if (std::fabs(s - (a == b ? 1.0 : 0.0)) > 9.5367431640625e-7) ok = false;
+      }
+    double det = R[0][0] * (R[1][1] * R[2][2] - R[1][2] * R[2][1]) - R[0][1] * (R[1][0] * R[2][2] - R[1][2] * R[2][0]) +
+                 R[0][2] * (R[1][0] * R[2][1] - R[1][1] * R[2][0]);
+    if (!ok || !(det > 0.0)) fail(OMVGBA_INVALID_PROBLEM, "pose " + std::to_string(i) + " is not a valid rigid transform");
+  }
+  for (size_t i = 0; i < pr.intrinsic_count; ++i)
+    if (pr.intrinsics[i].fixed_model && pr.intrinsics[i].variables != 0)
+      fail(OMVGBA_INVALID_PROBLEM, "a fixed intrinsic cannot expose variable coordinates");
+  for (size_t i = 0; i < pr.point_count; ++i)
+    if (!all_finite(pr.points + 3 * i, 3)) fail(OMVGBA_INVALID_PROBLEM, "point coordinates must be finite");
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    if (!all_finite(pr.observation_pixel + 2 * o, 2)) fail(OMVGBA_INVALID_PROBLEM, "observation pixels must be finite");
+    if (pr.observation_pose[o] >= pr.pose_count)
+      fail(OMVGBA_INVALID_PROBLEM, "observation " + std::to_string(o) + " references pose out of bounds");
+    if (pr.observation_point[o] >= pr.point_count)
+      fail(OMVGBA_INVALID_PROBLEM, "observation " + std::to_string(o) + " references point out of bounds");
+    if (pr.observation_intrinsic[o] >= pr.intrinsic_count)
+      fail(OMVGBA_INVALID_PROBLEM, "observation " + std::to_string(o) + " references intrinsic out of bounds");
+  }
+  if (pr.loss_kind != OMVGBA_LOSS_SQUARED && pr.loss_scale_space != pr.residual_space)
+    fail(OMVGBA_INVALID_PROBLEM, "robust-loss scale units do not match the problem residual space");
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) {
+    if (pr.gauge_first >= pr.pose_count || pr.gauge_second >= pr.pose_count)
+      fail(OMVGBA_INVALID_PROBLEM, "fixed-baseline gauge references an out-of-range pose");
+    if (pr.gauge_first == pr.gauge_second) fail(OMVGBA_INVALID_PROBLEM, "fixed-baseline gauge requires two distinct poses");
+    if (!std::isfinite(pr.gauge_distance) || pr.gauge_distance <= 0.0)
+      fail(OMVGBA_INVALID_PROBLEM, "fixed-baseline distance must be finite and positive");
+  }
+}
+
+void validate_config(const omvgba_config& c) {
+  if (c.max_iterations == 0) fail(OMVGBA_INVALID_CONFIG, "max_iterations must be positive");
+  const char* names[3] = {"function_tolerance", "gradient_tolerance", "parameter_tolerance"};
+  double vals[3] = {c.function_tolerance, c.gradient_tolerance, c.parameter_tolerance};
+  for (int i = 0; i < 3; ++i)
+    if (!std::isfinite(vals[i]) || vals[i] <= 0.0) fail(OMVGBA_INVALID_CONFIG, names[i]);
+  if (c.has_workspace_budget && c.workspace_budget_bytes == 0)
+    fail(OMVGBA_INVALID_CONFIG, "workspace_budget_bytes must be positive");
+  if (c.precision != OMVGBA_PRECISION_FP64 && c.precision != OMVGBA_PRECISION_MIXED)
+    fail(OMVGBA_INVALID_CONFIG, "precision must be FP64 or MIXED");
+}
+
+// ---- gauge plans ---------------------------------------------------------------------------
+std::vector<uint8_t> observed_cameras(const omvgba_problem& pr) {
+  std::vector<uint8_t> o(pr.pose_count, 0);
+  for (size_t i = 0; i < pr.observation_count; ++i) o[pr.observation_pose[i]] = 1;
+  return o;
+}
+int farthest_camera(const std::vector<std::pair<int, double>>& cands) {
+  int best = -1;
+  double bs = 0.0;
+  for (auto& c : cands) {
+    if (!std::isfinite(c.second)) continue;
+    if (best < 0 || c.second > bs || (c.second == bs && c.first < best)) {
+      best = c.first;
+      bs = c.second;
+    }
+  }
+  return (best >= 0 && bs > 0.0) ? best : -1;
+}
+
+struct GaugePlan {
+  size_t anchor = 0;
+  double scale = 1.0;
+  int native_cam = -1;
+  std::vector<uint32_t> masks;
+};
+
+GaugePlan gauge_plan(const omvgba_problem& pr) {
+  auto observed = observed_cameras(pr);
+  bool controls = false;
+  for (size_t o = 0; o < pr.observation_count; ++o) controls = controls || point_fixed(pr, pr.observation_point[o]);
+  if (pr.gauge_kind == OMVGBA_GAUGE_FREE && controls) {
+    bool any = false;
+    for (size_t i = 0; i < pr.pose_count; ++i) any = any || (observed[i] && pr.poses[i].variables == 0);
+    if (!any)
+      fail(OMVGBA_UNSUPPORTED,
+           "native BA with fixed world points requires an explicitly fixed observed pose or fixed-baseline anchor");
+  }
+  GaugePlan plan;
+  for (size_t i = 0; i < pr.pose_count; ++i) plan.masks.push_back(pr.poses[i].variables);
+  if (pr.gauge_kind == OMVGBA_GAUGE_FREE) {
+    size_t anchor = SIZE_MAX, first = SIZE_MAX;
+    for (size_t i = 0; i < pr.pose_count; ++i) {
+      if (observed[i] && pr.poses[i].variables == 0) {
+        anchor = i;
+        break;
+      }
+      if (observed[i] && first == SIZE_MAX) first = i;
+    }
+    if (anchor == SIZE_MAX) anchor = first == SIZE_MAX ? 0 : first;
+    Vec3 ac = pose_C(pr.poses[anchor]);
+    bool sets = false;
+    for (size_t i = 0; i < pr.pose_count; ++i)
+      sets = sets || (i != anchor && observed[i] && pr.poses[i].variables == 0 && sqdist(pose_C(pr.poses[i]), ac) > 0.0);
+    for (size_t o = 0; o < pr.observation_count; ++o) {
+      size_t p = pr.observation_point[o];
+      sets = sets || (point_fixed(pr, p) && sqdist(point_at(pr, p), ac) > 0.0);
+    }
+    plan.anchor = anchor;
+    if (!sets) {
+      std::vector<std::pair<int, double>> c;
+      for (size_t i = 0; i < pr.pose_count; ++i)
+        if (i != anchor && observed[i] && pr.poses[i].variables != 0) c.push_back({(int)i, sqdist(pose_C(pr.poses[i]), ac)});
+      int cam = farthest_camera(c);
+      if (cam < 0) fail(OMVGBA_UNSUPPORTED, "free-scale BA has no nonzero active baseline");
+      plan.native_cam = cam;
+    }
+    return plan;
+  }
+  Vec3 c1 = pose_C(pr.poses[pr.gauge_first]), c2 = pose_C(pr.poses[pr.gauge_second]);
+  double current = std::sqrt(sqdist(c2, c1));
+  if (!std::isfinite(current) || current <= 0.0) fail(OMVGBA_UNSUPPORTED, "fixed-baseline cameras have no usable separation");
+  double raw = pr.gauge_distance / current;
+  double tol = 256.0 * kEps * std::max({std::fabs(current), std::fabs(pr.gauge_distance), 1.0});
+  double scale = std::fabs(current - pr.gauge_distance) <= tol ? 1.0 : raw;
+  if (scale != 1.0) {
+    bool moves = false;
+    for (size_t i = 0; i < pr.pose_count; ++i)
+      moves = moves || (i != pr.gauge_first && !(pr.poses[i].variables & OMVGBA_POSE_TRANSLATION));
+    for (size_t i = 0; i < pr.point_count; ++i) moves = moves || point_fixed(pr, i);
+    if (moves) fail(OMVGBA_UNSUPPORTED, "fixed-baseline scaling would move fixed state");
+  }
+  plan.anchor = pr.gauge_first;
+  plan.scale = scale;
+  plan.native_cam = (pr.poses[pr.gauge_second].variables & OMVGBA_POSE_TRANSLATION) ? (int)pr.gauge_second : -1;
+  return plan;
+}
+
+GaugePlan calibrated_gauge_plan(const omvgba_problem& pr) {
+  auto observed = observed_cameras(pr);
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) {
+    GaugePlan p = gauge_plan(pr);
+    p.masks[p.anchor] = 0;
+    return p;
+  }
+  GaugePlan plan;
+  for (size_t i = 0; i < pr.pose_count; ++i) plan.masks.push_back(pr.poses[i].variables);
+  size_t first = SIZE_MAX;
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (observed[i]) {
+      first = i;
+      break;
+    }
+  if (first == SIZE_MAX) fail(OMVGBA_INTERNAL, "checked bundle has no observed pose");
+  size_t fixed_anchor = SIZE_MAX;
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (observed[i] && plan.masks[i] == 0) {
+      fixed_anchor = i;
+      break;
+    }
+  bool controls = false;
+  for (size_t o = 0; o < pr.observation_count; ++o) controls = controls || point_fixed(pr, pr.observation_point[o]);
+  if (controls && fixed_anchor == SIZE_MAX) {
+    plan.anchor = first;
+    return plan;
+  }
+  std::vector<size_t> held;
+  size_t known_rot = SIZE_MAX;
+  for (size_t i = 0; i < pr.pose_count; ++i) {
+    if (observed[i] && !(plan.masks[i] & OMVGBA_POSE_TRANSLATION)) held.push_back(i);
+    if (known_rot == SIZE_MAX && observed[i] && !(plan.masks[i] & OMVGBA_POSE_ROTATION)) known_rot = i;
+  }
+  size_t anchor = fixed_anchor != SIZE_MAX ? fixed_anchor : (!held.empty() ? held[0] : (known_rot != SIZE_MAX ? known_rot : first));
+  Vec3 ac = pose_C(pr.poses[anchor]);
+  bool distinct = false;
+  for (size_t c : held) distinct = distinct || sqdist(pose_C(pr.poses[c]), ac) > 0.0;
+  if (!controls && held.empty())
+    plan.masks[anchor] = 0;
+  else if (!controls && known_rot == SIZE_MAX && !distinct)
+    plan.masks[anchor] = 0;
+  bool control_scale = false;
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    size_t p = pr.observation_point[o];
+    control_scale = control_scale || (point_fixed(pr, p) && sqdist(point_at(pr, p), ac) > 0.0);
+  }
+  plan.anchor = anchor;
+  if (!(distinct || control_scale)) {
+    std::vector<std::pair<int, double>> c;
+    for (size_t i = 0; i < pr.pose_count; ++i)
+      if (i != anchor && observed[i] && (plan.masks[i] & OMVGBA_POSE_TRANSLATION))
+        c.push_back({(int)i, sqdist(pose_C(pr.poses[i]), ac)});
+    int cam = farthest_camera(c);
+    if (cam < 0) fail(OMVGBA_UNSUPPORTED, "free-scale BA has no nonzero active baseline");
+    plan.native_cam = cam;
+  }
+  return plan;
+}
+
+// ---- lowering --------------------------------------------------------------------------------
+struct Rebase {
+  Mat3 R;
+  Vec3 C;
+  double scale = 1.0;
+  std::vector<size_t> camera_source_order;
+};
+
+void set_anchor(const omvgba_problem& pr, Rebase& rb, size_t anchor, double scale) {
+  rb.R = pose_R(pr.poses[anchor]);
+  rb.C = pose_C(pr.poses[anchor]);
+  rb.scale = scale;
+  if (!std::isfinite(scale) || scale <= 0.0) fail(OMVGBA_UNSUPPORTED, "world scale must be finite and positive");
+  rb.camera_source_order.clear();
+  rb.camera_source_order.push_back(anchor);
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (i != anchor) rb.camera_source_order.push_back(i);
+}
+void pose_to_native(const Rebase& rb, const omvgba_pose& p, double* R9, double* t3) {
+  Mat3 R = pose_R(p);
+  Vec3 C = pose_C(p);
+  if (R == rb.R && C == rb.C) {
+    for (int k = 0; k < 9; ++k) R9[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    t3[0] = t3[1] = t3[2] = 0.0;
+    return;
+  }
+  Mat3 AT;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) AT[i][j] = rb.R[j][i];
+  Mat3 rot = mat_mul(R, AT);
+  Vec3 t = rotate(R, {rb.C[0] - C[0], rb.C[1] - C[1], rb.C[2] - C[2]});
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) R9[3 * i + j] = rot[i][j];
+  for (int k = 0; k < 3; ++k) t3[k] = t[k] * rb.scale;
+}
+Vec3 point_to_native(const Rebase& rb, const Vec3& X) {
+  Vec3 r = rotate(rb.R, {X[0] - rb.C[0], X[1] - rb.C[1], X[2] - rb.C[2]});
+  return {r[0] * rb.scale, r[1] * rb.scale, r[2] * rb.scale};
+}
+void pose_from_native(const Rebase& rb, const double* R9, const double* t3, double* Rout, double* Cout) {
+  Mat3 Rr;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Rr[i][j] = R9[3 * i + j];
+  Mat3 R = mat_mul(Rr, rb.R);
+  Vec3 rc = rotate_t(Rr, {t3[0], t3[1], t3[2]});
+  Vec3 wc = rotate_t(rb.R, {-rc[0], -rc[1], -rc[2]});
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Rout[3 * i + j] = R[i][j];
+  for (int k = 0; k < 3; ++k) Cout[k] = rb.C[k] + wc[k];
+}
+Vec3 point_from_native(const Rebase& rb, const double* X) {
+  Vec3 r = rotate_t(rb.R, {X[0], X[1], X[2]});
+  return {rb.C[0] + r[0], rb.C[1] + r[1], rb.C[2] + r[2]};
+}
+
+bool has_free_intrinsics(const omvgba_problem& pr) {
+  for (size_t o = 0; o < pr.observation_count; ++o)
+    if (pr.intrinsics[pr.observation_intrinsic[o]].variables != 0) return true;
+  return false;
+}
+bool single_pose_intrinsics(const omvgba_problem& pr, std::vector<size_t>* out) {
+  std::vector<size_t> idx(pr.pose_count, SIZE_MAX);
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    size_t& s = idx[pr.observation_pose[o]];
+    if (s != SIZE_MAX && s != pr.observation_intrinsic[o]) return false;
+    s = pr.observation_intrinsic[o];
+  }
+  for (auto& s : idx)
+    if (s == SIZE_MAX) s = 0;
+  *out = idx;
+  return true;
+}
+
+// point-major CSR with a stable sort by point (counting sort keeps source order within a track)
+void sort_observations(const omvgba_problem& pr, NativeProblem& n, const std::vector<size_t>& dest,
+                       std::vector<size_t>* order_out) {
+  size_t N = pr.observation_count, P = pr.point_count;
+  n.pt_off.assign(P + 1, 0);
+  for (size_t o = 0; o < N; ++o) n.pt_off[pr.observation_point[o] + 1]++;
+  for (size_t p = 0; p < P; ++p) n.pt_off[p + 1] += n.pt_off[p];
+  std::vector<size_t> order(N);
+  std::vector<uint64_t> fill(n.pt_off.begin(), n.pt_off.end() - 1);
+  for (size_t o = 0; o < N; ++o) order[fill[pr.observation_point[o]]++] = o;
+  n.obs_cam.resize(N);
+  n.obs_src.resize(N);
+  for (size_t i = 0; i < N; ++i) {
+    n.obs_cam[i] = (uint32_t)dest[pr.observation_pose[order[i]]];
+    n.obs_src[i] = order[i];
+  }
+  *order_out = std::move(order);
+}
+
+struct Lowered {
+  NativeProblem n;
+  Rebase rb;
+};
+
+Lowered lower_calibrated(const omvgba_problem& pr) {
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    int m = pr.intrinsics[pr.observation_intrinsic[o]].model;
+    if (m == OMVGBA_CAMERA_FISHEYE || m == OMVGBA_CAMERA_SPHERICAL)
+      fail(OMVGBA_UNSUPPORTED,
+           "pixel BA supports fixed pinhole and Brown-Conrady cameras; use angular residuals for wide-angle cameras");
+  }
+  GaugePlan plan = calibrated_gauge_plan(pr);
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (plan.masks[i] != 0 && plan.masks[i] != OMVGBA_POSE_FREE)
+      fail(OMVGBA_UNSUPPORTED, "partial pose-variable masks (rotation-only or translation-only) are not supported by this adjuster");
+  auto observed = observed_cameras(pr);
+  Lowered L;
+  NativeProblem& n = L.n;
+  n.self_cal = false;
+  set_anchor(pr, L.rb, plan.anchor, plan.scale);
+  n.ncam = (int)pr.pose_count;
+  std::vector<size_t> dest(pr.pose_count);
+  for (size_t d = 0; d < L.rb.camera_source_order.size(); ++d) dest[L.rb.camera_source_order[d]] = d;
+  n.rotation.resize(9 * pr.pose_count);
+  n.translation.resize(3 * pr.pose_count);
+  for (size_t d = 0; d < L.rb.camera_source_order.size(); ++d) {
+    size_t s = L.rb.camera_source_order[d];
+    if (observed[s]) {
+      pose_to_native(L.rb, pr.poses[s], &n.rotation[9 * d], &n.translation[3 * d]);
+    } else {
+      for (int k = 0; k < 9; ++k) n.rotation[9 * d + k] = (k % 4 == 0) ? 1.0 : 0.0;
+      for (int k = 0; k < 3; ++k) n.translation[3 * d + k] = 0.0;
+    }
+    n.fixed_poses.push_back(plan.masks[s] == 0);
+  }
+  std::vector<uint8_t> pobs(pr.point_count, 0);
+  for (size_t o = 0; o < pr.observation_count; ++o) pobs[pr.observation_point[o]] = 1;
+  n.points.resize(3 * pr.point_count);
+  for (size_t i = 0; i < pr.point_count; ++i) {
+    Vec3 X = (point_fixed(pr, i) && !pobs[i]) ? Vec3{0, 0, 0} : point_to_native(L.rb, point_at(pr, i));
+    for (int k = 0; k < 3; ++k) n.points[3 * i + k] = X[k];
+    n.fixed_points.push_back(point_fixed(pr, i) ? 1 : 0);
+  }
+  std::vector<size_t> pose_intr;
+  bool single = single_pose_intrinsics(pr, &pose_intr);
+  bool uses_full = !single;
+  for (size_t o = 0; o < pr.observation_count && !uses_full; ++o) {
+    const auto& in = pr.intrinsics[pr.observation_intrinsic[o]];
+    uses_full = in.model == OMVGBA_CAMERA_BROWN_CONRADY && (in.radial_kind != 0 || in.tangential_kind != 0);
+  }
+  n.pixel_model = !uses_full;
+  for (size_t i = 0; i < pr.intrinsic_count; ++i) n.models.push_back(make_fixed_camera(pr.intrinsics[i]));
+  n.gauge_cam = plan.native_cam >= 0 ? (int)dest[plan.native_cam] : -1;
+  std::vector<size_t> order;
+  sort_observations(pr, n, dest, &order);
+  n.obs_px.resize(2 * order.size());
+  n.obs_model.resize(order.size());
+  for (size_t i = 0; i < order.size(); ++i) {
+    n.obs_px[2 * i] = pr.observation_pixel[2 * order[i]];
+    n.obs_px[2 * i + 1] = pr.observation_pixel[2 * order[i] + 1];
+    n.obs_model[i] = pr.observation_intrinsic[order[i]];
+  }
+  return L;
+}
+
+int free_radial_dimension(const omvgba_intrinsic& in) {
+  if (in.model == OMVGBA_CAMERA_BROWN_CONRADY && (in.variables & OMVGBA_INTRINSIC_RADIAL)) {
+    if (in.radial_kind == 0) return 1;
+    if (in.radial_kind == 1) return 2;
+    return 3;
+  }
+  return 1;
+}
+
+Lowered lower_self_calibrating(const omvgba_problem& pr) {
+  std::vector<size_t> pose_intr;
+  if (!single_pose_intrinsics(pr, &pose_intr))
+    fail(OMVGBA_UNSUPPORTED, "native self-calibration requires one intrinsic group per observed pose");
+  auto observed = observed_cameras(pr);
+  for (size_t i = 0; i < pr.pose_count; ++i) {
+    uint32_t v = pr.poses[i].variables;
+    if (!observed[i] || v == 0) continue;
+    if (!(v & OMVGBA_POSE_TRANSLATION))
+      fail(OMVGBA_UNSUPPORTED, "direct native lowering cannot optimize rotation without translation");
+    if (!(v & OMVGBA_POSE_ROTATION)) fail(OMVGBA_UNSUPPORTED, "self-calibration requires full-pose or fixed camera blocks");
+  }
+  for (size_t i = 0; i < pr.intrinsic_count; ++i) {
+    const auto& in = pr.intrinsics[i];
+    if ((in.variables & OMVGBA_INTRINSIC_RADIAL) && in.model == OMVGBA_CAMERA_BROWN_CONRADY && in.radial_kind == 3)
+      fail(OMVGBA_UNSUPPORTED, "native self-calibration refines at most two declared radial coefficients");
+    if (in.variables != 0 && (!(in.variables & OMVGBA_INTRINSIC_FOCAL) || (in.variables & OMVGBA_INTRINSIC_PRINCIPAL_POINT) ||
+                              (in.variables & OMVGBA_INTRINSIC_TANGENTIAL)))
+      fail(OMVGBA_UNSUPPORTED,
+           "self-calibration refines the focal length and radial coefficients with a fixed principal point");
+  }
+  GaugePlan plan = gauge_plan(pr);
+  Lowered L;
+  NativeProblem& n = L.n;
+  n.self_cal = true;
+  set_anchor(pr, L.rb, plan.anchor, plan.scale);
+  n.ncam = (int)pr.pose_count;
+  std::vector<size_t> dest(pr.pose_count);
+  for (size_t d = 0; d < L.rb.camera_source_order.size(); ++d) dest[L.rb.camera_source_order[d]] = d;
+  n.rotation.resize(9 * pr.pose_count);
+  n.translation.resize(3 * pr.pose_count);
+  for (size_t d = 0; d < L.rb.camera_source_order.size(); ++d) {
+    size_t s = L.rb.camera_source_order[d];
+    pose_to_native(L.rb, pr.poses[s], &n.rotation[9 * d], &n.translation[3 * d]);
+    n.fixed_poses.push_back((s == plan.anchor || pr.poses[s].variables == 0) ? 1 : 0);
+    n.cam_group.push_back((uint32_t)pose_intr[s]);
+  }
+  n.points.resize(3 * pr.point_count);
+  for (size_t i = 0; i < pr.point_count; ++i) {
+    Vec3 X = point_to_native(L.rb, point_at(pr, i));
+    for (int k = 0; k < 3; ++k) n.points[3 * i + k] = X[k];
+    n.fixed_points.push_back(point_fixed(pr, i) ? 1 : 0);
+  }
+  for (size_t i = 0; i < pr.intrinsic_count; ++i) {
+    const auto& in = pr.intrinsics[i];
+    if (in.model == OMVGBA_CAMERA_FISHEYE || in.model == OMVGBA_CAMERA_SPHERICAL)
+      fail(OMVGBA_UNSUPPORTED, "self-calibration supports perspective cameras only");
+    double k1 = 0, k2 = 0, k3 = 0, p1 = 0, p2 = 0;
+    if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+      k1 = in.radial_kind >= 1 ? in.k1 : 0.0;
+      k2 = in.radial_kind >= 2 ? in.k2 : 0.0;
+      k3 = in.radial_kind >= 3 ? in.k3 : 0.0;
+      p1 = in.tangential_kind >= 1 ? in.p1 : 0.0;
+      p2 = in.tangential_kind >= 2 ? in.p2 : 0.0;
+    }
+    if (in.fx != in.fy || k3 != 0.0 || p1 != 0.0 || p2 != 0.0)
+      fail(OMVGBA_UNSUPPORTED,
+           "self-calibration requires isotropic focal length, k1+k2 radial distortion, and no tangential distortion");
+    n.groups.push_back(in.fx);
+    n.groups.push_back(k1);
+    n.groups.push_back(k2);
+    n.group_dim.push_back(in.variables == 0 ? 0 : free_radial_dimension(in));
+  }
+  n.gauge_cam = plan.native_cam >= 0 ? (int)dest[plan.native_cam] : -1;
+  std::vector<size_t> order;
+  sort_observations(pr, n, dest, &order);
+  n.obs_px.resize(2 * order.size());
+  for (size_t i = 0; i < order.size(); ++i) {
+    const auto& in = pr.intrinsics[pr.observation_intrinsic[order[i]]];
+    n.obs_px[2 * i] = pr.observation_pixel[2 * order[i]] - in.cx;
+    n.obs_px[2 * i + 1] = pr.observation_pixel[2 * order[i] + 1] - in.cy;
+  }
+  return L;
+}
+
+Lowered lower(const omvgba_problem& pr) {
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR)
+    fail(OMVGBA_UNSUPPORTED, "angular residuals are not supported by this adjuster");
+  return has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+}
+
+int reduced_dimension(const NativeProblem& n) {
+  int D = 0;
+  for (int c = 0; c < n.ncam; ++c) D += (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+  if (n.self_cal)
+    for (int d : n.group_dim) D += d;
+  return D;
+}
+
+LmOptions lm_options(const omvgba_problem& pr, const omvgba_config& cfg, const NativeProblem& n) {
+  LmOptions o;
+  o.max_iterations = cfg.max_iterations;
+  o.loss = problem_loss(pr);
+  o.gradient_tolerance = cfg.gradient_tolerance;
+  o.step_tolerance = cfg.parameter_tolerance;
+  o.relative_cost_tolerance = cfg.function_tolerance;
+  int D = reduced_dimension(n);
+  if (cfg.linear_solver == OMVGBA_SOLVER_DIRECT)
+    o.iterative = false;
+  else if (cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE)
+    o.iterative = true;
+  else
+    o.iterative = D > o.dense_rank_limit;  // Auto: dense direct below the dense limit
+  if (!o.iterative && D > 8192)
+    fail(OMVGBA_RESOURCE_EXHAUSTED, "direct solve of a reduced system above 8192 unknowns is not supported; use Iterative");
+  o.pcg_tolerance = cfg.pcg_relative_tolerance > 0.0 ? cfg.pcg_relative_tolerance : 1e-1;
+  o.pcg_max_iterations = cfg.pcg_max_iterations > 0 ? cfg.pcg_max_iterations : 600;
+  o.precision = cfg.precision;
+  o.matvec = cfg.matvec;
+  return o;
+}
+
+// ---- solution ----------------------------------------------------------------------------------
+struct Result {
+  std::vector<omvgba_pose> poses;
+  std::vector<omvgba_intrinsic> intrinsics;
+  std::vector<double> points;
+  std::vector<uint64_t> quarantined;
+  omvgba_report report{};
+};
+
+bool residual_norm(const omvgba_problem& pr, size_t o, const omvgba_pose& pose, const omvgba_intrinsic& in,
+                   const double* X, double* out) {
+  if (in.model != OMVGBA_CAMERA_PINHOLE && in.model != OMVGBA_CAMERA_BROWN_CONRADY) return false;
+  Mat3 R = pose_R(pose);
+  Vec3 C = pose_C(pose);
+  Vec3 xc = rotate(R, {X[0] - C[0], X[1] - C[1], X[2] - C[2]});
+  FixedCameraDev m = make_fixed_camera(in);
+  double u, v;
+  if (!m.project(xc[0], xc[1], xc[2], &u, &v)) return false;
+  double nrm = std::hypot(u - pr.observation_pixel[2 * o], v - pr.observation_pixel[2 * o + 1]);
+  if (!std::isfinite(nrm)) return false;
+  *out = nrm;
+  return true;
+}
+
+bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active, const Result* sol, double* cost,
+                    double* rmse) {
+  LossDev loss = problem_loss(pr);
+  double total = 0.0, rs = 0.0, ssr = 1.0;
+  size_t count = 0;
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    size_t p = pr.observation_point[o];
+    if (!active[p]) continue;
+    const omvgba_pose& pose = sol ? sol->poses[pr.observation_pose[o]] : pr.poses[pr.observation_pose[o]];
+    const omvgba_intrinsic& in = sol ? sol->intrinsics[pr.observation_intrinsic[o]] : pr.intrinsics[pr.observation_intrinsic[o]];
+    const double* X = sol ? &sol->points[3 * p] : pr.points + 3 * p;
+    double nrm;
+    if (!residual_norm(pr, o, pose, in, X, &nrm)) return false;
+    total += loss.cost(nrm);
+    if (nrm > 0.0) {
+      if (rs < nrm) {
+        ssr = 1.0 + ssr * (rs / nrm) * (rs / nrm);
+        rs = nrm;
+      } else {
+        ssr += (nrm / rs) * (nrm / rs);
+      }
+    }
+    count++;
+  }
+  if (count == 0 || !std::isfinite(total) || total < 0.0) return false;
+  double r = rs * std::sqrt(ssr / double(count));
+  if (!std::isfinite(r)) return false;
+  *cost = total;
+  *rmse = r;
+  return true;
+}
+
+void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& active, Result& res) {
+  double limit = pr.loss_kind == OMVGBA_LOSS_SQUARED ? INFINITY : pr.loss_scale;
+  uint64_t count = 0;
+  double ss = 0.0;
+  res.report.has_inlier_count = 0;
+  res.report.has_final_inlier_rmse = 0;
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    size_t p = pr.observation_point[o];
+    if (!active[p]) continue;
+    double nrm;
+    if (!residual_norm(pr, o, res.poses[pr.observation_pose[o]], res.intrinsics[pr.observation_intrinsic[o]],
+                       &res.points[3 * p], &nrm))
+      return;
+    if (nrm <= limit) {
+      count++;
+      ss += nrm * nrm;
+    }
+  }
+  res.report.has_inlier_count = 1;
+  res.report.inlier_count = count;
+  if (count > 0) {
+    double r = std::sqrt(ss / double(count));
+    if (std::isfinite(r)) {
+      res.report.has_final_inlier_rmse = 1;
+      res.report.final_inlier_rmse = r;
+    }
+  }
+}
+
+Result raise(const omvgba_problem& pr, const Lowered& L, const std::vector<double>& rot, const std::vector<double>& tr,
+             const std::vector<double>& points, const std::vector<double>& groups, const NativeReport& nr,
+             bool iterative) {
+  Result res;
+  auto observed = observed_cameras(pr);
+  const NativeProblem& n = L.n;
+  res.poses.assign(pr.poses, pr.poses + pr.pose_count);
+  for (size_t d = 0; d < L.rb.camera_source_order.size(); ++d) {
+    size_t s = L.rb.camera_source_order[d];
+    const omvgba_pose& in = pr.poses[s];
+    if (in.variables == 0 || !observed[s]) continue;
+    double R[9], C[3];
+    pose_from_native(L.rb, &rot[9 * d], &tr[3 * d], R, C);
+    if (in.variables & OMVGBA_POSE_ROTATION) std::memcpy(res.poses[s].rotation, R, sizeof(R));
+    if (in.variables & OMVGBA_POSE_TRANSLATION) std::memcpy(res.poses[s].center, C, sizeof(C));
+  }
+  res.points.resize(3 * pr.point_count);
+  for (size_t i = 0; i < pr.point_count; ++i) {
+    Vec3 X = point_fixed(pr, i) ? point_at(pr, i) : point_from_native(L.rb, &points[3 * i]);
+    if (!all_finite(X.data(), 3)) fail(OMVGBA_NUMERICAL, "native BA returned a non-finite point");
+    for (int k = 0; k < 3; ++k) res.points[3 * i + k] = X[k];
+  }
+  res.intrinsics.assign(pr.intrinsics, pr.intrinsics + pr.intrinsic_count);
+  if (n.self_cal)
+    for (size_t i = 0; i < pr.intrinsic_count; ++i) {
+      auto& out = res.intrinsics[i];
+      if (out.variables == 0) continue;
+      out.fx = groups[3 * i];
+      out.fy = groups[3 * i];
+      if (out.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+        if (out.radial_kind >= 1) out.k1 = groups[3 * i + 1];
+        if (out.radial_kind >= 2) out.k2 = groups[3 * i + 2];
+      }
+    }
+  omvgba_report& r = res.report;
+  std::memset(&r, 0, sizeof(r));
+  r.status = nr.status == 0 ? OMVGBA_STATUS_CONVERGED
+                            : (nr.status == 1 ? OMVGBA_STATUS_MAX_ITERATIONS
+                                              : (nr.status == 2 ? OMVGBA_STATUS_STALLED : OMVGBA_STATUS_DEGENERATE));
+  r.convergence_reason = nr.status == 0 ? nr.reason : OMVGBA_REASON_NONE;
+  r.iteration_count = nr.iterations;
+  r.initial_objective = nr.initial_cost;
+  r.final_objective = nr.final_cost;
+  r.initial_rmse = nr.initial_rmse * std::sqrt(2.0);
+  r.final_rmse = nr.final_rmse * std::sqrt(2.0);
+  r.accepted_step_count = nr.accepted;
+  r.rejected_step_count = nr.rejected;
+  r.rejected_linearization = nr.rej[0];
+  r.rejected_step_solve = nr.rej[1];
+  r.rejected_candidate = nr.rej[2];
+  r.rejected_insufficient_reduction = nr.rej[3];
+  if (!std::isfinite(nr.gradient_inf_norm) || nr.gradient_inf_norm < 0.0)
+    fail(OMVGBA_NUMERICAL, "stationarity audit requires a finite non-negative gradient norm");
+  r.has_stationarity = 1;
+  r.scaled_gradient_inf_norm = nr.gradient_inf_norm;
+  r.observability = nr.rank == 0 ? OMVGBA_OBS_FULL_RANK : (nr.rank == 2 ? OMVGBA_OBS_RANK_DEFICIENT : OMVGBA_OBS_NOT_ASSESSED);
+  r.has_weak_point_count = 1;
+  r.weak_point_count = nr.weak;
+  r.has_noninvertible_observation_count = 1;
+  r.noninvertible_observation_count = nr.noninvertible;
+  if (r.observability != OMVGBA_OBS_NOT_ASSESSED && nr.D > 0) {
+    r.has_observability_details = 1;
+    r.details_pose_rank = r.observability == OMVGBA_OBS_FULL_RANK ? nr.D : 0;
+    r.details_pose_dimension = nr.D;
+    r.details_weak_point_count = nr.weak;
+  }
+  r.has_linear_solver = 1;
+  r.linear_solver = iterative ? OMVGBA_SOLVER_ITERATIVE : OMVGBA_SOLVER_DIRECT;
+  r.pcg_iteration_count = nr.pcg_terms;
+  r.reduced_dimension = nr.D;
+  r.final_damping = nr.final_damping;
+  double vals[4] = {r.initial_objective, r.final_objective, r.initial_rmse, r.final_rmse};
+  for (double v : vals)
+    if (!std::isfinite(v) || v < 0.0) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  if (r.accepted_step_count > r.iteration_count) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  return res;
+}
+
+void finish_solution(const omvgba_problem& pr, Result& res) {
+  std::vector<uint8_t> active(pr.point_count, 1);
+  for (auto q : res.quarantined) active[q] = 0;
+  uint64_t cnt = 0;
+  for (size_t o = 0; o < pr.observation_count; ++o) cnt += active[pr.observation_point[o]];
+  res.report.has_observation_count = 1;
+  res.report.observation_count = cnt;
+  res.report.quarantined_point_count = res.quarantined.size();
+  if (!res.quarantined.empty()) {
+    double c0, r0, c1, r1;
+    if (!active_metrics(pr, active, nullptr, &c0, &r0) || !active_metrics(pr, active, &res, &c1, &r1))
+      fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+    res.report.initial_objective = c0;
+    res.report.initial_rmse = r0;
+    res.report.final_objective = c1;
+    res.report.final_rmse = r1;
+  }
+  refresh_inliers(pr, active, res);
+}
+
+void canonicalize(const omvgba_problem& pr, Result& res) {
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) {
+    double init = std::sqrt(sqdist(pose_C(pr.poses[pr.gauge_first]), pose_C(pr.poses[pr.gauge_second])));
+    if (!std::isfinite(init) || std::fabs(init - pr.gauge_distance) > 512.0 * kEps * std::max(init, pr.gauge_distance))
+      return;
+  }
+  auto& r = res.report;
+  double inc = r.final_objective - r.initial_objective;
+  double tol = 2.0 * std::sqrt(kEps) * std::max(std::fabs(r.initial_objective), 1.0);
+  if (!(inc > 0.0 && inc <= tol && r.status == OMVGBA_STATUS_CONVERGED && r.observability != OMVGBA_OBS_RANK_DEFICIENT))
+    return;
+  std::vector<uint8_t> active(pr.point_count, 1);
+  for (auto q : res.quarantined) active[q] = 0;
+  double c0, r0;
+  if (!active_metrics(pr, active, nullptr, &c0, &r0)) return;
+  bool same = true;
+  for (size_t i = 0; i < pr.pose_count && same; ++i)
+    same = std::memcmp(res.poses[i].rotation, pr.poses[i].rotation, sizeof(double) * 9) == 0 &&
+           std::memcmp(res.poses[i].center, pr.poses[i].center, sizeof(double) * 3) == 0;
+  for (size_t i = 0; i < pr.intrinsic_count && same; ++i)
+    same = std::memcmp(&res.intrinsics[i], &pr.intrinsics[i], sizeof(omvgba_intrinsic)) == 0;
+  same = same && std::memcmp(res.points.data(), pr.points, sizeof(double) * 3 * pr.point_count) == 0;
+  if (!same) {
+    res.poses.assign(pr.poses, pr.poses + pr.pose_count);
+    res.intrinsics.assign(pr.intrinsics, pr.intrinsics + pr.intrinsic_count);
+    res.points.assign(pr.points, pr.points + 3 * pr.point_count);
+    r.has_stationarity = 0;
+    r.observability = OMVGBA_OBS_NOT_ASSESSED;
+    r.has_weak_point_count = 0;
+    r.has_noninvertible_observation_count = 0;
+    r.has_observability_details = 0;
+  }
+  r.initial_objective = c0;
+  r.final_objective = c0;
+  r.initial_rmse = r0;
+  r.final_rmse = r0;
+  r.status = OMVGBA_STATUS_SKIPPED;
+  r.convergence_reason = OMVGBA_REASON_NONE;
+  refresh_inliers(pr, active, res);
+}
+
+Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  validate_config(cfg);
+  Lowered L = lower(pr);
+  LmOptions opt = lm_options(pr, cfg, L.n);
+  std::vector<double> rot, tr, pts, grp;
+  NativeReport nr = gpu_refine(ctx, L.n, opt, rot, tr, pts, grp);
+  Result res = raise(pr, L, rot, tr, pts, grp, nr, opt.iterative);
+  finish_solution(pr, res);
+  canonicalize(pr, res);
+  return res;
+}
+
+// ---- quarantine --------------------------------------------------------------------------------
+std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pose* poses, const double* points) {
+  size_t N = pr.observation_count;
+  std::vector<Vec3> off(N);
+  std::vector<double> dist(N);
+  for (size_t o = 0; o < N; ++o) {
+    size_t p = pr.observation_point[o];
+    const double* C = poses[pr.observation_pose[o]].center;
+    off[o] = {points[3 * p] - C[0], points[3 * p + 1] - C[1], points[3 * p + 2] - C[2]};
+    dist[o] = std::sqrt(off[o][0] * off[o][0] + off[o][1] * off[o][1] + off[o][2] * off[o][2]);
+  }
+  double scene = 0.0;
+  if (N > 0) {
+    std::nth_element(dist.begin(), dist.begin() + N / 2, dist.end());
+    scene = dist[N / 2];
+  }
+  std::vector<TrackGeometryDev> geo(pr.point_count);
+  for (auto& g : geo) g.init(scene);
+  for (size_t o = 0; o < N; ++o) geo[pr.observation_point[o]].push(off[o][0], off[o][1], off[o][2]);
+  std::vector<size_t> out;
+  for (size_t p = 0; p < pr.point_count; ++p)
+    if (geo[p].degenerate()) out.push_back(p);
+  return out;
+}
+
+struct Restricted {
+  std::vector<omvgba_pose> poses;
+  std::vector<omvgba_intrinsic> intrinsics;
+  std::vector<double> points;
+  std::vector<uint8_t> fixed;
+  std::vector<uint32_t> op, oi, opt;
+  std::vector<double> px;
+  omvgba_problem view{};
+  std::vector<size_t> kept;
+};
+
+void without_points(const omvgba_problem& pr, const Result* warm, const std::set<size_t>& dropped, Restricted& r) {
+  r.poses.assign(pr.poses, pr.poses + pr.pose_count);
+  r.intrinsics.assign(pr.intrinsics, pr.intrinsics + pr.intrinsic_count);
+  if (warm) {
+    for (size_t i = 0; i < pr.pose_count; ++i) {
+      uint32_t v = pr.poses[i].variables;
+      r.poses[i] = warm->poses[i];
+      r.poses[i].variables = v;
+    }
+    for (size_t i = 0; i < pr.intrinsic_count; ++i) {
+      uint32_t v = pr.intrinsics[i].variables;
+      int32_t c = pr.intrinsics[i].certification;
+      r.intrinsics[i] = warm->intrinsics[i];
+      r.intrinsics[i].variables = v;
+      r.intrinsics[i].certification = c;
+    }
+  }
+  std::vector<size_t> ni(pr.point_count, SIZE_MAX);
+  r.kept.clear();
+  for (size_t i = 0; i < pr.point_count; ++i) {
+    if (dropped.count(i)) continue;
+    ni[i] = r.kept.size();
+    r.kept.push_back(i);
+    for (int k = 0; k < 3; ++k) r.points.push_back(warm ? warm->points[3 * i + k] : pr.points[3 * i + k]);
+    r.fixed.push_back(point_fixed(pr, i) ? 1 : 0);
+  }
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    if (ni[pr.observation_point[o]] == SIZE_MAX) continue;
+    r.op.push_back(pr.observation_pose[o]);
+    r.oi.push_back(pr.observation_intrinsic[o]);
+    r.opt.push_back((uint32_t)ni[pr.observation_point[o]]);
+    r.px.push_back(pr.observation_pixel[2 * o]);
+    r.px.push_back(pr.observation_pixel[2 * o + 1]);
+  }
+  r.view = pr;
+  r.view.poses = r.poses.data();
+  r.view.intrinsics = r.intrinsics.data();
+  r.view.point_count = r.kept.size();
+  r.view.points = r.points.data();
+  r.view.point_fixed = r.fixed.data();
+  r.view.observation_count = r.op.size();
+  r.view.observation_pose = r.op.data();
+  r.view.observation_intrinsic = r.oi.data();
+  r.view.observation_point = r.opt.data();
+  r.view.observation_pixel = r.px.data();
+  validate_problem(r.view);
+}
+
+// smallest/largest eigenvalue of a symmetric 3x3 by cyclic Jacobi rotations
+void sym3_eigen_extrema(double A[3][3], double* mn, double* mx) {
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    if (off < 1e-300) break;
+    for (int a = 0; a < 3; ++a)
+      for (int b = a + 1; b < 3; ++b) {
+        double apq = A[a][b];
+        if (std::fabs(apq) < 1e-300) continue;
+        double th = (A[b][b] - A[a][a]) / (2.0 * apq);
+        double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+        double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 3; ++k) {
+          double x = A[k][a], y = A[k][b];
+          A[k][a] = c * x - s * y;
+          A[k][b] = s * x + c * y;
+        }
+        for (int k = 0; k < 3; ++k) {
+          double x = A[a][k], y = A[b][k];
+          A[a][k] = c * x - s * y;
+          A[b][k] = s * x + c * y;
+        }
+      }
+  }
+  *mx = std::max({A[0][0], A[1][1], A[2][2]});
+  *mn = std::min({A[0][0], A[1][1], A[2][2]});
+}
+
+std::vector<size_t> weak_points(const omvgba_problem& pr, const Result& sol) {
+  LossDev loss = problem_loss(pr);
+  size_t P = pr.point_count;
+  std::vector<std::array<double, 9>> blocks(P, std::array<double, 9>{});
+  std::vector<uint8_t> ok(P, 1);
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    size_t p = pr.observation_point[o];
+    if (!ok[p]) continue;
+    const omvgba_pose& pose = sol.poses[pr.observation_pose[o]];
+    Mat3 R = pose_R(pose);
+    Vec3 C = pose_C(pose);
+    Vec3 xc = rotate(R, {sol.points[3 * p] - C[0], sol.points[3 * p + 1] - C[1], sol.points[3 * p + 2] - C[2]});
+    FixedCameraDev m = make_fixed_camera(sol.intrinsics[pr.observation_intrinsic[o]]);
+    double r[2], J[2][3];
+    bool good = m.linearize(xc[0], xc[1], xc[2], pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1], r, J);
+    double rn = good ? std::hypot(r[0], r[1]) : INFINITY;
+    if (!good || !std::isfinite(rn)) {
+      ok[p] = 0;
+      continue;
+    }
+    double Jw[2][3];
+    for (int a = 0; a < 2; ++a)
+      for (int c = 0; c < 3; ++c) Jw[a][c] = J[a][0] * R[0][c] + J[a][1] * R[1][c] + J[a][2] * R[2][c];
+    double w = loss.sqrt_weight(rn);
+    w *= w;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) blocks[p][3 * i + j] += w * (Jw[0][i] * Jw[0][j] + Jw[1][i] * Jw[1][j]);
+  }
+  std::vector<uint8_t> deg(P, 0);
+  for (auto q : sol.quarantined) deg[q] = 1;
+  for (size_t p : degenerate_points(pr, sol.poses.data(), sol.points.data()))
+    if (!point_fixed(pr, p)) deg[p] = 1;
+  std::vector<size_t> out;
+  for (size_t p = 0; p < P; ++p) {
+    bool weak = deg[p];
+    if (!weak && !point_fixed(pr, p)) {
+      if (!ok[p]) {
+        weak = true;
+      } else {
+        double A[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) A[i][j] = blocks[p][3 * i + j];
+        double mn, mx;
+        sym3_eigen_extrema(A, &mn, &mx);
+        weak = !(mn > 1.0e-5 * mx);
+      }
+    }
+    if (weak) out.push_back(p);
+  }
+  return out;
+}
+
+bool needs_resolve(const Result& r) {
+  return (r.report.has_weak_point_count && r.report.weak_point_count > 0) ||
+         r.report.observability == OMVGBA_OBS_RANK_DEFICIENT || r.report.status == OMVGBA_STATUS_DEGENERATE;
+}
+
+void add_origin(omvgba_report& r, const omvgba_report& origin) {
+  r.initial_objective = origin.initial_objective;
+  r.initial_rmse = origin.initial_rmse;
+  r.iteration_count += origin.iteration_count;
+  r.accepted_step_count += origin.accepted_step_count;
+  r.rejected_step_count += origin.rejected_step_count;
+  r.rejected_linearization += origin.rejected_linearization;
+  r.rejected_step_solve += origin.rejected_step_solve;
+  r.rejected_candidate += origin.rejected_candidate;
+  r.rejected_insufficient_reduction += origin.rejected_insufficient_reduction;
+  r.pcg_iteration_count += origin.pcg_iteration_count;
+}
+
+Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  validate_config(cfg);
+  std::vector<uint64_t> counts(pr.point_count, 0);
+  for (size_t o = 0; o < pr.observation_count; ++o) counts[pr.observation_point[o]]++;
+  std::vector<uint8_t> weak(pr.point_count, 0);
+  for (size_t p = 0; p < pr.point_count; ++p) weak[p] = counts[p] < 2;
+  for (size_t p : degenerate_points(pr, pr.poses, pr.points)) weak[p] = 1;
+  std::set<size_t> input_deg;
+  for (size_t p = 0; p < pr.point_count; ++p)
+    if (weak[p] && !point_fixed(pr, p)) input_deg.insert(p);
+  if (input_deg.size() == pr.point_count)
+    fail(OMVGBA_UNSUPPORTED, "no point can be adjusted: every point is seen fewer than twice or without parallax");
+  Restricted first;
+  const omvgba_problem* working = &pr;
+  std::vector<size_t> kept(pr.point_count);
+  std::iota(kept.begin(), kept.end(), 0);
+  if (!input_deg.empty()) {
+    without_points(pr, nullptr, input_deg, first);
+    working = &first.view;
+    kept = first.kept;
+  }
+  size_t quarantined = input_deg.size();
+  bool changes_scale = false;
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) changes_scale = std::fabs(gauge_plan(pr).scale - 1.0) > 1e-9;
+  if (changes_scale && quarantined > 0)
+    fail(OMVGBA_UNSUPPORTED, "native BA cannot change its physical baseline while holding out points");
+  Result sol = solve_once(ctx, *working, cfg);
+  omvgba_config retry = cfg;
+  retry.max_iterations = std::min<uint64_t>(cfg.max_iterations, 8);
+  std::vector<Restricted> chain;
+  chain.reserve(4);
+  const omvgba_problem* current = working;
+  bool have_origin = false;
+  omvgba_report origin{};
+  for (int round = 0; round < 4; ++round) {
+    if (!needs_resolve(sol)) break;
+    std::set<size_t> wk;
+    for (size_t p : weak_points(*current, sol))
+      if (!point_fixed(*current, p)) wk.insert(p);
+    if (wk.empty()) break;
+    chain.emplace_back();
+    Restricted& next = chain.back();
+    try {
+      without_points(*current, &sol, wk, next);
+    } catch (const SolveFailure&) {
+      chain.pop_back();
+      break;
+    }
+    Result resolved;
+    try {
+      resolved = solve_once(ctx, next.view, retry);
+    } catch (const SolveFailure& f) {
+      if (f.code == OMVGBA_CUDA_ERROR) throw;
+      chain.pop_back();
+      break;
+    }
+    std::vector<size_t> nk;
+    for (size_t k : next.kept) nk.push_back(kept[k]);
+    kept = nk;
+    quarantined += wk.size();
+    omvgba_report prev = sol.report;
+    if (have_origin) add_origin(prev, origin);
+    origin = prev;
+    have_origin = true;
+    sol = resolved;
+    current = &next.view;
+  }
+  if (changes_scale && quarantined > 0)
+    fail(OMVGBA_UNSUPPORTED, "native BA cannot change its physical baseline while holding out points");
+  if (quarantined == 0) return sol;
+  Result out;
+  out.poses = sol.poses;
+  out.intrinsics = sol.intrinsics;
+  out.points.assign(pr.points, pr.points + 3 * pr.point_count);
+  std::vector<uint8_t> retained(pr.point_count, 0);
+  for (size_t r = 0; r < kept.size(); ++r) {
+    retained[kept[r]] = 1;
+    for (int k = 0; k < 3; ++k) out.points[3 * kept[r] + k] = sol.points[3 * r + k];
+  }
+  for (size_t p = 0; p < pr.point_count; ++p)
+    if (!retained[p]) out.quarantined.push_back(p);
+  out.report = sol.report;
+  if (have_origin) add_origin(out.report, origin);
+  finish_solution(pr, out);
+  return out;
+}
+
+int write_error(omvgba_error* e, int code, const std::string& msg) {
+  if (e) {
+    e->code = code;
+    e->detail = -1;
+    std::snprintf(e->message, sizeof(e->message), "%s", msg.c_str());
+  }
+  return code;
+}
+
+}  // namespace
+}  // namespace omvgba
+
+struct omvgba_context {
+  omvgba::Context* ctx;
+};
+
+using namespace omvgba;
+
+extern "C" {
+
+uint32_t omvgba_abi_version(void) { return OMVGBA_ABI_VERSION; }
+const char* omvgba_adjuster_name(void) { return "openmvg-ba-cuda-b200"; }
+
+void omvgba_config_default(omvgba_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->max_iterations = 50;
+  c->function_tolerance = 1.0e-6;
+  c->gradient_tolerance = 1.0e-10;
+  c->parameter_tolerance = 1.0e-8;
+  c->linear_solver = OMVGBA_SOLVER_AUTO;
+  c->precision = OMVGBA_PRECISION_FP64;
+  c->matvec = OMVGBA_MATVEC_AUTO;
+}
+
+// Reports the struct sizes this library was compiled with, so bindings can check their layout.
+void omvgba_struct_sizes(uint64_t* out) {
+  out[0] = sizeof(omvgba_error);
+  out[1] = sizeof(omvgba_pose);
+  out[2] = sizeof(omvgba_intrinsic);
+  out[3] = sizeof(omvgba_problem);
+  out[4] = sizeof(omvgba_config);
+  out[5] = sizeof(omvgba_report);
+  out[6] = sizeof(omvgba_solution);
+}
+
+omvgba_context* omvgba_context_create(int32_t device, omvgba_error* error) {
+  std::string msg;
+  Context* c = context_create(device, &msg);
+  if (!c) {
+    write_error(error, OMVGBA_CUDA_ERROR, "context creation failed: " + msg);
+    return nullptr;
+  }
+  if (error) {
+    error->code = 0;
+    error->message[0] = 0;
+  }
+  return new omvgba_context{c};
+}
+
+void omvgba_context_destroy(omvgba_context* context) {
+  if (!context) return;
+  context_destroy(context->ctx);
+  delete context;
+}
+
+int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                     omvgba_solution* solution, omvgba_error* error) {
+  if (error) {
+    error->code = 0;
+    error->detail = -1;
+    error->message[0] = 0;
+  }
+  if (!context || !problem || !config || !solution || !solution->poses || !solution->intrinsics || !solution->points)
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  auto t0 = std::chrono::steady_clock::now();
+  try {
+    validate_problem(*problem);
+    Result r = solve_with_quarantine(context->ctx, *problem, *config);
+    std::memcpy(solution->poses, r.poses.data(), sizeof(omvgba_pose) * problem->pose_count);
+    std::memcpy(solution->intrinsics, r.intrinsics.data(), sizeof(omvgba_intrinsic) * problem->intrinsic_count);
+    std::memcpy(solution->points, r.points.data(), sizeof(double) * 3 * problem->point_count);
+    if (solution->quarantined_points)
+      for (size_t i = 0; i < r.quarantined.size(); ++i) solution->quarantined_points[i] = r.quarantined[i];
+    solution->report = r.report;
+    solution->report.solve_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
+int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                               double* residual, double* sqrt_weight, double* point_jacobian, double* camera_jacobian,
+                               uint64_t* source_index, omvgba_error* error) {
+  if (!context || !problem || !config || !residual || !sqrt_weight || !point_jacobian || !camera_jacobian || !source_index)
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  try {
+    validate_problem(*problem);
+    validate_config(*config);
+    Lowered L = lower(*problem);
+    LmOptions opt = lm_options(*problem, *config, L.n);
+    gpu_debug_linearize(context->ctx, L.n, opt, residual, sqrt_weight, point_jacobian, camera_jacobian);
+    for (size_t o = 0; o < L.n.obs_src.size(); ++o) source_index[o] = L.n.obs_src[o];
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,51 @@
+"""Loader for the in-tree libomvgba_cuda.so. There is no fallback: if the library is missing the
+import fails loudly, so a CPU or pure-Python path can never stand in for the GPU solver."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libomvgba_cuda.so")
+_lib = None
+
+
+class NativeLibraryMissing(ImportError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NativeLibraryMissing(
+            f"{LIB_PATH} is not built; run `python openmvg-rs_b200/build.py` (nvcc, sm_100a) first")
+    L = C.CDLL(LIB_PATH)
+    L.omvgba_abi_version.restype = C.c_uint32
+    L.omvgba_adjuster_name.restype = C.c_char_p
+    L.omvgba_config_default.argtypes = [C.POINTER(abi.Config)]
+    L.omvgba_struct_sizes.argtypes = [C.POINTER(C.c_uint64)]
+    L.omvgba_context_create.argtypes = [C.c_int32, C.POINTER(abi.Error)]
+    L.omvgba_context_create.restype = C.c_void_p
+    L.omvgba_context_destroy.argtypes = [C.c_void_p]
+    L.omvgba_solve.argtypes = [C.c_void_p, C.POINTER(abi.Problem), C.POINTER(abi.Config), C.POINTER(abi.Solution),
+                               C.POINTER(abi.Error)]
+    L.omvgba_solve.restype = C.c_int32
+    dp = C.POINTER(C.c_double)
+    L.omvgba_debug_linearize.argtypes = [C.c_void_p, C.POINTER(abi.Problem), C.POINTER(abi.Config), dp, dp, dp, dp,
+                                         C.POINTER(C.c_uint64), C.POINTER(abi.Error)]
+    L.omvgba_debug_linearize.restype = C.c_int32
+    L.omvgba_solve_batched.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(abi.Problem), C.POINTER(abi.Config),
+                                       C.POINTER(abi.Solution), C.POINTER(abi.Error)]
+    L.omvgba_solve_batched.restype = C.c_int32
+    _lib = L
+    return L
+
+
+def struct_sizes() -> dict:
+    out = (C.c_uint64 * 7)()
+    lib().omvgba_struct_sizes(out)
+    names = ["error", "pose", "intrinsic", "problem", "config", "report", "solution"]
+    return dict(zip(names, list(out)))

@@ -1,0 +1,67 @@
+"""``CudaBundleAdjuster``: the ``BundleAdjuster`` trait (crates/openmvg-ba/src/solver.rs:1562-1573)
+implemented by the B200 solver through the C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import lib
+from .problem import BundleProblem, Solution, SolveConfig, raise_for
+
+
+class CudaBundleAdjuster:
+    """One GPU solver context (device workspaces and stream). ``solve`` never mutates the problem."""
+
+    def __init__(self, device: int = 0):
+        err = abi.Error()
+        self._ctx = lib().omvgba_context_create(device, C.byref(err))
+        if not self._ctx:
+            raise_for(err.code or abi.OMVGBA_CUDA_ERROR, err)
+        self.device = device
+
+    def name(self) -> str:
+        return lib().omvgba_adjuster_name().decode()
+
+    def solve(self, problem: BundleProblem, config: SolveConfig | None = None) -> Solution:
+        config = config or SolveConfig()
+        mp = abi.MarshalledProblem(problem)
+        out = abi.SolutionBuffers(problem)
+        cfg = config.to_struct()
+        err = abi.Error()
+        code = lib().omvgba_solve(self._ctx, C.byref(mp.struct), C.byref(cfg), C.byref(out.struct), C.byref(err))
+        raise_for(code, err)
+        return Solution.from_buffers(out)
+
+    def debug_linearize(self, problem: BundleProblem, config: SolveConfig | None = None) -> dict:
+        config = config or SolveConfig()
+        mp = abi.MarshalledProblem(problem)
+        n = problem.observation_count
+        res = np.zeros((n, 2)); sw = np.zeros(n); jp = np.zeros((n, 2, 3)); jc = np.zeros((n, 2, 9))
+        src = np.zeros(n, dtype=np.uint64)
+        cfg = config.to_struct()
+        err = abi.Error()
+        dp = C.POINTER(C.c_double)
+        code = lib().omvgba_debug_linearize(self._ctx, C.byref(mp.struct), C.byref(cfg), res.ctypes.data_as(dp),
+                                            sw.ctypes.data_as(dp), jp.ctypes.data_as(dp), jc.ctypes.data_as(dp),
+                                            src.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(err))
+        raise_for(code, err)
+        return {"residual": res, "sqrt_weight": sw, "point_jacobian": jp, "camera_jacobian": jc, "source_index": src}
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            lib().omvgba_context_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,119 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes loader for the CPU oracle (oracle/_build/liboracle.so).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs as the checker.
+The shipped solver never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        from openmvg_ba_cuda import abi
+        L = C.CDLL(LIB_PATH)
+        L.omvgba_oracle_solve.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config), C.POINTER(abi.Solution),
+                                          C.POINTER(abi.Error)]
+        L.omvgba_oracle_solve.restype = C.c_int32
+        dp = C.POINTER(C.c_double)
+        L.omvgba_oracle_debug_linearize.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config), dp, dp, dp, dp,
+                                                    C.POINTER(C.c_uint64), C.POINTER(abi.Error)]
+        L.omvgba_oracle_debug_linearize.restype = C.c_int32
+        L.omvgba_oracle_set_threads.argtypes = [C.c_int]
+        L.omvgba_oracle_set_shards.argtypes = [C.c_int]
+        L.omvgba_oracle_max_threads.restype = C.c_int
+        L.omvgba_oracle_loss_cost.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.omvgba_oracle_loss_cost.restype = C.c_double
+        L.omvgba_oracle_loss_sqrt_weight.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.omvgba_oracle_loss_sqrt_weight.restype = C.c_double
+        L.omvgba_oracle_radial_linearize.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp, dp]
+        L.omvgba_oracle_radial_linearize.restype = C.c_int
+        L.omvgba_oracle_bc_project.argtypes = [C.POINTER(abi.Intrinsic), dp, dp]
+        L.omvgba_oracle_bc_project.restype = C.c_int
+        L.omvgba_oracle_bc_remove_distortion.argtypes = [C.POINTER(abi.Intrinsic), C.c_double, C.c_double, dp]
+        L.omvgba_oracle_bc_remove_distortion.restype = C.c_int
+        ip = C.POINTER(C.c_int)
+        L.omvgba_oracle_nielsen.argtypes = [C.c_int, ip, dp, dp, C.c_double, dp, ip, dp, ip]
+        L.omvgba_oracle_exp_so3.argtypes = [dp, dp]
+        L.omvgba_oracle_point_block_inverse.argtypes = [dp, C.c_double, dp, dp]
+        L.omvgba_oracle_point_block_inverse.restype = C.c_int
+        L.omvgba_oracle_stages.argtypes = [C.c_int, C.c_uint64, C.POINTER(C.c_uint64), ip]
+        u32p = C.POINTER(C.c_uint32)
+        L.omvgba_oracle_residual_vjp.argtypes = [C.c_uint64, u32p, u32p, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().omvgba_oracle_set_threads(int(n))
+
+
+def set_shards(n: int) -> None:
+    lib().omvgba_oracle_set_shards(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().omvgba_oracle_max_threads())
+
+
+def solve(problem, config):
+    """Run the oracle's BundleAdjuster::solve; returns openmvg_ba_cuda.problem.Solution."""
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.problem import Solution, raise_for
+    mp = abi.MarshalledProblem(problem)
+    out = abi.SolutionBuffers(problem)
+    cfg = config.to_struct()
+    err = abi.Error()
+    code = lib().omvgba_oracle_solve(C.byref(mp.struct), C.byref(cfg), C.byref(out.struct), C.byref(err))
+    raise_for(code, err)
+    return Solution.from_buffers(out)
+
+
+def debug_linearize(problem, config):
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.problem import raise_for
+    mp = abi.MarshalledProblem(problem)
+    n = problem.observation_count
+    res = np.zeros((n, 2)); sw = np.zeros(n); jp = np.zeros((n, 2, 3)); jc = np.zeros((n, 2, 9))
+    src = np.zeros(n, dtype=np.uint64)
+    err = abi.Error()
+    cfg = config.to_struct()
+    dp = C.POINTER(C.c_double)
+    code = lib().omvgba_oracle_debug_linearize(C.byref(mp.struct), C.byref(cfg), res.ctypes.data_as(dp),
+                                               sw.ctypes.data_as(dp), jp.ctypes.data_as(dp), jc.ctypes.data_as(dp),
+                                               src.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(err))
+    raise_for(code, err)
+    return {"residual": res, "sqrt_weight": sw, "point_jacobian": jp, "camera_jacobian": jc, "source_index": src}
+
+
+def residual_vjp(inputs: dict, grad=None):
+    """Analytic residual and J^T grad (float64) for the centred radial model."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    cam = np.ascontiguousarray(inputs["camera_index"], dtype=np.uint32)
+    pt = np.ascontiguousarray(inputs["point_index"], dtype=np.uint32)
+    px, rv, t, it, X = (f64(inputs[k]) for k in ("pixel", "rotvec", "translation", "intrinsics", "points"))
+    n = len(cam)
+    res = np.zeros((n, 2))
+    g = f64(grad) if grad is not None else None
+    gr, gt, gi, gp = np.zeros_like(rv), np.zeros_like(t), np.zeros_like(it), np.zeros_like(X)
+    dp = C.POINTER(C.c_double)
+    P = lambda a: a.ctypes.data_as(dp) if a is not None else None
+    u32p = C.POINTER(C.c_uint32)
+    lib().omvgba_oracle_residual_vjp(n, cam.ctypes.data_as(u32p), pt.ctypes.data_as(u32p), P(px), P(rv), P(t), P(it),
+                                     P(X), P(g), P(res), P(gr), P(gt), P(gi), P(gp))
+    return res, {"rotvec": gr, "translation": gt, "intrinsics": gi, "points": gp}

@@ -1,0 +1,97 @@
+"""GPU solver vs the CPU oracle on the same seeded problems, through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle as O
+from openmvg_ba_cuda import SolveConfig, abi, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+def _oracle_spread(problem, cfg):
+    """The oracle's own parameter sensitivity: solve again with a different (fixed) grouping of its
+    floating-point sums. GPU-vs-oracle differences are judged against this rounding floor."""
+    O.set_shards(7)
+    try:
+        return O.solve(problem, cfg)
+    finally:
+        O.set_shards(0)
+
+
+def _check_parameters(g, o, o2):
+    """Poses and intrinsics within 1e-7; every point within max(1e-7, 10x the oracle's own
+    reordering spread for that point) -- weakly observed points amplify rounding differences."""
+    assert np.max(np.abs(g.rotations - o.rotations)) < 1e-7
+    assert np.max(np.abs(g.centers - o.centers)) < 1e-7
+    for ia, ib in zip(g.intrinsics, o.intrinsics):
+        assert abs(ia.fx - ib.fx) / max(abs(ib.fx), 1.0) < 1e-7
+        assert abs(ia.k1 - ib.k1) / max(abs(ib.k1), 1.0) < 1e-7
+        assert abs(ia.k2 - ib.k2) / max(abs(ib.k2), 1.0) < 1e-7
+    dp = np.abs(g.points - o.points).max(axis=1)
+    spread = np.abs(o2.points - o.points).max(axis=1)
+    assert np.all(dp <= np.maximum(1e-7, 10.0 * spread)), (dp.max(), spread[np.argmax(dp)])
+    assert np.quantile(dp, 0.99) < 1e-7
+
+
+def _param_diff(sa, sb):
+    """max abs difference of rotations, centres, points and intrinsics between two solutions"""
+    d = max(np.max(np.abs(sa.rotations - sb.rotations)), np.max(np.abs(sa.centers - sb.centers)),
+            np.max(np.abs(sa.points - sb.points)))
+    for ia, ib in zip(sa.intrinsics, sb.intrinsics):
+        d = max(d, abs(ia.fx - ib.fx) / max(abs(ib.fx), 1.0), abs(ia.k1 - ib.k1), abs(ia.k2 - ib.k2))
+    return d
+
+
+@pytest.mark.parametrize("self_cal", [False, True])
+def test_first_linearization_matches_oracle(adjuster, self_cal):
+    p = synthetic.ring_problem(seed=3, self_calibrating=self_cal)
+    cfg = SolveConfig(linear_solver=abi.SOLVER_DIRECT)
+    g = adjuster.debug_linearize(p, cfg)
+    o = O.debug_linearize(p, cfg)
+    assert np.array_equal(g["source_index"], o["source_index"])
+    for k in ("residual", "sqrt_weight", "point_jacobian", "camera_jacobian"):
+        a, b = g[k], o[k]
+        scale = np.maximum(np.abs(b), 1.0)
+        assert np.max(np.abs(a - b) / scale) < 1e-12, k
+
+
+@pytest.mark.parametrize("self_cal", [False, True])
+def test_direct_fp64_solve_matches_oracle(adjuster, self_cal):
+    p = synthetic.ring_problem(seed=7, self_calibrating=self_cal)
+    cfg = SolveConfig(linear_solver=abi.SOLVER_DIRECT)
+    g = adjuster.solve(p, cfg)
+    o = O.solve(p, cfg)
+    rg, ro = g.report, o.report
+    for k in ("iteration_count", "accepted_step_count", "rejected_step_count", "status", "quarantined_point_count",
+              "observability", "weak_point_count", "inlier_count"):
+        assert rg[k] == ro[k], (k, rg[k], ro[k])
+    assert _rel(rg["final_objective"], ro["final_objective"]) < 1e-9
+    assert _rel(rg["initial_objective"], ro["initial_objective"]) < 1e-12
+    _check_parameters(g, o, _oracle_spread(p, cfg))
+
+
+@pytest.mark.parametrize("self_cal", [False, True])
+def test_iterative_fp64_solve_matches_oracle(adjuster, self_cal):
+    p = synthetic.ring_problem(seed=9, self_calibrating=self_cal)
+    cfg = SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, max_iterations=30)
+    g = adjuster.solve(p, cfg)
+    o = O.solve(p, cfg)
+    rg, ro = g.report, o.report
+    assert rg["iteration_count"] == ro["iteration_count"]
+    assert rg["accepted_step_count"] == ro["accepted_step_count"]
+    assert _rel(rg["final_objective"], ro["final_objective"]) < 1e-9
+    _check_parameters(g, o, _oracle_spread(p, cfg))
+
+
+def test_solve_is_bitwise_deterministic(adjuster):
+    p = synthetic.ring_problem(seed=5, self_calibrating=True)
+    cfg = SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, max_iterations=10)
+    a = adjuster.solve(p, cfg)
+    b = adjuster.solve(p, cfg)
+    assert np.array_equal(a.points, b.points)
+    assert np.array_equal(a.rotations, b.rotations)
+    assert a.report["final_objective"] == b.report["final_objective"]

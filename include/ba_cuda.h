@@ -244,6 +244,16 @@ int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* pr
                                omvgba_error* error);
 
 /*
+ * Reduced camera system product S_lambda x at the first linearization of the lowered problem,
+ * computed twice: by the matrix-free kernel the PCG uses (y_matvec) and from the explicit dense
+ * Schur complement (y_dense). With x == NULL only *dimension is written. FP64; for operator
+ * parity tests. Reference operator: crates/openmvg-ba/src/kernel/multi_view/sparse/retained/operator.rs:137-227.
+ */
+int32_t omvgba_debug_schur_product(omvgba_context* context, const omvgba_problem* problem,
+                                   const omvgba_config* config, double lambda, const double* x, double* y_matvec,
+                                   double* y_dense, int32_t* dimension, omvgba_error* error);
+
+/*
  * Reprojection residual of the centred radial model (self_calibration/model.rs:26-129) over an
  * unsorted observation list, and its vector-Jacobian product. Camera j has rotation vector
  * rotvec[3j..3j+3] (R = exp(rotvec)), translation t[3j..], intrinsics intr[3j..] = (f, k1, k2);

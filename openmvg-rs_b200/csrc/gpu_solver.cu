@@ -8,7 +8,7 @@
 //                            damping diagonal, pose/intrinsic edges, diagonal point coupling
 //       k_pairs ............ explicit Schur blocks S_bb' -= W V^-1 W^T (schur/assembly.rs:999-1038)
 //   K3  k_dense_cholesky ... dense FP64 Cholesky for small reduced systems (stands in for faer LLT)
-//       k_mv_points/blocks . matrix-free reduced-camera-system product S x (retained/operator.rs:137-227)
+//       k_mv_tiles ......... matrix-free reduced-camera-system product S x (retained/operator.rs:137-227)
 //       block-Jacobi PCG ... sparse/pcg.rs:23-119, retained/mod.rs:682-934, retained/block.rs:148-246
 //   K4  k_retract, k_candidate_points: step cap, retraction, back-substitution and candidate rule
 //                            (optimizer.rs:376-702, sparse/calibrated/candidate.rs:23-333,
@@ -21,6 +21,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -283,10 +284,22 @@ __global__ void k_dots(DotArgs args, int n, double* out) {
 // ----------------------------------------------------------------------------------------------
 // K1: per-point linearization (+ point-block factorization)
 // ----------------------------------------------------------------------------------------------
+// Per-observation Jacobian record (sqrt-weighted): 2 x 9 camera columns (pose | intrinsics), then
+// 2 x 3 point columns: kRec = 24 components. Records are stored tile-blocked and component-major:
+// component k of the observation at tile-local index i lives at tile_base + k * rs + i, rs being
+// the tile capacity. A tile's block is contiguous and 16 B aligned (one bulk async copy), and
+// threads reading one component of consecutive observations hit consecutive shared-memory banks.
+constexpr int kRec = 24;
+constexpr int kJp = 18;
+
 template <typename T>
 struct LinOut {
-  T* jc;           // N x 18 (2 rows x 9 columns: pose | intrinsics), sqrt-weighted
-  T* jp;           // N x 6, sqrt-weighted
+  T* rec;                  // ntiles x rs x kRec
+  const uint32_t* obs_rec; // N: element index of each observation's component 0
+  int rs;                  // component stride (tile capacity)
+  float* rec32;            // optional FP32 copy of the records for mixed-precision products
+  const uint32_t* obs_rec32;
+  int rs32;
   double* rw;      // N x 2, sqrt-weighted residual
   double* vinv;    // P x 6: damped point-block inverse (zero for fixed points)
   double* ig;      // P x 3: Vhat^-1 g_p (zero for fixed points)
@@ -333,8 +346,9 @@ __global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge 
     double r[2], J[2][3], Ji[2][3];
     if (!project_obs(v, s.groups, o, xc, r, J, Ji)) {
       ok = false;
-      for (int k = 0; k < 18; ++k) out.jc[(size_t)18 * o + k] = T(0);
-      for (int k = 0; k < 6; ++k) out.jp[(size_t)6 * o + k] = T(0);
+      for (int k = 0; k < kRec; ++k) out.rec[out.obs_rec[o] + (size_t)k * out.rs] = T(0);
+      if (out.rec32)
+        for (int k = 0; k < kRec; ++k) out.rec32[out.obs_rec32[o] + (size_t)k * out.rs32] = 0.0f;
       out.rw[2 * o] = 0.0;
       out.rw[2 * o + 1] = 0.0;
       continue;
@@ -374,12 +388,21 @@ __global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge 
       for (int a = 0; a < 2; ++a)
         for (int k = 0; k < id; ++k) jc[a][pd + k] = Ji[a][k];
     }
-    T* jco = out.jc + (size_t)18 * o;
+    T* jco = out.rec + out.obs_rec[o];
+    const int rs = out.rs;
     for (int a = 0; a < 2; ++a)
-      for (int k = 0; k < 9; ++k) jco[9 * a + k] = T(sw * jc[a][k]);
-    T* jpo = out.jp + (size_t)6 * o;
+      for (int k = 0; k < 9; ++k) jco[(9 * a + k) * rs] = T(sw * jc[a][k]);
+    T* jpo = jco + kJp * rs;
     for (int a = 0; a < 2; ++a)
-      for (int c = 0; c < 3; ++c) jpo[3 * a + c] = T(sw * jp[a][c]);
+      for (int c = 0; c < 3; ++c) jpo[(3 * a + c) * rs] = T(sw * jp[a][c]);
+    if (out.rec32) {
+      float* j32 = out.rec32 + out.obs_rec32[o];
+      const int r32 = out.rs32;
+      for (int a = 0; a < 2; ++a)
+        for (int k = 0; k < 9; ++k) j32[(9 * a + k) * r32] = (float)(sw * jc[a][k]);
+      for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < 3; ++c) j32[(kJp + 3 * a + c) * r32] = (float)(sw * jp[a][c]);
+    }
     out.rw[2 * o] = sw * r[0];
     out.rw[2 * o + 1] = sw * r[1];
     if (out.sw) out.sw[o] = sw;
@@ -496,17 +519,18 @@ __global__ void __launch_bounds__(32) k_block_chunks(BlockTables bt, LinOut<T> l
     uint32_t e = bt.ent[i];
     uint32_t o = e >> 1;
     uint32_t p = bt.ent_point[i];
-    const T* jc = lin.jc + (size_t)18 * o;
+    const T* jc = lin.rec + lin.obs_rec[o];
+    const int rs = lin.rs;
     double a0[6], a1[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      a0[k] = k < d ? (double)jc[col + k] : 0.0;
-      a1[k] = k < d ? (double)jc[9 + col + k] : 0.0;
+      a0[k] = k < d ? (double)jc[(col + k) * rs] : 0.0;
+      a1[k] = k < d ? (double)jc[(9 + col + k) * rs] : 0.0;
     }
     double r0 = lin.rw[2 * o], r1 = lin.rw[2 * o + 1];
-    const T* jp = lin.jp + (size_t)6 * o;
-    double p0[3] = {(double)jp[0], (double)jp[1], (double)jp[2]};
-    double p1[3] = {(double)jp[3], (double)jp[4], (double)jp[5]};
+    const T* jp = jc + kJp * rs;
+    double p0[3] = {(double)jp[0], (double)jp[rs], (double)jp[2 * rs]};
+    double p1[3] = {(double)jp[3 * rs], (double)jp[4 * rs], (double)jp[5 * rs]};
     const double* ig = lin.ig + 3 * (size_t)p;
     // reduced residual: r_w - Jp (Vhat^-1 g_p)
     double q0 = r0 - (p0[0] * ig[0] + p0[1] * ig[1] + p0[2] * ig[2]);
@@ -543,7 +567,7 @@ __global__ void __launch_bounds__(32) k_block_chunks(BlockTables bt, LinOut<T> l
       for (int r = 0; r < 6; ++r)
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-          if (k < id) E[3 * r + k] += a0[r] * (double)jc[icol + k] + a1[r] * (double)jc[9 + icol + k];
+          if (k < id) E[3 * r + k] += a0[r] * (double)jc[(icol + k) * rs] + a1[r] * (double)jc[(9 + icol + k) * rs];
     }
   }
   double* rec = chunk_out + (size_t)kAsmRec * c;
@@ -651,11 +675,14 @@ __global__ void __launch_bounds__(32) k_pairs(PairTables pt, BlockTables bt, Lin
     uint32_t ea = pt.pair_a[i], eb = pt.pair_b[i], p = pt.pair_p[i];
     uint32_t oa = ea >> 1, ob = eb >> 1;
     int ca = seg_col[ea], cbcol = seg_col[eb];
-    const T* jpa = lin.jp + (size_t)6 * oa;
-    const T* jpb = lin.jp + (size_t)6 * ob;
+    const int rs = lin.rs;
+    const T* jpa = lin.rec + lin.obs_rec[oa] + kJp * rs;
+    const T* jpb = lin.rec + lin.obs_rec[ob] + kJp * rs;
     const double* vi = lin.vinv + 6 * (size_t)p;
-    double pa0[3] = {(double)jpa[0], (double)jpa[1], (double)jpa[2]}, pa1[3] = {(double)jpa[3], (double)jpa[4], (double)jpa[5]};
-    double pb0[3] = {(double)jpb[0], (double)jpb[1], (double)jpb[2]}, pb1[3] = {(double)jpb[3], (double)jpb[4], (double)jpb[5]};
+    double pa0[3] = {(double)jpa[0], (double)jpa[rs], (double)jpa[2 * rs]};
+    double pa1[3] = {(double)jpa[3 * rs], (double)jpa[4 * rs], (double)jpa[5 * rs]};
+    double pb0[3] = {(double)jpb[0], (double)jpb[rs], (double)jpb[2 * rs]};
+    double pb1[3] = {(double)jpb[3 * rs], (double)jpb[4 * rs], (double)jpb[5 * rs]};
     double t0[3], t1[3];
     sym3_apply(vi, pb0, t0);
     sym3_apply(vi, pb1, t1);
@@ -663,17 +690,17 @@ __global__ void __launch_bounds__(32) k_pairs(PairTables pt, BlockTables bt, Lin
     double A01 = pa0[0] * t1[0] + pa0[1] * t1[1] + pa0[2] * t1[2];
     double A10 = pa1[0] * t0[0] + pa1[1] * t0[1] + pa1[2] * t0[2];
     double A11 = pa1[0] * t1[0] + pa1[1] * t1[1] + pa1[2] * t1[2];
-    const T* ja = lin.jc + (size_t)18 * oa;
-    const T* jb = lin.jc + (size_t)18 * ob;
+    const T* ja = lin.rec + lin.obs_rec[oa];
+    const T* jb = lin.rec + lin.obs_rec[ob];
 #pragma unroll
     for (int r = 0; r < 6; ++r) {
       if (r >= dr) break;
-      double a0 = (double)ja[ca + r], a1 = (double)ja[9 + ca + r];
+      double a0 = (double)ja[(ca + r) * rs], a1 = (double)ja[(9 + ca + r) * rs];
       double c0 = a0 * A00 + a1 * A10, c1 = a0 * A01 + a1 * A11;
 #pragma unroll
       for (int s2 = 0; s2 < 6; ++s2) {
         if (s2 >= dc) break;
-        acc[6 * r + s2] += c0 * (double)jb[cbcol + s2] + c1 * (double)jb[9 + cbcol + s2];
+        acc[6 * r + s2] += c0 * (double)jb[(cbcol + s2) * rs] + c1 * (double)jb[(9 + cbcol + s2) * rs];
       }
     }
   }
@@ -795,89 +822,124 @@ __global__ void k_dense_matvec(int D, const double* S, const double* x, double* 
 }
 
 // ----------------------------------------------------------------------------------------------
+// Device-side PCG control (sparse/pcg.rs:23-119). One CTA computes each scalar reduction and, in
+// its epilogue, the recurrence coefficient and the loop status, so the PCG iterations run as a
+// CUDA graph without host round trips. Every kernel of an iteration returns immediately once the
+// status leaves kRunning, so iterations launched past termination cost only their launch.
+// ----------------------------------------------------------------------------------------------
+enum PcgStatus : int { kRunning = 0, kCheckResidual = 1, kRejected = 2, kExhausted = 3 };
+struct PcgCtl {
+  double n0, rho, alpha, beta, curv, rr, rz, ratio, tol;
+  int status, terms, max_it, pad;
+};
+
+__device__ __forceinline__ bool pcg_stopped(const PcgCtl* ctl) { return ctl && ctl->status != kRunning; }
+
+// curvature = d.q, alpha = rho / curvature
+__global__ void __launch_bounds__(1024) k_pcg_alpha(int n, const double* d, const double* q, PcgCtl* ctl) {
+  if (ctl->status != kRunning) return;
+  __shared__ double sh[32];
+  int tid = threadIdx.x;
+  double acc = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) acc += d[i] * q[i];
+  acc = warp_sum(acc);
+  if ((tid & 31) == 0) sh[tid >> 5] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    double curv = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) curv += sh[w];
+    ctl->curv = curv;
+    int it = ctl->terms + 1;
+    if (!(isfinite(curv) && curv > 0.0)) {
+      ctl->terms = it - 1;
+      ctl->status = kRejected;
+      return;
+    }
+    double alpha = ctl->rho / curv;
+    if (!isfinite(alpha)) {
+      ctl->terms = it - 1;
+      ctl->status = kRejected;
+      return;
+    }
+    ctl->alpha = alpha;
+  }
+}
+
+__global__ void k_pcg_update(int n, const double* d, const double* q, double* x, double* r, const PcgCtl* ctl) {
+  if (ctl->status != kRunning) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double alpha = ctl->alpha;
+  if (i < n) {
+    x[i] += alpha * d[i];
+    r[i] -= alpha * q[i];
+  }
+}
+
+// ratio = |r| / n0, next rho = r.z, beta = next rho / rho
+__global__ void __launch_bounds__(1024) k_pcg_beta(int n, const double* r, const double* z, PcgCtl* ctl) {
+  if (ctl->status != kRunning) return;
+  __shared__ double s1[32], s2[32];
+  int tid = threadIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    a += r[i] * r[i];
+    b += r[i] * z[i];
+  }
+  a = warp_sum(a);
+  b = warp_sum(b);
+  if ((tid & 31) == 0) {
+    s1[tid >> 5] = a;
+    s2[tid >> 5] = b;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double rr = 0.0, rz = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+      rr += s1[w];
+      rz += s2[w];
+    }
+    int it = ctl->terms + 1;
+    ctl->terms = it;
+    ctl->rr = rr;
+    ctl->rz = rz;
+    double ratio = sqrt(rr) / ctl->n0;
+    ctl->ratio = ratio;
+    if (!isfinite(ratio)) {
+      ctl->status = kRejected;
+      return;
+    }
+    if (ratio <= ctl->tol) {
+      ctl->status = kCheckResidual;
+      return;
+    }
+    if (!(isfinite(rz) && rz > 0.0)) {
+      ctl->status = kRejected;
+      return;
+    }
+    double beta = rz / ctl->rho;
+    if (!isfinite(beta)) {
+      ctl->status = kRejected;
+      return;
+    }
+    ctl->beta = beta;
+    ctl->rho = rz;
+    if (it >= ctl->max_it) ctl->status = kExhausted;
+  }
+}
+
+__global__ void k_pcg_direction(int n, const double* z, double* d, const PcgCtl* ctl) {
+  // runs after k_pcg_beta; on exhaustion the reference still forms the next direction, harmlessly
+  if (ctl->status != kRunning && ctl->status != kExhausted) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = z[i] + ctl->beta * d[i];
+}
+
+// ----------------------------------------------------------------------------------------------
 // Matrix-free reduced camera system product (implicit Schur)
 // ----------------------------------------------------------------------------------------------
-// Pass 1 (point-major): e_o = Jc_o x_o; z_p = Vhat^-1 sum_o Jp_o^T e_o; f_o = e_o - Jp_o z_p
-template <typename T>
-__global__ void __launch_bounds__(128) k_mv_points(DevView v, LinOut<T> lin, const double* x, T* f) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= v.P) return;
-  uint32_t o0 = v.pt_off[p], o1 = v.pt_off[p + 1];
-  T b0 = 0, b1 = 0, b2 = 0;
-  // first pass: accumulate b
-  for (uint32_t o = o0; o < o1; ++o) {
-    int cam = v.obs_cam[o];
-    int pd = v.pose_dim[cam], po = v.pose_off[cam];
-    const T* jc = lin.jc + (size_t)18 * o;
-    T e0 = 0, e1 = 0;
-    for (int k = 0; k < pd; ++k) {
-      T xv = (T)x[po + k];
-      e0 += jc[k] * xv;
-      e1 += jc[9 + k] * xv;
-    }
-    if (v.self_cal) {
-      int g = v.cam_group[cam];
-      int id = v.intr_dim[g], io = v.intr_off[g];
-      for (int k = 0; k < id; ++k) {
-        T xv = (T)x[io + k];
-        e0 += jc[pd + k] * xv;
-        e1 += jc[9 + pd + k] * xv;
-      }
-    }
-    const T* jp = lin.jp + (size_t)6 * o;
-    b0 += jp[0] * e0 + jp[3] * e1;
-    b1 += jp[1] * e0 + jp[4] * e1;
-    b2 += jp[2] * e0 + jp[5] * e1;
-    f[2 * o] = e0;
-    f[2 * o + 1] = e1;
-  }
-  const double* vi = lin.vinv + 6 * (size_t)p;
-  T z0 = (T)vi[0] * b0 + (T)vi[1] * b1 + (T)vi[3] * b2;
-  T z1 = (T)vi[1] * b0 + (T)vi[2] * b1 + (T)vi[4] * b2;
-  T z2 = (T)vi[3] * b0 + (T)vi[4] * b1 + (T)vi[5] * b2;
-  for (uint32_t o = o0; o < o1; ++o) {
-    const T* jp = lin.jp + (size_t)6 * o;
-    f[2 * o] -= jp[0] * z0 + jp[1] * z1 + jp[2] * z2;
-    f[2 * o + 1] -= jp[3] * z0 + jp[4] * z1 + jp[5] * z2;
-  }
-}
-
-// Pass 2 (block chunks): partial y_b = sum_e Jc_e^T f_o
-template <typename T>
-__global__ void __launch_bounds__(32) k_mv_chunks(BlockTables bt, LinOut<T> lin, const T* f, double* chunk_y) {
-  int c = blockIdx.x;
-  if (c >= bt.nchunks) return;
-  int lane = threadIdx.x;
-  int b = bt.chunk_block[c];
-  int d = bt.blk_dim[b];
-  int col = bt.chunk_col[c];
-  T acc[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t i = bt.chunk_begin[c] + lane; i < bt.chunk_end[c]; i += 32) {
-    uint32_t o = bt.ent[i] >> 1;
-    const T* jc = lin.jc + (size_t)18 * o;
-    T f0 = f[2 * o], f1 = f[2 * o + 1];
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
-      if (k < d) acc[k] += jc[col + k] * f0 + jc[9 + col + k] * f1;
-  }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    double s = warp_sum((double)acc[k]);
-    if (lane == 0) chunk_y[(size_t)6 * c + k] = s;
-  }
-}
-
-// y_b = sum of chunk partials (chunk order) + lambda * diag_b x_b
-__global__ void k_mv_finalize(BlockTables bt, const double* chunk_y, const double* diag, double lambda,
-                              const double* x, double* y) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= bt.nblocks) return;
-  int o = bt.blk_off[b], d = bt.blk_dim[b];
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int c = bt.blk_chunk_begin[b]; c < bt.blk_chunk_end[b]; ++c)
-    for (int k = 0; k < d; ++k) acc[k] += chunk_y[(size_t)6 * c + k];
-  for (int k = 0; k < d; ++k) y[o + k] = acc[k] + lambda * diag[o + k] * x[o + k];
-}
+}  // namespace omvgba
+#include "mv_tiles.cuh"
+namespace omvgba {
 
 // ----------------------------------------------------------------------------------------------
 // Block-Jacobi preconditioner (FP64): P_b = U_bb + lambda D_b - C_b - cross pairs
@@ -936,7 +998,9 @@ __global__ void k_block_factor(BlockTables bt, const double* blk_out, const doub
   fail[b] = 0;
 }
 
-__global__ void k_block_precond(BlockTables bt, const double* factor, const double* r, double* z) {
+__global__ void k_block_precond(BlockTables bt, const double* factor, const double* r, double* z,
+                                const PcgCtl* ctl) {
+  if (pcg_stopped(ctl)) return;
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= bt.nblocks) return;
   int d = bt.blk_dim[b], o = bt.blk_off[b];
@@ -969,6 +1033,14 @@ __global__ void k_xpby(int n, const double* z, double beta, double* d) {
 __global__ void k_neg_copy(int n, const double* a, double* b) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = -a[i];
+}
+__global__ void k_sub(int n, const double* b, const double* q, double* r) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = b[i] - q[i];
+}
+__global__ void k_axpy(int n, double a, const double* x, double* y) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a * x[i];
 }
 __global__ void k_residual_update(int n, const double* g, const double* q, double* r) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1143,24 +1215,25 @@ __global__ void __launch_bounds__(128) k_candidate_points(DevView v, LinOut<T> l
   for (uint32_t o = v.pt_off[p]; o < v.pt_off[p + 1]; ++o) {
     int cam = v.obs_cam[o];
     int pd = v.pose_dim[cam], po = v.pose_off[cam];
-    const T* jc = lin.jc + (size_t)18 * o;
+    const T* jc = lin.rec + lin.obs_rec[o];
+    const int rs = lin.rs;
     double e0 = 0, e1 = 0;
     for (int k = 0; k < pd; ++k) {
-      e0 += (double)jc[k] * step[po + k];
-      e1 += (double)jc[9 + k] * step[po + k];
+      e0 += (double)jc[k * rs] * step[po + k];
+      e1 += (double)jc[(9 + k) * rs] * step[po + k];
     }
     if (v.self_cal) {
       int gi = v.cam_group[cam];
       int id = v.intr_dim[gi], io = v.intr_off[gi];
       for (int k = 0; k < id; ++k) {
-        e0 += (double)jc[pd + k] * step[io + k];
-        e1 += (double)jc[9 + pd + k] * step[io + k];
+        e0 += (double)jc[(pd + k) * rs] * step[io + k];
+        e1 += (double)jc[(9 + pd + k) * rs] * step[io + k];
       }
     }
-    const T* jp = lin.jp + (size_t)6 * o;
-    b0 += (double)jp[0] * e0 + (double)jp[3] * e1;
-    b1 += (double)jp[1] * e0 + (double)jp[4] * e1;
-    b2 += (double)jp[2] * e0 + (double)jp[5] * e1;
+    const T* jp = jc + kJp * rs;
+    b0 += (double)jp[0] * e0 + (double)jp[3 * rs] * e1;
+    b1 += (double)jp[rs] * e0 + (double)jp[4 * rs] * e1;
+    b2 += (double)jp[2 * rs] * e0 + (double)jp[5 * rs] * e1;
   }
   const double* vi = lin.vinv + 6 * (size_t)p;
   const double* ig = lin.ig + 3 * (size_t)p;
@@ -1244,23 +1317,6 @@ __global__ void k_noninvertible(DevView v, int N, const double* groups, RedVec<1
 // ----------------------------------------------------------------------------------------------
 static inline int grid_for(size_t n, int threads) { return (int)std::max<size_t>(1, (n + threads - 1) / threads); }
 
-struct Setup {
-  // block tables (host copies)
-  std::vector<int> blk_off, blk_dim, blk_col, blk_edge;
-  std::vector<uint32_t> ent, ent_point;
-  std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
-  std::vector<uint32_t> chunk_begin, chunk_end;
-  std::vector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment
-  std::vector<int> seg_col;       // per entity id (obs*2+seg): column
-  // pair tables
-  std::vector<int> grp_row, grp_col;
-  std::vector<uint32_t> grp_begin, grp_end, pair_a, pair_b, pair_p;
-  // cross same-block pairs (preconditioner)
-  std::vector<int> xgrp_row, xgrp_col;
-  std::vector<uint32_t> xgrp_begin, xgrp_end, xpair_a, xpair_b, xpair_p;
-  std::vector<int> blk_cross_begin, blk_cross_end;
-};
-
 struct Layout {
   int D = 0;
   std::vector<int> pose_off, pose_dim, intr_off, intr_dim;
@@ -1288,6 +1344,139 @@ static Layout make_layout(const NativeProblem& n) {
   }
   L.D = off;
   return L;
+}
+
+struct Setup {
+  // block tables (host copies)
+  std::vector<int> blk_off, blk_dim, blk_col, blk_edge;
+  std::vector<uint32_t> ent, ent_point;
+  std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
+  std::vector<uint32_t> chunk_begin, chunk_end;
+  std::vector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment
+  std::vector<int> seg_col;       // per entity id (obs*2+seg): column
+  // pair tables
+  std::vector<int> grp_row, grp_col;
+  std::vector<uint32_t> grp_begin, grp_end, pair_a, pair_b, pair_p;
+  // cross same-block pairs (preconditioner)
+  std::vector<int> xgrp_row, xgrp_col;
+  std::vector<uint32_t> xgrp_begin, xgrp_end, xpair_a, xpair_b, xpair_p;
+  std::vector<int> blk_cross_begin, blk_cross_end;
+  std::vector<int> ent_block;  // entity (observation * 2 + segment) -> parameter block, -1 when absent
+};
+
+// Tiles of the fused matvec for one record precision (host tables).
+struct TileSet {
+  int tile = 0;
+  std::vector<uint32_t> tile_obs, tile_pt, blk_seg_off, blk_segs;
+  std::vector<uint32_t> obs_rec;  // element index of each observation's record component 0
+  std::vector<uint64_t> tile_blob;
+  std::vector<unsigned char> blob;
+  uint32_t nseg = 0;
+};
+
+// Tiles of whole points with at most `tile` observations (and points). For each tile a metadata
+// blob (layout in mv_tiles.cuh) holds per-observation parameter offsets, local point indices,
+// point ranges and the tile's entities (observation, segment) sorted by parameter block, whose
+// runs are the segments of the fused matvec.
+static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
+  const std::vector<int>& ent_block = setup.ent_block;
+  const int nblocks = (int)setup.blk_off.size();
+  S.tile = tile;
+  size_t P = n.points.size() / 3;
+  S.tile_obs.clear();
+  S.tile_pt.clear();
+  S.tile_blob.clear();
+  S.blob.clear();
+  S.obs_rec.assign(n.obs_cam.size(), 0);
+  std::vector<std::vector<uint32_t>> blk_segs(nblocks);
+  uint32_t nseg_total = 0;
+  size_t p = 0;
+  std::vector<std::pair<int, uint16_t>> ents;
+  std::vector<uint32_t> w0, w1, sg;
+  std::vector<uint16_t> lpt, poff, segb, ent;
+  while (p < P) {
+    size_t p0 = p;
+    uint64_t o0 = n.pt_off[p];
+    while (p < P && p - p0 < (size_t)tile && (n.pt_off[p + 1] - o0 <= (uint64_t)tile || p == p0)) ++p;
+    uint64_t o1 = n.pt_off[p];
+    if (o1 - o0 > (uint64_t)tile) throw SolveFailure{2, "a point track is longer than the matvec tile"};
+    uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
+    w0.assign(nobs, 0);
+    w1.assign(nobs, 0);
+    lpt.assign(nobs, 0);
+    poff.assign(npt + 1, 0);
+    for (size_t q = p0; q < p; ++q) {
+      poff[q - p0] = (uint16_t)(n.pt_off[q] - o0);
+      for (uint64_t o = n.pt_off[q]; o < n.pt_off[q + 1]; ++o) lpt[o - o0] = (uint16_t)(q - p0);
+    }
+    poff[npt] = (uint16_t)nobs;
+    ents.clear();
+    for (uint64_t o = o0; o < o1; ++o) {
+      int c = n.obs_cam[o];
+      w0[o - o0] = (uint32_t)L.pose_off[c] | ((uint32_t)L.pose_dim[c] << 28);
+      if (n.self_cal) {
+        int g = n.cam_group[c];
+        w1[o - o0] = (uint32_t)L.intr_off[g] | ((uint32_t)L.intr_dim[g] << 28);
+      }
+      for (int sgm = 0; sgm < 2; ++sgm) {
+        int b = ent_block[2 * o + sgm];
+        if (b < 0) continue;
+        int col = sgm == 0 ? 0 : L.pose_dim[c];
+        int code = col == 0 ? 0 : (col == 5 ? 1 : 2);
+        ents.push_back({b, (uint16_t)((o - o0) | (code << 12))});
+      }
+    }
+    std::stable_sort(ents.begin(), ents.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    sg.clear();
+    segb.clear();
+    ent.clear();
+    size_t i = 0;
+    while (i < ents.size()) {
+      size_t j = i;
+      while (j < ents.size() && ents[j].first == ents[i].first) ++j;
+      int b = ents[i].first;
+      blk_segs[b].push_back(nseg_total + (uint32_t)sg.size());
+      sg.push_back((uint32_t)setup.blk_off[b] | ((uint32_t)setup.blk_dim[b] << 28));
+      segb.push_back((uint16_t)ent.size());
+      for (size_t k = i; k < j; ++k) ent.push_back(ents[k].second);
+      i = j;
+    }
+    uint32_t nseg = (uint32_t)sg.size();
+    segb.push_back((uint16_t)ent.size());
+    size_t off[7];
+    size_t bytes = blob_layout(nobs, npt, nseg, (uint32_t)ent.size(), off);
+    size_t base = S.blob.size();
+    S.blob.resize(base + bytes, 0);
+    unsigned char* B = S.blob.data() + base;
+    uint32_t hdr[4] = {nobs, npt, nseg, nseg_total};
+    std::memcpy(B, hdr, 16);
+    std::memcpy(B + off[0], w0.data(), 4 * (size_t)nobs);
+    std::memcpy(B + off[1], w1.data(), 4 * (size_t)nobs);
+    std::memcpy(B + off[2], lpt.data(), 2 * (size_t)nobs);
+    std::memcpy(B + off[3], poff.data(), 2 * (size_t)(npt + 1));
+    std::memcpy(B + off[4], sg.data(), 4 * (size_t)nseg);
+    std::memcpy(B + off[5], segb.data(), 2 * (size_t)(nseg + 1));
+    std::memcpy(B + off[6], ent.data(), 2 * ent.size());
+    if (bytes > mv_blob_max(tile)) throw SolveFailure{5, "matvec tile metadata exceeds its bound"};
+    size_t t = S.tile_obs.size();
+    if ((t + 1) * (size_t)tile * kRec >= (1ull << 32)) throw SolveFailure{3, "record storage exceeds 2^32 elements"};
+    for (uint64_t o = o0; o < o1; ++o) S.obs_rec[o] = (uint32_t)(t * (size_t)tile * kRec + (o - o0));
+    S.tile_obs.push_back((uint32_t)o0);
+    S.tile_pt.push_back((uint32_t)p0);
+    S.tile_blob.push_back(base);
+    nseg_total += nseg;
+  }
+  S.tile_obs.push_back((uint32_t)n.pt_off[P]);
+  S.tile_pt.push_back((uint32_t)P);
+  S.tile_blob.push_back(S.blob.size());
+  S.nseg = nseg_total;
+  S.blk_seg_off.assign(nblocks + 1, 0);
+  S.blk_segs.clear();
+  for (int b = 0; b < nblocks; ++b) {
+    S.blk_seg_off[b] = (uint32_t)S.blk_segs.size();
+    S.blk_segs.insert(S.blk_segs.end(), blk_segs[b].begin(), blk_segs[b].end());
+  }
+  S.blk_seg_off[nblocks] = (uint32_t)S.blk_segs.size();
 }
 
 static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_pairs, Setup& S) {
@@ -1445,7 +1634,49 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
   }
   for (int b = 0; b < nb; ++b)
     if (S.blk_cross_end[b] == 0) S.blk_cross_begin[b] = 0;
+  S.ent_block = std::move(ent_block);
 }
+
+// Device copy of a TileSet plus the fused-matvec launch shape.
+struct TileSetDev {
+  DBuf<uint32_t> tile_obs, tile_pt, blk_seg_off, blk_segs, obs_rec;
+  DBuf<uint64_t> tile_blob;
+  DBuf<unsigned char> blob;
+  DBuf<double> partial;
+  int ntiles = 0, grid = 1;
+  void upload(const TileSet& t, cudaStream_t st) {
+    auto up = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) {
+      std::vector<uint32_t> x = v;
+      if (x.empty()) x.push_back(0);
+      b.upload(x.data(), x.size(), st);
+    };
+    up(tile_obs, t.tile_obs);
+    up(tile_pt, t.tile_pt);
+    up(blk_seg_off, t.blk_seg_off);
+    up(blk_segs, t.blk_segs);
+    up(obs_rec, t.obs_rec);
+    tile_blob.upload(t.tile_blob.data(), t.tile_blob.size(), st);
+    std::vector<unsigned char> b = t.blob;
+    b.resize(std::max<size_t>(b.size(), 16));
+    blob.upload(b.data(), b.size(), st);
+    partial.alloc((size_t)6 * std::max<size_t>(1, t.nseg), st);
+    ntiles = (int)t.tile_obs.size() - 1;
+  }
+  MvTiles view(const int* blk_dim, const int* blk_off, int nblocks) const {
+    MvTiles m;
+    m.ntiles = ntiles;
+    m.tile_obs = tile_obs.p;
+    m.tile_pt = tile_pt.p;
+    m.tile_blob = tile_blob.p;
+    m.blob = blob.p;
+    m.blk_dim = blk_dim;
+    m.blk_off = blk_off;
+    m.blk_seg_off = blk_seg_off.p;
+    m.blk_segs = blk_segs.p;
+    m.nblocks = nblocks;
+    return m;
+  }
+};
 
 template <typename T>
 struct Solver {
@@ -1465,7 +1696,11 @@ struct Solver {
   DBuf<uint8_t> d_fixed_points;
   DBuf<double> d_pose[2], d_points[2], d_groups[2];
   int cur = 0;
-  DBuf<T> d_jc, d_jp, d_f;
+  DBuf<T> d_rec;
+  DBuf<float> d_rec32;
+  TileSet T64, T32;
+  TileSetDev dT64, dT32;
+  bool mixed = false;
   DBuf<double> d_rw, d_vinv, d_ig, d_gp, d_ddiag;
   DBuf<PointSummary> d_summary, d_summary_part;
   DBuf<int> d_blk_off, d_blk_dim, d_blk_col, d_blk_edge, d_chunk_block, d_chunk_col, d_blk_chunk_begin, d_blk_chunk_end;
@@ -1482,9 +1717,12 @@ struct Solver {
   DBuf<double> d_S, d_Lf;
   DBuf<int> d_status;
   // PCG vectors
-  DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_chunk_y, d_factor, d_tmp;
+  DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e;
   DBuf<int> d_fail;
-  DBuf<double> d_scalars, d_cam_norm;
+
+  DBuf<int> d_fault;
+
+  DBuf<double> d_scalars, d_cam_norm, d_ctl;
   DBuf<RedVec<4>> d_cand, d_cand_part;
   DBuf<RedVec<3>> d_met, d_met_part;
   DBuf<RedVec<1>> d_one, d_one_part;
@@ -1499,6 +1737,9 @@ struct Solver {
     ng = n.self_cal ? (int)n.group_dim.size() : 0;
     direct = !opt.iterative;
     build_tables(n, L, direct || D <= opt.dense_rank_limit, S);
+    build_tiles(n, L, S, mv_tile_obs<double>(), T64);
+    mixed = opt.precision == 1 && !direct;
+    if (mixed) build_tiles(n, L, S, mv_tile_obs<float>(), T32);
     nb = (int)S.blk_off.size();
     red_blocks = std::min(1024, grid_for(std::max(P, N), kReduceThreads));
     upload();
@@ -1525,7 +1766,8 @@ struct Solver {
   }
   DevState state(int which) const { return {d_pose[which].p, d_points[which].p, d_groups[which].p}; }
   LinOut<T> lin() const {
-    return {d_jc.p, d_jp.p, d_rw.p, d_vinv.p, d_ig.p, d_gp.p, d_ddiag.p, d_summary.p, nullptr};
+    return {d_rec.p,         dT64.obs_rec.p, mv_tile_obs<T>(), mixed ? d_rec32.p : nullptr, dT32.obs_rec.p,
+            mv_tile_obs<float>(), d_rw.p, d_vinv.p, d_ig.p, d_gp.p, d_ddiag.p, d_summary.p, nullptr};
   }
   BlockTables tables() const {
     BlockTables b;
@@ -1600,9 +1842,16 @@ struct Solver {
       if (gr.empty()) gr.assign(3, 0.0);
       d_groups[w].upload(gr.data(), gr.size(), st);
     }
-    d_jc.alloc((size_t)18 * N, st);
-    d_jp.alloc((size_t)6 * N, st);
-    d_f.alloc((size_t)2 * N, st);
+    {
+      dT64.upload(T64, st);
+      d_rec.alloc((size_t)std::max(1, dT64.ntiles) * T64.tile * kRec, st);
+      d_rec.zero();  // padding slots of partial tiles stay zero
+      if (mixed) {
+        dT32.upload(T32, st);
+        d_rec32.alloc((size_t)std::max(1, dT32.ntiles) * T32.tile * kRec, st);
+        d_rec32.zero();
+      }
+    }
     d_rw.alloc((size_t)2 * N, st);
     d_vinv.alloc((size_t)6 * P, st);
     d_ig.alloc((size_t)3 * P, st);
@@ -1667,11 +1916,23 @@ struct Solver {
       d_Lf.alloc((size_t)std::max(1, D) * std::max(1, D), st);
     }
     d_status.alloc(4, st);
-    for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp}) b->alloc(std::max(1, D), st);
-    d_chunk_y.alloc((size_t)6 * std::max<size_t>(1, S.chunk_block.size()), st);
+    for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp, &d_rhs, &d_r64, &d_e}) b->alloc(std::max(1, D), st);
     d_factor.alloc((size_t)42 * std::max(1, nb), st);
     d_fail.alloc(std::max(1, nb), st);
+    d_fault.alloc(1, st);
+    d_fault.zero();
+    {
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+      dT64.grid = std::max(1, std::min(dT64.ntiles, 2 * sms));
+      dT32.grid = std::max(1, std::min(dT32.ntiles, 2 * sms));
+      CUDA_OK(cudaFuncSetAttribute(k_mv_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)mv_smem_bytes<float>()));
+      CUDA_OK(cudaFuncSetAttribute(k_mv_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)mv_smem_bytes<T>()));
+    }
     d_scalars.alloc(16, st);
+    d_ctl.alloc((sizeof(PcgCtl) + sizeof(double) - 1) / sizeof(double), st);
     d_cam_norm.alloc(std::max(1, n.ncam), st);
     d_cand.alloc(P, st);
     d_cand_part.alloc(red_blocks, st);
@@ -1850,16 +2111,26 @@ struct Solver {
     sync();
   }
 
-  // y = S_lambda x (implicit, matrix-free)
-  void matvec(const double* x, double* y, double lambda) {
-    if (direct || !d_S.p || false) {
+  // y = S_lambda x (implicit, matrix-free); ctl: optional PCG control for graph-launched iterations
+  // fp32: use the FP32 record copy (mixed precision inner solves)
+  void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false) {
+    const TileSetDev& ts = fp32 ? dT32 : dT64;
+    MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
+    if (mt.ntiles > 0) {
+      if (fp32)
+        k_mv_tiles<float><<<ts.grid, 256, mv_smem_bytes<float>(), st>>>(mt, d_rec32.p, d_vinv.p, x, ts.partial.p,
+                                                                        ctl, d_fault.p);
+      else
+        k_mv_tiles<T><<<ts.grid, 256, mv_smem_bytes<T>(), st>>>(mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl, d_fault.p);
     }
-    DevView v = view();
-    k_mv_points<T><<<grid_for(P, 128), 128, 0, st>>>(v, lin(), x, d_f.p);
-    BlockTables bt = tables();
-    if (bt.nchunks > 0) k_mv_chunks<T><<<bt.nchunks, 32, 0, st>>>(bt, lin(), d_f.p, d_chunk_y.p);
-    k_mv_finalize<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_chunk_y.p, d_diag.p, lambda, x, y);
+    k_mv_tiles_finalize<<<grid_for((size_t)nb * 32, 256), 256, 0, st>>>(mt, ts.partial.p, d_diag.p, lambda, x, y, ctl);
     check_launch();
+  }
+  void check_fault() {
+    int f = 0;
+    CUDA_OK(cudaMemcpyAsync(&f, d_fault.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (f) throw SolveFailure{8, "a bulk shared-memory copy did not complete within its wait limit"};
   }
 
   bool factor_preconditioner(double lambda) {
@@ -1876,21 +2147,42 @@ struct Solver {
       if (fail[b]) return false;
     return true;
   }
-  void precond(const double* r, double* z) {
-    k_block_precond<<<grid_for(nb, 64), 64, 0, st>>>(tables(), d_factor.p, r, z);
+  void precond(const double* r, double* z, const PcgCtl* ctl = nullptr) {
+    k_block_precond<<<grid_for(nb, 64), 64, 0, st>>>(tables(), d_factor.p, r, z, ctl);
     check_launch();
   }
 
   struct PcgResult {
     bool accepted = false;
+    bool exhausted = false;
     uint64_t terms = 0;
     double rel = NAN;
   };
-  // pcg::solve (sparse/pcg.rs:23-119), require_bounded_residual
-  PcgResult pcg(double lambda, uint64_t max_it, double tol) {
+  // pcg::solve (sparse/pcg.rs:23-119), require_bounded_residual, for S x = b with x0 = 0. The
+  // iteration body runs as a CUDA graph; the host polls the device status every kPoll iterations.
+  // confirm: when the recursive residual meets the tolerance, confirm it with the true residual
+  // b - S x (the reference's rule); without it the recursive residual decides (inner solves of the
+  // mixed-precision refinement, whose outer loop checks the FP64 residual). fp32: FP32 products.
+  static constexpr int kPoll = 8;
+  PcgResult pcg_run(const double* b, double* x, double lambda, uint64_t max_it, double tol, bool fp32, bool confirm) {
+    double t_start = now();
+    int launches = 0, restarts = 0;
     PcgResult res;
-    CUDA_OK(cudaMemsetAsync(d_step.p, 0, sizeof(double) * D, st));
-    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_r.p);
+    struct Report {
+      double t0;
+      int* launches;
+      int* restarts;
+      PcgResult* res;
+      bool fp32;
+      ~Report() {
+        if (std::getenv("OMVGBA_PCG_TRACE"))
+          std::fprintf(stderr, "[pcg%s] %.3f ms terms %llu accepted %d rel %.3e launches %d restarts %d\n",
+                       fp32 ? "32" : "64", (now() - t0) * 1e3, (unsigned long long)res->terms, (int)res->accepted,
+                       res->rel, *launches, *restarts);
+      }
+    } rpt{t_start, &launches, &restarts, &res, fp32};
+    CUDA_OK(cudaMemsetAsync(x, 0, sizeof(double) * D, st));
+    CUDA_OK(cudaMemcpyAsync(d_r.p, b, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
     double h[4];
     dots({{d_r.p, d_r.p}}, h);
     double n0 = std::sqrt(h[0]);
@@ -1905,75 +2197,154 @@ struct Solver {
     dots({{d_r.p, d_z.p}}, h);
     double rho = h[0];
     if (!(std::isfinite(rho) && rho > 0.0)) return res;
+    if (max_it == 0) return res;
+    PcgCtl ctl{};
+    ctl.n0 = n0;
+    ctl.rho = rho;
+    ctl.tol = tol;
+    ctl.status = kRunning;
+    ctl.terms = 0;
+    ctl.max_it = (int)std::min<uint64_t>(max_it, (uint64_t)INT32_MAX);
+    PcgCtl* dctl = reinterpret_cast<PcgCtl*>(d_ctl.p);
+    CUDA_OK(cudaMemcpyAsync(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    matvec(d_dir.p, d_q.p, lambda, dctl, fp32);
+    k_pcg_alpha<<<1, 1024, 0, st>>>(D, d_dir.p, d_q.p, dctl);
+    k_pcg_update<<<grid_for(D, 256), 256, 0, st>>>(D, d_dir.p, d_q.p, x, d_r.p, dctl);
+    precond(d_r.p, d_z.p, dctl);
+    k_pcg_beta<<<1, 1024, 0, st>>>(D, d_r.p, d_z.p, dctl);
+    k_pcg_direction<<<grid_for(D, 256), 256, 0, st>>>(D, d_z.p, d_dir.p, dctl);
+    CUDA_OK(cudaStreamEndCapture(st, &graph));
+    CUDA_OK(cudaGraphInstantiate(&exec, graph, 0));
+    struct GraphGuard {
+      cudaGraph_t g;
+      cudaGraphExec_t e;
+      ~GraphGuard() {
+        cudaGraphExecDestroy(e);
+        cudaGraphDestroy(g);
+      }
+    } guard{graph, exec};
     auto recompute = [&]() {
-      matvec(d_step.p, d_q.p, lambda);
-      k_residual_update<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_q.p, d_r.p);
+      matvec(x, d_q.p, lambda, nullptr, fp32);
+      k_sub<<<grid_for(D, 256), 256, 0, st>>>(D, b, d_q.p, d_r.p);
       check_launch();
     };
-    for (uint64_t it = 1; it <= max_it; ++it) {
-      matvec(d_dir.p, d_q.p, lambda);
-      dots({{d_dir.p, d_q.p}}, h);
-      double curv = h[0];
-      if (!(std::isfinite(curv) && curv > 0.0)) {
-        res.terms = it - 1;
+    for (;;) {
+      for (int k = 0; k < kPoll; ++k) CUDA_OK(cudaGraphLaunch(exec, st));
+      launches += kPoll;
+      CUDA_OK(cudaMemcpyAsync(&ctl, dctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+      sync();
+      check_fault();
+      if (ctl.status == kRunning) continue;
+      if (ctl.status == kRejected) {
+        res.terms = ctl.terms;
         return res;
       }
-      double alpha = rho / curv;
-      if (!std::isfinite(alpha)) {
-        res.terms = it - 1;
+      if (ctl.status == kExhausted) break;
+      if (!confirm) {  // kCheckResidual without confirmation: the recursive residual decides
+        res.accepted = true;
+        res.terms = ctl.terms;
+        res.rel = ctl.ratio;
         return res;
       }
-      k_axpy2<<<grid_for(D, 256), 256, 0, st>>>(D, alpha, d_dir.p, d_q.p, d_step.p, d_r.p);
+      // kCheckResidual: the recursive residual met the tolerance; confirm with the true residual
+      ++restarts;
+      recompute();
+      dots({{d_r.p, d_r.p}}, h);
+      double tr = std::sqrt(h[0]) / n0;
+      if (std::isfinite(tr) && tr <= tol) {
+        res.accepted = true;
+        res.terms = ctl.terms;
+        res.rel = tr;
+        return res;
+      }
+      if (!std::isfinite(tr)) {
+        res.terms = ctl.terms;
+        return res;
+      }
       precond(d_r.p, d_z.p);
-      dots({{d_r.p, d_r.p}, {d_r.p, d_z.p}}, h);
-      double ratio = std::sqrt(h[0]) / n0;
-      if (!std::isfinite(ratio)) {
-        res.terms = it;
-        return res;
-      }
-      if (ratio <= tol) {
-        recompute();
-        dots({{d_r.p, d_r.p}}, h);
-        double tr = std::sqrt(h[0]) / n0;
-        if (std::isfinite(tr) && tr <= tol) {
-          res.accepted = true;
-          res.terms = it;
-          res.rel = tr;
-          return res;
-        }
-        if (!std::isfinite(tr)) {
-          res.terms = it;
-          return res;
-        }
-        precond(d_r.p, d_z.p);
-        CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
-        dots({{d_r.p, d_z.p}}, h);
-        rho = h[0];
-        if (!(std::isfinite(rho) && rho > 0.0)) {
-          res.terms = it;
-          res.rel = tr;
-          return res;
-        }
-        continue;
-      }
-      double nrho = h[1];
+      CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+      dots({{d_r.p, d_z.p}}, h);
+      double nrho = h[0];
       if (!(std::isfinite(nrho) && nrho > 0.0)) {
-        res.terms = it;
+        res.terms = ctl.terms;
+        res.rel = tr;
         return res;
       }
-      double beta = nrho / rho;
-      if (!std::isfinite(beta)) {
-        res.terms = it;
-        return res;
-      }
-      k_xpby<<<grid_for(D, 256), 256, 0, st>>>(D, d_z.p, beta, d_dir.p);
-      check_launch();
-      rho = nrho;
+      if ((uint64_t)ctl.terms >= max_it) break;
+      ctl.rho = nrho;
+      ctl.status = kRunning;
+      CUDA_OK(cudaMemcpyAsync(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
     }
     recompute();
     dots({{d_r.p, d_r.p}}, h);
     res.terms = max_it;
     res.rel = std::sqrt(h[0]) / n0;
+    res.exhausted = true;
+    return res;
+  }
+
+  PcgResult pcg(double lambda, uint64_t max_it, double tol) {
+    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_rhs.p);
+    check_launch();
+    return pcg_run(d_rhs.p, d_step.p, lambda, max_it, tol, false, true);
+  }
+
+  // Mixed precision: FP32-product PCG inner solves refined against the FP64 residual
+  // r = -g - S x; the step is accepted when the FP64 relative residual meets the tolerance, the
+  // same acceptance rule as the FP64 solve, within the same iteration budget.
+  PcgResult pcg_mixed(double lambda, uint64_t max_it, double tol) {
+    PcgResult res;
+    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_rhs.p);
+    check_launch();
+    double h[4];
+    dots({{d_rhs.p, d_rhs.p}}, h);
+    double n0 = std::sqrt(h[0]);
+    if (!std::isfinite(n0)) return res;
+    CUDA_OK(cudaMemsetAsync(d_step.p, 0, sizeof(double) * D, st));
+    if (n0 == 0.0) {
+      res.accepted = true;
+      res.rel = 0.0;
+      return res;
+    }
+    CUDA_OK(cudaMemcpyAsync(d_r64.p, d_rhs.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    double rel = 1.0;
+    uint64_t terms = 0;
+    for (int outer = 0; outer < 32 && terms < max_it; ++outer) {
+      double eta = std::min(0.5, std::max(0.5 * tol / rel, 1e-4));
+      PcgResult in = pcg_run(d_r64.p, d_e.p, lambda, max_it - terms, eta, true, false);
+      terms += in.terms;
+      if (!in.accepted && !in.exhausted) {
+        res.terms = terms;
+        return res;  // curvature or finiteness failure
+      }
+      k_axpy<<<grid_for(D, 256), 256, 0, st>>>(D, 1.0, d_e.p, d_step.p);
+      matvec(d_step.p, d_q.p, lambda, nullptr, false);
+      k_sub<<<grid_for(D, 256), 256, 0, st>>>(D, d_rhs.p, d_q.p, d_r64.p);
+      check_launch();
+      dots({{d_r64.p, d_r64.p}}, h);
+      double nrel = std::sqrt(h[0]) / n0;
+      if (!std::isfinite(nrel)) {
+        res.terms = terms;
+        return res;
+      }
+      if (nrel <= tol) {
+        res.accepted = true;
+        res.terms = terms;
+        res.rel = nrel;
+        return res;
+      }
+      if (nrel > 0.9 * rel) {  // the FP32 correction no longer reduces the FP64 residual
+        res.terms = terms;
+        res.rel = nrel;
+        return res;
+      }
+      rel = nrel;
+    }
+    res.terms = terms;
+    res.rel = rel;
     return res;
   }
 
@@ -2024,9 +2395,15 @@ struct Solver {
     *rmse = std::sqrt(r.v[1] / double(2 * (size_t)N));
   }
 
+  double t_assemble = 0, t_solve = 0, t_candidate = 0;
+  static double now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  }
+
   NativeReport refine(std::vector<double>& rotation, std::vector<double>& translation, std::vector<double>& points,
                       std::vector<double>& groups) {
     NativeReport rep;
+    double t_begin = now();
     double scene = scene_scale_host();
     // stages (continuation.rs:18-74)
     struct Stage {
@@ -2080,8 +2457,11 @@ struct Solver {
       bool confirm = false;
       for (uint64_t it = 0; it < stages[si].iters; ++it) {
         iterations++;
+        double t0 = now();
         Gauge g = gauge_for(cur, scene);
         Assembly a = assemble(cur, g, stages[si].loss, lambda, direct);
+        double t1 = now();
+        t_assemble += t1 - t0;
         if (!have_initial && std::isfinite(a.cost) && std::isfinite(a.sq) && N > 0) {
           init_cost = a.cost;
           init_rmse = std::sqrt(a.sq / double(2 * (size_t)N));
@@ -2101,29 +2481,27 @@ struct Solver {
         }
         bool iterative_step = false;
         double rel_res = 0.0;
+        bool solved = true;
         if (direct) {
-          if (D > 0 && !direct_step()) {
-            rej[1]++;
-            increase();
-            continue;
-          }
+          solved = D == 0 || direct_step();
         } else {
-          if (!factor_preconditioner(lambda)) {
-            rej[1]++;
-            increase();
-            continue;
+          solved = factor_preconditioner(lambda);
+          if (solved) {
+            double tol = confirm ? std::min(opt.pcg_tolerance, iter_tol) : opt.pcg_tolerance;
+            uint64_t limit = confirm ? opt.pcg_max_iterations : std::min<uint64_t>(opt.pcg_max_iterations, (uint64_t)D);
+            PcgResult r = mixed ? pcg_mixed(lambda, limit, tol) : pcg(lambda, limit, tol);
+            pcg_terms += r.terms;
+            solved = r.accepted;
+            iterative_step = true;
+            rel_res = r.rel;
           }
-          double tol = confirm ? std::min(opt.pcg_tolerance, iter_tol) : opt.pcg_tolerance;
-          uint64_t limit = confirm ? opt.pcg_max_iterations : std::min<uint64_t>(opt.pcg_max_iterations, (uint64_t)D);
-          PcgResult r = pcg(lambda, limit, tol);
-          pcg_terms += r.terms;
-          if (!r.accepted) {
-            rej[1]++;
-            increase();
-            continue;
-          }
-          iterative_step = true;
-          rel_res = r.rel;
+        }
+        double t2 = now();
+        t_solve += t2 - t1;
+        if (!solved) {
+          rej[1]++;
+          increase();
+          continue;
         }
         // step cap (calibrated only)
         if (!n.self_cal && D > 0) {
@@ -2151,6 +2529,7 @@ struct Solver {
         if (cr.v[3] > 0.0) {
           rej[2]++;
           increase();
+          t_candidate += now() - t2;
           continue;
         }
         double point_rms =
@@ -2188,6 +2567,7 @@ struct Solver {
           h[2] = ss;
         }
         double predicted = damped + 0.5 * lambda * (cd[0] + cr.v[2]);
+        t_candidate += now() - t2;
         double reduction = current - cr.v[0];
         // NielsenController::accept
         double gain = (std::isfinite(reduction) && std::isfinite(predicted) && predicted > 0.0) ? reduction / predicted
@@ -2222,6 +2602,7 @@ struct Solver {
         }
       }
     }
+    check_fault();
     // final undamped assembly and certificate
     Gauge g = gauge_for(cur, scene);
     bool dense_rank = D <= opt.dense_rank_limit && !S.grp_row.empty();
@@ -2236,6 +2617,9 @@ struct Solver {
         rep.rank = rank_full() ? 0 : 2;
     }
     bool well = rep.rank != 2 && fa.weak == 0;
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr, "[omvgba] final: valid=%d rank=%d weak=%llu D=%d min_rcond=%.3e cost=%.12e\n", (int)fa.valid,
+                   rep.rank, (unsigned long long)fa.weak, D, fa.min_rcond, fa.cost);
     if (!well)
       rep.status = 3;
     else if (convergence >= 0)
@@ -2267,6 +2651,13 @@ struct Solver {
     }
     rep.pcg_terms = pcg_terms;
     rep.final_damping = lambda;
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr,
+                   "[omvgba] assemble %.3fs solve %.3fs candidate %.3fs total %.3fs pcg_terms %llu rejections "
+                   "lin %llu solve %llu cand %llu gain %llu\n",
+                   t_assemble, t_solve, t_candidate, now() - t_begin, (unsigned long long)pcg_terms,
+                   (unsigned long long)rej[0], (unsigned long long)rej[1], (unsigned long long)rej[2],
+                   (unsigned long long)rej[3]);
     rep.D = D;
     // download state
     std::vector<double> pose(12 * (size_t)n.ncam);
@@ -2286,8 +2677,10 @@ struct Solver {
     return rep;
   }
 
-  // Rank certificate on the final undamped dense S: Jacobi-equilibrated Cholesky with a pivot floor
-  // of 64 eps D (the equilibrated spectrum is bounded by D).
+  // Rank certificate on the final undamped dense S (sparse/direct.rs:342-455): after Jacobi
+  // equilibration the spectral test counts eigenvalues above tol = 64 eps D lambda_max. Full rank
+  // holds exactly when every eigenvalue exceeds tol, i.e. when S_eq - tol I is positive definite,
+  // which one Cholesky factorization decides; lambda_max comes from power iteration.
   bool rank_full() {
     std::vector<double> Sh((size_t)D * D);
     CUDA_OK(cudaMemcpyAsync(Sh.data(), d_S.p, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost, st));
@@ -2297,24 +2690,51 @@ struct Solver {
     if (!(std::isfinite(ds) && ds > 0.0)) return false;
     double fl = 64.0 * kEps * ds;
     std::vector<double> sc(D);
-    for (int i = 0; i < D; ++i) sc[i] = 1.0 / std::sqrt(std::max(Sh[(size_t)i * D + i], fl));
+    for (int i = 0; i < D; ++i) {
+      double d = Sh[(size_t)i * D + i];
+      if (!std::isfinite(d)) return false;
+      sc[i] = 1.0 / std::sqrt(std::max(d, fl));
+    }
     for (int i = 0; i < D; ++i)
-      for (int j = 0; j < D; ++j) Sh[(size_t)i * D + j] *= sc[i] * sc[j];
+      for (int j = 0; j < D; ++j) {
+        double v = Sh[(size_t)i * D + j] * sc[i] * sc[j];
+        if (!std::isfinite(v)) return false;
+        Sh[(size_t)i * D + j] = v;
+      }
+    CUDA_OK(cudaMemcpyAsync(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
+    // power iteration for the largest |eigenvalue| (Rayleigh quotient of the converged iterate)
+    std::vector<double> v(D, 1.0 / std::sqrt((double)D)), w(D);
+    double lam = 0.0;
+    for (int it = 0; it < 200; ++it) {
+      CUDA_OK(cudaMemcpyAsync(d_tmp.p, v.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
+      k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, st>>>(D, d_Lf.p, d_tmp.p, d_q.p);
+      check_launch();
+      CUDA_OK(cudaMemcpyAsync(w.data(), d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+      sync();
+      double nrm = 0.0, rq = 0.0;
+      for (int i = 0; i < D; ++i) {
+        nrm += w[i] * w[i];
+        rq += v[i] * w[i];
+      }
+      nrm = std::sqrt(nrm);
+      if (!(std::isfinite(nrm) && nrm > 0.0)) return false;
+      bool settled = it > 8 && std::fabs(rq - lam) <= 1e-10 * std::fabs(rq);
+      lam = rq;
+      for (int i = 0; i < D; ++i) v[i] = w[i] / nrm;
+      if (settled) break;
+    }
+    double largest = std::fabs(lam);
+    if (!(std::isfinite(largest) && largest > 0.0)) return false;
+    double tol = 64.0 * kEps * D * largest;
+    if (std::getenv("OMVGBA_PHASE_TIMES")) std::fprintf(stderr, "[omvgba] rank: lambda_max %.6e tol %.3e\n", largest, tol);
+    for (int i = 0; i < D; ++i) Sh[(size_t)i * D + i] -= tol;
     CUDA_OK(cudaMemcpyAsync(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
     k_dense_cholesky<<<1, 1024, 0, st>>>(D, d_Lf.p, d_status.p);
     check_launch();
     int ok = 0;
     CUDA_OK(cudaMemcpyAsync(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    std::vector<double> Lh((size_t)D * D);
-    CUDA_OK(cudaMemcpyAsync(Lh.data(), d_Lf.p, sizeof(double) * Lh.size(), cudaMemcpyDeviceToHost, st));
     sync();
-    if (!ok) return false;
-    double tol = 64.0 * kEps * D * D;
-    for (int i = 0; i < D; ++i) {
-      double pv = Lh[(size_t)i * D + i];
-      if (!(pv * pv > tol)) return false;
-    }
-    return true;
+    return ok != 0;
   }
 };
 
@@ -2323,10 +2743,6 @@ NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOpti
                         std::vector<double>& groups) {
   CUDA_OK(cudaSetDevice(ctx->device));
   if (problem.obs_cam.size() >= (1ull << 31)) throw SolveFailure{3, "observation count exceeds 2^31"};
-  if (options.precision == 1) {
-    Solver<float> s(ctx, problem, options);
-    return s.refine(rotation, translation, points, groups);
-  }
   Solver<double> s(ctx, problem, options);
   return s.refine(rotation, translation, points, groups);
 }
@@ -2344,9 +2760,8 @@ void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOpt
   lo.sw = d_sw.p;
   k_linearize<double><<<grid_for(s.P, 128), 128, 0, s.st>>>(s.view(), s.state(s.cur), g, options.loss, 0.0, lo);
   s.check_launch();
-  std::vector<double> jc(18 * N), jp(6 * N), rw(2 * N), sw(N);
-  CUDA_OK(cudaMemcpyAsync(jc.data(), s.d_jc.p, sizeof(double) * jc.size(), cudaMemcpyDeviceToHost, s.st));
-  CUDA_OK(cudaMemcpyAsync(jp.data(), s.d_jp.p, sizeof(double) * jp.size(), cudaMemcpyDeviceToHost, s.st));
+  std::vector<double> rec(s.d_rec.n), rw(2 * N), sw(N);
+  CUDA_OK(cudaMemcpyAsync(rec.data(), s.d_rec.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.st));
   CUDA_OK(cudaMemcpyAsync(rw.data(), s.d_rw.p, sizeof(double) * rw.size(), cudaMemcpyDeviceToHost, s.st));
   CUDA_OK(cudaMemcpyAsync(sw.data(), d_sw.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s.st));
   s.sync();
@@ -2355,9 +2770,35 @@ void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOpt
     double w = sw[o];
     sqrt_weight[o] = w;
     for (int k = 0; k < 2; ++k) residual[2 * o + k] = rw[2 * o + k] / w;
-    for (int k = 0; k < 6; ++k) point_jacobian[6 * o + k] = jp[6 * o + k] / w;
-    for (int k = 0; k < 18; ++k) camera_jacobian[18 * o + k] = jc[18 * o + k] / w;
+    const size_t base = s.T64.obs_rec[o], rs = (size_t)mv_tile_obs<double>();
+    for (int k = 0; k < 6; ++k) point_jacobian[6 * o + k] = rec[base + (kJp + k) * rs] / w;
+    for (int k = 0; k < 18; ++k) camera_jacobian[18 * o + k] = rec[base + k * rs] / w;
   }
+}
+
+// Debug: y_mv = S_lambda x by the matrix-free tile kernel and y_dense = S_lambda x from the explicit
+// dense Schur complement, both at the first linearization (FP64), for operator parity tests.
+void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const LmOptions& options, double lambda,
+                             const double* x, double* y_mv, double* y_dense, int* dimension) {
+  CUDA_OK(cudaSetDevice(ctx->device));
+  LmOptions o = options;
+  o.iterative = false;
+  Solver<double> s(ctx, problem, o);
+  double scene = s.scene_scale_host();
+  Gauge g = s.gauge_for(s.cur, scene);
+  auto a = s.assemble(s.cur, g, options.loss, lambda, true);
+  if (!a.valid) throw SolveFailure{4, "linearization is not valid"};
+  int D = s.D;
+  *dimension = D;
+  if (!x) return;
+  CUDA_OK(cudaMemcpyAsync(s.d_tmp.p, x, sizeof(double) * D, cudaMemcpyHostToDevice, s.st));
+  s.matvec(s.d_tmp.p, s.d_q.p, lambda);
+  k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, s.st>>>(D, s.d_S.p, s.d_tmp.p, s.d_z.p);
+  s.check_launch();
+  CUDA_OK(cudaMemcpyAsync(y_mv, s.d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(cudaMemcpyAsync(y_dense, s.d_z.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
+  s.sync();
+  s.check_fault();
 }
 
 }  // namespace omvgba

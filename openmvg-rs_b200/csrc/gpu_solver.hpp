@@ -30,6 +30,7 @@ struct NativeProblem {
   std::vector<uint64_t> obs_src;    // input observation index
   std::vector<uint32_t> obs_model;  // calibrated: fixed camera model per observation
   std::vector<uint64_t> pt_off;     // P + 1
+  std::vector<uint64_t> point_source;  // native point -> input point (points are regrouped for locality)
   bool pixel_model = true;          // pinhole pixel projection (no distortion anywhere)
   std::vector<FixedCameraDev> models;
   std::vector<double> groups;       // self-calibration: ng x 3 (focal, k1, k2)
@@ -79,6 +80,10 @@ NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOpti
 // First linearization, per observation (point-major): see omvgba_debug_linearize.
 void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOptions& options, double* residual,
                          double* sqrt_weight, double* point_jacobian, double* camera_jacobian);
+
+// Matrix-free S x versus the explicit dense S x at the first linearization (operator parity).
+void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const LmOptions& options, double lambda,
+                             const double* x, double* y_mv, double* y_dense, int* dimension);
 
 // Residual norms of an input problem's observations with a world-frame state, for the Solution
 // metrics (solver.rs:1052-1131). active: per point flag. Returns false when a projection fails.

@@ -546,10 +546,54 @@ Lowered lower_self_calibrating(const omvgba_problem& pr) {
   return L;
 }
 
+// Regroups points so that consecutive points share cameras: stable order by the smallest native
+// camera index of the track. Points are independent given the cameras, so this changes only the
+// grouping of the camera-side sums; it lets the GPU kernels reduce each tile of points into few
+// camera segments. Observations stay point-major and keep their source order within a track.
+void reorder_points_for_locality(NativeProblem& n) {
+  size_t P = n.points.size() / 3, N = n.obs_cam.size();
+  std::vector<uint32_t> key(P, UINT32_MAX);
+  for (size_t p = 0; p < P; ++p)
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) key[p] = std::min(key[p], n.obs_cam[o]);
+  std::vector<uint64_t> order(P);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return key[a] < key[b]; });
+  std::vector<double> points(3 * P);
+  std::vector<uint8_t> fixed(P);
+  std::vector<uint64_t> off(P + 1, 0);
+  std::vector<uint32_t> cam(N), model(n.obs_model.empty() ? 0 : N);
+  std::vector<double> px(2 * N);
+  std::vector<uint64_t> src(N);
+  uint64_t w = 0;
+  for (size_t q = 0; q < P; ++q) {
+    uint64_t p = order[q];
+    for (int k = 0; k < 3; ++k) points[3 * q + k] = n.points[3 * p + k];
+    fixed[q] = n.fixed_points[p];
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o, ++w) {
+      cam[w] = n.obs_cam[o];
+      if (!model.empty()) model[w] = n.obs_model[o];
+      px[2 * w] = n.obs_px[2 * o];
+      px[2 * w + 1] = n.obs_px[2 * o + 1];
+      src[w] = n.obs_src[o];
+    }
+    off[q + 1] = w;
+  }
+  n.points.swap(points);
+  n.fixed_points.swap(fixed);
+  n.pt_off.swap(off);
+  n.obs_cam.swap(cam);
+  if (!model.empty()) n.obs_model.swap(model);
+  n.obs_px.swap(px);
+  n.obs_src.swap(src);
+  n.point_source = std::move(order);
+}
+
 Lowered lower(const omvgba_problem& pr) {
   if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR)
     fail(OMVGBA_UNSUPPORTED, "angular residuals are not supported by this adjuster");
-  return has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+  Lowered L = has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+  reorder_points_for_locality(L.n);
+  return L;
 }
 
 int reduced_dimension(const NativeProblem& n) {
@@ -685,8 +729,9 @@ Result raise(const omvgba_problem& pr, const Lowered& L, const std::vector<doubl
     if (in.variables & OMVGBA_POSE_TRANSLATION) std::memcpy(res.poses[s].center, C, sizeof(C));
   }
   res.points.resize(3 * pr.point_count);
-  for (size_t i = 0; i < pr.point_count; ++i) {
-    Vec3 X = point_fixed(pr, i) ? point_at(pr, i) : point_from_native(L.rb, &points[3 * i]);
+  for (size_t q = 0; q < pr.point_count; ++q) {
+    size_t i = n.point_source[q];
+    Vec3 X = point_fixed(pr, i) ? point_at(pr, i) : point_from_native(L.rb, &points[3 * q]);
     if (!all_finite(X.data(), 3)) fail(OMVGBA_NUMERICAL, "native BA returned a non-finite point");
     for (int k = 0; k < 3; ++k) res.points[3 * i + k] = X[k];
   }
@@ -1195,6 +1240,27 @@ int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* pr
     LmOptions opt = lm_options(*problem, *config, L.n);
     gpu_debug_linearize(context->ctx, L.n, opt, residual, sqrt_weight, point_jacobian, camera_jacobian);
     for (size_t o = 0; o < L.n.obs_src.size(); ++o) source_index[o] = L.n.obs_src[o];
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
+}
+
+// Debug: the reduced camera system product S_lambda x at the first linearization, by the
+// matrix-free kernel (y_matvec) and by the explicit dense Schur complement (y_dense). Call with
+// x == NULL to query the dimension into *dimension.
+int32_t omvgba_debug_schur_product(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                                   double lambda, const double* x, double* y_matvec, double* y_dense,
+                                   int32_t* dimension, omvgba_error* error) {
+  if (!context || !problem || !config || !dimension) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  try {
+    validate_problem(*problem);
+    validate_config(*config);
+    Lowered L = lower(*problem);
+    LmOptions opt = lm_options(*problem, *config, L.n);
+    int d = 0;
+    gpu_debug_schur_product(context->ctx, L.n, opt, lambda, x, y_matvec, y_dense, &d);
+    *dimension = d;
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {
     return write_error(error, f.code, f.message);

@@ -49,6 +49,29 @@ class CudaBundleAdjuster:
         raise_for(code, err)
         return {"residual": res, "sqrt_weight": sw, "point_jacobian": jp, "camera_jacobian": jc, "source_index": src}
 
+    def debug_schur_product(self, problem: BundleProblem, x: np.ndarray | None, damping: float = 0.0,
+                            config: SolveConfig | None = None):
+        """(y_matvec, y_dense) = S_lambda x by the matrix-free kernel and by the dense Schur complement."""
+        config = config or SolveConfig()
+        mp = abi.MarshalledProblem(problem)
+        cfg = config.to_struct()
+        err = abi.Error()
+        dim = C.c_int32(0)
+        dp = C.POINTER(C.c_double)
+        code = lib().omvgba_debug_schur_product(self._ctx, C.byref(mp.struct), C.byref(cfg), damping, None, None, None,
+                                                C.byref(dim), C.byref(err))
+        raise_for(code, err)
+        if x is None:
+            return dim.value
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert x.shape == (dim.value,)
+        ym, yd = np.zeros(dim.value), np.zeros(dim.value)
+        code = lib().omvgba_debug_schur_product(self._ctx, C.byref(mp.struct), C.byref(cfg), damping,
+                                                x.ctypes.data_as(dp), ym.ctypes.data_as(dp), yd.ctypes.data_as(dp),
+                                                C.byref(dim), C.byref(err))
+        raise_for(code, err)
+        return ym, yd
+
     def close(self) -> None:
         if getattr(self, "_ctx", None):
             lib().omvgba_context_destroy(self._ctx)

@@ -86,8 +86,11 @@ def _perturb(rng, R, C, X, rot=0.01, trans=0.05, pts=0.02):
 
 
 def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_calibrating: bool = False,
-                 loss: RobustLoss | None = None) -> BundleProblem:
+                 loss: RobustLoss | None = None, radius: float = 10.0) -> BundleProblem:
     """20 radial3 cameras on a ring of radius 10 looking at points uniform in [-1, 1]^3.
+
+    At radius 10 the cube spans about +-50 px, where radial distortion is barely observable; a
+    smaller ``radius`` spreads the points over the image.
 
     ``self_calibrating=False``: fixed Brown-Conrady (k1, k2, k3) intrinsics.
     ``self_calibrating=True``: one shared Brown-Conrady K1K2 group with free (f, k1, k2) and a fixed
@@ -95,7 +98,7 @@ def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_cali
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     ang = 2 * np.pi * np.arange(cameras) / cameras
-    C = np.stack([10 * np.cos(ang), 10 * np.sin(ang), 0.5 * np.sin(3 * ang)], axis=1)
+    C = np.stack([radius * np.cos(ang), radius * np.sin(ang), 0.05 * radius * np.sin(3 * ang)], axis=1)
     R = _look_at(C, np.zeros_like(C))
     X = rng.uniform(-1.0, 1.0, size=(points, 3))
     f, cx, cy = 500.0, 320.0, 240.0

@@ -998,6 +998,13 @@ static double scene_scale_plain(const Native& n, const std::vector<NPose>& poses
 // eigenvalues from cyclic Jacobi rotations (a published symmetric eigenvalue method).
 static int spectral_rank(std::vector<double> A, int D, bool* ok) {
   *ok = false;
+  if (const char* dump = std::getenv("OMVGBA_ORACLE_DUMP_S")) {
+    if (FILE* f = std::fopen(dump, "ab")) {
+      std::fwrite(&D, sizeof(int), 1, f);
+      std::fwrite(A.data(), sizeof(double), A.size(), f);
+      std::fclose(f);
+    }
+  }
   double ds = 0.0;
   for (int i = 0; i < D; ++i) ds = std::max(ds, std::fabs(A[(size_t)i * D + i]));
   if (!(std::isfinite(ds) && ds > 0.0)) return 0;
@@ -1039,10 +1046,15 @@ static int spectral_rank(std::vector<double> A, int D, bool* ok) {
         }
       }
   }
-  double largest = 0.0;
-  for (int i = 0; i < D; ++i) largest = std::max(largest, std::fabs(A[(size_t)i * D + i]));
+  double largest = 0.0, smallest = kInf;
+  for (int i = 0; i < D; ++i) {
+    largest = std::max(largest, std::fabs(A[(size_t)i * D + i]));
+    smallest = std::min(smallest, A[(size_t)i * D + i]);
+  }
   if (!(std::isfinite(largest) && largest > 0.0)) return 0;
   double tol = 64.0 * kEps * D * largest;
+  if (std::getenv("OMVGBA_ORACLE_TRACE"))
+    std::fprintf(stderr, "rank: lambda_max %.6e lambda_min %.6e tol %.3e\n", largest, smallest, tol);
   int rank = 0;
   for (int i = 0; i < D; ++i) {
     double v = A[(size_t)i * D + i];
@@ -1349,6 +1361,9 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
   }
   bool well = rep.rank != 2 && fa.weak == 0;
   rep.status = run.status(well);
+  if (std::getenv("OMVGBA_ORACLE_TRACE"))
+    std::fprintf(stderr, "final: valid=%d rank=%d weak=%llu status=%d D=%d min_rcond=%.3e\n", (int)fa.valid, rep.rank,
+                 (unsigned long long)fa.weak, rep.status, D, fa.min_rcond);
   rep.reason = run.convergence;
   if (fa.valid) {
     rep.final_cost = fa.cost;

@@ -1,0 +1,405 @@
+#!/usr/bin/env python3
+"""Benchmark: bundle-adjustment time-to-converge and LM iterations/s on one B200 (or N replicas).
+
+Workload: the 500-camera problem with per-camera intrinsics (6-DoF pose + log f, k1, k2 per
+camera, D = 4,493) over a 100 x 100 ground plane, 200,000 points with geometric track lengths
+(mean ~6, minimum 2; 1,184,956 observations at seed 11), pixel noise N(0, 0.5^2), 5% outliers,
+Huber loss (1 px), 50 LM iterations, block-Jacobi PCG with forcing tolerance 1e-6. Seeded synthetic
+data (no dataset exists for it). One step = one complete solve of that problem.
+
+value  : LM iterations/s of the mixed-precision solve (FP32 products, FP64 everything the
+         reference's acceptance depends on), problem resident in device memory (omvgba_plan_solve),
+         summed over replicas, divided by the slowest rank's time.
+e2e    : the same through omvgba_solve from host arrays (lowering, upload and download included).
+fp64   : the plain FP64 solve of the same problem, for the mixed-vs-FP64 comparison at equal cost.
+roofline: the matrix-free product's tile kernel (k_mv_tiles<float>, the dominant kernel of the
+         solve), timed alone with CUDA events on the plan's stream with L2 flushed before each launch.
+cpu_baseline: the C++ restatement of the reference CPU solver (the oracle) on the first LM
+         iterations of the same problem, all host threads.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch under torch.distributed.run; every rank solves its own seeded replica.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "openmvg-rs_b200"))
+
+METRIC = "BA time-to-converge (s) & LM iters/s, mixed vs FP64 GPU, same final cost"
+UNIT = "LM iterations/s"
+L2_BYTES = 126 * 1024 * 1024
+FLUSH_BYTES = 512 * 1024 * 1024
+WORKLOAD = ("plane500: 500 cameras with per-camera (f, k1, k2) over a 100x100 ground plane, 200k points, "
+            "geometric tracks mean ~6 (1,184,956 observations at seed 11), noise 0.5 px, 5% outliers, "
+            "Huber 1 px, 50 LM iterations, block-Jacobi PCG tolerance 1e-6")
+CPU_SAMPLE_ITERATIONS = 3
+TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane500.txt")
+
+
+def problem_for(rank: int):
+    from openmvg_ba_cuda import synthetic
+    return synthetic.plane_problem(seed=11 + rank, mean_track=6.5)
+
+
+def solve_config(precision: int, max_iterations: int = 50, stream: int = 0):
+    from openmvg_ba_cuda import SolveConfig, abi
+    return SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, precision=precision, pcg_relative_tolerance=1e-6,
+                       max_iterations=max_iterations, stream=stream)
+
+
+# ---- distributed plumbing (replicas: no data-path collective) -----------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def aggregate(seconds: float, units: float, device=None) -> tuple[float, float]:
+    """(max seconds over ranks, sum of units over ranks); identity without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return seconds, units
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+# ---- clocks sampled during the timed region -----------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "nvidia-smi unavailable"}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        return summarize_clocks(open(self.path).read())
+
+
+def summarize_clocks(text: str) -> dict:
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    sm, mx, power, reasons = [], [], [], set()
+    for line in text.splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx.append(float(f[2]))
+            power.append(float(f[3]))
+        except ValueError:
+            continue
+        for name, val in zip(names, f[5:9]):
+            if val.lower().startswith("active"):
+                reasons.add(name)
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+            "samples": len(sm), "power_w_max": max(power)}
+
+
+def measured_peak() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "of measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "of fallback"
+
+
+def traffic_per_launch(observations: int):
+    """DRAM bytes per launch of k_mv_tiles<float> from the committed ncu summary, scaled to this
+    problem's observation count when the capture ran on another size."""
+    try:
+        fields = {}
+        for line in open(TRAFFIC_SUMMARY):
+            if ":" in line:
+                k, v = line.split(":", 1)
+                fields[k.strip()] = v.strip()
+        per_launch = float(fields["dram_bytes_per_launch"])
+        captured = float(fields["observations"])
+        return per_launch * observations / captured
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---- CPU baseline: the oracle (C++ restatement of the reference CPU solver) ----------------------
+def cpu_sample(problem, iterations: int) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from openmvg_ba_cuda import abi
+    threads = oracle.max_threads()
+    oracle.set_threads(threads)
+    cfg = solve_config(abi.PRECISION_FP64, max_iterations=iterations)
+    t0 = time.perf_counter()
+    sol = oracle.solve(problem, cfg)
+    dt = time.perf_counter() - t0
+    its = int(sol.report["iteration_count"])
+    return {"value": its / dt, "unit": UNIT, "cores": threads, "kind": "port", "seconds": dt, "iterations": its,
+            "pcg_iterations": int(sol.report.get("pcg_iteration_count", 0)),
+            "sample": (f"oracle (C++/OpenMP restatement of the reference CPU solver) on the first {its} LM "
+                       f"iterations of the same problem, lowering and final certificate included, {threads} "
+                       "threads; early iterations need fewer PCG iterations than the 50-iteration average, "
+                       "so this rate favours the CPU")}
+
+
+def cpu_info() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args) -> int:
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    problem = problem_for(0)
+    for _ in range(args.warmup):
+        cpu_sample(problem, 1)
+    samples = [cpu_sample(problem, CPU_SAMPLE_ITERATIONS) for _ in range(args.steps)]
+    total_s = sum(s["seconds"] for s in samples)
+    total_it = sum(s["iterations"] for s in samples)
+    value = total_it / total_s
+    base = dict(samples[-1])
+    base["value"] = value
+    base.pop("seconds"), base.pop("iterations"), base.pop("pcg_iterations")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads", "cpu": cpu_info(),
+                   "sample_lm_iterations_per_step": CPU_SAMPLE_ITERATIONS},
+        "cpu_baseline": base,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- our arm ---------------------------------------------------------------------------------
+def timed_solves(solve, stream, flush, steps: int):
+    """Run `steps` solves, each timed by CUDA events on `stream` after an L2 flush."""
+    import torch
+    reports, ms = [], []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sol = solve()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        reports.append(sol.report)
+    return reports, ms, sol
+
+
+def kernel_roofline(plan, info: dict, stream, flush, launches: int = 20) -> dict:
+    """Average duration of the tile kernel k_mv_tiles<float> alone (CUDA events on the plan's
+    stream, L2 flushed before every launch) and its algorithmic bytes per launch: the FP32 Jacobian
+    entries, one camera index per observation, the FP64 damped point inverse (6 values) per point
+    and the camera vector x read once."""
+    import torch
+    D = int(info["reduced_dimension"])
+    x = torch.randn(D, dtype=torch.float64, device="cuda")
+    y = torch.empty(D, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    plan.schur_product(x.data_ptr(), y.data_ptr(), 0.1, fp32=True, stage=0)  # linearize once
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(launches):
+        with torch.cuda.stream(stream):
+            flush.fill_(2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.schur_product(x.data_ptr(), y.data_ptr(), 0.1, fp32=True, stage=1)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    avg_s = total / launches / 1e3
+    algorithmic = (4 * int(info["jacobian_entries"]) + 4 * int(info["observation_count"])
+                   + 48 * int(info["point_count"]) + 8 * D)
+    peak, which = measured_peak()
+    achieved = algorithmic / avg_s / 1e9
+    traffic = traffic_per_launch(int(info["observation_count"]))
+    return {"bound": "hbm", "kernel": "k_mv_tiles<float>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": which, "traffic": traffic,
+            "algorithmic_bytes_per_launch": algorithmic, "avg_launch_us": avg_s * 1e6, "launches_timed": launches}
+
+
+def run_ours(args) -> int:
+    import torch
+    world, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the solver has no CPU path)")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.adjuster import CudaBundleAdjuster
+
+    problem = problem_for(rank)
+    stream = torch.cuda.Stream(device=local)  # the solver's stream: events and flushes go here too
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    adjuster = CudaBundleAdjuster(local)
+    mixed_cfg = solve_config(abi.PRECISION_MIXED, stream=stream.cuda_stream)
+    fp64_cfg = solve_config(abi.PRECISION_FP64, stream=stream.cuda_stream)
+
+    # value: mixed precision, problem resident in device memory
+    plan = adjuster.plan(problem, mixed_cfg)
+    info = plan.info()
+    for _ in range(args.warmup):
+        plan.solve()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_wall = time.perf_counter()
+    reports, ms, mixed_sol = timed_solves(plan.solve, stream, flush, args.steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clock_summary = clocks.stop()
+    barrier()
+    local_s = sum(ms) / 1e3
+    local_its = sum(r["iteration_count"] for r in reports)
+    total_s, total_its = aggregate(local_s, float(local_its), device="cuda")
+    value = total_its / total_s
+    launches = sum(r["kernel_launches"] for r in reports)
+    roofline = kernel_roofline(plan, info, stream, flush)
+    plan.close()
+
+    if args.legs == "value":  # profiling runs: the resident mixed solve and the kernel timing only
+        adjuster.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "legs": "value", "gpu_launches": int(launches),
+                              "roofline": roofline, "clocks": clock_summary}), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    # FP64 on the same problem: the comparison at equal final cost
+    plan64 = adjuster.plan(problem, fp64_cfg)
+    plan64.solve()
+    torch.cuda.synchronize()
+    barrier()
+    reports64, ms64, sol64 = timed_solves(plan64.solve, stream, flush, args.steps)
+    barrier()
+    plan64.close()
+    s64, its64 = aggregate(sum(ms64) / 1e3, float(sum(r["iteration_count"] for r in reports64)), device="cuda")
+
+    # e2e: omvgba_solve from host arrays every step
+    barrier()
+    e2e_reports, e2e_ms, _ = timed_solves(lambda: adjuster.solve(problem, mixed_cfg), stream, flush, args.steps)
+    barrier()
+    e2e_s, e2e_its = aggregate(sum(e2e_ms) / 1e3, float(sum(r["iteration_count"] for r in e2e_reports)),
+                               device="cuda")
+    adjuster.close()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_sample(problem, CPU_SAMPLE_ITERATIONS)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"cpu": cpu_info()}
+
+    if rank == 0:
+        cost_mixed = reports[-1]["final_objective"]
+        cost_fp64 = reports64[-1]["final_objective"]
+        steps = args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total_s / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "mixed", "parallelism": f"replicas x{world}",
+                       "observations": int(info["observation_count"]), "points": int(info["point_count"]),
+                       "cameras": int(info["camera_count"]), "reduced_dimension": int(info["reduced_dimension"]),
+                       "l2": ("inputs larger than L2: %.0f MB of Jacobian records and tile tables per solve vs "
+                              "126 MB L2; L2 also flushed (512 MB write) before every step"
+                              % ((info["record_bytes_fp32"] + info["record_bytes_fp64"] + info["metadata_bytes_fp32"]
+                                  + info["metadata_bytes_fp64"]) / 1e6))},
+            "time_to_converge_s": total_s / steps,
+            "lm_iterations_per_step": local_its / steps,
+            "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports) / steps,
+            "final_cost": cost_mixed,
+            "fp64": {"value": its64 / s64, "unit": UNIT, "time_to_converge_s": s64 / steps, "final_cost": cost_fp64,
+                     "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports64) / steps},
+            "mixed_vs_fp64": {"speedup": (s64 / steps) / (total_s / steps),
+                              "final_cost_rel_diff": abs(cost_mixed - cost_fp64) / abs(cost_fp64)},
+            "clocks": clock_summary,
+            "e2e": {"value": e2e_its / e2e_s, "unit": UNIT, "time_to_converge_s": e2e_s / steps,
+                    "h2d_bytes_per_step": int(sum(r["h2d_bytes"] for r in e2e_reports) / steps),
+                    "d2h_bytes_per_step": int(sum(r["d2h_bytes"] for r in e2e_reports) / steps),
+                    "host_buffers": "numpy arrays passed to omvgba_solve (lowering on the host inside the step)"},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--legs", choices=["all", "value"], default="all",
+                    help="value: only the resident mixed solve and the kernel timing (for profiler runs)")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

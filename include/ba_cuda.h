@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OMVGBA_ABI_VERSION 1u
+#define OMVGBA_ABI_VERSION 2u
 
 /* ---- return codes (SolveError, solver.rs:1474-1493; ProblemError, problem.rs:731) ---- */
 enum omvgba_code {
@@ -204,6 +204,8 @@ typedef struct omvgba_report {
   double final_damping;
   double solve_seconds;           /* wall time inside omvgba_solve */
   double upload_seconds;          /* host->device problem upload inside that time */
+  uint64_t kernel_launches;       /* GPU kernels the call launched (graph-launched ones included) */
+  uint64_t h2d_bytes, d2h_bytes;  /* host<->device bytes the call copied */
 } omvgba_report;
 
 /* Solution (solver.rs:788-1314). Every array is caller-allocated. */
@@ -229,6 +231,47 @@ int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, con
 
 /* BundleAdjuster::name (solver.rs:1566). */
 const char* omvgba_adjuster_name(void);
+
+/*
+ * A problem prepared once for repeated solves: validation, the quarantine of input points that
+ * cannot be adjusted (quarantine.rs:34-96), lowering (native/mod.rs:260-367) and the upload to
+ * device memory happen in omvgba_plan_create; every omvgba_plan_solve then starts from the
+ * problem's initial state with everything already in device memory, and returns what omvgba_solve
+ * would return for the same problem and config. The problem's arrays must stay alive and unchanged
+ * until omvgba_plan_destroy. A plan runs on config->stream (or the context's stream) and, like its
+ * context, is used by one thread at a time. No reference counterpart: the reference lowers and
+ * solves in one call (native/mod.rs:117-367).
+ */
+typedef struct omvgba_plan omvgba_plan;
+
+typedef struct omvgba_plan_info {
+  uint64_t observation_count;     /* observations in the solved problem (after input quarantine) */
+  uint64_t point_count;
+  uint64_t camera_count;
+  uint64_t reduced_dimension;     /* D, schur/layout.rs:143-205 */
+  uint64_t jacobian_entries;      /* sum over observations of 2 x (free camera dim + free point dim) */
+  uint64_t tile_count_fp64, tile_count_fp32;
+  uint64_t record_bytes_fp64, record_bytes_fp32;      /* per-observation Jacobian records in device memory */
+  uint64_t metadata_bytes_fp64, metadata_bytes_fp32;  /* per-tile segment tables of the matrix-free product */
+  int32_t iterative;              /* 1: PCG steps; 0: dense Cholesky steps */
+  int32_t mixed;                  /* 1: FP32 products with FP64 refinement */
+} omvgba_plan_info;
+
+int32_t omvgba_plan_create(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                           omvgba_plan** plan, omvgba_error* error);
+int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_error* error);
+int32_t omvgba_plan_info_get(const omvgba_plan* plan, omvgba_plan_info* info, omvgba_error* error);
+/*
+ * The reduced camera system product y = S_lambda x of a PCG plan at its initial state's
+ * linearization (the first call, and the first after a solve or a new lambda, re-linearizes).
+ * x and y are DEVICE pointers of reduced_dimension doubles. fp32 selects the FP32 records of a
+ * mixed plan. stage 0 computes the whole product; stage 1 launches only the tile pass (the
+ * per-point coupling partials, y untouched), for timing the kernel by itself. Runs on the plan's
+ * stream without synchronizing. Operator: retained/operator.rs:137-227.
+ */
+int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32, int32_t stage, const double* x,
+                                  double* y, omvgba_error* error);
+void omvgba_plan_destroy(omvgba_plan* plan);
 
 /*
  * First linearization of the lowered problem, per observation in the solver's

@@ -41,6 +41,32 @@ namespace omvgba {
 constexpr int kChunk = 256;     // entities per block chunk
 constexpr int kReduceThreads = 256;
 
+// Telemetry of the calling thread: kernels launched and host<->device bytes copied. A solve runs
+// on the thread that called it, so the report takes the difference across the call.
+struct Telemetry {
+  uint64_t launches = 0, h2d = 0, d2h = 0;
+};
+thread_local Telemetry tl_telemetry;
+
+void telemetry_read(uint64_t* launches, uint64_t* h2d, uint64_t* d2h) {
+  *launches = tl_telemetry.launches;
+  *h2d = tl_telemetry.h2d;
+  *d2h = tl_telemetry.d2h;
+}
+
+// Every kernel launch goes through this macro so that the report can state how many ran.
+#define OMVGBA_LAUNCH(kernel, grid, block, smem, stream, ...)   \
+  do {                                                          \
+    kernel<<<grid, block, smem, stream>>>(__VA_ARGS__);         \
+    ++tl_telemetry.launches;                                    \
+  } while (0)
+
+inline cudaError_t copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  if (kind == cudaMemcpyHostToDevice) tl_telemetry.h2d += bytes;
+  if (kind == cudaMemcpyDeviceToHost) tl_telemetry.d2h += bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, st);
+}
+
 // ----------------------------------------------------------------------------------------------
 // Context
 // ----------------------------------------------------------------------------------------------
@@ -92,7 +118,7 @@ struct DBuf {
   }
   void upload(const T* host, size_t count, cudaStream_t stream) {
     alloc(count, stream);
-    if (count) CUDA_OK(cudaMemcpyAsync(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, stream));
+    if (count) CUDA_OK(copy_async(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, stream));
   }
   void zero() {
     if (n) CUDA_OK(cudaMemsetAsync(p, 0, sizeof(T) * n, s));
@@ -1729,7 +1755,8 @@ struct Solver {
   DBuf<RedVec<1>> d_norm_part;
   int red_blocks;
 
-  Solver(Context* c, const NativeProblem& prob, const LmOptions& o) : ctx(c), st(c->stream), n(prob), opt(o) {
+  Solver(Context* c, const NativeProblem& prob, const LmOptions& o)
+      : ctx(c), st(o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream), n(prob), opt(o) {
     L = make_layout(n);
     N = (int)n.obs_cam.size();
     P = (int)(n.points.size() / 3);
@@ -1947,11 +1974,11 @@ struct Solver {
 
   template <int NV>
   RedVec<NV> reduce(const RedVec<NV>* in, int count, DBuf<RedVec<NV>>& part) {
-    k_reduce_vec<NV><<<red_blocks, kReduceThreads, 0, st>>>(in, count, part.p);
-    k_reduce_vec<NV><<<1, kReduceThreads, 0, st>>>(part.p, red_blocks, part.p + 0);
+    OMVGBA_LAUNCH(k_reduce_vec<NV>, red_blocks, kReduceThreads, 0, st, in, count, part.p);
+    OMVGBA_LAUNCH(k_reduce_vec<NV>, 1, kReduceThreads, 0, st, part.p, red_blocks, part.p + 0);
     check_launch();
     RedVec<NV> h;
-    CUDA_OK(cudaMemcpyAsync(&h, part.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&h, part.p, sizeof(h), cudaMemcpyDeviceToHost, st));
     sync();
     return h;
   }
@@ -1962,7 +1989,7 @@ struct Solver {
     g.scene = scene;
     if (n.gauge_cam >= 0) {
       double t[3];
-      CUDA_OK(cudaMemcpyAsync(t, d_pose[which].p + 12 * n.gauge_cam + 9, sizeof(t), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(t, d_pose[which].p + 12 * n.gauge_cam + 9, sizeof(t), cudaMemcpyDeviceToHost, st));
       sync();
       g.baseline = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
       for (int k = 0; k < 3; ++k) g.dir[k] = t[k] / g.baseline;
@@ -2006,46 +2033,46 @@ struct Solver {
   // Full linearization + camera-side reductions at the given damping.
   Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_dense) {
     DevView v = view();
-    k_linearize<T><<<grid_for(P, 128), 128, 0, st>>>(v, state(which), g, loss, lambda, lin());
+    OMVGBA_LAUNCH(k_linearize<T>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin());
     check_launch();
-    k_reduce_summary<<<red_blocks, kReduceThreads, 0, st>>>(d_summary.p, P, d_summary_part.p);
-    k_reduce_summary<<<1, kReduceThreads, 0, st>>>(d_summary_part.p, red_blocks, d_summary_part.p);
+    OMVGBA_LAUNCH(k_reduce_summary, red_blocks, kReduceThreads, 0, st, d_summary.p, P, d_summary_part.p);
+    OMVGBA_LAUNCH(k_reduce_summary, 1, kReduceThreads, 0, st, d_summary_part.p, red_blocks, d_summary_part.p);
     check_launch();
     BlockTables bt = tables();
     if (bt.nchunks > 0) {
-      k_block_chunks<T><<<bt.nchunks, 32, 0, st>>>(bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
-      k_block_finalize<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_chunk_out.p, d_blk_out.p);
+      OMVGBA_LAUNCH(k_block_chunks<T>, bt.nchunks, 32, 0, st, bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
+      OMVGBA_LAUNCH(k_block_finalize, grid_for(nb, 64), 64, 0, st, bt, d_chunk_out.p, d_blk_out.p);
       CUDA_OK(cudaMemsetAsync(d_gfull.p, 0, sizeof(double) * std::max(1, D), st));
       CUDA_OK(cudaMemsetAsync(d_gred.p, 0, sizeof(double) * std::max(1, D), st));
       CUDA_OK(cudaMemsetAsync(d_diag.p, 0, sizeof(double) * std::max(1, D), st));
-      k_block_vectors<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_blk_out.p, d_gfull.p, d_gred.p, d_diag.p, d_clamp.p,
+      OMVGBA_LAUNCH(k_block_vectors, grid_for(nb, 64), 64, 0, st, bt, d_blk_out.p, d_gfull.p, d_gred.p, d_diag.p, d_clamp.p,
                                                      d_diag_minmax.p);
       check_launch();
     }
     if (build_dense && D > 0) {
       PairTables pt = pairs(false);
-      if (pt.ngroups > 0) k_pairs<T><<<pt.ngroups, 32, 0, st>>>(pt, bt, lin(), d_seg_col.p, d_pair_out.p);
+      if (pt.ngroups > 0) OMVGBA_LAUNCH(k_pairs<T>, pt.ngroups, 32, 0, st, pt, bt, lin(), d_seg_col.p, d_pair_out.p);
       CUDA_OK(cudaMemsetAsync(d_S.p, 0, sizeof(double) * (size_t)D * D, st));
-      k_dense_from_blocks<<<nb, 32, 0, st>>>(bt, d_blk_out.p, D, d_S.p);
-      if (pt.ngroups > 0) k_dense_pairs<<<grid_for(pt.ngroups, 64), 64, 0, st>>>(pt, bt, d_pair_out.p, D, d_S.p);
-      k_dense_add_diag<<<grid_for(D, 128), 128, 0, st>>>(D, d_diag.p, lambda, d_S.p);
+      OMVGBA_LAUNCH(k_dense_from_blocks, nb, 32, 0, st, bt, d_blk_out.p, D, d_S.p);
+      if (pt.ngroups > 0) OMVGBA_LAUNCH(k_dense_pairs, grid_for(pt.ngroups, 64), 64, 0, st, pt, bt, d_pair_out.p, D, d_S.p);
+      OMVGBA_LAUNCH(k_dense_add_diag, grid_for(D, 128), 128, 0, st, D, d_diag.p, lambda, d_S.p);
       check_launch();
     }
     PointSummary ps;
-    CUDA_OK(cudaMemcpyAsync(&ps, d_summary_part.p, sizeof(ps), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&ps, d_summary_part.p, sizeof(ps), cudaMemcpyDeviceToHost, st));
     std::vector<double> mm(2 * std::max(nb, 1));
     std::vector<int> cl(std::max(nb, 1));
     std::vector<double> gvals(std::max(D, 1)), dvals(std::max(D, 1));
     if (nb > 0) {
-      CUDA_OK(cudaMemcpyAsync(mm.data(), d_diag_minmax.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaMemcpyAsync(cl.data(), d_clamp.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(mm.data(), d_diag_minmax.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(cl.data(), d_clamp.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
     }
     if (D > 0) {
-      CUDA_OK(cudaMemcpyAsync(gvals.data(), d_gfull.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaMemcpyAsync(dvals.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(gvals.data(), d_gfull.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(dvals.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
     }
     std::vector<double> gr(std::max(D, 1));
-    if (D > 0) CUDA_OK(cudaMemcpyAsync(gr.data(), d_gred.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+    if (D > 0) CUDA_OK(copy_async(gr.data(), d_gred.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
     sync();
     Assembly a;
     a.valid = ps.invalid == 0.0;
@@ -2083,15 +2110,15 @@ struct Solver {
 
   // ---- camera step ----
   bool direct_step() {
-    CUDA_OK(cudaMemcpyAsync(d_Lf.p, d_S.p, sizeof(double) * (size_t)D * D, cudaMemcpyDeviceToDevice, st));
-    k_dense_cholesky<<<1, 1024, 0, st>>>(D, d_Lf.p, d_status.p);
-    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_step.p);
+    CUDA_OK(copy_async(d_Lf.p, d_S.p, sizeof(double) * (size_t)D * D, cudaMemcpyDeviceToDevice, st));
+    OMVGBA_LAUNCH(k_dense_cholesky, 1, 1024, 0, st, D, d_Lf.p, d_status.p);
+    OMVGBA_LAUNCH(k_neg_copy, grid_for(D, 256), 256, 0, st, D, d_gred.p, d_step.p);
     check_launch();
     int ok = 0;
-    CUDA_OK(cudaMemcpyAsync(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
     if (!ok) return false;
-    k_dense_solve<<<1, 32, 0, st>>>(D, d_Lf.p, d_step.p);
+    OMVGBA_LAUNCH(k_dense_solve, 1, 32, 0, st, D, d_Lf.p, d_step.p);
     check_launch();
     return true;
   }
@@ -2105,30 +2132,36 @@ struct Solver {
       ++k;
     }
     a.count = k;
-    k_dots<<<1, 1024, 0, st>>>(a, D, d_scalars.p);
+    OMVGBA_LAUNCH(k_dots, 1, 1024, 0, st, a, D, d_scalars.p);
     check_launch();
-    CUDA_OK(cudaMemcpyAsync(out, d_scalars.p, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(out, d_scalars.p, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
     sync();
   }
 
   // y = S_lambda x (implicit, matrix-free); ctl: optional PCG control for graph-launched iterations
   // fp32: use the FP32 record copy (mixed precision inner solves)
   void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false) {
+    matvec_tiles(x, ctl, fp32);
+    const TileSetDev& ts = fp32 ? dT32 : dT64;
+    MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
+    OMVGBA_LAUNCH(k_mv_tiles_finalize, grid_for((size_t)nb * 32, 256), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda, x, y, ctl);
+    check_launch();
+  }
+  // The tile pass of the product alone: per-(segment, component) partials of the point coupling.
+  void matvec_tiles(const double* x, const PcgCtl* ctl, bool fp32) {
     const TileSetDev& ts = fp32 ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        k_mv_tiles<float><<<ts.grid, 256, mv_smem_bytes<float>(), st>>>(mt, d_rec32.p, d_vinv.p, x, ts.partial.p,
+        OMVGBA_LAUNCH(k_mv_tiles<float>, ts.grid, 256, mv_smem_bytes<float>(), st, mt, d_rec32.p, d_vinv.p, x, ts.partial.p,
                                                                         ctl, d_fault.p);
       else
-        k_mv_tiles<T><<<ts.grid, 256, mv_smem_bytes<T>(), st>>>(mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl, d_fault.p);
+        OMVGBA_LAUNCH(k_mv_tiles<T>, ts.grid, 256, mv_smem_bytes<T>(), st, mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl, d_fault.p);
     }
-    k_mv_tiles_finalize<<<grid_for((size_t)nb * 32, 256), 256, 0, st>>>(mt, ts.partial.p, d_diag.p, lambda, x, y, ctl);
-    check_launch();
   }
   void check_fault() {
     int f = 0;
-    CUDA_OK(cudaMemcpyAsync(&f, d_fault.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&f, d_fault.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
     if (f) throw SolveFailure{8, "a bulk shared-memory copy did not complete within its wait limit"};
   }
@@ -2136,19 +2169,19 @@ struct Solver {
   bool factor_preconditioner(double lambda) {
     BlockTables bt = tables();
     PairTables xt = pairs(true);
-    if (xt.ngroups > 0) k_pairs<T><<<xt.ngroups, 32, 0, st>>>(xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
-    k_block_factor<<<grid_for(nb, 64), 64, 0, st>>>(bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
+    if (xt.ngroups > 0) OMVGBA_LAUNCH(k_pairs<T>, xt.ngroups, 32, 0, st, xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
+    OMVGBA_LAUNCH(k_block_factor, grid_for(nb, 64), 64, 0, st, bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
                                                    d_blk_cross_begin.p, d_blk_cross_end.p, d_factor.p, d_fail.p);
     check_launch();
     std::vector<int> fail(std::max(nb, 1));
-    if (nb > 0) CUDA_OK(cudaMemcpyAsync(fail.data(), d_fail.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    if (nb > 0) CUDA_OK(copy_async(fail.data(), d_fail.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
     sync();
     for (int b = 0; b < nb; ++b)
       if (fail[b]) return false;
     return true;
   }
   void precond(const double* r, double* z, const PcgCtl* ctl = nullptr) {
-    k_block_precond<<<grid_for(nb, 64), 64, 0, st>>>(tables(), d_factor.p, r, z, ctl);
+    OMVGBA_LAUNCH(k_block_precond, grid_for(nb, 64), 64, 0, st, tables(), d_factor.p, r, z, ctl);
     check_launch();
   }
 
@@ -2182,7 +2215,7 @@ struct Solver {
       }
     } rpt{t_start, &launches, &restarts, &res, fp32};
     CUDA_OK(cudaMemsetAsync(x, 0, sizeof(double) * D, st));
-    CUDA_OK(cudaMemcpyAsync(d_r.p, b, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(copy_async(d_r.p, b, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
     double h[4];
     dots({{d_r.p, d_r.p}}, h);
     double n0 = std::sqrt(h[0]);
@@ -2193,7 +2226,7 @@ struct Solver {
       return res;
     }
     precond(d_r.p, d_z.p);
-    CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(copy_async(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
     dots({{d_r.p, d_z.p}}, h);
     double rho = h[0];
     if (!(std::isfinite(rho) && rho > 0.0)) return res;
@@ -2206,17 +2239,20 @@ struct Solver {
     ctl.terms = 0;
     ctl.max_it = (int)std::min<uint64_t>(max_it, (uint64_t)INT32_MAX);
     PcgCtl* dctl = reinterpret_cast<PcgCtl*>(d_ctl.p);
-    CUDA_OK(cudaMemcpyAsync(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+    CUDA_OK(copy_async(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
     cudaGraph_t graph;
     cudaGraphExec_t exec;
+    const uint64_t launches_before = tl_telemetry.launches;
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     matvec(d_dir.p, d_q.p, lambda, dctl, fp32);
-    k_pcg_alpha<<<1, 1024, 0, st>>>(D, d_dir.p, d_q.p, dctl);
-    k_pcg_update<<<grid_for(D, 256), 256, 0, st>>>(D, d_dir.p, d_q.p, x, d_r.p, dctl);
+    OMVGBA_LAUNCH(k_pcg_alpha, 1, 1024, 0, st, D, d_dir.p, d_q.p, dctl);
+    OMVGBA_LAUNCH(k_pcg_update, grid_for(D, 256), 256, 0, st, D, d_dir.p, d_q.p, x, d_r.p, dctl);
     precond(d_r.p, d_z.p, dctl);
-    k_pcg_beta<<<1, 1024, 0, st>>>(D, d_r.p, d_z.p, dctl);
-    k_pcg_direction<<<grid_for(D, 256), 256, 0, st>>>(D, d_z.p, d_dir.p, dctl);
+    OMVGBA_LAUNCH(k_pcg_beta, 1, 1024, 0, st, D, d_r.p, d_z.p, dctl);
+    OMVGBA_LAUNCH(k_pcg_direction, grid_for(D, 256), 256, 0, st, D, d_z.p, d_dir.p, dctl);
     CUDA_OK(cudaStreamEndCapture(st, &graph));
+    const uint64_t kernels_per_graph = tl_telemetry.launches - launches_before;  // counted at capture
+    tl_telemetry.launches = launches_before;
     CUDA_OK(cudaGraphInstantiate(&exec, graph, 0));
     struct GraphGuard {
       cudaGraph_t g;
@@ -2228,13 +2264,14 @@ struct Solver {
     } guard{graph, exec};
     auto recompute = [&]() {
       matvec(x, d_q.p, lambda, nullptr, fp32);
-      k_sub<<<grid_for(D, 256), 256, 0, st>>>(D, b, d_q.p, d_r.p);
+      OMVGBA_LAUNCH(k_sub, grid_for(D, 256), 256, 0, st, D, b, d_q.p, d_r.p);
       check_launch();
     };
     for (;;) {
       for (int k = 0; k < kPoll; ++k) CUDA_OK(cudaGraphLaunch(exec, st));
+      tl_telemetry.launches += kPoll * kernels_per_graph;
       launches += kPoll;
-      CUDA_OK(cudaMemcpyAsync(&ctl, dctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(&ctl, dctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
       sync();
       check_fault();
       if (ctl.status == kRunning) continue;
@@ -2265,7 +2302,7 @@ struct Solver {
         return res;
       }
       precond(d_r.p, d_z.p);
-      CUDA_OK(cudaMemcpyAsync(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+      CUDA_OK(copy_async(d_dir.p, d_z.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
       dots({{d_r.p, d_z.p}}, h);
       double nrho = h[0];
       if (!(std::isfinite(nrho) && nrho > 0.0)) {
@@ -2276,7 +2313,7 @@ struct Solver {
       if ((uint64_t)ctl.terms >= max_it) break;
       ctl.rho = nrho;
       ctl.status = kRunning;
-      CUDA_OK(cudaMemcpyAsync(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+      CUDA_OK(copy_async(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
     }
     recompute();
     dots({{d_r.p, d_r.p}}, h);
@@ -2287,7 +2324,7 @@ struct Solver {
   }
 
   PcgResult pcg(double lambda, uint64_t max_it, double tol) {
-    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_rhs.p);
+    OMVGBA_LAUNCH(k_neg_copy, grid_for(D, 256), 256, 0, st, D, d_gred.p, d_rhs.p);
     check_launch();
     return pcg_run(d_rhs.p, d_step.p, lambda, max_it, tol, false, true);
   }
@@ -2297,7 +2334,7 @@ struct Solver {
   // same acceptance rule as the FP64 solve, within the same iteration budget.
   PcgResult pcg_mixed(double lambda, uint64_t max_it, double tol) {
     PcgResult res;
-    k_neg_copy<<<grid_for(D, 256), 256, 0, st>>>(D, d_gred.p, d_rhs.p);
+    OMVGBA_LAUNCH(k_neg_copy, grid_for(D, 256), 256, 0, st, D, d_gred.p, d_rhs.p);
     check_launch();
     double h[4];
     dots({{d_rhs.p, d_rhs.p}}, h);
@@ -2309,7 +2346,7 @@ struct Solver {
       res.rel = 0.0;
       return res;
     }
-    CUDA_OK(cudaMemcpyAsync(d_r64.p, d_rhs.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(copy_async(d_r64.p, d_rhs.p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
     double rel = 1.0;
     uint64_t terms = 0;
     for (int outer = 0; outer < 32 && terms < max_it; ++outer) {
@@ -2320,9 +2357,9 @@ struct Solver {
         res.terms = terms;
         return res;  // curvature or finiteness failure
       }
-      k_axpy<<<grid_for(D, 256), 256, 0, st>>>(D, 1.0, d_e.p, d_step.p);
+      OMVGBA_LAUNCH(k_axpy, grid_for(D, 256), 256, 0, st, D, 1.0, d_e.p, d_step.p);
       matvec(d_step.p, d_q.p, lambda, nullptr, false);
-      k_sub<<<grid_for(D, 256), 256, 0, st>>>(D, d_rhs.p, d_q.p, d_r64.p);
+      OMVGBA_LAUNCH(k_sub, grid_for(D, 256), 256, 0, st, D, d_rhs.p, d_q.p, d_r64.p);
       check_launch();
       dots({{d_r64.p, d_r64.p}}, h);
       double nrel = std::sqrt(h[0]) / n0;
@@ -2383,7 +2420,7 @@ struct Solver {
   }
 
   void metrics(int which, const LossDev& loss, double* cost, double* rmse) {
-    k_metrics<<<grid_for(P, 128), 128, 0, st>>>(view(), state(which), loss, d_met.p);
+    OMVGBA_LAUNCH(k_metrics, grid_for(P, 128), 128, 0, st, view(), state(which), loss, d_met.p);
     check_launch();
     RedVec<3> r = reduce<3>(d_met.p, P, d_met_part);
     if (r.v[2] > 0.0) {
@@ -2398,6 +2435,24 @@ struct Solver {
   double t_assemble = 0, t_solve = 0, t_candidate = 0;
   static double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  }
+
+  // Resident use (one upload, many solves): the initial state is kept and restored before each solve.
+  DBuf<double> d_pose_init, d_points_init, d_groups_init;
+  void keep_initial() {
+    for (auto pr : {std::make_pair(&d_pose_init, &d_pose[cur]), std::make_pair(&d_points_init, &d_points[cur]),
+                    std::make_pair(&d_groups_init, &d_groups[cur])}) {
+      pr.first->alloc(pr.second->n, st);
+      CUDA_OK(copy_async(pr.first->p, pr.second->p, sizeof(double) * pr.second->n, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  void restore_initial() {
+    cur = 0;
+    for (auto pr : {std::make_pair(&d_pose_init, &d_pose[0]), std::make_pair(&d_points_init, &d_points[0]),
+                    std::make_pair(&d_groups_init, &d_groups[0])})
+      CUDA_OK(copy_async(pr.second->p, pr.first->p, sizeof(double) * pr.first->n, cudaMemcpyDeviceToDevice, st));
+    d_fault.zero();
+    t_assemble = t_solve = t_candidate = 0;
   }
 
   NativeReport refine(std::vector<double>& rotation, std::vector<double>& translation, std::vector<double>& points,
@@ -2505,24 +2560,24 @@ struct Solver {
         }
         // step cap (calibrated only)
         if (!n.self_cal && D > 0) {
-          k_step_block_norm<<<grid_for(n.ncam, 128), 128, 0, st>>>(n.ncam, d_pose_off.p, d_pose_dim.p, d_step.p,
+          OMVGBA_LAUNCH(k_step_block_norm, grid_for(n.ncam, 128), 128, 0, st, n.ncam, d_pose_off.p, d_pose_dim.p, d_step.p,
                                                                    d_cam_norm.p);
           check_launch();
           std::vector<double> norms(n.ncam);
-          CUDA_OK(cudaMemcpyAsync(norms.data(), d_cam_norm.p, sizeof(double) * n.ncam, cudaMemcpyDeviceToHost, st));
+          CUDA_OK(copy_async(norms.data(), d_cam_norm.p, sizeof(double) * n.ncam, cudaMemcpyDeviceToHost, st));
           sync();
           double largest = 0.0;
           for (double x : norms) largest = std::max(largest, x);
           if (largest > 0.5) {
-            k_scale<<<grid_for(D, 256), 256, 0, st>>>(D, 0.5 / largest, d_step.p);
+            OMVGBA_LAUNCH(k_scale, grid_for(D, 256), 256, 0, st, D, 0.5 / largest, d_step.p);
             check_launch();
           }
         }
         DevView v = view();
-        k_retract<<<grid_for(std::max(n.ncam, ng), 128), 128, 0, st>>>(v, ng, d_step.p, g, d_pose[cur].p,
+        OMVGBA_LAUNCH(k_retract, grid_for(std::max(n.ncam, ng), 128), 128, 0, st, v, ng, d_step.p, g, d_pose[cur].p,
                                                                         d_groups[cur].p, d_pose[cand].p,
                                                                         d_groups[cand].p);
-        k_candidate_points<T><<<grid_for(P, 128), 128, 0, st>>>(v, lin(), d_step.p, state(cur), state(cand), g,
+        OMVGBA_LAUNCH(k_candidate_points<T>, grid_for(P, 128), 128, 0, st, v, lin(), d_step.p, state(cur), state(cand), g,
                                                                 stages[si].loss, d_cand.p);
         check_launch();
         RedVec<4> cr = reduce<4>(d_cand.p, P, d_cand_part);
@@ -2538,7 +2593,7 @@ struct Solver {
         double damped;
         if (!iterative_step) {
           if (D > 0)
-            k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, st>>>(D, d_S.p, d_step.p, d_q.p);
+            OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, st, D, d_S.p, d_step.p, d_q.p);
           else
             CUDA_OK(cudaMemsetAsync(d_q.p, 0, sizeof(double), st));
           check_launch();
@@ -2554,12 +2609,12 @@ struct Solver {
           if (!(std::isfinite(damped) && damped > 0.0)) damped = NAN;
         }
         // camera damping norm: sum diag * step^2
-        CUDA_OK(cudaMemcpyAsync(d_tmp.p, d_step.p, sizeof(double) * std::max(D, 1), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(copy_async(d_tmp.p, d_step.p, sizeof(double) * std::max(D, 1), cudaMemcpyDeviceToDevice, st));
         double cd[1] = {0.0};
         if (D > 0) {
           std::vector<double> hs(D), hd(D);
-          CUDA_OK(cudaMemcpyAsync(hs.data(), d_step.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
-          CUDA_OK(cudaMemcpyAsync(hd.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+          CUDA_OK(copy_async(hs.data(), d_step.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+          CUDA_OK(copy_async(hd.data(), d_diag.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
           sync();
           for (int i = 0; i < D; ++i) cd[0] += hd[i] * hs[i] * hs[i];
           double ss = 0.0;
@@ -2644,7 +2699,7 @@ struct Solver {
     rep.rejected = rej[0] + rej[1] + rej[2] + rej[3];
     rep.weak = fa.weak;
     {
-      k_noninvertible<<<grid_for(N, 256), 256, 0, st>>>(view(), N, d_groups[cur].p, d_one.p);
+      OMVGBA_LAUNCH(k_noninvertible, grid_for(N, 256), 256, 0, st, view(), N, d_groups[cur].p, d_one.p);
       check_launch();
       RedVec<1> r = reduce<1>(d_one.p, N, d_one_part);
       rep.noninvertible = (uint64_t)r.v[0];
@@ -2661,12 +2716,12 @@ struct Solver {
     rep.D = D;
     // download state
     std::vector<double> pose(12 * (size_t)n.ncam);
-    CUDA_OK(cudaMemcpyAsync(pose.data(), d_pose[cur].p, sizeof(double) * pose.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(pose.data(), d_pose[cur].p, sizeof(double) * pose.size(), cudaMemcpyDeviceToHost, st));
     points.resize(n.points.size());
-    CUDA_OK(cudaMemcpyAsync(points.data(), d_points[cur].p, sizeof(double) * points.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(points.data(), d_points[cur].p, sizeof(double) * points.size(), cudaMemcpyDeviceToHost, st));
     groups.assign(n.groups.size(), 0.0);
     if (!groups.empty())
-      CUDA_OK(cudaMemcpyAsync(groups.data(), d_groups[cur].p, sizeof(double) * groups.size(), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(groups.data(), d_groups[cur].p, sizeof(double) * groups.size(), cudaMemcpyDeviceToHost, st));
     sync();
     rotation.resize(9 * (size_t)n.ncam);
     translation.resize(3 * (size_t)n.ncam);
@@ -2683,7 +2738,7 @@ struct Solver {
   // which one Cholesky factorization decides; lambda_max comes from power iteration.
   bool rank_full() {
     std::vector<double> Sh((size_t)D * D);
-    CUDA_OK(cudaMemcpyAsync(Sh.data(), d_S.p, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(Sh.data(), d_S.p, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost, st));
     sync();
     double ds = 0.0;
     for (int i = 0; i < D; ++i) ds = std::max(ds, std::fabs(Sh[(size_t)i * D + i]));
@@ -2701,15 +2756,15 @@ struct Solver {
         if (!std::isfinite(v)) return false;
         Sh[(size_t)i * D + j] = v;
       }
-    CUDA_OK(cudaMemcpyAsync(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
+    CUDA_OK(copy_async(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
     // power iteration for the largest |eigenvalue| (Rayleigh quotient of the converged iterate)
     std::vector<double> v(D, 1.0 / std::sqrt((double)D)), w(D);
     double lam = 0.0;
     for (int it = 0; it < 200; ++it) {
-      CUDA_OK(cudaMemcpyAsync(d_tmp.p, v.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
-      k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, st>>>(D, d_Lf.p, d_tmp.p, d_q.p);
+      CUDA_OK(copy_async(d_tmp.p, v.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
+      OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, st, D, d_Lf.p, d_tmp.p, d_q.p);
       check_launch();
-      CUDA_OK(cudaMemcpyAsync(w.data(), d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(copy_async(w.data(), d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
       sync();
       double nrm = 0.0, rq = 0.0;
       for (int i = 0; i < D; ++i) {
@@ -2728,11 +2783,11 @@ struct Solver {
     double tol = 64.0 * kEps * D * largest;
     if (std::getenv("OMVGBA_PHASE_TIMES")) std::fprintf(stderr, "[omvgba] rank: lambda_max %.6e tol %.3e\n", largest, tol);
     for (int i = 0; i < D; ++i) Sh[(size_t)i * D + i] -= tol;
-    CUDA_OK(cudaMemcpyAsync(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
-    k_dense_cholesky<<<1, 1024, 0, st>>>(D, d_Lf.p, d_status.p);
+    CUDA_OK(copy_async(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
+    OMVGBA_LAUNCH(k_dense_cholesky, 1, 1024, 0, st, D, d_Lf.p, d_status.p);
     check_launch();
     int ok = 0;
-    CUDA_OK(cudaMemcpyAsync(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
     return ok != 0;
   }
@@ -2747,6 +2802,94 @@ NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOpti
   return s.refine(rotation, translation, points, groups);
 }
 
+struct Resident {
+  Context* ctx = nullptr;
+  Solver<double>* solver = nullptr;
+  bool linearized = false;  // the records hold the initial state's linearization at `lambda`
+  double lambda = 0.0;
+  ~Resident() { delete solver; }
+};
+
+Resident* resident_create(Context* ctx, const NativeProblem& problem, const LmOptions& options) {
+  CUDA_OK(cudaSetDevice(ctx->device));
+  if (problem.obs_cam.size() >= (1ull << 31)) throw SolveFailure{3, "observation count exceeds 2^31"};
+  Resident* r = new Resident();
+  r->ctx = ctx;
+  try {
+    r->solver = new Solver<double>(ctx, problem, options);
+    r->solver->keep_initial();
+    r->solver->sync();
+  } catch (...) {
+    delete r;
+    throw;
+  }
+  return r;
+}
+
+void resident_destroy(Resident* r) {
+  if (!r) return;
+  cudaSetDevice(r->ctx->device);
+  cudaStream_t st = r->solver ? r->solver->st : nullptr;
+  delete r;
+  if (st) cudaStreamSynchronize(st);
+}
+
+NativeReport resident_refine(Resident* r, std::vector<double>& rotation, std::vector<double>& translation,
+                             std::vector<double>& points, std::vector<double>& groups) {
+  CUDA_OK(cudaSetDevice(r->ctx->device));
+  r->linearized = false;
+  r->solver->restore_initial();
+  return r->solver->refine(rotation, translation, points, groups);
+}
+
+ResidentInfo resident_info(const Resident* r) {
+  const Solver<double>& s = *r->solver;
+  ResidentInfo info;
+  info.observations = (uint64_t)s.N;
+  info.points = (uint64_t)s.P;
+  info.cameras = (uint64_t)s.n.ncam;
+  info.dimension = (uint64_t)s.D;
+  info.iterative = s.direct ? 0 : 1;
+  info.mixed = s.mixed ? 1 : 0;
+  for (int p = 0; p < s.P; ++p) {
+    const int point_dim = s.n.fixed_points[p] ? 0 : 3;
+    for (uint64_t o = s.n.pt_off[p]; o < s.n.pt_off[p + 1]; ++o) {
+      const int c = (int)s.n.obs_cam[o];
+      int cam_dim = s.L.pose_dim[c];
+      if (s.n.self_cal) cam_dim += s.L.intr_dim[s.n.cam_group[c]];
+      info.jacobian_entries += 2 * (uint64_t)(cam_dim + point_dim);
+    }
+  }
+  info.tiles64 = (uint64_t)s.dT64.ntiles;
+  info.tiles32 = s.mixed ? (uint64_t)s.dT32.ntiles : 0;
+  info.record_bytes64 = sizeof(double) * s.d_rec.n;
+  info.record_bytes32 = sizeof(float) * s.d_rec32.n;
+  info.metadata_bytes64 = s.dT64.blob.n + sizeof(uint64_t) * s.dT64.tile_blob.n;
+  info.metadata_bytes32 = s.mixed ? s.dT32.blob.n + sizeof(uint64_t) * s.dT32.tile_blob.n : 0;
+  return info;
+}
+
+void resident_schur_product(Resident* r, double lambda, bool fp32, int stage, const double* x, double* y) {
+  CUDA_OK(cudaSetDevice(r->ctx->device));
+  Solver<double>& s = *r->solver;
+  if (s.direct) throw SolveFailure{2, "the plan's linear solver is direct; the tile product serves PCG plans"};
+  if (fp32 && !s.mixed) throw SolveFailure{1, "FP32 products need a mixed-precision plan"};
+  if (!r->linearized || r->lambda != lambda) {
+    s.restore_initial();
+    double scene = s.scene_scale_host();
+    Gauge g = s.gauge_for(s.cur, scene);
+    auto a = s.assemble(s.cur, g, s.opt.loss, lambda, false);
+    if (!a.valid) throw SolveFailure{4, "linearization is not valid"};
+    r->linearized = true;
+    r->lambda = lambda;
+  }
+  if (stage == 1)
+    s.matvec_tiles(x, nullptr, fp32);
+  else
+    s.matvec(x, y, lambda, nullptr, fp32);
+  s.check_launch();
+}
+
 void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOptions& options, double* residual,
                          double* sqrt_weight, double* point_jacobian, double* camera_jacobian) {
   CUDA_OK(cudaSetDevice(ctx->device));
@@ -2758,12 +2901,12 @@ void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOpt
   d_sw.alloc(std::max<size_t>(N, 1), s.st);
   LinOut<double> lo = s.lin();
   lo.sw = d_sw.p;
-  k_linearize<double><<<grid_for(s.P, 128), 128, 0, s.st>>>(s.view(), s.state(s.cur), g, options.loss, 0.0, lo);
+  OMVGBA_LAUNCH(k_linearize<double>, grid_for(s.P, 128), 128, 0, s.st, s.view(), s.state(s.cur), g, options.loss, 0.0, lo);
   s.check_launch();
   std::vector<double> rec(s.d_rec.n), rw(2 * N), sw(N);
-  CUDA_OK(cudaMemcpyAsync(rec.data(), s.d_rec.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.st));
-  CUDA_OK(cudaMemcpyAsync(rw.data(), s.d_rw.p, sizeof(double) * rw.size(), cudaMemcpyDeviceToHost, s.st));
-  CUDA_OK(cudaMemcpyAsync(sw.data(), d_sw.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(copy_async(rec.data(), s.d_rec.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(copy_async(rw.data(), s.d_rw.p, sizeof(double) * rw.size(), cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(copy_async(sw.data(), d_sw.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s.st));
   s.sync();
   // the kernel stores sqrt-weighted rows; divide the weight back out
   for (size_t o = 0; o < N; ++o) {
@@ -2791,12 +2934,12 @@ void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const L
   int D = s.D;
   *dimension = D;
   if (!x) return;
-  CUDA_OK(cudaMemcpyAsync(s.d_tmp.p, x, sizeof(double) * D, cudaMemcpyHostToDevice, s.st));
+  CUDA_OK(copy_async(s.d_tmp.p, x, sizeof(double) * D, cudaMemcpyHostToDevice, s.st));
   s.matvec(s.d_tmp.p, s.d_q.p, lambda);
-  k_dense_matvec<<<grid_for((size_t)D * 32, 256), 256, 0, s.st>>>(D, s.d_S.p, s.d_tmp.p, s.d_z.p);
+  OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, s.st, D, s.d_S.p, s.d_tmp.p, s.d_z.p);
   s.check_launch();
-  CUDA_OK(cudaMemcpyAsync(y_mv, s.d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
-  CUDA_OK(cudaMemcpyAsync(y_dense, s.d_z.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(copy_async(y_mv, s.d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
+  CUDA_OK(copy_async(y_dense, s.d_z.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
   s.sync();
   s.check_fault();
 }

@@ -49,6 +49,7 @@ struct LmOptions {
   int precision = 0;  // 0 FP64, 1 mixed
   int matvec = 0;     // 0 auto, 1 explicit, 2 implicit
   int dense_rank_limit = 2048;
+  void* stream = nullptr;  // cudaStream_t the solve runs on; null: the context's own stream
 };
 
 struct NativeReport {
@@ -84,6 +85,28 @@ void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOpt
 // Matrix-free S x versus the explicit dense S x at the first linearization (operator parity).
 void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const LmOptions& options, double lambda,
                              const double* x, double* y_mv, double* y_dense, int* dimension);
+
+// A lowered problem kept resident in device memory for repeated solves from its initial state.
+// The NativeProblem must outlive the Resident.
+struct Resident;
+struct ResidentInfo {
+  uint64_t observations = 0, points = 0, cameras = 0, dimension = 0;
+  uint64_t jacobian_entries = 0;  // sum over observations of 2 x (free camera dim + free point dim)
+  uint64_t tiles64 = 0, tiles32 = 0;
+  uint64_t record_bytes64 = 0, record_bytes32 = 0, metadata_bytes64 = 0, metadata_bytes32 = 0;
+  int iterative = 0, mixed = 0;
+};
+Resident* resident_create(Context* ctx, const NativeProblem& problem, const LmOptions& options);
+void resident_destroy(Resident* resident);
+NativeReport resident_refine(Resident* resident, std::vector<double>& rotation, std::vector<double>& translation,
+                             std::vector<double>& points, std::vector<double>& groups);
+ResidentInfo resident_info(const Resident* resident);
+// S_lambda x at the initial state's linearization; x and y are device pointers. stage 0: the
+// whole product; stage 1: the tile pass alone (y is not written).
+void resident_schur_product(Resident* resident, double lambda, bool fp32, int stage, const double* x, double* y);
+
+// Kernels launched and host<->device bytes copied by the calling thread so far.
+void telemetry_read(uint64_t* launches, uint64_t* h2d, uint64_t* d2h);
 
 // Residual norms of an input problem's observations with a world-frame state, for the Solution
 // metrics (solver.rs:1052-1131). active: per point flag. Returns false when a projection fails.

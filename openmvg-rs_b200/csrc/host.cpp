@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <set>
 #include <string>
@@ -624,6 +625,7 @@ LmOptions lm_options(const omvgba_problem& pr, const omvgba_config& cfg, const N
   o.pcg_max_iterations = cfg.pcg_max_iterations > 0 ? cfg.pcg_max_iterations : 600;
   o.precision = cfg.precision;
   o.matvec = cfg.matvec;
+  o.stream = cfg.stream;
   return o;
 }
 
@@ -1046,7 +1048,17 @@ void add_origin(omvgba_report& r, const omvgba_report& origin) {
   r.pcg_iteration_count += origin.pcg_iteration_count;
 }
 
-Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+// The part of the quarantine protocol before the first solve (quarantine.rs:34-96): points seen
+// fewer than twice or without parallax in the input are held out of the problem that is solved.
+struct Prepared {
+  Restricted first;
+  const omvgba_problem* working = nullptr;
+  std::vector<size_t> kept;
+  size_t quarantined = 0;
+  bool changes_scale = false;
+};
+
+void prepare_quarantine(const omvgba_problem& pr, const omvgba_config& cfg, Prepared& out) {
   validate_config(cfg);
   std::vector<uint64_t> counts(pr.point_count, 0);
   for (size_t o = 0; o < pr.observation_count; ++o) counts[pr.observation_point[o]]++;
@@ -1058,26 +1070,33 @@ Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgb
     if (weak[p] && !point_fixed(pr, p)) input_deg.insert(p);
   if (input_deg.size() == pr.point_count)
     fail(OMVGBA_UNSUPPORTED, "no point can be adjusted: every point is seen fewer than twice or without parallax");
-  Restricted first;
-  const omvgba_problem* working = &pr;
-  std::vector<size_t> kept(pr.point_count);
-  std::iota(kept.begin(), kept.end(), 0);
+  out.working = &pr;
+  out.kept.resize(pr.point_count);
+  std::iota(out.kept.begin(), out.kept.end(), 0);
   if (!input_deg.empty()) {
-    without_points(pr, nullptr, input_deg, first);
-    working = &first.view;
-    kept = first.kept;
+    without_points(pr, nullptr, input_deg, out.first);
+    out.working = &out.first.view;
+    out.kept = out.first.kept;
   }
-  size_t quarantined = input_deg.size();
-  bool changes_scale = false;
-  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) changes_scale = std::fabs(gauge_plan(pr).scale - 1.0) > 1e-9;
-  if (changes_scale && quarantined > 0)
+  out.quarantined = input_deg.size();
+  out.changes_scale = false;
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) out.changes_scale = std::fabs(gauge_plan(pr).scale - 1.0) > 1e-9;
+  if (out.changes_scale && out.quarantined > 0)
     fail(OMVGBA_UNSUPPORTED, "native BA cannot change its physical baseline while holding out points");
-  Result sol = solve_once(ctx, *working, cfg);
+}
+
+// The rest of the protocol after the first solve `sol` of prep.working: up to four re-solves
+// without the weak points of the previous solution, then the solution in the input's indexing.
+Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg, const Prepared& prep,
+                         Result sol) {
+  std::vector<size_t> kept = prep.kept;
+  size_t quarantined = prep.quarantined;
+  const bool changes_scale = prep.changes_scale;
   omvgba_config retry = cfg;
   retry.max_iterations = std::min<uint64_t>(cfg.max_iterations, 8);
   std::vector<Restricted> chain;
   chain.reserve(4);
-  const omvgba_problem* current = working;
+  const omvgba_problem* current = prep.working;
   bool have_origin = false;
   omvgba_report origin{};
   for (int round = 0; round < 4; ++round) {
@@ -1133,6 +1152,13 @@ Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgb
   return out;
 }
 
+Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  Prepared prep;
+  prepare_quarantine(pr, cfg, prep);
+  Result sol = solve_once(ctx, *prep.working, cfg);
+  return finish_quarantine(ctx, pr, cfg, prep, std::move(sol));
+}
+
 int write_error(omvgba_error* e, int code, const std::string& msg) {
   if (e) {
     e->code = code;
@@ -1150,6 +1176,55 @@ struct omvgba_context {
 };
 
 using namespace omvgba;
+
+struct omvgba_plan {
+  Context* ctx = nullptr;
+  const omvgba_problem* problem = nullptr;
+  omvgba_config config{};
+  Prepared prep;
+  Lowered lowered;
+  LmOptions options;
+  Resident* resident = nullptr;
+  ~omvgba_plan() { resident_destroy(resident); }
+};
+
+namespace {
+
+struct Telemetry {
+  uint64_t launches = 0, h2d = 0, d2h = 0;
+};
+
+Telemetry telemetry_now() {
+  Telemetry t;
+  telemetry_read(&t.launches, &t.h2d, &t.d2h);
+  return t;
+}
+
+void stamp_telemetry(omvgba_report& r, const Telemetry& before, std::chrono::steady_clock::time_point t0) {
+  const Telemetry after = telemetry_now();
+  r.kernel_launches = after.launches - before.launches;
+  r.h2d_bytes = after.h2d - before.h2d;
+  r.d2h_bytes = after.d2h - before.d2h;
+  r.solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void write_solution(const omvgba_problem& problem, const Result& r, omvgba_solution* solution) {
+  std::memcpy(solution->poses, r.poses.data(), sizeof(omvgba_pose) * problem.pose_count);
+  std::memcpy(solution->intrinsics, r.intrinsics.data(), sizeof(omvgba_intrinsic) * problem.intrinsic_count);
+  std::memcpy(solution->points, r.points.data(), sizeof(double) * 3 * problem.point_count);
+  if (solution->quarantined_points)
+    for (size_t i = 0; i < r.quarantined.size(); ++i) solution->quarantined_points[i] = r.quarantined[i];
+  solution->report = r.report;
+}
+
+void clear_error(omvgba_error* error) {
+  if (!error) return;
+  error->code = 0;
+  error->detail = -1;
+  error->message[0] = 0;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -1211,15 +1286,10 @@ int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, con
   auto t0 = std::chrono::steady_clock::now();
   try {
     validate_problem(*problem);
+    const Telemetry before = telemetry_now();
     Result r = solve_with_quarantine(context->ctx, *problem, *config);
-    std::memcpy(solution->poses, r.poses.data(), sizeof(omvgba_pose) * problem->pose_count);
-    std::memcpy(solution->intrinsics, r.intrinsics.data(), sizeof(omvgba_intrinsic) * problem->intrinsic_count);
-    std::memcpy(solution->points, r.points.data(), sizeof(double) * 3 * problem->point_count);
-    if (solution->quarantined_points)
-      for (size_t i = 0; i < r.quarantined.size(); ++i) solution->quarantined_points[i] = r.quarantined[i];
-    solution->report = r.report;
-    solution->report.solve_seconds =
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    write_solution(*problem, r, solution);
+    stamp_telemetry(solution->report, before, t0);
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {
     return write_error(error, f.code, f.message);
@@ -1266,5 +1336,94 @@ int32_t omvgba_debug_schur_product(omvgba_context* context, const omvgba_problem
     return write_error(error, f.code, f.message);
   }
 }
+
+int32_t omvgba_plan_create(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                           omvgba_plan** plan, omvgba_error* error) {
+  clear_error(error);
+  if (!context || !problem || !config || !plan) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  *plan = nullptr;
+  try {
+    validate_problem(*problem);
+    validate_config(*config);
+    std::unique_ptr<omvgba_plan> p(new omvgba_plan());
+    p->ctx = context->ctx;
+    p->problem = problem;
+    p->config = *config;
+    prepare_quarantine(*problem, p->config, p->prep);
+    p->lowered = lower(*p->prep.working);
+    p->options = lm_options(*p->prep.working, p->config, p->lowered.n);
+    p->resident = resident_create(p->ctx, p->lowered.n, p->options);
+    *plan = p.release();
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
+int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_error* error) {
+  clear_error(error);
+  if (!plan || !solution || !solution->poses || !solution->intrinsics || !solution->points)
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  auto t0 = std::chrono::steady_clock::now();
+  try {
+    const Telemetry before = telemetry_now();
+    const omvgba_problem& working = *plan->prep.working;
+    std::vector<double> rot, tr, pts, grp;
+    NativeReport nr = resident_refine(plan->resident, rot, tr, pts, grp);
+    Result first = raise(working, plan->lowered, rot, tr, pts, grp, nr, plan->options.iterative);
+    finish_solution(working, first);
+    canonicalize(working, first);
+    Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first));
+    write_solution(*plan->problem, r, solution);
+    stamp_telemetry(solution->report, before, t0);
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
+int32_t omvgba_plan_info_get(const omvgba_plan* plan, omvgba_plan_info* info, omvgba_error* error) {
+  clear_error(error);
+  if (!plan || !info) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  ResidentInfo r = resident_info(plan->resident);
+  std::memset(info, 0, sizeof(*info));
+  info->observation_count = r.observations;
+  info->point_count = r.points;
+  info->camera_count = r.cameras;
+  info->reduced_dimension = r.dimension;
+  info->jacobian_entries = r.jacobian_entries;
+  info->tile_count_fp64 = r.tiles64;
+  info->tile_count_fp32 = r.tiles32;
+  info->record_bytes_fp64 = r.record_bytes64;
+  info->record_bytes_fp32 = r.record_bytes32;
+  info->metadata_bytes_fp64 = r.metadata_bytes64;
+  info->metadata_bytes_fp32 = r.metadata_bytes32;
+  info->iterative = r.iterative;
+  info->mixed = r.mixed;
+  return OMVGBA_OK;
+}
+
+int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32, int32_t stage, const double* x,
+                                  double* y, omvgba_error* error) {
+  clear_error(error);
+  if (!plan || !x || (stage == 0 && !y)) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  if (stage != 0 && stage != 1) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0 or 1");
+  if (!(std::isfinite(lambda) && lambda >= 0.0))
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "lambda must be finite and non-negative");
+  try {
+    resident_schur_product(plan->resident, lambda, fp32 != 0, stage, x, y);
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
+void omvgba_plan_destroy(omvgba_plan* plan) { delete plan; }
 
 }  // extern "C"

@@ -43,6 +43,17 @@ def lib():
     L.omvgba_solve_batched.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(abi.Problem), C.POINTER(abi.Config),
                                        C.POINTER(abi.Solution), C.POINTER(abi.Error)]
     L.omvgba_solve_batched.restype = C.c_int32
+    L.omvgba_plan_create.argtypes = [C.c_void_p, C.POINTER(abi.Problem), C.POINTER(abi.Config),
+                                     C.POINTER(C.c_void_p), C.POINTER(abi.Error)]
+    L.omvgba_plan_create.restype = C.c_int32
+    L.omvgba_plan_solve.argtypes = [C.c_void_p, C.POINTER(abi.Solution), C.POINTER(abi.Error)]
+    L.omvgba_plan_solve.restype = C.c_int32
+    L.omvgba_plan_info_get.argtypes = [C.c_void_p, C.POINTER(abi.PlanInfo), C.POINTER(abi.Error)]
+    L.omvgba_plan_info_get.restype = C.c_int32
+    L.omvgba_plan_schur_product.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                            C.POINTER(abi.Error)]
+    L.omvgba_plan_schur_product.restype = C.c_int32
+    L.omvgba_plan_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
 

@@ -155,6 +155,9 @@ class Report(C.Structure):
         ("final_damping", C.c_double),
         ("solve_seconds", C.c_double),
         ("upload_seconds", C.c_double),
+        ("kernel_launches", C.c_uint64),
+        ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64),
     ]
 
 
@@ -250,3 +253,25 @@ class SolutionBuffers:
 
 def report_to_dict(r: Report) -> dict:
     return {name: getattr(r, name) for name, _ in Report._fields_}
+
+
+class PlanInfo(C.Structure):
+    """omvgba_plan_info."""
+    _fields_ = [
+        ("observation_count", C.c_uint64),
+        ("point_count", C.c_uint64),
+        ("camera_count", C.c_uint64),
+        ("reduced_dimension", C.c_uint64),
+        ("jacobian_entries", C.c_uint64),
+        ("tile_count_fp64", C.c_uint64),
+        ("tile_count_fp32", C.c_uint64),
+        ("record_bytes_fp64", C.c_uint64),
+        ("record_bytes_fp32", C.c_uint64),
+        ("metadata_bytes_fp64", C.c_uint64),
+        ("metadata_bytes_fp32", C.c_uint64),
+        ("iterative", C.c_int32),
+        ("mixed", C.c_int32),
+    ]
+
+    def to_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}

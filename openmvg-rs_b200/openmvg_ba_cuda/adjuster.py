@@ -72,10 +72,68 @@ class CudaBundleAdjuster:
         raise_for(code, err)
         return ym, yd
 
+    def plan(self, problem: BundleProblem, config: SolveConfig | None = None) -> "Plan":
+        """Prepare ``problem`` once (lowering, upload) for repeated solves from its initial state."""
+        return Plan(self, problem, config or SolveConfig())
+
     def close(self) -> None:
         if getattr(self, "_ctx", None):
             lib().omvgba_context_destroy(self._ctx)
             self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Plan:
+    """A problem resident in device memory: ``solve`` returns what ``CudaBundleAdjuster.solve``
+    returns, without the per-call lowering and upload. Keeps the marshalled problem alive."""
+
+    def __init__(self, adjuster: CudaBundleAdjuster, problem: BundleProblem, config: SolveConfig):
+        self._adjuster = adjuster
+        self._problem = problem
+        self._mp = abi.MarshalledProblem(problem)
+        self._cfg = config.to_struct()
+        self._out = abi.SolutionBuffers(problem)
+        handle = C.c_void_p()
+        err = abi.Error()
+        code = lib().omvgba_plan_create(adjuster._ctx, C.byref(self._mp.struct), C.byref(self._cfg),
+                                        C.byref(handle), C.byref(err))
+        raise_for(code, err)
+        self._plan = handle
+
+    def solve(self) -> Solution:
+        err = abi.Error()
+        code = lib().omvgba_plan_solve(self._plan, C.byref(self._out.struct), C.byref(err))
+        raise_for(code, err)
+        return Solution.from_buffers(self._out)
+
+    def info(self) -> dict:
+        info = abi.PlanInfo()
+        err = abi.Error()
+        raise_for(lib().omvgba_plan_info_get(self._plan, C.byref(info), C.byref(err)), err)
+        return info.to_dict()
+
+    def schur_product(self, x_ptr: int, y_ptr: int, damping: float, fp32: bool = False, stage: int = 0) -> None:
+        """y = S_lambda x on device pointers (stage 1: the tile pass alone), on the plan's stream."""
+        err = abi.Error()
+        code = lib().omvgba_plan_schur_product(self._plan, damping, int(fp32), stage, C.c_void_p(x_ptr),
+                                               C.c_void_p(y_ptr), C.byref(err))
+        raise_for(code, err)
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None):
+            lib().omvgba_plan_destroy(self._plan)
+            self._plan = None
 
     def __del__(self):
         try:

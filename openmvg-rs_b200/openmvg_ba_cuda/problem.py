@@ -188,6 +188,7 @@ class SolveConfig:
     pcg_relative_tolerance: float = 0.0
     pcg_max_iterations: int = 0
     device: int = 0
+    stream: int = 0  # cudaStream_t handle (e.g. torch.cuda.current_stream().cuda_stream); 0: the context's
 
     def with_(self, **kwargs) -> "SolveConfig":
         return dataclasses.replace(self, **kwargs)
@@ -206,7 +207,7 @@ class SolveConfig:
         c.pcg_relative_tolerance = self.pcg_relative_tolerance
         c.pcg_max_iterations = self.pcg_max_iterations
         c.device = self.device
-        c.stream = None
+        c.stream = self.stream or None
         return c
 
 

@@ -221,6 +221,9 @@ typedef struct omvgba_solution {
 /* One solver context per thread or stream: device workspaces, streams, no global state. */
 typedef struct omvgba_context omvgba_context;
 
+/* Number of CUDA devices visible to this process (0 when none or when the driver is missing). */
+int32_t omvgba_device_count(void);
+
 omvgba_context* omvgba_context_create(int32_t device, omvgba_error* error);
 void omvgba_context_destroy(omvgba_context* context);
 uint32_t omvgba_abi_version(void);

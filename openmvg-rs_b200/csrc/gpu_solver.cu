@@ -77,6 +77,15 @@ struct Context {
   size_t pinned_count = 0;
 };
 
+int device_count() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 Context* context_create(int device, std::string* error) {
   Context* c = new Context();
   c->device = device;

@@ -69,6 +69,7 @@ struct NativeReport {
 
 struct Context;  // device, stream, pinned scratch
 
+int device_count();
 Context* context_create(int device, std::string* error);
 void context_destroy(Context* ctx);
 

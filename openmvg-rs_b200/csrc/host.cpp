@@ -1254,6 +1254,8 @@ void omvgba_struct_sizes(uint64_t* out) {
   out[6] = sizeof(omvgba_solution);
 }
 
+int32_t omvgba_device_count(void) { return device_count(); }
+
 omvgba_context* omvgba_context_create(int32_t device, omvgba_error* error) {
   std::string msg;
   Context* c = context_create(device, &msg);

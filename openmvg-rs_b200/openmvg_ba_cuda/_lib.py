@@ -54,6 +54,17 @@ def lib():
                                             C.POINTER(abi.Error)]
     L.omvgba_plan_schur_product.restype = C.c_int32
     L.omvgba_plan_destroy.argtypes = [C.c_void_p]
+    L.omvgba_device_count.restype = C.c_int32
+    vp, u64 = C.c_void_p, C.c_uint64
+    L.omvgba_residual_forward_f32.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, C.POINTER(abi.Error)]
+    L.omvgba_residual_forward_f32.restype = C.c_int32
+    L.omvgba_residual_forward_f64.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, C.POINTER(abi.Error)]
+    L.omvgba_residual_forward_f64.restype = C.c_int32
+    L.omvgba_residual_vjp_f32.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, vp, vp, vp, vp, vp, u64,
+                                          C.POINTER(abi.Error)]
+    L.omvgba_residual_vjp_f32.restype = C.c_int32
+    L.omvgba_residual_vjp_workspace_bytes.argtypes = [u64, u64, u64]
+    L.omvgba_residual_vjp_workspace_bytes.restype = u64
     _lib = L
     return L
 
@@ -63,3 +74,7 @@ def struct_sizes() -> dict:
     lib().omvgba_struct_sizes(out)
     names = ["error", "pose", "intrinsic", "problem", "config", "report", "solution"]
     return dict(zip(names, list(out)))
+
+
+def device_count() -> int:
+    return int(lib().omvgba_device_count())

@@ -331,6 +331,26 @@ int32_t omvgba_residual_forward_f64(void* stream, uint64_t observation_count, co
                                     omvgba_error* error);
 
 /*
+ * omvgba_residual_vjp_f32 for callers that cannot allocate device memory: hosts whose GPU memory
+ * is reserved up front by another allocator, or loops that allow no driver allocation (nor the
+ * synchronisation a cudaMalloc / cudaFree may cause) after start-up. No counterpart in the
+ * reference. The scratch is a static device array of OMVGBA_RESIDUAL_STATIC_SCRATCH_BYTES that
+ * every GPU loading this library holds until exit; sizes whose omvgba_residual_vjp_workspace_bytes
+ * exceed it (about 440,000 points with 3,000 cameras) are rejected with OMVGBA_INVALID_ARGUMENT
+ * before any device work. It allocates nothing. The first call on a device (with that device
+ * current) resolves the array's device address, so make that first call before any stream capture.
+ * Runs on the current device; arguments and results as omvgba_residual_vjp_f32. All calls share the
+ * one array: calls that overlap on the GPU race, so order them on one stream.
+ */
+#define OMVGBA_RESIDUAL_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int32_t omvgba_residual_vjp_f32_static(void* stream, uint64_t observation_count, const uint32_t* camera_index,
+                                       const uint32_t* point_index, const float* pixel, uint64_t camera_count,
+                                       const float* rotvec, const float* translation, const float* intrinsics,
+                                       uint64_t point_count, const float* points, const float* grad_residual,
+                                       float* grad_rotvec, float* grad_translation, float* grad_intrinsics,
+                                       float* grad_points, omvgba_error* error);
+
+/*
  * Many independent problems (local-BA windows) solved together: one persistent launch per LM
  * phase over all windows, per-window convergence masks, graph-captured. Each window follows
  * omvgba_solve's contract; solutions[i] receives window i. No reference counterpart: the

@@ -63,6 +63,9 @@ def lib():
     L.omvgba_residual_vjp_f32.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, vp, vp, vp, vp, vp, u64,
                                           C.POINTER(abi.Error)]
     L.omvgba_residual_vjp_f32.restype = C.c_int32
+    L.omvgba_residual_vjp_f32_static.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, vp, vp, vp, vp,
+                                                 C.POINTER(abi.Error)]
+    L.omvgba_residual_vjp_f32_static.restype = C.c_int32
     L.omvgba_residual_vjp_workspace_bytes.argtypes = [u64, u64, u64]
     L.omvgba_residual_vjp_workspace_bytes.restype = u64
     _lib = L

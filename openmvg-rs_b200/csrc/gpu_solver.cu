@@ -1409,10 +1409,12 @@ struct TileSet {
   uint32_t nseg = 0;
 };
 
-// Tiles of whole points with at most `tile` observations (and points). For each tile a metadata
-// blob (layout in mv_tiles.cuh) holds per-observation parameter offsets, local point indices,
-// point ranges and the tile's entities (observation, segment) sorted by parameter block, whose
-// runs are the segments of the fused matvec.
+// Tiles of whole points with at most `tile` observations. A tile's observations are grouped by
+// camera into segments (ascending camera, observation order inside); each segment feeds the
+// camera's pose block and its intrinsic block. The metadata blob (layout in mv_tiles.cuh) holds the
+// per-observation segment and local point, the segment entity lists, the point ranges and the
+// segments' parameter offsets. blk_segs lists, per block, (segment << 2 | column code) in tile
+// order: the fixed order in which the product sums a block's partials.
 static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
   const std::vector<int>& ent_block = setup.ent_block;
   const int nblocks = (int)setup.blk_off.size();
@@ -1426,9 +1428,9 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
   std::vector<std::vector<uint32_t>> blk_segs(nblocks);
   uint32_t nseg_total = 0;
   size_t p = 0;
-  std::vector<std::pair<int, uint16_t>> ents;
-  std::vector<uint32_t> w0, w1, sg;
-  std::vector<uint16_t> lpt, poff, segb, ent;
+  std::vector<std::pair<uint32_t, uint16_t>> by_cam;
+  std::vector<uint16_t> oseg, lpt, pos, poff, segb;
+  std::vector<uint32_t> w0, w1;
   while (p < P) {
     size_t p0 = p;
     uint64_t o0 = n.pt_off[p];
@@ -1436,63 +1438,65 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
     uint64_t o1 = n.pt_off[p];
     if (o1 - o0 > (uint64_t)tile) throw SolveFailure{2, "a point track is longer than the matvec tile"};
     uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
-    w0.assign(nobs, 0);
-    w1.assign(nobs, 0);
     lpt.assign(nobs, 0);
+    oseg.assign(nobs, 0);
+    pos.assign(nobs, 0);
     poff.assign(npt + 1, 0);
     for (size_t q = p0; q < p; ++q) {
       poff[q - p0] = (uint16_t)(n.pt_off[q] - o0);
       for (uint64_t o = n.pt_off[q]; o < n.pt_off[q + 1]; ++o) lpt[o - o0] = (uint16_t)(q - p0);
     }
     poff[npt] = (uint16_t)nobs;
-    ents.clear();
-    for (uint64_t o = o0; o < o1; ++o) {
-      int c = n.obs_cam[o];
-      w0[o - o0] = (uint32_t)L.pose_off[c] | ((uint32_t)L.pose_dim[c] << 28);
-      if (n.self_cal) {
-        int g = n.cam_group[c];
-        w1[o - o0] = (uint32_t)L.intr_off[g] | ((uint32_t)L.intr_dim[g] << 28);
-      }
-      for (int sgm = 0; sgm < 2; ++sgm) {
-        int b = ent_block[2 * o + sgm];
-        if (b < 0) continue;
-        int col = sgm == 0 ? 0 : L.pose_dim[c];
-        int code = col == 0 ? 0 : (col == 5 ? 1 : 2);
-        ents.push_back({b, (uint16_t)((o - o0) | (code << 12))});
-      }
-    }
-    std::stable_sort(ents.begin(), ents.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    sg.clear();
+    by_cam.clear();
+    for (uint64_t o = o0; o < o1; ++o) by_cam.push_back({n.obs_cam[o], (uint16_t)(o - o0)});
+    std::stable_sort(by_cam.begin(), by_cam.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
     segb.clear();
-    ent.clear();
+    w0.clear();
+    w1.clear();
     size_t i = 0;
-    while (i < ents.size()) {
+    while (i < by_cam.size()) {
       size_t j = i;
-      while (j < ents.size() && ents[j].first == ents[i].first) ++j;
-      int b = ents[i].first;
-      blk_segs[b].push_back(nseg_total + (uint32_t)sg.size());
-      sg.push_back((uint32_t)setup.blk_off[b] | ((uint32_t)setup.blk_dim[b] << 28));
-      segb.push_back((uint16_t)ent.size());
-      for (size_t k = i; k < j; ++k) ent.push_back(ents[k].second);
+      while (j < by_cam.size() && by_cam[j].first == by_cam[i].first) ++j;
+      const int c = (int)by_cam[i].first;
+      const uint32_t s = (uint32_t)segb.size();
+      const uint64_t o_any = o0 + by_cam[i].second;
+      const int pose_b = ent_block[2 * o_any], intr_b = ent_block[2 * o_any + 1];
+      const int pd = L.pose_dim[c];
+      uint32_t iw = 0;
+      if (n.self_cal) {
+        const int g = n.cam_group[c];
+        iw = (uint32_t)L.intr_off[g] | ((uint32_t)L.intr_dim[g] << 28);
+      }
+      w0.push_back((uint32_t)L.pose_off[c] | ((uint32_t)pd << 28));
+      w1.push_back(iw);
+      segb.push_back((uint16_t)i);
+      for (size_t k = i; k < j; ++k) {
+        pos[by_cam[k].second] = (uint16_t)k;
+        oseg[by_cam[k].second] = (uint16_t)s;
+      }
+      const uint32_t sg = nseg_total + s;
+      if (sg >= (1u << 30)) throw SolveFailure{3, "matvec segment count exceeds 2^30"};
+      if (pose_b >= 0) blk_segs[pose_b].push_back(sg << 2);
+      if (intr_b >= 0) blk_segs[intr_b].push_back((sg << 2) | (uint32_t)(pd == 0 ? 0 : (pd == 5 ? 1 : 2)));
       i = j;
     }
-    uint32_t nseg = (uint32_t)sg.size();
-    segb.push_back((uint16_t)ent.size());
+    const uint32_t nseg = (uint32_t)segb.size();
+    segb.push_back((uint16_t)nobs);
     size_t off[7];
-    size_t bytes = blob_layout(nobs, npt, nseg, (uint32_t)ent.size(), off);
+    size_t bytes = blob_layout(nobs, npt, nseg, off);
+    if (bytes > mv_blob_max(tile)) throw SolveFailure{5, "matvec tile metadata exceeds its bound"};
     size_t base = S.blob.size();
     S.blob.resize(base + bytes, 0);
     unsigned char* B = S.blob.data() + base;
     uint32_t hdr[4] = {nobs, npt, nseg, nseg_total};
     std::memcpy(B, hdr, 16);
-    std::memcpy(B + off[0], w0.data(), 4 * (size_t)nobs);
-    std::memcpy(B + off[1], w1.data(), 4 * (size_t)nobs);
-    std::memcpy(B + off[2], lpt.data(), 2 * (size_t)nobs);
+    std::memcpy(B + off[0], oseg.data(), 2 * (size_t)nobs);
+    std::memcpy(B + off[1], lpt.data(), 2 * (size_t)nobs);
+    std::memcpy(B + off[2], pos.data(), 2 * (size_t)nobs);
     std::memcpy(B + off[3], poff.data(), 2 * (size_t)(npt + 1));
-    std::memcpy(B + off[4], sg.data(), 4 * (size_t)nseg);
-    std::memcpy(B + off[5], segb.data(), 2 * (size_t)(nseg + 1));
-    std::memcpy(B + off[6], ent.data(), 2 * ent.size());
-    if (bytes > mv_blob_max(tile)) throw SolveFailure{5, "matvec tile metadata exceeds its bound"};
+    std::memcpy(B + off[4], segb.data(), 2 * (size_t)(nseg + 1));
+    std::memcpy(B + off[5], w0.data(), 4 * (size_t)nseg);
+    std::memcpy(B + off[6], w1.data(), 4 * (size_t)nseg);
     size_t t = S.tile_obs.size();
     if ((t + 1) * (size_t)tile * kRec >= (1ull << 32)) throw SolveFailure{3, "record storage exceeds 2^32 elements"};
     for (uint64_t o = o0; o < o1; ++o) S.obs_rec[o] = (uint32_t)(t * (size_t)tile * kRec + (o - o0));
@@ -1694,7 +1698,7 @@ struct TileSetDev {
     std::vector<unsigned char> b = t.blob;
     b.resize(std::max<size_t>(b.size(), 16));
     blob.upload(b.data(), b.size(), st);
-    partial.alloc((size_t)6 * std::max<size_t>(1, t.nseg), st);
+    partial.alloc((size_t)kSegParams * std::max<size_t>(1, t.nseg), st);
     ntiles = (int)t.tile_obs.size() - 1;
   }
   MvTiles view(const int* blk_dim, const int* blk_off, int nblocks) const {
@@ -2153,19 +2157,21 @@ struct Solver {
     matvec_tiles(x, ctl, fp32);
     const TileSetDev& ts = fp32 ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
-    OMVGBA_LAUNCH(k_mv_tiles_finalize, grid_for((size_t)nb * 32, 256), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda, x, y, ctl);
+    OMVGBA_LAUNCH(k_mv_tiles_finalize, grid_for((size_t)nb * 32, 256), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda,
+                  x, y, ctl);
     check_launch();
   }
-  // The tile pass of the product alone: per-(segment, component) partials of the point coupling.
+  // The tile pass of the product alone: the per-(segment, parameter) partials.
   void matvec_tiles(const double* x, const PcgCtl* ctl, bool fp32) {
     const TileSetDev& ts = fp32 ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        OMVGBA_LAUNCH(k_mv_tiles<float>, ts.grid, 256, mv_smem_bytes<float>(), st, mt, d_rec32.p, d_vinv.p, x, ts.partial.p,
-                                                                        ctl, d_fault.p);
+        OMVGBA_LAUNCH(k_mv_tiles<float>, ts.grid, kMvThreads, mv_smem_bytes<float>(), st, mt, d_rec32.p, d_vinv.p, x,
+                      ts.partial.p, ctl, d_fault.p);
       else
-        OMVGBA_LAUNCH(k_mv_tiles<T>, ts.grid, 256, mv_smem_bytes<T>(), st, mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl, d_fault.p);
+        OMVGBA_LAUNCH(k_mv_tiles<T>, ts.grid, kMvThreads, mv_smem_bytes<T>(), st, mt, d_rec.p, d_vinv.p, x,
+                      ts.partial.p, ctl, d_fault.p);
     }
   }
   void check_fault() {

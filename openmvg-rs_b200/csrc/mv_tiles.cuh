@@ -1,19 +1,29 @@
-// mv_tiles.cuh — fused matrix-free reduced-camera-system product S x for the PCG hot loop.
+// mv_tiles.cuh — matrix-free reduced-camera-system product y = S_lambda x for the PCG loop.
 //
-// S x = sum_o Jc_o^T (e_o - Jp_o z_p)   with e_o = Jc_o x_o and z_p = Vhat_p^-1 sum_o Jp_o^T e_o,
-// plus lambda * diag * x in the finalize (retained/operator.rs:137-227 computes the same product
-// from cached Vhat^-1 W^T rows).
+// S x = sum_o Jc_o^T (e_o - Jp_o z_p) + lambda diag x, with e_o = Jc_o x and
+// z_p = Vhat_p^-1 sum_o Jp_o^T e_o (retained/operator.rs:137-227 computes the same product from
+// cached Vhat^-1 W^T rows).
 //
 // Layout: observations are point-major; a tile is a run of whole points with at most TILE
 // observations. Everything a tile needs is contiguous in HBM and 16 B aligned: its Jacobian
-// records, its points' damped inverses, and a metadata blob (per-observation column offsets,
-// local point indices, point ranges, block segments and their entities) built once per solve.
-// A persistent CTA walks tiles with two shared-memory stages: while it computes one tile, the
-// bulk async copies (cp.async.bulk, completion on one mbarrier per stage) stream the next, so
-// every Jacobian byte crosses HBM once per product and no thread waits on a dependent load.
-// Inside a tile: observation-parallel e_o, point-parallel z_p, observation-parallel f_o, and one
-// thread per (tile, parameter block) segment summing its entities in a fixed order into a partial.
-// The finalize sums each block's partials in tile order: the product is bitwise deterministic.
+// records (component-major, so a warp's shared-memory reads are conflict-free), its points'
+// damped inverses and a metadata blob built once per solve. A persistent CTA walks tiles with
+// two shared-memory stages filled by bulk asynchronous copies (cp.async.bulk, one mbarrier per
+// stage): every Jacobian byte crosses HBM once per product, and the next tile streams in while
+// the current one is computed.
+//
+// Per tile, with a (tile, camera) "segment" for each camera the tile's observations see:
+//   P0  x of each segment's pose and intrinsic parameters into shared memory (one gather per
+//       segment and parameter instead of one per observation);
+//   P1  thread per observation: e = Jc x, point terms Jp^T e;
+//   P2  four lanes per point (one per component of the track sum, in track order, exchanged by
+//       shuffles): z = Vhat^-1 (sum of the point terms);
+//   P3  thread per observation: f = e - Jp z and its camera terms Jc^T f, stored in segment order;
+//   P4  thread per (segment, parameter): the sum of the segment's contiguous run of camera terms,
+//       in observation order, written as the segment's partial.
+// The finalize kernel sums each block's partials in tile order (one warp per block, fixed lane
+// assignment and shuffle tree) and adds lambda diag x. No sum depends on scheduling, so the
+// product is bitwise reproducible run to run.
 #pragma once
 
 #include <cstdint>
@@ -22,55 +32,54 @@ namespace omvgba {
 
 struct MvTiles {
   int ntiles;
-  const uint32_t* tile_obs;    // ntiles + 1: first observation (record) of each tile
-  const uint32_t* tile_pt;     // ntiles + 1: first point of each tile
-  const uint64_t* tile_blob;   // ntiles + 1: byte offset of each tile's metadata blob
-  const unsigned char* blob;   // metadata blobs
+  const uint32_t* tile_obs;     // ntiles + 1: first observation of each tile
+  const uint32_t* tile_pt;      // ntiles + 1: first point of each tile
+  const uint64_t* tile_blob;    // ntiles + 1: byte offset of each tile's metadata blob
+  const unsigned char* blob;    // metadata blobs
+  int nblocks;
   const int* blk_dim;
   const int* blk_off;
   const uint32_t* blk_seg_off;  // nblocks + 1
-  const uint32_t* blk_segs;     // segments of each block in tile order
-  int nblocks;
+  const uint32_t* blk_segs;     // per block: (segment << 2) | column code, in tile order
 };
 
-// Metadata blob of a tile (every section starts on a 16 B boundary):
+// Metadata blob of a tile (header, then 16 B aligned sections):
 //   u32 header[4] = {nobs, npt, nseg, seg_base}
-//   u32 w0[nobs]      pose parameter offset | pose dim << 28
-//   u32 w1[nobs]      intrinsic parameter offset | intrinsic dim << 28
-//   u16 lpt[nobs]     local point of the observation
+//   u16 oseg[nobs]    segment of each observation
+//   u16 lpt[nobs]     local point of each observation
+//   u16 pos[nobs]     position of each observation in segment order
 //   u16 poff[npt+1]   local observation range of each point
-//   u32 sg[nseg]      block parameter offset | block dim << 28
-//   u16 segb[nseg+1]  entity range of each segment
-//   u16 ent[nent]     local observation | column code << 12 (0: column 0, 1: 5, 2: 6)
+//   u16 segb[nseg+1]  range of each segment in ent
+//   u32 w0[nseg]      pose parameter offset | pose dim << 28
+//   u32 w1[nseg]      intrinsic parameter offset | intrinsic dim << 28
 struct BlobView {
   uint32_t nobs, npt, nseg, seg_base;
+  const uint16_t* oseg;
+  const uint16_t* lpt;
+  const uint16_t* pos;
+  const uint16_t* poff;
+  const uint16_t* segb;
   const uint32_t* w0;
   const uint32_t* w1;
-  const uint16_t* lpt;
-  const uint16_t* poff;
-  const uint32_t* sg;
-  const uint16_t* segb;
-  const uint16_t* ent;
 };
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 // Section offsets of a blob with the given counts; returns the total (16 B multiple) size.
-__host__ __device__ __forceinline__ size_t blob_layout(uint32_t nobs, uint32_t npt, uint32_t nseg, uint32_t nent,
-                                                      size_t off[7]) {
+__host__ __device__ __forceinline__ size_t blob_layout(uint32_t nobs, uint32_t npt, uint32_t nseg, size_t off[7]) {
   size_t o = 16;
   off[0] = o;
-  o = align16(o + 4 * (size_t)nobs);
+  o = align16(o + 2 * (size_t)nobs);
   off[1] = o;
-  o = align16(o + 4 * (size_t)nobs);
+  o = align16(o + 2 * (size_t)nobs);
   off[2] = o;
   o = align16(o + 2 * (size_t)nobs);
   off[3] = o;
   o = align16(o + 2 * (size_t)(npt + 1));
   off[4] = o;
-  o = align16(o + 4 * (size_t)nseg);
-  off[5] = o;
   o = align16(o + 2 * (size_t)(nseg + 1));
+  off[5] = o;
+  o = align16(o + 4 * (size_t)nseg);
   off[6] = o;
-  o = align16(o + 2 * (size_t)nent);
+  o = align16(o + 4 * (size_t)nseg);
   return o;
 }
 __device__ __forceinline__ BlobView blob_view(const unsigned char* b) {
@@ -81,14 +90,14 @@ __device__ __forceinline__ BlobView blob_view(const unsigned char* b) {
   v.nseg = h[2];
   v.seg_base = h[3];
   size_t off[7];
-  blob_layout(v.nobs, v.npt, v.nseg, 0, off);
-  v.w0 = reinterpret_cast<const uint32_t*>(b + off[0]);
-  v.w1 = reinterpret_cast<const uint32_t*>(b + off[1]);
-  v.lpt = reinterpret_cast<const uint16_t*>(b + off[2]);
+  blob_layout(v.nobs, v.npt, v.nseg, off);
+  v.oseg = reinterpret_cast<const uint16_t*>(b + off[0]);
+  v.lpt = reinterpret_cast<const uint16_t*>(b + off[1]);
+  v.pos = reinterpret_cast<const uint16_t*>(b + off[2]);
   v.poff = reinterpret_cast<const uint16_t*>(b + off[3]);
-  v.sg = reinterpret_cast<const uint32_t*>(b + off[4]);
-  v.segb = reinterpret_cast<const uint16_t*>(b + off[5]);
-  v.ent = reinterpret_cast<const uint16_t*>(b + off[6]);
+  v.segb = reinterpret_cast<const uint16_t*>(b + off[4]);
+  v.w0 = reinterpret_cast<const uint32_t*>(b + off[5]);
+  v.w1 = reinterpret_cast<const uint32_t*>(b + off[6]);
   return v;
 }
 
@@ -132,25 +141,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+constexpr int kMvThreads = 256;
+constexpr int kSegParams = 9;  // pose (<= 6) then intrinsic (<= 3) parameters of a segment
+
 template <typename T>
 __host__ __device__ constexpr int mv_tile_obs() {
   return sizeof(T) == 4 ? 256 : 128;
 }
-// Upper bound of a tile's metadata blob (nseg <= 2 TILE, nent <= 2 TILE, npt <= TILE).
-__host__ __device__ constexpr size_t mv_blob_max(int tile) { return 16 + 28 * (size_t)tile + 8 * 16 + 16; }
+// Upper bound of a tile's metadata blob (npt <= nobs <= TILE, nseg <= TILE).
+__host__ __device__ constexpr size_t mv_blob_max(int tile) { return 18 * (size_t)tile + 144; }
 template <typename T>
 __host__ __device__ constexpr size_t mv_stage_bytes() {
   return align16(sizeof(T) * (size_t)mv_tile_obs<T>() * kRec) + align16(mv_blob_max(mv_tile_obs<T>())) +
          48 * (size_t)mv_tile_obs<T>();
 }
-// Records of a tile live at rec + t * TILE * kRec; a partial tile's unused slots are zero.
+// Row stride of the per-observation term arrays: one element of padding, so the 9 lanes that
+// read the 9 parameter rows of one observation hit 9 different banks.
+template <typename T>
+__host__ __device__ constexpr int mv_term_stride() {
+  return mv_tile_obs<T>() + 1;
+}
+// Two stages, then x per segment (9 TILE), the point / camera terms (9 padded rows) and z (3 TILE).
 template <typename T>
 __host__ __device__ constexpr size_t mv_smem_bytes() {
-  // two stages, plus e/f (2 per observation), point terms (3 per observation), z (3 per point)
-  return 2 * mv_stage_bytes<T>() + sizeof(T) * (size_t)mv_tile_obs<T>() * 8;
+  return 2 * mv_stage_bytes<T>() +
+         sizeof(T) * ((size_t)mv_tile_obs<T>() * 12 + (size_t)kSegParams * mv_term_stride<T>() + 4);
 }
 
-__device__ __forceinline__ int colcode_to_col(int code) { return code == 0 ? 0 : (code == 1 ? 5 : 6); }
+__host__ __device__ __forceinline__ int colcode_to_col(int code) { return code == 0 ? 0 : (code == 1 ? 5 : 6); }
 
 template <typename T>
 __device__ __forceinline__ void mv_issue_tile(const MvTiles& mt, int t, const T* rec, const double* vinv,
@@ -172,17 +190,16 @@ __device__ __forceinline__ void mv_issue_tile(const MvTiles& mt, int t, const T*
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_mv_tiles(MvTiles mt, const T* __restrict__ rec,
-                                                  const double* __restrict__ vinv, const double* __restrict__ x,
-                                                  double* __restrict__ partial, const PcgCtl* ctl, int* fault) {
+__global__ void __launch_bounds__(kMvThreads, 2)
+    k_mv_tiles(MvTiles mt, const T* __restrict__ rec, const double* __restrict__ vinv, const double* __restrict__ x,
+               double* __restrict__ partial, const PcgCtl* ctl, int* fault) {
   if (pcg_stopped(ctl)) return;
   constexpr int TILE = mv_tile_obs<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char* stage_ptr[2] = {smem_raw, smem_raw + mv_stage_bytes<T>()};
-  T* f0 = reinterpret_cast<T*>(smem_raw + 2 * mv_stage_bytes<T>());
-  T* f1 = f0 + TILE;
-  T* tb = f1 + TILE;
-  T* zz = tb + 3 * TILE;
+  constexpr int TS = mv_term_stride<T>();
+  T* xs = reinterpret_cast<T*>(smem_raw + 2 * mv_stage_bytes<T>());  // kSegParams per segment
+  T* zz = xs + kSegParams * TILE;                                    // z, component-major
+  T* terms = zz + 3 * TILE;                                          // point terms, then camera terms
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int abort_flag;
   const int tid = threadIdx.x;
@@ -194,7 +211,9 @@ __global__ void __launch_bounds__(256) k_mv_tiles(MvTiles mt, const T* __restric
   }
   __syncthreads();
   int t = blockIdx.x;
-  if (t < mt.ntiles && tid == 0) mv_issue_tile<T>(mt, t, rec, vinv, stage_ptr[0], &bar[0]);
+  if (t < mt.ntiles && tid == 0) {
+    mv_issue_tile<T>(mt, t, rec, vinv, smem_raw, &bar[0]);
+  }
   for (int k = 0; t < mt.ntiles; t += gridDim.x, ++k) {
     const int stage = k & 1;
     const int tn = t + gridDim.x;
@@ -202,7 +221,7 @@ __global__ void __launch_bounds__(256) k_mv_tiles(MvTiles mt, const T* __restric
     if (tid == 0 && tn < mt.ntiles) {
       // the other stage was last read by the previous tile; order those reads before the async writes
       fence_proxy_async();
-      mv_issue_tile<T>(mt, tn, rec, vinv, stage_ptr[stage ^ 1], &bar[stage ^ 1]);
+      mv_issue_tile<T>(mt, tn, rec, vinv, smem_raw + (stage ^ 1) * mv_stage_bytes<T>(), &bar[stage ^ 1]);
       issued_next = true;
     }
     // every thread observes the phase completion (acquire of the async-proxy writes), bounded
@@ -215,98 +234,126 @@ __global__ void __launch_bounds__(256) k_mv_tiles(MvTiles mt, const T* __restric
       }
       return;
     }
-    const T* cur = reinterpret_cast<const T*>(stage_ptr[stage]);
-    const BlobView bv = blob_view(stage_ptr[stage] + align16(sizeof(T) * (size_t)TILE * kRec));
-    const double* vi_s = reinterpret_cast<const double*>(stage_ptr[stage] + align16(sizeof(T) * (size_t)TILE * kRec) +
-                                                         align16(mv_blob_max(TILE)));
+    const unsigned char* sp = smem_raw + stage * mv_stage_bytes<T>();
+    const T* cur = reinterpret_cast<const T*>(sp);
+    const BlobView bv = blob_view(sp + align16(sizeof(T) * (size_t)TILE * kRec));
+    const double* vi_s =
+        reinterpret_cast<const double*>(sp + align16(sizeof(T) * (size_t)TILE * kRec) + align16(mv_blob_max(TILE)));
     const uint32_t nobs = bv.nobs, npt = bv.npt, nseg = bv.nseg;
-    // e_o = Jc_o x_o and the point terms Jp_o^T e_o (component k of observation i at k * TILE + i)
-    for (uint32_t i = tid; i < nobs; i += blockDim.x) {
-      const T* r = cur + i;
-      const uint32_t w0 = bv.w0[i], w1 = bv.w1[i];
-      const int pd = (int)(w0 >> 28), id = (int)(w1 >> 28);
-      const uint32_t po = w0 & 0x0FFFFFFFu, io = w1 & 0x0FFFFFFFu;
-      T e0 = 0, e1 = 0;
-      for (int c = 0; c < pd; ++c) {
-        T xv = (T)__ldg(x + po + c);
-        e0 += r[c * TILE] * xv;
-        e1 += r[(9 + c) * TILE] * xv;
-      }
-      for (int c = 0; c < id; ++c) {
-        T xv = (T)__ldg(x + io + c);
-        e0 += r[(pd + c) * TILE] * xv;
-        e1 += r[(9 + pd + c) * TILE] * xv;
-      }
-      f0[i] = e0;
-      f1[i] = e1;
-      const T* jp = r + kJp * TILE;
-      tb[3 * i] = jp[0] * e0 + jp[3 * TILE] * e1;
-      tb[3 * i + 1] = jp[TILE] * e0 + jp[4 * TILE] * e1;
-      tb[3 * i + 2] = jp[2 * TILE] * e0 + jp[5 * TILE] * e1;
+    // P0: x of each segment's parameters (zero beyond the segment's dimensions)
+    for (uint32_t w = tid; w < kSegParams * nseg; w += blockDim.x) {
+      const uint32_t s = w / kSegParams, c = w - kSegParams * s;
+      const uint32_t w0 = bv.w0[s], w1 = bv.w1[s];
+      const uint32_t pd = w0 >> 28, id = w1 >> 28;
+      double v = 0.0;
+      if (c < pd)
+        v = __ldg(x + (w0 & 0x0FFFFFFFu) + c);
+      else if (c - pd < id)
+        v = __ldg(x + (w1 & 0x0FFFFFFFu) + (c - pd));
+      xs[w] = (T)v;
     }
     __syncthreads();
-    // z_p = Vhat_p^-1 sum_o Jp_o^T e_o (sequential per point: fixed order)
-    for (uint32_t lp = tid; lp < npt; lp += blockDim.x) {
-      const uint32_t a = bv.poff[lp], b = bv.poff[lp + 1];
-      T b0 = 0, b1 = 0, b2 = 0;
-      for (uint32_t i = a; i < b; ++i) {
-        b0 += tb[3 * i];
-        b1 += tb[3 * i + 1];
-        b2 += tb[3 * i + 2];
+    // P1: e = Jc x and the point terms Jp^T e (record component k of observation i at k TILE + i)
+    // The observation's Jacobian stays in registers until P3.
+    T e0 = 0, e1 = 0, jc[18], jp[6];
+    if ((uint32_t)tid < nobs) {
+      const T* r = cur + tid;
+      const T* xv = xs + kSegParams * bv.oseg[tid];
+#pragma unroll
+      for (int c = 0; c < 18; ++c) jc[c] = r[c * TILE];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) jp[c] = r[(kJp + c) * TILE];
+#pragma unroll
+      for (int c = 0; c < 9; c += 2) {  // two accumulators per row: shorter dependency chains
+        const T xa = xv[c];
+        e0 += jc[c] * xa;
+        e1 += jc[9 + c] * xa;
       }
-      const double* vi = vi_s + 6 * (size_t)lp;
-      const T v0 = (T)vi[0], v1 = (T)vi[1], v2 = (T)vi[2], v3 = (T)vi[3], v4 = (T)vi[4], v5 = (T)vi[5];
-      zz[3 * lp] = v0 * b0 + v1 * b1 + v3 * b2;
-      zz[3 * lp + 1] = v1 * b0 + v2 * b1 + v4 * b2;
-      zz[3 * lp + 2] = v3 * b0 + v4 * b1 + v5 * b2;
+      T e0b = 0, e1b = 0;
+#pragma unroll
+      for (int c = 1; c < 9; c += 2) {
+        const T xb = xv[c];
+        e0b += jc[c] * xb;
+        e1b += jc[9 + c] * xb;
+      }
+      e0 += e0b;
+      e1 += e1b;
+      terms[tid] = jp[0] * e0 + jp[3] * e1;
+      terms[TS + tid] = jp[1] * e0 + jp[4] * e1;
+      terms[2 * TS + tid] = jp[2] * e0 + jp[5] * e1;
     }
     __syncthreads();
-    // f_o = e_o - Jp_o z_p
-    for (uint32_t i = tid; i < nobs; i += blockDim.x) {
-      const int lp = bv.lpt[i];
-      const T* jp = cur + kJp * TILE + i;
-      const T z0 = zz[3 * lp], z1 = zz[3 * lp + 1], z2 = zz[3 * lp + 2];
-      f0[i] -= jp[0] * z0 + jp[TILE] * z1 + jp[2 * TILE] * z2;
-      f1[i] -= jp[3 * TILE] * z0 + jp[4 * TILE] * z1 + jp[5 * TILE] * z2;
+    // P2: z_p = Vhat_p^-1 sum_o Jp_o^T e_o; lanes 4q..4q+2 of a warp sum the three components of
+    // point q's track (in track order), lane 4q+3 idles; the sums are exchanged by shuffles.
+    for (uint32_t base = 0; base < npt; base += blockDim.x >> 2) {
+      const uint32_t lp = base + (tid >> 2), k = tid & 3;
+      const bool active = lp < npt && k < 3;
+      T bk = 0;
+      if (active) {
+        const T* row = terms + k * TS;
+        for (uint32_t i = bv.poff[lp]; i < bv.poff[lp + 1]; ++i) bk += row[i];
+      }
+      const int lead = (tid & 31) & ~3;
+      const T b0 = __shfl_sync(0xffffffffu, bk, lead), b1 = __shfl_sync(0xffffffffu, bk, lead + 1),
+              b2 = __shfl_sync(0xffffffffu, bk, lead + 2);
+      if (active) {
+        // row k of the packed symmetric inverse (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
+        const double* vi = vi_s + 6 * (size_t)lp;
+        const int i0 = k == 0 ? 0 : (k == 1 ? 1 : 3), i1 = k == 0 ? 1 : (k == 1 ? 2 : 4), i2 = k == 0 ? 3 : (k == 1 ? 4 : 5);
+        zz[k * TILE + lp] = (T)vi[i0] * b0 + (T)vi[i1] * b1 + (T)vi[i2] * b2;
+      }
     }
     __syncthreads();
-    // one thread per (segment, component): partial_c = sum_e (Jc_e^T f_o)_c in entity order
-    for (uint32_t w = tid; w < 6 * nseg; w += blockDim.x) {
-      const uint32_t s = w / 6, c = w - 6 * s;
-      const int d = (int)(bv.sg[s] >> 28);
-      if ((int)c >= d) continue;
+    // P3: f = e - Jp z and the camera terms Jc^T f (overwrite the point terms, read in P2 only)
+    if ((uint32_t)tid < nobs) {
+      const uint32_t lp = bv.lpt[tid];
+      const T z0 = zz[lp], z1 = zz[TILE + lp], z2 = zz[2 * TILE + lp];
+      const T f0 = e0 - (jp[0] * z0 + jp[1] * z1 + jp[2] * z2);
+      const T f1 = e1 - (jp[3] * z0 + jp[4] * z1 + jp[5] * z2);
+      const uint32_t q = bv.pos[tid];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) terms[c * TS + q] = jc[c] * f0 + jc[9 + c] * f1;
+    }
+    __syncthreads();
+    // P4: per (segment, parameter) sum of the segment's run of camera terms in observation order
+    for (uint32_t w = tid; w < kSegParams * nseg; w += blockDim.x) {
+      const uint32_t s = w / kSegParams, c = w - kSegParams * s;
+      if (c >= (bv.w0[s] >> 28) + (bv.w1[s] >> 28)) continue;
       T acc = 0;
-      for (uint32_t j = bv.segb[s]; j < bv.segb[s + 1]; ++j) {
-        const uint16_t e = bv.ent[j];
-        const int li = e & 0x0fff, col = colcode_to_col(e >> 12);
-        acc += cur[(col + c) * TILE + li] * f0[li] + cur[(9 + col + c) * TILE + li] * f1[li];
-      }
-      partial[6 * (size_t)(bv.seg_base + s) + c] = (double)acc;
+      const T* col = terms + c * TS;
+      for (uint32_t j = bv.segb[s]; j < bv.segb[s + 1]; ++j) acc += col[j];
+      partial[(size_t)kSegParams * (bv.seg_base + s) + c] = (double)acc;
     }
     __syncthreads();
   }
 }
 
-// y_b = sum over the block's segments + lambda * diag_b * x_b; one warp per block, lane l sums
-// segments l, l+32, ... in tile order, then a fixed shuffle tree: deterministic.
-__global__ void k_mv_tiles_finalize(MvTiles mt, const double* partial, const double* diag, double lambda,
-                                    const double* x, double* y, const PcgCtl* ctl) {
+// y_b = sum of block b's segment partials (tile order) + lambda diag_b x_b: one warp per block,
+// lane l sums entries l, l + 32, ... in order, then a fixed shuffle tree.
+__global__ void k_mv_tiles_finalize(MvTiles mt, const double* __restrict__ partial, const double* __restrict__ diag,
+                                    double lambda, const double* __restrict__ x, double* __restrict__ y,
+                                    const PcgCtl* ctl) {
   if (pcg_stopped(ctl)) return;
-  int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
+  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (b >= mt.nblocks) return;
-  int o = mt.blk_off[b], d = mt.blk_dim[b];
+  const int o = mt.blk_off[b], d = mt.blk_dim[b];
+  const uint32_t i0 = mt.blk_seg_off[b], i1 = mt.blk_seg_off[b + 1];
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t i = mt.blk_seg_off[b] + lane; i < mt.blk_seg_off[b + 1]; i += 32) {
-    const double* pp = partial + 6 * (size_t)mt.blk_segs[i];
+  for (uint32_t i = i0 + lane; i < i1; i += 32) {
+    const uint32_t e = mt.blk_segs[i];
+    const double* pp = partial + (size_t)kSegParams * (e >> 2) + colcode_to_col((int)(e & 3u));
 #pragma unroll
     for (int c = 0; c < 6; ++c)
       if (c < d) acc[c] += pp[c];
   }
 #pragma unroll
   for (int c = 0; c < 6; ++c) acc[c] = warp_sum(acc[c]);  // full sums land in lane 0
-  if (lane == 0)
-    for (int c = 0; c < d; ++c) y[o + c] = acc[c] + lambda * diag[o + c] * x[o + c];
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      if (c < d) y[o + c] = acc[c] + lambda * diag[o + c] * x[o + c];
+  }
 }
 
 }  // namespace omvgba

@@ -1402,46 +1402,54 @@ struct Setup {
 // Tiles of the fused matvec for one record precision (host tables).
 struct TileSet {
   int tile = 0;
-  std::vector<uint32_t> tile_obs, tile_pt, blk_seg_off, blk_segs;
-  std::vector<uint32_t> obs_rec;  // element index of each observation's record component 0
-  std::vector<uint64_t> tile_blob;
-  std::vector<unsigned char> blob;
-  uint32_t nseg = 0;
+  std::vector<uint32_t> tile_hdr;  // 4 per tile: observations, points, segments, first point
+  std::vector<unsigned char> slots;
+  std::vector<uint32_t> blk_part;  // nblocks + 1
+  std::vector<uint32_t> obs_rec;   // element index of each observation's record component 0
 };
 
 // Tiles of whole points with at most `tile` observations. A tile's observations are grouped by
 // camera into segments (ascending camera, observation order inside); each segment feeds the
-// camera's pose block and its intrinsic block. The metadata blob (layout in mv_tiles.cuh) holds the
-// per-observation segment and local point, the segment entity lists, the point ranges and the
-// segments' parameter offsets. blk_segs lists, per block, (segment << 2 | column code) in tile
-// order: the fixed order in which the product sums a block's partials.
+// camera's pose block and its intrinsic block. Each block owns a contiguous partial region with one
+// dim-wide row per segment that feeds it, in tile order: the fixed order in which the product sums
+// a block's partials. The tile's metadata slot (layout in mv_tiles.cuh) holds the per-observation
+// segment, local point and segment-order position, the point ranges, and per segment its parameter
+// offsets and the rows of its partials.
 static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
   const std::vector<int>& ent_block = setup.ent_block;
   const int nblocks = (int)setup.blk_off.size();
+  const size_t slot_bytes = MvSlot::bytes(tile);
   S.tile = tile;
   size_t P = n.points.size() / 3;
-  S.tile_obs.clear();
-  S.tile_pt.clear();
-  S.tile_blob.clear();
-  S.blob.clear();
+  S.tile_hdr.clear();
+  S.slots.clear();
   S.obs_rec.assign(n.obs_cam.size(), 0);
-  std::vector<std::vector<uint32_t>> blk_segs(nblocks);
-  uint32_t nseg_total = 0;
+  struct SegRef {
+    uint32_t tile, s;
+    int bp, bi;
+  };
+  std::vector<SegRef> segs;
+  std::vector<uint32_t> blk_count(nblocks, 0);
   size_t p = 0;
   std::vector<std::pair<uint32_t, uint16_t>> by_cam;
-  std::vector<uint16_t> oseg, lpt, pos, poff, segb;
-  std::vector<uint32_t> w0, w1;
   while (p < P) {
     size_t p0 = p;
     uint64_t o0 = n.pt_off[p];
     while (p < P && p - p0 < (size_t)tile && (n.pt_off[p + 1] - o0 <= (uint64_t)tile || p == p0)) ++p;
     uint64_t o1 = n.pt_off[p];
     if (o1 - o0 > (uint64_t)tile) throw SolveFailure{2, "a point track is longer than the matvec tile"};
-    uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
-    lpt.assign(nobs, 0);
-    oseg.assign(nobs, 0);
-    pos.assign(nobs, 0);
-    poff.assign(npt + 1, 0);
+    const uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
+    const size_t t = S.tile_hdr.size() / 4;
+    if ((t + 1) * (size_t)tile * kRec >= (1ull << 32)) throw SolveFailure{3, "record storage exceeds 2^32 elements"};
+    S.slots.resize((t + 1) * slot_bytes, 0);
+    unsigned char* B = S.slots.data() + t * slot_bytes;
+    uint32_t* w0 = reinterpret_cast<uint32_t*>(B + MvSlot::w0(tile));
+    uint32_t* w1 = reinterpret_cast<uint32_t*>(B + MvSlot::w1(tile));
+    uint16_t* segb = reinterpret_cast<uint16_t*>(B + MvSlot::segb(tile));
+    uint16_t* oseg = reinterpret_cast<uint16_t*>(B + MvSlot::oseg(tile));
+    uint16_t* lpt = reinterpret_cast<uint16_t*>(B + MvSlot::lpt(tile));
+    uint16_t* pos = reinterpret_cast<uint16_t*>(B + MvSlot::pos(tile));
+    uint16_t* poff = reinterpret_cast<uint16_t*>(B + MvSlot::poff(tile));
     for (size_t q = p0; q < p; ++q) {
       poff[q - p0] = (uint16_t)(n.pt_off[q] - o0);
       for (uint64_t o = n.pt_off[q]; o < n.pt_off[q + 1]; ++o) lpt[o - o0] = (uint16_t)(q - p0);
@@ -1450,72 +1458,55 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
     by_cam.clear();
     for (uint64_t o = o0; o < o1; ++o) by_cam.push_back({n.obs_cam[o], (uint16_t)(o - o0)});
     std::stable_sort(by_cam.begin(), by_cam.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    segb.clear();
-    w0.clear();
-    w1.clear();
+    uint32_t nseg = 0;
     size_t i = 0;
     while (i < by_cam.size()) {
       size_t j = i;
       while (j < by_cam.size() && by_cam[j].first == by_cam[i].first) ++j;
       const int c = (int)by_cam[i].first;
-      const uint32_t s = (uint32_t)segb.size();
       const uint64_t o_any = o0 + by_cam[i].second;
       const int pose_b = ent_block[2 * o_any], intr_b = ent_block[2 * o_any + 1];
-      const int pd = L.pose_dim[c];
       uint32_t iw = 0;
       if (n.self_cal) {
         const int g = n.cam_group[c];
         iw = (uint32_t)L.intr_off[g] | ((uint32_t)L.intr_dim[g] << 28);
       }
-      w0.push_back((uint32_t)L.pose_off[c] | ((uint32_t)pd << 28));
-      w1.push_back(iw);
-      segb.push_back((uint16_t)i);
+      w0[nseg] = (uint32_t)L.pose_off[c] | ((uint32_t)L.pose_dim[c] << 28);
+      w1[nseg] = iw;
+      segb[nseg] = (uint16_t)i;
       for (size_t k = i; k < j; ++k) {
         pos[by_cam[k].second] = (uint16_t)k;
-        oseg[by_cam[k].second] = (uint16_t)s;
+        oseg[by_cam[k].second] = (uint16_t)nseg;
       }
-      const uint32_t sg = nseg_total + s;
-      if (sg >= (1u << 30)) throw SolveFailure{3, "matvec segment count exceeds 2^30"};
-      if (pose_b >= 0) blk_segs[pose_b].push_back(sg << 2);
-      if (intr_b >= 0) blk_segs[intr_b].push_back((sg << 2) | (uint32_t)(pd == 0 ? 0 : (pd == 5 ? 1 : 2)));
+      segs.push_back({(uint32_t)t, nseg, pose_b, intr_b});
+      if (pose_b >= 0) blk_count[pose_b]++;
+      if (intr_b >= 0) blk_count[intr_b]++;
+      ++nseg;
       i = j;
     }
-    const uint32_t nseg = (uint32_t)segb.size();
-    segb.push_back((uint16_t)nobs);
-    size_t off[7];
-    size_t bytes = blob_layout(nobs, npt, nseg, off);
-    if (bytes > mv_blob_max(tile)) throw SolveFailure{5, "matvec tile metadata exceeds its bound"};
-    size_t base = S.blob.size();
-    S.blob.resize(base + bytes, 0);
-    unsigned char* B = S.blob.data() + base;
-    uint32_t hdr[4] = {nobs, npt, nseg, nseg_total};
-    std::memcpy(B, hdr, 16);
-    std::memcpy(B + off[0], oseg.data(), 2 * (size_t)nobs);
-    std::memcpy(B + off[1], lpt.data(), 2 * (size_t)nobs);
-    std::memcpy(B + off[2], pos.data(), 2 * (size_t)nobs);
-    std::memcpy(B + off[3], poff.data(), 2 * (size_t)(npt + 1));
-    std::memcpy(B + off[4], segb.data(), 2 * (size_t)(nseg + 1));
-    std::memcpy(B + off[5], w0.data(), 4 * (size_t)nseg);
-    std::memcpy(B + off[6], w1.data(), 4 * (size_t)nseg);
-    size_t t = S.tile_obs.size();
-    if ((t + 1) * (size_t)tile * kRec >= (1ull << 32)) throw SolveFailure{3, "record storage exceeds 2^32 elements"};
+    segb[nseg] = (uint16_t)nobs;
     for (uint64_t o = o0; o < o1; ++o) S.obs_rec[o] = (uint32_t)(t * (size_t)tile * kRec + (o - o0));
-    S.tile_obs.push_back((uint32_t)o0);
-    S.tile_pt.push_back((uint32_t)p0);
-    S.tile_blob.push_back(base);
-    nseg_total += nseg;
+    S.tile_hdr.insert(S.tile_hdr.end(), {nobs, npt, nseg, (uint32_t)p0});
   }
-  S.tile_obs.push_back((uint32_t)n.pt_off[P]);
-  S.tile_pt.push_back((uint32_t)P);
-  S.tile_blob.push_back(S.blob.size());
-  S.nseg = nseg_total;
-  S.blk_seg_off.assign(nblocks + 1, 0);
-  S.blk_segs.clear();
+  // partial regions: block b's rows follow the blocks before it; segment rows in tile order
+  S.blk_part.assign(nblocks + 1, 0);
+  uint64_t total = 0;
   for (int b = 0; b < nblocks; ++b) {
-    S.blk_seg_off[b] = (uint32_t)S.blk_segs.size();
-    S.blk_segs.insert(S.blk_segs.end(), blk_segs[b].begin(), blk_segs[b].end());
+    S.blk_part[b] = (uint32_t)total;
+    total += (uint64_t)blk_count[b] * (uint64_t)setup.blk_dim[b];
   }
-  S.blk_seg_off[nblocks] = (uint32_t)S.blk_segs.size();
+  if (total >= kNoPartial) throw SolveFailure{3, "matvec partial storage exceeds 2^32 elements"};
+  S.blk_part[nblocks] = (uint32_t)total;
+  std::vector<uint32_t> next(nblocks, 0);
+  for (const SegRef& sr : segs) {
+    unsigned char* B = S.slots.data() + sr.tile * slot_bytes;
+    uint32_t* dpose = reinterpret_cast<uint32_t*>(B + MvSlot::dpose(tile));
+    uint32_t* dintr = reinterpret_cast<uint32_t*>(B + MvSlot::dintr(tile));
+    dpose[sr.s] = kNoPartial;
+    dintr[sr.s] = kNoPartial;
+    if (sr.bp >= 0) dpose[sr.s] = S.blk_part[sr.bp] + next[sr.bp]++ * (uint32_t)setup.blk_dim[sr.bp];
+    if (sr.bi >= 0) dintr[sr.s] = S.blk_part[sr.bi] + next[sr.bi]++ * (uint32_t)setup.blk_dim[sr.bi];
+  }
 }
 
 static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_pairs, Setup& S) {
@@ -1678,41 +1669,36 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
 
 // Device copy of a TileSet plus the fused-matvec launch shape.
 struct TileSetDev {
-  DBuf<uint32_t> tile_obs, tile_pt, blk_seg_off, blk_segs, obs_rec;
-  DBuf<uint64_t> tile_blob;
-  DBuf<unsigned char> blob;
+  DBuf<uint32_t> tile_hdr, blk_part, obs_rec;
+  DBuf<unsigned char> slots;
   DBuf<double> partial;
-  int ntiles = 0, grid = 1;
+  int ntiles = 0;
   void upload(const TileSet& t, cudaStream_t st) {
     auto up = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) {
       std::vector<uint32_t> x = v;
-      if (x.empty()) x.push_back(0);
+      if (x.empty()) x.assign(4, 0);
       b.upload(x.data(), x.size(), st);
     };
-    up(tile_obs, t.tile_obs);
-    up(tile_pt, t.tile_pt);
-    up(blk_seg_off, t.blk_seg_off);
-    up(blk_segs, t.blk_segs);
+    up(tile_hdr, t.tile_hdr);
+    up(blk_part, t.blk_part);
     up(obs_rec, t.obs_rec);
-    tile_blob.upload(t.tile_blob.data(), t.tile_blob.size(), st);
-    std::vector<unsigned char> b = t.blob;
+    std::vector<unsigned char> b = t.slots;
     b.resize(std::max<size_t>(b.size(), 16));
-    blob.upload(b.data(), b.size(), st);
-    partial.alloc((size_t)kSegParams * std::max<size_t>(1, t.nseg), st);
-    ntiles = (int)t.tile_obs.size() - 1;
+    slots.upload(b.data(), b.size(), st);
+    partial.alloc(std::max<size_t>(1, t.blk_part.empty() ? 1 : t.blk_part.back()), st);
+    ntiles = (int)(t.tile_hdr.size() / 4);
   }
+  int prefetch_ahead = 0;
   MvTiles view(const int* blk_dim, const int* blk_off, int nblocks) const {
     MvTiles m;
+    m.prefetch_ahead = prefetch_ahead;
     m.ntiles = ntiles;
-    m.tile_obs = tile_obs.p;
-    m.tile_pt = tile_pt.p;
-    m.tile_blob = tile_blob.p;
-    m.blob = blob.p;
+    m.tile_hdr = reinterpret_cast<const uint4*>(tile_hdr.p);
+    m.slots = slots.p;
+    m.nblocks = nblocks;
     m.blk_dim = blk_dim;
     m.blk_off = blk_off;
-    m.blk_seg_off = blk_seg_off.p;
-    m.blk_segs = blk_segs.p;
-    m.nblocks = nblocks;
+    m.blk_part = blk_part.p;
     return m;
   }
 };
@@ -1962,14 +1948,13 @@ struct Solver {
     d_fault.alloc(1, st);
     d_fault.zero();
     {
-      int sms = 148;
+      // one resident wave of product CTAs: how far ahead each CTA prefetches into L2
+      int sms = 148, per64 = 1, per32 = 1;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-      dT64.grid = std::max(1, std::min(dT64.ntiles, 2 * sms));
-      dT32.grid = std::max(1, std::min(dT32.ntiles, 2 * sms));
-      CUDA_OK(cudaFuncSetAttribute(k_mv_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)mv_smem_bytes<float>()));
-      CUDA_OK(cudaFuncSetAttribute(k_mv_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)mv_smem_bytes<T>()));
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_mv_tiles<T>, mv_tile_obs<T>(), 0));
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_mv_tiles<float>, mv_tile_obs<float>(), 0));
+      dT64.prefetch_ahead = per64 * sms;
+      dT32.prefetch_ahead = per32 * sms;
     }
     d_scalars.alloc(16, st);
     d_ctl.alloc((sizeof(PcgCtl) + sizeof(double) - 1) / sizeof(double), st);
@@ -2167,11 +2152,10 @@ struct Solver {
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        OMVGBA_LAUNCH(k_mv_tiles<float>, ts.grid, kMvThreads, mv_smem_bytes<float>(), st, mt, d_rec32.p, d_vinv.p, x,
-                      ts.partial.p, ctl, d_fault.p);
+        OMVGBA_LAUNCH(k_mv_tiles<float>, mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
+                      ts.partial.p, ctl);
       else
-        OMVGBA_LAUNCH(k_mv_tiles<T>, ts.grid, kMvThreads, mv_smem_bytes<T>(), st, mt, d_rec.p, d_vinv.p, x,
-                      ts.partial.p, ctl, d_fault.p);
+        OMVGBA_LAUNCH(k_mv_tiles<T>, mt.ntiles, mv_tile_obs<T>(), 0, st, mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl);
     }
   }
   void check_fault() {
@@ -2879,8 +2863,8 @@ ResidentInfo resident_info(const Resident* r) {
   info.tiles32 = s.mixed ? (uint64_t)s.dT32.ntiles : 0;
   info.record_bytes64 = sizeof(double) * s.d_rec.n;
   info.record_bytes32 = sizeof(float) * s.d_rec32.n;
-  info.metadata_bytes64 = s.dT64.blob.n + sizeof(uint64_t) * s.dT64.tile_blob.n;
-  info.metadata_bytes32 = s.mixed ? s.dT32.blob.n + sizeof(uint64_t) * s.dT32.tile_blob.n : 0;
+  info.metadata_bytes64 = s.dT64.slots.n + sizeof(uint32_t) * s.dT64.tile_hdr.n;
+  info.metadata_bytes32 = s.mixed ? s.dT32.slots.n + sizeof(uint32_t) * s.dT32.tile_hdr.n : 0;
   return info;
 }
 

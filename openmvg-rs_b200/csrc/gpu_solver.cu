@@ -864,109 +864,150 @@ __global__ void k_dense_matvec(int D, const double* S, const double* x, double* 
 // ----------------------------------------------------------------------------------------------
 enum PcgStatus : int { kRunning = 0, kCheckResidual = 1, kRejected = 2, kExhausted = 3 };
 struct PcgCtl {
-  double n0, rho, alpha, beta, curv, rr, rz, ratio, tol;
+  // rho_slot: r.z of the current residual, in one of two slots: an iteration reads slot p and its
+  // direction kernel writes slot p ^ 1, so no CTA reads a value another CTA of the same kernel writes.
+  double n0, rho_slot[2], alpha, beta, curv, rr, rz, ratio, tol;
   int status, terms, max_it, pad;
 };
 
 __device__ __forceinline__ bool pcg_stopped(const PcgCtl* ctl) { return ctl && ctl->status != kRunning; }
 
-// curvature = d.q, alpha = rho / curvature
-__global__ void __launch_bounds__(1024) k_pcg_alpha(int n, const double* d, const double* q, PcgCtl* ctl) {
-  if (ctl->status != kRunning) return;
-  __shared__ double sh[32];
-  int tid = threadIdx.x;
+// Sum of v[0..n) by one warp in a fixed order (lane-strided partial sums, then a shuffle tree); the
+// result is valid in lane 0 and identical in every CTA that evaluates it.
+__device__ __forceinline__ double warp_fixed_sum(const double* __restrict__ v, int n, int lane) {
   double acc = 0.0;
-  for (int i = tid; i < n; i += blockDim.x) acc += d[i] * q[i];
-  acc = warp_sum(acc);
-  if ((tid & 31) == 0) sh[tid >> 5] = acc;
-  __syncthreads();
-  if (tid == 0) {
-    double curv = 0.0;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w) curv += sh[w];
-    ctl->curv = curv;
-    int it = ctl->terms + 1;
-    if (!(isfinite(curv) && curv > 0.0)) {
-      ctl->terms = it - 1;
-      ctl->status = kRejected;
-      return;
-    }
-    double alpha = ctl->rho / curv;
-    if (!isfinite(alpha)) {
-      ctl->terms = it - 1;
-      ctl->status = kRejected;
-      return;
-    }
-    ctl->alpha = alpha;
-  }
+  for (int i = lane; i < n; i += 32) acc += v[i];
+  return warp_sum(acc);
 }
 
-__global__ void k_pcg_update(int n, const double* d, const double* q, double* x, double* r, const PcgCtl* ctl) {
+// PCG iteration, part 1, after the product q = S d (sparse/pcg.rs:23-119). Every CTA sums the
+// finalize's per-CTA curvature terms in the same order, so all agree on alpha; a curvature <= 0
+// or a non-finite alpha rejects. Thread per block: x += alpha d, r -= alpha q, z = M^-1 r with the
+// Jacobi-scaled Cholesky factor, and the block's |r|^2 and r.z, reduced per CTA in a fixed order.
+__global__ void __launch_bounds__(128) k_pcg_update_precond(BlockTables bt, const double* __restrict__ factor,
+                                                            const double* __restrict__ dq_part, int ndq,
+                                                            const double* __restrict__ d, const double* __restrict__ q,
+                                                            double* x, double* r, double* z, double* rr_part,
+                                                            double* rz_part, int slot, PcgCtl* ctl) {
   if (ctl->status != kRunning) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double alpha = ctl->alpha;
-  if (i < n) {
-    x[i] += alpha * d[i];
-    r[i] -= alpha * q[i];
-  }
-}
-
-// ratio = |r| / n0, next rho = r.z, beta = next rho / rho
-__global__ void __launch_bounds__(1024) k_pcg_beta(int n, const double* r, const double* z, PcgCtl* ctl) {
-  if (ctl->status != kRunning) return;
-  __shared__ double s1[32], s2[32];
-  int tid = threadIdx.x;
-  double a = 0.0, b = 0.0;
-  for (int i = tid; i < n; i += blockDim.x) {
-    a += r[i] * r[i];
-    b += r[i] * z[i];
-  }
-  a = warp_sum(a);
-  b = warp_sum(b);
-  if ((tid & 31) == 0) {
-    s1[tid >> 5] = a;
-    s2[tid >> 5] = b;
+  __shared__ double s_alpha;
+  __shared__ int s_go;
+  __shared__ double s1[4], s2[4];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (warp == 0) {
+    const double curv = warp_fixed_sum(dq_part, ndq, lane);
+    if (lane == 0) {
+      s_go = 0;
+      double alpha = 0.0;
+      if (isfinite(curv) && curv > 0.0) {
+        alpha = ctl->rho_slot[slot] / curv;
+        if (isfinite(alpha)) s_go = 1;
+      }
+      s_alpha = alpha;
+      if (blockIdx.x == 0) {
+        ctl->curv = curv;
+        if (s_go)
+          ctl->alpha = alpha;
+        else
+          ctl->status = kRejected;
+      }
+    }
   }
   __syncthreads();
+  if (!s_go) return;
+  const double alpha = s_alpha;
+  double rr = 0.0, rz = 0.0;
+  const int b = blockIdx.x * blockDim.x + tid;
+  if (b < bt.nblocks) {
+    const int dim = bt.blk_dim[b], o = bt.blk_off[b];
+    const double* F = factor + 42 * (size_t)b;
+    double rv[6], sv[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+      if (i < dim) {
+        x[o + i] += alpha * d[o + i];
+        rv[i] = r[o + i] - alpha * q[o + i];
+        r[o + i] = rv[i];
+      }
+    for (int i = 0; i < dim; ++i) {
+      double v = rv[i] / F[36 + i];
+      for (int k = 0; k < i; ++k) v -= F[6 * i + k] * sv[k];
+      sv[i] = v / F[6 * i + i];
+    }
+    for (int i = dim - 1; i >= 0; --i) {
+      double v = sv[i];
+      for (int k = i + 1; k < dim; ++k) v -= F[6 * k + i] * sv[k];
+      sv[i] = v / F[6 * i + i];
+    }
+    for (int i = 0; i < dim; ++i) {
+      const double zi = sv[i] / F[36 + i];
+      z[o + i] = zi;
+      rr += rv[i] * rv[i];
+      rz += rv[i] * zi;
+    }
+  }
+  rr = warp_sum(rr);
+  rz = warp_sum(rz);
+  if (lane == 0) {
+    s1[warp] = rr;
+    s2[warp] = rz;
+  }
+  __syncthreads();
   if (tid == 0) {
-    double rr = 0.0, rz = 0.0;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
-      rr += s1[w];
-      rz += s2[w];
-    }
-    int it = ctl->terms + 1;
-    ctl->terms = it;
-    ctl->rr = rr;
-    ctl->rz = rz;
-    double ratio = sqrt(rr) / ctl->n0;
-    ctl->ratio = ratio;
-    if (!isfinite(ratio)) {
-      ctl->status = kRejected;
-      return;
-    }
-    if (ratio <= ctl->tol) {
-      ctl->status = kCheckResidual;
-      return;
-    }
-    if (!(isfinite(rz) && rz > 0.0)) {
-      ctl->status = kRejected;
-      return;
-    }
-    double beta = rz / ctl->rho;
-    if (!isfinite(beta)) {
-      ctl->status = kRejected;
-      return;
-    }
-    ctl->beta = beta;
-    ctl->rho = rz;
-    if (it >= ctl->max_it) ctl->status = kExhausted;
+    rr_part[blockIdx.x] = (s1[0] + s1[1]) + (s1[2] + s1[3]);
+    rz_part[blockIdx.x] = (s2[0] + s2[1]) + (s2[2] + s2[3]);
   }
 }
 
-__global__ void k_pcg_direction(int n, const double* z, double* d, const PcgCtl* ctl) {
-  // runs after k_pcg_beta; on exhaustion the reference still forms the next direction, harmlessly
+// PCG iteration, part 2: every CTA sums the per-CTA |r|^2 and r.z in the same order and takes the
+// same decision: the recursive residual ratio at or below the tolerance hands over to the host's
+// true-residual check; r.z <= 0 or a non-finite value rejects; otherwise beta = r.z / rho and
+// d = z + beta d (also at the iteration limit, which ends the loop after this direction).
+__global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const double* __restrict__ rz_part,
+                                int nparts, const double* __restrict__ z, double* d, int slot, PcgCtl* ctl) {
   if (ctl->status != kRunning && ctl->status != kExhausted) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) d[i] = z[i] + ctl->beta * d[i];
+  __shared__ double s_beta;
+  __shared__ int s_go;
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid < 32) {
+    const double rr = warp_fixed_sum(rr_part, nparts, lane);
+    const double rz = warp_fixed_sum(rz_part, nparts, lane);
+    if (lane == 0) {
+      const double ratio = sqrt(rr) / ctl->n0;
+      int status = kRunning;
+      double beta = 0.0;
+      if (!isfinite(ratio)) {
+        status = kRejected;
+      } else if (ratio <= ctl->tol) {
+        status = kCheckResidual;
+      } else if (!(isfinite(rz) && rz > 0.0)) {
+        status = kRejected;
+      } else {
+        beta = rz / ctl->rho_slot[slot];
+        if (!isfinite(beta)) status = kRejected;
+      }
+      s_go = status == kRunning;
+      s_beta = beta;
+      if (blockIdx.x == 0) {  // only CTA 0 writes the control block
+        const int it = ctl->terms + 1;
+        ctl->terms = it;
+        ctl->rr = rr;
+        ctl->rz = rz;
+        ctl->ratio = ratio;
+        if (status == kRunning) {
+          ctl->beta = beta;
+          ctl->rho_slot[slot ^ 1] = rz;
+          if (it >= ctl->max_it) status = kExhausted;
+        }
+        ctl->status = status;
+      }
+    }
+  }
+  __syncthreads();
+  if (!s_go) return;
+  const double beta = s_beta;
+  const int i = blockIdx.x * blockDim.x + tid;
+  if (i < n) d[i] = z[i] + beta * d[i];
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -1742,7 +1783,7 @@ struct Solver {
   DBuf<double> d_S, d_Lf;
   DBuf<int> d_status;
   // PCG vectors
-  DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e;
+  DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
   DBuf<int> d_fail;
 
   DBuf<int> d_fault;
@@ -1944,6 +1985,9 @@ struct Solver {
     d_status.alloc(4, st);
     for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp, &d_rhs, &d_r64, &d_e}) b->alloc(std::max(1, D), st);
     d_factor.alloc((size_t)42 * std::max(1, nb), st);
+    d_dq.alloc(std::max(1, nb), st);
+    d_rr_part.alloc(std::max(1, grid_for(nb, 128)), st);
+    d_rz_part.alloc(std::max(1, grid_for(nb, 128)), st);
     d_fail.alloc(std::max(1, nb), st);
     d_fault.alloc(1, st);
     d_fault.zero();
@@ -2138,12 +2182,15 @@ struct Solver {
 
   // y = S_lambda x (implicit, matrix-free); ctl: optional PCG control for graph-launched iterations
   // fp32: use the FP32 record copy (mixed precision inner solves)
-  void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false) {
+  int mv_finalize_ctas() const { return std::max(1, grid_for((size_t)nb * 32, 256)); }
+  // xy: optional per-finalize-CTA sums of x_b . y_b over the CTA's blocks (the PCG curvature terms)
+  void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false,
+              double* xy = nullptr) {
     matvec_tiles(x, ctl, fp32);
     const TileSetDev& ts = fp32 ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
-    OMVGBA_LAUNCH(k_mv_tiles_finalize, grid_for((size_t)nb * 32, 256), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda,
-                  x, y, ctl);
+    OMVGBA_LAUNCH(k_mv_tiles_finalize, mv_finalize_ctas(), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda, x, y, xy,
+                  ctl);
     check_launch();
   }
   // The tile pass of the product alone: the per-(segment, parameter) partials.
@@ -2232,7 +2279,7 @@ struct Solver {
     if (max_it == 0) return res;
     PcgCtl ctl{};
     ctl.n0 = n0;
-    ctl.rho = rho;
+    ctl.rho_slot[0] = rho;
     ctl.tol = tol;
     ctl.status = kRunning;
     ctl.terms = 0;
@@ -2243,12 +2290,15 @@ struct Solver {
     cudaGraphExec_t exec;
     const uint64_t launches_before = tl_telemetry.launches;
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    matvec(d_dir.p, d_q.p, lambda, dctl, fp32);
-    OMVGBA_LAUNCH(k_pcg_alpha, 1, 1024, 0, st, D, d_dir.p, d_q.p, dctl);
-    OMVGBA_LAUNCH(k_pcg_update, grid_for(D, 256), 256, 0, st, D, d_dir.p, d_q.p, x, d_r.p, dctl);
-    precond(d_r.p, d_z.p, dctl);
-    OMVGBA_LAUNCH(k_pcg_beta, 1, 1024, 0, st, D, d_r.p, d_z.p, dctl);
-    OMVGBA_LAUNCH(k_pcg_direction, grid_for(D, 256), 256, 0, st, D, d_z.p, d_dir.p, dctl);
+    // two iterations per graph: the even one reads rho slot 0, the odd one slot 1
+    for (int slot = 0; slot < 2; ++slot) {
+      matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p);
+      const int nupd = grid_for(nb, 128);
+      OMVGBA_LAUNCH(k_pcg_update_precond, nupd, 128, 0, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
+                    d_dir.p, d_q.p, x, d_r.p, d_z.p, d_rr_part.p, d_rz_part.p, slot, dctl);
+      OMVGBA_LAUNCH(k_pcg_direction, grid_for(D, 256), 256, 0, st, D, d_rr_part.p, d_rz_part.p, nupd, d_z.p,
+                    d_dir.p, slot, dctl);
+    }
     CUDA_OK(cudaStreamEndCapture(st, &graph));
     const uint64_t kernels_per_graph = tl_telemetry.launches - launches_before;  // counted at capture
     tl_telemetry.launches = launches_before;
@@ -2267,8 +2317,8 @@ struct Solver {
       check_launch();
     };
     for (;;) {
-      for (int k = 0; k < kPoll; ++k) CUDA_OK(cudaGraphLaunch(exec, st));
-      tl_telemetry.launches += kPoll * kernels_per_graph;
+      for (int k = 0; k < kPoll / 2; ++k) CUDA_OK(cudaGraphLaunch(exec, st));  // two iterations per graph
+      tl_telemetry.launches += (kPoll / 2) * kernels_per_graph;
       launches += kPoll;
       CUDA_OK(copy_async(&ctl, dctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
       sync();
@@ -2310,7 +2360,7 @@ struct Solver {
         return res;
       }
       if ((uint64_t)ctl.terms >= max_it) break;
-      ctl.rho = nrho;
+      ctl.rho_slot[0] = nrho;
       ctl.status = kRunning;
       CUDA_OK(copy_async(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
     }

@@ -225,29 +225,48 @@ __global__ void __launch_bounds__(mv_tile_obs<T>(), 4)
 // y_b = sum of block b's partials (its segments in tile order) + lambda diag_b x_b: one warp per
 // block; lane l sums segments l, l + 32, ... of the block's contiguous region in order, then a
 // fixed shuffle tree. A block no observation touches has an empty region: y_b = lambda diag_b x_b.
-__global__ void k_mv_tiles_finalize(MvTiles mt, const double* __restrict__ partial, const double* __restrict__ diag,
-                                    double lambda, const double* __restrict__ x, double* __restrict__ y,
-                                    const PcgCtl* ctl) {
+// With xy non-null, xy[CTA] = sum over the CTA's blocks, in block order, of x_b . y_b (the PCG
+// curvature terms).
+__global__ void __launch_bounds__(256) k_mv_tiles_finalize(MvTiles mt, const double* __restrict__ partial,
+                                                           const double* __restrict__ diag, double lambda,
+                                                           const double* __restrict__ x, double* __restrict__ y,
+                                                           double* __restrict__ xy, const PcgCtl* ctl) {
   if (pcg_stopped(ctl)) return;
-  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= mt.nblocks) return;
-  const int o = mt.blk_off[b], d = mt.blk_dim[b];
-  const uint32_t a0 = mt.blk_part[b], a1 = mt.blk_part[b + 1];
-  const uint32_t nseg = d > 0 ? (a1 - a0) / (uint32_t)d : 0u;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t j = lane; j < nseg; j += 32) {
-    const double* pp = partial + a0 + (size_t)j * d;
+  __shared__ double s_dot[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 8 + warp;
+  double dot = 0.0;
+  if (b < mt.nblocks) {
+    const int o = mt.blk_off[b], d = mt.blk_dim[b];
+    const uint32_t a0 = mt.blk_part[b], a1 = mt.blk_part[b + 1];
+    const uint32_t nseg = d > 0 ? (a1 - a0) / (uint32_t)d : 0u;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t j = lane; j < nseg; j += 32) {
+      const double* pp = partial + a0 + (size_t)j * d;
 #pragma unroll
-    for (int c = 0; c < 6; ++c)
-      if (c < d) acc[c] += pp[c];
+      for (int c = 0; c < 6; ++c)
+        if (c < d) acc[c] += pp[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] = warp_sum(acc[c]);  // full sums land in lane 0
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+        if (c < d) {
+          const double v = acc[c] + lambda * diag[o + c] * x[o + c];
+          y[o + c] = v;
+          dot += x[o + c] * v;
+        }
+    }
   }
-#pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = warp_sum(acc[c]);  // full sums land in lane 0
-  if (lane == 0) {
-#pragma unroll
-    for (int c = 0; c < 6; ++c)
-      if (c < d) y[o + c] = acc[c] + lambda * diag[o + c] * x[o + c];
+  if (xy) {
+    if (lane == 0) s_dot[warp] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += s_dot[w];
+      xy[blockIdx.x] = t;
+    }
   }
 }
 

@@ -38,16 +38,28 @@ METRIC = "BA time-to-converge (s) & LM iters/s, mixed vs FP64 GPU, same final co
 UNIT = "LM iterations/s"
 L2_BYTES = 126 * 1024 * 1024
 FLUSH_BYTES = 512 * 1024 * 1024
-WORKLOAD = ("plane500: 500 cameras with per-camera (f, k1, k2) over a 100x100 ground plane, 200k points, "
-            "geometric tracks mean ~6 (1,184,956 observations at seed 11), noise 0.5 px, 5% outliers, "
-            "Huber 1 px, 50 LM iterations, block-Jacobi PCG tolerance 1e-6")
+# Workloads: plane500 is the headline (the single large problem of the benchmark's configuration
+# list); plane3000 is the 12M-observation global-refinement problem, run on request.
+WORKLOADS = {
+    "plane500": dict(
+        kwargs=dict(cameras=500, points=200_000, mean_track=6.5, extent=100.0),
+        text=("plane500: 500 cameras with per-camera (f, k1, k2) over a 100x100 ground plane, 200k points, "
+              "geometric tracks mean ~6 (1,184,956 observations at seed 11), noise 0.5 px, 5% outliers, "
+              "Huber 1 px, block-Jacobi PCG tolerance 1e-6")),
+    "plane3000": dict(
+        kwargs=dict(cameras=3000, points=2_000_000, mean_track=6.5, extent=245.0),
+        text=("plane3000: 3,000 cameras with per-camera (f, k1, k2) over a 245x245 ground plane (the plane500 "
+              "camera density), 2M points, geometric tracks mean ~6 (~12M observations), noise 0.5 px, 5% "
+              "outliers, Huber 1 px, matrix-free block-Jacobi PCG tolerance 1e-6")),
+}
 CPU_SAMPLE_ITERATIONS = 3
 TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane500.txt")
+WORKLOAD = WORKLOADS["plane500"]["text"]
 
 
-def problem_for(rank: int):
+def problem_for(rank: int, workload: str = "plane500"):
     from openmvg_ba_cuda import synthetic
-    return synthetic.plane_problem(seed=11 + rank, mean_track=6.5)
+    return synthetic.plane_problem(seed=11 + rank, **WORKLOADS[workload]["kwargs"])
 
 
 def solve_config(precision: int, max_iterations: int = 50, stream: int = 0):
@@ -196,7 +208,7 @@ def run_reference(args) -> int:
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    problem = problem_for(0)
+    problem = problem_for(0, args.workload)
     for _ in range(args.warmup):
         cpu_sample(problem, 1)
     samples = [cpu_sample(problem, CPU_SAMPLE_ITERATIONS) for _ in range(args.steps)]
@@ -210,7 +222,8 @@ def run_reference(args) -> int:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "parallelism": "host threads", "cpu": cpu_info(),
+        "config": {"workload": WORKLOADS[args.workload]["text"], "max_iterations": args.max_iterations,
+                   "parallelism": "host threads", "cpu": cpu_info(),
                    "sample_lm_iterations_per_step": CPU_SAMPLE_ITERATIONS},
         "cpu_baseline": base,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -283,12 +296,12 @@ def run_ours(args) -> int:
     from openmvg_ba_cuda import abi
     from openmvg_ba_cuda.adjuster import CudaBundleAdjuster
 
-    problem = problem_for(rank)
+    problem = problem_for(rank, args.workload)
     stream = torch.cuda.Stream(device=local)  # the solver's stream: events and flushes go here too
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     adjuster = CudaBundleAdjuster(local)
-    mixed_cfg = solve_config(abi.PRECISION_MIXED, stream=stream.cuda_stream)
-    fp64_cfg = solve_config(abi.PRECISION_FP64, stream=stream.cuda_stream)
+    mixed_cfg = solve_config(abi.PRECISION_MIXED, max_iterations=args.max_iterations, stream=stream.cuda_stream)
+    fp64_cfg = solve_config(abi.PRECISION_FP64, max_iterations=args.max_iterations, stream=stream.cuda_stream)
 
     # value: mixed precision, problem resident in device memory
     plan = adjuster.plan(problem, mixed_cfg)
@@ -343,7 +356,7 @@ def run_ours(args) -> int:
     adjuster.close()
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.legs == "all":
         cpu = cpu_sample(problem, CPU_SAMPLE_ITERATIONS)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"cpu": cpu_info()}
 
@@ -355,7 +368,8 @@ def run_ours(args) -> int:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total_s / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": "mixed", "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOADS[args.workload]["text"], "max_iterations": args.max_iterations,
+                       "precision": "mixed", "parallelism": f"replicas x{world}",
                        "observations": int(info["observation_count"]), "points": int(info["point_count"]),
                        "cameras": int(info["camera_count"]), "reduced_dimension": int(info["reduced_dimension"]),
                        "l2": ("inputs larger than L2: %.0f MB of Jacobian records and tile tables per solve vs "
@@ -366,7 +380,9 @@ def run_ours(args) -> int:
             "lm_iterations_per_step": local_its / steps,
             "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports) / steps,
             "final_cost": cost_mixed,
+            "converged": reports[-1]["status"] == 0,
             "fp64": {"value": its64 / s64, "unit": UNIT, "time_to_converge_s": s64 / steps, "final_cost": cost_fp64,
+                     "converged": reports64[-1]["status"] == 0,
                      "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports64) / steps},
             "mixed_vs_fp64": {"speedup": (s64 / steps) / (total_s / steps),
                               "final_cost_rel_diff": abs(cost_mixed - cost_fp64) / abs(cost_fp64)},
@@ -393,8 +409,11 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--legs", choices=["all", "value"], default="all",
-                    help="value: only the resident mixed solve and the kernel timing (for profiler runs)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plane500")
+    ap.add_argument("--max-iterations", type=int, default=50, help="LM iteration budget of every solve")
+    ap.add_argument("--legs", choices=["all", "gpu", "value"], default="all",
+                    help="gpu: every leg but the CPU baseline; value: only the resident mixed solve and the kernel "
+                         "timing (for profiler runs)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

@@ -55,7 +55,7 @@ def build(debug: bool = False, verbose: bool = False) -> str:
             cmd += ["-x", "c++"]
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    link = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    link = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
     subprocess.run(link, check=True)
     return LIB
 

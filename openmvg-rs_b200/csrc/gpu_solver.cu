@@ -1803,13 +1803,22 @@ struct Solver {
     D = L.D;
     ng = n.self_cal ? (int)n.group_dim.size() : 0;
     direct = !opt.iterative;
+    const double t0 = now();
     build_tables(n, L, direct || D <= opt.dense_rank_limit, S);
-    build_tiles(n, L, S, mv_tile_obs<double>(), T64);
+    const double t1 = now();
+    // mixed precision keeps only FP32 Jacobian records (and their tiles); FP64 mode only FP64 ones
     mixed = opt.precision == 1 && !direct;
-    if (mixed) build_tiles(n, L, S, mv_tile_obs<float>(), T32);
+    if (mixed)
+      build_tiles(n, L, S, mv_tile_obs<float>(), T32);
+    else
+      build_tiles(n, L, S, mv_tile_obs<double>(), T64);
+    const double t2 = now();
     nb = (int)S.blk_off.size();
     red_blocks = std::min(1024, grid_for(std::max(P, N), kReduceThreads));
     upload();
+    sync();
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr, "[omvgba] setup: tables %.3fs tiles %.3fs upload %.3fs\n", t1 - t0, t2 - t1, now() - t2);
   }
 
   DevView view() const {
@@ -1832,9 +1841,14 @@ struct Solver {
     return v;
   }
   DevState state(int which) const { return {d_pose[which].p, d_points[which].p, d_groups[which].p}; }
+  // the FP32 records of mixed precision (assembly, pairs and candidate read them, computing in FP64)
+  LinOut<float> lin32() const {
+    return {d_rec32.p, dT32.obs_rec.p, mv_tile_obs<float>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_ig.p, d_gp.p,
+            d_ddiag.p, d_summary.p, nullptr};
+  }
   LinOut<T> lin() const {
-    return {d_rec.p,         dT64.obs_rec.p, mv_tile_obs<T>(), mixed ? d_rec32.p : nullptr, dT32.obs_rec.p,
-            mv_tile_obs<float>(), d_rw.p, d_vinv.p, d_ig.p, d_gp.p, d_ddiag.p, d_summary.p, nullptr};
+    return {d_rec.p, dT64.obs_rec.p, mv_tile_obs<T>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_ig.p, d_gp.p,
+            d_ddiag.p, d_summary.p, nullptr};
   }
   BlockTables tables() const {
     BlockTables b;
@@ -1910,10 +1924,11 @@ struct Solver {
       d_groups[w].upload(gr.data(), gr.size(), st);
     }
     {
-      dT64.upload(T64, st);
-      d_rec.alloc((size_t)std::max(1, dT64.ntiles) * T64.tile * kRec, st);
-      d_rec.zero();  // padding slots of partial tiles stay zero
-      if (mixed) {
+      if (!mixed) {
+        dT64.upload(T64, st);
+        d_rec.alloc((size_t)std::max(1, dT64.ntiles) * T64.tile * kRec, st);
+        d_rec.zero();  // padding slots of partial tiles stay zero
+      } else {
         dT32.upload(T32, st);
         d_rec32.alloc((size_t)std::max(1, dT32.ntiles) * T32.tile * kRec, st);
         d_rec32.zero();
@@ -1995,8 +2010,8 @@ struct Solver {
       // one resident wave of product CTAs: how far ahead each CTA prefetches into L2
       int sms = 148, per64 = 1, per32 = 1;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_mv_tiles<T>, mv_tile_obs<T>(), 0));
-      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_mv_tiles<float>, mv_tile_obs<float>(), 0));
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_mv_tiles<T, T>, mv_tile_obs<T>(), 0));
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_mv_tiles<float, float>, mv_tile_obs<float>(), 0));
       dT64.prefetch_ahead = per64 * sms;
       dT32.prefetch_ahead = per32 * sms;
     }
@@ -2075,14 +2090,20 @@ struct Solver {
   // Full linearization + camera-side reductions at the given damping.
   Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_dense) {
     DevView v = view();
-    OMVGBA_LAUNCH(k_linearize<T>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin());
+    if (mixed)
+      OMVGBA_LAUNCH(k_linearize<float>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin32());
+    else
+      OMVGBA_LAUNCH(k_linearize<T>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin());
     check_launch();
     OMVGBA_LAUNCH(k_reduce_summary, red_blocks, kReduceThreads, 0, st, d_summary.p, P, d_summary_part.p);
     OMVGBA_LAUNCH(k_reduce_summary, 1, kReduceThreads, 0, st, d_summary_part.p, red_blocks, d_summary_part.p);
     check_launch();
     BlockTables bt = tables();
     if (bt.nchunks > 0) {
-      OMVGBA_LAUNCH(k_block_chunks<T>, bt.nchunks, 32, 0, st, bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
+      if (mixed)
+        OMVGBA_LAUNCH(k_block_chunks<float>, bt.nchunks, 32, 0, st, bt, lin32(), d_obs_intr_col.p, d_chunk_out.p);
+      else
+        OMVGBA_LAUNCH(k_block_chunks<T>, bt.nchunks, 32, 0, st, bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
       OMVGBA_LAUNCH(k_block_finalize, grid_for(nb, 64), 64, 0, st, bt, d_chunk_out.p, d_blk_out.p);
       CUDA_OK(cudaMemsetAsync(d_gfull.p, 0, sizeof(double) * std::max(1, D), st));
       CUDA_OK(cudaMemsetAsync(d_gred.p, 0, sizeof(double) * std::max(1, D), st));
@@ -2093,7 +2114,12 @@ struct Solver {
     }
     if (build_dense && D > 0) {
       PairTables pt = pairs(false);
-      if (pt.ngroups > 0) OMVGBA_LAUNCH(k_pairs<T>, pt.ngroups, 32, 0, st, pt, bt, lin(), d_seg_col.p, d_pair_out.p);
+      if (pt.ngroups > 0) {
+        if (mixed)
+          OMVGBA_LAUNCH(k_pairs<float>, pt.ngroups, 32, 0, st, pt, bt, lin32(), d_seg_col.p, d_pair_out.p);
+        else
+          OMVGBA_LAUNCH(k_pairs<T>, pt.ngroups, 32, 0, st, pt, bt, lin(), d_seg_col.p, d_pair_out.p);
+      }
       CUDA_OK(cudaMemsetAsync(d_S.p, 0, sizeof(double) * (size_t)D * D, st));
       OMVGBA_LAUNCH(k_dense_from_blocks, nb, 32, 0, st, bt, d_blk_out.p, D, d_S.p);
       if (pt.ngroups > 0) OMVGBA_LAUNCH(k_dense_pairs, grid_for(pt.ngroups, 64), 64, 0, st, pt, bt, d_pair_out.p, D, d_S.p);
@@ -2187,7 +2213,7 @@ struct Solver {
   void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false,
               double* xy = nullptr) {
     matvec_tiles(x, ctl, fp32);
-    const TileSetDev& ts = fp32 ? dT32 : dT64;
+    const TileSetDev& ts = mixed ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     OMVGBA_LAUNCH(k_mv_tiles_finalize, mv_finalize_ctas(), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda, x, y, xy,
                   ctl);
@@ -2195,14 +2221,18 @@ struct Solver {
   }
   // The tile pass of the product alone: the per-(segment, parameter) partials.
   void matvec_tiles(const double* x, const PcgCtl* ctl, bool fp32) {
-    const TileSetDev& ts = fp32 ? dT32 : dT64;
+    const TileSetDev& ts = mixed ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        OMVGBA_LAUNCH(k_mv_tiles<float>, mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
+        OMVGBA_LAUNCH((k_mv_tiles<float, float>), mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
+                      ts.partial.p, ctl);
+      else if (mixed)  // FP64 arithmetic on the FP32 records: the refinement's residual product
+        OMVGBA_LAUNCH((k_mv_tiles<float, double>), mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
                       ts.partial.p, ctl);
       else
-        OMVGBA_LAUNCH(k_mv_tiles<T>, mt.ntiles, mv_tile_obs<T>(), 0, st, mt, d_rec.p, d_vinv.p, x, ts.partial.p, ctl);
+        OMVGBA_LAUNCH((k_mv_tiles<T, T>), mt.ntiles, mv_tile_obs<T>(), 0, st, mt, d_rec.p, d_vinv.p, x, ts.partial.p,
+                      ctl);
     }
   }
   void check_fault() {
@@ -2215,7 +2245,12 @@ struct Solver {
   bool factor_preconditioner(double lambda) {
     BlockTables bt = tables();
     PairTables xt = pairs(true);
-    if (xt.ngroups > 0) OMVGBA_LAUNCH(k_pairs<T>, xt.ngroups, 32, 0, st, xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
+    if (xt.ngroups > 0) {
+      if (mixed)
+        OMVGBA_LAUNCH(k_pairs<float>, xt.ngroups, 32, 0, st, xt, bt, lin32(), d_seg_col.p, d_xpair_out.p);
+      else
+        OMVGBA_LAUNCH(k_pairs<T>, xt.ngroups, 32, 0, st, xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
+    }
     OMVGBA_LAUNCH(k_block_factor, grid_for(nb, 64), 64, 0, st, bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
                                                    d_blk_cross_begin.p, d_blk_cross_end.p, d_factor.p, d_fail.p);
     check_launch();
@@ -2624,10 +2659,13 @@ struct Solver {
         }
         DevView v = view();
         OMVGBA_LAUNCH(k_retract, grid_for(std::max(n.ncam, ng), 128), 128, 0, st, v, ng, d_step.p, g, d_pose[cur].p,
-                                                                        d_groups[cur].p, d_pose[cand].p,
-                                                                        d_groups[cand].p);
-        OMVGBA_LAUNCH(k_candidate_points<T>, grid_for(P, 128), 128, 0, st, v, lin(), d_step.p, state(cur), state(cand), g,
-                                                                stages[si].loss, d_cand.p);
+                      d_groups[cur].p, d_pose[cand].p, d_groups[cand].p);
+        if (mixed)
+          OMVGBA_LAUNCH(k_candidate_points<float>, grid_for(P, 128), 128, 0, st, v, lin32(), d_step.p, state(cur),
+                        state(cand), g, stages[si].loss, d_cand.p);
+        else
+          OMVGBA_LAUNCH(k_candidate_points<T>, grid_for(P, 128), 128, 0, st, v, lin(), d_step.p, state(cur),
+                        state(cand), g, stages[si].loss, d_cand.p);
         check_launch();
         RedVec<4> cr = reduce<4>(d_cand.p, P, d_cand_part);
         if (cr.v[3] > 0.0) {
@@ -2909,11 +2947,11 @@ ResidentInfo resident_info(const Resident* r) {
       info.jacobian_entries += 2 * (uint64_t)(cam_dim + point_dim);
     }
   }
-  info.tiles64 = (uint64_t)s.dT64.ntiles;
+  info.tiles64 = s.mixed ? 0 : (uint64_t)s.dT64.ntiles;
   info.tiles32 = s.mixed ? (uint64_t)s.dT32.ntiles : 0;
   info.record_bytes64 = sizeof(double) * s.d_rec.n;
   info.record_bytes32 = sizeof(float) * s.d_rec32.n;
-  info.metadata_bytes64 = s.dT64.slots.n + sizeof(uint32_t) * s.dT64.tile_hdr.n;
+  info.metadata_bytes64 = s.mixed ? 0 : s.dT64.slots.n + sizeof(uint32_t) * s.dT64.tile_hdr.n;
   info.metadata_bytes32 = s.mixed ? s.dT32.slots.n + sizeof(uint32_t) * s.dT32.tile_hdr.n : 0;
   return info;
 }

@@ -13,6 +13,7 @@
 //   quarantine ....................... quarantine.rs:34-96
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include <numeric>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ba_cuda.h"
@@ -654,28 +656,126 @@ bool residual_norm(const omvgba_problem& pr, size_t o, const omvgba_pose& pose, 
 }
 
 bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active, const Result* sol, double* cost,
-                    double* rmse) {
-  LossDev loss = problem_loss(pr);
-  double total = 0.0, rs = 0.0, ssr = 1.0;
-  size_t count = 0;
-  for (size_t o = 0; o < pr.observation_count; ++o) {
-    size_t p = pr.observation_point[o];
-    if (!active[p]) continue;
-    const omvgba_pose& pose = sol ? sol->poses[pr.observation_pose[o]] : pr.poses[pr.observation_pose[o]];
-    const omvgba_intrinsic& in = sol ? sol->intrinsics[pr.observation_intrinsic[o]] : pr.intrinsics[pr.observation_intrinsic[o]];
-    const double* X = sol ? &sol->points[3 * p] : pr.points + 3 * p;
-    double nrm;
-    if (!residual_norm(pr, o, pose, in, X, &nrm)) return false;
-    total += loss.cost(nrm);
-    if (nrm > 0.0) {
-      if (rs < nrm) {
-        ssr = 1.0 + ssr * (rs / nrm) * (rs / nrm);
-        rs = nrm;
-      } else {
-        ssr += (nrm / rs) * (nrm / rs);
+                    double* rmse);
+
+// Runs body(chunk, begin, end) over `count` items cut into a fixed number of contiguous chunks, on
+// up to hardware_concurrency threads. Callers combine per-chunk results in chunk order, so every
+// result is independent of the thread count.
+template <typename Body>
+void for_fixed_chunks(size_t count, size_t chunks, Body body) {
+  const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (size_t c; (c = next.fetch_add(1)) < chunks;) {
+      const size_t b = std::min(count, c * per), e = std::min(count, b + per);
+      body(c, b, e);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t i = 1; i < nthreads; ++i) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
+// Inlier count and RMSE of the solution (solver.rs:1317-1402): residual norms of the active
+// observations within the loss scale (every one for squared loss). 64 fixed chunks.
+void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& active, Result& res) {
+  double limit = pr.loss_kind == OMVGBA_LOSS_SQUARED ? INFINITY : pr.loss_scale;
+  constexpr size_t kChunks = 64;
+  std::vector<uint64_t> count(kChunks, 0);
+  std::vector<double> ss(kChunks, 0.0);
+  std::vector<uint8_t> ok(kChunks, 1);
+  res.report.has_inlier_count = 0;
+  res.report.has_final_inlier_rmse = 0;
+  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    for (size_t o = b; o < e; ++o) {
+      size_t p = pr.observation_point[o];
+      if (!active[p]) continue;
+      double nrm;
+      if (!residual_norm(pr, o, res.poses[pr.observation_pose[o]], res.intrinsics[pr.observation_intrinsic[o]],
+                         &res.points[3 * p], &nrm)) {
+        ok[c] = 0;
+        return;
+      }
+      if (nrm <= limit) {
+        count[c]++;
+        ss[c] += nrm * nrm;
       }
     }
-    count++;
+  });
+  uint64_t total = 0;
+  double sum = 0.0;
+  for (size_t c = 0; c < kChunks; ++c) {
+    if (!ok[c]) return;
+    total += count[c];
+    sum += ss[c];
+  }
+  res.report.has_inlier_count = 1;
+  res.report.inlier_count = total;
+  if (total > 0) {
+    double r = std::sqrt(sum / double(total));
+    if (std::isfinite(r)) {
+      res.report.has_final_inlier_rmse = 1;
+      res.report.final_inlier_rmse = r;
+    }
+  }
+}
+
+// Objective and RMSE of the active observations at the input state (sol == nullptr) or at a
+// solution (solver.rs:1052-1131): the RMSE accumulates a scaled sum of squares (largest norm and
+// the sum of squares relative to it) so it cannot overflow. 64 fixed chunks combined in order.
+bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active, const Result* sol, double* cost,
+                    double* rmse) {
+  LossDev loss = problem_loss(pr);
+  constexpr size_t kChunks = 64;
+  struct Part {
+    double total = 0.0, rs = 0.0, ssr = 1.0;
+    size_t count = 0;
+    bool ok = true;
+  };
+  std::vector<Part> parts(kChunks);
+  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    Part& pt = parts[c];
+    for (size_t o = b; o < e; ++o) {
+      size_t p = pr.observation_point[o];
+      if (!active[p]) continue;
+      const omvgba_pose& pose = sol ? sol->poses[pr.observation_pose[o]] : pr.poses[pr.observation_pose[o]];
+      const omvgba_intrinsic& in =
+          sol ? sol->intrinsics[pr.observation_intrinsic[o]] : pr.intrinsics[pr.observation_intrinsic[o]];
+      const double* X = sol ? &sol->points[3 * p] : pr.points + 3 * p;
+      double nrm;
+      if (!residual_norm(pr, o, pose, in, X, &nrm)) {
+        pt.ok = false;
+        return;
+      }
+      pt.total += loss.cost(nrm);
+      if (nrm > 0.0) {
+        if (pt.rs < nrm) {
+          pt.ssr = 1.0 + pt.ssr * (pt.rs / nrm) * (pt.rs / nrm);
+          pt.rs = nrm;
+        } else {
+          pt.ssr += (nrm / pt.rs) * (nrm / pt.rs);
+        }
+      }
+      pt.count++;
+    }
+  });
+  double total = 0.0, rs = 0.0, ssr = 1.0;
+  size_t count = 0;
+  for (const Part& pt : parts) {
+    if (!pt.ok) return false;
+    total += pt.total;
+    count += pt.count;
+    if (pt.rs > 0.0) {  // merge the chunk's scaled sum of squares
+      if (rs < pt.rs) {
+        ssr = pt.ssr + ssr * (rs / pt.rs) * (rs / pt.rs);
+        rs = pt.rs;
+      } else {
+        ssr += pt.ssr * (pt.rs / rs) * (pt.rs / rs);
+      }
+    }
   }
   if (count == 0 || !std::isfinite(total) || total < 0.0) return false;
   double r = rs * std::sqrt(ssr / double(count));
@@ -683,35 +783,6 @@ bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active
   *cost = total;
   *rmse = r;
   return true;
-}
-
-void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& active, Result& res) {
-  double limit = pr.loss_kind == OMVGBA_LOSS_SQUARED ? INFINITY : pr.loss_scale;
-  uint64_t count = 0;
-  double ss = 0.0;
-  res.report.has_inlier_count = 0;
-  res.report.has_final_inlier_rmse = 0;
-  for (size_t o = 0; o < pr.observation_count; ++o) {
-    size_t p = pr.observation_point[o];
-    if (!active[p]) continue;
-    double nrm;
-    if (!residual_norm(pr, o, res.poses[pr.observation_pose[o]], res.intrinsics[pr.observation_intrinsic[o]],
-                       &res.points[3 * p], &nrm))
-      return;
-    if (nrm <= limit) {
-      count++;
-      ss += nrm * nrm;
-    }
-  }
-  res.report.has_inlier_count = 1;
-  res.report.inlier_count = count;
-  if (count > 0) {
-    double r = std::sqrt(ss / double(count));
-    if (std::isfinite(r)) {
-      res.report.has_final_inlier_rmse = 1;
-      res.report.final_inlier_rmse = r;
-    }
-  }
 }
 
 Result raise(const omvgba_problem& pr, const Lowered& L, const std::vector<double>& rot, const std::vector<double>& tr,
@@ -856,13 +927,19 @@ void canonicalize(const omvgba_problem& pr, Result& res) {
 
 Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
+  const auto t0 = std::chrono::steady_clock::now();
   Lowered L = lower(pr);
+  const double t_lower = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   LmOptions opt = lm_options(pr, cfg, L.n);
   std::vector<double> rot, tr, pts, grp;
   NativeReport nr = gpu_refine(ctx, L.n, opt, rot, tr, pts, grp);
+  const double t_gpu = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_lower;
   Result res = raise(pr, L, rot, tr, pts, grp, nr, opt.iterative);
   finish_solution(pr, res);
   canonicalize(pr, res);
+  if (std::getenv("OMVGBA_PHASE_TIMES"))
+    std::fprintf(stderr, "[omvgba] solve_once: lower %.3fs gpu %.3fs raise+finish %.3fs\n", t_lower, t_gpu,
+                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_lower - t_gpu);
   return res;
 }
 
@@ -871,12 +948,14 @@ std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pos
   size_t N = pr.observation_count;
   std::vector<Vec3> off(N);
   std::vector<double> dist(N);
-  for (size_t o = 0; o < N; ++o) {
-    size_t p = pr.observation_point[o];
-    const double* C = poses[pr.observation_pose[o]].center;
-    off[o] = {points[3 * p] - C[0], points[3 * p + 1] - C[1], points[3 * p + 2] - C[2]};
-    dist[o] = std::sqrt(off[o][0] * off[o][0] + off[o][1] * off[o][1] + off[o][2] * off[o][2]);
-  }
+  for_fixed_chunks(N, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t o = b; o < e; ++o) {
+      size_t p = pr.observation_point[o];
+      const double* C = poses[pr.observation_pose[o]].center;
+      off[o] = {points[3 * p] - C[0], points[3 * p + 1] - C[1], points[3 * p + 2] - C[2]};
+      dist[o] = std::sqrt(off[o][0] * off[o][0] + off[o][1] * off[o][1] + off[o][2] * off[o][2]);
+    }
+  });
   double scene = 0.0;
   if (N > 0) {
     std::nth_element(dist.begin(), dist.begin() + N / 2, dist.end());
@@ -1152,11 +1231,22 @@ Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_co
   return out;
 }
 
+double seconds_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
 Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  const auto t0 = std::chrono::steady_clock::now();
   Prepared prep;
   prepare_quarantine(pr, cfg, prep);
+  const double t_prep = seconds_since(t0);
   Result sol = solve_once(ctx, *prep.working, cfg);
-  return finish_quarantine(ctx, pr, cfg, prep, std::move(sol));
+  const double t_solve = seconds_since(t0) - t_prep;
+  Result out = finish_quarantine(ctx, pr, cfg, prep, std::move(sol));
+  if (std::getenv("OMVGBA_PHASE_TIMES"))
+    std::fprintf(stderr, "[omvgba] host: prepare %.3fs solve_once %.3fs finish %.3fs\n", t_prep, t_solve,
+                 seconds_since(t0) - t_prep - t_solve);
+  return out;
 }
 
 int write_error(omvgba_error* e, int code, const std::string& msg) {

@@ -77,12 +77,14 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
-template <typename T>
-__global__ void __launch_bounds__(mv_tile_obs<T>(), 4)
-    k_mv_tiles(MvTiles mt, const T* __restrict__ rec, const double* __restrict__ vinv, const double* __restrict__ x,
+// R: the records' storage type (it sets the tile size); T: the arithmetic type (T = double with
+// R = float is the FP64 product of FP32-stored Jacobians that mixed-precision refinement uses).
+template <typename R, typename T = R>
+__global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 : 2)
+    k_mv_tiles(MvTiles mt, const R* __restrict__ rec, const double* __restrict__ vinv, const double* __restrict__ x,
                double* __restrict__ partial, const PcgCtl* ctl) {
   if (pcg_stopped(ctl)) return;
-  constexpr int TILE = mv_tile_obs<T>();
+  constexpr int TILE = mv_tile_obs<R>();
   constexpr int TS = TILE + 1;  // padded row stride: the 9 parameter rows of one column use 9 banks
   __shared__ T xs[kSegParams * TILE];
   __shared__ T zz[3 * TILE];
@@ -93,16 +95,16 @@ __global__ void __launch_bounds__(mv_tile_obs<T>(), 4)
   const int t = blockIdx.x, tid = threadIdx.x;
   // The CTA that starts about one resident wave later finds its records in L2.
   if (tid == 0 && mt.prefetch_ahead > 0 && t + mt.prefetch_ahead < mt.ntiles)
-    bulk_prefetch_l2(rec + (size_t)(t + mt.prefetch_ahead) * TILE * kRec, (uint32_t)(sizeof(T) * TILE * kRec));
+    bulk_prefetch_l2(rec + (size_t)(t + mt.prefetch_ahead) * TILE * kRec, (uint32_t)(sizeof(R) * TILE * kRec));
   // Every first load depends only on (t, tid), so they all issue together: the records, the header
   // and one entry of each slot column (thread s loads segment s's row; rows past the tile's
   // segment count are zero).
-  const T* r = rec + (size_t)t * TILE * kRec + tid;  // a partial tile's unused records are zero
+  const R* r = rec + (size_t)t * TILE * kRec + tid;  // a partial tile's unused records are zero
   T jc[18], jp[6];
 #pragma unroll
-  for (int c = 0; c < 18; ++c) jc[c] = __ldg(r + c * TILE);
+  for (int c = 0; c < 18; ++c) jc[c] = (T)__ldg(r + c * TILE);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) jp[c] = __ldg(r + (kJp + c) * TILE);
+  for (int c = 0; c < 6; ++c) jp[c] = (T)__ldg(r + (kJp + c) * TILE);
   const uint4 hdr = mt.tile_hdr[t];
   const unsigned char* slot = mt.slots + (size_t)t * MvSlot::bytes(TILE);
   const uint32_t my_w0 = __ldg(reinterpret_cast<const uint32_t*>(slot + MvSlot::w0(TILE)) + tid);

@@ -884,7 +884,9 @@ __device__ __forceinline__ double warp_fixed_sum(const double* __restrict__ v, i
 // finalize's per-CTA curvature terms in the same order, so all agree on alpha; a curvature <= 0
 // or a non-finite alpha rejects. Thread per block: x += alpha d, r -= alpha q, z = M^-1 r with the
 // Jacobi-scaled Cholesky factor, and the block's |r|^2 and r.z, reduced per CTA in a fixed order.
-__global__ void __launch_bounds__(128) k_pcg_update_precond(BlockTables bt, const double* __restrict__ factor,
+constexpr int kUpdThreads = 32;  // one warp per CTA: many CTAs, so the blocks' solves spread over the SMs
+
+__global__ void __launch_bounds__(kUpdThreads) k_pcg_update_precond(BlockTables bt, const double* __restrict__ factor,
                                                             const double* __restrict__ dq_part, int ndq,
                                                             const double* __restrict__ d, const double* __restrict__ q,
                                                             double* x, double* r, double* z, double* rr_part,
@@ -892,9 +894,8 @@ __global__ void __launch_bounds__(128) k_pcg_update_precond(BlockTables bt, cons
   if (ctl->status != kRunning) return;
   __shared__ double s_alpha;
   __shared__ int s_go;
-  __shared__ double s1[4], s2[4];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (warp == 0) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  {
     const double curv = warp_fixed_sum(dq_part, ndq, lane);
     if (lane == 0) {
       s_go = 0;
@@ -920,7 +921,16 @@ __global__ void __launch_bounds__(128) k_pcg_update_precond(BlockTables bt, cons
   const int b = blockIdx.x * blockDim.x + tid;
   if (b < bt.nblocks) {
     const int dim = bt.blk_dim[b], o = bt.blk_off[b];
-    const double* F = factor + 42 * (size_t)b;
+    double F[42];  // the block's factor (lower 6x6 row-major, then the 6 Jacobi scales), 16 B loads
+    {
+      const double2* f2 = reinterpret_cast<const double2*>(factor + 42 * (size_t)b);
+#pragma unroll
+      for (int q = 0; q < 21; ++q) {
+        const double2 v = __ldg(f2 + q);
+        F[2 * q] = v.x;
+        F[2 * q + 1] = v.y;
+      }
+    }
     double rv[6], sv[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i)
@@ -929,33 +939,41 @@ __global__ void __launch_bounds__(128) k_pcg_update_precond(BlockTables bt, cons
         rv[i] = r[o + i] - alpha * q[o + i];
         r[o + i] = rv[i];
       }
-    for (int i = 0; i < dim; ++i) {
-      double v = rv[i] / F[36 + i];
-      for (int k = 0; k < i; ++k) v -= F[6 * i + k] * sv[k];
-      sv[i] = v / F[6 * i + i];
+    // forward and back substitution, unrolled over the maximum block size (6) so F stays in registers
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      if (i < dim) {
+        double v = rv[i] / F[36 + i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) v -= F[6 * i + k] * sv[k];
+        sv[i] = v / F[6 * i + i];
+      }
     }
-    for (int i = dim - 1; i >= 0; --i) {
-      double v = sv[i];
-      for (int k = i + 1; k < dim; ++k) v -= F[6 * k + i] * sv[k];
-      sv[i] = v / F[6 * i + i];
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+      if (i < dim) {
+        double v = sv[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k)
+          if (k < dim) v -= F[6 * k + i] * sv[k];
+        sv[i] = v / F[6 * i + i];
+      }
     }
-    for (int i = 0; i < dim; ++i) {
-      const double zi = sv[i] / F[36 + i];
-      z[o + i] = zi;
-      rr += rv[i] * rv[i];
-      rz += rv[i] * zi;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      if (i < dim) {
+        const double zi = sv[i] / F[36 + i];
+        z[o + i] = zi;
+        rr += rv[i] * rv[i];
+        rz += rv[i] * zi;
+      }
     }
   }
   rr = warp_sum(rr);
   rz = warp_sum(rz);
-  if (lane == 0) {
-    s1[warp] = rr;
-    s2[warp] = rz;
-  }
-  __syncthreads();
   if (tid == 0) {
-    rr_part[blockIdx.x] = (s1[0] + s1[1]) + (s1[2] + s1[3]);
-    rz_part[blockIdx.x] = (s2[0] + s2[1]) + (s2[2] + s2[3]);
+    rr_part[blockIdx.x] = rr;
+    rz_part[blockIdx.x] = rz;
   }
 }
 
@@ -2001,8 +2019,8 @@ struct Solver {
     for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp, &d_rhs, &d_r64, &d_e}) b->alloc(std::max(1, D), st);
     d_factor.alloc((size_t)42 * std::max(1, nb), st);
     d_dq.alloc(std::max(1, nb), st);
-    d_rr_part.alloc(std::max(1, grid_for(nb, 128)), st);
-    d_rz_part.alloc(std::max(1, grid_for(nb, 128)), st);
+    d_rr_part.alloc(std::max(1, grid_for(nb, kUpdThreads)), st);
+    d_rz_part.alloc(std::max(1, grid_for(nb, kUpdThreads)), st);
     d_fail.alloc(std::max(1, nb), st);
     d_fault.alloc(1, st);
     d_fault.zero();
@@ -2328,8 +2346,8 @@ struct Solver {
     // two iterations per graph: the even one reads rho slot 0, the odd one slot 1
     for (int slot = 0; slot < 2; ++slot) {
       matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p);
-      const int nupd = grid_for(nb, 128);
-      OMVGBA_LAUNCH(k_pcg_update_precond, nupd, 128, 0, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
+      const int nupd = grid_for(nb, kUpdThreads);
+      OMVGBA_LAUNCH(k_pcg_update_precond, nupd, kUpdThreads, 0, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
                     d_dir.p, d_q.p, x, d_r.p, d_z.p, d_rr_part.p, d_rz_part.p, slot, dctl);
       OMVGBA_LAUNCH(k_pcg_direction, grid_for(D, 256), 256, 0, st, D, d_rr_part.p, d_rz_part.p, nupd, d_z.p,
                     d_dir.p, slot, dctl);

@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(256) k_mv_tiles_finalize(MvTiles mt, const dou
     const uint32_t a0 = mt.blk_part[b], a1 = mt.blk_part[b + 1];
     const uint32_t nseg = d > 0 ? (a1 - a0) / (uint32_t)d : 0u;
     double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 4
     for (uint32_t j = lane; j < nseg; j += 32) {
       const double* pp = partial + a0 + (size_t)j * d;
 #pragma unroll

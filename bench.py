@@ -51,8 +51,14 @@ WORKLOADS = {
         text=("plane3000: 3,000 cameras with per-camera (f, k1, k2) over a 245x245 ground plane (the plane500 "
               "camera density), 2M points, geometric tracks mean ~6 (~12M observations), noise 0.5 px, 5% "
               "outliers, Huber 1 px, matrix-free block-Jacobi PCG tolerance 1e-6")),
+    "windows256": dict(
+        kwargs=dict(),
+        text=("windows256: 256 independent local-BA windows (5-40 calibrated cameras, 500-5,290 points, tracks "
+              "2-10, 1,408,836 observations at seed 23), Huber 1 px, dense Cholesky steps per window, solved "
+              "in one batched call")),
 }
 CPU_SAMPLE_ITERATIONS = 3
+CPU_SAMPLE_WINDOWS = 32
 TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane500.txt")
 WORKLOAD = WORKLOADS["plane500"]["text"]
 
@@ -283,6 +289,76 @@ def kernel_roofline(plan, info: dict, stream, flush, launches: int = 20) -> dict
             "algorithmic_bytes_per_launch": algorithmic, "avg_launch_us": avg_s * 1e6, "launches_timed": launches}
 
 
+def run_batched(args) -> int:
+    """windows256: LM iterations/s summed over the windows of one omvgba_solve_batched call, timed
+    on the host clock around the synchronous call (its workers run on their own streams), with the
+    problems in host memory (so value and e2e are the same measurement)."""
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from openmvg_ba_cuda import RobustLoss, SolveConfig, synthetic
+    from openmvg_ba_cuda.adjuster import CudaBundleAdjuster
+    problems = [dataclasses_replace_loss(p, RobustLoss.huber(1.0)) for p in synthetic.window_problems(seed=23 + rank)]
+    cfg = SolveConfig(max_iterations=args.max_iterations)
+    adjuster = CudaBundleAdjuster(local)
+    for _ in range(args.warmup):
+        adjuster.solve_batched(problems, cfg)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    total_s, its, launches, conv = 0.0, 0, 0, 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sols = adjuster.solve_batched(problems, cfg)
+        torch.cuda.synchronize()
+        total_s += time.perf_counter() - t0
+        its += sum(s.report["iteration_count"] for s in sols)
+        launches += sum(s.report["kernel_launches"] for s in sols)
+        conv = sum(1 for s in sols if s.report["status"] == 0)
+    clock_summary = clocks.stop()
+    barrier()
+    s_max, its_all = aggregate(total_s, float(its), device="cuda")
+    cpu = None
+    if rank == 0 and world == 1 and args.legs == "all":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        oracle.set_threads(oracle.max_threads())
+        sample = problems[:CPU_SAMPLE_WINDOWS]
+        t0 = time.perf_counter()
+        cits = sum(oracle.solve(p, cfg).report["iteration_count"] for p in sample)
+        dt = time.perf_counter() - t0
+        cpu = {"value": cits / dt, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port", "cpu": cpu_info(),
+               "sample": f"oracle on the first {len(sample)} windows, one after another, all host threads"}
+    adjuster.close()
+    if rank == 0:
+        value = its_all / s_max
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * s_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS["windows256"]["text"], "max_iterations": args.max_iterations,
+                       "windows": len(problems), "observations": int(sum(p.observation_count for p in problems)),
+                       "parallelism": f"replicas x{world}", "timing": "host clock around the batched call"},
+            "windows_per_s": len(problems) * args.steps * world / s_max,
+            "windows_converged": conv, "clocks": clock_summary,
+            "e2e": {"value": value, "unit": UNIT, "note": "the batched call takes host arrays: same as value"},
+            "gpu_launches": int(launches), "roofline": None, "cpu_baseline": cpu}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def dataclasses_replace_loss(problem, loss):
+    import dataclasses
+    return dataclasses.replace(problem, robust_loss=loss)
+
+
 def run_ours(args) -> int:
     import torch
     world, rank, local = dist_env()
@@ -417,6 +493,8 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "windows256":
+        return run_batched(args)
     return run_ours(args)
 
 

@@ -102,6 +102,8 @@ Context* context_create(int device, std::string* error) {
   return c;
 }
 
+int context_device(const Context* c) { return c->device; }
+
 void context_destroy(Context* c) {
   if (!c) return;
   cudaSetDevice(c->device);

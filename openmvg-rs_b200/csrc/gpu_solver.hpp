@@ -71,6 +71,7 @@ struct Context;  // device, stream, pinned scratch
 
 int device_count();
 Context* context_create(int device, std::string* error);
+int context_device(const Context* ctx);
 void context_destroy(Context* ctx);
 
 // Runs the LM refinement on the GPU; on return points/rotation/translation/groups hold the refined

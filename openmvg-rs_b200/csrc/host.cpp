@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <set>
 #include <string>
@@ -1388,6 +1389,71 @@ int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, con
   } catch (const std::exception& ex) {
     return write_error(error, OMVGBA_INTERNAL, ex.what());
   }
+}
+
+// Windows solved concurrently by kBatchWorkers host threads, each with its own context and stream;
+// each window goes through exactly the omvgba_solve path, so its solution is the one omvgba_solve
+// returns for it alone, whichever worker takes it.
+int32_t omvgba_solve_batched(omvgba_context* context, uint64_t window_count, const omvgba_problem* windows,
+                             const omvgba_config* config, omvgba_solution* solutions, omvgba_error* error) {
+  clear_error(error);
+  if (!context || !config || (window_count > 0 && (!windows || !solutions)))
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  for (uint64_t i = 0; i < window_count; ++i)
+    if (!solutions[i].poses || !solutions[i].intrinsics || !solutions[i].points)
+      return write_error(error, OMVGBA_INVALID_ARGUMENT, "null solution buffer for window " + std::to_string(i));
+  try {
+    validate_config(*config);
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
+  constexpr uint64_t kBatchWorkers = 12;
+  const int device = context_device(context->ctx);
+  const uint64_t workers = std::min<uint64_t>(window_count, kBatchWorkers);
+  std::vector<int32_t> codes(window_count, OMVGBA_OK);
+  std::vector<std::string> messages(window_count);
+  std::atomic<uint64_t> next{0};
+  std::string setup_error;
+  std::mutex setup_mutex;
+  omvgba_config cfg = *config;
+  cfg.stream = nullptr;  // every worker runs on its own context's stream
+  auto worker = [&]() {
+    std::string msg;
+    Context* ctx = context_create(device, &msg);
+    if (!ctx) {
+      std::lock_guard<std::mutex> lock(setup_mutex);
+      setup_error = "worker context creation failed: " + msg;
+      return;
+    }
+    for (uint64_t i; (i = next.fetch_add(1)) < window_count;) {
+      const auto t0 = std::chrono::steady_clock::now();
+      try {
+        validate_problem(windows[i]);
+        const Telemetry before = telemetry_now();
+        Result r = solve_with_quarantine(ctx, windows[i], cfg);
+        write_solution(windows[i], r, &solutions[i]);
+        stamp_telemetry(solutions[i].report, before, t0);
+      } catch (const SolveFailure& f) {
+        codes[i] = f.code;
+        messages[i] = f.message;
+      } catch (const std::exception& ex) {
+        codes[i] = OMVGBA_INTERNAL;
+        messages[i] = ex.what();
+      }
+    }
+    context_destroy(ctx);
+  };
+  std::vector<std::thread> pool;
+  for (uint64_t w = 0; w < workers; ++w) pool.emplace_back(worker);
+  for (auto& t : pool) t.join();
+  if (!setup_error.empty() && next.load() < window_count) return write_error(error, OMVGBA_CUDA_ERROR, setup_error);
+  for (uint64_t i = 0; i < window_count; ++i)
+    if (codes[i] != OMVGBA_OK) {
+      const int32_t code = write_error(error, codes[i], "window " + std::to_string(i) + ": " + messages[i]);
+      if (error) error->detail = (int32_t)i;
+      return code;
+    }
+  return OMVGBA_OK;
 }
 
 int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,

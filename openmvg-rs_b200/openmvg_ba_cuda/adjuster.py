@@ -72,6 +72,24 @@ class CudaBundleAdjuster:
         raise_for(code, err)
         return ym, yd
 
+    def solve_batched(self, problems: list, config: SolveConfig | None = None) -> list:
+        """Solve independent windows in one call; window i's solution is what ``solve`` returns for it."""
+        config = config or SolveConfig()
+        marshalled = [abi.MarshalledProblem(p) for p in problems]
+        outs = [abi.SolutionBuffers(p) for p in problems]
+        n = len(problems)
+        probs = (abi.Problem * max(n, 1))(*[m.struct for m in marshalled])
+        sols = (abi.Solution * max(n, 1))(*[o.struct for o in outs])
+        cfg = config.to_struct()
+        err = abi.Error()
+        code = lib().omvgba_solve_batched(self._ctx, n, probs, C.byref(cfg), sols, C.byref(err))
+        raise_for(code, err)
+        results = []
+        for o, s in zip(outs, sols):
+            o.struct = s  # the report was written into the array copy of the struct
+            results.append(Solution.from_buffers(o))
+        return results
+
     def plan(self, problem: BundleProblem, config: SolveConfig | None = None) -> "Plan":
         """Prepare ``problem`` once (lowering, upload) for repeated solves from its initial state."""
         return Plan(self, problem, config or SolveConfig())

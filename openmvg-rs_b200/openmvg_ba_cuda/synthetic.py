@@ -229,20 +229,27 @@ def plane_problem(seed: int = 11, cameras: int = 500, points: int = 200_000, mea
 def window_problems(seed: int = 23, windows: int = 256, total_observations: int = 1_500_000,
                     min_cameras: int = 5, max_cameras: int = 40, min_points: int = 500,
                     max_points: int = 20_000) -> list:
-    """Uneven local-BA windows; point counts log-uniform in [min_points, max_points] then scaled so
-    the windows hold about ``total_observations`` observations together (tracks 2-10)."""
+    """Uneven local-BA windows: cameras uniform in [min_cameras, max_cameras], point counts
+    log-uniform in [min_points, max_points] and then scaled together so that the windows hold about
+    ``total_observations`` observations (tracks 2-10, capped by the cameras that see a point). The
+    scale is set from a first draw's observation count and the windows are drawn again with it."""
     rng = np.random.Generator(np.random.PCG64(seed))
     cams = rng.integers(min_cameras, max_cameras + 1, size=windows)
     raw = np.exp(rng.uniform(np.log(min_points), np.log(max_points), size=windows))
-    scale = total_observations / (raw.sum() * 6.0)
-    pts = np.clip(np.round(raw * min(scale, 1.0)), min_points, max_points).astype(int)
-    out = []
-    for w in range(windows):
-        side = 30.0
-        p = plane_problem(seed=int(rng.integers(1 << 31)), cameras=int(cams[w]), points=int(pts[w]), mean_track=6.0,
-                          altitude=16.0, extent=side, per_camera_intrinsics=False, free_intrinsics=False)
-        out.append(p)
-    return out
+    seeds = rng.integers(1 << 31, size=windows)
+
+    def draw(scale):
+        pts = np.clip(np.round(raw * scale), min_points, max_points).astype(int)
+        return [plane_problem(seed=int(seeds[w]), cameras=int(cams[w]), points=int(pts[w]), mean_track=6.0,
+                              altitude=16.0, extent=30.0, per_camera_intrinsics=False, free_intrinsics=False)
+                for w in range(windows)]
+
+    scale = min(1.0, total_observations / (raw.sum() * 6.0))
+    first = draw(scale)
+    got = sum(p.observation_count for p in first)
+    if got == 0 or abs(got - total_observations) < 0.02 * total_observations:
+        return first
+    return draw(scale * total_observations / got)
 
 
 def residual_inputs(seed: int = 5, observations: int = 10_000_000, cameras: int = 3000, points: int = 2_000_000,

@@ -353,8 +353,9 @@ int32_t omvgba_residual_vjp_f32_static(void* stream, uint64_t observation_count,
 /*
  * Many independent problems (local-BA windows) in one call: solutions[i] receives window i, which is
  * solved exactly as omvgba_solve would solve it alone (so each window carries its own status and
- * convergence reason in its report). The windows run concurrently on a fixed pool of host workers,
- * each with its own stream on the context's device; config->stream is not used. Returns OMVGBA_OK
+ * convergence reason in its report). The windows run concurrently on a pool of host workers (16,
+ * or the OMVGBA_BATCH_WORKERS environment variable), each with its own stream on the context's
+ * device; config->stream is not used. Returns OMVGBA_OK
  * when every window succeeded, else the code of the lowest-numbered failing window with its index in
  * error->detail (the other windows' solutions are still written). No reference counterpart: the
  * reference solves one problem per call (crates/openmvg-ba/src/solver.rs:1562).

@@ -61,9 +61,53 @@ void telemetry_read(uint64_t* launches, uint64_t* h2d, uint64_t* d2h) {
     ++tl_telemetry.launches;                                    \
   } while (0)
 
+// Pinned staging buffer of the calling thread for small host<->device copies: a copy from or to
+// pageable memory goes through the driver's shared staging path, which serializes concurrent solves
+// on different threads; a copy through pinned memory does not.
+struct PinnedStage {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~PinnedStage() {
+    if (p) cudaFreeHost(p);
+  }
+  void* get(size_t need) {
+    if (need <= bytes) return p;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t size = std::max<size_t>(need, 64 * 1024);
+    if (cudaMallocHost(&p, size) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return nullptr;
+    }
+    bytes = size;
+    return p;
+  }
+};
+thread_local PinnedStage tl_pinned;
+constexpr size_t kStagedCopyMax = 1u << 20;
+
+// Host<->device copy on `st`, counted in the telemetry. Copies of at most kStagedCopyMax bytes go
+// through the thread's pinned stage and have completed when the call returns (callers read the
+// host side right after their next synchronize, so nothing relies on them staying asynchronous).
 inline cudaError_t copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
   if (kind == cudaMemcpyHostToDevice) tl_telemetry.h2d += bytes;
   if (kind == cudaMemcpyDeviceToHost) tl_telemetry.d2h += bytes;
+  if ((kind == cudaMemcpyHostToDevice || kind == cudaMemcpyDeviceToHost) && bytes > 0 && bytes <= kStagedCopyMax) {
+    if (void* stage = tl_pinned.get(bytes)) {
+      if (kind == cudaMemcpyHostToDevice) {
+        std::memcpy(stage, src, bytes);
+        cudaError_t e = cudaMemcpyAsync(dst, stage, bytes, kind, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the stage is reused by the next copy
+        return e;
+      }
+      cudaError_t e = cudaMemcpyAsync(stage, src, bytes, kind, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e == cudaSuccess) std::memcpy(dst, stage, bytes);
+      return e;
+    }
+  }
   return cudaMemcpyAsync(dst, src, bytes, kind, st);
 }
 

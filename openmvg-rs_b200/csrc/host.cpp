@@ -641,15 +641,35 @@ struct Result {
   omvgba_report report{};
 };
 
-bool residual_norm(const omvgba_problem& pr, size_t o, const omvgba_pose& pose, const omvgba_intrinsic& in,
-                   const double* X, double* out) {
-  if (in.model != OMVGBA_CAMERA_PINHOLE && in.model != OMVGBA_CAMERA_BROWN_CONRADY) return false;
-  Mat3 R = pose_R(pose);
-  Vec3 C = pose_C(pose);
-  Vec3 xc = rotate(R, {X[0] - C[0], X[1] - C[1], X[2] - C[2]});
-  FixedCameraDev m = make_fixed_camera(in);
+// The poses' rotations and centres and the intrinsics' camera models of one state, built once so
+// that per-observation residuals only rotate and project.
+struct StateView {
+  std::vector<Mat3> R;
+  std::vector<Vec3> C;
+  std::vector<FixedCameraDev> model;
+  std::vector<uint8_t> supported;
+  StateView(const omvgba_problem& pr, const omvgba_pose* poses, const omvgba_intrinsic* intrinsics)
+      : R(pr.pose_count), C(pr.pose_count), model(pr.intrinsic_count), supported(pr.intrinsic_count) {
+    for (size_t i = 0; i < pr.pose_count; ++i) {
+      R[i] = pose_R(poses[i]);
+      C[i] = pose_C(poses[i]);
+    }
+    for (size_t i = 0; i < pr.intrinsic_count; ++i) {
+      const omvgba_intrinsic& in = intrinsics[i];
+      supported[i] = in.model == OMVGBA_CAMERA_PINHOLE || in.model == OMVGBA_CAMERA_BROWN_CONRADY;
+      if (supported[i]) model[i] = make_fixed_camera(in);
+    }
+  }
+};
+
+// Pixel residual norm of observation o with the point at X.
+bool residual_norm(const omvgba_problem& pr, const StateView& sv, size_t o, const double* X, double* out) {
+  const size_t pi = pr.observation_pose[o], ii = pr.observation_intrinsic[o];
+  if (!sv.supported[ii]) return false;
+  const Vec3& C = sv.C[pi];
+  Vec3 xc = rotate(sv.R[pi], {X[0] - C[0], X[1] - C[1], X[2] - C[2]});
   double u, v;
-  if (!m.project(xc[0], xc[1], xc[2], &u, &v)) return false;
+  if (!sv.model[ii].project(xc[0], xc[1], xc[2], &u, &v)) return false;
   double nrm = std::hypot(u - pr.observation_pixel[2 * o], v - pr.observation_pixel[2 * o + 1]);
   if (!std::isfinite(nrm)) return false;
   *out = nrm;
@@ -690,13 +710,13 @@ void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& activ
   std::vector<uint8_t> ok(kChunks, 1);
   res.report.has_inlier_count = 0;
   res.report.has_final_inlier_rmse = 0;
+  const StateView sv(pr, res.poses.data(), res.intrinsics.data());
   for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
     for (size_t o = b; o < e; ++o) {
       size_t p = pr.observation_point[o];
       if (!active[p]) continue;
       double nrm;
-      if (!residual_norm(pr, o, res.poses[pr.observation_pose[o]], res.intrinsics[pr.observation_intrinsic[o]],
-                         &res.points[3 * p], &nrm)) {
+      if (!residual_norm(pr, sv, o, &res.points[3 * p], &nrm)) {
         ok[c] = 0;
         return;
       }
@@ -737,17 +757,15 @@ bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active
     bool ok = true;
   };
   std::vector<Part> parts(kChunks);
+  const StateView sv(pr, sol ? sol->poses.data() : pr.poses, sol ? sol->intrinsics.data() : pr.intrinsics);
   for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
     Part& pt = parts[c];
     for (size_t o = b; o < e; ++o) {
       size_t p = pr.observation_point[o];
       if (!active[p]) continue;
-      const omvgba_pose& pose = sol ? sol->poses[pr.observation_pose[o]] : pr.poses[pr.observation_pose[o]];
-      const omvgba_intrinsic& in =
-          sol ? sol->intrinsics[pr.observation_intrinsic[o]] : pr.intrinsics[pr.observation_intrinsic[o]];
       const double* X = sol ? &sol->points[3 * p] : pr.points + 3 * p;
       double nrm;
-      if (!residual_norm(pr, o, pose, in, X, &nrm)) {
+      if (!residual_norm(pr, sv, o, X, &nrm)) {
         pt.ok = false;
         return;
       }

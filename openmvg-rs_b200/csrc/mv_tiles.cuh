@@ -77,6 +77,28 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
+// The records are read once per product and are larger than L2; an evict-first policy on their
+// prefetch and loads keeps the data that every product re-reads (slots, point blocks, x) resident.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void bulk_prefetch_l2_hint(const void* src, uint32_t bytes, uint64_t pol) {
+  asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(src), "r"(bytes), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ float ld_stream(const float* p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // R: the records' storage type (it sets the tile size); T: the arithmetic type (T = double with
 // R = float is the FP64 product of FP32-stored Jacobians that mixed-precision refinement uses).
 template <typename R, typename T = R>
@@ -94,17 +116,19 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
   __shared__ uint16_t pt_begin[TILE + 1];
   const int t = blockIdx.x, tid = threadIdx.x;
   // The CTA that starts about one resident wave later finds its records in L2.
+  const uint64_t stream_pol = l2_evict_first();
   if (tid == 0 && mt.prefetch_ahead > 0 && t + mt.prefetch_ahead < mt.ntiles)
-    bulk_prefetch_l2(rec + (size_t)(t + mt.prefetch_ahead) * TILE * kRec, (uint32_t)(sizeof(R) * TILE * kRec));
+    bulk_prefetch_l2_hint(rec + (size_t)(t + mt.prefetch_ahead) * TILE * kRec, (uint32_t)(sizeof(R) * TILE * kRec),
+                          stream_pol);
   // Every first load depends only on (t, tid), so they all issue together: the records, the header
   // and one entry of each slot column (thread s loads segment s's row; rows past the tile's
   // segment count are zero).
   const R* r = rec + (size_t)t * TILE * kRec + tid;  // a partial tile's unused records are zero
   T jc[18], jp[6];
 #pragma unroll
-  for (int c = 0; c < 18; ++c) jc[c] = (T)__ldg(r + c * TILE);
+  for (int c = 0; c < 18; ++c) jc[c] = (T)ld_stream(r + c * TILE, stream_pol);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) jp[c] = (T)__ldg(r + (kJp + c) * TILE);
+  for (int c = 0; c < 6; ++c) jp[c] = (T)ld_stream(r + (kJp + c) * TILE, stream_pol);
   const uint4 hdr = mt.tile_hdr[t];
   const unsigned char* slot = mt.slots + (size_t)t * MvSlot::bytes(TILE);
   const uint32_t my_w0 = __ldg(reinterpret_cast<const uint32_t*>(slot + MvSlot::w0(TILE)) + tid);

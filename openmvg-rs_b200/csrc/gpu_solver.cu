@@ -61,6 +61,25 @@ void telemetry_read(uint64_t* launches, uint64_t* h2d, uint64_t* d2h) {
     ++tl_telemetry.launches;                                    \
   } while (0)
 
+// A launch that, with pdl set, may overlap the end of the previous kernel on the stream
+// (programmatic stream serialization; the kernel orders itself with pdl_wait). A failed launch is
+// reported by the next launch check, like the <<<>>> launches.
+template <typename... KArgs, typename... Args>
+void launch_pdl(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  (void)cudaLaunchKernelEx(&cfg, kernel, args...);
+  ++tl_telemetry.launches;
+}
+
 // Pinned staging buffer of the calling thread for small host<->device copies: a copy from or to
 // pageable memory goes through the driver's shared staging path, which serializes concurrent solves
 // on different threads; a copy through pinned memory does not.
@@ -918,6 +937,15 @@ struct PcgCtl {
 
 __device__ __forceinline__ bool pcg_stopped(const PcgCtl* ctl) { return ctl && ctl->status != kRunning; }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialization may start
+// while the kernel before it on the stream is still running: it first issues the loads of data that
+// stays constant during the PCG loop, then lets its own successor launch (pdl_trigger) and waits for
+// its predecessor to complete with its writes visible (pdl_wait) before it reads anything that
+// kernel, or any earlier one, writes. A successor launches only after every CTA of this kernel has
+// triggered or exited, so the waits always end. Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Sum of v[0..n) by one warp in a fixed order (lane-strided partial sums, then a shuffle tree); the
 // result is valid in lane 0 and identical in every CTA that evaluates it.
 __device__ __forceinline__ double warp_fixed_sum(const double* __restrict__ v, int n, int lane) {
@@ -937,10 +965,37 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_update_precond(BlockTables 
                                                             const double* __restrict__ d, const double* __restrict__ q,
                                                             double* x, double* r, double* z, double* rr_part,
                                                             double* rz_part, int slot, PcgCtl* ctl) {
-  if (ctl->status != kRunning) return;
   __shared__ double s_alpha;
   __shared__ int s_go;
   const int tid = threadIdx.x, lane = tid & 31;
+  // the block's factor (lower 6x6 row-major, then the 6 Jacobi scales; constant during PCG), 16 B
+  // loads, before the wait
+  const int b = blockIdx.x * blockDim.x + tid;
+  const bool have = b < bt.nblocks;
+  const int dim = have ? bt.blk_dim[b] : 0, o = have ? bt.blk_off[b] : 0;
+  double F[42];
+  if (have) {
+    const double2* f2 = reinterpret_cast<const double2*>(factor + 42 * (size_t)b);
+#pragma unroll
+    for (int q = 0; q < 21; ++q) {
+      const double2 v = __ldg(f2 + q);
+      F[2 * q] = v.x;
+      F[2 * q + 1] = v.y;
+    }
+  }
+  pdl_trigger();
+  pdl_wait();
+  if (ctl->status != kRunning) return;
+  // this block's d, q, r and x, requested together with the curvature terms
+  double dv[6], qv[6], rv[6], xv[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    if (i < dim) {
+      dv[i] = d[o + i];
+      qv[i] = q[o + i];
+      rv[i] = r[o + i];
+      xv[i] = x[o + i];
+    }
   {
     const double curv = warp_fixed_sum(dq_part, ndq, lane);
     if (lane == 0) {
@@ -964,25 +1019,13 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_update_precond(BlockTables 
   if (!s_go) return;
   const double alpha = s_alpha;
   double rr = 0.0, rz = 0.0;
-  const int b = blockIdx.x * blockDim.x + tid;
-  if (b < bt.nblocks) {
-    const int dim = bt.blk_dim[b], o = bt.blk_off[b];
-    double F[42];  // the block's factor (lower 6x6 row-major, then the 6 Jacobi scales), 16 B loads
-    {
-      const double2* f2 = reinterpret_cast<const double2*>(factor + 42 * (size_t)b);
-#pragma unroll
-      for (int q = 0; q < 21; ++q) {
-        const double2 v = __ldg(f2 + q);
-        F[2 * q] = v.x;
-        F[2 * q + 1] = v.y;
-      }
-    }
-    double rv[6], sv[6];
+  if (have) {
+    double sv[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i)
       if (i < dim) {
-        x[o + i] += alpha * d[o + i];
-        rv[i] = r[o + i] - alpha * q[o + i];
+        x[o + i] = xv[i] + alpha * dv[i];
+        rv[i] = rv[i] - alpha * qv[i];
         r[o + i] = rv[i];
       }
     // forward and back substitution, unrolled over the maximum block size (6) so F stays in registers
@@ -1029,10 +1072,18 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_update_precond(BlockTables 
 // d = z + beta d (also at the iteration limit, which ends the loop after this direction).
 __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const double* __restrict__ rz_part,
                                 int nparts, const double* __restrict__ z, double* d, int slot, PcgCtl* ctl) {
+  pdl_trigger();
+  pdl_wait();
   if (ctl->status != kRunning && ctl->status != kExhausted) return;
   __shared__ double s_beta;
   __shared__ int s_go;
   const int tid = threadIdx.x, lane = tid & 31;
+  const int i = blockIdx.x * blockDim.x + tid;
+  double zi = 0.0, di = 0.0;  // requested together with the partial sums
+  if (i < n) {
+    zi = z[i];
+    di = d[i];
+  }
   if (tid < 32) {
     const double rr = warp_fixed_sum(rr_part, nparts, lane);
     const double rz = warp_fixed_sum(rz_part, nparts, lane);
@@ -1070,8 +1121,7 @@ __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const
   __syncthreads();
   if (!s_go) return;
   const double beta = s_beta;
-  const int i = blockIdx.x * blockDim.x + tid;
-  if (i < n) d[i] = z[i] + beta * d[i];
+  if (i < n) d[i] = zi + beta * di;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -2274,29 +2324,31 @@ struct Solver {
   // fp32: use the FP32 record copy (mixed precision inner solves)
   int mv_finalize_ctas() const { return std::max(1, grid_for((size_t)nb * 32, 256)); }
   // xy: optional per-finalize-CTA sums of x_b . y_b over the CTA's blocks (the PCG curvature terms)
+  // pdl_tiles / pdl: launch the tile pass / the finalize as programmatic dependents of the kernel
+  // before them (inside the PCG graph)
   void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false,
-              double* xy = nullptr) {
-    matvec_tiles(x, ctl, fp32);
+              double* xy = nullptr, bool pdl_tiles = false, bool pdl = false) {
+    matvec_tiles(x, ctl, fp32, pdl_tiles);
     const TileSetDev& ts = mixed ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
-    OMVGBA_LAUNCH(k_mv_tiles_finalize, mv_finalize_ctas(), 256, 0, st, mt, ts.partial.p, d_diag.p, lambda, x, y, xy,
-                  ctl);
+    launch_pdl(pdl, k_mv_tiles_finalize, mv_finalize_ctas(), 256, st, mt, ts.partial.p, d_diag.p, lambda, x, y, xy,
+               ctl);
     check_launch();
   }
   // The tile pass of the product alone: the per-(segment, parameter) partials.
-  void matvec_tiles(const double* x, const PcgCtl* ctl, bool fp32) {
+  void matvec_tiles(const double* x, const PcgCtl* ctl, bool fp32, bool pdl = false) {
     const TileSetDev& ts = mixed ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        OMVGBA_LAUNCH((k_mv_tiles<float, float>), mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
-                      ts.partial.p, ctl);
+        launch_pdl(pdl, k_mv_tiles<float, float>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vinv.p, x,
+                   ts.partial.p, ctl);
       else if (mixed)  // FP64 arithmetic on the FP32 records: the refinement's residual product
-        OMVGBA_LAUNCH((k_mv_tiles<float, double>), mt.ntiles, mv_tile_obs<float>(), 0, st, mt, d_rec32.p, d_vinv.p, x,
-                      ts.partial.p, ctl);
+        launch_pdl(pdl, k_mv_tiles<float, double>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vinv.p, x,
+                   ts.partial.p, ctl);
       else
-        OMVGBA_LAUNCH((k_mv_tiles<T, T>), mt.ntiles, mv_tile_obs<T>(), 0, st, mt, d_rec.p, d_vinv.p, x, ts.partial.p,
-                      ctl);
+        launch_pdl(pdl, k_mv_tiles<T, T>, mt.ntiles, mv_tile_obs<T>(), st, mt, d_rec.p, d_vinv.p, x, ts.partial.p,
+                   ctl);
     }
   }
   void check_fault() {
@@ -2390,13 +2442,14 @@ struct Solver {
     const uint64_t launches_before = tl_telemetry.launches;
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     // two iterations per graph: the even one reads rho slot 0, the odd one slot 1
+    // (every kernel after the graph's first is a programmatic dependent of the one before it)
     for (int slot = 0; slot < 2; ++slot) {
-      matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p);
+      matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p, slot > 0, true);
       const int nupd = grid_for(nb, kUpdThreads);
-      OMVGBA_LAUNCH(k_pcg_update_precond, nupd, kUpdThreads, 0, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
-                    d_dir.p, d_q.p, x, d_r.p, d_z.p, d_rr_part.p, d_rz_part.p, slot, dctl);
-      OMVGBA_LAUNCH(k_pcg_direction, grid_for(D, 256), 256, 0, st, D, d_rr_part.p, d_rz_part.p, nupd, d_z.p,
-                    d_dir.p, slot, dctl);
+      launch_pdl(true, k_pcg_update_precond, nupd, kUpdThreads, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
+                 d_dir.p, d_q.p, x, d_r.p, d_z.p, d_rr_part.p, d_rz_part.p, slot, dctl);
+      launch_pdl(true, k_pcg_direction, grid_for(D, 256), 256, st, D, d_rr_part.p, d_rz_part.p, nupd, d_z.p, d_dir.p,
+                 slot, dctl);
     }
     CUDA_OK(cudaStreamEndCapture(st, &graph));
     const uint64_t kernels_per_graph = tl_telemetry.launches - launches_before;  // counted at capture

@@ -105,7 +105,6 @@ template <typename R, typename T = R>
 __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 : 2)
     k_mv_tiles(MvTiles mt, const R* __restrict__ rec, const double* __restrict__ vinv, const double* __restrict__ x,
                double* __restrict__ partial, const PcgCtl* ctl) {
-  if (pcg_stopped(ctl)) return;
   constexpr int TILE = mv_tile_obs<R>();
   constexpr int TS = TILE + 1;  // padded row stride: the 9 parameter rows of one column use 9 banks
   __shared__ T xs[kSegParams * TILE];
@@ -152,6 +151,11 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
     v1 = __ldg(vi + i1);
     v2 = __ldg(vi + i2);
   }
+  // Everything above is constant during the PCG loop; x and the control block come from the kernels
+  // before this one.
+  pdl_trigger();
+  pdl_wait();
+  if (pcg_stopped(ctl)) return;
   // P0: thread s gathers x for segment s's parameters (zero beyond its dimensions) and stages the
   // segment's row, the segment ranges and the point ranges in shared memory
   {
@@ -257,14 +261,24 @@ __global__ void __launch_bounds__(256) k_mv_tiles_finalize(MvTiles mt, const dou
                                                            const double* __restrict__ diag, double lambda,
                                                            const double* __restrict__ x, double* __restrict__ y,
                                                            double* __restrict__ xy, const PcgCtl* ctl) {
-  if (pcg_stopped(ctl)) return;
   __shared__ double s_dot[8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = blockIdx.x * 8 + warp;
+  // the block's layout and diagonal are constant during the PCG loop: loaded before the wait
+  const bool have = b < mt.nblocks;
+  const int o = have ? mt.blk_off[b] : 0, d = have ? mt.blk_dim[b] : 0;
+  const uint32_t a0 = have ? mt.blk_part[b] : 0u, a1 = have ? mt.blk_part[b + 1] : 0u;
+  double dg[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) dg[c] = lane == 0 && c < d ? diag[o + c] : 0.0;
+  pdl_trigger();
+  pdl_wait();
+  if (pcg_stopped(ctl)) return;
   double dot = 0.0;
-  if (b < mt.nblocks) {
-    const int o = mt.blk_off[b], d = mt.blk_dim[b];
-    const uint32_t a0 = mt.blk_part[b], a1 = mt.blk_part[b + 1];
+  if (have) {
+    double xv[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) xv[c] = lane == 0 && c < d ? x[o + c] : 0.0;
     const uint32_t nseg = d > 0 ? (a1 - a0) / (uint32_t)d : 0u;
     double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 4
@@ -280,9 +294,9 @@ __global__ void __launch_bounds__(256) k_mv_tiles_finalize(MvTiles mt, const dou
 #pragma unroll
       for (int c = 0; c < 6; ++c)
         if (c < d) {
-          const double v = acc[c] + lambda * diag[o + c] * x[o + c];
+          const double v = acc[c] + lambda * dg[c] * xv[c];
           y[o + c] = v;
-          dot += x[o + c] * v;
+          dot += xv[c] * v;
         }
     }
   }

@@ -105,6 +105,7 @@ struct PinnedStage {
   }
 };
 thread_local PinnedStage tl_pinned;
+thread_local PinnedStage tl_poll;  // the PCG loop's status mirrors (read while the next batch runs)
 constexpr size_t kStagedCopyMax = 1u << 20;
 
 // Host<->device copy on `st`, counted in the telemetry. Copies of at most kStagedCopyMax bytes go
@@ -1900,7 +1901,6 @@ struct Solver {
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
   DBuf<int> d_fail;
 
-  DBuf<int> d_fault;
 
   DBuf<double> d_scalars, d_cam_norm, d_ctl;
   DBuf<RedVec<4>> d_cand, d_cand_part;
@@ -2118,8 +2118,6 @@ struct Solver {
     d_rr_part.alloc(std::max(1, grid_for(nb, kUpdThreads)), st);
     d_rz_part.alloc(std::max(1, grid_for(nb, kUpdThreads)), st);
     d_fail.alloc(std::max(1, nb), st);
-    d_fault.alloc(1, st);
-    d_fault.zero();
     {
       // one resident wave of product CTAs: how far ahead each CTA prefetches into L2
       int sms = 148, per64 = 1, per32 = 1;
@@ -2351,12 +2349,6 @@ struct Solver {
                    ctl);
     }
   }
-  void check_fault() {
-    int f = 0;
-    CUDA_OK(copy_async(&f, d_fault.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    sync();
-    if (f) throw SolveFailure{8, "a bulk shared-memory copy did not complete within its wait limit"};
-  }
 
   bool factor_preconditioner(double lambda) {
     BlockTables bt = tables();
@@ -2468,14 +2460,39 @@ struct Solver {
       OMVGBA_LAUNCH(k_sub, grid_for(D, 256), 256, 0, st, D, b, d_q.p, d_r.p);
       check_launch();
     };
-    for (;;) {
+    PcgCtl* mirror = static_cast<PcgCtl*>(tl_poll.get(2 * sizeof(PcgCtl)));
+    if (!mirror) throw SolveFailure{8, "pinned host memory for the PCG status is not available"};
+    struct Events {
+      cudaEvent_t e[2] = {nullptr, nullptr};
+      ~Events() {
+        for (cudaEvent_t x : e)
+          if (x) cudaEventDestroy(x);
+      }
+    } ev;
+    for (cudaEvent_t& e : ev.e) CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // one batch: kPoll iterations, then the status copied into mirror[i]
+    auto enqueue = [&](int i) {
       for (int k = 0; k < kPoll / 2; ++k) CUDA_OK(cudaGraphLaunch(exec, st));  // two iterations per graph
       tl_telemetry.launches += (kPoll / 2) * kernels_per_graph;
       launches += kPoll;
-      CUDA_OK(copy_async(&ctl, dctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
-      sync();
-      check_fault();
+      CUDA_OK(cudaMemcpyAsync(&mirror[i], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
+      tl_telemetry.d2h += sizeof(PcgCtl);
+      CUDA_OK(cudaEventRecord(ev.e[i], st));
+    };
+    // The next batch is enqueued before the host waits for the current batch's status, so the device
+    // keeps running while the host reads it. A batch that runs after the loop stopped changes nothing
+    // the host reads: its products and updates return at once, and at the iteration limit its
+    // direction kernels only rewrite the direction and the term count, which the host replaces. The
+    // host waits for that batch before it acts on the status.
+    int cur = 0;
+    enqueue(cur);
+    for (;;) {
+      enqueue(cur ^ 1);
+      CUDA_OK(cudaEventSynchronize(ev.e[cur]));
+      ctl = mirror[cur];
+      cur ^= 1;
       if (ctl.status == kRunning) continue;
+      CUDA_OK(cudaEventSynchronize(ev.e[cur]));
       if (ctl.status == kRejected) {
         res.terms = ctl.terms;
         return res;
@@ -2515,6 +2532,7 @@ struct Solver {
       ctl.rho_slot[0] = nrho;
       ctl.status = kRunning;
       CUDA_OK(copy_async(dctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+      enqueue(cur);
     }
     recompute();
     dots({{d_r.p, d_r.p}}, h);
@@ -2652,7 +2670,6 @@ struct Solver {
     for (auto pr : {std::make_pair(&d_pose_init, &d_pose[0]), std::make_pair(&d_points_init, &d_points[0]),
                     std::make_pair(&d_groups_init, &d_groups[0])})
       CUDA_OK(copy_async(pr.second->p, pr.first->p, sizeof(double) * pr.first->n, cudaMemcpyDeviceToDevice, st));
-    d_fault.zero();
     t_assemble = t_solve = t_candidate = 0;
   }
 
@@ -2861,7 +2878,6 @@ struct Solver {
         }
       }
     }
-    check_fault();
     // final undamped assembly and certificate
     Gauge g = gauge_for(cur, scene);
     bool dense_rank = D <= opt.dense_rank_limit && !S.grp_row.empty();
@@ -3145,7 +3161,6 @@ void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const L
   CUDA_OK(copy_async(y_mv, s.d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
   CUDA_OK(copy_async(y_dense, s.d_z.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
   s.sync();
-  s.check_fault();
 }
 
 }  // namespace omvgba

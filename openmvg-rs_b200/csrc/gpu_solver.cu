@@ -2433,10 +2433,13 @@ struct Solver {
     cudaGraphExec_t exec;
     const uint64_t launches_before = tl_telemetry.launches;
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    // two iterations per graph: the even one reads rho slot 0, the odd one slot 1
-    // (every kernel after the graph's first is a programmatic dependent of the one before it)
-    for (int slot = 0; slot < 2; ++slot) {
-      matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p, slot > 0, true);
+    // one poll batch (kPoll iterations, an even count) per graph: even iterations read rho slot 0,
+    // odd ones slot 1 (every kernel after the graph's first is a programmatic dependent of the one
+    // before it)
+    static_assert(kPoll % 2 == 0, "the rho slots alternate");
+    for (int it = 0; it < kPoll; ++it) {
+      const int slot = it & 1;
+      matvec(d_dir.p, d_q.p, lambda, dctl, fp32, d_dq.p, it > 0, true);
       const int nupd = grid_for(nb, kUpdThreads);
       launch_pdl(true, k_pcg_update_precond, nupd, kUpdThreads, st, tables(), d_factor.p, d_dq.p, mv_finalize_ctas(),
                  d_dir.p, d_q.p, x, d_r.p, d_z.p, d_rr_part.p, d_rz_part.p, slot, dctl);
@@ -2472,8 +2475,8 @@ struct Solver {
     for (cudaEvent_t& e : ev.e) CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     // one batch: kPoll iterations, then the status copied into mirror[i]
     auto enqueue = [&](int i) {
-      for (int k = 0; k < kPoll / 2; ++k) CUDA_OK(cudaGraphLaunch(exec, st));  // two iterations per graph
-      tl_telemetry.launches += (kPoll / 2) * kernels_per_graph;
+      CUDA_OK(cudaGraphLaunch(exec, st));  // kPoll iterations
+      tl_telemetry.launches += kernels_per_graph;
       launches += kPoll;
       CUDA_OK(cudaMemcpyAsync(&mirror[i], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
       tl_telemetry.d2h += sizeof(PcgCtl);

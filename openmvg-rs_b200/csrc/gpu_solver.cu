@@ -2937,6 +2937,7 @@ struct Solver {
                    (unsigned long long)rej[0], (unsigned long long)rej[1], (unsigned long long)rej[2],
                    (unsigned long long)rej[3]);
     rep.D = D;
+    const double t_download = now();
     // download state
     std::vector<double> pose(12 * (size_t)n.ncam);
     CUDA_OK(copy_async(pose.data(), d_pose[cur].p, sizeof(double) * pose.size(), cudaMemcpyDeviceToHost, st));
@@ -2952,6 +2953,7 @@ struct Solver {
       for (int k = 0; k < 9; ++k) rotation[9 * c + k] = pose[12 * c + k];
       for (int k = 0; k < 3; ++k) translation[3 * c + k] = pose[12 * c + 9 + k];
     }
+    if (std::getenv("OMVGBA_PHASE_TIMES")) std::fprintf(stderr, "[omvgba] download %.3fs\n", now() - t_download);
     return rep;
   }
 

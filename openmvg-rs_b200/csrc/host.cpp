@@ -711,20 +711,25 @@ void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& activ
   res.report.has_inlier_count = 0;
   res.report.has_final_inlier_rmse = 0;
   const StateView sv(pr, res.poses.data(), res.intrinsics.data());
+  const double* X = res.points.data();
   for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    uint64_t n = 0;  // locals: the chunks' slots share cache lines
+    double sum = 0.0;
     for (size_t o = b; o < e; ++o) {
       size_t p = pr.observation_point[o];
       if (!active[p]) continue;
       double nrm;
-      if (!residual_norm(pr, sv, o, &res.points[3 * p], &nrm)) {
+      if (!residual_norm(pr, sv, o, X + 3 * p, &nrm)) {
         ok[c] = 0;
         return;
       }
       if (nrm <= limit) {
-        count[c]++;
-        ss[c] += nrm * nrm;
+        n++;
+        sum += nrm * nrm;
       }
     }
+    count[c] = n;
+    ss[c] = sum;
   });
   uint64_t total = 0;
   double sum = 0.0;
@@ -747,43 +752,54 @@ void refresh_inliers(const omvgba_problem& pr, const std::vector<uint8_t>& activ
 // Objective and RMSE of the active observations at the input state (sol == nullptr) or at a
 // solution (solver.rs:1052-1131): the RMSE accumulates a scaled sum of squares (largest norm and
 // the sum of squares relative to it) so it cannot overflow. 64 fixed chunks combined in order.
+// One chunk's share of the objective and of the scaled sum of squares of the residual norms.
+struct MetricPart {
+  double total = 0.0, rs = 0.0, ssr = 1.0;
+  size_t count = 0;
+  bool ok = true;
+  void add(const LossDev& loss, double nrm) {
+    total += loss.cost(nrm);
+    if (nrm > 0.0) {
+      if (rs < nrm) {
+        ssr = 1.0 + ssr * (rs / nrm) * (rs / nrm);
+        rs = nrm;
+      } else {
+        ssr += (nrm / rs) * (nrm / rs);
+      }
+    }
+    count++;
+  }
+};
+bool merge_metrics(const std::vector<MetricPart>& parts, double* cost, double* rmse);
+
 bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active, const Result* sol, double* cost,
                     double* rmse) {
   LossDev loss = problem_loss(pr);
   constexpr size_t kChunks = 64;
-  struct Part {
-    double total = 0.0, rs = 0.0, ssr = 1.0;
-    size_t count = 0;
-    bool ok = true;
-  };
-  std::vector<Part> parts(kChunks);
+  std::vector<MetricPart> parts(kChunks);
   const StateView sv(pr, sol ? sol->poses.data() : pr.poses, sol ? sol->intrinsics.data() : pr.intrinsics);
+  const double* X0 = sol ? sol->points.data() : pr.points;
   for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
-    Part& pt = parts[c];
-    for (size_t o = b; o < e; ++o) {
+    MetricPart pt;  // a local: the chunks' slots share cache lines
+    for (size_t o = b; o < e && pt.ok; ++o) {
       size_t p = pr.observation_point[o];
       if (!active[p]) continue;
-      const double* X = sol ? &sol->points[3 * p] : pr.points + 3 * p;
       double nrm;
-      if (!residual_norm(pr, sv, o, X, &nrm)) {
+      if (!residual_norm(pr, sv, o, X0 + 3 * p, &nrm))
         pt.ok = false;
-        return;
-      }
-      pt.total += loss.cost(nrm);
-      if (nrm > 0.0) {
-        if (pt.rs < nrm) {
-          pt.ssr = 1.0 + pt.ssr * (pt.rs / nrm) * (pt.rs / nrm);
-          pt.rs = nrm;
-        } else {
-          pt.ssr += (nrm / pt.rs) * (nrm / pt.rs);
-        }
-      }
-      pt.count++;
+      else
+        pt.add(loss, nrm);
     }
+    parts[c] = pt;
   });
+  return merge_metrics(parts, cost, rmse);
+}
+
+// Chunks combined in order: objective, count and the scaled sums of squares of the RMSE.
+bool merge_metrics(const std::vector<MetricPart>& parts, double* cost, double* rmse) {
   double total = 0.0, rs = 0.0, ssr = 1.0;
   size_t count = 0;
-  for (const Part& pt : parts) {
+  for (const MetricPart& pt : parts) {
     if (!pt.ok) return false;
     total += pt.total;
     count += pt.count;
@@ -883,24 +899,93 @@ Result raise(const omvgba_problem& pr, const Lowered& L, const std::vector<doubl
   return res;
 }
 
+// The solution's report over the active observations (points not held out): their count, and, with
+// points held out, the objective and RMSE at the input state and at the solution; then the inlier
+// count and RMSE of the solution. One pass over the observations: each quantity is accumulated per
+// chunk as active_metrics and refresh_inliers accumulate it and combined in the same chunk order, and
+// the solution's residual norm, which both use, is evaluated once.
 void finish_solution(const omvgba_problem& pr, Result& res) {
   std::vector<uint8_t> active(pr.point_count, 1);
   for (auto q : res.quarantined) active[q] = 0;
+  const bool held_out = !res.quarantined.empty();
+  const LossDev loss = problem_loss(pr);
+  const double limit = pr.loss_kind == OMVGBA_LOSS_SQUARED ? INFINITY : pr.loss_scale;
+  constexpr size_t kChunks = 64;
+  std::vector<uint64_t> seen(kChunks, 0), inliers(kChunks, 0);
+  std::vector<double> inlier_ss(kChunks, 0.0);
+  std::vector<MetricPart> at_input(kChunks), at_solution(kChunks);  // at_solution[c].ok: chunk c's norms
+  const StateView sv(pr, res.poses.data(), res.intrinsics.data());
+  std::unique_ptr<StateView> sv_input;
+  if (held_out) sv_input = std::make_unique<StateView>(pr, pr.poses, pr.intrinsics);
+  // each chunk accumulates in locals and stores once: the chunks' slots share cache lines
+  const double* X1 = res.points.data();
+  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    MetricPart m1, m0;
+    uint64_t n_seen = 0, n_in = 0;
+    double ss = 0.0;
+    for (size_t o = b; o < e; ++o) {
+      const size_t p = pr.observation_point[o];
+      if (!active[p]) continue;
+      n_seen++;
+      if (m1.ok) {
+        double nrm;
+        if (!residual_norm(pr, sv, o, X1 + 3 * p, &nrm)) {
+          m1.ok = false;
+        } else {
+          if (held_out) m1.add(loss, nrm);
+          if (nrm <= limit) {
+            n_in++;
+            ss += nrm * nrm;
+          }
+        }
+      }
+      if (held_out && m0.ok) {
+        double nrm;
+        if (!residual_norm(pr, *sv_input, o, pr.points + 3 * p, &nrm))
+          m0.ok = false;
+        else
+          m0.add(loss, nrm);
+      }
+    }
+    at_solution[c] = m1;
+    at_input[c] = m0;
+    seen[c] = n_seen;
+    inliers[c] = n_in;
+    inlier_ss[c] = ss;
+  });
   uint64_t cnt = 0;
-  for (size_t o = 0; o < pr.observation_count; ++o) cnt += active[pr.observation_point[o]];
+  for (uint64_t k : seen) cnt += k;
   res.report.has_observation_count = 1;
   res.report.observation_count = cnt;
   res.report.quarantined_point_count = res.quarantined.size();
-  if (!res.quarantined.empty()) {
+  if (held_out) {
     double c0, r0, c1, r1;
-    if (!active_metrics(pr, active, nullptr, &c0, &r0) || !active_metrics(pr, active, &res, &c1, &r1))
+    if (!merge_metrics(at_input, &c0, &r0) || !merge_metrics(at_solution, &c1, &r1))
       fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
     res.report.initial_objective = c0;
     res.report.initial_rmse = r0;
     res.report.final_objective = c1;
     res.report.final_rmse = r1;
   }
-  refresh_inliers(pr, active, res);
+  // inlier count and RMSE, as refresh_inliers reports them
+  res.report.has_inlier_count = 0;
+  res.report.has_final_inlier_rmse = 0;
+  uint64_t total = 0;
+  double sum = 0.0;
+  for (size_t c = 0; c < kChunks; ++c) {
+    if (!at_solution[c].ok) return;
+    total += inliers[c];
+    sum += inlier_ss[c];
+  }
+  res.report.has_inlier_count = 1;
+  res.report.inlier_count = total;
+  if (total > 0) {
+    double r = std::sqrt(sum / double(total));
+    if (std::isfinite(r)) {
+      res.report.has_final_inlier_rmse = 1;
+      res.report.final_inlier_rmse = r;
+    }
+  }
 }
 
 void canonicalize(const omvgba_problem& pr, Result& res) {
@@ -1550,12 +1635,25 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     const Telemetry before = telemetry_now();
     const omvgba_problem& working = *plan->prep.working;
     std::vector<double> rot, tr, pts, grp;
+    double laps[6];
     NativeReport nr = resident_refine(plan->resident, rot, tr, pts, grp);
+    laps[0] = seconds_since(t0);
     Result first = raise(working, plan->lowered, rot, tr, pts, grp, nr, plan->options.iterative);
+    laps[1] = seconds_since(t0);
     finish_solution(working, first);
+    laps[2] = seconds_since(t0);
     canonicalize(working, first);
+    laps[3] = seconds_since(t0);
     Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first));
+    laps[4] = seconds_since(t0);
     write_solution(*plan->problem, r, solution);
+    laps[5] = seconds_since(t0);
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr,
+                   "[omvgba] plan_solve: refine %.3fs raise %.3fs finish %.3fs canonicalize %.3fs quarantine %.3fs "
+                   "write %.3fs\n",
+                   laps[0], laps[1] - laps[0], laps[2] - laps[1], laps[3] - laps[2], laps[4] - laps[3],
+                   laps[5] - laps[4]);
     stamp_telemetry(solution->report, before, t0);
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {

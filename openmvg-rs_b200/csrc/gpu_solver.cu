@@ -29,6 +29,8 @@
 
 #include "gpu_solver.hpp"
 
+#include <thread>
+
 namespace omvgba {
 
 #define CUDA_OK(expr)                                                                                 \
@@ -1571,33 +1573,56 @@ struct TileSet {
 // a block's partials. The tile's metadata slot (layout in mv_tiles.cuh) holds the per-observation
 // segment, local point and segment-order position, the point ranges, and per segment its parameter
 // offsets and the rows of its partials.
+// Runs body(i) for i in [0, count) on up to hardware_concurrency threads, in contiguous ranges. The
+// bodies write disjoint outputs, so the result does not depend on the thread count.
+template <typename Body>
+static void host_parallel_for(size_t count, Body body) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min<size_t>(hw, count / 64 + 1);
+  const size_t per = (count + nthreads - 1) / std::max<size_t>(nthreads, 1);
+  auto run = [&](size_t k) {
+    const size_t b = std::min(count, k * per), e = std::min(count, b + per);
+    for (size_t i = b; i < e; ++i) body(i);
+  };
+  std::vector<std::thread> pool;
+  for (size_t k = 1; k < nthreads; ++k) pool.emplace_back(run, k);
+  run(0);
+  for (auto& t : pool) t.join();
+}
+
 static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
   const std::vector<int>& ent_block = setup.ent_block;
   const int nblocks = (int)setup.blk_off.size();
   const size_t slot_bytes = MvSlot::bytes(tile);
   S.tile = tile;
   size_t P = n.points.size() / 3;
-  S.tile_hdr.clear();
-  S.slots.clear();
   S.obs_rec.assign(n.obs_cam.size(), 0);
   struct SegRef {
     uint32_t tile, s;
     int bp, bi;
   };
-  std::vector<SegRef> segs;
-  std::vector<uint32_t> blk_count(nblocks, 0);
-  size_t p = 0;
-  std::vector<std::pair<uint32_t, uint16_t>> by_cam;
-  while (p < P) {
+  // whole points, in order, packed greedily into tiles of at most `tile` observations
+  std::vector<std::pair<uint32_t, uint32_t>> range;  // each tile's points [first, end)
+  for (size_t p = 0; p < P;) {
     size_t p0 = p;
     uint64_t o0 = n.pt_off[p];
     while (p < P && p - p0 < (size_t)tile && (n.pt_off[p + 1] - o0 <= (uint64_t)tile || p == p0)) ++p;
-    uint64_t o1 = n.pt_off[p];
-    if (o1 - o0 > (uint64_t)tile) throw SolveFailure{2, "a point track is longer than the matvec tile"};
+    if (n.pt_off[p] - o0 > (uint64_t)tile) throw SolveFailure{2, "a point track is longer than the matvec tile"};
+    if ((range.size() + 1) * (size_t)tile * kRec >= (1ull << 32))
+      throw SolveFailure{3, "record storage exceeds 2^32 elements"};
+    range.push_back({(uint32_t)p0, (uint32_t)p});
+  }
+  const size_t ntiles = range.size();
+  S.slots.assign(ntiles * slot_bytes, 0);
+  S.tile_hdr.assign(4 * ntiles, 0);
+  // each tile's slot, independently; its segments' blocks are kept for the partial regions
+  std::vector<std::vector<SegRef>> tile_segs(ntiles);
+  host_parallel_for(ntiles, [&](size_t t) {
+    std::vector<std::pair<uint32_t, uint16_t>> by_cam;
+    std::vector<SegRef>& segs = tile_segs[t];
+    const size_t p0 = range[t].first, p = range[t].second;
+    const uint64_t o0 = n.pt_off[p0], o1 = n.pt_off[p];
     const uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
-    const size_t t = S.tile_hdr.size() / 4;
-    if ((t + 1) * (size_t)tile * kRec >= (1ull << 32)) throw SolveFailure{3, "record storage exceeds 2^32 elements"};
-    S.slots.resize((t + 1) * slot_bytes, 0);
     unsigned char* B = S.slots.data() + t * slot_bytes;
     uint32_t* w0 = reinterpret_cast<uint32_t*>(B + MvSlot::w0(tile));
     uint32_t* w1 = reinterpret_cast<uint32_t*>(B + MvSlot::w1(tile));
@@ -1635,16 +1660,24 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
         oseg[by_cam[k].second] = (uint16_t)nseg;
       }
       segs.push_back({(uint32_t)t, nseg, pose_b, intr_b});
-      if (pose_b >= 0) blk_count[pose_b]++;
-      if (intr_b >= 0) blk_count[intr_b]++;
       ++nseg;
       i = j;
     }
     segb[nseg] = (uint16_t)nobs;
     for (uint64_t o = o0; o < o1; ++o) S.obs_rec[o] = (uint32_t)(t * (size_t)tile * kRec + (o - o0));
-    S.tile_hdr.insert(S.tile_hdr.end(), {nobs, npt, nseg, (uint32_t)p0});
-  }
+    uint32_t* hdr = &S.tile_hdr[4 * t];
+    hdr[0] = nobs;
+    hdr[1] = npt;
+    hdr[2] = nseg;
+    hdr[3] = (uint32_t)p0;
+  });
   // partial regions: block b's rows follow the blocks before it; segment rows in tile order
+  std::vector<uint32_t> blk_count(nblocks, 0);
+  for (const auto& segs : tile_segs)
+    for (const SegRef& sr : segs) {
+      if (sr.bp >= 0) blk_count[sr.bp]++;
+      if (sr.bi >= 0) blk_count[sr.bi]++;
+    }
   S.blk_part.assign(nblocks + 1, 0);
   uint64_t total = 0;
   for (int b = 0; b < nblocks; ++b) {
@@ -1654,15 +1687,16 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
   if (total >= kNoPartial) throw SolveFailure{3, "matvec partial storage exceeds 2^32 elements"};
   S.blk_part[nblocks] = (uint32_t)total;
   std::vector<uint32_t> next(nblocks, 0);
-  for (const SegRef& sr : segs) {
-    unsigned char* B = S.slots.data() + sr.tile * slot_bytes;
-    uint32_t* dpose = reinterpret_cast<uint32_t*>(B + MvSlot::dpose(tile));
-    uint32_t* dintr = reinterpret_cast<uint32_t*>(B + MvSlot::dintr(tile));
-    dpose[sr.s] = kNoPartial;
-    dintr[sr.s] = kNoPartial;
-    if (sr.bp >= 0) dpose[sr.s] = S.blk_part[sr.bp] + next[sr.bp]++ * (uint32_t)setup.blk_dim[sr.bp];
-    if (sr.bi >= 0) dintr[sr.s] = S.blk_part[sr.bi] + next[sr.bi]++ * (uint32_t)setup.blk_dim[sr.bi];
-  }
+  for (const auto& segs : tile_segs)
+    for (const SegRef& sr : segs) {
+      unsigned char* B = S.slots.data() + sr.tile * slot_bytes;
+      uint32_t* dpose = reinterpret_cast<uint32_t*>(B + MvSlot::dpose(tile));
+      uint32_t* dintr = reinterpret_cast<uint32_t*>(B + MvSlot::dintr(tile));
+      dpose[sr.s] = kNoPartial;
+      dintr[sr.s] = kNoPartial;
+      if (sr.bp >= 0) dpose[sr.s] = S.blk_part[sr.bp] + next[sr.bp]++ * (uint32_t)setup.blk_dim[sr.bp];
+      if (sr.bi >= 0) dintr[sr.s] = S.blk_part[sr.bi] + next[sr.bi]++ * (uint32_t)setup.blk_dim[sr.bi];
+    }
 }
 
 static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_pairs, Setup& S) {

@@ -29,6 +29,7 @@
 
 #include "gpu_solver.hpp"
 
+#include <atomic>
 #include <thread>
 
 namespace omvgba {
@@ -1590,6 +1591,27 @@ static void host_parallel_for(size_t count, Body body) {
   for (auto& t : pool) t.join();
 }
 
+// Runs body(chunk, begin, end) over [0, count) cut into `chunks` contiguous ranges of equal size (the
+// last shorter), on up to hardware_concurrency threads. Callers that combine per-chunk results do so
+// in chunk order, so the result does not depend on the thread count.
+template <typename Body>
+static void host_parallel_chunks(size_t count, size_t chunks, Body body) {
+  const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (size_t c; (c = next.fetch_add(1)) < chunks;) {
+      const size_t b = std::min(count, c * per), e = std::min(count, b + per);
+      body(c, b, e);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t i = 1; i < nthreads; ++i) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
 static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
   const std::vector<int>& ent_block = setup.ent_block;
   const int nblocks = (int)setup.blk_off.size();
@@ -1728,49 +1750,74 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
   S.seg_col.assign(2 * N, 0);
   S.obs_intr_col.assign(N, 0);
   std::vector<int> ent_block(2 * N, -1);
-  std::vector<uint32_t> counts(nb + 1, 0);
-  for (size_t o = 0; o < N; ++o) {
-    int c = n.obs_cam[o];
-    int pd = L.pose_dim[c];
-    if (cam_block[c] >= 0) {
-      ent_block[2 * o] = cam_block[c];
-      S.seg_col[2 * o] = 0;
-      counts[cam_block[c] + 1]++;
-    }
-    if (n.self_cal) {
-      int g = n.cam_group[c];
-      S.obs_intr_col[o] = (L.intr_dim[g] << 8) | pd;
-      if (grp_block[g] >= 0) {
-        ent_block[2 * o + 1] = grp_block[g];
-        S.seg_col[2 * o + 1] = pd;
-        counts[grp_block[g] + 1]++;
+  host_parallel_chunks(N, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t o = b; o < e; ++o) {
+      int c = n.obs_cam[o];
+      int pd = L.pose_dim[c];
+      if (cam_block[c] >= 0) {
+        ent_block[2 * o] = cam_block[c];
+        S.seg_col[2 * o] = 0;
+      }
+      if (n.self_cal) {
+        int g = n.cam_group[c];
+        S.obs_intr_col[o] = (L.intr_dim[g] << 8) | pd;
+        if (grp_block[g] >= 0) {
+          ent_block[2 * o + 1] = grp_block[g];
+          S.seg_col[2 * o + 1] = pd;
+        }
       }
     }
+  });
+  // each block's entities in entity order (a stable counting sort): per-chunk counts of every block,
+  // ranges laid out block by block and, inside a block, chunk by chunk; then each chunk fills its own
+  constexpr size_t kEntChunks = 64;
+  const size_t E = 2 * N;
+  std::vector<uint32_t> chunk_count(kEntChunks * (size_t)nb, 0);
+  host_parallel_chunks(E, kEntChunks, [&](size_t c, size_t b, size_t e) {
+    uint32_t* cc = &chunk_count[c * (size_t)nb];
+    for (size_t i = b; i < e; ++i)
+      if (ent_block[i] >= 0) cc[ent_block[i]]++;
+  });
+  std::vector<uint32_t> counts(nb + 1, 0);
+  std::vector<uint32_t> chunk_at(kEntChunks * (size_t)nb, 0);
+  {
+    uint32_t at = 0;
+    for (int b = 0; b < nb; ++b) {
+      counts[b] = at;
+      for (size_t c = 0; c < kEntChunks; ++c) {
+        chunk_at[c * (size_t)nb + b] = at;
+        at += chunk_count[c * (size_t)nb + b];
+      }
+    }
+    counts[nb] = at;
   }
-  for (int b = 0; b < nb; ++b) counts[b + 1] += counts[b];
   S.ent.assign(counts[nb], 0);
   S.ent_point.assign(counts[nb], 0);
-  std::vector<uint32_t> fill(counts.begin(), counts.end() - 1);
   std::vector<uint32_t> obs_point(N);
-  for (size_t p = 0; p < P; ++p)
-    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) obs_point[o] = (uint32_t)p;
-  for (size_t e = 0; e < 2 * N; ++e) {
-    int b = ent_block[e];
-    if (b < 0) continue;
-    uint32_t at = fill[b]++;
-    S.ent[at] = (uint32_t)e;
-    S.ent_point[at] = obs_point[e >> 1];
-  }
+  host_parallel_chunks(P, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t p = b; p < e; ++p)
+      for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) obs_point[o] = (uint32_t)p;
+  });
+  host_parallel_chunks(E, kEntChunks, [&](size_t c, size_t b, size_t e) {
+    uint32_t* fill = &chunk_at[c * (size_t)nb];
+    for (size_t i = b; i < e; ++i) {
+      const int blk = ent_block[i];
+      if (blk < 0) continue;
+      const uint32_t at = fill[blk]++;
+      S.ent[at] = (uint32_t)i;
+      S.ent_point[at] = obs_point[i >> 1];
+    }
+  });
   // intrinsic blocks have a per-observation column: stored via seg_col; blk_col = -1 means "use seg"
   // For kernels that take blk_col, intrinsic blocks read their column from obs_intr_col. To keep the
   // chunk kernel simple, split entity lists so every chunk has one column: intrinsic entities of
   // cameras with different pose dims (0, 5, 6) are grouped by column inside the block.
-  for (int b = 0; b < nb; ++b) {
-    if (S.blk_col[b] >= 0) continue;
+  host_parallel_for((size_t)nb, [&](size_t b) {
+    if (S.blk_col[b] >= 0) return;
     std::stable_sort(S.ent.begin() + counts[b], S.ent.begin() + counts[b + 1],
                      [&](uint32_t a, uint32_t c) { return S.seg_col[a] < S.seg_col[c]; });
     for (uint32_t i = counts[b]; i < counts[b + 1]; ++i) S.ent_point[i] = obs_point[S.ent[i] >> 1];
-  }
+  });
   // chunks (never mixing columns)
   S.blk_chunk_begin.assign(nb, 0);
   S.blk_chunk_end.assign(nb, 0);
@@ -1796,29 +1843,52 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
     int rb, cb;
     uint32_t p, a, b;
   };
+  // per point, in point order; point ranges run in parallel into their own lists, joined in order
+  constexpr size_t kPairChunks = 64;
+  std::vector<std::vector<Pair>> chunk_pairs(kPairChunks), chunk_xpairs(kPairChunks);
+  host_parallel_chunks(P, kPairChunks, [&](size_t c, size_t pb, size_t pe) {
+    std::vector<Pair>& pairs = chunk_pairs[c];
+    std::vector<Pair>& xpairs = chunk_xpairs[c];
+    std::vector<uint32_t> ents;
+    std::vector<int64_t> seen_at;  // point that last used each block (the same-block test)
+    if (!want_all_pairs) seen_at.assign(nb, -1);
+    for (size_t p = pb; p < pe; ++p) {
+      if (n.fixed_points[p]) continue;
+      ents.clear();
+      bool shared = false;
+      for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o)
+        for (int sgm = 0; sgm < 2; ++sgm)
+          if (ent_block[2 * o + sgm] >= 0) {
+            ents.push_back((uint32_t)(2 * o + sgm));
+            if (!want_all_pairs) {
+              int64_t& s = seen_at[ent_block[2 * o + sgm]];
+              shared = shared || s == (int64_t)p;
+              s = (int64_t)p;
+            }
+          }
+      // only same-block pairs are kept without the dense tables: none when every block is distinct
+      if (!want_all_pairs && !shared) continue;
+      for (size_t i = 0; i < ents.size(); ++i)
+        for (size_t j = 0; j <= i; ++j) {
+          uint32_t a = ents[i], b = ents[j];
+          int ba = ent_block[a], bb = ent_block[b];
+          if (ba < bb) {
+            std::swap(a, b);
+            std::swap(ba, bb);
+          }
+          if (want_all_pairs) {
+            pairs.push_back({ba, bb, (uint32_t)p, a, b});
+            // a diagonal-block pair with distinct entities contributes both orientations
+            if (ba == bb && a != b) pairs.push_back({ba, bb, (uint32_t)p, b, a});
+          }
+          if (ba == bb && a != b) xpairs.push_back({ba, bb, (uint32_t)p, a, b});
+        }
+    }
+  });
   std::vector<Pair> pairs, xpairs;
-  std::vector<uint32_t> ents;
-  for (size_t p = 0; p < P; ++p) {
-    if (n.fixed_points[p]) continue;
-    ents.clear();
-    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o)
-      for (int sgm = 0; sgm < 2; ++sgm)
-        if (ent_block[2 * o + sgm] >= 0) ents.push_back((uint32_t)(2 * o + sgm));
-    for (size_t i = 0; i < ents.size(); ++i)
-      for (size_t j = 0; j <= i; ++j) {
-        uint32_t a = ents[i], b = ents[j];
-        int ba = ent_block[a], bb = ent_block[b];
-        if (ba < bb) {
-          std::swap(a, b);
-          std::swap(ba, bb);
-        }
-        if (want_all_pairs) {
-          pairs.push_back({ba, bb, (uint32_t)p, a, b});
-          // a diagonal-block pair with distinct entities contributes both orientations
-          if (ba == bb && a != b) pairs.push_back({ba, bb, (uint32_t)p, b, a});
-        }
-        if (ba == bb && a != b) xpairs.push_back({ba, bb, (uint32_t)p, a, b});
-      }
+  for (size_t c = 0; c < kPairChunks; ++c) {
+    pairs.insert(pairs.end(), chunk_pairs[c].begin(), chunk_pairs[c].end());
+    xpairs.insert(xpairs.end(), chunk_xpairs[c].begin(), chunk_xpairs[c].end());
   }
   auto build = [&](std::vector<Pair>& v, std::vector<int>& gr, std::vector<int>& gc, std::vector<uint32_t>& gb,
                    std::vector<uint32_t>& ge, std::vector<uint32_t>& pa, std::vector<uint32_t>& pbv,

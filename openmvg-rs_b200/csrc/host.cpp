@@ -103,6 +103,27 @@ LossDev problem_loss(const omvgba_problem& pr) {
   return {kLossL2, 0.0};
 }
 
+// Runs body(chunk, begin, end) over `count` items cut into a fixed number of contiguous chunks, on
+// up to hardware_concurrency threads. Callers combine per-chunk results in chunk order, so every
+// result is independent of the thread count.
+template <typename Body>
+void for_fixed_chunks(size_t count, size_t chunks, Body body) {
+  const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (size_t c; (c = next.fetch_add(1)) < chunks;) {
+      const size_t b = std::min(count, c * per), e = std::min(count, b + per);
+      body(c, b, e);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t i = 1; i < nthreads; ++i) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
 // ---- validation ----------------------------------------------------------------------------
 void validate_problem(const omvgba_problem& pr) {
   if (pr.pose_count == 0) fail(OMVGBA_INVALID_PROBLEM, "bundle adjustment requires at least one pose");
@@ -393,10 +414,12 @@ void sort_observations(const omvgba_problem& pr, NativeProblem& n, const std::ve
   for (size_t o = 0; o < N; ++o) order[fill[pr.observation_point[o]]++] = o;
   n.obs_cam.resize(N);
   n.obs_src.resize(N);
-  for (size_t i = 0; i < N; ++i) {
-    n.obs_cam[i] = (uint32_t)dest[pr.observation_pose[order[i]]];
-    n.obs_src[i] = order[i];
-  }
+  for_fixed_chunks(N, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      n.obs_cam[i] = (uint32_t)dest[pr.observation_pose[order[i]]];
+      n.obs_src[i] = order[i];
+    }
+  });
   *order_out = std::move(order);
 }
 
@@ -542,11 +565,13 @@ Lowered lower_self_calibrating(const omvgba_problem& pr) {
   std::vector<size_t> order;
   sort_observations(pr, n, dest, &order);
   n.obs_px.resize(2 * order.size());
-  for (size_t i = 0; i < order.size(); ++i) {
-    const auto& in = pr.intrinsics[pr.observation_intrinsic[order[i]]];
-    n.obs_px[2 * i] = pr.observation_pixel[2 * order[i]] - in.cx;
-    n.obs_px[2 * i + 1] = pr.observation_pixel[2 * order[i] + 1] - in.cy;
-  }
+  for_fixed_chunks(order.size(), 64, [&](size_t, size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      const auto& in = pr.intrinsics[pr.observation_intrinsic[order[i]]];
+      n.obs_px[2 * i] = pr.observation_pixel[2 * order[i]] - in.cx;
+      n.obs_px[2 * i + 1] = pr.observation_pixel[2 * order[i] + 1] - in.cy;
+    }
+  });
   return L;
 }
 
@@ -556,32 +581,44 @@ Lowered lower_self_calibrating(const omvgba_problem& pr) {
 // camera segments. Observations stay point-major and keep their source order within a track.
 void reorder_points_for_locality(NativeProblem& n) {
   size_t P = n.points.size() / 3, N = n.obs_cam.size();
-  std::vector<uint32_t> key(P, UINT32_MAX);
-  for (size_t p = 0; p < P; ++p)
-    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) key[p] = std::min(key[p], n.obs_cam[o]);
+  // key: the smallest camera index of the track (ncam for a point without observations)
+  std::vector<uint32_t> key(P);
+  const uint32_t none = (uint32_t)n.ncam;
+  for_fixed_chunks(P, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t p = b; p < e; ++p) {
+      uint32_t k = UINT32_MAX;
+      for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) k = std::min(k, n.obs_cam[o]);
+      key[p] = std::min(k, none);
+    }
+  });
+  // stable order by key: a counting sort (equal keys keep their point order)
+  std::vector<uint64_t> start((size_t)none + 2, 0);
+  for (size_t p = 0; p < P; ++p) start[key[p] + 1]++;
+  for (size_t k = 0; k <= none; ++k) start[k + 1] += start[k];
   std::vector<uint64_t> order(P);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return key[a] < key[b]; });
+  for (size_t p = 0; p < P; ++p) order[start[key[p]]++] = p;
   std::vector<double> points(3 * P);
   std::vector<uint8_t> fixed(P);
   std::vector<uint64_t> off(P + 1, 0);
+  for (size_t q = 0; q < P; ++q) off[q + 1] = off[q] + (n.pt_off[order[q] + 1] - n.pt_off[order[q]]);
   std::vector<uint32_t> cam(N), model(n.obs_model.empty() ? 0 : N);
   std::vector<double> px(2 * N);
   std::vector<uint64_t> src(N);
-  uint64_t w = 0;
-  for (size_t q = 0; q < P; ++q) {
-    uint64_t p = order[q];
-    for (int k = 0; k < 3; ++k) points[3 * q + k] = n.points[3 * p + k];
-    fixed[q] = n.fixed_points[p];
-    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o, ++w) {
-      cam[w] = n.obs_cam[o];
-      if (!model.empty()) model[w] = n.obs_model[o];
-      px[2 * w] = n.obs_px[2 * o];
-      px[2 * w + 1] = n.obs_px[2 * o + 1];
-      src[w] = n.obs_src[o];
+  for_fixed_chunks(P, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t q = b; q < e; ++q) {
+      uint64_t p = order[q];
+      for (int k = 0; k < 3; ++k) points[3 * q + k] = n.points[3 * p + k];
+      fixed[q] = n.fixed_points[p];
+      uint64_t w = off[q];
+      for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o, ++w) {
+        cam[w] = n.obs_cam[o];
+        if (!model.empty()) model[w] = n.obs_model[o];
+        px[2 * w] = n.obs_px[2 * o];
+        px[2 * w + 1] = n.obs_px[2 * o + 1];
+        src[w] = n.obs_src[o];
+      }
     }
-    off[q + 1] = w;
-  }
+  });
   n.points.swap(points);
   n.fixed_points.swap(fixed);
   n.pt_off.swap(off);
@@ -679,26 +716,6 @@ bool residual_norm(const omvgba_problem& pr, const StateView& sv, size_t o, cons
 bool active_metrics(const omvgba_problem& pr, const std::vector<uint8_t>& active, const Result* sol, double* cost,
                     double* rmse);
 
-// Runs body(chunk, begin, end) over `count` items cut into a fixed number of contiguous chunks, on
-// up to hardware_concurrency threads. Callers combine per-chunk results in chunk order, so every
-// result is independent of the thread count.
-template <typename Body>
-void for_fixed_chunks(size_t count, size_t chunks, Body body) {
-  const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
-  std::atomic<size_t> next{0};
-  auto worker = [&]() {
-    for (size_t c; (c = next.fetch_add(1)) < chunks;) {
-      const size_t b = std::min(count, c * per), e = std::min(count, b + per);
-      body(c, b, e);
-    }
-  };
-  std::vector<std::thread> pool;
-  for (size_t i = 1; i < nthreads; ++i) pool.emplace_back(worker);
-  worker();
-  for (auto& t : pool) t.join();
-}
 
 // Inlier count and RMSE of the solution (solver.rs:1317-1402): residual norms of the active
 // observations within the loss scale (every one for squared loss). 64 fixed chunks.
@@ -1102,23 +1119,52 @@ void without_points(const omvgba_problem& pr, const Result* warm, const std::set
       r.intrinsics[i].certification = c;
     }
   }
+  std::vector<uint8_t> drop(pr.point_count, 0);
+  size_t ndrop = 0;
+  for (size_t i : dropped)
+    if (i < pr.point_count) {
+      drop[i] = 1;
+      ++ndrop;
+    }
   std::vector<size_t> ni(pr.point_count, SIZE_MAX);
   r.kept.clear();
+  r.kept.reserve(pr.point_count - ndrop);
+  r.points.reserve(r.points.size() + 3 * (pr.point_count - ndrop));
+  r.fixed.reserve(r.fixed.size() + pr.point_count - ndrop);
   for (size_t i = 0; i < pr.point_count; ++i) {
-    if (dropped.count(i)) continue;
+    if (drop[i]) continue;
     ni[i] = r.kept.size();
     r.kept.push_back(i);
     for (int k = 0; k < 3; ++k) r.points.push_back(warm ? warm->points[3 * i + k] : pr.points[3 * i + k]);
     r.fixed.push_back(point_fixed(pr, i) ? 1 : 0);
   }
-  for (size_t o = 0; o < pr.observation_count; ++o) {
-    if (ni[pr.observation_point[o]] == SIZE_MAX) continue;
-    r.op.push_back(pr.observation_pose[o]);
-    r.oi.push_back(pr.observation_intrinsic[o]);
-    r.opt.push_back((uint32_t)ni[pr.observation_point[o]]);
-    r.px.push_back(pr.observation_pixel[2 * o]);
-    r.px.push_back(pr.observation_pixel[2 * o + 1]);
-  }
+  // the observations of kept points, in order: per-chunk counts, then each chunk fills its range
+  constexpr size_t kChunks = 64;
+  std::vector<size_t> at(kChunks + 1, 0);
+  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    size_t k = 0;
+    for (size_t o = b; o < e; ++o) k += ni[pr.observation_point[o]] != SIZE_MAX;
+    at[c + 1] = k;
+  });
+  for (size_t c = 0; c < kChunks; ++c) at[c + 1] += at[c];
+  const size_t base = r.op.size(), M = at[kChunks];
+  r.op.resize(base + M);
+  r.oi.resize(base + M);
+  r.opt.resize(base + M);
+  r.px.resize(2 * (base + M));
+  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
+    size_t w = base + at[c];
+    for (size_t o = b; o < e; ++o) {
+      const size_t q = ni[pr.observation_point[o]];
+      if (q == SIZE_MAX) continue;
+      r.op[w] = pr.observation_pose[o];
+      r.oi[w] = pr.observation_intrinsic[o];
+      r.opt[w] = (uint32_t)q;
+      r.px[2 * w] = pr.observation_pixel[2 * o];
+      r.px[2 * w + 1] = pr.observation_pixel[2 * o + 1];
+      ++w;
+    }
+  });
   r.view = pr;
   r.view.poses = r.poses.data();
   r.view.intrinsics = r.intrinsics.data();

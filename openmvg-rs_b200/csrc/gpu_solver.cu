@@ -209,6 +209,19 @@ struct DBuf {
   ~DBuf() { release(); }
 };
 
+// Uploads v, or, when v holds fewer than min_count elements, a zero-padded copy of it (device
+// tables are never empty); a long enough table goes up from its own storage without a host copy.
+template <typename T>
+void upload_padded(DBuf<T>& b, const std::vector<T>& v, size_t min_count, cudaStream_t st) {
+  if (v.size() >= min_count) {
+    b.upload(v.data(), v.size(), st);
+    return;
+  }
+  std::vector<T> padded(v);
+  padded.resize(min_count, T{});
+  b.upload(padded.data(), padded.size(), st);
+}
+
 // ----------------------------------------------------------------------------------------------
 // Device problem view
 // ----------------------------------------------------------------------------------------------
@@ -1934,17 +1947,12 @@ struct TileSetDev {
   DBuf<double> partial;
   int ntiles = 0;
   void upload(const TileSet& t, cudaStream_t st) {
-    auto up = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) {
-      std::vector<uint32_t> x = v;
-      if (x.empty()) x.assign(4, 0);
-      b.upload(x.data(), x.size(), st);
-    };
+    // an empty table goes up as 4 zeros (the slots as 16 zero bytes)
+    auto up = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) { upload_padded(b, v, v.empty() ? 4 : 0, st); };
     up(tile_hdr, t.tile_hdr);
     up(blk_part, t.blk_part);
     up(obs_rec, t.obs_rec);
-    std::vector<unsigned char> b = t.slots;
-    b.resize(std::max<size_t>(b.size(), 16));
-    slots.upload(b.data(), b.size(), st);
+    upload_padded(slots, t.slots, 16, st);
     partial.alloc(std::max<size_t>(1, t.blk_part.empty() ? 1 : t.blk_part.back()), st);
     ntiles = (int)(t.tile_hdr.size() / 4);
   }
@@ -2115,9 +2123,7 @@ struct Solver {
     d_pt_off.upload(pt_off.data(), pt_off.size(), st);
     d_obs_cam.upload(n.obs_cam.data(), n.obs_cam.size(), st);
     d_obs_px.upload(n.obs_px.data(), n.obs_px.size(), st);
-    std::vector<uint32_t> om = n.obs_model;
-    if (om.empty()) om.assign(1, 0);
-    d_obs_model.upload(om.data(), om.size(), st);
+    upload_padded(d_obs_model, n.obs_model, 1, st);
     std::vector<FixedCameraDev> models = n.models;
     if (models.empty()) models.resize(1);
     d_models.upload(models.data(), models.size(), st);
@@ -2160,16 +2166,8 @@ struct Solver {
     d_ddiag.zero();
     d_summary.alloc(P, st);
     d_summary_part.alloc(red_blocks, st);
-    auto up_i = [&](DBuf<int>& b, const std::vector<int>& v) {
-      std::vector<int> t = v;
-      if (t.empty()) t.push_back(0);
-      b.upload(t.data(), t.size(), st);
-    };
-    auto up_u = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) {
-      std::vector<uint32_t> t = v;
-      if (t.empty()) t.push_back(0);
-      b.upload(t.data(), t.size(), st);
-    };
+    auto up_i = [&](DBuf<int>& b, const std::vector<int>& v) { upload_padded(b, v, 1, st); };
+    auto up_u = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) { upload_padded(b, v, 1, st); };
     up_i(d_blk_off, S.blk_off);
     up_i(d_blk_dim, S.blk_dim);
     std::vector<int> col = S.blk_col;

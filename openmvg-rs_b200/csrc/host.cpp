@@ -1532,6 +1532,7 @@ int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, con
     Result r = solve_with_quarantine(context->ctx, *problem, *config);
     write_solution(*problem, r, solution);
     stamp_telemetry(solution->report, before, t0);
+    if (std::getenv("OMVGBA_PHASE_TIMES")) std::fprintf(stderr, "[omvgba] omvgba_solve %.3fs\n", seconds_since(t0));
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {
     return write_error(error, f.code, f.message);

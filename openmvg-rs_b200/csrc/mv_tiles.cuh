@@ -163,11 +163,9 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
     T xv[kSegParams];
 #pragma unroll
     for (int c = 0; c < kSegParams; ++c) {
-      double v = 0.0;
-      if ((uint32_t)c < pd)
-        v = __ldg(x + (my_w0 & 0x0FFFFFFFu) + c);
-      else if ((uint32_t)c - pd < id)
-        v = __ldg(x + (my_w1 & 0x0FFFFFFFu) + (c - pd));
+      // one predicated load per column (pose columns, then intrinsic columns, then zeros)
+      const uint32_t at = (uint32_t)c < pd ? (my_w0 & 0x0FFFFFFFu) + c : (my_w1 & 0x0FFFFFFFu) + ((uint32_t)c - pd);
+      const double v = (uint32_t)c < pd + id ? __ldg(x + at) : 0.0;
       xv[c] = (T)v;
     }
     if ((uint32_t)tid < nseg) {

@@ -28,6 +28,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -115,7 +116,10 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.device_index = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        # the raw samples go to OMVGBA_CLOCKS_DIR (default: the temporary directory); the JSON line
+        # carries their summary
+        clock_dir = os.environ.get("OMVGBA_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(clock_dir, f"clocks_rank{device_index}.csv")
 
     def start(self):
         try:

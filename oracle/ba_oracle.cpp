@@ -5,8 +5,7 @@
 //
 // Parity pins: the Rust reference cannot be built here (no toolchain), so this restatement is pinned
 // against the reference's unit-test known answers and central differences (tests/test_oracle_pins.py)
-// and against fixtures it generated itself (tests/golden/). Deviations from the reference are listed
-// in DESIGN.md ("Oracle scope").
+// and against fixtures it generated itself (tests/golden/).
 //
 // File map (reference paths relative to the openmvg-rs root):
 //   lowering .......... native/mod.rs:235-367, native/gauge.rs:123-330, native/world_rebase.rs:19-87,

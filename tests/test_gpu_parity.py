@@ -14,7 +14,7 @@ def _rel(a, b):
 
 def _oracle_spread(problem, cfg):
     """The oracle's own parameter sensitivity: solve again with a different (fixed) grouping of its
-    floating-point sums. GPU-vs-oracle differences are judged against this rounding floor."""
+    floating-point sums. GPU-vs-oracle differences are measured against this rounding floor."""
     O.set_shards(7)
     try:
         return O.solve(problem, cfg)

@@ -1067,14 +1067,17 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
 // ---- quarantine --------------------------------------------------------------------------------
 std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pose* poses, const double* points) {
   size_t N = pr.observation_count;
-  std::vector<Vec3> off(N);
+  // the ray from the camera centre to the point (recomputed where it is used, bit for bit)
+  auto offset = [&](size_t o) -> Vec3 {
+    const size_t p = pr.observation_point[o];
+    const double* C = poses[pr.observation_pose[o]].center;
+    return {points[3 * p] - C[0], points[3 * p + 1] - C[1], points[3 * p + 2] - C[2]};
+  };
   std::vector<double> dist(N);
   for_fixed_chunks(N, 64, [&](size_t, size_t b, size_t e) {
     for (size_t o = b; o < e; ++o) {
-      size_t p = pr.observation_point[o];
-      const double* C = poses[pr.observation_pose[o]].center;
-      off[o] = {points[3 * p] - C[0], points[3 * p + 1] - C[1], points[3 * p + 2] - C[2]};
-      dist[o] = std::sqrt(off[o][0] * off[o][0] + off[o][1] * off[o][1] + off[o][2] * off[o][2]);
+      const Vec3 v = offset(o);
+      dist[o] = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     }
   });
   double scene = 0.0;
@@ -1084,7 +1087,10 @@ std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pos
   }
   std::vector<TrackGeometryDev> geo(pr.point_count);
   for (auto& g : geo) g.init(scene);
-  for (size_t o = 0; o < N; ++o) geo[pr.observation_point[o]].push(off[o][0], off[o][1], off[o][2]);
+  for (size_t o = 0; o < N; ++o) {
+    const Vec3 v = offset(o);
+    geo[pr.observation_point[o]].push(v[0], v[1], v[2]);
+  }
   std::vector<size_t> out;
   for (size_t p = 0; p < pr.point_count; ++p)
     if (geo[p].degenerate()) out.push_back(p);

@@ -290,6 +290,17 @@ int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* pr
                                omvgba_error* error);
 
 /*
+ * Digest (64-bit FNV-1a) of the host side of a solve's set-up: the quarantine preparation (points
+ * held out before the solve, native/mod.rs:260-340, quarantine.rs:34-96), the lowering
+ * (native/self_calibration.rs:47-198, native/calibrated.rs:200-494) and the block tables and
+ * matvec tiles the solver uploads, built with at most `threads` host threads (0: all of them).
+ * Uses no GPU and needs no context. The set-up's result does not depend on the thread count (the
+ * reference's reproducibility rule); this entry point exists to test that.
+ */
+int32_t omvgba_debug_setup_digest(const omvgba_problem* problem, const omvgba_config* config, uint32_t threads,
+                                  uint64_t* digest, omvgba_error* error);
+
+/*
  * Reduced camera system product S_lambda x at the first linearization of the lowered problem,
  * computed twice: by the matrix-free kernel the PCG uses (y_matvec) and from the explicit dense
  * Schur complement (y_dense). With x == NULL only *dimension is written. FP64; for operator

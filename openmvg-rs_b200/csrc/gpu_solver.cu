@@ -1587,11 +1587,17 @@ struct TileSet {
 // a block's partials. The tile's metadata slot (layout in mv_tiles.cuh) holds the per-observation
 // segment, local point and segment-order position, the point ranges, and per segment its parameter
 // offsets and the rows of its partials.
-// Runs body(i) for i in [0, count) on up to hardware_concurrency threads, in contiguous ranges. The
+thread_local unsigned tl_host_threads = 0;  // 0: hardware_concurrency
+void set_host_thread_limit(unsigned threads) { tl_host_threads = threads; }
+unsigned host_thread_limit() {
+  return tl_host_threads ? tl_host_threads : std::max(1u, std::thread::hardware_concurrency());
+}
+
+// Runs body(i) for i in [0, count) on up to host_thread_limit() threads, in contiguous ranges. The
 // bodies write disjoint outputs, so the result does not depend on the thread count.
 template <typename Body>
 static void host_parallel_for(size_t count, Body body) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned hw = host_thread_limit();
   const size_t nthreads = std::min<size_t>(hw, count / 64 + 1);
   const size_t per = (count + nthreads - 1) / std::max<size_t>(nthreads, 1);
   auto run = [&](size_t k) {
@@ -1605,12 +1611,12 @@ static void host_parallel_for(size_t count, Body body) {
 }
 
 // Runs body(chunk, begin, end) over [0, count) cut into `chunks` contiguous ranges of equal size (the
-// last shorter), on up to hardware_concurrency threads. Callers that combine per-chunk results do so
+// last shorter), on up to host_thread_limit() threads. Callers that combine per-chunk results do so
 // in chunk order, so the result does not depend on the thread count.
 template <typename Body>
 static void host_parallel_chunks(size_t count, size_t chunks, Body body) {
   const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned hw = host_thread_limit();
   const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
   std::atomic<size_t> next{0};
   auto worker = [&]() {
@@ -1938,6 +1944,34 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
   for (int b = 0; b < nb; ++b)
     if (S.blk_cross_end[b] == 0) S.blk_cross_begin[b] = 0;
   S.ent_block = std::move(ent_block);
+}
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h) {
+  const unsigned char* c = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < bytes; ++i) h = (h ^ c[i]) * 1099511628211ull;
+  return h;
+}
+
+uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
+  const Layout L = make_layout(n);
+  const bool direct = !opt.iterative;
+  Setup S;
+  build_tables(n, L, direct || L.D <= opt.dense_rank_limit, S);
+  TileSet T;
+  const bool mixed = opt.precision == 1 && !direct;
+  build_tiles(n, L, S, mixed ? mv_tile_obs<float>() : mv_tile_obs<double>(), T);
+  uint64_t h = 1469598103934665603ull;
+  auto add = [&](const auto& v) { h = fnv1a(v.data(), v.size() * sizeof(v[0]), h); };
+  for (const auto* v : {&S.blk_off, &S.blk_dim, &S.blk_col, &S.blk_edge, &S.chunk_block, &S.chunk_col,
+                        &S.blk_chunk_begin, &S.blk_chunk_end, &S.obs_intr_col, &S.seg_col, &S.grp_row, &S.grp_col,
+                        &S.xgrp_row, &S.xgrp_col, &S.blk_cross_begin, &S.blk_cross_end, &S.ent_block})
+    add(*v);
+  for (const auto* v : {&S.ent, &S.ent_point, &S.chunk_begin, &S.chunk_end, &S.grp_begin, &S.grp_end, &S.pair_a,
+                        &S.pair_b, &S.pair_p, &S.xgrp_begin, &S.xgrp_end, &S.xpair_a, &S.xpair_b, &S.xpair_p,
+                        &T.tile_hdr, &T.blk_part, &T.obs_rec})
+    add(*v);
+  add(T.slots);
+  return h;
 }
 
 // Device copy of a TileSet plus the fused-matvec launch shape.

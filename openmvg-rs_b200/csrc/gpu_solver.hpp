@@ -110,6 +110,17 @@ void resident_schur_product(Resident* resident, double lambda, bool fp32, int st
 // Kernels launched and host<->device bytes copied by the calling thread so far.
 void telemetry_read(uint64_t* launches, uint64_t* h2d, uint64_t* d2h);
 
+// Host threads that the set-up run by the calling thread may use (0: hardware_concurrency). Every
+// parallel host loop writes disjoint outputs or combines per-chunk results in chunk order, so the
+// result does not depend on this; it exists so that this can be tested.
+void set_host_thread_limit(unsigned threads);
+unsigned host_thread_limit();
+// FNV-1a digest of the host-built device set-up of a lowered problem: the block tables and the
+// matvec tiles in the precision the options select. Uses no GPU.
+uint64_t setup_digest(const NativeProblem& problem, const LmOptions& options);
+// FNV-1a over bytes, continuing from h.
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h);
+
 // Residual norms of an input problem's observations with a world-frame state, for the Solution
 // metrics (solver.rs:1052-1131). active: per point flag. Returns false when a projection fails.
 struct WorldMetrics {

@@ -104,12 +104,12 @@ LossDev problem_loss(const omvgba_problem& pr) {
 }
 
 // Runs body(chunk, begin, end) over `count` items cut into a fixed number of contiguous chunks, on
-// up to hardware_concurrency threads. Callers combine per-chunk results in chunk order, so every
+// up to host_thread_limit() threads. Callers combine per-chunk results in chunk order, so every
 // result is independent of the thread count.
 template <typename Body>
 void for_fixed_chunks(size_t count, size_t chunks, Body body) {
   const size_t per = (count + chunks - 1) / std::max<size_t>(chunks, 1);
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned hw = host_thread_limit();
   const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, chunks), count / 65536 + 1);
   std::atomic<size_t> next{0};
   auto worker = [&]() {
@@ -1630,6 +1630,54 @@ int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* pr
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {
     return write_error(error, f.code, f.message);
+  }
+}
+
+// Debug: digest of the host side of a solve's set-up (quarantine preparation, lowering, block
+// tables and matvec tiles) built with at most `threads` host threads (0: all); uses no GPU. Every
+// parallel loop of the set-up is arranged so that this does not depend on `threads`.
+int32_t omvgba_debug_setup_digest(const omvgba_problem* problem, const omvgba_config* config, uint32_t threads,
+                                  uint64_t* digest, omvgba_error* error) {
+  clear_error(error);
+  if (!problem || !config || !digest) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  struct Limit {
+    explicit Limit(unsigned t) { set_host_thread_limit(t); }
+    ~Limit() { set_host_thread_limit(0); }
+  } limit(threads);
+  try {
+    validate_problem(*problem);
+    validate_config(*config);
+    Prepared prep;
+    prepare_quarantine(*problem, *config, prep);
+    const omvgba_problem& w = *prep.working;
+    Lowered L = lower(w);
+    LmOptions opt = lm_options(w, *config, L.n);
+    const NativeProblem& n = L.n;
+    uint64_t h = 1469598103934665603ull;
+    auto add = [&](const void* p, size_t bytes) { h = fnv1a(p, bytes, h); };
+    add(prep.kept.data(), sizeof(size_t) * prep.kept.size());
+    add(w.points, sizeof(double) * 3 * w.point_count);
+    add(w.observation_pose, sizeof(uint32_t) * w.observation_count);
+    add(w.observation_intrinsic, sizeof(uint32_t) * w.observation_count);
+    add(w.observation_point, sizeof(uint32_t) * w.observation_count);
+    add(w.observation_pixel, sizeof(double) * 2 * w.observation_count);
+    add(n.points.data(), sizeof(double) * n.points.size());
+    add(n.fixed_points.data(), n.fixed_points.size());
+    add(n.pt_off.data(), sizeof(uint64_t) * n.pt_off.size());
+    add(n.obs_cam.data(), sizeof(uint32_t) * n.obs_cam.size());
+    add(n.obs_px.data(), sizeof(double) * n.obs_px.size());
+    add(n.obs_src.data(), sizeof(uint64_t) * n.obs_src.size());
+    add(n.point_source.data(), sizeof(uint64_t) * n.point_source.size());
+    add(n.rotation.data(), sizeof(double) * n.rotation.size());
+    add(n.translation.data(), sizeof(double) * n.translation.size());
+    const uint64_t tables = setup_digest(n, opt);
+    add(&tables, sizeof(tables));
+    *digest = h;
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
   }
 }
 

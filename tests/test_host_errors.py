@@ -1,8 +1,9 @@
 """Problem validation and the lowering's unsupported cases run on the host before any device work,
-so their error behaviour is checked on the CPU: for each malformed or unsupported problem the
-library, through omvgba_debug_setup_digest (validation, quarantine preparation and lowering without
-a GPU), returns the same error code as the oracle's solve (problem.rs:470-577,
-native/mod.rs:235-367, quarantine.rs:34-96), and a valid problem passes both."""
+so their error behaviour is checked on the CPU: for each malformed or unsupported problem, and each
+invalid configuration, the library, through omvgba_debug_setup_digest (validation, quarantine
+preparation and lowering without a GPU), returns the same error code as the oracle's solve
+(problem.rs:470-577, solver.rs:122-155, native/mod.rs:235-367, quarantine.rs:34-96), and a valid
+problem passes both."""
 import ctypes as C
 import dataclasses
 
@@ -101,3 +102,19 @@ def test_invalid_problem_gets_the_oracles_error(ring, name):
 
 def test_valid_problem_passes_the_host_checks(ring):
     assert _lib_code(ring, SolveConfig()) == abi.OMVGBA_OK
+
+
+CONFIG_CASES = {
+    "no iterations": dict(max_iterations=0),
+    "zero function tolerance": dict(function_tolerance=0.0),
+    "non-finite gradient tolerance": dict(gradient_tolerance=float("nan")),
+    "negative parameter tolerance": dict(parameter_tolerance=-1.0),
+    "zero workspace budget": dict(workspace_budget_bytes=0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CONFIG_CASES))
+def test_invalid_config_gets_the_oracles_error(ring, name):
+    cfg = dataclasses.replace(SolveConfig(), **CONFIG_CASES[name])
+    assert _oracle_code(ring, cfg) == abi.OMVGBA_INVALID_CONFIG
+    assert _lib_code(ring, cfg) == abi.OMVGBA_INVALID_CONFIG

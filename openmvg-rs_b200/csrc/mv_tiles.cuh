@@ -72,13 +72,9 @@ struct MvTiles {
   int prefetch_ahead;          // tiles ahead (about one resident wave) whose records are prefetched
 };
 
-// Bulk prefetch of global memory into L2 (a hint: nothing waits for it). bytes % 16 == 0.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
 // The records are read once per product and are larger than L2; an evict-first policy on their
 // prefetch and loads keeps the data that every product re-reads (slots, point blocks, x) resident.
+// The bulk prefetch into L2 is a hint (nothing waits for it); bytes % 16 == 0.
 __device__ __forceinline__ uint64_t l2_evict_first() {
   uint64_t pol;
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));

@@ -211,13 +211,13 @@ struct DBuf {
 
 // Uploads v, or, when v holds fewer than min_count elements, a zero-padded copy of it (device
 // tables are never empty); a long enough table goes up from its own storage without a host copy.
-template <typename T>
-void upload_padded(DBuf<T>& b, const std::vector<T>& v, size_t min_count, cudaStream_t st) {
+template <typename T, typename A>
+void upload_padded(DBuf<T>& b, const std::vector<T, A>& v, size_t min_count, cudaStream_t st) {
   if (v.size() >= min_count) {
     b.upload(v.data(), v.size(), st);
     return;
   }
-  std::vector<T> padded(v);
+  std::vector<T> padded(v.begin(), v.end());
   padded.resize(min_count, T{});
   b.upload(padded.data(), padded.size(), st);
 }
@@ -1556,7 +1556,7 @@ static Layout make_layout(const NativeProblem& n) {
 struct Setup {
   // block tables (host copies)
   std::vector<int> blk_off, blk_dim, blk_col, blk_edge;
-  std::vector<uint32_t> ent, ent_point;
+  FillVector<uint32_t> ent, ent_point;  // written completely by the construction
   std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
   std::vector<uint32_t> chunk_begin, chunk_end;
   std::vector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment
@@ -1577,7 +1577,7 @@ struct TileSet {
   std::vector<uint32_t> tile_hdr;  // 4 per tile: observations, points, segments, first point
   std::vector<unsigned char> slots;
   std::vector<uint32_t> blk_part;  // nblocks + 1
-  std::vector<uint32_t> obs_rec;   // element index of each observation's record component 0
+  FillVector<uint32_t> obs_rec;    // element index of each observation's record component 0 (all written)
 };
 
 // Tiles of whole points with at most `tile` observations. A tile's observations are grouped by
@@ -1637,7 +1637,7 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
   const size_t slot_bytes = MvSlot::bytes(tile);
   S.tile = tile;
   size_t P = n.points.size() / 3;
-  S.obs_rec.assign(n.obs_cam.size(), 0);
+  S.obs_rec.resize(n.obs_cam.size());  // every observation lies in exactly one tile
   struct SegRef {
     uint32_t tile, s;
     int bp, bi;
@@ -1810,9 +1810,9 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
     }
     counts[nb] = at;
   }
-  S.ent.assign(counts[nb], 0);
-  S.ent_point.assign(counts[nb], 0);
-  std::vector<uint32_t> obs_point(N);
+  S.ent.resize(counts[nb]);  // the fill below writes every position
+  S.ent_point.resize(counts[nb]);
+  FillVector<uint32_t> obs_point(N);
   host_parallel_chunks(P, 64, [&](size_t, size_t b, size_t e) {
     for (size_t p = b; p < e; ++p)
       for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) obs_point[o] = (uint32_t)p;
@@ -1966,9 +1966,12 @@ uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
                         &S.blk_chunk_begin, &S.blk_chunk_end, &S.obs_intr_col, &S.seg_col, &S.grp_row, &S.grp_col,
                         &S.xgrp_row, &S.xgrp_col, &S.blk_cross_begin, &S.blk_cross_end, &S.ent_block})
     add(*v);
-  for (const auto* v : {&S.ent, &S.ent_point, &S.chunk_begin, &S.chunk_end, &S.grp_begin, &S.grp_end, &S.pair_a,
+  add(S.ent);
+  add(S.ent_point);
+  add(T.obs_rec);
+  for (const auto* v : {&S.chunk_begin, &S.chunk_end, &S.grp_begin, &S.grp_end, &S.pair_a,
                         &S.pair_b, &S.pair_p, &S.xgrp_begin, &S.xgrp_end, &S.xpair_a, &S.xpair_b, &S.xpair_p,
-                        &T.tile_hdr, &T.blk_part, &T.obs_rec})
+                        &T.tile_hdr, &T.blk_part})
     add(*v);
   add(T.slots);
   return h;
@@ -1982,7 +1985,7 @@ struct TileSetDev {
   int ntiles = 0;
   void upload(const TileSet& t, cudaStream_t st) {
     // an empty table goes up as 4 zeros (the slots as 16 zero bytes)
-    auto up = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) { upload_padded(b, v, v.empty() ? 4 : 0, st); };
+    auto up = [&](DBuf<uint32_t>& b, const auto& v) { upload_padded(b, v, v.empty() ? 4 : 0, st); };
     up(tile_hdr, t.tile_hdr);
     up(blk_part, t.blk_part);
     up(obs_rec, t.obs_rec);
@@ -2201,7 +2204,7 @@ struct Solver {
     d_summary.alloc(P, st);
     d_summary_part.alloc(red_blocks, st);
     auto up_i = [&](DBuf<int>& b, const std::vector<int>& v) { upload_padded(b, v, 1, st); };
-    auto up_u = [&](DBuf<uint32_t>& b, const std::vector<uint32_t>& v) { upload_padded(b, v, 1, st); };
+    auto up_u = [&](DBuf<uint32_t>& b, const auto& v) { upload_padded(b, v, 1, st); };
     up_i(d_blk_off, S.blk_off);
     up_i(d_blk_dim, S.blk_dim);
     std::vector<int> col = S.blk_col;

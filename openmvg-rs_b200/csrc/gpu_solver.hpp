@@ -4,6 +4,9 @@
 
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "ba_device.cuh"
@@ -17,20 +20,44 @@ struct SolveFailure {
 };
 
 // The problem after native lowering (anchor frame, point-major observations, native camera order).
+// Allocator whose value-less construct() default-initializes: resize() of a vector of a trivial
+// type then leaves the new elements unwritten. For large host buffers that are filled completely
+// right after allocation (by parallel loops), so that they are not first zeroed by one thread.
+template <typename T>
+struct DefaultInitAllocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = DefaultInitAllocator<U>;
+  };
+  DefaultInitAllocator() noexcept = default;
+  template <typename U>
+  DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using FillVector = std::vector<T, DefaultInitAllocator<T>>;
+
 struct NativeProblem {
   bool self_cal = false;
   int ncam = 0;
   std::vector<double> rotation;     // ncam x 9 (row-major, world -> camera in the anchor frame)
   std::vector<double> translation;  // ncam x 3
-  std::vector<double> points;       // P x 3
+  FillVector<double> points;        // P x 3
   std::vector<uint8_t> fixed_points;
   std::vector<uint8_t> fixed_poses;
-  std::vector<uint32_t> obs_cam;    // native camera per observation (point-major order)
-  std::vector<double> obs_px;       // N x 2 (self-calibration: centred at the principal point)
-  std::vector<uint64_t> obs_src;    // input observation index
-  std::vector<uint32_t> obs_model;  // calibrated: fixed camera model per observation
-  std::vector<uint64_t> pt_off;     // P + 1
-  std::vector<uint64_t> point_source;  // native point -> input point (points are regrouped for locality)
+  FillVector<uint32_t> obs_cam;     // native camera per observation (point-major order)
+  FillVector<double> obs_px;        // N x 2 (self-calibration: centred at the principal point)
+  FillVector<uint64_t> obs_src;     // input observation index
+  FillVector<uint32_t> obs_model;   // calibrated: fixed camera model per observation
+  FillVector<uint64_t> pt_off;      // P + 1
+  FillVector<uint64_t> point_source;  // native point -> input point (points are regrouped for locality)
   bool pixel_model = true;          // pinhole pixel projection (no distortion anywhere)
   std::vector<FixedCameraDev> models;
   std::vector<double> groups;       // self-calibration: ng x 3 (focal, k1, k2)

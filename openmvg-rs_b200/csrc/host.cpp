@@ -404,12 +404,12 @@ bool single_pose_intrinsics(const omvgba_problem& pr, std::vector<size_t>* out) 
 
 // point-major CSR with a stable sort by point (counting sort keeps source order within a track)
 void sort_observations(const omvgba_problem& pr, NativeProblem& n, const std::vector<size_t>& dest,
-                       std::vector<size_t>* order_out) {
+                       FillVector<size_t>* order_out) {
   size_t N = pr.observation_count, P = pr.point_count;
   n.pt_off.assign(P + 1, 0);
   for (size_t o = 0; o < N; ++o) n.pt_off[pr.observation_point[o] + 1]++;
   for (size_t p = 0; p < P; ++p) n.pt_off[p + 1] += n.pt_off[p];
-  std::vector<size_t> order(N);
+  FillVector<size_t> order(N);  // every position is written below
   std::vector<uint64_t> fill(n.pt_off.begin(), n.pt_off.end() - 1);
   for (size_t o = 0; o < N; ++o) order[fill[pr.observation_point[o]]++] = o;
   n.obs_cam.resize(N);
@@ -477,7 +477,7 @@ Lowered lower_calibrated(const omvgba_problem& pr) {
   n.pixel_model = !uses_full;
   for (size_t i = 0; i < pr.intrinsic_count; ++i) n.models.push_back(make_fixed_camera(pr.intrinsics[i]));
   n.gauge_cam = plan.native_cam >= 0 ? (int)dest[plan.native_cam] : -1;
-  std::vector<size_t> order;
+  FillVector<size_t> order;
   sort_observations(pr, n, dest, &order);
   n.obs_px.resize(2 * order.size());
   n.obs_model.resize(order.size());
@@ -562,7 +562,7 @@ Lowered lower_self_calibrating(const omvgba_problem& pr) {
     n.group_dim.push_back(in.variables == 0 ? 0 : free_radial_dimension(in));
   }
   n.gauge_cam = plan.native_cam >= 0 ? (int)dest[plan.native_cam] : -1;
-  std::vector<size_t> order;
+  FillVector<size_t> order;
   sort_observations(pr, n, dest, &order);
   n.obs_px.resize(2 * order.size());
   for_fixed_chunks(order.size(), 64, [&](size_t, size_t b, size_t e) {
@@ -595,15 +595,15 @@ void reorder_points_for_locality(NativeProblem& n) {
   std::vector<uint64_t> start((size_t)none + 2, 0);
   for (size_t p = 0; p < P; ++p) start[key[p] + 1]++;
   for (size_t k = 0; k <= none; ++k) start[k + 1] += start[k];
-  std::vector<uint64_t> order(P);
+  FillVector<uint64_t> order(P);  // every array below is written completely before it is read
   for (size_t p = 0; p < P; ++p) order[start[key[p]]++] = p;
-  std::vector<double> points(3 * P);
+  FillVector<double> points(3 * P);
   std::vector<uint8_t> fixed(P);
-  std::vector<uint64_t> off(P + 1, 0);
+  FillVector<uint64_t> off(P + 1, 0);
   for (size_t q = 0; q < P; ++q) off[q + 1] = off[q] + (n.pt_off[order[q] + 1] - n.pt_off[order[q]]);
-  std::vector<uint32_t> cam(N), model(n.obs_model.empty() ? 0 : N);
-  std::vector<double> px(2 * N);
-  std::vector<uint64_t> src(N);
+  FillVector<uint32_t> cam(N), model(n.obs_model.empty() ? 0 : N);
+  FillVector<double> px(2 * N);
+  FillVector<uint64_t> src(N);
   for_fixed_chunks(P, 64, [&](size_t, size_t b, size_t e) {
     for (size_t q = b; q < e; ++q) {
       uint64_t p = order[q];
@@ -1102,8 +1102,8 @@ struct Restricted {
   std::vector<omvgba_intrinsic> intrinsics;
   std::vector<double> points;
   std::vector<uint8_t> fixed;
-  std::vector<uint32_t> op, oi, opt;
-  std::vector<double> px;
+  FillVector<uint32_t> op, oi, opt;  // written completely by without_points
+  FillVector<double> px;
   omvgba_problem view{};
   std::vector<size_t> kept;
 };

@@ -1559,8 +1559,8 @@ struct Setup {
   FillVector<uint32_t> ent, ent_point;  // written completely by the construction
   std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
   std::vector<uint32_t> chunk_begin, chunk_end;
-  std::vector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment
-  std::vector<int> seg_col;       // per entity id (obs*2+seg): column
+  FillVector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment (all written)
+  FillVector<int> seg_col;       // per entity id (obs*2+seg): column (all written)
   // pair tables
   std::vector<int> grp_row, grp_col;
   std::vector<uint32_t> grp_begin, grp_end, pair_a, pair_b, pair_p;
@@ -1568,7 +1568,7 @@ struct Setup {
   std::vector<int> xgrp_row, xgrp_col;
   std::vector<uint32_t> xgrp_begin, xgrp_end, xpair_a, xpair_b, xpair_p;
   std::vector<int> blk_cross_begin, blk_cross_end;
-  std::vector<int> ent_block;  // entity (observation * 2 + segment) -> parameter block, -1 when absent
+  FillVector<int> ent_block;  // entity (observation * 2 + segment) -> parameter block, -1 when absent
 };
 
 // Tiles of the fused matvec for one record precision (host tables).
@@ -1632,7 +1632,7 @@ static void host_parallel_chunks(size_t count, size_t chunks, Body body) {
 }
 
 static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& setup, int tile, TileSet& S) {
-  const std::vector<int>& ent_block = setup.ent_block;
+  const auto& ent_block = setup.ent_block;
   const int nblocks = (int)setup.blk_off.size();
   const size_t slot_bytes = MvSlot::bytes(tile);
   S.tile = tile;
@@ -1766,25 +1766,28 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
       if (cam_block[c] >= 0 && grp_block[n.cam_group[c]] >= 0) S.blk_edge[cam_block[c]] = grp_block[n.cam_group[c]];
   int nb = (int)S.blk_off.size();
   // entity lists per block (stable in observation order)
-  S.seg_col.assign(2 * N, 0);
-  S.obs_intr_col.assign(N, 0);
-  std::vector<int> ent_block(2 * N, -1);
+  // every entry is written below (-1: no block, column 0 and no intrinsic when absent)
+  S.seg_col.resize(2 * N);
+  S.obs_intr_col.resize(N);
+  FillVector<int> ent_block(2 * N);
   host_parallel_chunks(N, 64, [&](size_t, size_t b, size_t e) {
     for (size_t o = b; o < e; ++o) {
       int c = n.obs_cam[o];
       int pd = L.pose_dim[c];
-      if (cam_block[c] >= 0) {
-        ent_block[2 * o] = cam_block[c];
-        S.seg_col[2 * o] = 0;
-      }
+      ent_block[2 * o] = cam_block[c];  // -1 when the pose has no block
+      S.seg_col[2 * o] = 0;
+      int intr_b = -1, intr_col = 0, intr = 0;
       if (n.self_cal) {
         int g = n.cam_group[c];
-        S.obs_intr_col[o] = (L.intr_dim[g] << 8) | pd;
+        intr = (L.intr_dim[g] << 8) | pd;
         if (grp_block[g] >= 0) {
-          ent_block[2 * o + 1] = grp_block[g];
-          S.seg_col[2 * o + 1] = pd;
+          intr_b = grp_block[g];
+          intr_col = pd;
         }
       }
+      S.obs_intr_col[o] = intr;
+      ent_block[2 * o + 1] = intr_b;
+      S.seg_col[2 * o + 1] = intr_col;
     }
   });
   // each block's entities in entity order (a stable counting sort): per-chunk counts of every block,
@@ -1963,9 +1966,12 @@ uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
   uint64_t h = 1469598103934665603ull;
   auto add = [&](const auto& v) { h = fnv1a(v.data(), v.size() * sizeof(v[0]), h); };
   for (const auto* v : {&S.blk_off, &S.blk_dim, &S.blk_col, &S.blk_edge, &S.chunk_block, &S.chunk_col,
-                        &S.blk_chunk_begin, &S.blk_chunk_end, &S.obs_intr_col, &S.seg_col, &S.grp_row, &S.grp_col,
-                        &S.xgrp_row, &S.xgrp_col, &S.blk_cross_begin, &S.blk_cross_end, &S.ent_block})
+                        &S.blk_chunk_begin, &S.blk_chunk_end, &S.grp_row, &S.grp_col, &S.xgrp_row, &S.xgrp_col,
+                        &S.blk_cross_begin, &S.blk_cross_end})
     add(*v);
+  add(S.obs_intr_col);
+  add(S.seg_col);
+  add(S.ent_block);
   add(S.ent);
   add(S.ent_point);
   add(T.obs_rec);
@@ -2203,7 +2209,7 @@ struct Solver {
     d_ddiag.zero();
     d_summary.alloc(P, st);
     d_summary_part.alloc(red_blocks, st);
-    auto up_i = [&](DBuf<int>& b, const std::vector<int>& v) { upload_padded(b, v, 1, st); };
+    auto up_i = [&](DBuf<int>& b, const auto& v) { upload_padded(b, v, 1, st); };
     auto up_u = [&](DBuf<uint32_t>& b, const auto& v) { upload_padded(b, v, 1, st); };
     up_i(d_blk_off, S.blk_off);
     up_i(d_blk_dim, S.blk_dim);

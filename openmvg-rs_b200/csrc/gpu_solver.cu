@@ -1575,7 +1575,7 @@ struct Setup {
 struct TileSet {
   int tile = 0;
   std::vector<uint32_t> tile_hdr;  // 4 per tile: observations, points, segments, first point
-  std::vector<unsigned char> slots;
+  FillVector<unsigned char> slots;  // each tile's body zeroes its own slot first
   std::vector<uint32_t> blk_part;  // nblocks + 1
   FillVector<uint32_t> obs_rec;    // element index of each observation's record component 0 (all written)
 };
@@ -1654,7 +1654,7 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
     range.push_back({(uint32_t)p0, (uint32_t)p});
   }
   const size_t ntiles = range.size();
-  S.slots.assign(ntiles * slot_bytes, 0);
+  S.slots.resize(ntiles * slot_bytes);
   S.tile_hdr.assign(4 * ntiles, 0);
   // each tile's slot, independently; its segments' blocks are kept for the partial regions
   std::vector<std::vector<SegRef>> tile_segs(ntiles);
@@ -1665,6 +1665,7 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
     const uint64_t o0 = n.pt_off[p0], o1 = n.pt_off[p];
     const uint32_t nobs = (uint32_t)(o1 - o0), npt = (uint32_t)(p - p0);
     unsigned char* B = S.slots.data() + t * slot_bytes;
+    std::memset(B, 0, slot_bytes);  // unused rows and padding stay zero
     uint32_t* w0 = reinterpret_cast<uint32_t*>(B + MvSlot::w0(tile));
     uint32_t* w1 = reinterpret_cast<uint32_t*>(B + MvSlot::w1(tile));
     uint16_t* segb = reinterpret_cast<uint16_t*>(B + MvSlot::segb(tile));

@@ -315,7 +315,10 @@ int32_t omvgba_debug_schur_product(omvgba_context* context, const omvgba_problem
  * unsorted observation list, and its vector-Jacobian product. Camera j has rotation vector
  * rotvec[3j..3j+3] (R = exp(rotvec)), translation t[3j..], intrinsics intr[3j..] = (f, k1, k2);
  * residual_i = f (1 + k1 r^2 + k2 r^4) n_i - pixel_i with n_i the normalized camera point.
- * Inadmissible observations produce NaN residuals and zero gradients.
+ * Inadmissible observations produce NaN residuals and zero gradients. An observation whose camera
+ * index is >= camera_count or point index >= point_count (a negative int32 index reads as a large
+ * uint32) reads no camera or point: the forward writes a NaN residual for it, and the VJP then writes
+ * NaN into every gradient output of the call.
  * The VJP accumulates into grad_* (caller zeroes them): for each input the adjoint sum over
  * observations of J^T grad_residual, in a fixed order (deterministic run to run).
  * Pointers are DEVICE pointers; stream is a cudaStream_t (NULL = legacy default stream).
@@ -348,8 +351,12 @@ int32_t omvgba_residual_forward_f64(void* stream, uint64_t observation_count, co
  * reference. The scratch is a static device array of OMVGBA_RESIDUAL_STATIC_SCRATCH_BYTES that
  * every GPU loading this library holds until exit; sizes whose omvgba_residual_vjp_workspace_bytes
  * exceed it (about 440,000 points with 3,000 cameras) are rejected with OMVGBA_INVALID_ARGUMENT
- * before any device work. It allocates nothing. The first call on a device (with that device
- * current) resolves the array's device address, so make that first call before any stream capture.
+ * before any device work. It allocates nothing itself, but CUDA loads the library's modules
+ * lazily by default: the first call on a device loads the module that holds the array, which is
+ * when the driver reserves its 16 MiB. Callers that allow no driver allocation after start-up make
+ * one warm-up call at start-up (or run with CUDA_MODULE_LOADING=EAGER). Every call resolves the
+ * array's device address on the current device with cudaGetSymbolAddress (no allocation), so make
+ * the first call before any stream capture.
  * Runs on the current device; arguments and results as omvgba_residual_vjp_f32. All calls share the
  * one array: calls that overlap on the GPU race, so order them on one stream.
  */

@@ -525,7 +525,6 @@ __global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge 
     if (out.sw) out.sw[o] = sw;
   }
   PointSummary sm{0, 0, 0, 0, 1.0, 0, 0, 0};
-  double zero6[6] = {0, 0, 0, 0, 0, 0};
   double* vi = out.vinv + 6 * (size_t)p;
   double* ig = out.ig + 3 * (size_t)p;
   for (int k = 0; k < 6; ++k) vi[k] = 0.0;
@@ -533,7 +532,6 @@ __global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge 
   out.gp[3 * (size_t)p] = gp[0];
   out.gp[3 * (size_t)p + 1] = gp[1];
   out.gp[3 * (size_t)p + 2] = gp[2];
-  (void)zero6;
   if (!ok) {
     sm.invalid = 1;
     out.summary[p] = sm;

@@ -146,13 +146,21 @@ __device__ __forceinline__ void camera_point(const CamPre<T>& c, const T* t, con
 }
 
 // Forward pass: the camera constants are recomputed per observation, so the pass needs no scratch.
+// An observation whose camera or point index is out of range (a negative int32 index reads as a
+// large uint32) touches no camera or point and gets a NaN residual.
 template <typename T>
 __global__ void k_forward(uint64_t n, const uint32_t* __restrict__ cam, const uint32_t* __restrict__ pt,
                           const T* __restrict__ pixel, const T* __restrict__ rotvec, const T* __restrict__ intr,
-                          const T* __restrict__ trans, const T* __restrict__ points, T* __restrict__ residual) {
+                          const T* __restrict__ trans, const T* __restrict__ points, uint64_t ncam, uint64_t npts,
+                          T* __restrict__ residual) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t j = cam[i], p = pt[i];
+  if (j >= ncam || p >= npts) {
+    residual[2 * i] = T(NAN);
+    residual[2 * i + 1] = T(NAN);
+    return;
+  }
   const CamPre<T> c = make_pre(rotvec, intr, j);
   const T X[3] = {points[3 * (uint64_t)p], points[3 * (uint64_t)p + 1], points[3 * (uint64_t)p + 2]};
   const T t[3] = {trans[3 * (uint64_t)j], trans[3 * (uint64_t)j + 1], trans[3 * (uint64_t)j + 2]};
@@ -174,6 +182,7 @@ struct Accum {
   uint32_t* maxbits;  // pass 0: largest |contribution| (float bits); then the component's exponent
   unsigned long long* sum;
   uint64_t ncomp;
+  uint32_t* bad_index;  // set when an observation's camera or point index is out of range
 };
 
 constexpr int kCamComps = 9;
@@ -191,17 +200,23 @@ __device__ __forceinline__ void add_fixed(const Accum& acc, uint64_t k, float v)
   atomicAdd(acc.sum + k, (unsigned long long)q);
 }
 
-// One observation's contributions; PASS 0 records maxima, PASS 1 adds fixed-point values.
+// One observation's contributions; PASS 0 records maxima, PASS 1 adds fixed-point values. An
+// observation whose camera or point index is out of range adds nothing anywhere and raises the
+// bad-index word, which makes the finish pass write NaN into every gradient output.
 template <int PASS>
 __global__ void k_vjp(uint64_t n, const uint32_t* __restrict__ cam, const uint32_t* __restrict__ pt,
                       const float* __restrict__ pixel, const CamPre<float>* __restrict__ pre,
                       const float* __restrict__ trans, const float* __restrict__ points,
-                      const float* __restrict__ grad, uint64_t ncam, Accum acc) {
+                      const float* __restrict__ grad, uint64_t ncam, uint64_t npts, Accum acc) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const uint32_t j = cam[i], p = pt[i];
+  if (j >= ncam || p >= npts) {
+    if (PASS == 0) atomicOr(acc.bad_index, 1u);
+    return;
+  }
   const float g0 = grad[2 * i], g1 = grad[2 * i + 1];
   if (g0 == 0.0f && g1 == 0.0f) return;
-  const uint32_t j = cam[i], p = pt[i];
   const CamPre<float> c = pre[j];
   const float X[3] = {points[3 * (uint64_t)p], points[3 * (uint64_t)p + 1], points[3 * (uint64_t)p + 2]};
   const float t[3] = {trans[3 * (uint64_t)j], trans[3 * (uint64_t)j + 1], trans[3 * (uint64_t)j + 2]};
@@ -262,7 +277,7 @@ __global__ void k_vjp_finish(Accum acc, uint64_t ncam, float* __restrict__ g_rot
   if (k >= acc.ncomp) return;
   const int e = (int)acc.maxbits[k];
   float val;
-  if (e == INT32_MIN)
+  if (e == INT32_MIN || *acc.bad_index != 0u)
     val = NAN;
   else
     val = (float)ldexp((double)(long long)acc.sum[k], -e);
@@ -281,8 +296,9 @@ __global__ void k_vjp_finish(Accum acc, uint64_t ncam, float* __restrict__ g_rot
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Workspace: camera table, then the cleared region (maxima, sums, bad-index word).
 struct VjpLayout {
-  size_t pre, maxbits, sum, total;
+  size_t pre, maxbits, sum, bad, total;
 };
 inline VjpLayout vjp_layout(uint64_t ncam, uint64_t npts) {
   VjpLayout l;
@@ -290,7 +306,8 @@ inline VjpLayout vjp_layout(uint64_t ncam, uint64_t npts) {
   l.pre = 0;
   l.maxbits = align256(sizeof(CamPre<float>) * ncam);
   l.sum = l.maxbits + align256(sizeof(uint32_t) * ncomp);
-  l.total = l.sum + align256(sizeof(unsigned long long) * ncomp);
+  l.bad = l.sum + align256(sizeof(unsigned long long) * ncomp);
+  l.total = l.bad + 256;
   return l;
 }
 
@@ -328,10 +345,12 @@ int cuda_status(omvgba_error* e) {
 }
 
 template <typename T>
-int forward(void* stream, uint64_t n, const uint32_t* cam, const uint32_t* pt, const T* pixel, const T* rotvec,
-            const T* trans, const T* intr, const T* points, T* residual, omvgba_error* err) {
+int forward(void* stream, uint64_t n, const uint32_t* cam, const uint32_t* pt, const T* pixel, uint64_t ncam,
+            const T* rotvec, const T* trans, const T* intr, uint64_t npts, const T* points, T* residual,
+            omvgba_error* err) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_forward<T><<<grid_for(n), kThreads, 0, st>>>(n, cam, pt, pixel, rotvec, intr, trans, points, residual);
+  k_forward<T><<<grid_for(n), kThreads, 0, st>>>(n, cam, pt, pixel, rotvec, intr, trans, points, ncam, npts,
+                                                  residual);
   return cuda_status(err);
 }
 
@@ -362,10 +381,8 @@ int32_t omvgba_residual_forward_f32(void* stream, uint64_t observation_count, co
   if (observation_count == 0) return ok(error);
   if (any_null({camera_index, point_index, pixel, rotvec, translation, intrinsics, points, residual}))
     return fail(error, OMVGBA_INVALID_ARGUMENT, "null argument");
-  (void)camera_count;
-  (void)point_count;
-  return forward<float>(stream, observation_count, camera_index, point_index, pixel, rotvec, translation, intrinsics,
-                        points, residual, error);
+  return forward<float>(stream, observation_count, camera_index, point_index, pixel, camera_count, rotvec,
+                        translation, intrinsics, point_count, points, residual, error);
 }
 
 int32_t omvgba_residual_forward_f64(void* stream, uint64_t observation_count, const uint32_t* camera_index,
@@ -376,10 +393,8 @@ int32_t omvgba_residual_forward_f64(void* stream, uint64_t observation_count, co
   if (observation_count == 0) return ok(error);
   if (any_null({camera_index, point_index, pixel, rotvec, translation, intrinsics, points, residual}))
     return fail(error, OMVGBA_INVALID_ARGUMENT, "null argument");
-  (void)camera_count;
-  (void)point_count;
-  return forward<double>(stream, observation_count, camera_index, point_index, pixel, rotvec, translation,
-                         intrinsics, points, residual, error);
+  return forward<double>(stream, observation_count, camera_index, point_index, pixel, camera_count, rotvec,
+                         translation, intrinsics, point_count, points, residual, error);
 }
 
 int32_t omvgba_residual_vjp_f32(void* stream, uint64_t observation_count, const uint32_t* camera_index,
@@ -403,14 +418,16 @@ int32_t omvgba_residual_vjp_f32(void* stream, uint64_t observation_count, const 
   unsigned char* ws = static_cast<unsigned char*>(workspace);
   CamPre<float>* pre = reinterpret_cast<CamPre<float>*>(ws + l.pre);
   Accum acc{reinterpret_cast<uint32_t*>(ws + l.maxbits), reinterpret_cast<unsigned long long*>(ws + l.sum),
-            kCamComps * camera_count + 3 * point_count};
+            kCamComps * camera_count + 3 * point_count, reinterpret_cast<uint32_t*>(ws + l.bad)};
   if (cudaMemsetAsync(ws + l.maxbits, 0, l.total - l.maxbits, st) != cudaSuccess) return cuda_status(error);
   k_cam_prepare<float><<<grid_for(camera_count), kThreads, 0, st>>>(camera_count, rotvec, intrinsics, pre);
   k_vjp<0><<<grid_for(observation_count), kThreads, 0, st>>>(observation_count, camera_index, point_index, pixel, pre,
-                                                             translation, points, grad_residual, camera_count, acc);
+                                                             translation, points, grad_residual, camera_count,
+                                                             point_count, acc);
   k_vjp_scales<<<grid_for(acc.ncomp), kThreads, 0, st>>>(acc, ceil_log2(observation_count) + 1);
   k_vjp<1><<<grid_for(observation_count), kThreads, 0, st>>>(observation_count, camera_index, point_index, pixel, pre,
-                                                             translation, points, grad_residual, camera_count, acc);
+                                                             translation, points, grad_residual, camera_count,
+                                                             point_count, acc);
   k_vjp_finish<<<grid_for(acc.ncomp), kThreads, 0, st>>>(acc, camera_count, grad_rotvec, grad_translation,
                                                          grad_intrinsics, grad_points);
   return cuda_status(error);

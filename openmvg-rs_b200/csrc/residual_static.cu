@@ -10,12 +10,19 @@
 //
 // How. The scratch is one file-scope device array of OMVGBA_RESIDUAL_STATIC_SCRATCH_BYTES (16 MiB),
 // which every GPU that loads this library holds until the process exits. Host code cannot use the
-// array's name as a device address, so the first call on each device (with that device current)
-// resolves the address with cudaGetSymbolAddress and keeps it; later calls on that device reuse it.
+// array's name as a device address, so every call resolves the address on the current device with
+// cudaGetSymbolAddress (cheap, allocates nothing). Resolving it per call rather than caching it per
+// device ordinal keeps it right when the module is loaded again at another address: after a
+// cudaDeviceReset, or for a driver-API caller whose current context is not the primary one.
 // The entry then runs the ordinary omvgba_residual_vjp_f32 with the array as its workspace: that
 // path clears the accumulators on the stream before use and overwrites the camera table, so the
 // previous call's leftovers never leak into a result. Nothing here calls cudaMalloc, cudaFree or any
 // allocating routine.
+//
+// Module loading. CUDA loads a library's modules lazily by default, so the driver reserves the
+// array's 16 MiB when the first call on a device loads this file's module (the symbol lookup does
+// that), not at process start. Callers that allow no driver allocation after start-up make one
+// warm-up call at start-up, or set CUDA_MODULE_LOADING=EAGER.
 //
 // Because every call shares the one array, calls that overlap on the GPU (on different streams, or
 // from different threads without ordering) race on it; order them on one stream or synchronise.
@@ -23,7 +30,6 @@
 
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/ba_cuda.h"
@@ -31,10 +37,6 @@
 static __device__ __align__(256) unsigned char g_vjp_scratch[OMVGBA_RESIDUAL_STATIC_SCRATCH_BYTES];
 
 namespace {
-
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_address[kMaxDevices] = {};
 
 int report(omvgba_error* e, int code, const std::string& msg) {
   if (e) {
@@ -46,23 +48,14 @@ int report(omvgba_error* e, int code, const std::string& msg) {
   return code;
 }
 
-// Device address of the scratch array on the current device, resolved once per device.
+// Device address of the scratch array in the current context.
 int scratch_on_current_device(void** out, omvgba_error* error) {
-  int device = 0;
-  cudaError_t st = cudaGetDevice(&device);
-  if (st != cudaSuccess) return report(error, OMVGBA_CUDA_ERROR, std::string("cudaGetDevice: ") + cudaGetErrorString(st));
-  if (device < 0 || device >= kMaxDevices)
-    return report(error, OMVGBA_CUDA_ERROR, "device ordinal " + std::to_string(device) + " out of range");
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_address[device]) {
-    void* ptr = nullptr;
-    st = cudaGetSymbolAddress((void**)&ptr, g_vjp_scratch);
-    if (st != cudaSuccess || !ptr)
-      return report(error, OMVGBA_CUDA_ERROR,
-                    std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(st));
-    g_scratch_address[device] = ptr;
-  }
-  *out = g_scratch_address[device];
+  void* ptr = nullptr;
+  const cudaError_t st = cudaGetSymbolAddress((void**)&ptr, g_vjp_scratch);
+  if (st != cudaSuccess || !ptr)
+    return report(error, OMVGBA_CUDA_ERROR,
+                  std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(st));
+  *out = ptr;
   return OMVGBA_OK;
 }
 

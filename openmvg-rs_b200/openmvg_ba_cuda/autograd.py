@@ -8,7 +8,9 @@ tensors must live on a CUDA device and the library must be built.
 Model (crates/openmvg-ba/src/kernel/multi_view/self_calibration/model.rs:26-129): for observation i
 of camera j and point p, X_c = exp(rotvec_j) X_p + t_j, n = X_c.xy / X_c.z and
 residual_i = f_j (1 + k1_j |n|^2 + k2_j |n|^4) n - pixel_i. Inadmissible observations give NaN
-residuals and no gradient.
+residuals and no gradient. Indices are checked on the device: an out-of-range camera or point index
+gives that observation a NaN residual and makes the backward's gradients NaN (no memory outside the
+inputs is read or written).
 """
 from __future__ import annotations
 
@@ -21,9 +23,11 @@ from ._lib import lib
 from .problem import raise_for
 
 
-def _check(t: torch.Tensor, name: str, dtype, shape_tail=None) -> torch.Tensor:
+def _check(t: torch.Tensor, name: str, dtype, shape_tail=None, device=None) -> torch.Tensor:
     if not t.is_cuda:
         raise ValueError(f"{name} must be a CUDA tensor")
+    if device is not None and t.device != device:
+        raise ValueError(f"{name} is on {t.device}, the other inputs on {device}")
     if t.dtype != dtype:
         raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
     if shape_tail is not None and tuple(t.shape[1:]) != shape_tail:
@@ -38,13 +42,16 @@ class ReprojectionResidual(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, camera_index, point_index, pixel, rotvec, translation, intrinsics, points):
-        cam = _check(camera_index, "camera_index", torch.int32)
-        pt = _check(point_index, "point_index", torch.int32)
         px = _check(pixel, "pixel", torch.float32, (2,))
-        rv = _check(rotvec, "rotvec", torch.float32, (3,))
-        tr = _check(translation, "translation", torch.float32, (3,))
-        it = _check(intrinsics, "intrinsics", torch.float32, (3,))
-        X = _check(points, "points", torch.float32, (3,))
+        dev = px.device
+        cam = _check(camera_index, "camera_index", torch.int32, device=dev)
+        pt = _check(point_index, "point_index", torch.int32, device=dev)
+        rv = _check(rotvec, "rotvec", torch.float32, (3,), dev)
+        tr = _check(translation, "translation", torch.float32, (3,), dev)
+        it = _check(intrinsics, "intrinsics", torch.float32, (3,), dev)
+        X = _check(points, "points", torch.float32, (3,), dev)
+        if cam.shape[0] != px.shape[0] or pt.shape[0] != px.shape[0]:
+            raise ValueError("camera_index, point_index and pixel must have one row per observation")
         n = cam.shape[0]
         residual = torch.empty((n, 2), dtype=torch.float32, device=px.device)
         err = abi.Error()
@@ -65,7 +72,17 @@ class ReprojectionResidual(torch.autograd.Function):
 
 
 def vjp(cam, pt, px, rv, tr, it, X, grad_residual):
-    """(d rotvec, d translation, d intrinsics, d points) = J^T grad_residual by the adjoint kernel."""
+    """(d rotvec, d translation, d intrinsics, d points) = J^T grad_residual by the adjoint kernel.
+    An out-of-range camera or point index makes every returned gradient NaN."""
+    dev = px.device
+    for t, name in ((cam, "camera_index"), (pt, "point_index"), (rv, "rotvec"), (tr, "translation"),
+                    (it, "intrinsics"), (X, "points"), (grad_residual, "grad_residual")):
+        if t.device != dev:
+            raise ValueError(f"{name} is on {t.device}, the other inputs on {dev}")
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+    if grad_residual.dtype != torch.float32 or tuple(grad_residual.shape) != (cam.shape[0], 2):
+        raise ValueError("grad_residual must be float32 with shape (n, 2)")
     n = cam.shape[0]
     g_rot, g_t, g_int, g_pt = (torch.zeros_like(a) for a in (rv, tr, it, X))
     ws_bytes = int(lib().omvgba_residual_vjp_workspace_bytes(n, rv.shape[0], X.shape[0]))
@@ -87,11 +104,15 @@ def reprojection_residual(camera_index, point_index, pixel, rotvec, translation,
 
 def residual_f64(camera_index, point_index, pixel, rotvec, translation, intrinsics, points) -> torch.Tensor:
     """FP64 forward (no autograd), for finite-difference checks of the adjoint."""
-    cam = _check(camera_index, "camera_index", torch.int32)
-    pt = _check(point_index, "point_index", torch.int32)
-    px, rv, tr, it, X = (_check(a, nm, torch.float64) for a, nm in
-                         ((pixel, "pixel"), (rotvec, "rotvec"), (translation, "translation"),
-                          (intrinsics, "intrinsics"), (points, "points")))
+    px = _check(pixel, "pixel", torch.float64, (2,))
+    dev = px.device
+    cam = _check(camera_index, "camera_index", torch.int32, device=dev)
+    pt = _check(point_index, "point_index", torch.int32, device=dev)
+    rv, tr, it, X = (_check(a, nm, torch.float64, (3,), dev) for a, nm in
+                     ((rotvec, "rotvec"), (translation, "translation"), (intrinsics, "intrinsics"),
+                      (points, "points")))
+    if cam.shape[0] != px.shape[0] or pt.shape[0] != px.shape[0]:
+        raise ValueError("camera_index, point_index and pixel must have one row per observation")
     residual = torch.empty((cam.shape[0], 2), dtype=torch.float64, device=px.device)
     err = abi.Error()
     stream = torch.cuda.current_stream(px.device).cuda_stream

@@ -255,7 +255,11 @@ def window_problems(seed: int = 23, windows: int = 256, total_observations: int 
 def residual_inputs(seed: int = 5, observations: int = 10_000_000, cameras: int = 3000, points: int = 2_000_000,
                     dtype=np.float32):
     """Random radial-camera residual inputs: rotations from random rotation vectors, translations in
-    the unit box, points at depths 2-50 in front of their camera, intrinsics (f, k1, k2)."""
+    the unit box, points at depths 2-50 in front of their camera, intrinsics (f, k1, k2).
+
+    Each point is placed in front of an owning camera and observed from the owner's 16 cameras with
+    the closest viewing directions (the owner included), so a point's gradient sums contributions
+    from several cameras, as it does in a real track."""
     rng = np.random.Generator(np.random.PCG64(seed))
     rotvec = rng.normal(0.0, 1.0, size=(cameras, 3))
     rotvec *= (rng.uniform(0, np.pi, size=cameras) / np.linalg.norm(rotvec, axis=1))[:, None]
@@ -271,7 +275,10 @@ def residual_inputs(seed: int = 5, observations: int = 10_000_000, cameras: int 
     pc = np.concatenate([xy, depth[:, None]], axis=1)
     R = _exp_so3(rotvec)
     X = np.einsum("nji,nj->ni", R[owner], pc - t[owner])  # R^T (pc - t)
-    cam = owner[pt].astype(np.uint32)  # every observation sees its point from the owning camera
+    # the 16 cameras whose optical axes (third rows of R) are closest to each camera's, itself first
+    axis = R[:, 2, :]
+    near = np.argsort(-(axis @ axis.T), axis=1, kind="stable")[:, :16]
+    cam = near[owner[pt], rng.integers(0, near.shape[1], size=observations)].astype(np.uint32)
     pix = rng.uniform(-200, 200, size=(observations, 2))
     return {
         "camera_index": cam, "point_index": pt, "pixel": pix.astype(dtype), "rotvec": rotvec.astype(dtype),

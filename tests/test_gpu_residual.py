@@ -124,3 +124,27 @@ def test_inadmissible_observations_are_nan_without_gradient(inputs):
     g[bad] = 1.0  # upstream gradient only on inadmissible observations
     for x in vjp(cam, pt, px, rv, tr, it, X, g):
         assert float(x.abs().max()) == 0.0
+
+
+def test_out_of_range_indices_give_nan_not_a_fault(inputs):
+    """A camera index past the camera count and a negative point index are caught on the device: the
+    forward gives those observations NaN residuals and the adjoint returns NaN gradients; the rest of
+    the forward is unchanged and later calls on the same context still work."""
+    from openmvg_ba_cuda.autograd import reprojection_residual, vjp
+    cam, pt, px, rv, tr, it, X = to_dev(inputs, torch.float32)
+    good = reprojection_residual(cam, pt, px, rv, tr, it, X)
+    bad_cam, bad_pt = cam.clone(), pt.clone()
+    bad_cam[5] = N_CAM
+    bad_pt[7] = -1
+    res = reprojection_residual(bad_cam, bad_pt, px, rv, tr, it, X)
+    assert bool(torch.isnan(res[5]).all()) and bool(torch.isnan(res[7]).all())
+    keep = torch.ones(N_OBS, dtype=torch.bool, device="cuda")
+    keep[5] = keep[7] = False
+    assert torch.equal(torch.isnan(res[keep]), torch.isnan(good[keep]))
+    assert torch.equal(torch.nan_to_num(res[keep]), torch.nan_to_num(good[keep]))
+    g = torch.ones(N_OBS, 2, device="cuda")
+    for x in vjp(bad_cam, bad_pt, px, rv, tr, it, X, g):
+        assert bool(torch.isnan(x).all())
+    torch.cuda.synchronize()
+    for x in vjp(cam, pt, px, rv, tr, it, X, g):  # the context is still usable
+        assert bool(torch.isfinite(x).any())

@@ -54,11 +54,18 @@ def test_static_scratch_vjp_matches_the_workspace_vjp_on_two_calls():
     assert code == abi.OMVGBA_OK, err.message
     torch.cuda.synchronize()
 
-    for _ in range(2):  # two calls in a row share the static scratch
+    for call in range(2):  # two calls in a row share the static scratch
         out = [torch.zeros_like(a) for a in (rv, tr, it, X)]
+        torch.cuda.synchronize()
+        # the first call may load the module that holds the array (lazy module loading); from the
+        # second call on, neither torch's allocator nor the device's free memory may change
+        allocated, (free, _) = torch.cuda.memory_allocated(), torch.cuda.mem_get_info()
         code, err = _call_static(stream, N_OBS, ptrs, N_CAM, N_PTS, [a.data_ptr() for a in out])
         assert code == abi.OMVGBA_OK, err.message
         torch.cuda.synchronize()
+        if call == 1:
+            assert torch.cuda.memory_allocated() == allocated
+            assert torch.cuda.mem_get_info()[0] == free
         for got, want in zip(out, ref):
             # the tolerance of the adjoint's parity tests (relative norm 2e-4) ...
             rel = float(torch.linalg.vector_norm((got - want).double()) / torch.linalg.vector_norm(want.double()))

@@ -1,21 +1,26 @@
 #!/usr/bin/env python3
 """Benchmark: bundle-adjustment time-to-converge and LM iterations/s on one B200 (or N replicas).
 
-Workload: the 500-camera problem with per-camera intrinsics (6-DoF pose + log f, k1, k2 per
-camera, D = 4,493) over a 100 x 100 ground plane, 200,000 points with geometric track lengths
-(mean ~6, minimum 2; 1,184,956 observations at seed 11), pixel noise N(0, 0.5^2), 5% outliers,
-Huber loss (1 px), 50 LM iterations, block-Jacobi PCG with forcing tolerance 1e-6. Seeded synthetic
-data (no dataset exists for it). One step = one complete solve of that problem.
+Workload (default): the 12M-observation global refinement: 3,000 cameras with per-camera
+intrinsics (6-DoF pose + log f, k1, k2 per camera, D = 26,993) over a 245 x 245 ground plane, 2M
+points with geometric track lengths (mean ~6, minimum 2; ~12.0M observations), pixel noise
+N(0, 0.5^2), 5% outliers, Huber loss (1 px), matrix-free block-Jacobi PCG with forcing tolerance
+1e-6, run to convergence (LM budget 200). Seeded synthetic data (no dataset exists for it). One
+step = one complete solve of that problem. A second leg in the same line solves the 500-camera,
+1.2M-observation problem to convergence in both precisions.
 
-value  : LM iterations/s of the mixed-precision solve (FP32 products, FP64 everything the
-         reference's acceptance depends on), problem resident in device memory (omvgba_plan_solve),
-         summed over replicas, divided by the slowest rank's time.
+value  : LM iterations/s of the mixed-precision solve (FP32 Jacobians and products, FP64 everything
+         the reference's acceptance depends on), problem resident in device memory
+         (omvgba_plan_solve), summed over replicas, divided by the slowest rank's time.
 e2e    : the same through omvgba_solve from host arrays (lowering, upload and download included).
 fp64   : the plain FP64 solve of the same problem, for the mixed-vs-FP64 comparison at equal cost.
+targets: whether the mixed solve is >= 2x the FP64 solve's speed, whether both converged, and whether
+         their final costs agree to 1e-6 relative.
 roofline: the matrix-free product's tile kernel (k_mv_tiles<float>, the dominant kernel of the
-         solve), timed alone with CUDA events on the plan's stream with L2 flushed before each launch.
+         PCG loop), timed alone with CUDA events on the plan's stream with L2 flushed before each launch.
 cpu_baseline: the C++ restatement of the reference CPU solver (the oracle) on the first LM
-         iterations of the same problem, all host threads.
+         iteration of the same problem, all host threads; a single-thread sample on the
+         500-camera problem beside it.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 launch under torch.distributed.run; every rank solves its own seeded replica.
@@ -39,8 +44,9 @@ METRIC = "BA time-to-converge (s) & LM iters/s, mixed vs FP64 GPU, same final co
 UNIT = "LM iterations/s"
 L2_BYTES = 126 * 1024 * 1024
 FLUSH_BYTES = 512 * 1024 * 1024
-# Workloads: plane500 is the headline (the single large problem of the benchmark's configuration
-# list); plane3000 is the 12M-observation global-refinement problem, run on request.
+# Workloads: plane3000 is the headline (the 12M-observation global refinement the mixed-precision
+# target is stated on); plane500 is the single large 500-camera problem, also run as the second leg
+# of the headline line.
 WORKLOADS = {
     "plane500": dict(
         kwargs=dict(cameras=500, points=200_000, mean_track=6.5, extent=100.0),
@@ -63,13 +69,16 @@ WORKLOADS = {
               "(3,000 cameras from random rotations and translations in the unit box, 2M points at depths 2-50, "
               "FP32), forward + backward through the torch.autograd.Function")),
 }
-CPU_SAMPLE_ITERATIONS = 3
+CPU_SAMPLE_ITERATIONS = {"plane500": 3, "plane3000": 1}
 CPU_SAMPLE_WINDOWS = 32
-TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane500.txt")
-WORKLOAD = WORKLOADS["plane500"]["text"]
+DEFAULT_WORKLOAD = "plane3000"
+SECOND_LEG = "plane500"
+MAX_ITERATIONS = 200  # LM budget: every bench solve converges well inside it
+TRAFFIC_SUMMARY = {"plane500": os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane500.txt"),
+                   "plane3000": os.path.join(ROOT, "profiles", "k_mv_tiles_fp32_plane3000.txt")}
 
 
-def problem_for(rank: int, workload: str = "plane500"):
+def problem_for(rank: int, workload: str = DEFAULT_WORKLOAD):
     from openmvg_ba_cuda import synthetic
     return synthetic.plane_problem(seed=11 + rank, **WORKLOADS[workload]["kwargs"])
 
@@ -173,12 +182,16 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "of fallback"
 
 
-def traffic_per_launch(observations: int):
-    """DRAM bytes per launch of k_mv_tiles<float> from the committed ncu summary, scaled to this
-    problem's observation count when the capture ran on another size."""
+def traffic_per_launch(observations: int, workload: str):
+    """DRAM bytes per launch of k_mv_tiles<float> from the committed ncu summary of this workload
+    (else the plane500 one), scaled to this problem's observation count when the capture ran on
+    another size."""
+    path = TRAFFIC_SUMMARY.get(workload)
+    if not path or not os.path.exists(path):
+        path = TRAFFIC_SUMMARY["plane500"]
     try:
         fields = {}
-        for line in open(TRAFFIC_SUMMARY):
+        for line in open(path):
             if ":" in line:
                 k, v = line.split(":", 1)
                 fields[k.strip()] = v.strip()
@@ -190,11 +203,11 @@ def traffic_per_launch(observations: int):
 
 
 # ---- CPU baseline: the oracle (C++ restatement of the reference CPU solver) ----------------------
-def cpu_sample(problem, iterations: int) -> dict:
+def cpu_sample(problem, iterations: int, threads: int | None = None) -> dict:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from openmvg_ba_cuda import abi
-    threads = oracle.max_threads()
+    threads = threads or oracle.max_threads()
     oracle.set_threads(threads)
     cfg = solve_config(abi.PRECISION_FP64, max_iterations=iterations)
     t0 = time.perf_counter()
@@ -204,9 +217,9 @@ def cpu_sample(problem, iterations: int) -> dict:
     return {"value": its / dt, "unit": UNIT, "cores": threads, "kind": "port", "seconds": dt, "iterations": its,
             "pcg_iterations": int(sol.report.get("pcg_iteration_count", 0)),
             "sample": (f"oracle (C++/OpenMP restatement of the reference CPU solver) on the first {its} LM "
-                       f"iterations of the same problem, lowering and final certificate included, {threads} "
-                       "threads; early iterations need fewer PCG iterations than the 50-iteration average, "
-                       "so this rate favours the CPU")}
+                       f"iteration(s) of the same problem, lowering and final certificate included, {threads} "
+                       "thread(s); early iterations need fewer PCG iterations than the average of a solve run "
+                       "to convergence, so this rate favours the CPU")}
 
 
 def cpu_info() -> str:
@@ -220,13 +233,17 @@ def cpu_info() -> str:
 
 
 def run_reference(args) -> int:
+    """The reference arm: the oracle on this workload's problem, all host threads, each step a
+    bounded sample (the first LM iteration(s) of the problem, set-up and final certificate
+    included)."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
     problem = problem_for(0, args.workload)
+    iterations = CPU_SAMPLE_ITERATIONS.get(args.workload, 1)
     for _ in range(args.warmup):
         cpu_sample(problem, 1)
-    samples = [cpu_sample(problem, CPU_SAMPLE_ITERATIONS) for _ in range(args.steps)]
+    samples = [cpu_sample(problem, iterations) for _ in range(args.steps)]
     total_s = sum(s["seconds"] for s in samples)
     total_it = sum(s["iterations"] for s in samples)
     value = total_it / total_s
@@ -239,7 +256,7 @@ def run_reference(args) -> int:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["text"], "max_iterations": args.max_iterations,
                    "parallelism": "host threads", "cpu": cpu_info(),
-                   "sample_lm_iterations_per_step": CPU_SAMPLE_ITERATIONS},
+                   "sample_lm_iterations_per_step": iterations},
         "cpu_baseline": base,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -265,7 +282,7 @@ def timed_solves(solve, stream, flush, steps: int):
     return reports, ms, sol
 
 
-def kernel_roofline(plan, info: dict, stream, flush, launches: int = 20) -> dict:
+def kernel_roofline(plan, info: dict, stream, flush, workload: str, launches: int = 20) -> dict:
     """Average duration of the tile kernel k_mv_tiles<float> alone (CUDA events on the plan's
     stream, L2 flushed before every launch) and its algorithmic bytes per launch: the FP32 Jacobian
     entries, one camera index per observation, the FP64 damped point inverse (6 values) per point
@@ -292,7 +309,7 @@ def kernel_roofline(plan, info: dict, stream, flush, launches: int = 20) -> dict
                    + 48 * int(info["point_count"]) + 8 * D)
     peak, which = measured_peak()
     achieved = algorithmic / avg_s / 1e9
-    traffic = traffic_per_launch(int(info["observation_count"]))
+    traffic = traffic_per_launch(int(info["observation_count"]), workload)
     return {"bound": "hbm", "kernel": "k_mv_tiles<float>", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": which, "traffic": traffic,
             "algorithmic_bytes_per_launch": algorithmic, "avg_launch_us": avg_s * 1e6, "launches_timed": launches}
@@ -430,6 +447,52 @@ def dataclasses_replace_loss(problem, loss):
     return dataclasses.replace(problem, robust_loss=loss)
 
 
+def precision_pair(adjuster, problem, stream, flush, steps: int, warmup: int, max_iterations: int) -> dict:
+    """Resident mixed-precision and FP64 solves of one problem, `steps` timed solves each (CUDA
+    events on the solver's stream, L2 flushed before each), after `warmup` untimed ones."""
+    import torch
+    from openmvg_ba_cuda import abi
+    out = {}
+    for name, precision in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
+        plan = adjuster.plan(problem, solve_config(precision, max_iterations=max_iterations,
+                                                   stream=stream.cuda_stream))
+        for _ in range(warmup):
+            plan.solve()
+        torch.cuda.synchronize()
+        barrier()
+        reports, ms, _ = timed_solves(plan.solve, stream, flush, steps)
+        barrier()
+        info = plan.info()
+        plan.close()
+        seconds, its = aggregate(sum(ms) / 1e3, float(sum(r["iteration_count"] for r in reports)), device="cuda")
+        out[name] = {"reports": reports, "seconds": seconds, "iterations": its, "info": info,
+                     "local_iterations": sum(r["iteration_count"] for r in reports)}
+    return out
+
+
+def leg_summary(pair: dict, steps: int) -> dict:
+    """Time-to-converge, rates, final costs and the target checks of a mixed/FP64 pair."""
+    m, f = pair["mixed"], pair["fp64"]
+    rm, rf = m["reports"][-1], f["reports"][-1]
+    t_m, t_f = m["seconds"] / steps, f["seconds"] / steps
+    conv_m, conv_f = rm["status"] == 0, rf["status"] == 0
+    gap = abs(rm["final_objective"] - rf["final_objective"]) / abs(rf["final_objective"])
+    speedup = t_f / t_m
+    return {
+        "mixed": {"value": m["iterations"] / m["seconds"], "unit": UNIT, "converged": conv_m,
+                  "time_to_converge_s": t_m if conv_m else None, "seconds_per_solve": t_m,
+                  "lm_iterations": rm["iteration_count"], "pcg_iterations": rm["pcg_iteration_count"],
+                  "final_cost": rm["final_objective"]},
+        "fp64": {"value": f["iterations"] / f["seconds"], "unit": UNIT, "converged": conv_f,
+                 "time_to_converge_s": t_f if conv_f else None, "seconds_per_solve": t_f,
+                 "lm_iterations": rf["iteration_count"], "pcg_iterations": rf["pcg_iteration_count"],
+                 "final_cost": rf["final_objective"]},
+        "mixed_vs_fp64": {"speedup": speedup, "final_cost_rel_diff": gap},
+        "targets": {"both_converged": conv_m and conv_f, "speedup_ge_2x": speedup >= 2.0,
+                    "final_cost_rel_diff_le_1e-6": gap <= 1e-6},
+    }
+
+
 def run_ours(args) -> int:
     import torch
     world, rank, local = dist_env()
@@ -438,7 +501,7 @@ def run_ours(args) -> int:
     torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
                                 device_id=torch.device("cuda", local))
     from openmvg_ba_cuda import abi
     from openmvg_ba_cuda.adjuster import CudaBundleAdjuster
@@ -448,7 +511,6 @@ def run_ours(args) -> int:
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     adjuster = CudaBundleAdjuster(local)
     mixed_cfg = solve_config(abi.PRECISION_MIXED, max_iterations=args.max_iterations, stream=stream.cuda_stream)
-    fp64_cfg = solve_config(abi.PRECISION_FP64, max_iterations=args.max_iterations, stream=stream.cuda_stream)
 
     # value: mixed precision, problem resident in device memory
     plan = adjuster.plan(problem, mixed_cfg)
@@ -470,7 +532,7 @@ def run_ours(args) -> int:
     total_s, total_its = aggregate(local_s, float(local_its), device="cuda")
     value = total_its / total_s
     launches = sum(r["kernel_launches"] for r in reports)
-    roofline = kernel_roofline(plan, info, stream, flush)
+    roofline = kernel_roofline(plan, info, stream, flush, args.workload)
     plan.close()
 
     if args.legs == "value":  # profiling runs: the resident mixed solve and the kernel timing only
@@ -485,6 +547,7 @@ def run_ours(args) -> int:
         return 0
 
     # FP64 on the same problem: the comparison at equal final cost
+    fp64_cfg = solve_config(abi.PRECISION_FP64, max_iterations=args.max_iterations, stream=stream.cuda_stream)
     plan64 = adjuster.plan(problem, fp64_cfg)
     plan64.solve()
     torch.cuda.synchronize()
@@ -500,16 +563,32 @@ def run_ours(args) -> int:
     barrier()
     e2e_s, e2e_its = aggregate(sum(e2e_ms) / 1e3, float(sum(r["iteration_count"] for r in e2e_reports)),
                                device="cuda")
+
+    # second leg: the 500-camera problem to convergence in both precisions (one timed solve each)
+    second = None
+    if args.workload != SECOND_LEG and args.second_leg:
+        p2 = problem_for(rank, SECOND_LEG)
+        pair = precision_pair(adjuster, p2, stream, flush, 1, 1, args.max_iterations)
+        second = {"workload": WORKLOADS[SECOND_LEG]["text"],
+                  "observations": int(pair["mixed"]["info"]["observation_count"]),
+                  "reduced_dimension": int(pair["mixed"]["info"]["reduced_dimension"])} | leg_summary(pair, 1)
     adjuster.close()
 
-    cpu = None
+    cpu = cpu1 = None
     if rank == 0 and world == 1 and args.legs == "all":
-        cpu = cpu_sample(problem, CPU_SAMPLE_ITERATIONS)
+        iterations = CPU_SAMPLE_ITERATIONS.get(args.workload, 1)
+        cpu = cpu_sample(problem, iterations)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"cpu": cpu_info()}
+        # one host thread on the 500-camera problem's first LM iteration
+        c1 = cpu_sample(problem_for(0, SECOND_LEG), 1, threads=1)
+        cpu1 = {k: c1[k] for k in ("value", "unit", "cores", "kind")} | {
+            "sample": "oracle on the first LM iteration of the 500-camera problem (plane500), one host thread, "
+                      "lowering and final certificate included", "cpu": cpu_info()}
 
     if rank == 0:
-        cost_mixed = reports[-1]["final_objective"]
-        cost_fp64 = reports64[-1]["final_objective"]
+        pair = {"mixed": {"reports": reports, "seconds": total_s, "iterations": total_its},
+                "fp64": {"reports": reports64, "seconds": s64, "iterations": its64}}
+        head = leg_summary(pair, args.steps)
         steps = args.steps
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
@@ -523,16 +602,15 @@ def run_ours(args) -> int:
                               "126 MB L2; L2 also flushed (512 MB write) before every step"
                               % ((info["record_bytes_fp32"] + info["record_bytes_fp64"] + info["metadata_bytes_fp32"]
                                   + info["metadata_bytes_fp64"]) / 1e6))},
-            "time_to_converge_s": total_s / steps,
+            "time_to_converge_s": head["mixed"]["time_to_converge_s"],
+            "converged": head["mixed"]["converged"],
             "lm_iterations_per_step": local_its / steps,
             "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports) / steps,
-            "final_cost": cost_mixed,
-            "converged": reports[-1]["status"] == 0,
-            "fp64": {"value": its64 / s64, "unit": UNIT, "time_to_converge_s": s64 / steps, "final_cost": cost_fp64,
-                     "converged": reports64[-1]["status"] == 0,
-                     "pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports64) / steps},
-            "mixed_vs_fp64": {"speedup": (s64 / steps) / (total_s / steps),
-                              "final_cost_rel_diff": abs(cost_mixed - cost_fp64) / abs(cost_fp64)},
+            "final_cost": head["mixed"]["final_cost"],
+            "fp64": head["fp64"] | {"pcg_iterations_per_step": sum(r["pcg_iteration_count"] for r in reports64) / steps},
+            "mixed_vs_fp64": head["mixed_vs_fp64"],
+            "targets": head["targets"],
+            "second_leg": second,
             "clocks": clock_summary,
             "e2e": {"value": e2e_its / e2e_s, "unit": UNIT, "time_to_converge_s": e2e_s / steps,
                     "h2d_bytes_per_step": int(sum(r["h2d_bytes"] for r in e2e_reports) / steps),
@@ -541,6 +619,7 @@ def run_ours(args) -> int:
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "cpu_baseline_single_thread": cpu1,
             "wall_s_timed_region": wall,
         }
         print(json.dumps(line), flush=True)
@@ -556,11 +635,13 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plane500")
-    ap.add_argument("--max-iterations", type=int, default=50, help="LM iteration budget of every solve")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--max-iterations", type=int, default=MAX_ITERATIONS, help="LM iteration budget of every solve")
     ap.add_argument("--legs", choices=["all", "gpu", "value"], default="all",
                     help="gpu: every leg but the CPU baseline; value: only the resident mixed solve and the kernel "
                          "timing (for profiler runs)")
+    ap.add_argument("--no-second-leg", dest="second_leg", action="store_false",
+                    help="skip the 500-camera mixed/FP64 leg of the headline line")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

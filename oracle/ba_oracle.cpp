@@ -20,6 +20,7 @@
 //   final certificate . sparse/direct.rs:288-460, schur/diagnostics.rs:18-140
 //   report/solution ... native/reporting.rs:24-141, solver.rs:803-1131
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -30,6 +31,15 @@
 
 #include "../include/ba_cuda.h"
 #include "oracle_core.hpp"
+
+// Phase timer printed to stderr when OMVGBA_ORACLE_TIMES is set (diagnostics only).
+static double oracle_now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+static void oracle_phase(const char* what, double t0) {
+  static const bool on = std::getenv("OMVGBA_ORACLE_TIMES") != nullptr;
+  if (on) std::fprintf(stderr, "[oracle] %s %.3fs\n", what, oracle_now() - t0);
+}
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -80,6 +90,7 @@ struct Layout {
   std::vector<int> intr_off, intr_dim;  // per group (self-calibration)
   std::vector<int> block_off, block_dim;
   std::vector<int> param_block;
+  std::vector<int> param_camera;  // camera owning each pose parameter, -1 for intrinsic parameters
 };
 
 struct GaugeState {
@@ -125,12 +136,16 @@ static Layout make_layout(const Native& n) {
   }
   L.D = off;
   L.param_block.assign(off, -1);
+  L.param_camera.assign(off, -1);
   for (int c = 0; c < n.ncam; ++c)
     if (L.pose_dim[c] > 0) {
       int b = (int)L.block_off.size();
       L.block_off.push_back(L.pose_off[c]);
       L.block_dim.push_back(L.pose_dim[c]);
-      for (int k = 0; k < L.pose_dim[c]; ++k) L.param_block[L.pose_off[c] + k] = b;
+      for (int k = 0; k < L.pose_dim[c]; ++k) {
+        L.param_block[L.pose_off[c] + k] = b;
+        L.param_camera[L.pose_off[c] + k] = c;
+      }
     }
   for (size_t g = 0; g < L.intr_dim.size(); ++g)
     if (L.intr_dim[g] > 0) {
@@ -233,12 +248,7 @@ struct Hessian {
     // pose/intrinsic edge: find the camera owning the pose parameter
     int pose_param = row, intr_param = col;
     if (row >= L->intr_off.front()) std::swap(pose_param, intr_param);
-    int cam = -1;
-    for (int c = 0; c < N->ncam; ++c)
-      if (L->pose_dim[c] > 0 && pose_param >= L->pose_off[c] && pose_param < L->pose_off[c] + L->pose_dim[c]) {
-        cam = c;
-        break;
-      }
+    const int cam = L->param_camera[pose_param];
     if (cam < 0) {
       valid = false;
       return;
@@ -1139,7 +1149,10 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
     for (uint64_t it = 0; it < st.max_iterations; ++it) {
       run.iterations++;
       GaugeState g = make_gauge(n, poses, scene);
+      double t_it = oracle_now();
       Assembly a = S.assemble(poses, points, groups, g, st.loss, run.damping.value, direct, ws);
+      oracle_phase("assemble", t_it);
+      t_it = oracle_now();
       if (!have_initial && std::isfinite(a.cost) && std::isfinite(a.sq) && N > 0) {
         init_cost = a.cost;
         init_rmse = std::sqrt(a.sq / double(2 * N));
@@ -1186,6 +1199,8 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
         iterative_step = true;
         rel_res = r.relative_residual;
       }
+      oracle_phase("camera step", t_it);
+      t_it = oracle_now();
       // candidate: step cap (calibrated only), retraction
       if (!n.self_cal) {
         double largest = 0.0;
@@ -2130,7 +2145,9 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
   if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR)
     fail(OMVGBA_UNSUPPORTED, "angular residuals are not supported by this adjuster");
+  double t0 = oracle_now();
   Native n = has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+  oracle_phase("lowering", t0);
   Layout L = make_layout(n);
   Options opt;
   opt.max_iterations = cfg.max_iterations;
@@ -2142,10 +2159,14 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   std::vector<NPose> poses = n.poses;
   std::vector<Vec3> points = n.points;
   std::vector<Radial> groups = n.groups;
+  t0 = oracle_now();
   NativeReport nr = refine(n, poses, points, groups, opt);
+  oracle_phase("refine", t0);
+  t0 = oracle_now();
   Result res = raise(pr, n, poses, points, groups, nr, opt.iterative);
   finish_solution(pr, res);
   canonicalize(pr, res);
+  oracle_phase("report", t0);
   return res;
 }
 
@@ -2326,7 +2347,9 @@ static Result solve_with_quarantine(const omvgba_problem& pr, const omvgba_confi
   for (size_t o = 0; o < pr.observation_count; ++o) counts[pr.observation_point[o]]++;
   std::vector<uint8_t> weak(pr.point_count, 0);
   for (size_t p = 0; p < pr.point_count; ++p) weak[p] = counts[p] < 2;
+  double t0 = oracle_now();
   for (size_t p : degenerate_points(pr, pr.poses, pr.points)) weak[p] = 1;
+  oracle_phase("degenerate points", t0);
   std::set<size_t> input_deg;
   for (size_t p = 0; p < pr.point_count; ++p)
     if (weak[p] && !point_fixed(pr, p)) input_deg.insert(p);

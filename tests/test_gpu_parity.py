@@ -125,3 +125,24 @@ def test_mixed_precision_reaches_fp64_final_cost(adjuster, self_cal):
     f64 = adjuster.solve(p, base)
     mix = adjuster.solve(p, base.with_(precision=abi.PRECISION_MIXED))
     assert _rel(mix.report["final_objective"], f64.report["final_objective"]) < 1e-6
+
+
+@pytest.mark.parametrize("loss", ["cauchy", "squared"])
+@pytest.mark.parametrize("solver", [abi.SOLVER_DIRECT, abi.SOLVER_ITERATIVE])
+def test_cauchy_and_squared_losses_match_oracle(adjuster, loss, solver):
+    """Cauchy runs the reference's continuation (squared warm-up stage, then Cauchy,
+    continuation.rs:18-74); the squared loss runs one stage with unit weights. Same iteration,
+    acceptance and status counts as the oracle, final cost to 1e-9, parameters to 1e-7."""
+    from openmvg_ba_cuda import RobustLoss
+    rl = RobustLoss.cauchy(2.0) if loss == "cauchy" else RobustLoss.squared()
+    p = synthetic.ring_problem(seed=17, loss=rl)
+    cfg = SolveConfig(linear_solver=solver, max_iterations=25, pcg_relative_tolerance=1e-10)
+    g = adjuster.solve(p, cfg)
+    o = O.solve(p, cfg)
+    rg, ro = g.report, o.report
+    for k in ("iteration_count", "accepted_step_count", "rejected_step_count", "status", "quarantined_point_count",
+              "inlier_count"):
+        assert rg[k] == ro[k], (k, rg[k], ro[k])
+    assert _rel(rg["initial_objective"], ro["initial_objective"]) < 1e-12
+    assert _rel(rg["final_objective"], ro["final_objective"]) < 1e-9
+    _check_parameters(g, o, _oracle_spread(p, cfg))

@@ -1,0 +1,602 @@
+// explicit_s.cuh — the explicit reduced camera system S and its banded tiled FP64 Cholesky factor.
+//
+// S = U - W Vhat^-1 W^T over the free camera parameters (schur/assembly.rs:832-1069 assembles the same
+// matrix into faer's sparse pattern, sparse/direct_assembly.rs:371-687). Here it is built by block
+// rows: one CTA per parameter block X computes every block S_XY of its row (all co-visible blocks Y,
+// both triangles), walking X's entities in a fixed order and the entities of each entity's point, so
+// the row is the same bits run to run and needs no atomics. The rows serve as a block-sparse (BSR)
+// operator directly (the PCG product and the model reduction) and are scattered into a banded tiled
+// matrix for the factorization.
+//
+// Factorization. The parameter blocks are permuted so that each camera's pose block is followed by
+// the intrinsic blocks it introduces; with cameras in their native order the co-visibility graph of
+// a survey is banded, so the factor fits in a band of tiles (64 x 64 FP64, column-major) and a
+// right-looking tiled Cholesky (POTRF of the diagonal tile, TRSM of the tiles below it, SYRK/GEMM
+// update of the trailing band) never leaves the band. faer's sparse LLT with an AMD ordering
+// (numerics/sparse.rs:119-250) factors the same matrix; the factors agree to rounding and the
+// positive-definiteness decision is the same away from rounding-level pivots. Every tile update
+// runs in a fixed order, so the factor is bitwise reproducible.
+//
+// Uses of the factor: the direct camera step (sparse/direct.rs:259-288), the camera rank test of the
+// final undamped system (sparse/direct.rs:288-455: the spectral test after Jacobi equilibration
+// when D <= 2048, a factorization otherwise), and the self-calibration intrinsic marginal
+// covariances (sparse/covariance.rs:564-587): (S^-1)_pq = (L^-1 e_p) . (L^-1 e_q), forward solves only.
+#pragma once
+
+#include <cstdint>
+
+namespace omvgba {
+
+// ---- block rows ---------------------------------------------------------------------------------
+struct RowTables {
+  int nblocks;
+  const int* blk_dim;
+  const int* blk_off;
+  const uint32_t* blk_ent;    // nb + 1: each block's range in ent
+  const uint32_t* ent;        // entity list (observation * 2 + segment), block-major
+  const uint32_t* ent_point;  // point of each entity (same order)
+  const int* seg_col;         // per entity id: column of its segment in the observation's record
+  const int* ent_block;       // per entity id: parameter block, -1 when absent
+  const uint32_t* pt_off;     // P + 1
+  const uint32_t* nbr_begin;  // nb + 1: each block's range in nbr / slot_off
+  const int* nbr;             // neighbour blocks of each block (ascending; the block itself included)
+  const int* nbr_row;         // block owning each neighbour entry
+  const uint64_t* slot_off;   // entries + 1: offset of block S_XY (dX x dY, row-major) in the rows
+  uint32_t entries;           // neighbour entries in total
+};
+
+constexpr int kRowThreads = 128;
+
+__device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n0, uint32_t n1, int Y) {
+  uint32_t lo = n0, hi = n1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (nbr[mid] < Y)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < n1 && nbr[lo] == Y) ? (int)(lo - n0) : -1;
+}
+
+// Row X of S. For each entity e of X (observation o at point p, camera columns cX..cX+dX) and each
+// entity e' of p in block Y (observation o', columns cY..): S_XY += Jc_e^T M Jc_e' with the 2 x 2
+// M = [o == o'] I - Jp_o Vhat_p^-1 Jp_o'^T (U, the pose/intrinsic edges and the point coupling in one
+// term). Targets of one point that fall in the same block are summed in target order by one thread
+// per element; entities are taken one after another, so every element is accumulated in entity
+// order. FP64 accumulation from records of type R. Dynamic shared memory: max_track x 24 doubles
+// plus 2 x 2 x max_track ints.
+template <typename R>
+__global__ void __launch_bounds__(kRowThreads) k_block_rows(RowTables rt, LinOut<R> lin, int max_track,
+                                                            double* __restrict__ rows) {
+  extern __shared__ double smem[];
+  double* jr = smem;                                            // per observation of the point: 24 record values
+  int* tslot = reinterpret_cast<int*>(jr + (size_t)max_track * kRec);  // per target: slot or -1
+  int* tcol = tslot + 2 * max_track;                            // per target: column of its segment
+  __shared__ double G[6];                                       // Jp_o Vhat^-1 (2 x 3)
+  __shared__ double aX[12];                                     // the entity's 2 x dX camera columns
+  const int X = blockIdx.x, tid = threadIdx.x;
+  if (X >= rt.nblocks) return;
+  const int dX = rt.blk_dim[X];
+  const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1];
+  const uint64_t r0 = rt.slot_off[n0], r1 = rt.slot_off[n1];
+  for (uint64_t k = r0 + tid; k < r1; k += blockDim.x) rows[k] = 0.0;
+  const int rs = lin.rs;
+  for (uint32_t i = rt.blk_ent[X]; i < rt.blk_ent[X + 1]; ++i) {
+    const uint32_t e = rt.ent[i], o = e >> 1, p = rt.ent_point[i];
+    const uint32_t o0 = rt.pt_off[p], L = rt.pt_off[p + 1] - o0;
+    __syncthreads();  // the previous entity is finished with the staging (and the row is zeroed)
+    for (uint32_t k = tid; k < (uint32_t)kRec * L; k += blockDim.x) {
+      const uint32_t c = k / L, j = k - c * L;
+      jr[j * kRec + c] = (double)lin.rec[lin.obs_rec[o0 + j] + (size_t)c * rs];
+    }
+    for (uint32_t t = tid; t < 2 * L; t += blockDim.x) {
+      const uint32_t eid = 2 * (o0 + (t >> 1)) + (t & 1);
+      const int Y = rt.ent_block[eid];
+      tslot[t] = Y >= 0 ? find_slot(rt.nbr, n0, n1, Y) : -1;
+      tcol[t] = rt.seg_col[eid];
+    }
+    __syncthreads();
+    const uint32_t jo = o - o0;
+    if (tid == 0) {
+      const double* vi = lin.vinv + 6 * (size_t)p;
+      const double Vi[6] = {vi[0], vi[1], vi[2], vi[3], vi[4], vi[5]};
+      sym3_apply(Vi, jr + jo * kRec + kJp, G);
+      sym3_apply(Vi, jr + jo * kRec + kJp + 3, G + 3);
+      const int cX = rt.seg_col[e];
+      for (int m = 0; m < 6; ++m) {
+        aX[m] = m < dX ? jr[jo * kRec + cX + m] : 0.0;
+        aX[6 + m] = m < dX ? jr[jo * kRec + 9 + cX + m] : 0.0;
+      }
+    }
+    __syncthreads();
+    for (uint32_t w = tid; w < 2 * L * 36; w += blockDim.x) {
+      const uint32_t t = w / 36, mn = w - 36 * t, m = mn / 6, n = mn - 6 * m;
+      const int s = tslot[t];
+      if (s < 0 || (int)m >= dX) continue;
+      const int dY = rt.blk_dim[rt.nbr[n0 + s]];
+      if ((int)n >= dY) continue;
+      bool leader = true;
+      for (uint32_t t2 = 0; t2 < t; ++t2) leader = leader && tslot[t2] != s;
+      if (!leader) continue;
+      const double a0 = aX[m], a1 = aX[6 + m];
+      double acc = 0.0;
+      for (uint32_t t2 = t; t2 < 2 * L; ++t2) {
+        if (tslot[t2] != s) continue;
+        const uint32_t j = t2 >> 1;
+        const double* rj = jr + j * kRec;
+        double M00 = -(G[0] * rj[kJp] + G[1] * rj[kJp + 1] + G[2] * rj[kJp + 2]);
+        double M01 = -(G[0] * rj[kJp + 3] + G[1] * rj[kJp + 4] + G[2] * rj[kJp + 5]);
+        double M10 = -(G[3] * rj[kJp] + G[4] * rj[kJp + 1] + G[5] * rj[kJp + 2]);
+        double M11 = -(G[3] * rj[kJp + 3] + G[4] * rj[kJp + 4] + G[5] * rj[kJp + 5]);
+        if (j == jo) {
+          M00 += 1.0;
+          M11 += 1.0;
+        }
+        const int cY = tcol[t2];
+        const double b0 = rj[cY + n], b1 = rj[9 + cY + n];
+        acc += a0 * (M00 * b0 + M01 * b1) + a1 * (M10 * b0 + M11 * b1);
+      }
+      rows[rt.slot_off[n0 + s] + m * dY + n] += acc;
+    }
+  }
+}
+
+// y = (S + lambda diag) x from the block rows: one warp per block row, lanes over the row's entries
+// in a fixed assignment, then a fixed shuffle tree. With scale non-null the operator is the Jacobi-
+// equilibrated D S D (D = diag(scale)) and lambda must be 0. With xy non-null, xy[CTA] = sum of
+// x_b . y_b over the CTA's blocks in block order.
+__global__ void __launch_bounds__(256) k_rows_matvec(RowTables rt, const double* __restrict__ rows,
+                                                     const double* __restrict__ diag, double lambda,
+                                                     const double* __restrict__ scale,
+                                                     const double* __restrict__ x, double* __restrict__ y,
+                                                     double* __restrict__ xy, const PcgCtl* ctl) {
+  __shared__ double s_dot[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int X = blockIdx.x * 8 + warp;
+  const bool have = X < rt.nblocks;
+  pdl_trigger();
+  pdl_wait();
+  if (pcg_stopped(ctl)) return;
+  double dot = 0.0;
+  if (have) {
+    const int dX = rt.blk_dim[X], oX = rt.blk_off[X];
+    const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t q = n0 + lane; q < n1; q += 32) {
+      const int Y = rt.nbr[q];
+      const int dY = rt.blk_dim[Y], oY = rt.blk_off[Y];
+      const double* S = rows + rt.slot_off[q];
+      double xv[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) xv[c] = c < dY ? x[oY + c] * (scale ? scale[oY + c] : 1.0) : 0.0;
+#pragma unroll
+      for (int m = 0; m < 6; ++m)
+        if (m < dX) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < 6; ++c)
+            if (c < dY) s += S[m * dY + c] * xv[c];
+          acc[m] += s;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) acc[m] = warp_sum(acc[m]);
+    if (lane == 0) {
+      for (int m = 0; m < dX; ++m) {
+        double v = acc[m];
+        if (scale) v *= scale[oX + m];
+        v += lambda * diag[oX + m] * x[oX + m];
+        y[oX + m] = v;
+        dot += x[oX + m] * v;
+      }
+    }
+  }
+  if (xy) {
+    if (lane == 0) s_dot[warp] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += s_dot[w];
+      xy[blockIdx.x] = t;
+    }
+  }
+}
+
+// Diagonal of S (no damping) from the rows: thread per block, its own slot.
+__global__ void k_rows_diag(RowTables rt, const double* __restrict__ rows, double* __restrict__ out) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  if (X >= rt.nblocks) return;
+  const int dX = rt.blk_dim[X], oX = rt.blk_off[X];
+  const int s = find_slot(rt.nbr, rt.nbr_begin[X], rt.nbr_begin[X + 1], X);
+  const double* S = s >= 0 ? rows + rt.slot_off[rt.nbr_begin[X] + s] : nullptr;
+  for (int m = 0; m < dX; ++m) out[oX + m] = S ? S[m * dX + m] : 0.0;
+}
+
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+// ---- banded tiled matrix -----------------------------------------------------------------------
+constexpr int kCT = 64;  // tile edge
+constexpr int kCTT = kCT * kCT;
+
+// Lower band of tiles of an n x n symmetric matrix in the permuted order: tile (i, j), 0 <= i - j <=
+// bwt, at t + (i (bwt + 1) + (i - j)) kCTT, column-major inside the tile. Rows past n are padding
+// (identity on the diagonal).
+struct TileBand {
+  int n, nt, bwt;
+  double* t;
+};
+__host__ __device__ __forceinline__ size_t tile_at(const TileBand& b, int i, int j) {
+  return ((size_t)i * (b.bwt + 1) + (size_t)(i - j)) * kCTT;
+}
+
+// Scatter of the rows into the band: element (m, n) of block S_XY lands at permuted (P, Q) =
+// (perm_off[X] + m, perm_off[Y] + n) when P >= Q. With scale non-null the stored value is
+// scale_P S_PQ scale_Q; the diagonal gets + lambda diag_P, then - shift. One thread per entry.
+__global__ void k_rows_to_tiles(RowTables rt, const double* __restrict__ rows, const int* __restrict__ perm_off,
+                                const double* __restrict__ diag, double lambda, const double* __restrict__ scale,
+                                double shift, TileBand tb) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= rt.entries) return;
+  const int X = rt.nbr_row[q], Y = rt.nbr[q];
+  const int dX = rt.blk_dim[X], dY = rt.blk_dim[Y];
+  const int pX = perm_off[X], pY = perm_off[Y], oX = rt.blk_off[X], oY = rt.blk_off[Y];
+  const double* S = rows + rt.slot_off[q];
+  for (int m = 0; m < dX; ++m)
+    for (int n = 0; n < dY; ++n) {
+      const int P = pX + m, Q = pY + n;
+      if (P < Q) continue;
+      double v = S[m * dY + n];
+      if (scale) v *= scale[oX + m] * scale[oY + n];
+      if (P == Q) v += lambda * diag[oX + m] - shift;
+      tb.t[tile_at(tb, P / kCT, Q / kCT) + (size_t)(Q % kCT) * kCT + (P % kCT)] = v;
+    }
+}
+
+// Identity on the padding rows of the last diagonal tile.
+__global__ void k_tiles_pad(TileBand tb) {
+  const int r = tb.n + threadIdx.x;
+  if (r >= tb.nt * kCT) return;
+  const int i = tb.nt - 1;
+  tb.t[tile_at(tb, i, i) + (size_t)(r % kCT) * kCT + (r % kCT)] = 1.0;
+}
+
+// POTRF of diagonal tile k (right-looking inside the tile). status[0] = 0 when a pivot is not finite
+// and positive; later launches of the factorization then return at once.
+__global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* status) {
+  __shared__ double A[kCT * (kCT + 1)];
+  __shared__ int fail;
+  if (status[0] == 0) return;
+  const int tid = threadIdx.x;
+  double* g = tb.t + tile_at(tb, k, k);
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    A[c * (kCT + 1) + r] = g[w];
+  }
+  if (tid == 0) fail = 0;
+  for (int j = 0; j < kCT; ++j) {
+    __syncthreads();
+    if (tid == 0) {
+      const double d = A[j * (kCT + 1) + j];
+      if (!(isfinite(d) && d > 0.0))
+        fail = 1;
+      else
+        A[j * (kCT + 1) + j] = sqrt(d);
+    }
+    __syncthreads();
+    if (fail) break;
+    const double piv = A[j * (kCT + 1) + j];
+    for (int i = j + 1 + tid; i < kCT; i += blockDim.x) A[j * (kCT + 1) + i] /= piv;
+    __syncthreads();
+    const int m = kCT - j - 1;
+    for (int w = tid; w < m * m; w += blockDim.x) {
+      const int c = j + 1 + w / m, i = j + 1 + w % m;
+      if (c <= i) A[c * (kCT + 1) + i] -= A[j * (kCT + 1) + i] * A[j * (kCT + 1) + c];
+    }
+  }
+  __syncthreads();
+  if (fail) {
+    if (tid == 0) status[0] = 0;
+    return;
+  }
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    g[w] = r >= c ? A[c * (kCT + 1) + r] : 0.0;
+  }
+}
+
+// TRSM: the tiles below diagonal tile k, L_ik = A_ik L_kk^-T (CTA per tile, thread per row). Dynamic
+// shared memory: two padded tiles (kTrsmSmem bytes).
+constexpr size_t kTrsmSmem = 2 * sizeof(double) * kCT * (kCT + 1);
+constexpr size_t kUpdateSmem = 2 * sizeof(double) * kCTT;
+__global__ void __launch_bounds__(kCT) k_tile_trsm(TileBand tb, int k, const int* status) {
+  extern __shared__ double shm[];
+  double* Lk = shm;
+  double* B = shm + kCT * (kCT + 1);
+  if (status[0] == 0) return;
+  const int i = k + 1 + blockIdx.x, tid = threadIdx.x;
+  const double* lk = tb.t + tile_at(tb, k, k);
+  double* bi = tb.t + tile_at(tb, i, k);
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    Lk[c * (kCT + 1) + r] = lk[w];
+    B[c * (kCT + 1) + r] = bi[w];
+  }
+  __syncthreads();
+  const int r = tid;  // X[r][c] = (B[r][c] - sum_{m<c} X[r][m] Lk[c][m]) / Lk[c][c]
+  for (int c = 0; c < kCT; ++c) {
+    double v = B[c * (kCT + 1) + r];
+    for (int m = 0; m < c; ++m) v -= B[m * (kCT + 1) + r] * Lk[m * (kCT + 1) + c];
+    B[c * (kCT + 1) + r] = v / Lk[c * (kCT + 1) + c];
+  }
+  __syncthreads();
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, rr = w - c * kCT;
+    bi[w] = B[c * (kCT + 1) + rr];
+  }
+}
+
+// Trailing update of step k: A_ij -= L_ik L_jk^T for k < j <= i <= min(k + bwt, nt - 1), one CTA per
+// tile, 16 x 16 threads with 4 x 4 outputs each; the sum over the tile's 64 columns runs in order.
+// Dynamic shared memory: two tiles (64 KB).
+__global__ void __launch_bounds__(256) k_tile_update(TileBand tb, int k, const int* status) {
+  extern __shared__ double sh[];
+  if (status[0] == 0) return;
+  double* Ti = sh;         // L_ik column-major: Ti[q * 64 + r] = L_ik[r][q]
+  double* Tj = sh + kCTT;  // L_jk column-major
+  int idx = blockIdx.x;
+  int ii = 0;
+  while ((ii + 1) * (ii + 2) / 2 <= idx) ++ii;
+  const int jj = idx - ii * (ii + 1) / 2;
+  const int i = k + 1 + ii, j = k + 1 + jj;
+  const int tid = threadIdx.x;
+  const double2* li = reinterpret_cast<const double2*>(tb.t + tile_at(tb, i, k));
+  const double2* lj = reinterpret_cast<const double2*>(tb.t + tile_at(tb, j, k));
+  for (int w = tid; w < kCTT / 2; w += blockDim.x) {
+    reinterpret_cast<double2*>(Ti)[w] = li[w];
+    reinterpret_cast<double2*>(Tj)[w] = lj[w];
+  }
+  __syncthreads();
+  const int ty = tid >> 4, tx = tid & 15;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+#pragma unroll 4
+  for (int q = 0; q < kCT; ++q) {
+    const double2 a01 = *reinterpret_cast<const double2*>(Ti + q * kCT + 4 * ty);
+    const double2 a23 = *reinterpret_cast<const double2*>(Ti + q * kCT + 4 * ty + 2);
+    const double2 b01 = *reinterpret_cast<const double2*>(Tj + q * kCT + 4 * tx);
+    const double2 b23 = *reinterpret_cast<const double2*>(Tj + q * kCT + 4 * tx + 2);
+    const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+  }
+  double* cij = tb.t + tile_at(tb, i, j);
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = 4 * tx + b;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = 4 * ty + a;
+      cij[(size_t)c * kCT + r] -= acc[a][b];
+    }
+  }
+}
+
+// Forward (L y = b) and backward (L^T x = y) substitution with the banded tiled factor, one CTA of
+// 256 threads, in place on the permuted vector v (n entries; the padding is not touched). Four
+// threads per row of a tile sum the band's products in quarters, combined in a fixed order; the
+// triangle inside a tile is solved by one warp with a fixed shuffle tree per row.
+__device__ void tile_forward_rows(const TileBand& tb, double* v, int i, int j_lo, double* part, double* yt) {
+  const int tid = threadIdx.x, r = tid & (kCT - 1), qtr = tid >> 6;  // 256 threads: 4 quarters
+  double s = 0.0;
+  const int j_first = max(j_lo, i - tb.bwt);
+  for (int j = j_first; j < i; ++j) {
+    const double* L = tb.t + tile_at(tb, i, j);
+    for (int c = qtr; c < kCT; c += 4) s += L[(size_t)c * kCT + r] * v[j * kCT + c];
+  }
+  part[qtr * kCT + r] = s;
+  __syncthreads();
+  if (tid < kCT) {
+    const int rr = tid;
+    const int P = i * kCT + rr;
+    const double b = P < tb.n ? v[P] : 0.0;
+    yt[rr] = b - (((part[rr] + part[kCT + rr]) + part[2 * kCT + rr]) + part[3 * kCT + rr]);
+  }
+  __syncthreads();
+  if (tid < 32) {  // in-tile forward solve, one warp
+    const double* L = tb.t + tile_at(tb, i, i);
+    for (int rr = 0; rr < kCT; ++rr) {
+      double d = 0.0;
+      for (int c = tid; c < rr; c += 32) d += L[(size_t)c * kCT + rr] * yt[c];
+      d = warp_sum(d);
+      if (tid == 0) yt[rr] = (yt[rr] - d) / L[(size_t)rr * kCT + rr];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (tid < kCT) {
+    const int P = i * kCT + tid;
+    if (P < tb.n) v[P] = yt[tid];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_tile_solve(TileBand tb, double* v, const int* status) {
+  __shared__ double part[4 * kCT];
+  __shared__ double yt[kCT];
+  if (status[0] == 0) return;
+  const int tid = threadIdx.x, r = tid & (kCT - 1), qtr = tid >> 6;
+  for (int i = 0; i < tb.nt; ++i) tile_forward_rows(tb, v, i, 0, part, yt);
+  for (int i = tb.nt - 1; i >= 0; --i) {
+    // x_i = L_ii^-T (y_i - sum_{j > i} L_ji^T x_j)
+    double s = 0.0;
+    const int j_last = min(tb.nt - 1, i + tb.bwt);
+    for (int j = i + 1; j <= j_last; ++j) {
+      const double* L = tb.t + tile_at(tb, j, i);
+      for (int c = qtr; c < kCT; c += 4) {
+        const int Q = j * kCT + c;
+        if (Q < tb.n) s += L[(size_t)r * kCT + c] * v[Q];
+      }
+    }
+    part[qtr * kCT + r] = s;
+    __syncthreads();
+    if (tid < kCT) {
+      const int P = i * kCT + tid;
+      const double b = P < tb.n ? v[P] : 0.0;
+      yt[tid] = b - (((part[tid] + part[kCT + tid]) + part[2 * kCT + tid]) + part[3 * kCT + tid]);
+    }
+    __syncthreads();
+    if (tid < 32) {  // in-tile backward solve with L_ii^T
+      const double* L = tb.t + tile_at(tb, i, i);
+      for (int rr = kCT - 1; rr >= 0; --rr) {
+        double d = 0.0;
+        for (int c = rr + 1 + tid; c < kCT; c += 32) d += L[(size_t)rr * kCT + c] * yt[c];
+        d = warp_sum(d);
+        if (tid == 0) yt[rr] = (yt[rr] - d) / L[(size_t)rr * kCT + rr];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (tid < kCT) {
+      const int P = i * kCT + tid;
+      if (P < tb.n) v[P] = yt[tid];
+    }
+    __syncthreads();
+  }
+}
+
+// Gather / scatter between the original and the permuted parameter order.
+__global__ void k_perm_gather(int n, const int* __restrict__ perm_to_orig, const double* __restrict__ src,
+                              double sign, double* __restrict__ dst) {
+  const int P = blockIdx.x * blockDim.x + threadIdx.x;
+  if (P < n) dst[P] = sign * src[perm_to_orig[P]];
+}
+__global__ void k_perm_scatter(int n, const int* __restrict__ perm_to_orig, const double* __restrict__ src,
+                               double* __restrict__ dst) {
+  const int P = blockIdx.x * blockDim.x + threadIdx.x;
+  if (P < n) dst[perm_to_orig[P]] = src[P];
+}
+
+// Intrinsic marginal covariances: CTA per free intrinsic group. For each of the group's parameters
+// (permuted positions pos[3 g .. 3 g + dim)) the forward solve y = L^-1 e_P, which is zero above
+// P's tile; then M_kl = sum_P y_k[P] y_l[P] (fixed order). scratch: 3 n doubles per CTA.
+// out: 9 per group, row-major; a non-finite result is left for the host to see.
+__global__ void __launch_bounds__(256) k_tile_marginals(TileBand tb, int ngroups, const int* __restrict__ pos,
+                                                        const int* __restrict__ dims, double* scratch,
+                                                        double* __restrict__ out, const int* status) {
+  __shared__ double part[4 * kCT];
+  __shared__ double yt[kCT];
+  __shared__ double red[8][9];
+  if (status[0] == 0) return;
+  const int g = blockIdx.x, tid = threadIdx.x;
+  if (g >= ngroups) return;
+  const int dim = dims[g];
+  int lo = tb.n;
+  for (int k = 0; k < dim; ++k) lo = min(lo, pos[3 * g + k]);
+  const int i0 = lo / kCT;
+  double* y = scratch + (size_t)blockIdx.x * 3 * tb.n;
+  for (int k = 0; k < dim; ++k) {
+    double* v = y + (size_t)k * tb.n;
+    for (int P = i0 * kCT + tid; P < tb.n; P += blockDim.x) v[P] = P == pos[3 * g + k] ? 1.0 : 0.0;
+    __syncthreads();
+    for (int i = i0; i < tb.nt; ++i) tile_forward_rows(tb, v, i, i0, part, yt);
+  }
+  // Gram of the solves, rows from i0 * 64 on (fixed per-thread stride, fixed shuffle and warp order)
+  double acc[9];
+  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  for (int P = i0 * kCT + tid; P < tb.n; P += blockDim.x)
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) acc[3 * a + b] += y[(size_t)a * tb.n + P] * y[(size_t)b * tb.n + P];
+  for (int k = 0; k < 9; ++k) acc[k] = warp_sum(acc[k]);
+  if ((tid & 31) == 0)
+    for (int k = 0; k < 9; ++k) red[tid >> 5][k] = acc[k];
+  __syncthreads();
+  if (tid < 9) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w][tid];
+    out[9 * (size_t)g + tid] = s;
+  }
+}
+
+// Largest |eigenvalue| of the equilibrated D S D by power iteration (Rayleigh quotient of the
+// normalized iterate), one CTA of 1024 threads running every iteration, so the host waits once:
+// out[0] = lambda, out[1] = 1 when it settled (|rq - lambda| <= 1e-10 |rq| after the 8th iteration) or
+// ran its 200 iterations with finite values, 0 otherwise. v, w: n doubles of scratch.
+__global__ void __launch_bounds__(1024) k_power_iteration(RowTables rt, const double* __restrict__ rows,
+                                                          const double* __restrict__ scale, int n, double* v,
+                                                          double* w, double* out) {
+  __shared__ double red[32][2];
+  __shared__ double s_nrm, s_rq;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double v0 = 1.0 / sqrt((double)n);
+  for (int i = tid; i < n; i += blockDim.x) v[i] = v0;
+  __syncthreads();
+  double lam = 0.0;
+  int ok = 0;
+  for (int it = 0; it < 200; ++it) {
+    // w = D S D v: warp per block row
+    for (int X = warp; X < rt.nblocks; X += 32) {
+      const int dX = rt.blk_dim[X], oX = rt.blk_off[X];
+      const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1];
+      double acc[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t q = n0 + lane; q < n1; q += 32) {
+        const int Y = rt.nbr[q];
+        const int dY = rt.blk_dim[Y], oY = rt.blk_off[Y];
+        const double* S = rows + rt.slot_off[q];
+        for (int m = 0; m < dX; ++m) {
+          double s = 0.0;
+          for (int c = 0; c < dY; ++c) s += S[m * dY + c] * (scale[oY + c] * v[oY + c]);
+          acc[m] += s;
+        }
+      }
+      for (int m = 0; m < 6; ++m) acc[m] = warp_sum(acc[m]);
+      if (lane == 0)
+        for (int m = 0; m < dX; ++m) w[oX + m] = acc[m] * scale[oX + m];
+    }
+    __syncthreads();
+    double nn = 0.0, rq = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+      nn += w[i] * w[i];
+      rq += v[i] * w[i];
+    }
+    nn = warp_sum(nn);
+    rq = warp_sum(rq);
+    if (lane == 0) {
+      red[warp][0] = nn;
+      red[warp][1] = rq;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int k = 0; k < 32; ++k) {
+        a += red[k][0];
+        b += red[k][1];
+      }
+      s_nrm = sqrt(a);
+      s_rq = b;
+    }
+    __syncthreads();
+    const double nrm = s_nrm, q = s_rq;
+    if (!(isfinite(nrm) && nrm > 0.0)) {
+      ok = 0;
+      break;
+    }
+    const bool settled = it > 8 && fabs(q - lam) <= 1e-10 * fabs(q);
+    lam = q;
+    for (int i = tid; i < n; i += blockDim.x) v[i] = w[i] / nrm;
+    __syncthreads();
+    ok = 1;
+    if (settled) break;
+  }
+  if (tid == 0) {
+    out[0] = lam;
+    out[1] = ok;
+  }
+}
+
+}  // namespace omvgba

@@ -7,7 +7,8 @@
 //   K2  k_block_chunks ..... camera-side deterministic segmented reductions: U blocks, g, reduced g,
 //                            damping diagonal, pose/intrinsic edges, diagonal point coupling
 //       k_pairs ............ explicit Schur blocks S_bb' -= W V^-1 W^T (schur/assembly.rs:999-1038)
-//   K3  k_dense_cholesky ... dense FP64 Cholesky for small reduced systems (stands in for faer LLT)
+//   K3  k_block_rows ....... explicit S by block rows (BSR), banded tiled FP64 Cholesky and solves
+//                            (explicit_s.cuh; stands in for faer's sparse LLT)
 //       k_mv_tiles ......... matrix-free reduced-camera-system product S x (retained/operator.rs:137-227)
 //       block-Jacobi PCG ... sparse/pcg.rs:23-119, retained/mod.rs:682-934, retained/block.rs:148-246
 //   K4  k_retract, k_candidate_points: step cap, retraction, back-substitution and candidate rule
@@ -826,116 +827,6 @@ __global__ void __launch_bounds__(32) k_pairs(PairTables pt, BlockTables bt, Lin
   }
 }
 
-// Dense S = U blocks + edges - pair sums + lambda * diag  (row-major D x D, both triangles)
-__global__ void k_dense_from_blocks(BlockTables bt, const double* blk_out, int D, double* S) {
-  int b = blockIdx.x;
-  if (b >= bt.nblocks) return;
-  const double* rec = blk_out + (size_t)kAsmRec * b;
-  int o = bt.blk_off[b], d = bt.blk_dim[b];
-  if (threadIdx.x == 0) {
-    int idx = 0;
-    for (int r = 0; r < 6; ++r)
-      for (int c = 0; c <= r; ++c, ++idx) {
-        if (r >= d || c >= d) continue;
-        S[(size_t)(o + r) * D + (o + c)] += rec[idx];
-        if (r != c) S[(size_t)(o + c) * D + (o + r)] += rec[idx];
-      }
-    int eb = bt.blk_edge[b];
-    if (eb >= 0) {
-      int io = bt.blk_off[eb], id = bt.blk_dim[eb];
-      for (int r = 0; r < d; ++r)
-        for (int k = 0; k < id; ++k) {
-          double v = rec[39 + 3 * r + k];
-          S[(size_t)(o + r) * D + (io + k)] += v;
-          S[(size_t)(io + k) * D + (o + r)] += v;
-        }
-    }
-  }
-}
-
-__global__ void k_dense_pairs(PairTables pt, BlockTables bt, const double* pair_out, int D, double* S) {
-  int gidx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gidx >= pt.ngroups) return;
-  int rb = pt.grp_row[gidx], cb = pt.grp_col[gidx];
-  int ro = bt.blk_off[rb], co = bt.blk_off[cb], dr = bt.blk_dim[rb], dc = bt.blk_dim[cb];
-  const double* v = pair_out + (size_t)36 * gidx;
-  // groups are unique per (row, col) with row >= col; diagonal groups hold both orientations
-  for (int r = 0; r < dr; ++r)
-    for (int c = 0; c < dc; ++c) {
-      double x = v[6 * r + c];
-      if (rb == cb) {
-        S[(size_t)(ro + r) * D + (co + c)] -= x;
-      } else {
-        S[(size_t)(ro + r) * D + (co + c)] -= x;
-        S[(size_t)(co + c) * D + (ro + r)] -= x;
-      }
-    }
-}
-
-__global__ void k_dense_add_diag(int D, const double* diag, double lambda, double* S) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < D) S[(size_t)i * D + i] += lambda * diag[i];
-}
-
-// Dense Cholesky (lower, in place) by one CTA, left-looking: every entry L[i][j] is one thread's
-// sequential dot over k < j, so the factor does not depend on the launch shape. status[0] = 1 on
-// success (every pivot finite and positive).
-__global__ void __launch_bounds__(1024) k_dense_cholesky(int D, double* A, int* status) {
-  __shared__ int ok;
-  __shared__ double piv;
-  if (threadIdx.x == 0) ok = 1;
-  __syncthreads();
-  for (int j = 0; j < D; ++j) {
-    if (threadIdx.x == 0) {
-      double s = A[(size_t)j * D + j];
-      for (int k = 0; k < j; ++k) s -= A[(size_t)j * D + k] * A[(size_t)j * D + k];
-      if (!(isfinite(s) && s > 0.0)) {
-        ok = 0;
-      } else {
-        piv = sqrt(s);
-        A[(size_t)j * D + j] = piv;
-      }
-    }
-    __syncthreads();
-    if (!ok) break;
-    double d = piv;
-    for (int i = j + 1 + threadIdx.x; i < D; i += blockDim.x) {
-      double v = A[(size_t)i * D + j];
-      for (int k = 0; k < j; ++k) v -= A[(size_t)i * D + k] * A[(size_t)j * D + k];
-      A[(size_t)i * D + j] = v / d;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) status[0] = ok;
-}
-
-// Solve L L^T x = b in place: row-oriented forward and backward substitution, one thread, so the
-// summation order is the textbook sequential one.
-__global__ void k_dense_solve(int D, const double* L, double* x) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int i = 0; i < D; ++i) {
-    double v = x[i];
-    for (int k = 0; k < i; ++k) v -= L[(size_t)i * D + k] * x[k];
-    x[i] = v / L[(size_t)i * D + i];
-  }
-  for (int i = D - 1; i >= 0; --i) {
-    double v = x[i];
-    for (int k = i + 1; k < D; ++k) v -= L[(size_t)k * D + i] * x[k];
-    x[i] = v / L[(size_t)i * D + i];
-  }
-}
-
-// y = S x for dense S (one warp per row), deterministic per-row order
-__global__ void k_dense_matvec(int D, const double* S, const double* x, double* y) {
-  int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (row >= D) return;
-  double s = 0.0;
-  for (int c = lane; c < D; c += 32) s += S[(size_t)row * D + c] * x[c];
-  s = warp_sum(s);
-  if (lane == 0) y[row] = s;
-}
-
 // ----------------------------------------------------------------------------------------------
 // Device-side PCG control (sparse/pcg.rs:23-119). One CTA computes each scalar reduction and, in
 // its epilogue, the recurrence coefficient and the loop status, so the PCG iterations run as a
@@ -1144,6 +1035,7 @@ __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const
 // ----------------------------------------------------------------------------------------------
 }  // namespace omvgba
 #include "mv_tiles.cuh"
+#include "explicit_s.cuh"
 namespace omvgba {
 
 // ----------------------------------------------------------------------------------------------
@@ -1554,19 +1446,26 @@ static Layout make_layout(const NativeProblem& n) {
 struct Setup {
   // block tables (host copies)
   std::vector<int> blk_off, blk_dim, blk_col, blk_edge;
+  std::vector<uint32_t> blk_ent;          // nb + 1: each block's range in ent
+  std::vector<int> cam_block, grp_block;  // parameter block of each camera's pose / each group, or -1
   FillVector<uint32_t> ent, ent_point;  // written completely by the construction
   std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
   std::vector<uint32_t> chunk_begin, chunk_end;
   FillVector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment (all written)
   FillVector<int> seg_col;       // per entity id (obs*2+seg): column (all written)
-  // pair tables
-  std::vector<int> grp_row, grp_col;
-  std::vector<uint32_t> grp_begin, grp_end, pair_a, pair_b, pair_p;
   // cross same-block pairs (preconditioner)
   std::vector<int> xgrp_row, xgrp_col;
   std::vector<uint32_t> xgrp_begin, xgrp_end, xpair_a, xpair_b, xpair_p;
   std::vector<int> blk_cross_begin, blk_cross_end;
   FillVector<int> ent_block;  // entity (observation * 2 + segment) -> parameter block, -1 when absent
+  // explicit S (block rows) and its banded factorization
+  std::vector<uint32_t> nbr_begin;  // nb + 1
+  std::vector<int> nbr, nbr_row;    // neighbour blocks of each block, ascending, and their row block
+  std::vector<uint64_t> slot_off;   // entries + 1
+  std::vector<int> perm_off;        // per block: first position in the factorization order
+  std::vector<int> perm_to_orig;    // D: parameter at each position of the factorization order
+  int bwt = 0, nt = 0;              // band width and side of the factor, in 64 x 64 tiles
+  int max_track = 0;                // longest track (staging of the block-row kernel)
 };
 
 // Tiles of the fused matvec for one record precision (host tables).
@@ -1739,7 +1638,7 @@ static void build_tiles(const NativeProblem& n, const Layout& L, const Setup& se
     }
 }
 
-static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_pairs, Setup& S) {
+static void build_tables(const NativeProblem& n, const Layout& L, Setup& S) {
   size_t N = n.obs_cam.size(), P = n.points.size() / 3;
   // blocks: pose blocks (camera order) then intrinsic blocks (group order)
   std::vector<int> cam_block(n.ncam, -1), grp_block(L.intr_dim.size(), -1);
@@ -1764,6 +1663,8 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
     for (int c = 0; c < n.ncam; ++c)
       if (cam_block[c] >= 0 && grp_block[n.cam_group[c]] >= 0) S.blk_edge[cam_block[c]] = grp_block[n.cam_group[c]];
   int nb = (int)S.blk_off.size();
+  S.cam_block = cam_block;
+  S.grp_block = grp_block;
   // entity lists per block (stable in observation order)
   // every entry is written below (-1: no block, column 0 and no intrinsic when absent)
   S.seg_col.resize(2 * N);
@@ -1812,6 +1713,7 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
     }
     counts[nb] = at;
   }
+  S.blk_ent = counts;
   S.ent.resize(counts[nb]);  // the fill below writes every position
   S.ent_point.resize(counts[nb]);
   FillVector<uint32_t> obs_point(N);
@@ -1866,13 +1768,11 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
   };
   // per point, in point order; point ranges run in parallel into their own lists, joined in order
   constexpr size_t kPairChunks = 64;
-  std::vector<std::vector<Pair>> chunk_pairs(kPairChunks), chunk_xpairs(kPairChunks);
+  std::vector<std::vector<Pair>> chunk_xpairs(kPairChunks);
   host_parallel_chunks(P, kPairChunks, [&](size_t c, size_t pb, size_t pe) {
-    std::vector<Pair>& pairs = chunk_pairs[c];
     std::vector<Pair>& xpairs = chunk_xpairs[c];
     std::vector<uint32_t> ents;
-    std::vector<int64_t> seen_at;  // point that last used each block (the same-block test)
-    if (!want_all_pairs) seen_at.assign(nb, -1);
+    std::vector<int64_t> seen_at(nb, -1);  // point that last used each block (the same-block test)
     for (size_t p = pb; p < pe; ++p) {
       if (n.fixed_points[p]) continue;
       ents.clear();
@@ -1881,14 +1781,12 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
         for (int sgm = 0; sgm < 2; ++sgm)
           if (ent_block[2 * o + sgm] >= 0) {
             ents.push_back((uint32_t)(2 * o + sgm));
-            if (!want_all_pairs) {
-              int64_t& s = seen_at[ent_block[2 * o + sgm]];
-              shared = shared || s == (int64_t)p;
-              s = (int64_t)p;
-            }
+            int64_t& s = seen_at[ent_block[2 * o + sgm]];
+            shared = shared || s == (int64_t)p;
+            s = (int64_t)p;
           }
-      // only same-block pairs are kept without the dense tables: none when every block is distinct
-      if (!want_all_pairs && !shared) continue;
+      // only same-block pairs are kept: none when every block of the point is distinct
+      if (!shared) continue;
       for (size_t i = 0; i < ents.size(); ++i)
         for (size_t j = 0; j <= i; ++j) {
           uint32_t a = ents[i], b = ents[j];
@@ -1897,20 +1795,12 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
             std::swap(a, b);
             std::swap(ba, bb);
           }
-          if (want_all_pairs) {
-            pairs.push_back({ba, bb, (uint32_t)p, a, b});
-            // a diagonal-block pair with distinct entities contributes both orientations
-            if (ba == bb && a != b) pairs.push_back({ba, bb, (uint32_t)p, b, a});
-          }
           if (ba == bb && a != b) xpairs.push_back({ba, bb, (uint32_t)p, a, b});
         }
     }
   });
-  std::vector<Pair> pairs, xpairs;
-  for (size_t c = 0; c < kPairChunks; ++c) {
-    pairs.insert(pairs.end(), chunk_pairs[c].begin(), chunk_pairs[c].end());
-    xpairs.insert(xpairs.end(), chunk_xpairs[c].begin(), chunk_xpairs[c].end());
-  }
+  std::vector<Pair> xpairs;
+  for (size_t c = 0; c < kPairChunks; ++c) xpairs.insert(xpairs.end(), chunk_xpairs[c].begin(), chunk_xpairs[c].end());
   auto build = [&](std::vector<Pair>& v, std::vector<int>& gr, std::vector<int>& gc, std::vector<uint32_t>& gb,
                    std::vector<uint32_t>& ge, std::vector<uint32_t>& pa, std::vector<uint32_t>& pbv,
                    std::vector<uint32_t>& pp) {
@@ -1936,7 +1826,6 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
       pp[k] = v[k].p;
     }
   };
-  if (want_all_pairs) build(pairs, S.grp_row, S.grp_col, S.grp_begin, S.grp_end, S.pair_a, S.pair_b, S.pair_p);
   build(xpairs, S.xgrp_row, S.xgrp_col, S.xgrp_begin, S.xgrp_end, S.xpair_a, S.xpair_b, S.xpair_p);
   for (size_t gidx = 0; gidx < S.xgrp_row.size(); ++gidx) {
     int b = S.xgrp_row[gidx];
@@ -1946,6 +1835,100 @@ static void build_tables(const NativeProblem& n, const Layout& L, bool want_all_
   for (int b = 0; b < nb; ++b)
     if (S.blk_cross_end[b] == 0) S.blk_cross_begin[b] = 0;
   S.ent_block = std::move(ent_block);
+}
+
+// Neighbour lists of the explicit S (every block Y that shares a point with block X, X included,
+// ascending), the offsets of the row blocks, and the factorization order: each camera's pose block,
+// then the intrinsic blocks whose first camera it is (cameras in native order), which makes the
+// reduced system of a survey banded. bwt is the band of the factor in tiles.
+static void build_explicit(const NativeProblem& n, const Layout& L, Setup& S) {
+  const int nb = (int)S.blk_off.size();
+  const size_t P = n.points.size() / 3;
+  S.max_track = 0;
+  for (size_t p = 0; p < P; ++p) S.max_track = std::max<int>(S.max_track, (int)(n.pt_off[p + 1] - n.pt_off[p]));
+  std::vector<std::vector<int>> nbrs(nb);
+  // blocks in contiguous ranges, one per host thread, each with its own marker array; every block's
+  // list depends only on the topology
+  const size_t nthreads = std::max<size_t>(1, std::min<size_t>(host_thread_limit(), (size_t)nb / 8 + 1));
+  const size_t per = ((size_t)nb + nthreads - 1) / nthreads;
+  auto run = [&](size_t k) {
+    const size_t b0 = std::min((size_t)nb, k * per), b1 = std::min((size_t)nb, b0 + per);
+    std::vector<int> stamp(nb, -1);
+    for (size_t X = b0; X < b1; ++X) {
+      std::vector<int>& out = nbrs[X];
+      for (uint32_t i = S.blk_ent[X]; i < S.blk_ent[X + 1]; ++i) {
+        const uint32_t p = S.ent_point[i];
+        for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o)
+          for (int sg = 0; sg < 2; ++sg) {
+            const int Y = S.ent_block[2 * o + sg];
+            if (Y >= 0 && stamp[Y] != (int)X) {
+              stamp[Y] = (int)X;
+              out.push_back(Y);
+            }
+          }
+      }
+      std::sort(out.begin(), out.end());
+    }
+  };
+  {
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < nthreads; ++k) pool.emplace_back(run, k);
+    run(0);
+    for (auto& t : pool) t.join();
+  }
+  S.nbr_begin.assign(nb + 1, 0);
+  for (int X = 0; X < nb; ++X) S.nbr_begin[X + 1] = S.nbr_begin[X] + (uint32_t)nbrs[X].size();
+  const size_t E = S.nbr_begin[nb];
+  S.nbr.resize(E);
+  S.nbr_row.resize(E);
+  S.slot_off.assign(E + 1, 0);
+  uint64_t off = 0;
+  for (int X = 0; X < nb; ++X)
+    for (size_t k = 0; k < nbrs[X].size(); ++k) {
+      const size_t q = S.nbr_begin[X] + k;
+      S.nbr[q] = nbrs[X][k];
+      S.nbr_row[q] = X;
+      S.slot_off[q] = off;
+      off += (uint64_t)S.blk_dim[X] * (uint64_t)S.blk_dim[nbrs[X][k]];
+    }
+  S.slot_off[E] = off;
+  // factorization order
+  std::vector<int> order;
+  order.reserve(nb);
+  std::vector<int> home(S.grp_block.size(), -1);
+  if (n.self_cal)
+    for (int c = n.ncam - 1; c >= 0; --c) home[n.cam_group[c]] = c;
+  std::vector<std::vector<int>> groups_at(std::max(1, n.ncam));
+  std::vector<int> homeless;
+  for (size_t g = 0; g < S.grp_block.size(); ++g)
+    if (S.grp_block[g] >= 0) {
+      if (home[g] >= 0)
+        groups_at[home[g]].push_back(S.grp_block[g]);
+      else
+        homeless.push_back(S.grp_block[g]);
+    }
+  for (int c = 0; c < n.ncam; ++c) {
+    if (S.cam_block[c] >= 0) order.push_back(S.cam_block[c]);
+    for (int b : groups_at[c]) order.push_back(b);
+  }
+  for (int b : homeless) order.push_back(b);
+  S.perm_off.assign(nb, 0);
+  S.perm_to_orig.assign(L.D, 0);
+  int pos = 0;
+  for (int b : order) {
+    S.perm_off[b] = pos;
+    for (int k = 0; k < S.blk_dim[b]; ++k) S.perm_to_orig[pos + k] = S.blk_off[b] + k;
+    pos += S.blk_dim[b];
+  }
+  S.nt = (L.D + kCT - 1) / kCT;
+  int bwt = 0;
+  for (int X = 0; X < nb; ++X)
+    for (uint32_t q = S.nbr_begin[X]; q < S.nbr_begin[X + 1]; ++q) {
+      const int Y = S.nbr[q];
+      if (S.perm_off[Y] > S.perm_off[X]) continue;
+      bwt = std::max(bwt, (S.perm_off[X] + S.blk_dim[X] - 1) / kCT - S.perm_off[Y] / kCT);
+    }
+  S.bwt = std::min(bwt, std::max(0, S.nt - 1));
 }
 
 uint64_t fnv1a(const void* data, size_t bytes, uint64_t h) {
@@ -1958,24 +1941,31 @@ uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
   const Layout L = make_layout(n);
   const bool direct = !opt.iterative;
   Setup S;
-  build_tables(n, L, direct || L.D <= opt.dense_rank_limit, S);
+  build_tables(n, L, S);
+  build_explicit(n, L, S);
   TileSet T;
   const bool mixed = opt.precision == 1 && !direct;
   build_tiles(n, L, S, mixed ? mv_tile_obs<float>() : mv_tile_obs<double>(), T);
   uint64_t h = 1469598103934665603ull;
   auto add = [&](const auto& v) { h = fnv1a(v.data(), v.size() * sizeof(v[0]), h); };
   for (const auto* v : {&S.blk_off, &S.blk_dim, &S.blk_col, &S.blk_edge, &S.chunk_block, &S.chunk_col,
-                        &S.blk_chunk_begin, &S.blk_chunk_end, &S.grp_row, &S.grp_col, &S.xgrp_row, &S.xgrp_col,
+                        &S.blk_chunk_begin, &S.blk_chunk_end, &S.xgrp_row, &S.xgrp_col,
                         &S.blk_cross_begin, &S.blk_cross_end})
     add(*v);
   add(S.obs_intr_col);
   add(S.seg_col);
   add(S.ent_block);
+  add(S.blk_ent);
+  add(S.nbr_begin);
+  add(S.nbr);
+  add(S.slot_off);
+  add(S.perm_off);
+  add(S.perm_to_orig);
+  h = fnv1a(&S.bwt, sizeof(S.bwt), h);
   add(S.ent);
   add(S.ent_point);
   add(T.obs_rec);
-  for (const auto* v : {&S.chunk_begin, &S.chunk_end, &S.grp_begin, &S.grp_end, &S.pair_a,
-                        &S.pair_b, &S.pair_p, &S.xgrp_begin, &S.xgrp_end, &S.xpair_a, &S.xpair_b, &S.xpair_p,
+  for (const auto* v : {&S.chunk_begin, &S.chunk_end, &S.xgrp_begin, &S.xgrp_end, &S.xpair_a, &S.xpair_b, &S.xpair_p,
                         &T.tile_hdr, &T.blk_part})
     add(*v);
   add(T.slots);
@@ -2045,12 +2035,16 @@ struct Solver {
   DBuf<double> d_gfull, d_gred, d_diag, d_diag_minmax;
   DBuf<int> d_clamp;
   // pairs
-  DBuf<int> d_grp_row, d_grp_col, d_xgrp_row, d_xgrp_col, d_blk_cross_begin, d_blk_cross_end;
-  DBuf<uint32_t> d_grp_begin, d_grp_end, d_pair_a, d_pair_b, d_pair_p;
+  DBuf<int> d_xgrp_row, d_xgrp_col, d_blk_cross_begin, d_blk_cross_end;
   DBuf<uint32_t> d_xgrp_begin, d_xgrp_end, d_xpair_a, d_xpair_b, d_xpair_p;
-  DBuf<double> d_pair_out, d_xpair_out;
-  DBuf<double> d_S, d_Lf;
+  DBuf<double> d_xpair_out;
   DBuf<int> d_status;
+  // explicit S: block rows, permutation and the banded tiled factor
+  DBuf<uint32_t> d_blk_ent, d_nbr_begin;
+  DBuf<int> d_ent_block, d_nbr, d_nbr_row, d_perm_off, d_perm_to_orig;
+  DBuf<uint64_t> d_slot_off;
+  DBuf<double> d_rows, d_tiles, d_perm_vec, d_marg_scratch, d_marg_out, d_power;
+  bool rows_valid = false;  // the rows hold S of the current assembly
   // PCG vectors
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
   DBuf<int> d_fail;
@@ -2072,7 +2066,8 @@ struct Solver {
     ng = n.self_cal ? (int)n.group_dim.size() : 0;
     direct = !opt.iterative;
     const double t0 = now();
-    build_tables(n, L, direct || D <= opt.dense_rank_limit, S);
+    build_tables(n, L, S);
+    build_explicit(n, L, S);
     const double t1 = now();
     // mixed precision keeps only FP32 Jacobian records (and their tiles); FP64 mode only FP64 ones
     mixed = opt.precision == 1 && !direct;
@@ -2136,29 +2131,38 @@ struct Solver {
     b.blk_chunk_end = d_blk_chunk_end.p;
     return b;
   }
-  PairTables pairs(bool cross) const {
+  // cross same-block pairs of the block-Jacobi preconditioner
+  PairTables pairs() const {
     PairTables t;
-    if (cross) {
-      t.ngroups = (int)S.xgrp_row.size();
-      t.grp_row = d_xgrp_row.p;
-      t.grp_col = d_xgrp_col.p;
-      t.grp_begin = d_xgrp_begin.p;
-      t.grp_end = d_xgrp_end.p;
-      t.pair_a = d_xpair_a.p;
-      t.pair_b = d_xpair_b.p;
-      t.pair_p = d_xpair_p.p;
-    } else {
-      t.ngroups = (int)S.grp_row.size();
-      t.grp_row = d_grp_row.p;
-      t.grp_col = d_grp_col.p;
-      t.grp_begin = d_grp_begin.p;
-      t.grp_end = d_grp_end.p;
-      t.pair_a = d_pair_a.p;
-      t.pair_b = d_pair_b.p;
-      t.pair_p = d_pair_p.p;
-    }
+    t.ngroups = (int)S.xgrp_row.size();
+    t.grp_row = d_xgrp_row.p;
+    t.grp_col = d_xgrp_col.p;
+    t.grp_begin = d_xgrp_begin.p;
+    t.grp_end = d_xgrp_end.p;
+    t.pair_a = d_xpair_a.p;
+    t.pair_b = d_xpair_b.p;
+    t.pair_p = d_xpair_p.p;
     return t;
   }
+  RowTables row_tables() const {
+    RowTables r;
+    r.nblocks = nb;
+    r.blk_dim = d_blk_dim.p;
+    r.blk_off = d_blk_off.p;
+    r.blk_ent = d_blk_ent.p;
+    r.ent = d_ent.p;
+    r.ent_point = d_ent_point.p;
+    r.seg_col = d_seg_col.p;
+    r.ent_block = d_ent_block.p;
+    r.pt_off = d_pt_off.p;
+    r.nbr_begin = d_nbr_begin.p;
+    r.nbr = d_nbr.p;
+    r.nbr_row = d_nbr_row.p;
+    r.slot_off = d_slot_off.p;
+    r.entries = (uint32_t)S.nbr.size();
+    return r;
+  }
+  TileBand tile_band() const { return TileBand{D, S.nt, S.bwt, d_tiles.p}; }
 
   void upload() {
     std::vector<uint32_t> pt_off(n.pt_off.begin(), n.pt_off.end());
@@ -2226,13 +2230,6 @@ struct Solver {
     up_i(d_blk_chunk_end, S.blk_chunk_end);
     up_i(d_obs_intr_col, S.obs_intr_col);
     up_i(d_seg_col, S.seg_col);
-    up_i(d_grp_row, S.grp_row);
-    up_i(d_grp_col, S.grp_col);
-    up_u(d_grp_begin, S.grp_begin);
-    up_u(d_grp_end, S.grp_end);
-    up_u(d_pair_a, S.pair_a);
-    up_u(d_pair_b, S.pair_b);
-    up_u(d_pair_p, S.pair_p);
     up_i(d_xgrp_row, S.xgrp_row);
     up_i(d_xgrp_col, S.xgrp_col);
     up_u(d_xgrp_begin, S.xgrp_begin);
@@ -2249,13 +2246,19 @@ struct Solver {
     d_diag.alloc(std::max(1, D), st);
     d_diag_minmax.alloc(2 * std::max(1, nb), st);
     d_clamp.alloc(std::max(1, nb), st);
-    d_pair_out.alloc((size_t)36 * std::max<size_t>(1, S.grp_row.size()), st);
     d_xpair_out.alloc((size_t)36 * std::max<size_t>(1, S.xgrp_row.size()), st);
-    if (!S.grp_row.empty() || direct) {
-      d_S.alloc((size_t)std::max(1, D) * std::max(1, D), st);
-      d_Lf.alloc((size_t)std::max(1, D) * std::max(1, D), st);
-    }
     d_status.alloc(4, st);
+    up_u(d_blk_ent, S.blk_ent);
+    up_i(d_ent_block, S.ent_block);
+    up_u(d_nbr_begin, S.nbr_begin);
+    up_i(d_nbr, S.nbr);
+    up_i(d_nbr_row, S.nbr_row);
+    upload_padded(d_slot_off, S.slot_off, 1, st);
+    up_i(d_perm_off, S.perm_off);
+    up_i(d_perm_to_orig, S.perm_to_orig);
+    d_rows.alloc(std::max<uint64_t>(1, S.slot_off.empty() ? 1 : S.slot_off.back()), st);
+    d_perm_vec.alloc(std::max(1, D), st);
+    d_power.alloc(2 * (size_t)std::max(1, D) + 2, st);
     for (DBuf<double>* b : {&d_step, &d_r, &d_z, &d_dir, &d_q, &d_tmp, &d_rhs, &d_r64, &d_e}) b->alloc(std::max(1, D), st);
     d_factor.alloc((size_t)42 * std::max(1, nb), st);
     d_dq.alloc(std::max(1, nb), st);
@@ -2344,7 +2347,7 @@ struct Solver {
   };
 
   // Full linearization + camera-side reductions at the given damping.
-  Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_dense) {
+  Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_rows) {
     DevView v = view();
     if (mixed)
       OMVGBA_LAUNCH(k_linearize<float>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin32());
@@ -2368,20 +2371,8 @@ struct Solver {
                                                      d_diag_minmax.p);
       check_launch();
     }
-    if (build_dense && D > 0) {
-      PairTables pt = pairs(false);
-      if (pt.ngroups > 0) {
-        if (mixed)
-          OMVGBA_LAUNCH(k_pairs<float>, pt.ngroups, 32, 0, st, pt, bt, lin32(), d_seg_col.p, d_pair_out.p);
-        else
-          OMVGBA_LAUNCH(k_pairs<T>, pt.ngroups, 32, 0, st, pt, bt, lin(), d_seg_col.p, d_pair_out.p);
-      }
-      CUDA_OK(cudaMemsetAsync(d_S.p, 0, sizeof(double) * (size_t)D * D, st));
-      OMVGBA_LAUNCH(k_dense_from_blocks, nb, 32, 0, st, bt, d_blk_out.p, D, d_S.p);
-      if (pt.ngroups > 0) OMVGBA_LAUNCH(k_dense_pairs, grid_for(pt.ngroups, 64), 64, 0, st, pt, bt, d_pair_out.p, D, d_S.p);
-      OMVGBA_LAUNCH(k_dense_add_diag, grid_for(D, 128), 128, 0, st, D, d_diag.p, lambda, d_S.p);
-      check_launch();
-    }
+    rows_valid = false;
+    if (build_rows && D > 0) this->build_rows();
     PointSummary ps;
     CUDA_OK(copy_async(&ps, d_summary_part.p, sizeof(ps), cudaMemcpyDeviceToHost, st));
     std::vector<double> mm(2 * std::max(nb, 1));
@@ -2426,24 +2417,155 @@ struct Solver {
     }
     a.grad_norm = std::max(a.grad_norm, gn);
     a.valid = a.valid && finite && std::isfinite(a.cost);
-    if (build_dense && D > 0 && a.valid) {
-      // the dense S must be finite (hessian.is_finite)
-    }
     return a;
   }
 
   // ---- camera step ----
-  bool direct_step() {
-    CUDA_OK(copy_async(d_Lf.p, d_S.p, sizeof(double) * (size_t)D * D, cudaMemcpyDeviceToDevice, st));
-    OMVGBA_LAUNCH(k_dense_cholesky, 1, 1024, 0, st, D, d_Lf.p, d_status.p);
-    OMVGBA_LAUNCH(k_neg_copy, grid_for(D, 256), 256, 0, st, D, d_gred.p, d_step.p);
+  bool direct_step(double lambda) {
+    if (!factor_band(lambda, nullptr, 0.0)) return false;
+    OMVGBA_LAUNCH(k_perm_gather, grid_for(D, 256), 256, 0, st, D, d_perm_to_orig.p, d_gred.p, -1.0, d_perm_vec.p);
+    OMVGBA_LAUNCH(k_tile_solve, 1, 256, 0, st, tile_band(), d_perm_vec.p, d_status.p);
+    OMVGBA_LAUNCH(k_perm_scatter, grid_for(D, 256), 256, 0, st, D, d_perm_to_orig.p, d_perm_vec.p, d_step.p);
+    check_launch();
+    return true;
+  }
+
+  // S of the current linearization (no damping) by block rows, from the FP64 or FP32 records.
+  void build_rows() {
+    const size_t smem = (size_t)S.max_track * kRec * sizeof(double) + 4 * (size_t)S.max_track * sizeof(int);
+    if (smem > 48 * 1024) {
+      CUDA_OK(cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CUDA_OK(cudaFuncSetAttribute(k_block_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    if (mixed)
+      OMVGBA_LAUNCH(k_block_rows<float>, nb, kRowThreads, smem, st, row_tables(), lin32(), S.max_track, d_rows.p);
+    else
+      OMVGBA_LAUNCH(k_block_rows<T>, nb, kRowThreads, smem, st, row_tables(), lin(), S.max_track, d_rows.p);
+    check_launch();
+    rows_valid = true;
+  }
+
+  // y = (S + lambda diag) x from the rows
+  void rows_matvec(const double* x, double* y, double lambda) {
+    OMVGBA_LAUNCH(k_rows_matvec, grid_for((size_t)nb * 32, 256), 256, 0, st, row_tables(), d_rows.p, d_diag.p, lambda,
+                  (const double*)nullptr, x, y, (double*)nullptr, (const PcgCtl*)nullptr);
+    check_launch();
+  }
+
+  // Cholesky of (S + lambda diag) -- equilibrated as scale S scale and shifted by -shift I when scale
+  // is given -- into the banded tiles; true when every pivot is finite and positive.
+  static constexpr size_t kMaxTileBytes = size_t(16) << 30;
+  bool factor_band(double lambda, const double* scale, double shift) {
+    if (D == 0) return true;
+    const size_t count = (size_t)S.nt * (S.bwt + 1) * kCTT;
+    if (sizeof(double) * count > kMaxTileBytes)
+      throw SolveFailure{3, "the banded factor of the reduced camera system exceeds 16 GiB"};
+    if (d_tiles.n != count) d_tiles.alloc(count, st);
+    static bool attrs = false;
+    if (!attrs) {
+      CUDA_OK(cudaFuncSetAttribute(k_tile_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+      CUDA_OK(cudaFuncSetAttribute(k_tile_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
+      attrs = true;
+    }
+    CUDA_OK(cudaMemsetAsync(d_tiles.p, 0, sizeof(double) * count, st));
+    OMVGBA_LAUNCH(k_set_int, 1, 1, 0, st, d_status.p, 1);
+    const TileBand tb = tile_band();
+    OMVGBA_LAUNCH(k_rows_to_tiles, grid_for(S.nbr.size(), 128), 128, 0, st, row_tables(), d_rows.p, d_perm_off.p,
+                  d_diag.p, lambda, scale, shift, tb);
+    OMVGBA_LAUNCH(k_tiles_pad, 1, kCT, 0, st, tb);
+    for (int k = 0; k < S.nt; ++k) {
+      OMVGBA_LAUNCH(k_tile_potrf, 1, 256, 0, st, tb, k, d_status.p);
+      const int m = std::min(S.bwt, S.nt - 1 - k);
+      if (m > 0) {
+        OMVGBA_LAUNCH(k_tile_trsm, m, kCT, kTrsmSmem, st, tb, k, d_status.p);
+        OMVGBA_LAUNCH(k_tile_update, m * (m + 1) / 2, 256, kUpdateSmem, st, tb, k, d_status.p);
+      }
+    }
     check_launch();
     int ok = 0;
     CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
-    if (!ok) return false;
-    OMVGBA_LAUNCH(k_dense_solve, 1, 32, 0, st, D, d_Lf.p, d_step.p);
+    return ok != 0;
+  }
+
+  // Camera rank of the final undamped system (sparse/direct.rs:288-455; the native lowering fixes the
+  // gauge with pose masks, so the expected nullity is zero): D <= dense_rank_limit: every eigenvalue
+  // of the Jacobi-equilibrated S above tol = 64 eps D lambda_max, i.e. S_eq - tol I positive definite;
+  // above the limit: S itself factors. Returns 0 (full rank) or 2 (rank deficient or indefinite);
+  // *factored_s tells whether the band holds the factor of S itself.
+  int rank_certificate(bool* factored_s) {
+    *factored_s = false;
+    if (D == 0) return 0;
+    if (D > opt.dense_rank_limit) {
+      const bool ok = factor_band(0.0, nullptr, 0.0);
+      *factored_s = ok;
+      return ok ? 0 : 2;
+    }
+    std::vector<double> dg(D);
+    OMVGBA_LAUNCH(k_rows_diag, grid_for(nb, 128), 128, 0, st, row_tables(), d_rows.p, d_tmp.p);
     check_launch();
+    CUDA_OK(copy_async(dg.data(), d_tmp.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+    sync();
+    double ds = 0.0;
+    for (int i = 0; i < D; ++i) ds = std::max(ds, std::fabs(dg[i]));
+    if (!(std::isfinite(ds) && ds > 0.0)) return 2;
+    const double fl = 64.0 * kEps * ds;
+    std::vector<double> sc(D);
+    for (int i = 0; i < D; ++i) {
+      if (!std::isfinite(dg[i])) return 2;
+      sc[i] = 1.0 / std::sqrt(std::max(dg[i], fl));
+    }
+    CUDA_OK(copy_async(d_e.p, sc.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
+    OMVGBA_LAUNCH(k_power_iteration, 1, 1024, 0, st, row_tables(), d_rows.p, d_e.p, D, d_power.p, d_power.p + D,
+                  d_power.p + 2 * (size_t)D);
+    check_launch();
+    double out[2];
+    CUDA_OK(copy_async(out, d_power.p + 2 * (size_t)D, sizeof(out), cudaMemcpyDeviceToHost, st));
+    sync();
+    const double largest = std::fabs(out[0]);
+    if (out[1] == 0.0 || !(std::isfinite(largest) && largest > 0.0)) return 2;
+    const double tol = 64.0 * kEps * D * largest;
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr, "[omvgba] rank: lambda_max %.6e tol %.3e\n", largest, tol);
+    return factor_band(0.0, d_e.p, tol) ? 0 : 2;
+  }
+
+  // Marginal covariances (S^-1)_gg of the free intrinsic groups of the final undamped system
+  // (sparse/covariance.rs:564-587 without the weight normalization): 9 values per group, row-major
+  // (the dim x dim corner used). False when S does not factor.
+  bool intrinsic_marginals(bool factored_s, std::vector<double>& out) {
+    out.assign(9 * (size_t)std::max(ng, 1), 0.0);
+    std::vector<int> pos, dims, gid;
+    for (int g = 0; g < ng; ++g)
+      if (L.intr_dim[g] > 0 && S.grp_block[g] >= 0) {
+        const int b = S.grp_block[g];
+        for (int k = 0; k < 3; ++k) pos.push_back(k < L.intr_dim[g] ? S.perm_off[b] + k : S.perm_off[b]);
+        dims.push_back(L.intr_dim[g]);
+        gid.push_back(g);
+      }
+    if (gid.empty()) return true;
+    if (!factored_s && !factor_band(0.0, nullptr, 0.0)) return false;
+    DBuf<int> d_pos, d_dims;
+    d_pos.upload(pos.data(), pos.size(), st);
+    d_dims.upload(dims.data(), dims.size(), st);
+    const int total = (int)gid.size();
+    const int batch = std::min(total, 512);
+    d_marg_scratch.alloc((size_t)batch * 3 * D, st);
+    d_marg_out.alloc(9 * (size_t)total, st);
+    for (int b0 = 0; b0 < total; b0 += batch) {
+      const int cnt = std::min(batch, total - b0);
+      OMVGBA_LAUNCH(k_tile_marginals, cnt, 256, 0, st, tile_band(), cnt, d_pos.p + 3 * b0, d_dims.p + b0,
+                    d_marg_scratch.p, d_marg_out.p + 9 * (size_t)b0, d_status.p);
+    }
+    check_launch();
+    std::vector<double> m(9 * (size_t)total);
+    int ok = 0;
+    CUDA_OK(copy_async(m.data(), d_marg_out.p, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (!ok) return false;
+    for (int i = 0; i < total; ++i)
+      for (int k = 0; k < 9; ++k) out[9 * (size_t)gid[i] + k] = m[9 * (size_t)i + k];
     return true;
   }
 
@@ -2496,7 +2618,7 @@ struct Solver {
 
   bool factor_preconditioner(double lambda) {
     BlockTables bt = tables();
-    PairTables xt = pairs(true);
+    PairTables xt = pairs();
     if (xt.ngroups > 0) {
       if (mixed)
         OMVGBA_LAUNCH(k_pairs<float>, xt.ngroups, 32, 0, st, xt, bt, lin32(), d_seg_col.p, d_xpair_out.p);
@@ -2903,7 +3025,7 @@ struct Solver {
         double rel_res = 0.0;
         bool solved = true;
         if (direct) {
-          solved = D == 0 || direct_step();
+          solved = D == 0 || direct_step(lambda);
         } else {
           solved = factor_preconditioner(lambda);
           if (solved) {
@@ -2961,10 +3083,9 @@ struct Solver {
         double damped;
         if (!iterative_step) {
           if (D > 0)
-            OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, st, D, d_S.p, d_step.p, d_q.p);
+            rows_matvec(d_step.p, d_q.p, lambda);
           else
             CUDA_OK(cudaMemsetAsync(d_q.p, 0, sizeof(double), st));
-          check_launch();
         } else {
           matvec(d_step.p, d_q.p, lambda);
         }
@@ -3025,18 +3146,17 @@ struct Solver {
         }
       }
     }
-    // final undamped assembly and certificate
+    // final undamped assembly and certificate: the camera rank (sparse/direct.rs:288-455) and, for
+    // self-calibration, the intrinsic marginal covariances (native/self_calibration.rs:255-303)
     Gauge g = gauge_for(cur, scene);
-    bool dense_rank = D <= opt.dense_rank_limit && !S.grp_row.empty();
-    Assembly fa = assemble(cur, g, opt.loss, 0.0, dense_rank);
-    rep.rank = 3;
-    if (dense_rank || D == 0) {
-      if (!fa.valid)
-        rep.rank = 2;
-      else if (D == 0)
-        rep.rank = 0;
-      else
-        rep.rank = rank_full() ? 0 : 2;
+    Assembly fa = assemble(cur, g, opt.loss, 0.0, true);
+    bool factored_s = false;
+    if (!fa.valid)
+      rep.rank = 2;
+    else
+      rep.rank = rank_certificate(&factored_s);
+    if (n.self_cal && opt.certify_intrinsics) {
+      rep.marginals_ok = fa.valid && intrinsic_marginals(factored_s, rep.marginals) ? 1 : 0;
     }
     bool well = rep.rank != 2 && fa.weak == 0;
     if (std::getenv("OMVGBA_PHASE_TIMES"))
@@ -3101,65 +3221,6 @@ struct Solver {
     return rep;
   }
 
-  // Rank certificate on the final undamped dense S (sparse/direct.rs:342-455): after Jacobi
-  // equilibration the spectral test counts eigenvalues above tol = 64 eps D lambda_max. Full rank
-  // holds exactly when every eigenvalue exceeds tol, i.e. when S_eq - tol I is positive definite,
-  // which one Cholesky factorization decides; lambda_max comes from power iteration.
-  bool rank_full() {
-    std::vector<double> Sh((size_t)D * D);
-    CUDA_OK(copy_async(Sh.data(), d_S.p, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost, st));
-    sync();
-    double ds = 0.0;
-    for (int i = 0; i < D; ++i) ds = std::max(ds, std::fabs(Sh[(size_t)i * D + i]));
-    if (!(std::isfinite(ds) && ds > 0.0)) return false;
-    double fl = 64.0 * kEps * ds;
-    std::vector<double> sc(D);
-    for (int i = 0; i < D; ++i) {
-      double d = Sh[(size_t)i * D + i];
-      if (!std::isfinite(d)) return false;
-      sc[i] = 1.0 / std::sqrt(std::max(d, fl));
-    }
-    for (int i = 0; i < D; ++i)
-      for (int j = 0; j < D; ++j) {
-        double v = Sh[(size_t)i * D + j] * sc[i] * sc[j];
-        if (!std::isfinite(v)) return false;
-        Sh[(size_t)i * D + j] = v;
-      }
-    CUDA_OK(copy_async(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
-    // power iteration for the largest |eigenvalue| (Rayleigh quotient of the converged iterate)
-    std::vector<double> v(D, 1.0 / std::sqrt((double)D)), w(D);
-    double lam = 0.0;
-    for (int it = 0; it < 200; ++it) {
-      CUDA_OK(copy_async(d_tmp.p, v.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
-      OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, st, D, d_Lf.p, d_tmp.p, d_q.p);
-      check_launch();
-      CUDA_OK(copy_async(w.data(), d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
-      sync();
-      double nrm = 0.0, rq = 0.0;
-      for (int i = 0; i < D; ++i) {
-        nrm += w[i] * w[i];
-        rq += v[i] * w[i];
-      }
-      nrm = std::sqrt(nrm);
-      if (!(std::isfinite(nrm) && nrm > 0.0)) return false;
-      bool settled = it > 8 && std::fabs(rq - lam) <= 1e-10 * std::fabs(rq);
-      lam = rq;
-      for (int i = 0; i < D; ++i) v[i] = w[i] / nrm;
-      if (settled) break;
-    }
-    double largest = std::fabs(lam);
-    if (!(std::isfinite(largest) && largest > 0.0)) return false;
-    double tol = 64.0 * kEps * D * largest;
-    if (std::getenv("OMVGBA_PHASE_TIMES")) std::fprintf(stderr, "[omvgba] rank: lambda_max %.6e tol %.3e\n", largest, tol);
-    for (int i = 0; i < D; ++i) Sh[(size_t)i * D + i] -= tol;
-    CUDA_OK(copy_async(d_Lf.p, Sh.data(), sizeof(double) * Sh.size(), cudaMemcpyHostToDevice, st));
-    OMVGBA_LAUNCH(k_dense_cholesky, 1, 1024, 0, st, D, d_Lf.p, d_status.p);
-    check_launch();
-    int ok = 0;
-    CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    sync();
-    return ok != 0;
-  }
 };
 
 NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOptions& options,
@@ -3305,8 +3366,7 @@ void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const L
   if (!x) return;
   CUDA_OK(copy_async(s.d_tmp.p, x, sizeof(double) * D, cudaMemcpyHostToDevice, s.st));
   s.matvec(s.d_tmp.p, s.d_q.p, lambda);
-  OMVGBA_LAUNCH(k_dense_matvec, grid_for((size_t)D * 32, 256), 256, 0, s.st, D, s.d_S.p, s.d_tmp.p, s.d_z.p);
-  s.check_launch();
+  s.rows_matvec(s.d_tmp.p, s.d_z.p, lambda);
   CUDA_OK(copy_async(y_mv, s.d_q.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
   CUDA_OK(copy_async(y_dense, s.d_z.p, sizeof(double) * D, cudaMemcpyDeviceToHost, s.st));
   s.sync();

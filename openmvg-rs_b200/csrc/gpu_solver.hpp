@@ -76,6 +76,7 @@ struct LmOptions {
   int precision = 0;  // 0 FP64, 1 mixed
   int matvec = 0;     // 0 auto, 1 explicit, 2 implicit
   int dense_rank_limit = 2048;
+  bool certify_intrinsics = true;  // self-calibration: compute the intrinsic marginal covariances
   void* stream = nullptr;  // cudaStream_t the solve runs on; null: the context's own stream
 };
 
@@ -92,6 +93,10 @@ struct NativeReport {
   uint64_t pcg_terms = 0;
   double final_damping = 0;
   int D = 0;
+  // self-calibration certificate: (S^-1)_gg of each intrinsic group at the final state, 9 values per
+  // group (row-major, the free dim x dim corner used); marginals_ok = 0 when S does not factor
+  std::vector<double> marginals;
+  int marginals_ok = 0;
 };
 
 struct Context;  // device, stream, pinned scratch

@@ -659,8 +659,6 @@ LmOptions lm_options(const omvgba_problem& pr, const omvgba_config& cfg, const N
     o.iterative = true;
   else
     o.iterative = D > o.dense_rank_limit;  // Auto: dense direct below the dense limit
-  if (!o.iterative && D > 8192)
-    fail(OMVGBA_RESOURCE_EXHAUSTED, "direct solve of a reduced system above 8192 unknowns is not supported; use Iterative");
   o.pcg_tolerance = cfg.pcg_relative_tolerance > 0.0 ? cfg.pcg_relative_tolerance : 1e-1;
   o.pcg_max_iterations = cfg.pcg_max_iterations > 0 ? cfg.pcg_max_iterations : 600;
   o.precision = cfg.precision;
@@ -675,8 +673,51 @@ struct Result {
   std::vector<omvgba_intrinsic> intrinsics;
   std::vector<double> points;
   std::vector<uint64_t> quarantined;
+  std::vector<uint64_t> unconstrained;  // intrinsic groups held at their input values by the certificate
   omvgba_report report{};
 };
+
+// Largest accepted marginal standard deviation of each free intrinsic parameter's contribution to the
+// relative radial displacement at the farthest image corner (native/self_calibration.rs:215-222).
+constexpr double kMaxIntrinsicCornerStd = 0.01;
+
+// Free intrinsic groups that the final information does not constrain
+// (native/self_calibration.rs:255-303): sigma(log f), sigma(k1) r^2 and sigma(k2) r^4 of the marginal
+// covariance (S^-1)_gg times the zero-residual weight, with r the normalized radius of the farthest
+// corner at the final focal length; a NaN deviation holds even a waived group, a deviation above the
+// bound holds a required one. Every free group when S does not factor or any marginal is not finite.
+std::vector<uint64_t> unconstrained_groups(const omvgba_problem& pr, const NativeProblem& n,
+                                           const std::vector<double>& groups, const NativeReport& nr,
+                                           const LossDev& loss) {
+  std::vector<uint64_t> all, out;
+  for (size_t g = 0; g < n.group_dim.size(); ++g)
+    if (n.group_dim[g] > 0) all.push_back(g);
+  if (all.empty()) return out;
+  if (!nr.marginals_ok || nr.marginals.size() < 9 * n.group_dim.size()) return all;
+  const double zw = loss.sqrt_weight(0.0);
+  const double wn = zw * zw;
+  for (uint64_t g : all) {
+    const int dim = n.group_dim[g];
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b)
+        if (!std::isfinite(nr.marginals[9 * g + 3 * a + b] * wn)) return all;
+  }
+  for (uint64_t g : all) {
+    const omvgba_intrinsic& in = pr.intrinsics[g];
+    const double f = groups[3 * g];
+    const double ux = std::max(in.cx, double(in.width) - in.cx) / f, uy = std::max(in.cy, double(in.height) - in.cy) / f;
+    const double r2 = ux * ux + uy * uy;
+    const double scales[3] = {1.0, r2, r2 * r2};
+    const bool waived = in.certification == 1;
+    bool held = false;
+    for (int k = 0; k < n.group_dim[g]; ++k) {
+      const double dev = std::sqrt(nr.marginals[9 * g + 4 * k] * wn) * scales[k];
+      held = held || std::isnan(dev) || (!waived && dev > kMaxIntrinsicCornerStd);
+    }
+    if (held) out.push_back(g);
+  }
+  return out;
+}
 
 // The poses' rotations and centres and the intrinsics' camera models of one state, built once so
 // that per-observation residuals only rotate and project.
@@ -1054,8 +1095,22 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
   LmOptions opt = lm_options(pr, cfg, L.n);
   std::vector<double> rot, tr, pts, grp;
   NativeReport nr = gpu_refine(ctx, L.n, opt, rot, tr, pts, grp);
+  std::vector<uint64_t> held;
+  if (L.n.self_cal) {
+    held = unconstrained_groups(pr, L.n, grp, nr, opt.loss);
+    if (!held.empty()) {
+      // re-solve from the input state with the unconstrained groups fixed
+      // (native/self_calibration.rs:236-249); the second solve is not certified again
+      for (uint64_t g : held) L.n.group_dim[g] = 0;
+      LmOptions again = lm_options(pr, cfg, L.n);
+      again.certify_intrinsics = false;
+      nr = gpu_refine(ctx, L.n, again, rot, tr, pts, grp);
+    }
+  }
   const double t_gpu = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_lower;
   Result res = raise(pr, L, rot, tr, pts, grp, nr, opt.iterative);
+  res.unconstrained = held;
+  res.report.unconstrained_intrinsic_count = held.size();
   finish_solution(pr, res);
   canonicalize(pr, res);
   if (std::getenv("OMVGBA_PHASE_TIMES"))
@@ -1381,6 +1436,7 @@ Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_co
   }
   for (size_t p = 0; p < pr.point_count; ++p)
     if (!retained[p]) out.quarantined.push_back(p);
+  out.unconstrained = sol.unconstrained;
   out.report = sol.report;
   if (have_origin) add_origin(out.report, origin);
   finish_solution(pr, out);
@@ -1460,7 +1516,10 @@ void write_solution(const omvgba_problem& problem, const Result& r, omvgba_solut
   std::memcpy(solution->points, r.points.data(), sizeof(double) * 3 * problem.point_count);
   if (solution->quarantined_points)
     for (size_t i = 0; i < r.quarantined.size(); ++i) solution->quarantined_points[i] = r.quarantined[i];
+  if (solution->unconstrained_intrinsics)
+    for (size_t i = 0; i < r.unconstrained.size(); ++i) solution->unconstrained_intrinsics[i] = r.unconstrained[i];
   solution->report = r.report;
+  solution->report.unconstrained_intrinsic_count = r.unconstrained.size();
 }
 
 void clear_error(omvgba_error* error) {
@@ -1738,8 +1797,24 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     std::vector<double> rot, tr, pts, grp;
     double laps[6];
     NativeReport nr = resident_refine(plan->resident, rot, tr, pts, grp);
+    std::vector<uint64_t> held;
+    Lowered held_lowering;
+    const Lowered* lowered = &plan->lowered;
+    if (plan->lowered.n.self_cal) {
+      held = unconstrained_groups(working, plan->lowered.n, grp, nr, plan->options.loss);
+      if (!held.empty()) {  // re-solve from the input state with the unconstrained groups fixed
+        held_lowering = plan->lowered;
+        for (uint64_t g : held) held_lowering.n.group_dim[g] = 0;
+        LmOptions again = lm_options(working, plan->config, held_lowering.n);
+        again.certify_intrinsics = false;
+        nr = gpu_refine(plan->ctx, held_lowering.n, again, rot, tr, pts, grp);
+        lowered = &held_lowering;
+      }
+    }
     laps[0] = seconds_since(t0);
-    Result first = raise(working, plan->lowered, rot, tr, pts, grp, nr, plan->options.iterative);
+    Result first = raise(working, *lowered, rot, tr, pts, grp, nr, plan->options.iterative);
+    first.unconstrained = held;
+    first.report.unconstrained_intrinsic_count = held.size();
     laps[1] = seconds_since(t0);
     finish_solution(working, first);
     laps[2] = seconds_since(t0);

@@ -221,12 +221,14 @@ class Solution:
     points: np.ndarray
     quarantined_points: np.ndarray
     report: dict
+    unconstrained_intrinsics: np.ndarray = None  # groups the self-calibration certificate held
 
     @classmethod
     def from_buffers(cls, buffers: abi.SolutionBuffers) -> "Solution":
         rot, cen = buffers.pose_arrays()
         report = abi.report_to_dict(buffers.struct.report)
         q = buffers.quarantined[: report["quarantined_point_count"]].copy()
+        u = buffers.unconstrained[: report["unconstrained_intrinsic_count"]].copy()
         return cls(
             rotations=rot,
             centers=cen,
@@ -234,4 +236,5 @@ class Solution:
             points=buffers.points.reshape(-1, 3).copy(),
             quarantined_points=q,
             report=report,
+            unconstrained_intrinsics=u,
         )

@@ -954,6 +954,7 @@ struct Options {
   bool iterative;
   double pcg_tol;
   uint64_t pcg_max;
+  bool certify_intrinsics = true;  // self-calibration: compute the intrinsic marginal covariances
 };
 
 struct NativeReport {
@@ -968,7 +969,223 @@ struct NativeReport {
   uint64_t pcg_terms;
   double final_damping;
   int D;
+  std::vector<double> marginals;  // self-calibration: (S^-1)_gg per group, 9 values (row-major corner)
+  bool marginals_ok = false;
 };
+
+// ------------------------------------------------------------------------------------------
+// Explicit reduced camera system in a band, its Cholesky factor, and the intrinsic marginal
+// covariances of the final undamped system (stands in for faer's sparse LLT, numerics/sparse.rs:119-250;
+// sparse/direct.rs:288-330 factors S for the rank, sparse/covariance.rs:564-587 solves S x = e_p for
+// the marginals). Parameters are ordered camera by camera -- each pose block, then the intrinsic
+// blocks it introduces -- which keeps the reduced system of a survey in a narrow band.
+// ------------------------------------------------------------------------------------------
+static bool g_certificate = true;  // test hook: timing runs skip the final certificate's factorization
+
+struct Band {
+  int n = 0, w = 0;
+  std::vector<double> a;  // row i, column j (i - w <= j <= i) at a[i (w + 1) + (i - j)]
+  double& at(int i, int j) { return a[(size_t)i * (w + 1) + (i - j)]; }
+  double at(int i, int j) const { return a[(size_t)i * (w + 1) + (i - j)]; }
+};
+
+// Position of every parameter in the factorization order.
+static std::vector<int> factor_order(const Native& n, const Layout& L) {
+  std::vector<int> pos(L.D, 0);
+  std::vector<int> home(L.intr_dim.size(), -1);
+  if (n.self_cal)
+    for (int c = n.ncam - 1; c >= 0; --c) home[n.cam_group[c]] = c;
+  int at = 0;
+  auto place_group = [&](size_t g) {
+    for (int k = 0; k < L.intr_dim[g]; ++k) pos[L.intr_off[g] + k] = at++;
+  };
+  for (int c = 0; c < n.ncam; ++c) {
+    for (int k = 0; k < L.pose_dim[c]; ++k) pos[L.pose_off[c] + k] = at++;
+    for (size_t g = 0; g < L.intr_dim.size(); ++g)
+      if (home[g] == c) place_group(g);
+  }
+  for (size_t g = 0; g < L.intr_dim.size(); ++g)
+    if (home[g] < 0) place_group(g);
+  return pos;
+}
+
+// Per point of the final state: the weighted camera rows of each observation and the point's
+// coupling terms, added into the rows of the band that [r0, r1) owns (lower triangle in the
+// factorization order). Every element receives its terms in point order, observation order.
+static void band_point_terms(const Native& n, const Layout& L, const std::vector<NPose>& poses,
+                             const std::vector<Vec3>& points, const std::vector<Radial>& groups, const GaugeState& g,
+                             const Loss& loss, const std::vector<int>& pos, size_t p, int r0, int r1, Band& B) {
+  struct ObsRows {
+    int cd;
+    int params[9];
+    double first[9], second[9];
+  };
+  std::vector<ObsRows> rows;
+  std::vector<int> qs;
+  std::vector<Vec3> cross;
+  Mat3 V{};
+  const Vec3& X = points[p];
+  for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) {
+    const int cam = n.obs_cam[o];
+    const NPose& P = poses[cam];
+    Vec3 rot = rotate(P.R, X);
+    Vec3 xc = {rot[0] + P.t[0], rot[1] + P.t[1], rot[2] + P.t[2]};
+    ObsLin ol;
+    if (!project_obs(n, groups, o, xc, &ol)) return;
+    const double rn = std::sqrt(ol.p.residual[0] * ol.p.residual[0] + ol.p.residual[1] * ol.p.residual[1]);
+    const double sw = loss.sqrt_weight(rn);
+    Mat23 Jp;
+    for (int r = 0; r < 2; ++r)
+      for (int c = 0; c < 3; ++c)
+        Jp[r][c] = (ol.p.jacobian[r][0] * P.R[0][c] + ol.p.jacobian[r][1] * P.R[1][c] + ol.p.jacobian[r][2] * P.R[2][c]) *
+                   g.scene_scale;
+    for (int r = 0; r < 2; ++r)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) V[i][j] += (sw * Jp[r][i]) * (sw * Jp[r][j]);
+    const int pd = L.pose_dim[cam];
+    const int grp = n.self_cal ? (int)n.cam_group[cam] : -1;
+    const int id = grp >= 0 ? L.intr_dim[grp] : 0;
+    if (pd == 0 && id == 0) continue;
+    ObsRows orow{};
+    double Jc[2][9] = {};
+    if (pd > 0) {
+      double m[3][6];
+      pose_motion(rot, cam, g, m);
+      for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < pd; ++c)
+          Jc[r][c] = ol.p.jacobian[r][0] * m[0][c] + ol.p.jacobian[r][1] * m[1][c] + ol.p.jacobian[r][2] * m[2][c];
+      for (int k = 0; k < pd; ++k) orow.params[k] = L.pose_off[cam] + k;
+    }
+    for (int r = 0; r < 2; ++r)
+      for (int c = 0; c < id; ++c) Jc[r][pd + c] = ol.jint[r][c];
+    for (int k = 0; k < id; ++k) orow.params[pd + k] = L.intr_off[grp] + k;
+    orow.cd = pd + id;
+    for (int k = 0; k < orow.cd; ++k) {
+      orow.first[k] = sw * Jc[0][k];
+      orow.second[k] = sw * Jc[1][k];
+      const int q = orow.params[k];
+      size_t at = 0;
+      while (at < qs.size() && qs[at] != q) ++at;
+      if (at == qs.size()) {
+        qs.push_back(q);
+        cross.push_back({0, 0, 0});
+      }
+      for (int i = 0; i < 3; ++i) cross[at][i] += (sw * Jp[0][i]) * orow.first[k] + (sw * Jp[1][i]) * orow.second[k];
+    }
+    rows.push_back(orow);
+  }
+  auto add = [&](int a, int b, double v) {
+    int P = pos[a], Q = pos[b];
+    if (P < Q) std::swap(P, Q);
+    if (P >= r0 && P < r1) B.at(P, Q) += v;
+  };
+  for (const ObsRows& r : rows)
+    for (int i = 0; i < r.cd; ++i)
+      for (int j = 0; j <= i; ++j) add(r.params[i], r.params[j], r.first[i] * r.first[j] + r.second[i] * r.second[j]);
+  if (n.fixed_points[p]) return;
+  auto f = point_block_factor(V, 0.0);
+  if (!f) return;
+  std::vector<Vec3> y(qs.size());
+  for (size_t i = 0; i < qs.size(); ++i) y[i] = f->solve(cross[i]);
+  for (size_t i = 0; i < qs.size(); ++i)
+    for (size_t j = 0; j <= i; ++j) add(qs[i], qs[j], -dot3(y[i], cross[j]));
+}
+
+// S of the final undamped state in the band; false when a projection or a point factor fails.
+static bool assemble_band(const Native& n, const Layout& L, const std::vector<NPose>& poses,
+                          const std::vector<Vec3>& points, const std::vector<Radial>& groups, const GaugeState& g,
+                          const Loss& loss, const std::vector<int>& pos, Band& B) {
+  const int D = L.D;
+  B.n = D;
+  B.w = 0;
+  for (size_t p = 0; p < points.size(); ++p) {
+    int lo = D, hi = -1;
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) {
+      const int cam = n.obs_cam[o];
+      for (int k = 0; k < L.pose_dim[cam]; ++k) {
+        lo = std::min(lo, pos[L.pose_off[cam] + k]);
+        hi = std::max(hi, pos[L.pose_off[cam] + k]);
+      }
+      if (n.self_cal) {
+        const int grp = n.cam_group[cam];
+        for (int k = 0; k < L.intr_dim[grp]; ++k) {
+          lo = std::min(lo, pos[L.intr_off[grp] + k]);
+          hi = std::max(hi, pos[L.intr_off[grp] + k]);
+        }
+      }
+    }
+    if (hi >= lo) B.w = std::max(B.w, hi - lo);
+  }
+  B.a.assign((size_t)D * (B.w + 1), 0.0);
+  // rows of the band in contiguous ranges, one per thread; each thread adds the terms of its rows
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  const int per = (D + nth - 1) / std::max(nth, 1);
+#pragma omp parallel for schedule(static, 1)
+  for (int t = 0; t < nth; ++t) {
+    const int r0 = t * per, r1 = std::min(D, r0 + per);
+    if (r0 >= r1) continue;
+    for (size_t p = 0; p < points.size(); ++p) band_point_terms(n, L, poses, points, groups, g, loss, pos, p, r0, r1, B);
+  }
+  for (double v : B.a)
+    if (!std::isfinite(v)) return false;
+  return true;
+}
+
+// In-place left-looking band Cholesky; false when a pivot is not finite and positive.
+static bool band_cholesky(Band& B) {
+  const int n = B.n, w = B.w;
+  for (int j = 0; j < n; ++j) {
+    double d = B.at(j, j);
+    for (int k = std::max(0, j - w); k < j; ++k) d -= B.at(j, k) * B.at(j, k);
+    if (!(std::isfinite(d) && d > 0.0)) return false;
+    const double piv = std::sqrt(d);
+    B.at(j, j) = piv;
+    const int i1 = std::min(n - 1, j + w);
+#pragma omp parallel for schedule(static)
+    for (int i = j + 1; i <= i1; ++i) {
+      double v = B.at(i, j);
+      for (int k = std::max(0, i - w); k < j; ++k) v -= B.at(i, k) * B.at(j, k);
+      B.at(i, j) = v / piv;
+    }
+  }
+  return true;
+}
+
+// (S^-1)_pq = (L^-1 e_P) . (L^-1 e_Q): forward solves from each parameter's position.
+static bool band_marginals(const Native& n, const Layout& L, const Band& B, const std::vector<int>& pos,
+                           std::vector<double>& out) {
+  const size_t ng = L.intr_dim.size();
+  out.assign(9 * std::max<size_t>(ng, 1), 0.0);
+  bool finite = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : finite)
+  for (long long g = 0; g < (long long)ng; ++g) {
+    const int dim = L.intr_dim[g];
+    if (dim == 0) continue;
+    std::vector<std::vector<double>> y(dim, std::vector<double>(B.n, 0.0));
+    int lo = B.n;
+    for (int k = 0; k < dim; ++k) lo = std::min(lo, pos[L.intr_off[g] + k]);
+    for (int k = 0; k < dim; ++k) {
+      const int P = pos[L.intr_off[g] + k];
+      std::vector<double>& v = y[k];
+      for (int i = P; i < B.n; ++i) {
+        double s = i == P ? 1.0 : 0.0;
+        for (int c = std::max(P, i - B.w); c < i; ++c) s -= B.at(i, c) * v[c];
+        v[i] = s / B.at(i, i);
+      }
+    }
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) {
+        double s = 0.0;
+        for (int i = lo; i < B.n; ++i) s += y[a][i] * y[b][i];
+        out[9 * g + 3 * a + b] = s;
+        finite = finite && std::isfinite(s);
+      }
+  }
+  return finite;
+}
 
 static double scene_scale_observed(const Native& n, const std::vector<NPose>& poses, const std::vector<Vec3>& points) {
   // observed_scene_scale (optimizer.rs:630-675); FixedBaseline gauges use the baseline norm
@@ -1361,17 +1578,30 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
   GaugeState g = make_gauge(n, poses, scene);
   bool dense_rank = D <= kDenseRankLimit;
   Assembly fa = S.assemble(poses, points, groups, g, opt.loss, 0.0, dense_rank, ws);
+  // the expected gauge nullity is zero: the native lowering fixes the gauge with pose masks
   rep.rank = 3;
-  if (dense_rank) {
-    if (!fa.valid)
-      rep.rank = 2;
-    else if (D == 0)
-      rep.rank = 0;
-    else {
-      bool ok;
-      int rank = spectral_rank(ws.H.S, D, &ok);
-      rep.rank = (ok && rank == D) ? 0 : 2;  // expected gauge nullity is zero with explicit pose masks
+  Band band;
+  bool band_factored = false;
+  std::vector<int> order;
+  if (!fa.valid) {
+    rep.rank = 2;
+  } else if (D == 0) {
+    rep.rank = 0;
+  } else if (dense_rank) {
+    bool ok;
+    int rank = spectral_rank(ws.H.S, D, &ok);
+    rep.rank = (ok && rank == D) ? 0 : 2;
+  } else if (g_certificate) {  // sparse/direct.rs:300-304: S factors
+    order = factor_order(n, L);
+    band_factored = assemble_band(n, L, poses, points, groups, g, opt.loss, order, band) && band_cholesky(band);
+    rep.rank = band_factored ? 0 : 2;
+  }
+  if (n.self_cal && opt.certify_intrinsics && g_certificate && fa.valid) {
+    if (order.empty()) {
+      order = factor_order(n, L);
+      band_factored = assemble_band(n, L, poses, points, groups, g, opt.loss, order, band) && band_cholesky(band);
     }
+    rep.marginals_ok = band_factored && band_marginals(n, L, band, order, rep.marginals);
   }
   bool well = rep.rank != 2 && fa.weak == 0;
   rep.status = run.status(well);
@@ -1889,8 +2119,49 @@ struct Result {
   std::vector<omvgba_intrinsic> intrinsics;
   std::vector<double> points;
   std::vector<uint64_t> quarantined;
+  std::vector<uint64_t> unconstrained;  // intrinsic groups the self-calibration certificate held
   omvgba_report report;
 };
+
+// Largest accepted marginal standard deviation of a free intrinsic parameter's contribution to the
+// relative radial displacement at the farthest image corner (native/self_calibration.rs:215-222).
+static const double kMaxIntrinsicCornerStd = 0.01;
+
+// unconstrained_intrinsics (native/self_calibration.rs:255-303): free groups whose sigma(log f),
+// sigma(k1) r^2 or sigma(k2) r^4 -- from (S^-1)_gg times the zero-residual weight, r the normalized
+// radius of the farthest corner at the final focal length -- is NaN, or above the bound for a group
+// whose certification is required; every free group when S does not factor or a marginal is not
+// finite.
+static std::vector<uint64_t> unconstrained_groups(const omvgba_problem& pr, const Native& n,
+                                                  const std::vector<Radial>& groups, const NativeReport& nr,
+                                                  const Loss& loss) {
+  std::vector<uint64_t> all, out;
+  for (size_t g = 0; g < n.group_dim.size(); ++g)
+    if (n.group_dim[g] > 0) all.push_back(g);
+  if (all.empty()) return out;
+  if (!nr.marginals_ok || nr.marginals.size() < 9 * n.group_dim.size()) return all;
+  const double zw = loss.sqrt_weight(0.0);
+  const double wn = zw * zw;
+  for (uint64_t g : all)
+    for (int a = 0; a < n.group_dim[g]; ++a)
+      for (int b = 0; b < n.group_dim[g]; ++b)
+        if (!std::isfinite(nr.marginals[9 * g + 3 * a + b] * wn)) return all;
+  for (uint64_t g : all) {
+    const omvgba_intrinsic& in = pr.intrinsics[g];
+    const double f = groups[g].focal;
+    const double ux = std::max(in.cx, double(in.width) - in.cx) / f, uy = std::max(in.cy, double(in.height) - in.cy) / f;
+    const double r2 = ux * ux + uy * uy;
+    const double scales[3] = {1.0, r2, r2 * r2};
+    const bool waived = in.certification == 1;
+    bool held = false;
+    for (int k = 0; k < n.group_dim[g]; ++k) {
+      const double dev = std::sqrt(nr.marginals[9 * g + 4 * k] * wn) * scales[k];
+      held = held || std::isnan(dev) || (!waived && dev > kMaxIntrinsicCornerStd);
+    }
+    if (held) out.push_back(g);
+  }
+  return out;
+}
 
 static bool camera_project_pixel(const omvgba_intrinsic& in, const Vec3& xc, Vec2* px) {
   if (in.model != OMVGBA_CAMERA_PINHOLE && in.model != OMVGBA_CAMERA_BROWN_CONRADY) return false;
@@ -2162,8 +2433,28 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   t0 = oracle_now();
   NativeReport nr = refine(n, poses, points, groups, opt);
   oracle_phase("refine", t0);
+  std::vector<uint64_t> held;
+  if (n.self_cal && g_certificate) {
+    held = unconstrained_groups(pr, n, groups, nr, opt.loss);
+    if (!held.empty()) {
+      // re-solve from the input state with the unconstrained groups fixed
+      // (native/self_calibration.rs:236-249); the second solve is not certified again
+      for (uint64_t g : held) n.group_dim[g] = 0;
+      poses = n.poses;
+      points = n.points;
+      groups = n.groups;
+      Options again = opt;
+      again.iterative = choose_iterative(cfg, make_layout(n).D);
+      again.certify_intrinsics = false;
+      t0 = oracle_now();
+      nr = refine(n, poses, points, groups, again);
+      oracle_phase("refine (held intrinsics)", t0);
+    }
+  }
   t0 = oracle_now();
   Result res = raise(pr, n, poses, points, groups, nr, opt.iterative);
+  res.unconstrained = held;
+  res.report.unconstrained_intrinsic_count = held.size();
   finish_solution(pr, res);
   canonicalize(pr, res);
   oracle_phase("report", t0);
@@ -2435,6 +2726,7 @@ static Result solve_with_quarantine(const omvgba_problem& pr, const omvgba_confi
   }
   for (size_t p = 0; p < pr.point_count; ++p)
     if (!retained[p]) out.quarantined.push_back(p);
+  out.unconstrained = sol.unconstrained;
   out.report = sol.report;
   if (have_origin) {
     auto& r = out.report;
@@ -2478,6 +2770,10 @@ void omvgba_oracle_set_threads(int threads) {
 // floating-point sums, which measures the algorithm's own rounding sensitivity.
 void omvgba_oracle_set_shards(int shards) { g_forced_shards = shards; }
 
+// Timing runs of the bench switch off the final certificate's band factorization (the rank above
+// D = 2048 and the self-calibration marginals); it does not run inside the LM loop they time.
+void omvgba_oracle_set_certificate(int on) { oracle::g_certificate = on != 0; }
+
 int omvgba_oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
@@ -2502,6 +2798,8 @@ int32_t omvgba_oracle_solve(const omvgba_problem* problem, const omvgba_config* 
     std::memcpy(solution->points, r.points.data(), sizeof(double) * 3 * problem->point_count);
     if (solution->quarantined_points)
       for (size_t i = 0; i < r.quarantined.size(); ++i) solution->quarantined_points[i] = r.quarantined[i];
+    if (solution->unconstrained_intrinsics)
+      for (size_t i = 0; i < r.unconstrained.size(); ++i) solution->unconstrained_intrinsics[i] = r.unconstrained[i];
     solution->report = r.report;
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {

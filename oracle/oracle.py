@@ -36,6 +36,7 @@ def lib():
         L.omvgba_oracle_debug_linearize.restype = C.c_int32
         L.omvgba_oracle_set_threads.argtypes = [C.c_int]
         L.omvgba_oracle_set_shards.argtypes = [C.c_int]
+        L.omvgba_oracle_set_certificate.argtypes = [C.c_int]
         L.omvgba_oracle_max_threads.restype = C.c_int
         L.omvgba_oracle_loss_cost.argtypes = [C.c_int, C.c_double, C.c_double]
         L.omvgba_oracle_loss_cost.restype = C.c_double
@@ -65,6 +66,12 @@ def set_threads(n: int) -> None:
 
 def set_shards(n: int) -> None:
     lib().omvgba_oracle_set_shards(int(n))
+
+
+def set_certificate(on: bool) -> None:
+    """Timing runs only: skip the final certificate's band factorization (rank above D = 2048 and
+    the self-calibration marginals), which runs after the LM loop."""
+    lib().omvgba_oracle_set_certificate(int(bool(on)))
 
 
 def max_threads() -> int:

@@ -982,6 +982,10 @@ struct NativeReport {
 // ------------------------------------------------------------------------------------------
 static bool g_certificate = true;  // test hook: timing runs skip the final certificate's factorization
 
+// Wall time of every LM iteration of the calling thread's last solve (the bench's per-iteration CPU
+// rate); each refine appends its iterations.
+thread_local std::vector<double> tl_iteration_seconds;
+
 struct Band {
   int n = 0, w = 0;
   std::vector<double> a;  // row i, column j (i - w <= j <= i) at a[i (w + 1) + (i - j)]
@@ -1363,7 +1367,14 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
   for (int si = 0; si < 3 && !done; ++si) {
     const Stage& st = schedule[si];
     bool confirm = false;
+    double t_iter = 0.0;
+    auto close_iteration = [&]() {
+      if (t_iter > 0.0) tl_iteration_seconds.push_back(oracle_now() - t_iter);
+      t_iter = 0.0;
+    };
     for (uint64_t it = 0; it < st.max_iterations; ++it) {
+      close_iteration();
+      t_iter = oracle_now();
       run.iterations++;
       GaugeState g = make_gauge(n, poses, scene);
       double t_it = oracle_now();
@@ -1572,6 +1583,7 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
         }
       }
     }
+    close_iteration();
   }
   // final undamped assembly and certificate
   NativeReport rep{};
@@ -2774,6 +2786,15 @@ void omvgba_oracle_set_shards(int shards) { g_forced_shards = shards; }
 // D = 2048 and the self-calibration marginals); it does not run inside the LM loop they time.
 void omvgba_oracle_set_certificate(int on) { oracle::g_certificate = on != 0; }
 
+// Wall time of each LM iteration of the calling thread's last omvgba_oracle_solve, in order (the
+// solve and, when the self-calibration certificate held groups, the re-solve); returns the count and
+// writes at most cap values.
+int omvgba_oracle_iteration_seconds(double* out, int cap) {
+  const int n = (int)oracle::tl_iteration_seconds.size();
+  for (int i = 0; i < n && i < cap; ++i) out[i] = oracle::tl_iteration_seconds[i];
+  return n;
+}
+
 int omvgba_oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
@@ -2792,6 +2813,7 @@ int32_t omvgba_oracle_solve(const omvgba_problem* problem, const omvgba_config* 
   if (!problem || !config || !solution) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
   try {
     validate_problem(*problem);
+    oracle::tl_iteration_seconds.clear();
     Result r = solve_with_quarantine(*problem, *config);
     std::memcpy(solution->poses, r.poses.data(), sizeof(omvgba_pose) * problem->pose_count);
     std::memcpy(solution->intrinsics, r.intrinsics.data(), sizeof(omvgba_intrinsic) * problem->intrinsic_count);

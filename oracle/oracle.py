@@ -37,6 +37,8 @@ def lib():
         L.omvgba_oracle_set_threads.argtypes = [C.c_int]
         L.omvgba_oracle_set_shards.argtypes = [C.c_int]
         L.omvgba_oracle_set_certificate.argtypes = [C.c_int]
+        L.omvgba_oracle_iteration_seconds.argtypes = [C.POINTER(C.c_double), C.c_int]
+        L.omvgba_oracle_iteration_seconds.restype = C.c_int
         L.omvgba_oracle_max_threads.restype = C.c_int
         L.omvgba_oracle_loss_cost.argtypes = [C.c_int, C.c_double, C.c_double]
         L.omvgba_oracle_loss_cost.restype = C.c_double
@@ -72,6 +74,13 @@ def set_certificate(on: bool) -> None:
     """Timing runs only: skip the final certificate's band factorization (rank above D = 2048 and
     the self-calibration marginals), which runs after the LM loop."""
     lib().omvgba_oracle_set_certificate(int(bool(on)))
+
+
+def iteration_seconds() -> list:
+    """Wall time of each LM iteration of this thread's last solve."""
+    buf = (C.c_double * 4096)()
+    n = lib().omvgba_oracle_iteration_seconds(buf, 4096)
+    return [buf[i] for i in range(min(n, 4096))]
 
 
 def max_threads() -> int:

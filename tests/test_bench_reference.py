@@ -30,7 +30,7 @@ def test_reference_arm_prints_the_contract_line():
                 "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in d, key
     assert d["unit"] == "LM iterations/s" and d["higher_is_better"] is True
-    assert d["value"] > 0 and d["steps"] == 1
+    assert d["value"] > 0 and d["steps"] == 1 and d["ms_per_step"] > 0
     assert d["config"]["workload"].startswith("plane500")
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]

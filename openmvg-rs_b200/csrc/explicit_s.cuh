@@ -20,7 +20,7 @@
 // Uses of the factor: the direct camera step (sparse/direct.rs:259-288), the camera rank test of the
 // final undamped system (sparse/direct.rs:288-455: the spectral test after Jacobi equilibration
 // when D <= 2048, a factorization otherwise), and the self-calibration intrinsic marginal
-// covariances (sparse/covariance.rs:564-587): (S^-1)_pq = (L^-1 e_p) . (L^-1 e_q), forward solves only.
+// covariances (sparse/covariance.rs:564-587) from the selected inverse of S inside the band.
 #pragma once
 
 #include <cstdint>
@@ -482,45 +482,178 @@ __global__ void k_perm_scatter(int n, const int* __restrict__ perm_to_orig, cons
   if (P < n) dst[perm_to_orig[P]] = src[P];
 }
 
-// Intrinsic marginal covariances: CTA per free intrinsic group. For each of the group's parameters
-// (permuted positions pos[3 g .. 3 g + dim)) the forward solve y = L^-1 e_P, which is zero above
-// P's tile; then M_kl = sum_P y_k[P] y_l[P] (fixed order). scratch: 3 n doubles per CTA.
-// out: 9 per group, row-major; a non-finite result is left for the host to see.
-__global__ void __launch_bounds__(256) k_tile_marginals(TileBand tb, int ngroups, const int* __restrict__ pos,
-                                                        const int* __restrict__ dims, double* scratch,
-                                                        double* __restrict__ out, const int* status) {
-  __shared__ double part[4 * kCT];
-  __shared__ double yt[kCT];
-  __shared__ double red[8][9];
+// ---- selected inverse within the band (intrinsic marginal covariances) -----------------------
+// Z = S^-1 restricted to the band of the factor, by the Takahashi recurrence on tiles, from the last
+// tile column to the first: with Z L = L^-T,
+//   Z_ij = -(sum_{k=j+1}^{j+bwt} Z_ik L_kj) L_jj^-1                      (i > j)
+//   Z_jj = (L_jj^-T - sum_{k=j+1}^{j+bwt} Z_kj^T L_kj) L_jj^-1
+// where Z_ik for i < k is Z_ki^T; every Z_ik needed lies in the band. The marginal covariance of a
+// group is the block of Z at its parameters' positions (sparse/covariance.rs:564-587 gets the same
+// block by solving S x = e_p column by column).
+//
+// acc (4 x 4 per thread, 16 x 16 threads) += A B for 64 x 64 tiles staged in shared memory as
+// Ta[q * 64 + r] = A[r][q] and Tb[q * 64 + c] = B[q][c]; the sum over q runs in order.
+__device__ __forceinline__ void tile_mma_acc(const double* Ta, const double* Tb, double acc[4][4]) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll 4
+  for (int q = 0; q < kCT; ++q) {
+    const double2 a01 = *reinterpret_cast<const double2*>(Ta + q * kCT + 4 * ty);
+    const double2 a23 = *reinterpret_cast<const double2*>(Ta + q * kCT + 4 * ty + 2);
+    const double2 b01 = *reinterpret_cast<const double2*>(Tb + q * kCT + 4 * tx);
+    const double2 b23 = *reinterpret_cast<const double2*>(Tb + q * kCT + 4 * tx + 2);
+    const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+  }
+}
+
+// Stage the column-major tile g (element (r, c) at g[c * 64 + r]) as an operand: transpose == false
+// gives T[q * 64 + r] = g(r, q) (the tile as A) and T[q * 64 + c] = g(q, c) with transpose == true
+// (the tile as B); `flip` uses the transposed tile g^T instead of g.
+__device__ __forceinline__ void stage_tile(const double* __restrict__ g, double* T, bool as_b, bool flip) {
+  // as A: T[q*64 + r] = M(r, q); as B: T[q*64 + c] = M(q, c); M = g or g^T
+  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {
+    const int hi = w / kCT, lo = w - hi * kCT;  // T index = hi * 64 + lo
+    // as A: (r, q) = (lo, hi); as B: (q, c) = (hi, lo)
+    const int row = as_b ? hi : lo, col = as_b ? lo : hi;  // element of M
+    const int gr = flip ? col : row, gc = flip ? row : col;  // element of g
+    T[w] = g[(size_t)gc * kCT + gr];
+  }
+}
+
+// Off-diagonal tiles of Z in column j: CTA per i in (j, min(j + bwt, nt - 1)]. Dynamic shared
+// memory: kTakahashiSmem (two staged operands and the accumulated tile).
+constexpr size_t kTakahashiSmem = 3 * sizeof(double) * kCTT;
+__global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand Z, int j, const int* status) {
+  extern __shared__ double sh[];
   if (status[0] == 0) return;
-  const int g = blockIdx.x, tid = threadIdx.x;
-  if (g >= ngroups) return;
-  const int dim = dims[g];
-  int lo = tb.n;
-  for (int k = 0; k < dim; ++k) lo = min(lo, pos[3 * g + k]);
-  const int i0 = lo / kCT;
-  double* y = scratch + (size_t)blockIdx.x * 3 * tb.n;
-  for (int k = 0; k < dim; ++k) {
-    double* v = y + (size_t)k * tb.n;
-    for (int P = i0 * kCT + tid; P < tb.n; P += blockDim.x) v[P] = P == pos[3 * g + k] ? 1.0 : 0.0;
+  double* Ta = sh;
+  double* Tb = sh + kCTT;
+  double* X = sh + 2 * kCTT;  // column-major accumulated tile
+  const int i = j + 1 + blockIdx.x, tid = threadIdx.x;
+  const int kmax = min(L.nt - 1, j + L.bwt);
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k = j + 1; k <= kmax; ++k) {
     __syncthreads();
-    for (int i = i0; i < tb.nt; ++i) tile_forward_rows(tb, v, i, i0, part, yt);
+    if (i >= k)
+      stage_tile(Z.t + tile_at(Z, i, k), Ta, false, false);  // Z_ik
+    else
+      stage_tile(Z.t + tile_at(Z, k, i), Ta, false, true);   // Z_ki^T
+    stage_tile(L.t + tile_at(L, k, j), Tb, true, false);     // L_kj
+    __syncthreads();
+    tile_mma_acc(Ta, Tb, acc);
   }
-  // Gram of the solves, rows from i0 * 64 on (fixed per-thread stride, fixed shuffle and warp order)
-  double acc[9];
-  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-  for (int P = i0 * kCT + tid; P < tb.n; P += blockDim.x)
-    for (int a = 0; a < dim; ++a)
-      for (int b = 0; b < dim; ++b) acc[3 * a + b] += y[(size_t)a * tb.n + P] * y[(size_t)b * tb.n + P];
-  for (int k = 0; k < 9; ++k) acc[k] = warp_sum(acc[k]);
-  if ((tid & 31) == 0)
-    for (int k = 0; k < 9; ++k) red[tid >> 5][k] = acc[k];
   __syncthreads();
-  if (tid < 9) {
-    double s = 0.0;
-    for (int w = 0; w < 8; ++w) s += red[w][tid];
-    out[9 * (size_t)g + tid] = s;
+  {
+    const int ty = tid >> 4, tx = tid & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) X[(4 * tx + b) * kCT + 4 * ty + a] = -acc[a][b];
   }
+  // L_jj (column-major) into Ta
+  for (int w = tid; w < kCTT; w += blockDim.x) Ta[w] = L.t[tile_at(L, j, j) + w];
+  __syncthreads();
+  if (tid < kCT) {  // row r of X: x L_jj = a, solved from the last column back
+    const int r = tid;
+    for (int c = kCT - 1; c >= 0; --c) {
+      double v = X[c * kCT + r];
+      for (int m = c + 1; m < kCT; ++m) v -= X[m * kCT + r] * Ta[c * kCT + m];
+      X[c * kCT + r] = v / Ta[c * kCT + c];
+    }
+  }
+  __syncthreads();
+  double* zij = Z.t + tile_at(Z, i, j);
+  for (int w = tid; w < kCTT; w += blockDim.x) zij[w] = X[w];
+}
+
+// Diagonal tile of Z in column j (after its off-diagonal tiles): one CTA.
+__global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, int j, const int* status) {
+  extern __shared__ double sh[];
+  if (status[0] == 0) return;
+  double* Ta = sh;
+  double* Tb = sh + kCTT;
+  double* X = sh + 2 * kCTT;
+  const int tid = threadIdx.x;
+  const int kmax = min(L.nt - 1, j + L.bwt);
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k = j + 1; k <= kmax; ++k) {
+    __syncthreads();
+    stage_tile(Z.t + tile_at(Z, k, j), Ta, false, true);  // Z_kj^T
+    stage_tile(L.t + tile_at(L, k, j), Tb, true, false);  // L_kj
+    __syncthreads();
+    tile_mma_acc(Ta, Tb, acc);
+  }
+  __syncthreads();
+  {
+    const int ty = tid >> 4, tx = tid & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) X[(4 * tx + b) * kCT + 4 * ty + a] = -acc[a][b];
+  }
+  // W = L_jj^-1 (lower, column-major) into Tb, column by column; L_jj into Ta
+  for (int w = tid; w < kCTT; w += blockDim.x) Ta[w] = L.t[tile_at(L, j, j) + w];
+  __syncthreads();
+  if (tid < kCT) {
+    const int c = tid;  // column c of W: L w = e_c
+    for (int r = 0; r < kCT; ++r) {
+      double v = r == c ? 1.0 : 0.0;
+      for (int m = c; m < r; ++m) v -= Ta[m * kCT + r] * Tb[c * kCT + m];
+      Tb[c * kCT + r] = r < c ? 0.0 : v / Ta[r * kCT + r];
+    }
+  }
+  __syncthreads();
+  // X = (W^T - acc) W, where X currently holds -acc
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    X[w] += Tb[r * kCT + c];  // + W^T(r, c) = W(c, r)
+  }
+  __syncthreads();
+  double out[16];
+  int n_out = 0;
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    double v = 0.0;
+    for (int m = c; m < kCT; ++m) v += X[m * kCT + r] * Tb[c * kCT + m];
+    out[n_out++] = v;
+  }
+  __syncthreads();
+  double* zjj = Z.t + tile_at(Z, j, j);
+  n_out = 0;
+  for (int w = tid; w < kCTT; w += blockDim.x) zjj[w] = out[n_out++];
+}
+
+// (S^-1)_gg of each free group from Z: 9 values per group (row-major), thread per group.
+__global__ void k_z_marginals(TileBand Z, int ngroups, const int* __restrict__ pos, const int* __restrict__ dims,
+                              double* __restrict__ out, const int* status) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups || status[0] == 0) return;
+  const int dim = dims[g];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double v = 0.0;
+      if (a < dim && b < dim) {
+        int P = pos[3 * g + a], Q = pos[3 * g + b];
+        if (P < Q) {
+          const int t = P;
+          P = Q;
+          Q = t;
+        }
+        v = Z.t[tile_at(Z, P / kCT, Q / kCT) + (size_t)(Q % kCT) * kCT + (P % kCT)];
+      }
+      out[9 * (size_t)g + 3 * a + b] = v;
+    }
 }
 
 // Largest |eigenvalue| of the equilibrated D S D by power iteration (Rayleigh quotient of the

@@ -1928,7 +1928,8 @@ static void build_explicit(const NativeProblem& n, const Layout& L, Setup& S) {
       if (S.perm_off[Y] > S.perm_off[X]) continue;
       bwt = std::max(bwt, (S.perm_off[X] + S.blk_dim[X] - 1) / kCT - S.perm_off[Y] / kCT);
     }
-  S.bwt = std::min(bwt, std::max(0, S.nt - 1));
+  // at least one tile below the diagonal, so a block that straddles a tile boundary stays inside
+  S.bwt = std::min(std::max(bwt, 1), std::max(0, S.nt - 1));
 }
 
 uint64_t fnv1a(const void* data, size_t bytes, uint64_t h) {
@@ -2043,7 +2044,7 @@ struct Solver {
   DBuf<uint32_t> d_blk_ent, d_nbr_begin;
   DBuf<int> d_ent_block, d_nbr, d_nbr_row, d_perm_off, d_perm_to_orig;
   DBuf<uint64_t> d_slot_off;
-  DBuf<double> d_rows, d_tiles, d_perm_vec, d_marg_scratch, d_marg_out, d_power;
+  DBuf<double> d_rows, d_tiles, d_ztiles, d_perm_vec, d_marg_out, d_power;
   bool rows_valid = false;  // the rows hold S of the current assembly
   // PCG vectors
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
@@ -2461,12 +2462,9 @@ struct Solver {
     if (sizeof(double) * count > kMaxTileBytes)
       throw SolveFailure{3, "the banded factor of the reduced camera system exceeds 16 GiB"};
     if (d_tiles.n != count) d_tiles.alloc(count, st);
-    static bool attrs = false;
-    if (!attrs) {
-      CUDA_OK(cudaFuncSetAttribute(k_tile_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
-      CUDA_OK(cudaFuncSetAttribute(k_tile_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
-      attrs = true;
-    }
+    // per device and cheap: set on every factorization
+    CUDA_OK(cudaFuncSetAttribute(k_tile_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    CUDA_OK(cudaFuncSetAttribute(k_tile_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
     CUDA_OK(cudaMemsetAsync(d_tiles.p, 0, sizeof(double) * count, st));
     OMVGBA_LAUNCH(k_set_int, 1, 1, 0, st, d_status.p, 1);
     const TileBand tb = tile_band();
@@ -2545,24 +2543,32 @@ struct Solver {
       }
     if (gid.empty()) return true;
     if (!factored_s && !factor_band(0.0, nullptr, 0.0)) return false;
+    // selected inverse of S inside the band (Takahashi recurrence), last tile column first
+    const size_t count = (size_t)S.nt * (S.bwt + 1) * kCTT;
+    d_ztiles.alloc(count, st);
+    CUDA_OK(cudaFuncSetAttribute(k_takahashi_offdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
+    CUDA_OK(cudaFuncSetAttribute(k_takahashi_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
+    const TileBand tl = tile_band();
+    const TileBand tz{D, S.nt, S.bwt, d_ztiles.p};
+    for (int j = S.nt - 1; j >= 0; --j) {
+      const int m = std::min(S.bwt, S.nt - 1 - j);
+      if (m > 0) OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, d_status.p);
+      OMVGBA_LAUNCH(k_takahashi_diag, 1, 256, kTakahashiSmem, st, tl, tz, j, d_status.p);
+    }
     DBuf<int> d_pos, d_dims;
     d_pos.upload(pos.data(), pos.size(), st);
     d_dims.upload(dims.data(), dims.size(), st);
     const int total = (int)gid.size();
-    const int batch = std::min(total, 512);
-    d_marg_scratch.alloc((size_t)batch * 3 * D, st);
     d_marg_out.alloc(9 * (size_t)total, st);
-    for (int b0 = 0; b0 < total; b0 += batch) {
-      const int cnt = std::min(batch, total - b0);
-      OMVGBA_LAUNCH(k_tile_marginals, cnt, 256, 0, st, tile_band(), cnt, d_pos.p + 3 * b0, d_dims.p + b0,
-                    d_marg_scratch.p, d_marg_out.p + 9 * (size_t)b0, d_status.p);
-    }
+    OMVGBA_LAUNCH(k_z_marginals, grid_for(total, 128), 128, 0, st, tz, total, d_pos.p, d_dims.p, d_marg_out.p,
+                  d_status.p);
     check_launch();
     std::vector<double> m(9 * (size_t)total);
     int ok = 0;
     CUDA_OK(copy_async(m.data(), d_marg_out.p, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, st));
     CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
+    d_ztiles.release();
     if (!ok) return false;
     for (int i = 0; i < total; ++i)
       for (int k = 0; k < 9; ++k) out[9 * (size_t)gid[i] + k] = m[9 * (size_t)i + k];

@@ -132,10 +132,16 @@ def test_mixed_precision_reaches_fp64_final_cost(adjuster, self_cal):
 def test_cauchy_and_squared_losses_match_oracle(adjuster, loss, solver):
     """Cauchy runs the reference's continuation (squared warm-up stage, then Cauchy,
     continuation.rs:18-74); the squared loss runs one stage with unit weights. Same iteration,
-    acceptance and status counts as the oracle, final cost to 1e-9, parameters to 1e-7."""
+    acceptance and status counts as the oracle, final cost to 1e-9, parameters to 1e-7.
+
+    The squared loss gives the 5% outliers full weight, which leaves some points nearly singular
+    (rcond ~1e-9); at seed 17 the final undamped S then has an eigenvalue of -1e-5 relative in the
+    oracle's summation order, so its rank certificate (and the quarantine re-solve it triggers) is
+    decided by rounding. Seed 20 keeps every point of the final state above rcond 1e-9 and the
+    smallest equilibrated eigenvalue 7e-5 above the tolerance."""
     from openmvg_ba_cuda import RobustLoss
     rl = RobustLoss.cauchy(2.0) if loss == "cauchy" else RobustLoss.squared()
-    p = synthetic.ring_problem(seed=17, loss=rl)
+    p = synthetic.ring_problem(seed=17 if loss == "cauchy" else 20, loss=rl)
     cfg = SolveConfig(linear_solver=solver, max_iterations=25, pcg_relative_tolerance=1e-10)
     g = adjuster.solve(p, cfg)
     o = O.solve(p, cfg)

@@ -301,6 +301,17 @@ int32_t omvgba_debug_setup_digest(const omvgba_problem* problem, const omvgba_co
                                   uint64_t* digest, omvgba_error* error);
 
 /*
+ * The linear solver a solve of this problem and config would use, without a GPU: an explicit
+ * Direct or Iterative choice as given; Auto resolved by the budget (the explicit
+ * workspace_budget_bytes, else 1 GiB): the direct step when its estimate fits 4/5 of the budget, the
+ * retained PCG first for calibrated problems with at least 250,000 observations and D >= 768
+ * (crates/openmvg-ba/src/kernel/multi_view/sparse/execution_policy.rs:122-253). Also reports both
+ * estimates in bytes. For tests of the policy.
+ */
+int32_t omvgba_debug_execution_plan(const omvgba_problem* problem, const omvgba_config* config, int32_t* iterative,
+                                    uint64_t* direct_estimate, uint64_t* cached_estimate, omvgba_error* error);
+
+/*
  * Reduced camera system product S_lambda x at the first linearization of the lowered problem,
  * computed twice: by the matrix-free kernel the PCG uses (y_matvec) and from the explicit dense
  * Schur complement (y_dense). With x == NULL only *dimension is written. FP64; for operator

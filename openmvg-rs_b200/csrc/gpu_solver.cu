@@ -180,6 +180,10 @@ void context_destroy(Context* c) {
   delete c;
 }
 
+// Device bytes held by the calling thread's live DBufs (a solve's workspace is the growth across its
+// set-up).
+thread_local uint64_t tl_device_bytes = 0;
+
 // Device buffer owned for one solve (stream-ordered allocation).
 template <typename T>
 struct DBuf {
@@ -193,7 +197,10 @@ struct DBuf {
     release();
     s = stream;
     n = count;
-    if (count) CUDA_OK(cudaMallocAsync((void**)&p, sizeof(T) * count, stream));
+    if (count) {
+      CUDA_OK(cudaMallocAsync((void**)&p, sizeof(T) * count, stream));
+      tl_device_bytes += sizeof(T) * count;
+    }
   }
   void upload(const T* host, size_t count, cudaStream_t stream) {
     alloc(count, stream);
@@ -203,7 +210,10 @@ struct DBuf {
     if (n) CUDA_OK(cudaMemsetAsync(p, 0, sizeof(T) * n, s));
   }
   void release() {
-    if (p) cudaFreeAsync(p, s);
+    if (p) {
+      cudaFreeAsync(p, s);
+      tl_device_bytes -= sizeof(T) * n;
+    }
     p = nullptr;
     n = 0;
   }
@@ -1932,6 +1942,63 @@ static void build_explicit(const NativeProblem& n, const Layout& L, Setup& S) {
   S.bwt = std::min(std::max(bwt, 1), std::max(0, S.nt - 1));
 }
 
+// Entries of the lower triangle of S (diagonal blocks included) in the block pattern, and the cross
+// rows of the point caches: per point, one 3-vector per distinct free camera parameter it touches.
+static void pattern_counts(const NativeProblem& n, const Layout& L, const Setup& S, uint64_t* nnz_lower,
+                           uint64_t* cross_rows) {
+  uint64_t nnz = 0;
+  const int nb = (int)S.blk_off.size();
+  for (int X = 0; X < nb; ++X) {
+    const uint64_t dX = (uint64_t)S.blk_dim[X];
+    for (uint32_t q = S.nbr_begin[X]; q < S.nbr_begin[X + 1]; ++q) {
+      const int Y = S.nbr[q];
+      if (Y < X) nnz += dX * (uint64_t)S.blk_dim[Y];
+      if (Y == X) nnz += dX * (dX + 1) / 2;
+    }
+  }
+  uint64_t rows = 0;
+  const size_t P = n.points.size() / 3;
+  std::vector<uint32_t> groups;
+  for (size_t p = 0; p < P; ++p) {
+    groups.clear();
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) {
+      const int c = (int)n.obs_cam[o];
+      rows += (uint64_t)L.pose_dim[c];
+      if (n.self_cal) {
+        const uint32_t g = n.cam_group[c];
+        if (std::find(groups.begin(), groups.end(), g) == groups.end()) {
+          groups.push_back(g);
+          rows += (uint64_t)L.intr_dim[g];
+        }
+      }
+    }
+  }
+  *nnz_lower = nnz;
+  *cross_rows = rows;
+}
+
+// The budget's automatic choice between the direct and the iterative step (SparseWorkspaceMemoryBudget
+// with AUTO_BYTES = 1 GiB unless an explicit budget is given, api.rs:43-52; select_calibrated /
+// select_self_calibrating, execution_policy.rs:122-214): the direct estimate is four values per entry
+// of the lower reduced pattern plus the point caches (execution_policy.rs:101-120, 66-97), the cached
+// retained estimate the point caches plus the camera-space vectors; the direct step must fit 4/5 of
+// the budget (execution_policy.rs:279-285). A calibrated problem with at least 250,000 observations
+// and D >= 768 prefers the retained PCG when it fits (execution_policy.rs:21-22, 139-148).
+static bool auto_prefers_direct(bool self_cal, uint64_t observations, int D, uint64_t points, uint64_t nnz_lower,
+                                uint64_t cross_rows, uint64_t budget, uint64_t* direct_out, uint64_t* cached_out) {
+  const uint64_t limit = budget ? budget : (uint64_t(1) << 30);
+  const uint64_t point_cache = (points + 1) * 8 + points * (1 + 2 * 24) + cross_rows * 24;
+  const uint64_t direct = nnz_lower * 8 * 4 + point_cache;
+  const uint64_t cached = point_cache + (uint64_t)D * (5 * 8 + 8);
+  *direct_out = direct;
+  *cached_out = cached;
+  const uint64_t guarded = limit / 5 * 4 + limit % 5 * 4 / 5;
+  const bool direct_fits = direct <= guarded;
+  if (self_cal) return direct_fits;
+  if (observations >= 250000 && D >= 768 && cached <= limit) return false;
+  return direct_fits;
+}
+
 uint64_t fnv1a(const void* data, size_t bytes, uint64_t h) {
   const unsigned char* c = static_cast<const unsigned char*>(data);
   for (size_t i = 0; i < bytes; ++i) h = (h ^ c[i]) * 1099511628211ull;
@@ -1971,6 +2038,20 @@ uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
     add(*v);
   add(T.slots);
   return h;
+}
+
+ExecutionPlan execution_plan(const NativeProblem& n, const LmOptions& opt) {
+  const Layout L = make_layout(n);
+  Setup S;
+  build_tables(n, L, S);
+  build_explicit(n, L, S);
+  ExecutionPlan plan;
+  uint64_t nnz = 0, rows = 0;
+  pattern_counts(n, L, S, &nnz, &rows);
+  const bool direct = auto_prefers_direct(n.self_cal, n.obs_cam.size(), L.D, n.points.size() / 3, nnz, rows,
+                                          opt.workspace_budget, &plan.direct_estimate, &plan.cached_estimate);
+  plan.iterative = opt.linear_solver == 0 ? !direct : opt.iterative;
+  return plan;
 }
 
 // Device copy of a TileSet plus the fused-matvec launch shape.
@@ -2057,6 +2138,7 @@ struct Solver {
   DBuf<RedVec<1>> d_one, d_one_part;
   DBuf<RedVec<1>> d_norm_part;
   int red_blocks;
+  uint64_t workspace_bytes = 0;
 
   Solver(Context* c, const NativeProblem& prob, const LmOptions& o)
       : ctx(c), st(o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream), n(prob), opt(o) {
@@ -2065,10 +2147,17 @@ struct Solver {
     P = (int)(n.points.size() / 3);
     D = L.D;
     ng = n.self_cal ? (int)n.group_dim.size() : 0;
-    direct = !opt.iterative;
     const double t0 = now();
     build_tables(n, L, S);
     build_explicit(n, L, S);
+    if (opt.linear_solver == 0) {  // Auto: the budget's choice
+      uint64_t nnz = 0, rows = 0, de = 0, ce = 0;
+      pattern_counts(n, L, S, &nnz, &rows);
+      opt.iterative = !auto_prefers_direct(n.self_cal, (uint64_t)N, D, (uint64_t)P, nnz, rows, opt.workspace_budget,
+                                           &de, &ce);
+    }
+    direct = !opt.iterative;
+    const uint64_t bytes_before = tl_device_bytes;
     const double t1 = now();
     // mixed precision keeps only FP32 Jacobian records (and their tiles); FP64 mode only FP64 ones
     mixed = opt.precision == 1 && !direct;
@@ -2081,6 +2170,13 @@ struct Solver {
     red_blocks = std::min(1024, grid_for(std::max(P, N), kReduceThreads));
     upload();
     sync();
+    // the workspace: everything uploaded and allocated for the solve, and the banded factor of the
+    // certificate (twice for self-calibration: the selected inverse has the factor's shape)
+    workspace_bytes = (tl_device_bytes - bytes_before) +
+                      sizeof(double) * (uint64_t)S.nt * (uint64_t)(S.bwt + 1) * kCTT * (n.self_cal ? 2 : 1);
+    if (opt.workspace_budget && workspace_bytes > opt.workspace_budget)
+      throw SolveFailure{3, "GPU workspace " + std::to_string(workspace_bytes) + " bytes exceeds the workspace budget " +
+                                std::to_string(opt.workspace_budget)};
     if (std::getenv("OMVGBA_PHASE_TIMES"))
       std::fprintf(stderr, "[omvgba] setup: tables %.3fs tiles %.3fs upload %.3fs\n", t1 - t0, t2 - t1, now() - t2);
   }
@@ -2438,11 +2534,18 @@ struct Solver {
       CUDA_OK(cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       CUDA_OK(cudaFuncSetAttribute(k_block_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
+    const bool timing = std::getenv("OMVGBA_PHASE_TIMES") != nullptr;
+    if (timing) sync();
+    const double t0 = now();
     if (mixed)
       OMVGBA_LAUNCH(k_block_rows<float>, nb, kRowThreads, smem, st, row_tables(), lin32(), S.max_track, d_rows.p);
     else
       OMVGBA_LAUNCH(k_block_rows<T>, nb, kRowThreads, smem, st, row_tables(), lin(), S.max_track, d_rows.p);
     check_launch();
+    if (timing) {
+      sync();
+      std::fprintf(stderr, "[omvgba] block rows %.4fs (%d blocks, %zu entries)\n", now() - t0, nb, S.nbr.size());
+    }
     rows_valid = true;
   }
 
@@ -2458,6 +2561,7 @@ struct Solver {
   static constexpr size_t kMaxTileBytes = size_t(16) << 30;
   bool factor_band(double lambda, const double* scale, double shift) {
     if (D == 0) return true;
+    const double t_factor = now();
     const size_t count = (size_t)S.nt * (S.bwt + 1) * kCTT;
     if (sizeof(double) * count > kMaxTileBytes)
       throw SolveFailure{3, "the banded factor of the reduced camera system exceeds 16 GiB"};
@@ -2483,6 +2587,8 @@ struct Solver {
     int ok = 0;
     CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
+    if (std::getenv("OMVGBA_PHASE_TIMES"))
+      std::fprintf(stderr, "[omvgba] band factor %.4fs (nt %d bwt %d) ok %d\n", now() - t_factor, S.nt, S.bwt, ok);
     return ok != 0;
   }
 
@@ -3154,16 +3260,26 @@ struct Solver {
     }
     // final undamped assembly and certificate: the camera rank (sparse/direct.rs:288-455) and, for
     // self-calibration, the intrinsic marginal covariances (native/self_calibration.rs:255-303)
+    const bool timing = std::getenv("OMVGBA_PHASE_TIMES") != nullptr;
+    double tc = now();
     Gauge g = gauge_for(cur, scene);
     Assembly fa = assemble(cur, g, opt.loss, 0.0, true);
+    if (timing) sync();
+    const double t_final_assembly = now() - tc;
+    tc = now();
     bool factored_s = false;
     if (!fa.valid)
       rep.rank = 2;
     else
       rep.rank = rank_certificate(&factored_s);
+    const double t_rank = now() - tc;
+    tc = now();
     if (n.self_cal && opt.certify_intrinsics) {
       rep.marginals_ok = fa.valid && intrinsic_marginals(factored_s, rep.marginals) ? 1 : 0;
     }
+    if (timing)
+      std::fprintf(stderr, "[omvgba] certificate: final assembly %.4fs rank %.4fs marginals %.4fs (nt %d bwt %d)\n",
+                   t_final_assembly, t_rank, now() - tc, S.nt, S.bwt);
     bool well = rep.rank != 2 && fa.weak == 0;
     if (std::getenv("OMVGBA_PHASE_TIMES"))
       std::fprintf(stderr, "[omvgba] final: valid=%d rank=%d weak=%llu D=%d min_rcond=%.3e cost=%.12e\n", (int)fa.valid,
@@ -3199,6 +3315,7 @@ struct Solver {
     }
     rep.pcg_terms = pcg_terms;
     rep.final_damping = lambda;
+    rep.iterative = direct ? 0 : 1;
     if (std::getenv("OMVGBA_PHASE_TIMES"))
       std::fprintf(stderr,
                    "[omvgba] assemble %.3fs solve %.3fs candidate %.3fs total %.3fs pcg_terms %llu rejections "
@@ -3362,6 +3479,7 @@ void gpu_debug_schur_product(Context* ctx, const NativeProblem& problem, const L
   CUDA_OK(cudaSetDevice(ctx->device));
   LmOptions o = options;
   o.iterative = false;
+  o.linear_solver = 1;
   Solver<double> s(ctx, problem, o);
   double scene = s.scene_scale_host();
   Gauge g = s.gauge_for(s.cur, scene);

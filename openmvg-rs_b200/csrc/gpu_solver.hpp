@@ -70,7 +70,9 @@ struct LmOptions {
   uint64_t max_iterations = 50;
   LossDev loss{kLossL2, 0.0};
   double gradient_tolerance = 1e-10, step_tolerance = 1e-8, relative_cost_tolerance = 1e-6;
-  bool iterative = false;
+  bool iterative = false;           // the linear solver in use (resolved from Auto by the solver)
+  int linear_solver = 1;            // the configuration's choice: 0 Auto, 1 Direct, 2 Iterative
+  uint64_t workspace_budget = 0;    // explicit workspace budget in bytes, 0 when none
   double pcg_tolerance = 1e-1;
   uint64_t pcg_max_iterations = 600;
   int precision = 0;  // 0 FP64, 1 mixed
@@ -97,7 +99,17 @@ struct NativeReport {
   // group (row-major, the free dim x dim corner used); marginals_ok = 0 when S does not factor
   std::vector<double> marginals;
   int marginals_ok = 0;
+  int iterative = 0;  // the linear solver the solve used (Auto resolved)
 };
+
+// The execution plan a solve would use, computed on the host without a GPU: Auto resolved against
+// the budget (sparse/execution_policy.rs:122-253 restated with this solver's estimates) and the
+// device workspace it needs.
+struct ExecutionPlan {
+  bool iterative = false;
+  uint64_t direct_estimate = 0, cached_estimate = 0, workspace_bytes = 0;
+};
+ExecutionPlan execution_plan(const NativeProblem& problem, const LmOptions& options);
 
 struct Context;  // device, stream, pinned scratch
 

@@ -653,12 +653,11 @@ LmOptions lm_options(const omvgba_problem& pr, const omvgba_config& cfg, const N
   o.step_tolerance = cfg.parameter_tolerance;
   o.relative_cost_tolerance = cfg.function_tolerance;
   int D = reduced_dimension(n);
-  if (cfg.linear_solver == OMVGBA_SOLVER_DIRECT)
-    o.iterative = false;
-  else if (cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE)
-    o.iterative = true;
-  else
-    o.iterative = D > o.dense_rank_limit;  // Auto: dense direct below the dense limit
+  (void)D;
+  // Auto is resolved by the solver once it knows the reduced pattern (execution_policy.rs:122-253)
+  o.linear_solver = cfg.linear_solver;
+  o.iterative = cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE;
+  o.workspace_budget = cfg.has_workspace_budget ? cfg.workspace_budget_bytes : 0;
   o.pcg_tolerance = cfg.pcg_relative_tolerance > 0.0 ? cfg.pcg_relative_tolerance : 1e-1;
   o.pcg_max_iterations = cfg.pcg_max_iterations > 0 ? cfg.pcg_max_iterations : 600;
   o.precision = cfg.precision;
@@ -1108,7 +1107,7 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
     }
   }
   const double t_gpu = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_lower;
-  Result res = raise(pr, L, rot, tr, pts, grp, nr, opt.iterative);
+  Result res = raise(pr, L, rot, tr, pts, grp, nr, nr.iterative != 0);
   res.unconstrained = held;
   res.report.unconstrained_intrinsic_count = held.size();
   finish_solution(pr, res);
@@ -1695,6 +1694,30 @@ int32_t omvgba_debug_linearize(omvgba_context* context, const omvgba_problem* pr
 // Debug: digest of the host side of a solve's set-up (quarantine preparation, lowering, block
 // tables and matvec tiles) built with at most `threads` host threads (0: all); uses no GPU. Every
 // parallel loop of the set-up is arranged so that this does not depend on `threads`.
+int32_t omvgba_debug_execution_plan(const omvgba_problem* problem, const omvgba_config* config, int32_t* iterative,
+                                    uint64_t* direct_estimate, uint64_t* cached_estimate, omvgba_error* error) {
+  clear_error(error);
+  if (!problem || !config || !iterative || !direct_estimate || !cached_estimate)
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  try {
+    validate_problem(*problem);
+    validate_config(*config);
+    Prepared prep;
+    prepare_quarantine(*problem, *config, prep);
+    Lowered L = lower(*prep.working);
+    LmOptions opt = lm_options(*prep.working, *config, L.n);
+    ExecutionPlan plan = execution_plan(L.n, opt);
+    *iterative = plan.iterative ? 1 : 0;
+    *direct_estimate = plan.direct_estimate;
+    *cached_estimate = plan.cached_estimate;
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
 int32_t omvgba_debug_setup_digest(const omvgba_problem* problem, const omvgba_config* config, uint32_t threads,
                                   uint64_t* digest, omvgba_error* error) {
   clear_error(error);
@@ -1812,7 +1835,7 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
       }
     }
     laps[0] = seconds_since(t0);
-    Result first = raise(working, *lowered, rot, tr, pts, grp, nr, plan->options.iterative);
+    Result first = raise(working, *lowered, rot, tr, pts, grp, nr, nr.iterative != 0);
     first.unconstrained = held;
     first.report.unconstrained_intrinsic_count = held.size();
     laps[1] = seconds_since(t0);

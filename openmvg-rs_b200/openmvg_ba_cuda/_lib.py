@@ -43,6 +43,9 @@ def lib():
     L.omvgba_debug_setup_digest.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config), C.c_uint32,
                                              C.POINTER(C.c_uint64), C.POINTER(abi.Error)]
     L.omvgba_debug_setup_digest.restype = C.c_int32
+    L.omvgba_debug_execution_plan.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config), C.POINTER(C.c_int32),
+                                              C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(abi.Error)]
+    L.omvgba_debug_execution_plan.restype = C.c_int32
     L.omvgba_solve_batched.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(abi.Problem), C.POINTER(abi.Config),
                                        C.POINTER(abi.Solution), C.POINTER(abi.Error)]
     L.omvgba_solve_batched.restype = C.c_int32

@@ -2418,10 +2418,90 @@ static void canonicalize(const omvgba_problem& pr, Result& res) {
   refresh_inliers(pr, active, res);
 }
 
-static bool choose_iterative(const omvgba_config& cfg, int D) {
+// Entries of the lower triangle of the reduced pattern (diagonal blocks included) and the cross rows
+// of the point caches (one per distinct free camera parameter a point touches).
+static void pattern_counts(const Native& n, const Layout& L, uint64_t* nnz_lower, uint64_t* cross_rows) {
+  const size_t nb = L.block_off.size();
+  std::vector<std::vector<int>> lower(nb);
+  std::vector<int> blocks;
+  uint64_t rows = 0;
+  for (size_t p = 0; p < n.points.size(); ++p) {
+    blocks.clear();
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) {
+      const int c = n.obs_cam[o];
+      if (L.pose_dim[c] > 0) {
+        blocks.push_back(L.param_block[L.pose_off[c]]);
+        rows += L.pose_dim[c];
+      }
+      if (n.self_cal) {
+        const int g = n.cam_group[c];
+        if (L.intr_dim[g] > 0) {
+          const int b = L.param_block[L.intr_off[g]];
+          if (std::find(blocks.begin(), blocks.end(), b) == blocks.end()) rows += L.intr_dim[g];
+          blocks.push_back(b);
+        }
+      }
+    }
+    std::sort(blocks.begin(), blocks.end());
+    blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
+    for (size_t i = 0; i < blocks.size(); ++i)
+      for (size_t j = 0; j <= i; ++j) lower[blocks[i]].push_back(blocks[j]);
+  }
+  uint64_t nnz = 0;
+  for (size_t X = 0; X < nb; ++X) {
+    std::sort(lower[X].begin(), lower[X].end());
+    lower[X].erase(std::unique(lower[X].begin(), lower[X].end()), lower[X].end());
+    const uint64_t dX = L.block_dim[X];
+    for (int Y : lower[X]) nnz += (size_t)Y == X ? dX * (dX + 1) / 2 : dX * (uint64_t)L.block_dim[Y];
+  }
+  *nnz_lower = nnz;
+  *cross_rows = rows;
+}
+
+// Auto: the budget's choice between the direct and the iterative step (sparse/execution_policy.rs:
+// 122-214 with SparseWorkspaceMemoryBudget::AUTO_BYTES = 1 GiB unless an explicit budget is given,
+// api.rs:43-52): the direct estimate (four values per entry of the lower reduced pattern plus the
+// point caches) must fit 4/5 of the budget; calibrated problems with at least 250,000 observations
+// and D >= 768 take the retained PCG first when its estimate (the point caches and the camera-space
+// vectors) fits the budget.
+static bool auto_prefers_direct(const Native& n, const Layout& L, uint64_t budget, uint64_t* direct_out,
+                                uint64_t* cached_out) {
+  uint64_t nnz = 0, rows = 0;
+  pattern_counts(n, L, &nnz, &rows);
+  const uint64_t limit = budget ? budget : (uint64_t(1) << 30);
+  const uint64_t points = n.points.size();
+  const uint64_t point_cache = (points + 1) * 8 + points * (1 + 2 * 24) + rows * 24;
+  const uint64_t direct = nnz * 8 * 4 + point_cache;
+  const uint64_t cached = point_cache + (uint64_t)L.D * (5 * 8 + 8);
+  *direct_out = direct;
+  *cached_out = cached;
+  const bool direct_fits = direct <= limit / 5 * 4 + limit % 5 * 4 / 5;
+  if (n.self_cal) return direct_fits;
+  if (n.obs_cam.size() >= 250000 && L.D >= 768 && cached <= limit) return false;
+  return direct_fits;
+}
+
+static bool choose_iterative(const omvgba_config& cfg, const Native& n, const Layout& L) {
   if (cfg.linear_solver == OMVGBA_SOLVER_DIRECT) return false;
   if (cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE) return true;
-  return D > kDenseRankLimit;  // Auto: dense direct for small reduced systems, PCG above
+  uint64_t de = 0, ce = 0;
+  return !auto_prefers_direct(n, L, cfg.has_workspace_budget ? cfg.workspace_budget_bytes : 0, &de, &ce);
+}
+
+// Refuse, before the first iteration, a workspace over an explicit budget (native/mod.rs:557-570):
+// the oracle's own storage for the solve -- point caches, the Hessian blocks (the dense S up to
+// D = 2048) and the camera-space vectors.
+static void check_workspace_budget(const omvgba_config& cfg, const Native& n, const Layout& L) {
+  if (!cfg.has_workspace_budget) return;
+  uint64_t nnz = 0, rows = 0;
+  pattern_counts(n, L, &nnz, &rows);
+  const uint64_t P = n.points.size(), D = (uint64_t)L.D;
+  uint64_t bytes = P * (1 + 48 + 48 + 24 + 24) + (P + 1) * 8 + rows * (24 + 4) + D * 8 * 12;
+  if (D <= (uint64_t)kDenseRankLimit) bytes += D * D * 8;
+  for (int d : L.block_dim) bytes += (uint64_t)d * d * 8 * 2;
+  if (bytes > cfg.workspace_budget_bytes)
+    fail(OMVGBA_RESOURCE_EXHAUSTED, "workspace " + std::to_string(bytes) + " bytes exceeds the workspace budget " +
+                                        std::to_string(cfg.workspace_budget_bytes));
 }
 
 static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
@@ -2436,7 +2516,8 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   opt.max_iterations = cfg.max_iterations;
   opt.loss = problem_loss(pr);
   opt.criteria = {cfg.gradient_tolerance, cfg.parameter_tolerance, cfg.function_tolerance};
-  opt.iterative = choose_iterative(cfg, L.D);
+  opt.iterative = choose_iterative(cfg, n, L);
+  check_workspace_budget(cfg, n, L);
   opt.pcg_tol = cfg.pcg_relative_tolerance > 0.0 ? cfg.pcg_relative_tolerance : 1e-1;
   opt.pcg_max = cfg.pcg_max_iterations > 0 ? cfg.pcg_max_iterations : 600;
   std::vector<NPose> poses = n.poses;
@@ -2456,7 +2537,7 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
       points = n.points;
       groups = n.groups;
       Options again = opt;
-      again.iterative = choose_iterative(cfg, make_layout(n).D);
+      again.iterative = choose_iterative(cfg, n, make_layout(n));
       again.certify_intrinsics = false;
       t0 = oracle_now();
       nr = refine(n, poses, points, groups, again);
@@ -2793,6 +2874,41 @@ int omvgba_oracle_iteration_seconds(double* out, int cap) {
   const int n = (int)oracle::tl_iteration_seconds.size();
   for (int i = 0; i < n && i < cap; ++i) out[i] = oracle::tl_iteration_seconds[i];
   return n;
+}
+
+// The oracle's execution plan: the linear solver it would use (Auto resolved) and its estimates.
+int omvgba_oracle_execution_plan(const omvgba_problem* problem, const omvgba_config* config, int32_t* iterative,
+                                 uint64_t* direct_estimate, uint64_t* cached_estimate, omvgba_error* error) {
+  try {
+    oracle::validate_problem(*problem);
+    oracle::validate_config(*config);
+    // the solve's input quarantine first (quarantine.rs:34-96): points seen fewer than twice or
+    // without parallax are held out before the lowering
+    const omvgba_problem& pr = *problem;
+    std::vector<uint64_t> counts(pr.point_count, 0);
+    for (size_t o = 0; o < pr.observation_count; ++o) counts[pr.observation_point[o]]++;
+    std::set<size_t> held;
+    for (size_t p = 0; p < pr.point_count; ++p)
+      if (counts[p] < 2 && !oracle::point_fixed(pr, p)) held.insert(p);
+    for (size_t p : oracle::degenerate_points(pr, pr.poses, pr.points))
+      if (!oracle::point_fixed(pr, p)) held.insert(p);
+    oracle::Restricted first;
+    const omvgba_problem* working = &pr;
+    if (!held.empty()) {
+      oracle::without_points(pr, nullptr, held, first);
+      working = &first.view;
+    }
+    oracle::Native n = oracle::has_free_intrinsics(*working) ? oracle::lower_self_calibrating(*working)
+                                                             : oracle::lower_calibrated(*working);
+    oracle::Layout L = oracle::make_layout(n);
+    const bool direct = oracle::auto_prefers_direct(
+        n, L, config->has_workspace_budget ? config->workspace_budget_bytes : 0, direct_estimate, cached_estimate);
+    *iterative = config->linear_solver == OMVGBA_SOLVER_AUTO ? !direct
+                                                             : config->linear_solver == OMVGBA_SOLVER_ITERATIVE;
+    return OMVGBA_OK;
+  } catch (const oracle::SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
 }
 
 int omvgba_oracle_max_threads(void) {

@@ -37,6 +37,10 @@ def lib():
         L.omvgba_oracle_set_threads.argtypes = [C.c_int]
         L.omvgba_oracle_set_shards.argtypes = [C.c_int]
         L.omvgba_oracle_set_certificate.argtypes = [C.c_int]
+        L.omvgba_oracle_execution_plan.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config),
+                                                   C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
+                                                   C.POINTER(C.c_uint64), C.POINTER(abi.Error)]
+        L.omvgba_oracle_execution_plan.restype = C.c_int32
         L.omvgba_oracle_iteration_seconds.argtypes = [C.POINTER(C.c_double), C.c_int]
         L.omvgba_oracle_iteration_seconds.restype = C.c_int
         L.omvgba_oracle_max_threads.restype = C.c_int
@@ -133,3 +137,16 @@ def residual_vjp(inputs: dict, grad=None):
     lib().omvgba_oracle_residual_vjp(n, cam.ctypes.data_as(u32p), pt.ctypes.data_as(u32p), P(px), P(rv), P(t), P(it),
                                      P(X), P(g), P(res), P(gr), P(gt), P(gi), P(gp))
     return res, {"rotvec": gr, "translation": gt, "intrinsics": gi, "points": gp}
+
+
+def execution_plan(problem, config):
+    """(iterative, direct estimate, cached estimate) the oracle would use for this problem and config."""
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.problem import raise_for
+    mp = abi.MarshalledProblem(problem)
+    cfg = config.to_struct()
+    it, de, ce, err = C.c_int32(), C.c_uint64(), C.c_uint64(), abi.Error()
+    code = lib().omvgba_oracle_execution_plan(C.byref(mp.struct), C.byref(cfg), C.byref(it), C.byref(de),
+                                              C.byref(ce), C.byref(err))
+    raise_for(code, err)
+    return bool(it.value), int(de.value), int(ce.value)

@@ -1051,6 +1051,33 @@ namespace omvgba {
 // ----------------------------------------------------------------------------------------------
 // Block-Jacobi preconditioner (FP64): P_b = U_bb + lambda D_b - C_b - cross pairs
 // ----------------------------------------------------------------------------------------------
+// PackedCameraBlockFactor::factor (retained/block.rs:171-218): Jacobi-scaled Cholesky of the d x d
+// block m into F (36 lower row-major, then the 6 scales); false when it is not positive definite.
+__device__ bool camera_block_factor(double m[6][6], int d, double* F) {
+  double ds = 0.0;
+  for (int i = 0; i < d; ++i) ds = fmax(ds, m[i][i]);
+  if (!(isfinite(ds) && ds > 0.0)) return false;
+  double fl = 64.0 * kEps * ds;
+  double sc[6];
+  for (int i = 0; i < d; ++i) sc[i] = sqrt(fmax(m[i][i], fl));
+  double L[6][6];
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c <= r; ++c) {
+      double v = m[r][c] / (sc[r] * sc[c]);
+      for (int k = 0; k < c; ++k) v -= L[r][k] * L[c][k];
+      if (r == c) {
+        if (!(isfinite(v) && v > 64.0 * kEps)) return false;
+        L[r][c] = sqrt(v);
+      } else {
+        L[r][c] = v / L[c][c];
+      }
+    }
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 6; ++c) F[6 * r + c] = (r < d && c <= r) ? L[r][c] : 0.0;
+  for (int i = 0; i < 6; ++i) F[36 + i] = i < d ? sc[i] : 1.0;
+  return true;
+}
+
 __global__ void k_block_factor(BlockTables bt, const double* blk_out, const double* diag, double lambda,
                                const double* cross, const int* blk_cross_begin, const int* blk_cross_end,
                                double* factor, int* fail) {
@@ -1073,36 +1100,27 @@ __global__ void k_block_factor(BlockTables bt, const double* blk_out, const doub
       for (int c = 0; c < d; ++c) m[r][c] -= cv[6 * r + c] + cv[6 * c + r];
   }
   for (int k = 0; k < d; ++k) m[k][k] += lambda * diag[o + k];
-  // PackedCameraBlockFactor::factor (retained/block.rs:171-218)
-  double* F = factor + 42 * (size_t)b;  // 36 lower + 6 scale
-  double ds = 0.0;
-  for (int i = 0; i < d; ++i) ds = fmax(ds, m[i][i]);
-  if (!(isfinite(ds) && ds > 0.0)) {
-    fail[b] = 1;
-    return;
-  }
-  double fl = 64.0 * kEps * ds;
-  double sc[6];
-  for (int i = 0; i < d; ++i) sc[i] = sqrt(fmax(m[i][i], fl));
-  double L[6][6];
-  for (int r = 0; r < d; ++r)
-    for (int c = 0; c <= r; ++c) {
-      double v = m[r][c] / (sc[r] * sc[c]);
-      for (int k = 0; k < c; ++k) v -= L[r][k] * L[c][k];
-      if (r == c) {
-        if (!(isfinite(v) && v > 64.0 * kEps)) {
-          fail[b] = 1;
-          return;
-        }
-        L[r][c] = sqrt(v);
-      } else {
-        L[r][c] = v / L[c][c];
-      }
-    }
+  fail[b] = camera_block_factor(m, d, factor + 42 * (size_t)b) ? 0 : 1;
+}
+
+// The same block-Jacobi factors from the explicit S: block b's diagonal block of the rows plus
+// lambda diag (retained/mod.rs:904-934).
+__global__ void k_block_factor_rows(RowTables rt, const double* rows, const double* diag, double lambda,
+                                    double* factor, int* fail) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= rt.nblocks) return;
+  const int d = rt.blk_dim[b], o = rt.blk_off[b];
+  const int s = find_slot(rt.nbr, rt.nbr_begin[b], rt.nbr_begin[b + 1], b);
+  double m[6][6];
   for (int r = 0; r < 6; ++r)
-    for (int c = 0; c < 6; ++c) F[6 * r + c] = (r < d && c <= r) ? L[r][c] : 0.0;
-  for (int i = 0; i < 6; ++i) F[36 + i] = i < d ? sc[i] : 1.0;
-  fail[b] = 0;
+    for (int c = 0; c < 6; ++c) m[r][c] = 0.0;
+  if (s >= 0) {
+    const double* S = rows + rt.slot_off[rt.nbr_begin[b] + s];
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c) m[r][c] = S[r * d + c];
+  }
+  for (int k = 0; k < d; ++k) m[k][k] += lambda * diag[o + k];
+  fail[b] = camera_block_factor(m, d, factor + 42 * (size_t)b) ? 0 : 1;
 }
 
 __global__ void k_block_precond(BlockTables bt, const double* factor, const double* r, double* z,
@@ -2139,6 +2157,7 @@ struct Solver {
   DBuf<RedVec<1>> d_norm_part;
   int red_blocks;
   uint64_t workspace_bytes = 0;
+  bool explicit_op = false;
 
   Solver(Context* c, const NativeProblem& prob, const LmOptions& o)
       : ctx(c), st(o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream), n(prob), opt(o) {
@@ -2157,6 +2176,9 @@ struct Solver {
                                            &de, &ce);
     }
     direct = !opt.iterative;
+    // the PCG operator: the explicit S by block rows (rebuilt every assembly, a block-sparse product
+    // that stays in L2) or the matrix-free tile product over the Jacobian records
+    explicit_op = !direct && opt.matvec == 1;
     const uint64_t bytes_before = tl_device_bytes;
     const double t1 = now();
     // mixed precision keeps only FP32 Jacobian records (and their tiles); FP64 mode only FP64 ones
@@ -2704,6 +2726,12 @@ struct Solver {
   // before them (inside the PCG graph)
   void matvec(const double* x, double* y, double lambda, const PcgCtl* ctl = nullptr, bool fp32 = false,
               double* xy = nullptr, bool pdl_tiles = false, bool pdl = false) {
+    if (explicit_op) {  // block-sparse product of the explicit S (FP64 rows)
+      launch_pdl(pdl_tiles, k_rows_matvec, mv_finalize_ctas(), 256, st, row_tables(), (const double*)d_rows.p,
+                 (const double*)d_diag.p, lambda, (const double*)nullptr, x, y, xy, ctl);
+      check_launch();
+      return;
+    }
     matvec_tiles(x, ctl, fp32, pdl_tiles);
     const TileSetDev& ts = mixed ? dT32 : dT64;
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
@@ -2731,14 +2759,18 @@ struct Solver {
   bool factor_preconditioner(double lambda) {
     BlockTables bt = tables();
     PairTables xt = pairs();
-    if (xt.ngroups > 0) {
+    if (explicit_op) {
+      OMVGBA_LAUNCH(k_block_factor_rows, grid_for(nb, 64), 64, 0, st, row_tables(), d_rows.p, d_diag.p, lambda,
+                    d_factor.p, d_fail.p);
+    } else if (xt.ngroups > 0) {
       if (mixed)
         OMVGBA_LAUNCH(k_pairs<float>, xt.ngroups, 32, 0, st, xt, bt, lin32(), d_seg_col.p, d_xpair_out.p);
       else
         OMVGBA_LAUNCH(k_pairs<T>, xt.ngroups, 32, 0, st, xt, bt, lin(), d_seg_col.p, d_xpair_out.p);
     }
-    OMVGBA_LAUNCH(k_block_factor, grid_for(nb, 64), 64, 0, st, bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
-                                                   d_blk_cross_begin.p, d_blk_cross_end.p, d_factor.p, d_fail.p);
+    if (!explicit_op)
+      OMVGBA_LAUNCH(k_block_factor, grid_for(nb, 64), 64, 0, st, bt, d_blk_out.p, d_diag.p, lambda, d_xpair_out.p,
+                    d_blk_cross_begin.p, d_blk_cross_end.p, d_factor.p, d_fail.p);
     check_launch();
     std::vector<int> fail(std::max(nb, 1));
     if (nb > 0) CUDA_OK(copy_async(fail.data(), d_fail.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
@@ -3113,7 +3145,7 @@ struct Solver {
         iterations++;
         double t0 = now();
         Gauge g = gauge_for(cur, scene);
-        Assembly a = assemble(cur, g, stages[si].loss, lambda, direct);
+        Assembly a = assemble(cur, g, stages[si].loss, lambda, direct || explicit_op);
         double t1 = now();
         t_assemble += t1 - t0;
         if (!have_initial && std::isfinite(a.cost) && std::isfinite(a.sq) && N > 0) {
@@ -3143,7 +3175,8 @@ struct Solver {
           if (solved) {
             double tol = confirm ? std::min(opt.pcg_tolerance, iter_tol) : opt.pcg_tolerance;
             uint64_t limit = confirm ? opt.pcg_max_iterations : std::min<uint64_t>(opt.pcg_max_iterations, (uint64_t)D);
-            PcgResult r = mixed ? pcg_mixed(lambda, limit, tol) : pcg(lambda, limit, tol);
+            // the explicit S is FP64 in both precisions, so its PCG needs no FP32 refinement loop
+            PcgResult r = mixed && !explicit_op ? pcg_mixed(lambda, limit, tol) : pcg(lambda, limit, tol);
             pcg_terms += r.terms;
             solved = r.accepted;
             iterative_step = true;

@@ -152,3 +152,24 @@ def test_cauchy_and_squared_losses_match_oracle(adjuster, loss, solver):
     assert _rel(rg["initial_objective"], ro["initial_objective"]) < 1e-12
     assert _rel(rg["final_objective"], ro["final_objective"]) < 1e-9
     _check_parameters(g, o, _oracle_spread(p, cfg))
+
+
+@pytest.mark.parametrize("case", ["ring_self_cal", "plane500_40k"])
+def test_explicit_schur_pcg_matches_matrix_free_pcg_and_oracle(adjuster, case):
+    """Block-Jacobi PCG on the explicit block-sparse S (block rows, rebuilt each LM iteration) and on
+    the matrix-free product agree to rounding, and both match the oracle's retained PCG."""
+    if case == "ring_self_cal":
+        p = synthetic.ring_problem(seed=9, self_calibrating=True, radius=3.0)
+        cfg = SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, max_iterations=30, pcg_relative_tolerance=1e-10)
+    else:
+        p = synthetic.plane_problem(seed=11, cameras=500, points=40_000, mean_track=6.5, extent=100.0)
+        cfg = SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, max_iterations=5, pcg_relative_tolerance=1e-10)
+    explicit = adjuster.solve(p, cfg.with_(matvec=abi.MATVEC_EXPLICIT))
+    implicit = adjuster.solve(p, cfg.with_(matvec=abi.MATVEC_IMPLICIT))
+    o = O.solve(p, cfg)
+    for g in (explicit, implicit):
+        for k in ("iteration_count", "accepted_step_count", "rejected_step_count", "status",
+                  "unconstrained_intrinsic_count"):
+            assert g.report[k] == o.report[k], (k, g.report[k], o.report[k])
+        assert _rel(g.report["final_objective"], o.report["final_objective"]) < 1e-9
+    assert _param_diff(explicit, implicit) < 1e-7

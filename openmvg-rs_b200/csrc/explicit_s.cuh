@@ -64,80 +64,126 @@ __device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n
 // M = [o == o'] I - Jp_o Vhat_p^-1 Jp_o'^T (U, the pose/intrinsic edges and the point coupling in one
 // term). Targets of one point that fall in the same block are summed in target order by one thread
 // per element; entities are taken one after another, so every element is accumulated in entity
-// order. FP64 accumulation from records of type R. Dynamic shared memory: max_track x 24 doubles
-// plus 2 x 2 x max_track ints.
+// order. FP64 accumulation from records of type R.
+//
+// Latency: a CTA walks thousands of entities one after another, so the per-entity chain is kept
+// short: the records of a track of up to kRowStage observations are staged in shared memory (longer
+// tracks are read from global memory), the block's neighbour list sits in shared memory when it has
+// at most kRowNbr entries, and thread 0 fetches the next entity's indices while the current one is
+// computed. Small static shared memory keeps many CTAs resident. Dynamic shared memory: 4 x
+// max_track ints (the target slots and columns).
+constexpr int kRowStage = 32;
+constexpr int kRowNbr = 1024;
 template <typename R>
 __global__ void __launch_bounds__(kRowThreads) k_block_rows(RowTables rt, LinOut<R> lin, int max_track,
                                                             double* __restrict__ rows) {
-  extern __shared__ double smem[];
-  double* jr = smem;                                            // per observation of the point: 24 record values
-  int* tslot = reinterpret_cast<int*>(jr + (size_t)max_track * kRec);  // per target: slot or -1
-  int* tcol = tslot + 2 * max_track;                            // per target: column of its segment
-  __shared__ double G[6];                                       // Jp_o Vhat^-1 (2 x 3)
-  __shared__ double aX[12];                                     // the entity's 2 x dX camera columns
+  extern __shared__ int ish[];
+  int* tslot = ish;                  // per target: slot or -1
+  int* tcol = ish + 2 * max_track;   // per target: column of its segment
+  __shared__ double jr[kRowStage * kRec];  // the point's records (tracks of at most kRowStage)
+  __shared__ int nbr_s[kRowNbr];
+  __shared__ double G[6];                  // Jp_o Vhat^-1 (2 x 3)
+  __shared__ double aX[12];                // the entity's 2 x dX camera columns
+  __shared__ uint32_t s_ent[2][4];         // current / next entity: e, point, first observation, track length
   const int X = blockIdx.x, tid = threadIdx.x;
   if (X >= rt.nblocks) return;
   const int dX = rt.blk_dim[X];
   const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1];
+  const bool nbr_local = n1 - n0 <= (uint32_t)kRowNbr;
+  if (nbr_local)
+    for (uint32_t k = tid; k < n1 - n0; k += blockDim.x) nbr_s[k] = rt.nbr[n0 + k];
   const uint64_t r0 = rt.slot_off[n0], r1 = rt.slot_off[n1];
   for (uint64_t k = r0 + tid; k < r1; k += blockDim.x) rows[k] = 0.0;
+  const uint32_t i0 = rt.blk_ent[X], i1 = rt.blk_ent[X + 1];
+  if (tid == 0 && i0 < i1) {
+    const uint32_t e = rt.ent[i0], p = rt.ent_point[i0];
+    const uint32_t a = rt.pt_off[p], b = rt.pt_off[p + 1];
+    s_ent[0][0] = e;
+    s_ent[0][1] = p;
+    s_ent[0][2] = a;
+    s_ent[0][3] = b - a;
+  }
   const int rs = lin.rs;
-  for (uint32_t i = rt.blk_ent[X]; i < rt.blk_ent[X + 1]; ++i) {
-    const uint32_t e = rt.ent[i], o = e >> 1, p = rt.ent_point[i];
-    const uint32_t o0 = rt.pt_off[p], L = rt.pt_off[p + 1] - o0;
-    __syncthreads();  // the previous entity is finished with the staging (and the row is zeroed)
-    for (uint32_t k = tid; k < (uint32_t)kRec * L; k += blockDim.x) {
-      const uint32_t c = k / L, j = k - c * L;
-      jr[j * kRec + c] = (double)lin.rec[lin.obs_rec[o0 + j] + (size_t)c * rs];
-    }
+  for (uint32_t i = i0; i < i1; ++i) {
+    __syncthreads();  // the previous entity is finished (and the row is zeroed, the list staged)
+    const int buf = (i - i0) & 1;
+    const uint32_t e = s_ent[buf][0], o = e >> 1, p = s_ent[buf][1], o0 = s_ent[buf][2], L = s_ent[buf][3];
+    const bool staged = L <= (uint32_t)kRowStage;
+    if (staged)
+      for (uint32_t k = tid; k < (uint32_t)kRec * L; k += blockDim.x) {
+        const uint32_t c = k / L, j = k - c * L;
+        jr[j * kRec + c] = (double)lin.rec[lin.obs_rec[o0 + j] + (size_t)c * rs];
+      }
     for (uint32_t t = tid; t < 2 * L; t += blockDim.x) {
       const uint32_t eid = 2 * (o0 + (t >> 1)) + (t & 1);
       const int Y = rt.ent_block[eid];
-      tslot[t] = Y >= 0 ? find_slot(rt.nbr, n0, n1, Y) : -1;
+      int sl = -1;
+      if (Y >= 0) sl = nbr_local ? find_slot(nbr_s, 0, n1 - n0, Y) : find_slot(rt.nbr, n0, n1, Y);
+      tslot[t] = sl;
       tcol[t] = rt.seg_col[eid];
     }
-    __syncthreads();
+    if (tid == 32 && i + 1 < i1) {  // the next entity's indices, fetched while this one is computed
+      const uint32_t en = rt.ent[i + 1], pn = rt.ent_point[i + 1];
+      const uint32_t a = rt.pt_off[pn], b = rt.pt_off[pn + 1];
+      s_ent[buf ^ 1][0] = en;
+      s_ent[buf ^ 1][1] = pn;
+      s_ent[buf ^ 1][2] = a;
+      s_ent[buf ^ 1][3] = b - a;
+    }
     const uint32_t jo = o - o0;
     if (tid == 0) {
       const double* vi = lin.vinv + 6 * (size_t)p;
       const double Vi[6] = {vi[0], vi[1], vi[2], vi[3], vi[4], vi[5]};
-      sym3_apply(Vi, jr + jo * kRec + kJp, G);
-      sym3_apply(Vi, jr + jo * kRec + kJp + 3, G + 3);
+      const R* ro = lin.rec + lin.obs_rec[o];
+      double jp[6];
+      for (int k = 0; k < 6; ++k) jp[k] = (double)ro[(size_t)(kJp + k) * rs];
+      sym3_apply(Vi, jp, G);
+      sym3_apply(Vi, jp + 3, G + 3);
       const int cX = rt.seg_col[e];
       for (int m = 0; m < 6; ++m) {
-        aX[m] = m < dX ? jr[jo * kRec + cX + m] : 0.0;
-        aX[6 + m] = m < dX ? jr[jo * kRec + 9 + cX + m] : 0.0;
+        aX[m] = m < dX ? (double)ro[(size_t)(cX + m) * rs] : 0.0;
+        aX[6 + m] = m < dX ? (double)ro[(size_t)(9 + cX + m) * rs] : 0.0;
       }
     }
     __syncthreads();
     for (uint32_t w = tid; w < 2 * L * 36; w += blockDim.x) {
       const uint32_t t = w / 36, mn = w - 36 * t, m = mn / 6, n = mn - 6 * m;
-      const int s = tslot[t];
-      if (s < 0 || (int)m >= dX) continue;
-      const int dY = rt.blk_dim[rt.nbr[n0 + s]];
+      const int sl = tslot[t];
+      if (sl < 0 || (int)m >= dX) continue;
+      const int dY = rt.blk_dim[nbr_local ? nbr_s[sl] : rt.nbr[n0 + sl]];
       if ((int)n >= dY) continue;
       bool leader = true;
-      for (uint32_t t2 = 0; t2 < t; ++t2) leader = leader && tslot[t2] != s;
+      for (uint32_t t2 = 0; t2 < t; ++t2) leader = leader && tslot[t2] != sl;
       if (!leader) continue;
       const double a0 = aX[m], a1 = aX[6 + m];
       double acc = 0.0;
       for (uint32_t t2 = t; t2 < 2 * L; ++t2) {
-        if (tslot[t2] != s) continue;
+        if (tslot[t2] != sl) continue;
         const uint32_t j = t2 >> 1;
-        const double* rj = jr + j * kRec;
-        double M00 = -(G[0] * rj[kJp] + G[1] * rj[kJp + 1] + G[2] * rj[kJp + 2]);
-        double M01 = -(G[0] * rj[kJp + 3] + G[1] * rj[kJp + 4] + G[2] * rj[kJp + 5]);
-        double M10 = -(G[3] * rj[kJp] + G[4] * rj[kJp + 1] + G[5] * rj[kJp + 2]);
-        double M11 = -(G[3] * rj[kJp + 3] + G[4] * rj[kJp + 4] + G[5] * rj[kJp + 5]);
+        const int cY = tcol[t2];
+        double q[6], b0, b1;
+        if (staged) {
+          const double* rj = jr + j * kRec;
+          for (int k = 0; k < 6; ++k) q[k] = rj[kJp + k];
+          b0 = rj[cY + n];
+          b1 = rj[9 + cY + n];
+        } else {
+          const R* rj = lin.rec + lin.obs_rec[o0 + j];
+          for (int k = 0; k < 6; ++k) q[k] = (double)rj[(size_t)(kJp + k) * rs];
+          b0 = (double)rj[(size_t)(cY + n) * rs];
+          b1 = (double)rj[(size_t)(9 + cY + n) * rs];
+        }
+        double M00 = -(G[0] * q[0] + G[1] * q[1] + G[2] * q[2]);
+        double M01 = -(G[0] * q[3] + G[1] * q[4] + G[2] * q[5]);
+        double M10 = -(G[3] * q[0] + G[4] * q[1] + G[5] * q[2]);
+        double M11 = -(G[3] * q[3] + G[4] * q[4] + G[5] * q[5]);
         if (j == jo) {
           M00 += 1.0;
           M11 += 1.0;
         }
-        const int cY = tcol[t2];
-        const double b0 = rj[cY + n], b1 = rj[9 + cY + n];
         acc += a0 * (M00 * b0 + M01 * b1) + a1 * (M10 * b0 + M11 * b1);
       }
-      rows[rt.slot_off[n0 + s] + m * dY + n] += acc;
+      rows[rt.slot_off[n0 + sl] + m * dY + n] += acc;
     }
   }
 }
@@ -225,6 +271,7 @@ constexpr int kCTT = kCT * kCT;
 struct TileBand {
   int n, nt, bwt;
   double* t;
+  double* w;  // nt tiles: the inverse of each diagonal tile of the factor (column-major)
 };
 __host__ __device__ __forceinline__ size_t tile_at(const TileBand& b, int i, int j) {
   return ((size_t)i * (b.bwt + 1) + (size_t)(i - j)) * kCTT;
@@ -261,8 +308,71 @@ __global__ void k_tiles_pad(TileBand tb) {
   tb.t[tile_at(tb, i, i) + (size_t)(r % kCT) * kCT + (r % kCT)] = 1.0;
 }
 
-// POTRF of diagonal tile k (right-looking inside the tile). status[0] = 0 when a pivot is not finite
-// and positive; later launches of the factorization then return at once.
+// Operands of the tile products are staged in shared memory with a padded row of kTS doubles (16-byte
+// aligned rows; transposed stores hit 8 banks per warp instead of one).
+constexpr int kTS = 66;
+constexpr size_t kStagedTile = sizeof(double) * kCT * kTS;
+
+// acc (4 x 4 per thread, 16 x 16 threads) += A B for 64 x 64 tiles staged as Ta[q * kTS + r] = A(r, q)
+// and Tb[q * kTS + c] = B(q, c); the sum over q runs in order.
+__device__ __forceinline__ void tile_mma_acc(const double* Ta, const double* Tb, double acc[4][4]) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll 4
+  for (int q = 0; q < kCT; ++q) {
+    const double2 a01 = *reinterpret_cast<const double2*>(Ta + q * kTS + 4 * ty);
+    const double2 a23 = *reinterpret_cast<const double2*>(Ta + q * kTS + 4 * ty + 2);
+    const double2 b01 = *reinterpret_cast<const double2*>(Tb + q * kTS + 4 * tx);
+    const double2 b23 = *reinterpret_cast<const double2*>(Tb + q * kTS + 4 * tx + 2);
+    const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+  }
+}
+
+// Stage the column-major tile g (element (r, c) at g[c * 64 + r]) as the operand M = g (flip false)
+// or g^T (flip true), in the A layout (T[q * kTS + r] = M(r, q)) or the B layout (T[q * kTS + c] =
+// M(q, c)). Global reads run along g's storage (coalesced).
+__device__ __forceinline__ void stage_tile(const double* __restrict__ g, double* T, bool as_b, bool flip) {
+  const bool direct = as_b == flip;  // A of g and B of g^T keep g's column-major order
+  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;  // g(r, c)
+    const double v = g[w];
+    if (direct)
+      T[c * kTS + r] = v;
+    else
+      T[r * kTS + c] = v;
+  }
+}
+
+__device__ __forceinline__ void zero_acc(double acc[4][4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+}
+
+// acc (output tile element (4 ty + a, 4 tx + b)) into a staged A operand: T[c * kTS + r] = scale acc(r, c)
+__device__ __forceinline__ void acc_to_a(const double acc[4][4], double scale, double* T) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) T[(4 * tx + b) * kTS + 4 * ty + a] = scale * acc[a][b];
+}
+
+__device__ __forceinline__ void acc_store(const double acc[4][4], double* g) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int a = 0; a < 4; ++a) g[(size_t)(4 * tx + b) * kCT + 4 * ty + a] = acc[a][b];
+}
+
+// POTRF of diagonal tile k (right-looking inside the tile) and the inverse W_k = L_kk^-1 of its factor
+// (column by column, forward substitution). status[0] = 0 when a pivot is not finite and positive;
+// later launches of the factorization then return at once.
 __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* status) {
   __shared__ double A[kCT * (kCT + 1)];
   __shared__ int fail;
@@ -303,88 +413,64 @@ __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* sta
     const int c = w / kCT, r = w - c * kCT;
     g[w] = r >= c ? A[c * (kCT + 1) + r] : 0.0;
   }
+  if (tid < kCT) {  // column c of W: L w = e_c, rows c..63
+    const int c = tid;
+    double* wc = tb.w + (size_t)k * kCTT + (size_t)c * kCT;
+    for (int r = 0; r < c; ++r) wc[r] = 0.0;
+    double x[kCT];
+    for (int r = c; r < kCT; ++r) {
+      double v = r == c ? 1.0 : 0.0;
+      for (int m = c; m < r; ++m) v -= A[m * (kCT + 1) + r] * x[m];
+      x[r] = v / A[r * (kCT + 1) + r];
+      wc[r] = x[r];
+    }
+  }
 }
 
-// TRSM: the tiles below diagonal tile k, L_ik = A_ik L_kk^-T (CTA per tile, thread per row). Dynamic
-// shared memory: two padded tiles (kTrsmSmem bytes).
-constexpr size_t kTrsmSmem = 2 * sizeof(double) * kCT * (kCT + 1);
-constexpr size_t kUpdateSmem = 2 * sizeof(double) * kCTT;
-__global__ void __launch_bounds__(kCT) k_tile_trsm(TileBand tb, int k, const int* status) {
+// TRSM as a product: the tiles below diagonal tile k, L_ik = A_ik W_k^T (CTA per tile). Dynamic shared
+// memory: two staged operands.
+constexpr size_t kTrsmSmem = 2 * kStagedTile;
+__global__ void __launch_bounds__(256) k_tile_trsm(TileBand tb, int k, const int* status) {
   extern __shared__ double shm[];
-  double* Lk = shm;
-  double* B = shm + kCT * (kCT + 1);
   if (status[0] == 0) return;
-  const int i = k + 1 + blockIdx.x, tid = threadIdx.x;
-  const double* lk = tb.t + tile_at(tb, k, k);
+  double* Ta = shm;
+  double* Tb = shm + kCT * kTS;
+  const int i = k + 1 + blockIdx.x;
   double* bi = tb.t + tile_at(tb, i, k);
-  for (int w = tid; w < kCTT; w += blockDim.x) {
-    const int c = w / kCT, r = w - c * kCT;
-    Lk[c * (kCT + 1) + r] = lk[w];
-    B[c * (kCT + 1) + r] = bi[w];
-  }
+  stage_tile(bi, Ta, false, false);                       // A_ik
+  stage_tile(tb.w + (size_t)k * kCTT, Tb, true, true);    // W_k^T
   __syncthreads();
-  const int r = tid;  // X[r][c] = (B[r][c] - sum_{m<c} X[r][m] Lk[c][m]) / Lk[c][c]
-  for (int c = 0; c < kCT; ++c) {
-    double v = B[c * (kCT + 1) + r];
-    for (int m = 0; m < c; ++m) v -= B[m * (kCT + 1) + r] * Lk[m * (kCT + 1) + c];
-    B[c * (kCT + 1) + r] = v / Lk[c * (kCT + 1) + c];
-  }
-  __syncthreads();
-  for (int w = tid; w < kCTT; w += blockDim.x) {
-    const int c = w / kCT, rr = w - c * kCT;
-    bi[w] = B[c * (kCT + 1) + rr];
-  }
+  double acc[4][4];
+  zero_acc(acc);
+  tile_mma_acc(Ta, Tb, acc);
+  acc_store(acc, bi);
 }
 
 // Trailing update of step k: A_ij -= L_ik L_jk^T for k < j <= i <= min(k + bwt, nt - 1), one CTA per
 // tile, 16 x 16 threads with 4 x 4 outputs each; the sum over the tile's 64 columns runs in order.
-// Dynamic shared memory: two tiles (64 KB).
+constexpr size_t kUpdateSmem = 2 * kStagedTile;
 __global__ void __launch_bounds__(256) k_tile_update(TileBand tb, int k, const int* status) {
   extern __shared__ double sh[];
   if (status[0] == 0) return;
-  double* Ti = sh;         // L_ik column-major: Ti[q * 64 + r] = L_ik[r][q]
-  double* Tj = sh + kCTT;  // L_jk column-major
+  double* Ta = sh;
+  double* Tb = sh + kCT * kTS;
   int idx = blockIdx.x;
   int ii = 0;
   while ((ii + 1) * (ii + 2) / 2 <= idx) ++ii;
   const int jj = idx - ii * (ii + 1) / 2;
   const int i = k + 1 + ii, j = k + 1 + jj;
-  const int tid = threadIdx.x;
-  const double2* li = reinterpret_cast<const double2*>(tb.t + tile_at(tb, i, k));
-  const double2* lj = reinterpret_cast<const double2*>(tb.t + tile_at(tb, j, k));
-  for (int w = tid; w < kCTT / 2; w += blockDim.x) {
-    reinterpret_cast<double2*>(Ti)[w] = li[w];
-    reinterpret_cast<double2*>(Tj)[w] = lj[w];
-  }
+  stage_tile(tb.t + tile_at(tb, i, k), Ta, false, false);  // L_ik
+  stage_tile(tb.t + tile_at(tb, j, k), Tb, true, true);    // L_jk^T
   __syncthreads();
-  const int ty = tid >> 4, tx = tid & 15;
   double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-#pragma unroll 4
-  for (int q = 0; q < kCT; ++q) {
-    const double2 a01 = *reinterpret_cast<const double2*>(Ti + q * kCT + 4 * ty);
-    const double2 a23 = *reinterpret_cast<const double2*>(Ti + q * kCT + 4 * ty + 2);
-    const double2 b01 = *reinterpret_cast<const double2*>(Tj + q * kCT + 4 * tx);
-    const double2 b23 = *reinterpret_cast<const double2*>(Tj + q * kCT + 4 * tx + 2);
-    const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
-  }
+  zero_acc(acc);
+  tile_mma_acc(Ta, Tb, acc);
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
   double* cij = tb.t + tile_at(tb, i, j);
 #pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    const int c = 4 * tx + b;
+  for (int b = 0; b < 4; ++b)
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int r = 4 * ty + a;
-      cij[(size_t)c * kCT + r] -= acc[a][b];
-    }
-  }
+    for (int a = 0; a < 4; ++a) cij[(size_t)(4 * tx + b) * kCT + 4 * ty + a] -= acc[a][b];
 }
 
 // Forward (L y = b) and backward (L^T x = y) substitution with the banded tiled factor, one CTA of
@@ -491,54 +577,18 @@ __global__ void k_perm_scatter(int n, const int* __restrict__ perm_to_orig, cons
 // group is the block of Z at its parameters' positions (sparse/covariance.rs:564-587 gets the same
 // block by solving S x = e_p column by column).
 //
-// acc (4 x 4 per thread, 16 x 16 threads) += A B for 64 x 64 tiles staged in shared memory as
-// Ta[q * 64 + r] = A[r][q] and Tb[q * 64 + c] = B[q][c]; the sum over q runs in order.
-__device__ __forceinline__ void tile_mma_acc(const double* Ta, const double* Tb, double acc[4][4]) {
-  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-#pragma unroll 4
-  for (int q = 0; q < kCT; ++q) {
-    const double2 a01 = *reinterpret_cast<const double2*>(Ta + q * kCT + 4 * ty);
-    const double2 a23 = *reinterpret_cast<const double2*>(Ta + q * kCT + 4 * ty + 2);
-    const double2 b01 = *reinterpret_cast<const double2*>(Tb + q * kCT + 4 * tx);
-    const double2 b23 = *reinterpret_cast<const double2*>(Tb + q * kCT + 4 * tx + 2);
-    const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
-  }
-}
-
-// Stage the column-major tile g (element (r, c) at g[c * 64 + r]) as an operand: transpose == false
-// gives T[q * 64 + r] = g(r, q) (the tile as A) and T[q * 64 + c] = g(q, c) with transpose == true
-// (the tile as B); `flip` uses the transposed tile g^T instead of g.
-__device__ __forceinline__ void stage_tile(const double* __restrict__ g, double* T, bool as_b, bool flip) {
-  // as A: T[q*64 + r] = M(r, q); as B: T[q*64 + c] = M(q, c); M = g or g^T
-  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {
-    const int hi = w / kCT, lo = w - hi * kCT;  // T index = hi * 64 + lo
-    // as A: (r, q) = (lo, hi); as B: (q, c) = (hi, lo)
-    const int row = as_b ? hi : lo, col = as_b ? lo : hi;  // element of M
-    const int gr = flip ? col : row, gc = flip ? row : col;  // element of g
-    T[w] = g[(size_t)gc * kCT + gr];
-  }
-}
-
-// Off-diagonal tiles of Z in column j: CTA per i in (j, min(j + bwt, nt - 1)]. Dynamic shared
-// memory: kTakahashiSmem (two staged operands and the accumulated tile).
-constexpr size_t kTakahashiSmem = 3 * sizeof(double) * kCTT;
+// Off-diagonal tiles of Z in column j: CTA per i in (j, min(j + bwt, nt - 1)]: acc = sum_k Z_ik L_kj,
+// then Z_ij = -acc W_j. Dynamic shared memory: kTakahashiSmem (two staged operands).
+constexpr size_t kTakahashiSmem = 2 * kStagedTile;
 __global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand Z, int j, const int* status) {
   extern __shared__ double sh[];
   if (status[0] == 0) return;
   double* Ta = sh;
-  double* Tb = sh + kCTT;
-  double* X = sh + 2 * kCTT;  // column-major accumulated tile
-  const int i = j + 1 + blockIdx.x, tid = threadIdx.x;
+  double* Tb = sh + kCT * kTS;
+  const int i = j + 1 + blockIdx.x;
   const int kmax = min(L.nt - 1, j + L.bwt);
   double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  zero_acc(acc);
   for (int k = j + 1; k <= kmax; ++k) {
     __syncthreads();
     if (i >= k)
@@ -550,43 +600,24 @@ __global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand 
     tile_mma_acc(Ta, Tb, acc);
   }
   __syncthreads();
-  {
-    const int ty = tid >> 4, tx = tid & 15;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) X[(4 * tx + b) * kCT + 4 * ty + a] = -acc[a][b];
-  }
-  // L_jj (column-major) into Ta
-  for (int w = tid; w < kCTT; w += blockDim.x) Ta[w] = L.t[tile_at(L, j, j) + w];
+  acc_to_a(acc, -1.0, Ta);
+  stage_tile(L.w + (size_t)j * kCTT, Tb, true, false);  // W_j
   __syncthreads();
-  if (tid < kCT) {  // row r of X: x L_jj = a, solved from the last column back
-    const int r = tid;
-    for (int c = kCT - 1; c >= 0; --c) {
-      double v = X[c * kCT + r];
-      for (int m = c + 1; m < kCT; ++m) v -= X[m * kCT + r] * Ta[c * kCT + m];
-      X[c * kCT + r] = v / Ta[c * kCT + c];
-    }
-  }
-  __syncthreads();
-  double* zij = Z.t + tile_at(Z, i, j);
-  for (int w = tid; w < kCTT; w += blockDim.x) zij[w] = X[w];
+  zero_acc(acc);
+  tile_mma_acc(Ta, Tb, acc);
+  acc_store(acc, Z.t + tile_at(Z, i, j));
 }
 
-// Diagonal tile of Z in column j (after its off-diagonal tiles): one CTA.
+// Diagonal tile of Z in column j (after its off-diagonal tiles): acc = sum_k Z_kj^T L_kj, then
+// Z_jj = (W_j^T - acc) W_j. One CTA.
 __global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, int j, const int* status) {
   extern __shared__ double sh[];
   if (status[0] == 0) return;
   double* Ta = sh;
-  double* Tb = sh + kCTT;
-  double* X = sh + 2 * kCTT;
-  const int tid = threadIdx.x;
+  double* Tb = sh + kCT * kTS;
   const int kmax = min(L.nt - 1, j + L.bwt);
   double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  zero_acc(acc);
   for (int k = j + 1; k <= kmax; ++k) {
     __syncthreads();
     stage_tile(Z.t + tile_at(Z, k, j), Ta, false, true);  // Z_kj^T
@@ -595,43 +626,18 @@ __global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, 
     tile_mma_acc(Ta, Tb, acc);
   }
   __syncthreads();
-  {
-    const int ty = tid >> 4, tx = tid & 15;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) X[(4 * tx + b) * kCT + 4 * ty + a] = -acc[a][b];
-  }
-  // W = L_jj^-1 (lower, column-major) into Tb, column by column; L_jj into Ta
-  for (int w = tid; w < kCTT; w += blockDim.x) Ta[w] = L.t[tile_at(L, j, j) + w];
+  acc_to_a(acc, -1.0, Ta);  // -acc
+  const double* wj = L.w + (size_t)j * kCTT;
   __syncthreads();
-  if (tid < kCT) {
-    const int c = tid;  // column c of W: L w = e_c
-    for (int r = 0; r < kCT; ++r) {
-      double v = r == c ? 1.0 : 0.0;
-      for (int m = c; m < r; ++m) v -= Ta[m * kCT + r] * Tb[c * kCT + m];
-      Tb[c * kCT + r] = r < c ? 0.0 : v / Ta[r * kCT + r];
-    }
+  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {  // + W_j^T: A(r, q) += W(q, r)
+    const int c = w / kCT, r = w - c * kCT;                // W(r, c) at wj[w]
+    Ta[r * kTS + c] += wj[w];                              // A element (c, r) of the operand
   }
+  stage_tile(wj, Tb, true, false);  // W_j
   __syncthreads();
-  // X = (W^T - acc) W, where X currently holds -acc
-  for (int w = tid; w < kCTT; w += blockDim.x) {
-    const int c = w / kCT, r = w - c * kCT;
-    X[w] += Tb[r * kCT + c];  // + W^T(r, c) = W(c, r)
-  }
-  __syncthreads();
-  double out[16];
-  int n_out = 0;
-  for (int w = tid; w < kCTT; w += blockDim.x) {
-    const int c = w / kCT, r = w - c * kCT;
-    double v = 0.0;
-    for (int m = c; m < kCT; ++m) v += X[m * kCT + r] * Tb[c * kCT + m];
-    out[n_out++] = v;
-  }
-  __syncthreads();
-  double* zjj = Z.t + tile_at(Z, j, j);
-  n_out = 0;
-  for (int w = tid; w < kCTT; w += blockDim.x) zjj[w] = out[n_out++];
+  zero_acc(acc);
+  tile_mma_acc(Ta, Tb, acc);
+  acc_store(acc, Z.t + tile_at(Z, j, j));
 }
 
 // (S^-1)_gg of each free group from Z: 9 values per group (row-major), thread per group.

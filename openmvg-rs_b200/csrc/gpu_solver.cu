@@ -1,8 +1,9 @@
 // gpu_solver.cu — B200 (sm_100a) Levenberg–Marquardt bundle adjustment.
 //
 // Hot path (reference paths relative to the openmvg-rs root):
-//   K1  k_linearize ........ per-observation projection, robust weight, analytic point / camera
-//                            Jacobians and the per-point 3x3 Gram + FP64 damped inverse
+//   K1  k_linearize_tiles .. per-observation projection, robust weight, analytic point / camera
+//                            Jacobians (one CTA per tile of whole points) and the per-point 3x3
+//                            Gram + FP64 damped inverse
 //                            (schur/point.rs:176-448, schur/assembly.rs:893-1040, point_block.rs:78-184)
 //   K2  k_block_chunks ..... camera-side deterministic segmented reductions: U blocks, g, reduced g,
 //                            damping diagonal, pose/intrinsic edges, diagonal point coupling
@@ -455,86 +456,12 @@ __device__ __forceinline__ void pose_jacobian(const double J[2][3], const double
     for (int c = 0; c < 6; ++c) out[r][c] = J[r][0] * m[0][c] + J[r][1] * m[1][c] + J[r][2] * m[2][c];
 }
 
+// The point part of the linearization (schur/assembly.rs:893-1040, point_block.rs:78-184): the
+// summary, g_p, the scaled gradient norm, the damped factor and its inverse, the damping diagonal,
+// the rcond at lambda = 0 and Vhat^-1 g_p.
 template <typename T>
-__global__ void __launch_bounds__(128) k_linearize(DevView v, DevState s, Gauge g, LossDev loss, double lambda,
-                                                   LinOut<T> out) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= v.P) return;
-  const double X0 = s.points[3 * p], X1 = s.points[3 * p + 1], X2 = s.points[3 * p + 2];
-  double V[6] = {0, 0, 0, 0, 0, 0}, gp[3] = {0, 0, 0};
-  double cost = 0.0, sq = 0.0;
-  bool ok = true;
-  uint32_t o0 = v.pt_off[p], o1 = v.pt_off[p + 1];
-  for (uint32_t o = o0; o < o1; ++o) {
-    int cam = v.obs_cam[o];
-    const double* P = s.pose + 12 * cam;
-    double rot[3] = {P[0] * X0 + P[1] * X1 + P[2] * X2, P[3] * X0 + P[4] * X1 + P[5] * X2,
-                     P[6] * X0 + P[7] * X1 + P[8] * X2};
-    double xc[3] = {rot[0] + P[9], rot[1] + P[10], rot[2] + P[11]};
-    double r[2], J[2][3], Ji[2][3];
-    if (!project_obs(v, s.groups, o, xc, r, J, Ji)) {
-      ok = false;
-      for (int k = 0; k < kRec; ++k) out.rec[out.obs_rec[o] + (size_t)k * out.rs] = T(0);
-      if (out.rec32)
-        for (int k = 0; k < kRec; ++k) out.rec32[out.obs_rec32[o] + (size_t)k * out.rs32] = 0.0f;
-      out.rw[2 * o] = 0.0;
-      out.rw[2 * o + 1] = 0.0;
-      continue;
-    }
-    double rn = sqrt(r[0] * r[0] + r[1] * r[1]);
-    double sw = loss.sqrt_weight(rn);
-    cost += loss.cost(rn);
-    sq += rn * rn;
-    double jp[2][3];
-    for (int a = 0; a < 2; ++a)
-      for (int c = 0; c < 3; ++c) jp[a][c] = (J[a][0] * P[c] + J[a][1] * P[3 + c] + J[a][2] * P[6 + c]) * g.scene;
-    for (int a = 0; a < 2; ++a) {
-      double wr = sw * r[a];
-      double w0 = sw * jp[a][0], w1 = sw * jp[a][1], w2 = sw * jp[a][2];
-      gp[0] += w0 * wr;
-      gp[1] += w1 * wr;
-      gp[2] += w2 * wr;
-      V[0] += w0 * w0;
-      V[1] += w1 * w0;
-      V[2] += w1 * w1;
-      V[3] += w2 * w0;
-      V[4] += w2 * w1;
-      V[5] += w2 * w2;
-    }
-    double jc[2][9];
-    for (int a = 0; a < 2; ++a)
-      for (int k = 0; k < 9; ++k) jc[a][k] = 0.0;
-    int pd = v.pose_dim[cam];
-    if (pd > 0) {
-      double pj[2][6];
-      pose_jacobian(J, rot, cam, g, pj);
-      for (int a = 0; a < 2; ++a)
-        for (int k = 0; k < pd; ++k) jc[a][k] = pj[a][k];
-    }
-    if (v.self_cal) {
-      int id = v.intr_dim[v.cam_group[cam]];
-      for (int a = 0; a < 2; ++a)
-        for (int k = 0; k < id; ++k) jc[a][pd + k] = Ji[a][k];
-    }
-    T* jco = out.rec + out.obs_rec[o];
-    const int rs = out.rs;
-    for (int a = 0; a < 2; ++a)
-      for (int k = 0; k < 9; ++k) jco[(9 * a + k) * rs] = T(sw * jc[a][k]);
-    T* jpo = jco + kJp * rs;
-    for (int a = 0; a < 2; ++a)
-      for (int c = 0; c < 3; ++c) jpo[(3 * a + c) * rs] = T(sw * jp[a][c]);
-    if (out.rec32) {
-      float* j32 = out.rec32 + out.obs_rec32[o];
-      const int r32 = out.rs32;
-      for (int a = 0; a < 2; ++a)
-        for (int k = 0; k < 9; ++k) j32[(9 * a + k) * r32] = (float)(sw * jc[a][k]);
-      for (int a = 0; a < 2; ++a)
-        for (int c = 0; c < 3; ++c) j32[(kJp + 3 * a + c) * r32] = (float)(sw * jp[a][c]);
-    }
-    out.rw[2 * o] = sw * r[0];
-    out.rw[2 * o + 1] = sw * r[1];
-    if (out.sw) out.sw[o] = sw;
-  }
+__device__ __forceinline__ void point_epilogue(const DevView& v, uint32_t p, const double V[6], const double gp[3],
+                                               double cost, double sq, bool ok, double lambda, LinOut<T>& out) {
   PointSummary sm{0, 0, 0, 0, 1.0, 0, 0, 0};
   double* vi = out.vinv + 6 * (size_t)p;
   double* ig = out.ig + 3 * (size_t)p;
@@ -1047,6 +974,128 @@ __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const
 #include "mv_tiles.cuh"
 #include "explicit_s.cuh"
 namespace omvgba {
+
+// ----------------------------------------------------------------------------------------------
+// K1: the linearization (schur/point.rs:176-448) with one CTA per matvec tile of whole points and
+// one thread per observation: project, robust weight, analytic point and camera Jacobians, each
+// record component written by a warp as one coalesced line. The per-point sums (V, g_p, cost,
+// squared residual) are formed by one thread per point from the observations' row contributions
+// staged in shared memory, in track order and row 0 before row 1 (the reference's accumulation
+// order, schur/point.rs:388-390), followed by the point epilogue.
+// ----------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(mv_tile_obs<T>(), sizeof(T) == 4 ? 3 : 6) k_linearize_tiles(DevView v, DevState s, Gauge g, LossDev loss,
+                                                                      double lambda, LinOut<T> out, MvTiles mt) {
+  constexpr int TILE = mv_tile_obs<T>();
+  __shared__ double contrib[TILE][2][9];  // per observation and Jacobian row: V (6), g_p (3)
+  __shared__ double cs[TILE][2];          // cost, squared residual norm
+  __shared__ unsigned char okf[TILE];
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const uint4 hdr = mt.tile_hdr[t];
+  const uint32_t nobs = hdr.x, npt = hdr.y, p0 = hdr.w;
+  const unsigned char* slot = mt.slots + (size_t)t * MvSlot::bytes(TILE);
+  const uint16_t* poff = reinterpret_cast<const uint16_t*>(slot + MvSlot::poff(TILE));
+  const uint16_t* lpt = reinterpret_cast<const uint16_t*>(slot + MvSlot::lpt(TILE));
+  const uint32_t o0 = v.pt_off[p0];
+  T* rec = out.rec + (size_t)t * TILE * kRec + tid;
+  if ((uint32_t)tid < nobs) {
+    const uint32_t o = o0 + tid;
+    const uint32_t p = p0 + lpt[tid];
+    const double X0 = s.points[3 * (size_t)p], X1 = s.points[3 * (size_t)p + 1], X2 = s.points[3 * (size_t)p + 2];
+    const int cam = v.obs_cam[o];
+    const double* P = s.pose + 12 * cam;
+    double rot[3] = {P[0] * X0 + P[1] * X1 + P[2] * X2, P[3] * X0 + P[4] * X1 + P[5] * X2,
+                     P[6] * X0 + P[7] * X1 + P[8] * X2};
+    double xc[3] = {rot[0] + P[9], rot[1] + P[10], rot[2] + P[11]};
+    double r[2], J[2][3], Ji[2][3];
+    if (!project_obs(v, s.groups, o, xc, r, J, Ji)) {
+      okf[tid] = 0;
+#pragma unroll
+      for (int k = 0; k < kRec; ++k) rec[k * TILE] = T(0);
+      out.rw[2 * (size_t)o] = 0.0;
+      out.rw[2 * (size_t)o + 1] = 0.0;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) contrib[tid][a][k] = 0.0;
+      cs[tid][0] = cs[tid][1] = 0.0;
+    } else {
+      okf[tid] = 1;
+      const double rn = sqrt(r[0] * r[0] + r[1] * r[1]);
+      const double sw = loss.sqrt_weight(rn);
+      cs[tid][0] = loss.cost(rn);
+      cs[tid][1] = rn * rn;
+      double jp[2][3];
+      for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < 3; ++c) jp[a][c] = (J[a][0] * P[c] + J[a][1] * P[3 + c] + J[a][2] * P[6 + c]) * g.scene;
+      for (int a = 0; a < 2; ++a) {
+        const double wr = sw * r[a];
+        const double w0 = sw * jp[a][0], w1 = sw * jp[a][1], w2 = sw * jp[a][2];
+        contrib[tid][a][0] = w0 * w0;
+        contrib[tid][a][1] = w1 * w0;
+        contrib[tid][a][2] = w1 * w1;
+        contrib[tid][a][3] = w2 * w0;
+        contrib[tid][a][4] = w2 * w1;
+        contrib[tid][a][5] = w2 * w2;
+        contrib[tid][a][6] = w0 * wr;
+        contrib[tid][a][7] = w1 * wr;
+        contrib[tid][a][8] = w2 * wr;
+      }
+      double jc[2][9];
+      for (int a = 0; a < 2; ++a)
+        for (int k = 0; k < 9; ++k) jc[a][k] = 0.0;
+      const int pd = v.pose_dim[cam];
+      if (pd > 0) {
+        double pj[2][6];
+        pose_jacobian(J, rot, cam, g, pj);
+        for (int a = 0; a < 2; ++a)
+          for (int k = 0; k < pd; ++k) jc[a][k] = pj[a][k];
+      }
+      if (v.self_cal) {
+        const int id = v.intr_dim[v.cam_group[cam]];
+        for (int a = 0; a < 2; ++a)
+          for (int k = 0; k < id; ++k) jc[a][pd + k] = Ji[a][k];
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) rec[(9 * a + k) * TILE] = T(sw * jc[a][k]);
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rec[(kJp + 3 * a + c) * TILE] = T(sw * jp[a][c]);
+      out.rw[2 * (size_t)o] = sw * r[0];
+      out.rw[2 * (size_t)o + 1] = sw * r[1];
+      if (out.sw) out.sw[o] = sw;
+    }
+  }
+  __syncthreads();
+  if ((uint32_t)tid >= npt) return;
+  const uint32_t p = p0 + tid;
+  double V[6] = {0, 0, 0, 0, 0, 0}, gp[3] = {0, 0, 0};
+  double cost = 0.0, sq = 0.0;
+  bool ok = true;
+  for (uint32_t i = poff[tid]; i < poff[tid + 1]; ++i) {
+    if (!okf[i]) {
+      ok = false;
+      continue;
+    }
+    cost += cs[i][0];
+    sq += cs[i][1];
+    for (int a = 0; a < 2; ++a) {
+      gp[0] += contrib[i][a][6];
+      gp[1] += contrib[i][a][7];
+      gp[2] += contrib[i][a][8];
+      V[0] += contrib[i][a][0];
+      V[1] += contrib[i][a][1];
+      V[2] += contrib[i][a][2];
+      V[3] += contrib[i][a][3];
+      V[4] += contrib[i][a][4];
+      V[5] += contrib[i][a][5];
+    }
+  }
+  point_epilogue(v, p, V, gp, cost, sq, ok, lambda, out);
+}
 
 // ----------------------------------------------------------------------------------------------
 // Block-Jacobi preconditioner (FP64): P_b = U_bb + lambda D_b - C_b - cross pairs
@@ -2143,7 +2192,7 @@ struct Solver {
   DBuf<uint32_t> d_blk_ent, d_nbr_begin;
   DBuf<int> d_ent_block, d_nbr, d_nbr_row, d_perm_off, d_perm_to_orig;
   DBuf<uint64_t> d_slot_off;
-  DBuf<double> d_rows, d_tiles, d_ztiles, d_perm_vec, d_marg_out, d_power;
+  DBuf<double> d_rows, d_tiles, d_winv, d_ztiles, d_perm_vec, d_marg_out, d_power;
   bool rows_valid = false;  // the rows hold S of the current assembly
   // PCG vectors
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
@@ -2195,7 +2244,7 @@ struct Solver {
     // the workspace: everything uploaded and allocated for the solve, and the banded factor of the
     // certificate (twice for self-calibration: the selected inverse has the factor's shape)
     workspace_bytes = (tl_device_bytes - bytes_before) +
-                      sizeof(double) * (uint64_t)S.nt * (uint64_t)(S.bwt + 1) * kCTT * (n.self_cal ? 2 : 1);
+                      sizeof(double) * (uint64_t)S.nt * kCTT * ((uint64_t)(S.bwt + 1) * (n.self_cal ? 2 : 1) + 1);
     if (opt.workspace_budget && workspace_bytes > opt.workspace_budget)
       throw SolveFailure{3, "GPU workspace " + std::to_string(workspace_bytes) + " bytes exceeds the workspace budget " +
                                 std::to_string(opt.workspace_budget)};
@@ -2281,7 +2330,7 @@ struct Solver {
     r.entries = (uint32_t)S.nbr.size();
     return r;
   }
-  TileBand tile_band() const { return TileBand{D, S.nt, S.bwt, d_tiles.p}; }
+  TileBand tile_band() const { return TileBand{D, S.nt, S.bwt, d_tiles.p, d_winv.p}; }
 
   void upload() {
     std::vector<uint32_t> pt_off(n.pt_off.begin(), n.pt_off.end());
@@ -2468,10 +2517,18 @@ struct Solver {
   // Full linearization + camera-side reductions at the given damping.
   Assembly assemble(int which, const Gauge& g, const LossDev& loss, double lambda, bool build_rows) {
     DevView v = view();
-    if (mixed)
-      OMVGBA_LAUNCH(k_linearize<float>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin32());
-    else
-      OMVGBA_LAUNCH(k_linearize<T>, grid_for(P, 128), 128, 0, st, v, state(which), g, loss, lambda, lin());
+    {
+      const TileSetDev& ts = mixed ? dT32 : dT64;
+      const MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
+      if (mt.ntiles > 0) {
+        if (mixed)
+          OMVGBA_LAUNCH(k_linearize_tiles<float>, mt.ntiles, mv_tile_obs<float>(), 0, st, v, state(which), g, loss,
+                        lambda, lin32(), mt);
+        else
+          OMVGBA_LAUNCH(k_linearize_tiles<T>, mt.ntiles, mv_tile_obs<T>(), 0, st, v, state(which), g, loss, lambda,
+                        lin(), mt);
+      }
+    }
     check_launch();
     OMVGBA_LAUNCH(k_reduce_summary, red_blocks, kReduceThreads, 0, st, d_summary.p, P, d_summary_part.p);
     OMVGBA_LAUNCH(k_reduce_summary, 1, kReduceThreads, 0, st, d_summary_part.p, red_blocks, d_summary_part.p);
@@ -2551,7 +2608,7 @@ struct Solver {
 
   // S of the current linearization (no damping) by block rows, from the FP64 or FP32 records.
   void build_rows() {
-    const size_t smem = (size_t)S.max_track * kRec * sizeof(double) + 4 * (size_t)S.max_track * sizeof(int);
+    const size_t smem = 4 * (size_t)std::max(S.max_track, 1) * sizeof(int);
     if (smem > 48 * 1024) {
       CUDA_OK(cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       CUDA_OK(cudaFuncSetAttribute(k_block_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -2588,6 +2645,7 @@ struct Solver {
     if (sizeof(double) * count > kMaxTileBytes)
       throw SolveFailure{3, "the banded factor of the reduced camera system exceeds 16 GiB"};
     if (d_tiles.n != count) d_tiles.alloc(count, st);
+    if (d_winv.n != (size_t)S.nt * kCTT) d_winv.alloc((size_t)S.nt * kCTT, st);
     // per device and cheap: set on every factorization
     CUDA_OK(cudaFuncSetAttribute(k_tile_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
     CUDA_OK(cudaFuncSetAttribute(k_tile_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
@@ -2601,7 +2659,7 @@ struct Solver {
       OMVGBA_LAUNCH(k_tile_potrf, 1, 256, 0, st, tb, k, d_status.p);
       const int m = std::min(S.bwt, S.nt - 1 - k);
       if (m > 0) {
-        OMVGBA_LAUNCH(k_tile_trsm, m, kCT, kTrsmSmem, st, tb, k, d_status.p);
+        OMVGBA_LAUNCH(k_tile_trsm, m, 256, kTrsmSmem, st, tb, k, d_status.p);
         OMVGBA_LAUNCH(k_tile_update, m * (m + 1) / 2, 256, kUpdateSmem, st, tb, k, d_status.p);
       }
     }
@@ -2677,7 +2735,7 @@ struct Solver {
     CUDA_OK(cudaFuncSetAttribute(k_takahashi_offdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
     CUDA_OK(cudaFuncSetAttribute(k_takahashi_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
     const TileBand tl = tile_band();
-    const TileBand tz{D, S.nt, S.bwt, d_ztiles.p};
+    const TileBand tz{D, S.nt, S.bwt, d_ztiles.p, nullptr};
     for (int j = S.nt - 1; j >= 0; --j) {
       const int m = std::min(S.bwt, S.nt - 1 - j);
       if (m > 0) OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, d_status.p);
@@ -3487,7 +3545,10 @@ void gpu_debug_linearize(Context* ctx, const NativeProblem& problem, const LmOpt
   d_sw.alloc(std::max<size_t>(N, 1), s.st);
   LinOut<double> lo = s.lin();
   lo.sw = d_sw.p;
-  OMVGBA_LAUNCH(k_linearize<double>, grid_for(s.P, 128), 128, 0, s.st, s.view(), s.state(s.cur), g, options.loss, 0.0, lo);
+  const MvTiles mt = s.dT64.view(s.d_blk_dim.p, s.d_blk_off.p, s.nb);
+  if (mt.ntiles > 0)
+    OMVGBA_LAUNCH(k_linearize_tiles<double>, mt.ntiles, mv_tile_obs<double>(), 0, s.st, s.view(), s.state(s.cur), g,
+                  options.loss, 0.0, lo, mt);
   s.check_launch();
   std::vector<double> rec(s.d_rec.n), rw(2 * N), sw(N);
   CUDA_OK(copy_async(rec.data(), s.d_rec.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.st));

@@ -536,6 +536,17 @@ def run_ours(args) -> int:
     # value: mixed precision, problem resident in device memory
     plan = adjuster.plan(problem, mixed_cfg)
     info = plan.info()
+    if args.legs == "kernel":  # the product kernel's timing alone, no solve (for a small ncu capture)
+        roofline = kernel_roofline(plan, info, stream, flush, args.workload, launches=max(args.steps, 3))
+        plan.close()
+        adjuster.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "legs": "kernel", "n_gpus": world, "roofline": roofline,
+                              "observations": int(info["observation_count"])}), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
     for _ in range(args.warmup):
         plan.solve()
     torch.cuda.synchronize()
@@ -658,9 +669,9 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--max-iterations", type=int, default=MAX_ITERATIONS, help="LM iteration budget of every solve")
-    ap.add_argument("--legs", choices=["all", "gpu", "value"], default="all",
+    ap.add_argument("--legs", choices=["all", "gpu", "value", "kernel"], default="all",
                     help="gpu: every leg but the CPU baseline; value: only the resident mixed solve and the kernel "
-                         "timing (for profiler runs)")
+                         "timing (for profiler runs); kernel: only the product kernel's timing, no solve")
     ap.add_argument("--no-second-leg", dest="second_leg", action="store_false",
                     help="skip the 500-camera mixed/FP64 leg of the headline line")
     args = ap.parse_args(argv)

@@ -392,6 +392,88 @@ int32_t omvgba_residual_vjp_f32_static(void* stream, uint64_t observation_count,
 int32_t omvgba_solve_batched(omvgba_context* context, uint64_t window_count, const omvgba_problem* windows,
                              const omvgba_config* config, omvgba_solution* solutions, omvgba_error* error);
 
+/*
+ * Observability probe of a translation-and-structure problem with fixed rotations
+ * (probe_fixed_rotation_observability, kernel/fixed_rotation/observability.rs:24-262; the problem,
+ * options and outcome of kernel/fixed_rotation/api.rs). A capped subset of tracks (shortest first,
+ * covering every free camera) is linearized, each point is eliminated in square-root form, and the
+ * camera system, scaled to unit diagonal and shifted by minimum_normalized_eigenvalue, must factor:
+ * FULL_RANK_CERTIFIED certifies the whole problem; any other status is not evidence of deficiency.
+ * Track selection and the per-point elimination run on the host (bounded by the options: at most
+ * max_observations observations); the factorization runs on the context's device.
+ */
+typedef struct omvgba_fixed_rotation_problem {
+  uint64_t camera_count;               /* >= 2 */
+  const double* rotations;             /* camera_count x 9, world-to-camera, row-major */
+  const double* centers;               /* camera_count x 3 */
+  const double* intrinsics;            /* camera_count x 9: fx, fy, cx, cy, k1, k2, k3, p1, p2 */
+  const uint8_t* fixed_cameras;        /* camera_count */
+  uint64_t point_count;                /* >= 1 */
+  const double* points;                /* point_count x 3 */
+  const uint64_t* track_offsets;       /* point_count + 1: each point's observations */
+  const uint32_t* observation_camera;  /* track_offsets[point_count] */
+  const double* observation_pixel;     /* track_offsets[point_count] x 2 */
+  int32_t gauge_kind;                  /* omvgba_gauge_kind: Free or FixedBaseline */
+  uint64_t anchor, scale_camera;
+  double distance;                     /* FixedBaseline: the baseline length */
+  int32_t loss_kind;                   /* omvgba_loss_kind; the weights are relative to the loss at 0 */
+  double loss_scale;                   /* Huber delta / Cauchy scale of the numerics loss */
+} omvgba_fixed_rotation_problem;
+
+typedef struct omvgba_probe_options {  /* FixedRotationObservabilityProbeOptions (api.rs) */
+  uint64_t max_tracks, max_observations, max_observations_per_track, max_coverage_observations_per_track;
+  uint64_t max_reduced_nonzeros, max_factor_nonzeros, max_symbolic_dense_nonzeros;
+  double minimum_normalized_eigenvalue;
+} omvgba_probe_options;
+
+enum omvgba_probe_status {
+  OMVGBA_PROBE_FULL_RANK_CERTIFIED = 0,
+  OMVGBA_PROBE_INSUFFICIENT_CAMERA_COVERAGE = 1,
+  OMVGBA_PROBE_RESOURCE_LIMIT = 2,
+  OMVGBA_PROBE_WEAK_POINT_GEOMETRY = 3,
+  OMVGBA_PROBE_SPARSE_FACTORIZATION_FAILED = 4
+};
+
+typedef struct omvgba_probe_report {  /* FixedRotationObservabilityProbe (api.rs) */
+  int32_t status;                     /* omvgba_probe_status */
+  int32_t reserved;
+  uint64_t pose_dimension, selected_tracks, selected_observations, covered_free_cameras, weak_point_count;
+  uint64_t reduced_nonzeros;          /* stored lower-triangle entries of the camera system */
+  uint64_t factor_nonzeros;           /* entries of the factor's profile (envelope) in coordinate order */
+} omvgba_probe_report;
+
+/* FixedRotationObservabilityProbeOptions::default. */
+void omvgba_probe_options_default(omvgba_probe_options* options);
+
+/* Invalid options: OMVGBA_INVALID_ARGUMENT; an inconsistent problem: OMVGBA_INVALID_PROBLEM
+   (FixedRotationError, api.rs). A point a camera cannot project counts as weak. */
+int32_t omvgba_probe_fixed_rotation(omvgba_context* context, const omvgba_fixed_rotation_problem* problem,
+                                    const omvgba_probe_options* options, omvgba_probe_report* report,
+                                    omvgba_error* error);
+
+/* NativeBundleAdjuster::preflight (native/mod.rs:120-230): a problem whose observed free poses all
+   move only their centres, with pixel residuals, no fixed point, an explicit scale camera and one
+   camera model per pose, runs the probe on its prepared (rebased) frame; every other problem
+   reports PROCEED with has_counts = 0. Errors of the preparation are returned as by omvgba_solve;
+   a probe error is OMVGBA_NUMERICAL. */
+enum omvgba_preflight_status {
+  OMVGBA_PREFLIGHT_PROCEED = 0,
+  OMVGBA_PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE = 1,
+  OMVGBA_PREFLIGHT_RESOURCE_LIMIT = 2,
+  OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY = 3,
+  OMVGBA_PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED = 4
+};
+typedef struct omvgba_preflight {      /* NativePreflight (native/mod.rs:143-165) */
+  int32_t status;                      /* omvgba_preflight_status */
+  int32_t has_counts;                  /* 0: the probe did not run (the counts are None) */
+  uint64_t pose_dimension, covered_free_pose_count, weak_point_count;
+  int32_t dense_observability_escalation;
+  int32_t reserved;
+} omvgba_preflight;
+
+int32_t omvgba_preflight_check(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                               omvgba_preflight* preflight, omvgba_error* error);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ OUT_DIR = os.path.join(HERE, "openmvg_ba_cuda", "_lib")
 LIB = os.path.join(OUT_DIR, "libomvgba_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["gpu_solver.cu", "residual.cu", "residual_static.cu"]
-CPP_SOURCES = ["host.cpp"]
+CPP_SOURCES = ["host.cpp", "fixed_rotation.cpp"]
 
 
 def nvcc() -> str:

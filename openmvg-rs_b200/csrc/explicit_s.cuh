@@ -45,7 +45,6 @@ struct RowTables {
   uint32_t entries;           // neighbour entries in total
 };
 
-constexpr int kRowThreads = 128;
 
 __device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n0, uint32_t n1, int Y) {
   uint32_t lo = n0, hi = n1;
@@ -59,133 +58,202 @@ __device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n
   return (lo < n1 && nbr[lo] == Y) ? (int)(lo - n0) : -1;
 }
 
-// Row X of S. For each entity e of X (observation o at point p, camera columns cX..cX+dX) and each
-// entity e' of p in block Y (observation o', columns cY..): S_XY += Jc_e^T M Jc_e' with the 2 x 2
-// M = [o == o'] I - Jp_o Vhat_p^-1 Jp_o'^T (U, the pose/intrinsic edges and the point coupling in one
-// term). Targets of one point that fall in the same block are summed in target order by one thread
-// per element; entities are taken one after another, so every element is accumulated in entity
-// order. FP64 accumulation from records of type R.
+// Row X of S. Each entity e of X (observation o of point p, camera columns cX..cX+dX of its
+// record) meets every entity e' of p's track in a block Y (observation k, columns cY..cY+dY):
+//   S_XY += [k == o] A_o,X^T A_o,Y - E_e W_k,Y^T,   E_e = A_o,X^T Jp_o Vhat_p^-1 (dX x 3),
+//   W_k,Y = A_k,Y^T Jp_k (dY x 3),
+// U, the pose/intrinsic edges and the point coupling in one sum (A = the 2 x 9 camera columns and
+// Jp the 2 x 3 point columns of a record).
 //
-// Latency: a CTA walks thousands of entities one after another, so the per-entity chain is kept
-// short: the records of a track of up to kRowStage observations are staged in shared memory (longer
-// tracks are read from global memory), the block's neighbour list sits in shared memory when it has
-// at most kRowNbr entries, and thread 0 fetches the next entity's indices while the current one is
-// computed. Small static shared memory keeps many CTAs resident. Dynamic shared memory: 4 x
-// max_track ints (the target slots and columns).
-constexpr int kRowStage = 32;
-constexpr int kRowNbr = 1024;
+// One CTA per row, kRowWarps warps. The row's entities are taken kRowWarps at a time, one per warp:
+// the warp computes E of its entity and W of every observation of the track (a chunk of at most
+// kRowStage observations per round; longer tracks take several rounds) into shared memory, and the
+// slot of each target. After a barrier every warp adds the batch's contributions to the slots it
+// owns (slot index mod kRowWarps), entity by entity in batch order and target by target in track
+// order, lanes over the dX x dY elements. Each element therefore has one writer and a fixed
+// summation order: the row is the same bits run to run, without atomics. The row accumulates in
+// shared memory when it has at most row_smem doubles (else in place in global memory) and is
+// stored once at the end. Each warp fetches the indices of its next entity a batch ahead.
+constexpr int kRowWarps = 8;
+constexpr int kRowThreads = 32 * kRowWarps;
+constexpr int kRowStage = 16;           // track observations per round (2 targets each: 32 lanes)
+constexpr int kRowNbr = 1024;           // neighbour lists up to this length sit in shared memory
+constexpr int kRowSmemDoubles = 8192;   // rows up to 64 KB accumulate in shared memory
 template <typename R>
-__global__ void __launch_bounds__(kRowThreads) k_block_rows(RowTables rt, LinOut<R> lin, int max_track,
-                                                            double* __restrict__ rows) {
-  extern __shared__ int ish[];
-  int* tslot = ish;                  // per target: slot or -1
-  int* tcol = ish + 2 * max_track;   // per target: column of its segment
-  __shared__ double jr[kRowStage * kRec];  // the point's records (tracks of at most kRowStage)
-  __shared__ int nbr_s[kRowNbr];
-  __shared__ double G[6];                  // Jp_o Vhat^-1 (2 x 3)
-  __shared__ double aX[12];                // the entity's 2 x dX camera columns
-  __shared__ uint32_t s_ent[2][4];         // current / next entity: e, point, first observation, track length
-  const int X = blockIdx.x, tid = threadIdx.x;
+__global__ void __launch_bounds__(kRowThreads, 2) k_block_rows(RowTables rt, LinOut<R> lin, int row_smem,
+                                                               double* __restrict__ rows) {
+  extern __shared__ double row_sh[];
+  __shared__ int nbr_s[kRowNbr];                       // neighbour blocks
+  __shared__ uint32_t ninf_s[kRowNbr];                 // (offset in the row) << 3 | dY
+  __shared__ double Wsh[kRowWarps][kRowStage][27];     // W of each chunk observation, 9 x 3 row-major
+  __shared__ double Osh[kRowWarps][32];                // the entity's record: A (18), Jp (6), Vhat^-1 (6)
+  __shared__ double Esh[kRowWarps][18];                // E (dX x 3)
+  __shared__ int tsl[kRowWarps][2 * kRowStage];        // per target: slot or -1
+  __shared__ uint32_t tinf[kRowWarps][2 * kRowStage];  // per target: offset << 3 | dY
+  __shared__ int tcd[kRowWarps][2 * kRowStage];        // per target: cY | own << 8 | chunk obs << 9
+  __shared__ int item_n[kRowWarps], item_cx[kRowWarps];
+  const int X = blockIdx.x, tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   if (X >= rt.nblocks) return;
   const int dX = rt.blk_dim[X];
-  const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1];
-  const bool nbr_local = n1 - n0 <= (uint32_t)kRowNbr;
-  if (nbr_local)
-    for (uint32_t k = tid; k < n1 - n0; k += blockDim.x) nbr_s[k] = rt.nbr[n0 + k];
+  const uint32_t n0 = rt.nbr_begin[X], n1 = rt.nbr_begin[X + 1], nn = n1 - n0;
+  const bool nbr_local = nn <= (uint32_t)kRowNbr;
   const uint64_t r0 = rt.slot_off[n0], r1 = rt.slot_off[n1];
-  for (uint64_t k = r0 + tid; k < r1; k += blockDim.x) rows[k] = 0.0;
+  if (nbr_local)
+    for (uint32_t k = tid; k < nn; k += kRowThreads) {
+      const int Y = rt.nbr[n0 + k];
+      nbr_s[k] = Y;
+      ninf_s[k] = (uint32_t)(rt.slot_off[n0 + k] - r0) << 3 | (uint32_t)rt.blk_dim[Y];
+    }
+  const uint32_t rlen = (uint32_t)(r1 - r0);
+  double* row = rlen <= (uint32_t)row_smem ? row_sh : rows + r0;
+  for (uint32_t k = tid; k < rlen; k += kRowThreads) row[k] = 0.0;
   const uint32_t i0 = rt.blk_ent[X], i1 = rt.blk_ent[X + 1];
-  if (tid == 0 && i0 < i1) {
-    const uint32_t e = rt.ent[i0], p = rt.ent_point[i0];
-    const uint32_t a = rt.pt_off[p], b = rt.pt_off[p + 1];
-    s_ent[0][0] = e;
-    s_ent[0][1] = p;
-    s_ent[0][2] = a;
-    s_ent[0][3] = b - a;
-  }
   const int rs = lin.rs;
-  for (uint32_t i = i0; i < i1; ++i) {
-    __syncthreads();  // the previous entity is finished (and the row is zeroed, the list staged)
-    const int buf = (i - i0) & 1;
-    const uint32_t e = s_ent[buf][0], o = e >> 1, p = s_ent[buf][1], o0 = s_ent[buf][2], L = s_ent[buf][3];
-    const bool staged = L <= (uint32_t)kRowStage;
-    if (staged)
-      for (uint32_t k = tid; k < (uint32_t)kRec * L; k += blockDim.x) {
-        const uint32_t c = k / L, j = k - c * L;
-        jr[j * kRec + c] = (double)lin.rec[lin.obs_rec[o0 + j] + (size_t)c * rs];
-      }
-    for (uint32_t t = tid; t < 2 * L; t += blockDim.x) {
-      const uint32_t eid = 2 * (o0 + (t >> 1)) + (t & 1);
-      const int Y = rt.ent_block[eid];
-      int sl = -1;
-      if (Y >= 0) sl = nbr_local ? find_slot(nbr_s, 0, n1 - n0, Y) : find_slot(rt.nbr, n0, n1, Y);
-      tslot[t] = sl;
-      tcol[t] = rt.seg_col[eid];
-    }
-    if (tid == 32 && i + 1 < i1) {  // the next entity's indices, fetched while this one is computed
-      const uint32_t en = rt.ent[i + 1], pn = rt.ent_point[i + 1];
-      const uint32_t a = rt.pt_off[pn], b = rt.pt_off[pn + 1];
-      s_ent[buf ^ 1][0] = en;
-      s_ent[buf ^ 1][1] = pn;
-      s_ent[buf ^ 1][2] = a;
-      s_ent[buf ^ 1][3] = b - a;
-    }
-    const uint32_t jo = o - o0;
-    if (tid == 0) {
-      const double* vi = lin.vinv + 6 * (size_t)p;
-      const double Vi[6] = {vi[0], vi[1], vi[2], vi[3], vi[4], vi[5]};
-      const R* ro = lin.rec + lin.obs_rec[o];
-      double jp[6];
-      for (int k = 0; k < 6; ++k) jp[k] = (double)ro[(size_t)(kJp + k) * rs];
-      sym3_apply(Vi, jp, G);
-      sym3_apply(Vi, jp + 3, G + 3);
-      const int cX = rt.seg_col[e];
-      for (int m = 0; m < 6; ++m) {
-        aX[m] = m < dX ? (double)ro[(size_t)(cX + m) * rs] : 0.0;
-        aX[6 + m] = m < dX ? (double)ro[(size_t)(9 + cX + m) * rs] : 0.0;
-      }
-    }
-    __syncthreads();
-    for (uint32_t w = tid; w < 2 * L * 36; w += blockDim.x) {
-      const uint32_t t = w / 36, mn = w - 36 * t, m = mn / 6, n = mn - 6 * m;
-      const int sl = tslot[t];
-      if (sl < 0 || (int)m >= dX) continue;
-      const int dY = rt.blk_dim[nbr_local ? nbr_s[sl] : rt.nbr[n0 + sl]];
-      if ((int)n >= dY) continue;
-      bool leader = true;
-      for (uint32_t t2 = 0; t2 < t; ++t2) leader = leader && tslot[t2] != sl;
-      if (!leader) continue;
-      const double a0 = aX[m], a1 = aX[6 + m];
-      double acc = 0.0;
-      for (uint32_t t2 = t; t2 < 2 * L; ++t2) {
-        if (tslot[t2] != sl) continue;
-        const uint32_t j = t2 >> 1;
-        const int cY = tcol[t2];
-        double q[6], b0, b1;
-        if (staged) {
-          const double* rj = jr + j * kRec;
-          for (int k = 0; k < 6; ++k) q[k] = rj[kJp + k];
-          b0 = rj[cY + n];
-          b1 = rj[9 + cY + n];
-        } else {
-          const R* rj = lin.rec + lin.obs_rec[o0 + j];
-          for (int k = 0; k < 6; ++k) q[k] = (double)rj[(size_t)(kJp + k) * rs];
-          b0 = (double)rj[(size_t)(cY + n) * rs];
-          b1 = (double)rj[(size_t)(9 + cY + n) * rs];
-        }
-        double M00 = -(G[0] * q[0] + G[1] * q[1] + G[2] * q[2]);
-        double M01 = -(G[0] * q[3] + G[1] * q[4] + G[2] * q[5]);
-        double M10 = -(G[3] * q[0] + G[4] * q[1] + G[5] * q[2]);
-        double M11 = -(G[3] * q[3] + G[4] * q[4] + G[5] * q[5]);
-        if (j == jo) {
-          M00 += 1.0;
-          M11 += 1.0;
-        }
-        acc += a0 * (M00 * b0 + M01 * b1) + a1 * (M10 * b0 + M11 * b1);
-      }
-      rows[rt.slot_off[n0 + sl] + m * dY + n] += acc;
-    }
+  // this warp's entity in the current batch (ce, cp, ca = first observation of the track, cl =
+  // track length; cl = 0: none) and the next batch's entity and point
+  uint32_t ce = 0, cp = 0, ca = 0, cl = 0, xe = 0, xp = 0;
+  if (i0 + w < i1) {
+    ce = rt.ent[i0 + w];
+    cp = rt.ent_point[i0 + w];
+    ca = rt.pt_off[cp];
+    cl = rt.pt_off[cp + 1] - ca;
   }
+  if (i0 + kRowWarps + w < i1) {
+    xe = rt.ent[i0 + kRowWarps + w];
+    xp = rt.ent_point[i0 + kRowWarps + w];
+  }
+  for (uint32_t base = i0; base < i1; base += kRowWarps) {
+    // indices a batch ahead: the track of the next entity, the entity and point after it
+    const uint32_t inext = base + kRowWarps + w, iafter = base + 2 * kRowWarps + w;
+    uint32_t xa = 0, xl = 0, ye = 0, yp = 0;
+    if (inext < i1) {
+      xa = rt.pt_off[xp];
+      xl = rt.pt_off[xp + 1] - xa;
+    }
+    if (iafter < i1) {
+      ye = rt.ent[iafter];
+      yp = rt.ent_point[iafter];
+    }
+    const uint32_t o = ce >> 1, ke = o - ca;
+    const int cX = cl ? rt.seg_col[ce] : 0;
+    for (uint32_t k0 = 0; __syncthreads_or(k0 < cl); k0 += kRowStage) {
+      // ---- this warp's chunk: E (first round), targets, W ----
+      // Loads are issued in two rounds: first every index (record offsets, target blocks and
+      // columns, the point inverse), then every record value, so a chunk costs two memory latencies.
+      const uint32_t Lc = k0 < cl ? min((uint32_t)kRowStage, cl - k0) : 0;
+      const bool first = Lc && k0 == 0;
+      const uint32_t rec_k = lane < Lc ? lin.obs_rec[ca + k0 + lane] : 0;  // record of chunk observation lane
+      const uint32_t rec_o = first ? lin.obs_rec[o] : 0;
+      int Y = -1, tcol = 0;
+      uint32_t eid = 0;
+      if (lane < 2 * Lc) {
+        eid = 2 * (ca + k0 + (lane >> 1)) + (lane & 1);
+        Y = rt.ent_block[eid];
+        tcol = rt.seg_col[eid];
+      }
+      const double vi = (first && lane < 6) ? lin.vinv[6 * (size_t)cp + lane] : 0.0;
+      // the entity's own record (E and the U term)
+      double own = 0.0;
+      if (first && lane < kRec) own = (double)lin.rec[rec_o + (size_t)lane * rs];
+      // W of the chunk: lane kk + 16 h holds observation kk, columns 5h .. 5h + 4 (h = 1: 5 .. 8)
+      const uint32_t kk = lane & 15, h = lane >> 4;
+      const uint32_t rk_off = __shfl_sync(0xffffffffu, rec_k, (int)kk);
+      const int c0 = h ? 5 : 0, nc = h ? 4 : 5;
+      double jp[6], a0[5], a1[5];
+      if (kk < Lc) {
+        const R* rk = lin.rec + rk_off;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) jp[c] = (double)rk[(size_t)(kJp + c) * rs];
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          a0[j] = j < nc ? (double)rk[(size_t)(c0 + j) * rs] : 0.0;
+          a1[j] = j < nc ? (double)rk[(size_t)(9 + c0 + j) * rs] : 0.0;
+        }
+      }
+      if (first) {
+        if (lane < kRec) Osh[w][lane] = own;
+        if (lane < 6) Osh[w][kRec + lane] = vi;
+      }
+      if (kk < Lc) {
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+          if (j < nc) {
+            double* wq = Wsh[w][kk] + 3 * (c0 + j);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) wq[c] = a0[j] * jp[c] + a1[j] * jp[3 + c];
+          }
+      }
+      if (lane < 2 * Lc) {
+        int sl = -1;
+        uint32_t inf = 0;
+        if (Y >= 0) {
+          sl = nbr_local ? find_slot(nbr_s, 0, nn, Y) : find_slot(rt.nbr, n0, n1, Y);
+          if (sl >= 0)
+            inf = nbr_local ? ninf_s[sl]
+                            : (uint32_t)(rt.slot_off[n0 + sl] - r0) << 3 | (uint32_t)rt.blk_dim[Y];
+        }
+        tsl[w][lane] = sl;
+        tinf[w][lane] = inf;
+        tcd[w][lane] = tcol | (k0 + (lane >> 1) == ke ? 1 << 8 : 0) | (int)(lane >> 1) << 9;
+      }
+      __syncwarp();
+      if (first && lane < 3 * dX) {
+        const int m = lane / 3, c = lane - 3 * m;
+        const double* A = Osh[w];
+        const double* P = Osh[w] + kRec;
+        double wm[3];
+        for (int d = 0; d < 3; ++d) wm[d] = A[cX + m] * A[kJp + d] + A[9 + cX + m] * A[kJp + 3 + d];
+        const double v0 = c == 0 ? P[0] : (c == 1 ? P[1] : P[3]);
+        const double v1 = c == 0 ? P[1] : (c == 1 ? P[2] : P[4]);
+        const double v2 = c == 0 ? P[3] : (c == 1 ? P[4] : P[5]);
+        Esh[w][lane] = wm[0] * v0 + wm[1] * v1 + wm[2] * v2;
+      }
+      if (lane == 0) {
+        item_n[w] = 2 * (int)Lc;
+        item_cx[w] = cX;
+      }
+      __syncthreads();
+      // ---- every warp adds the batch's contributions to the slots it owns ----
+      for (int b = 0; b < kRowWarps; ++b) {
+        const int nt = item_n[b];
+        if (nt == 0) continue;
+        const int sl = lane < nt ? tsl[b][lane] : -1;
+        unsigned mask = __ballot_sync(0xffffffffu, sl >= 0 && sl % kRowWarps == w);
+        const int cxb = item_cx[b];
+        const double* A = Osh[b];
+        const double* E = Esh[b];
+        while (mask) {
+          const int t = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const uint32_t inf = tinf[b][t];
+          const int cd = tcd[b][t], cY = cd & 0xff, own = (cd >> 8) & 1, dY = (int)(inf & 7);
+          const double* Wk = Wsh[b][cd >> 9];
+          double* out = row + (inf >> 3);
+          // lanes over a fixed 6 x 6 grid of (m, n): element l of the grid is (l / 6, l % 6)
+#pragma unroll
+          for (int pass = 0; pass < 2; ++pass) {
+            const int l = lane + 32 * pass;
+            const int m = l / 6, n = l - 6 * (l / 6);
+            if (l < 36 && m < dX && n < dY) {
+              const double* wn = Wk + 3 * (cY + n);
+              double acc = -(E[3 * m] * wn[0] + E[3 * m + 1] * wn[1] + E[3 * m + 2] * wn[2]);
+              if (own) acc += A[cxb + m] * A[cY + n] + A[9 + cxb + m] * A[9 + cY + n];
+              out[m * dY + n] += acc;
+            }
+          }
+        }
+      }
+    }
+    ce = xe;
+    cp = xp;
+    ca = xa;
+    cl = inext < i1 ? xl : 0;
+    xe = ye;
+    xp = yp;
+  }
+  __syncthreads();
+  if (row == row_sh)
+    for (uint32_t k = tid; k < rlen; k += kRowThreads) rows[r0 + k] = row_sh[k];
 }
 
 // y = (S + lambda diag) x from the block rows: one warp per block row, lanes over the row's entries
@@ -298,6 +366,16 @@ __global__ void k_rows_to_tiles(RowTables rt, const double* __restrict__ rows, c
       if (P == Q) v += lambda * diag[oX + m] - shift;
       tb.t[tile_at(tb, P / kCT, Q / kCT) + (size_t)(Q % kCT) * kCT + (P % kCT)] = v;
     }
+}
+
+// Scatter of lower-triangle entries (row >= col) given as triplets into the band.
+__global__ void k_triplets_to_tiles(uint32_t count, const int* __restrict__ rows, const int* __restrict__ cols,
+                                    const double* __restrict__ vals, TileBand tb) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= count) return;
+  const int P = rows[q], Q = cols[q];
+  if (P < Q || P >= tb.n || Q < 0 || (P / kCT) - (Q / kCT) > tb.bwt) return;
+  tb.t[tile_at(tb, P / kCT, Q / kCT) + (size_t)(Q % kCT) * kCT + (P % kCT)] = vals[q];
 }
 
 // Identity on the padding rows of the last diagonal tile.

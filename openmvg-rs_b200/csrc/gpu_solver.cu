@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "gpu_solver.hpp"
+#include "fixed_rotation.hpp"
 
 #include <atomic>
 #include <thread>
@@ -253,6 +254,7 @@ struct DevView {
   const uint32_t* cam_group;   // ncam
   const int* pose_off;         // ncam
   const int* pose_dim;         // ncam
+  const uint8_t* pose_mask;    // ncam: bit 0 rotation, bit 1 translation (3 when the layout is legacy)
   const int* intr_off;         // ng
   const int* intr_dim;         // ng
   const uint8_t* fixed_points; // P
@@ -438,19 +440,37 @@ struct LinOut {
   double* sw;      // optional N: sqrt weight per observation (debug linearization only)
 };
 
-// pose_motion (schur/point.rs:730-762) applied to the projection Jacobian: J * [-[RX]x | s I]
-__device__ __forceinline__ void pose_jacobian(const double J[2][3], const double rot[3], int cam, const Gauge& g,
-                                              double out[2][6]) {
-  double m[3][6] = {{0.0, rot[2], -rot[1], 0, 0, 0}, {-rot[2], 0.0, rot[0], 0, 0, 0}, {rot[1], -rot[0], 0.0, 0, 0, 0}};
-  if (cam == g.fixed_cam) {
-    for (int c = 0; c < 3; ++c) {
-      m[c][3] = g.baseline * g.b0[c];
-      m[c][4] = g.baseline * g.b1[c];
+// The pose columns of an observation's camera Jacobian (schur/point.rs:286-313), J times the motion
+// of the camera point: pose_motion (point.rs:730-762) [-[q]x | s I] at q = RX, or at the camera point
+// q = RX + t when the mask holds the translation (the camera turns about its fixed centre);
+// translation_motion (point.rs:764-786) alone, s I, when the mask holds the rotation. The FixedBaseline
+// camera's translation columns are the baseline times its S^2 tangent basis.
+__device__ __forceinline__ void pose_jacobian(const double J[2][3], const double rot[3], const double xc[3],
+                                              int mask, int cam, const Gauge& g, double out[2][6]) {
+  double m[3][6];
+  const double* q = (mask & 2) ? rot : xc;
+  const int ts = (mask & 1) ? 3 : 0;  // first translation column
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 6; ++c) m[r][c] = 0.0;
+  if (mask & 1) {
+    m[0][1] = q[2];
+    m[0][2] = -q[1];
+    m[1][0] = -q[2];
+    m[1][2] = q[0];
+    m[2][0] = q[1];
+    m[2][1] = -q[0];
+  }
+  if (mask & 2) {
+    if (cam == g.fixed_cam) {
+      for (int c = 0; c < 3; ++c) {
+        m[c][ts] = g.baseline * g.b0[c];
+        m[c][ts + 1] = g.baseline * g.b1[c];
+      }
+    } else {
+      m[0][ts] = g.scene;
+      m[1][ts + 1] = g.scene;
+      m[2][ts + 2] = g.scene;
     }
-  } else {
-    m[0][3] = g.scene;
-    m[1][4] = g.scene;
-    m[2][5] = g.scene;
   }
   for (int r = 0; r < 2; ++r)
     for (int c = 0; c < 6; ++c) out[r][c] = J[r][0] * m[0][c] + J[r][1] * m[1][c] + J[r][2] * m[2][c];
@@ -1047,7 +1067,7 @@ __global__ void __launch_bounds__(mv_tile_obs<T>(), sizeof(T) == 4 ? 3 : 6) k_li
       const int pd = v.pose_dim[cam];
       if (pd > 0) {
         double pj[2][6];
-        pose_jacobian(J, rot, cam, g, pj);
+        pose_jacobian(J, rot, xc, v.pose_mask[cam], cam, g, pj);
         for (int a = 0; a < 2; ++a)
           for (int k = 0; k < pd; ++k) jc[a][k] = pj[a][k];
       }
@@ -1279,21 +1299,32 @@ __global__ void k_retract(DevView v, int ng, const double* step, Gauge g, const 
     const double* P = cur_pose + 12 * c;
     double* Q = cand_pose + 12 * c;
     int d = v.pose_dim[c], o = v.pose_off[c];
+    const int mask = v.pose_mask[c];
     if (d == 0) {
       for (int k = 0; k < 12; ++k) Q[k] = P[k];
     } else {
-      double w[3] = {step[o], step[o + 1], step[o + 2]};
+      // retract_poses_with_masks (optimizer.rs:442-510); a full mask is retract_poses (:376-424)
       double U[9];
-      exp_so3_dev(w, U);
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-          double s = 0.0;
-          for (int k = 0; k < 3; ++k) s += U[3 * i + k] * P[3 * k + j];
-          Q[3 * i + j] = s;
-        }
-      if (c == g.fixed_cam) {
+      int ts = 0;
+      if (mask & 1) {
+        double w[3] = {step[o], step[o + 1], step[o + 2]};
+        exp_so3_dev(w, U);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 3; ++k) s += U[3 * i + k] * P[3 * k + j];
+            Q[3 * i + j] = s;
+          }
+        ts = 3;
+      } else {
+        for (int k = 0; k < 9; ++k) Q[k] = P[k];
+      }
+      if (!(mask & 2)) {  // t' = Exp(w) t keeps the centre -R^T t
+        for (int i = 0; i < 3; ++i)
+          Q[9 + i] = (mask & 1) ? U[3 * i] * P[9] + U[3 * i + 1] * P[10] + U[3 * i + 2] * P[11] : P[9 + i];
+      } else if (c == g.fixed_cam) {
         // retract_s2 (numerics/manifold.rs:133-147)
-        double d0 = step[o + 3], d1 = step[o + 4];
+        double d0 = step[o + ts], d1 = step[o + ts + 1];
         double vv[3] = {g.b0[0] * d0 + g.b1[0] * d1, g.b0[1] * d0 + g.b1[1] * d1, g.b0[2] * d0 + g.b1[2] * d1};
         double th = sqrt(vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]);
         double tn = sqrt(g.dir[0] * g.dir[0] + g.dir[1] * g.dir[1] + g.dir[2] * g.dir[2]);
@@ -1311,7 +1342,7 @@ __global__ void k_retract(DevView v, int ng, const double* step, Gauge g, const 
         }
         for (int k = 0; k < 3; ++k) Q[9 + k] = g.baseline * out[k];
       } else {
-        for (int k = 0; k < 3; ++k) Q[9 + k] = P[9 + k] + g.scene * step[o + 3 + k];
+        for (int k = 0; k < 3; ++k) Q[9 + k] = P[9 + k] + g.scene * step[o + ts + k];
       }
     }
   }
@@ -1503,7 +1534,7 @@ static Layout make_layout(const NativeProblem& n) {
   L.pose_dim.resize(n.ncam);
   int off = 0;
   for (int c = 0; c < n.ncam; ++c) {
-    int d = (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+    int d = pose_block_dim(n, c);
     L.pose_off[c] = off;
     L.pose_dim[c] = d;
     off += d;
@@ -1542,7 +1573,8 @@ struct Setup {
   std::vector<int> perm_off;        // per block: first position in the factorization order
   std::vector<int> perm_to_orig;    // D: parameter at each position of the factorization order
   int bwt = 0, nt = 0;              // band width and side of the factor, in 64 x 64 tiles
-  int max_track = 0;                // longest track (staging of the block-row kernel)
+  int max_track = 0;                // longest track
+  uint64_t max_row = 0;             // longest block row of S (doubles)
 };
 
 // Tiles of the fused matvec for one record precision (host tables).
@@ -1969,6 +2001,9 @@ static void build_explicit(const NativeProblem& n, const Layout& L, Setup& S) {
       off += (uint64_t)S.blk_dim[X] * (uint64_t)S.blk_dim[nbrs[X][k]];
     }
   S.slot_off[E] = off;
+  S.max_row = 0;
+  for (int X = 0; X < nb; ++X)
+    S.max_row = std::max<uint64_t>(S.max_row, S.slot_off[S.nbr_begin[X + 1]] - S.slot_off[S.nbr_begin[X]]);
   // factorization order
   std::vector<int> order;
   order.reserve(nb);
@@ -2117,8 +2152,57 @@ ExecutionPlan execution_plan(const NativeProblem& n, const LmOptions& opt) {
   pattern_counts(n, L, S, &nnz, &rows);
   const bool direct = auto_prefers_direct(n.self_cal, n.obs_cam.size(), L.D, n.points.size() / 3, nnz, rows,
                                           opt.workspace_budget, &plan.direct_estimate, &plan.cached_estimate);
-  plan.iterative = opt.linear_solver == 0 ? !direct : opt.iterative;
+  // a translation-only solve resolves Auto to the direct solver (native/mod.rs:398-407)
+  plan.iterative = opt.linear_solver == 0 ? (!direct && !(!n.self_cal && n.translation_only)) : opt.iterative;
   return plan;
+}
+
+// Positive-definiteness certificate of a symmetric matrix from its lower-triangle entries: the entries
+// are scattered into the banded tile layout of the explicit reduced camera system (bandwidth from the
+// entries themselves) and factored by the same tiled Cholesky kernels; the status word says whether
+// every pivot was positive.
+bool device_certify_positive_definite(Context* ctx, int n, const std::vector<int>& rows, const std::vector<int>& cols,
+                                      const std::vector<double>& values) {
+  if (n <= 0) return true;
+  CUDA_OK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  int bwt = 0;
+  for (size_t q = 0; q < rows.size(); ++q) bwt = std::max(bwt, rows[q] / kCT - cols[q] / kCT);
+  const int nt = (n + kCT - 1) / kCT;
+  bwt = std::min(std::max(bwt, 1), std::max(nt - 1, 1));
+  const size_t count = (size_t)nt * (bwt + 1) * kCTT;
+  if (sizeof(double) * count > (size_t(16) << 30))
+    throw SolveFailure{3, "the banded factor of the probe's camera system exceeds 16 GiB"};
+  DBuf<double> tiles, winv, vals;
+  DBuf<int> d_rows, d_cols, status;
+  tiles.alloc(count, st);
+  winv.alloc((size_t)nt * kCTT, st);
+  status.alloc(1, st);
+  d_rows.upload(rows.data(), rows.size(), st);
+  d_cols.upload(cols.data(), cols.size(), st);
+  vals.upload(values.data(), values.size(), st);
+  CUDA_OK(cudaFuncSetAttribute(k_tile_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+  CUDA_OK(cudaFuncSetAttribute(k_tile_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
+  CUDA_OK(cudaMemsetAsync(tiles.p, 0, sizeof(double) * count, st));
+  OMVGBA_LAUNCH(k_set_int, 1, 1, 0, st, status.p, 1);
+  TileBand tb{n, nt, bwt, tiles.p, winv.p};
+  if (!rows.empty())
+    OMVGBA_LAUNCH(k_triplets_to_tiles, grid_for(rows.size(), 256), 256, 0, st, (uint32_t)rows.size(), d_rows.p,
+                  d_cols.p, vals.p, tb);
+  OMVGBA_LAUNCH(k_tiles_pad, 1, kCT, 0, st, tb);
+  for (int k = 0; k < nt; ++k) {
+    OMVGBA_LAUNCH(k_tile_potrf, 1, 256, 0, st, tb, k, status.p);
+    const int m = std::min(bwt, nt - 1 - k);
+    if (m > 0) {
+      OMVGBA_LAUNCH(k_tile_trsm, m, 256, kTrsmSmem, st, tb, k, status.p);
+      OMVGBA_LAUNCH(k_tile_update, m * (m + 1) / 2, 256, kUpdateSmem, st, tb, k, status.p);
+    }
+  }
+  CUDA_OK(cudaGetLastError());
+  int ok = 0;
+  CUDA_OK(cudaMemcpyAsync(&ok, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  return ok != 0;
 }
 
 // Device copy of a TileSet plus the fused-matvec launch shape.
@@ -2152,6 +2236,11 @@ struct TileSetDev {
   }
 };
 
+// Auto operator switch: a PCG run of at least this many products moves the rest of the solve to the
+// explicit S. One build of the rows costs about as much as this many tile products on the survey
+// grids (plane500: ~2 ms of rows against ~60 us per product, the explicit product ~25 us).
+constexpr uint64_t kExplicitSwitchTerms = 64;
+
 template <typename T>
 struct Solver {
   Context* ctx;
@@ -2167,6 +2256,7 @@ struct Solver {
   DBuf<double> d_obs_px;
   DBuf<FixedCameraDev> d_models;
   DBuf<int> d_pose_off, d_pose_dim, d_intr_off, d_intr_dim;
+  DBuf<uint8_t> d_pose_mask;
   DBuf<uint8_t> d_fixed_points;
   DBuf<double> d_pose[2], d_points[2], d_groups[2];
   int cur = 0;
@@ -2194,6 +2284,7 @@ struct Solver {
   DBuf<uint64_t> d_slot_off;
   DBuf<double> d_rows, d_tiles, d_winv, d_ztiles, d_perm_vec, d_marg_out, d_power;
   bool rows_valid = false;  // the rows hold S of the current assembly
+  bool rows_attr = false;   // k_block_rows may take kRowSmemDoubles of dynamic shared memory
   // PCG vectors
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
   DBuf<int> d_fail;
@@ -2223,11 +2314,14 @@ struct Solver {
       pattern_counts(n, L, S, &nnz, &rows);
       opt.iterative = !auto_prefers_direct(n.self_cal, (uint64_t)N, D, (uint64_t)P, nnz, rows, opt.workspace_budget,
                                            &de, &ce);
+      // a translation-only solve resolves Auto to the direct solver, so its final rank is exact
+      // (native/mod.rs:398-407)
+      if (!n.self_cal && n.translation_only) opt.iterative = false;
     }
     direct = !opt.iterative;
     // the PCG operator: the explicit S by block rows (rebuilt every assembly, a block-sparse product
     // that stays in L2) or the matrix-free tile product over the Jacobian records
-    explicit_op = !direct && opt.matvec == 1;
+    explicit_op = !direct && opt.matvec == 1;  // Auto starts matrix-free (see kExplicitSwitchTerms)
     const uint64_t bytes_before = tl_device_bytes;
     const double t1 = now();
     // mixed precision keeps only FP32 Jacobian records (and their tiles); FP64 mode only FP64 ones
@@ -2266,6 +2360,7 @@ struct Solver {
     v.cam_group = d_cam_group.p;
     v.pose_off = d_pose_off.p;
     v.pose_dim = d_pose_dim.p;
+    v.pose_mask = d_pose_mask.p;
     v.intr_off = d_intr_off.p;
     v.intr_dim = d_intr_dim.p;
     v.fixed_points = d_fixed_points.p;
@@ -2346,6 +2441,12 @@ struct Solver {
     d_cam_group.upload(cg.data(), cg.size(), st);
     d_pose_off.upload(L.pose_off.data(), L.pose_off.size(), st);
     d_pose_dim.upload(L.pose_dim.data(), L.pose_dim.size(), st);
+    {
+      std::vector<uint8_t> masks(std::max(n.ncam, 1), (uint8_t)3);
+      if (n.explicit_masks)
+        for (int c = 0; c < n.ncam; ++c) masks[c] = n.pose_mask[c];
+      d_pose_mask.upload(masks.data(), masks.size(), st);
+    }
     d_intr_off.upload(L.intr_off.data(), L.intr_off.size(), st);
     d_intr_dim.upload(L.intr_dim.data(), L.intr_dim.size(), st);
     d_fixed_points.upload(n.fixed_points.data(), n.fixed_points.size(), st);
@@ -2608,18 +2709,22 @@ struct Solver {
 
   // S of the current linearization (no damping) by block rows, from the FP64 or FP32 records.
   void build_rows() {
-    const size_t smem = 4 * (size_t)std::max(S.max_track, 1) * sizeof(int);
-    if (smem > 48 * 1024) {
-      CUDA_OK(cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      CUDA_OK(cudaFuncSetAttribute(k_block_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int row_smem = (int)std::min<uint64_t>(S.max_row, (uint64_t)kRowSmemDoubles);
+    const size_t smem = (size_t)row_smem * sizeof(double);
+    if (!rows_attr) {
+      CUDA_OK(cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kRowSmemDoubles * (int)sizeof(double)));
+      CUDA_OK(cudaFuncSetAttribute(k_block_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kRowSmemDoubles * (int)sizeof(double)));
+      rows_attr = true;
     }
     const bool timing = std::getenv("OMVGBA_PHASE_TIMES") != nullptr;
     if (timing) sync();
     const double t0 = now();
     if (mixed)
-      OMVGBA_LAUNCH(k_block_rows<float>, nb, kRowThreads, smem, st, row_tables(), lin32(), S.max_track, d_rows.p);
+      OMVGBA_LAUNCH(k_block_rows<float>, nb, kRowThreads, smem, st, row_tables(), lin32(), row_smem, d_rows.p);
     else
-      OMVGBA_LAUNCH(k_block_rows<T>, nb, kRowThreads, smem, st, row_tables(), lin(), S.max_track, d_rows.p);
+      OMVGBA_LAUNCH(k_block_rows<T>, nb, kRowThreads, smem, st, row_tables(), lin(), row_smem, d_rows.p);
     check_launch();
     if (timing) {
       sync();
@@ -3239,6 +3344,9 @@ struct Solver {
             solved = r.accepted;
             iterative_step = true;
             rel_res = r.rel;
+            // Auto operator: once a PCG run needs many products, rebuilding the explicit S every
+            // assembly costs less than the tile products it replaces
+            if (opt.matvec == 0 && !explicit_op && r.terms >= kExplicitSwitchTerms) explicit_op = true;
           }
         }
         double t2 = now();

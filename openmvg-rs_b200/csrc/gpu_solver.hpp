@@ -64,7 +64,24 @@ struct NativeProblem {
   std::vector<uint32_t> cam_group;  // per native camera
   std::vector<int> group_dim;       // free (log f, k1, k2) prefix per group, 0 when fixed
   int gauge_cam = -1;               // FixedBaseline camera on the S^2 chart, -1 when free
+  // Calibrated solves carry explicit per-camera pose masks (bit 0 rotation, bit 1 translation, 0
+  // fixed; workspace/topology.rs:305-347): camera 0 is free when its mask is, a rotation-only block
+  // turns the camera about its fixed centre and a translation-only block moves only the centre.
+  // Self-calibration keeps the legacy layout (camera 0 fixed, the others full or fixed).
+  bool explicit_masks = false;
+  std::vector<uint8_t> pose_mask;   // per native camera
+  bool translation_only = false;    // no free mask moves a rotation (CameraPoseVariables)
 };
+
+// Free pose coordinates of native camera c (ReducedLayout, workspace/topology.rs:263-347).
+inline int pose_block_dim(const NativeProblem& n, int c) {
+  if (n.explicit_masks) {
+    const int m = n.pose_mask[c];
+    if (n.fixed_poses[c] || m == 0) return 0;
+    return 3 * (m & 1) + ((m & 2) ? (c == n.gauge_cam ? 2 : 3) : 0);
+  }
+  return (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+}
 
 struct LmOptions {
   uint64_t max_iterations = 50;

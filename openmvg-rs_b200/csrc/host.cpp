@@ -28,6 +28,7 @@
 
 #include "../../include/ba_cuda.h"
 #include "gpu_solver.hpp"
+#include "fixed_rotation.hpp"
 
 namespace omvgba {
 namespace {
@@ -436,13 +437,16 @@ Lowered lower_calibrated(const omvgba_problem& pr) {
            "pixel BA supports fixed pinhole and Brown-Conrady cameras; use angular residuals for wide-angle cameras");
   }
   GaugePlan plan = calibrated_gauge_plan(pr);
-  for (size_t i = 0; i < pr.pose_count; ++i)
-    if (plan.masks[i] != 0 && plan.masks[i] != OMVGBA_POSE_FREE)
-      fail(OMVGBA_UNSUPPORTED, "partial pose-variable masks (rotation-only or translation-only) are not supported by this adjuster");
   auto observed = observed_cameras(pr);
   Lowered L;
   NativeProblem& n = L.n;
   n.self_cal = false;
+  n.explicit_masks = true;
+  // CameraPoseVariables of the prepared problem (native/calibrated.rs:226-234): translation-only when
+  // no free mask moves a rotation (vacuously so when every pose is fixed)
+  n.translation_only = true;
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (plan.masks[i] != 0 && (plan.masks[i] & OMVGBA_POSE_ROTATION)) n.translation_only = false;
   set_anchor(pr, L.rb, plan.anchor, plan.scale);
   n.ncam = (int)pr.pose_count;
   std::vector<size_t> dest(pr.pose_count);
@@ -458,6 +462,8 @@ Lowered lower_calibrated(const omvgba_problem& pr) {
       for (int k = 0; k < 3; ++k) n.translation[3 * d + k] = 0.0;
     }
     n.fixed_poses.push_back(plan.masks[s] == 0);
+    n.pose_mask.push_back((uint8_t)((plan.masks[s] & OMVGBA_POSE_ROTATION ? 1 : 0) |
+                                    (plan.masks[s] & OMVGBA_POSE_TRANSLATION ? 2 : 0)));
   }
   std::vector<uint8_t> pobs(pr.point_count, 0);
   for (size_t o = 0; o < pr.observation_count; ++o) pobs[pr.observation_point[o]] = 1;
@@ -639,7 +645,7 @@ Lowered lower(const omvgba_problem& pr) {
 
 int reduced_dimension(const NativeProblem& n) {
   int D = 0;
-  for (int c = 0; c < n.ncam; ++c) D += (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+  for (int c = 0; c < n.ncam; ++c) D += pose_block_dim(n, c);
   if (n.self_cal)
     for (int d : n.group_dim) D += d;
   return D;
@@ -1086,6 +1092,189 @@ void canonicalize(const omvgba_problem& pr, Result& res) {
   refresh_inliers(pr, active, res);
 }
 
+// ---- translation-only observability: the preflight and the post-solve probe -------------------
+// common_pose_variables (native/gauge.rs:9-40): 1 when every observed free pose moves only its
+// centre, 0 when they move rotation and translation (or none is free), -1 when the masks are not one
+// of those forms (a rotation without translation, or a mixture).
+int common_pose_variables(const omvgba_problem& pr) {
+  const auto observed = observed_cameras(pr);
+  int selected = -1;
+  for (size_t i = 0; i < pr.pose_count; ++i) {
+    const uint32_t v = pr.poses[i].variables;
+    if (!observed[i] || v == 0) continue;
+    if (!(v & OMVGBA_POSE_TRANSLATION)) return -1;
+    const int candidate = (v & OMVGBA_POSE_ROTATION) ? 0 : 1;
+    if (selected >= 0 && selected != candidate) return -1;
+    selected = candidate;
+  }
+  return selected < 0 ? 0 : selected;
+}
+
+// can_probe_scale_representative (native/mod.rs:510-521)
+bool can_probe_scale_representative(const omvgba_problem& pr) {
+  if (pr.gauge_kind != OMVGBA_GAUGE_FIXED_BASELINE) return true;
+  const auto observed = observed_cameras(pr);
+  const double* f = pr.poses[pr.gauge_first].center;
+  for (size_t c = 0; c < pr.pose_count; ++c) {
+    const double* x = pr.poses[c].center;
+    if (c != pr.gauge_first && observed[c] && !(pr.poses[c].variables & OMVGBA_POSE_TRANSLATION) &&
+        !(x[0] == f[0] && x[1] == f[1] && x[2] == f[2]))
+      return false;
+  }
+  return true;
+}
+
+// The probe's problem on the prepared (rebased) frame of a calibrated lowering with the native state
+// rot / tr / pts (probe_prepared, native/fixed_rotation.rs:50-165): centres C = -R^T t, one camera
+// model per pose (the pinhole of its intrinsics, or the full Brown-Conrady camera when the lowering
+// uses full models), the tracks in the lowering's point order, the scale camera of the native gauge.
+ProbeProblem prepared_probe_problem(const omvgba_problem& pr, const Lowered& L, const std::vector<double>& rot,
+                                    const std::vector<double>& tr, const std::vector<double>& pts) {
+  const NativeProblem& n = L.n;
+  ProbeProblem q;
+  std::vector<size_t> pose_intr;
+  single_pose_intrinsics(pr, &pose_intr);
+  const auto observed = observed_cameras(pr);
+  const size_t fallback = pr.observation_count ? pr.observation_intrinsic[0] : 0;
+  q.cameras.resize(n.ncam);
+  for (int c = 0; c < n.ncam; ++c) {
+    ProbeCamera& cam = q.cameras[c];
+    for (int k = 0; k < 9; ++k) cam.R[k] = rot[9 * (size_t)c + k];
+    const double* t = &tr[3 * (size_t)c];
+    for (int j = 0; j < 3; ++j) cam.C[j] = -(cam.R[j] * t[0] + cam.R[3 + j] * t[1] + cam.R[6 + j] * t[2]);
+    cam.fixed = n.fixed_poses[c] != 0;
+    const size_t src = L.rb.camera_source_order[c];
+    for (double& v : cam.intrinsics) v = 0.0;
+    if (!observed[src] && n.pixel_model) {
+      cam.intrinsics[0] = cam.intrinsics[1] = 1.0;  // PinholeCamera::new(1, 1, 0, 0)
+      continue;
+    }
+    const omvgba_intrinsic& in = pr.intrinsics[observed[src] ? pose_intr[src] : fallback];
+    cam.intrinsics[0] = in.fx;
+    cam.intrinsics[1] = in.fy;
+    cam.intrinsics[2] = in.cx;
+    cam.intrinsics[3] = in.cy;
+    if (!n.pixel_model && in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+      cam.intrinsics[4] = in.radial_kind >= 1 ? in.k1 : 0.0;
+      cam.intrinsics[5] = in.radial_kind >= 2 ? in.k2 : 0.0;
+      cam.intrinsics[6] = in.radial_kind >= 3 ? in.k3 : 0.0;
+      cam.intrinsics[7] = in.tangential_kind >= 1 ? in.p1 : 0.0;
+      cam.intrinsics[8] = in.tangential_kind >= 2 ? in.p2 : 0.0;
+    }
+  }
+  // tracks in the prepared point order (the lowering regroups points for locality; point_source maps
+  // them back), observations of a track in their input order
+  const size_t P = n.points.size() / 3;
+  std::vector<size_t> native_of(P);
+  for (size_t p = 0; p < P; ++p) native_of[n.point_source[p]] = p;
+  q.points.resize(3 * P);
+  q.track_off.assign(P + 1, 0);
+  for (size_t i = 0; i < P; ++i) {
+    const size_t p = native_of[i];
+    for (int k = 0; k < 3; ++k) q.points[3 * i + k] = pts[3 * p + k];
+    q.track_off[i + 1] = q.track_off[i] + (n.pt_off[p + 1] - n.pt_off[p]);
+  }
+  q.obs_cam.resize(q.track_off[P]);
+  q.obs_px.resize(2 * q.track_off[P]);
+  for (size_t i = 0; i < P; ++i) {
+    const size_t p = native_of[i];
+    uint64_t w = q.track_off[i];
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o, ++w) {
+      q.obs_cam[w] = n.obs_cam[o];
+      q.obs_px[2 * w] = n.obs_px[2 * o];
+      q.obs_px[2 * w + 1] = n.obs_px[2 * o + 1];
+    }
+  }
+  q.fixed_baseline = pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE;
+  q.anchor = 0;
+  q.scale_camera = (uint64_t)std::max(n.gauge_cam, 0);
+  if (q.fixed_baseline) {
+    const double* a = q.cameras[0].C;
+    const double* b = q.cameras[q.scale_camera].C;
+    const double d[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    q.distance = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  }
+  q.loss = problem_loss(pr);
+  return q;
+}
+
+// probe_prepared + native_preflight_from_probe (native/fixed_rotation.rs:50-202)
+omvgba_preflight preflight_from_prepared(Context* ctx, const omvgba_problem& pr, const Lowered& L,
+                                         const std::vector<double>& rot, const std::vector<double>& tr,
+                                         const std::vector<double>& pts) {
+  omvgba_probe_options opt;
+  probe_options_default(&opt);
+  omvgba_probe_report probe;
+  try {
+    probe = probe_fixed_rotation(ctx, prepared_probe_problem(pr, L, rot, tr, pts), opt);
+  } catch (const SolveFailure& f) {
+    if (f.code == OMVGBA_INVALID_PROBLEM || f.code == OMVGBA_INVALID_ARGUMENT) fail(OMVGBA_NUMERICAL, f.message);
+    throw;
+  }
+  uint64_t required = 0;
+  for (int c = 1; c < L.n.ncam; ++c) required += L.n.fixed_poses[c] ? 0 : 1;
+  omvgba_preflight out{};
+  out.has_counts = 1;
+  out.pose_dimension = probe.pose_dimension;
+  out.covered_free_pose_count = probe.covered_free_cameras;
+  out.weak_point_count = probe.weak_point_count;
+  switch (probe.status) {
+    case OMVGBA_PROBE_FULL_RANK_CERTIFIED: out.status = OMVGBA_PREFLIGHT_PROCEED; break;
+    case OMVGBA_PROBE_INSUFFICIENT_CAMERA_COVERAGE: out.status = OMVGBA_PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE; break;
+    case OMVGBA_PROBE_RESOURCE_LIMIT: out.status = OMVGBA_PREFLIGHT_RESOURCE_LIMIT; break;
+    case OMVGBA_PROBE_WEAK_POINT_GEOMETRY: out.status = OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY; break;
+    default:
+      if (probe.weak_point_count == 0 && probe.covered_free_cameras >= required) {
+        out.status = OMVGBA_PREFLIGHT_PROCEED;
+        out.dense_observability_escalation = 1;
+      } else {
+        out.status = OMVGBA_PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED;
+      }
+  }
+  return out;
+}
+
+// The probe a translation-only calibrated solve runs on its accepted geometry (native/mod.rs:435-447).
+bool wants_post_solve_probe(const omvgba_problem& pr, const NativeProblem& n) {
+  bool fixed_points = false;
+  for (size_t i = 0; i < pr.point_count && !fixed_points; ++i) fixed_points = point_fixed(pr, i);
+  return !n.self_cal && n.translation_only && !fixed_points && n.pixel_model && can_probe_scale_representative(pr) &&
+         n.gauge_cam >= 0;
+}
+
+// certified_observability and the probe's observability details (native/reporting.rs:24-134).
+void apply_preflight(const omvgba_problem& pr, const omvgba_preflight& pf, omvgba_report& r) {
+  const bool certifies =
+      pf.status == OMVGBA_PREFLIGHT_PROCEED && !pf.dense_observability_escalation && pf.weak_point_count == 0;
+  if (r.observability == OMVGBA_OBS_NOT_ASSESSED && certifies)
+    r.observability = pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE ? OMVGBA_OBS_FULL_RANK : OMVGBA_OBS_ONLY_EXPECTED_GAUGE;
+  const bool ranked = pf.status == OMVGBA_PREFLIGHT_PROCEED &&
+                      (!pf.dense_observability_escalation || r.observability == OMVGBA_OBS_FULL_RANK ||
+                       r.observability == OMVGBA_OBS_ONLY_EXPECTED_GAUGE);
+  if (pf.pose_dimension == 0) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  r.has_observability_details = 1;
+  r.details_pose_rank = ranked ? pf.pose_dimension : 0;
+  r.details_pose_dimension = pf.pose_dimension;
+  r.details_weak_point_count = pf.weak_point_count;
+}
+
+// NativeBundleAdjuster::preflight (native/mod.rs:184-230)
+omvgba_preflight preflight_check(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  validate_config(cfg);
+  omvgba_preflight none{};
+  none.status = OMVGBA_PREFLIGHT_PROCEED;
+  bool fixed_points = false;
+  for (size_t i = 0; i < pr.point_count && !fixed_points; ++i) fixed_points = point_fixed(pr, i);
+  if (common_pose_variables(pr) != 1 || pr.residual_space == OMVGBA_RESIDUAL_ANGULAR || fixed_points) return none;
+  if (has_free_intrinsics(pr)) fail(OMVGBA_UNSUPPORTED, "direct native lowering does not support self-calibration");
+  Lowered L = lower(pr);
+  std::vector<size_t> pose_intr;
+  if (L.n.gauge_cam < 0 || !single_pose_intrinsics(pr, &pose_intr) || !can_probe_scale_representative(pr))
+    return none;
+  std::vector<double> pts(L.n.points.begin(), L.n.points.end());
+  return preflight_from_prepared(ctx, pr, L, L.n.rotation, L.n.translation, pts);
+}
+
 Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
   const auto t0 = std::chrono::steady_clock::now();
@@ -1110,6 +1299,7 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
   Result res = raise(pr, L, rot, tr, pts, grp, nr, nr.iterative != 0);
   res.unconstrained = held;
   res.report.unconstrained_intrinsic_count = held.size();
+  if (wants_post_solve_probe(pr, L.n)) apply_preflight(pr, preflight_from_prepared(ctx, pr, L, rot, tr, pts), res.report);
   finish_solution(pr, res);
   canonicalize(pr, res);
   if (std::getenv("OMVGBA_PHASE_TIMES"))
@@ -1605,6 +1795,72 @@ int32_t omvgba_solve(omvgba_context* context, const omvgba_problem* problem, con
   }
 }
 
+void omvgba_probe_options_default(omvgba_probe_options* options) {
+  if (options) probe_options_default(options);
+}
+
+int32_t omvgba_probe_fixed_rotation(omvgba_context* context, const omvgba_fixed_rotation_problem* problem,
+                                    const omvgba_probe_options* options, omvgba_probe_report* report,
+                                    omvgba_error* error) {
+  clear_error(error);
+  if (!context || !problem || !options || !report) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  const omvgba_fixed_rotation_problem& fp = *problem;
+  const uint64_t nobs = (fp.track_offsets && fp.point_count) ? fp.track_offsets[fp.point_count] : 0;
+  if ((fp.camera_count && (!fp.rotations || !fp.centers || !fp.intrinsics || !fp.fixed_cameras)) ||
+      (fp.point_count && (!fp.points || !fp.track_offsets)) || (nobs && (!fp.observation_camera || !fp.observation_pixel)))
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null array");
+  try {
+    ProbeProblem q;
+    q.cameras.resize(fp.camera_count);
+    for (uint64_t c = 0; c < fp.camera_count; ++c) {
+      ProbeCamera& cam = q.cameras[c];
+      std::memcpy(cam.R, fp.rotations + 9 * c, sizeof(cam.R));
+      std::memcpy(cam.C, fp.centers + 3 * c, sizeof(cam.C));
+      std::memcpy(cam.intrinsics, fp.intrinsics + 9 * c, sizeof(cam.intrinsics));
+      cam.fixed = fp.fixed_cameras[c] != 0;
+    }
+    q.points.assign(fp.points, fp.points + 3 * fp.point_count);
+    if (fp.point_count) q.track_off.assign(fp.track_offsets, fp.track_offsets + fp.point_count + 1);
+    for (size_t k = 0; k + 1 < q.track_off.size(); ++k)
+      if (q.track_off[k + 1] < q.track_off[k] || q.track_off[k + 1] > nobs)
+        return write_error(error, OMVGBA_INVALID_PROBLEM, "fixed-rotation BA dimensions are inconsistent");
+    q.obs_cam.assign(fp.observation_camera, fp.observation_camera + nobs);
+    q.obs_px.assign(fp.observation_pixel, fp.observation_pixel + 2 * nobs);
+    q.fixed_baseline = fp.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE;
+    q.anchor = fp.anchor;
+    q.scale_camera = fp.scale_camera;
+    q.distance = fp.distance;
+    if (fp.loss_kind == OMVGBA_LOSS_SQUARED)
+      q.loss = {kLossL2, 0.0};
+    else if ((fp.loss_kind == OMVGBA_LOSS_HUBER || fp.loss_kind == OMVGBA_LOSS_CAUCHY) && std::isfinite(fp.loss_scale) &&
+             fp.loss_scale > 0.0)
+      q.loss = {fp.loss_kind == OMVGBA_LOSS_HUBER ? kLossHuber : kLossCauchy, fp.loss_scale};
+    else
+      return write_error(error, OMVGBA_INVALID_ARGUMENT, "invalid robust loss");
+    *report = probe_fixed_rotation(context->ctx, q, *options);
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
+int32_t omvgba_preflight_check(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
+                               omvgba_preflight* preflight, omvgba_error* error) {
+  clear_error(error);
+  if (!context || !problem || !config || !preflight) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  try {
+    validate_problem(*problem);
+    *preflight = preflight_check(context->ctx, *problem, *config);
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}
+
 // Windows solved concurrently by a pool of host threads, each with its own context and stream;
 // each window goes through exactly the omvgba_solve path, so its solution is the one omvgba_solve
 // returns for it alone, whichever worker takes it.
@@ -1838,6 +2094,8 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     Result first = raise(working, *lowered, rot, tr, pts, grp, nr, nr.iterative != 0);
     first.unconstrained = held;
     first.report.unconstrained_intrinsic_count = held.size();
+    if (wants_post_solve_probe(working, lowered->n))
+      apply_preflight(working, preflight_from_prepared(plan->ctx, working, *lowered, rot, tr, pts), first.report);
     laps[1] = seconds_since(t0);
     finish_solution(working, first);
     laps[2] = seconds_since(t0);

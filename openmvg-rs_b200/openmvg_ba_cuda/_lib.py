@@ -61,6 +61,14 @@ def lib():
     L.omvgba_plan_schur_product.restype = C.c_int32
     L.omvgba_plan_destroy.argtypes = [C.c_void_p]
     L.omvgba_device_count.restype = C.c_int32
+    L.omvgba_probe_options_default.argtypes = [C.POINTER(abi.ProbeOptions)]
+    L.omvgba_probe_fixed_rotation.argtypes = [C.c_void_p, C.POINTER(abi.FixedRotationProblem),
+                                              C.POINTER(abi.ProbeOptions), C.POINTER(abi.ProbeReport),
+                                              C.POINTER(abi.Error)]
+    L.omvgba_probe_fixed_rotation.restype = C.c_int32
+    L.omvgba_preflight_check.argtypes = [C.c_void_p, C.POINTER(abi.Problem), C.POINTER(abi.Config),
+                                         C.POINTER(abi.Preflight), C.POINTER(abi.Error)]
+    L.omvgba_preflight_check.restype = C.c_int32
     vp, u64 = C.c_void_p, C.c_uint64
     L.omvgba_residual_forward_f32.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, C.POINTER(abi.Error)]
     L.omvgba_residual_forward_f32.restype = C.c_int32

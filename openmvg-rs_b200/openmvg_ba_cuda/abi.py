@@ -275,3 +275,82 @@ class PlanInfo(C.Structure):
 
     def to_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class FixedRotationProblem(C.Structure):
+    """omvgba_fixed_rotation_problem (kernel/fixed_rotation/api.rs FixedRotationProblem)."""
+    _fields_ = [
+        ("camera_count", C.c_uint64),
+        ("rotations", C.POINTER(C.c_double)),
+        ("centers", C.POINTER(C.c_double)),
+        ("intrinsics", C.POINTER(C.c_double)),
+        ("fixed_cameras", C.POINTER(C.c_uint8)),
+        ("point_count", C.c_uint64),
+        ("points", C.POINTER(C.c_double)),
+        ("track_offsets", C.POINTER(C.c_uint64)),
+        ("observation_camera", C.POINTER(C.c_uint32)),
+        ("observation_pixel", C.POINTER(C.c_double)),
+        ("gauge_kind", C.c_int32),
+        ("anchor", C.c_uint64),
+        ("scale_camera", C.c_uint64),
+        ("distance", C.c_double),
+        ("loss_kind", C.c_int32),
+        ("loss_scale", C.c_double),
+    ]
+
+
+class ProbeOptions(C.Structure):
+    """omvgba_probe_options (FixedRotationObservabilityProbeOptions)."""
+    _fields_ = [
+        ("max_tracks", C.c_uint64),
+        ("max_observations", C.c_uint64),
+        ("max_observations_per_track", C.c_uint64),
+        ("max_coverage_observations_per_track", C.c_uint64),
+        ("max_reduced_nonzeros", C.c_uint64),
+        ("max_factor_nonzeros", C.c_uint64),
+        ("max_symbolic_dense_nonzeros", C.c_uint64),
+        ("minimum_normalized_eigenvalue", C.c_double),
+    ]
+
+
+class ProbeReport(C.Structure):
+    """omvgba_probe_report (FixedRotationObservabilityProbe)."""
+    _fields_ = [
+        ("status", C.c_int32),
+        ("reserved", C.c_int32),
+        ("pose_dimension", C.c_uint64),
+        ("selected_tracks", C.c_uint64),
+        ("selected_observations", C.c_uint64),
+        ("covered_free_cameras", C.c_uint64),
+        ("weak_point_count", C.c_uint64),
+        ("reduced_nonzeros", C.c_uint64),
+        ("factor_nonzeros", C.c_uint64),
+    ]
+
+    def to_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class Preflight(C.Structure):
+    """omvgba_preflight (NativePreflight)."""
+    _fields_ = [
+        ("status", C.c_int32),
+        ("has_counts", C.c_int32),
+        ("pose_dimension", C.c_uint64),
+        ("covered_free_pose_count", C.c_uint64),
+        ("weak_point_count", C.c_uint64),
+        ("dense_observability_escalation", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+    def to_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        if not d["has_counts"]:  # None in the reference's NativePreflight
+            d["pose_dimension"] = d["covered_free_pose_count"] = d["weak_point_count"] = None
+        return d
+
+
+PROBE_FULL_RANK_CERTIFIED, PROBE_INSUFFICIENT_CAMERA_COVERAGE, PROBE_RESOURCE_LIMIT = 0, 1, 2
+PROBE_WEAK_POINT_GEOMETRY, PROBE_SPARSE_FACTORIZATION_FAILED = 3, 4
+PREFLIGHT_PROCEED, PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE, PREFLIGHT_RESOURCE_LIMIT = 0, 1, 2
+PREFLIGHT_WEAK_POINT_GEOMETRY, PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED = 3, 4

@@ -34,6 +34,28 @@ class CudaBundleAdjuster:
         raise_for(code, err)
         return Solution.from_buffers(out)
 
+    def preflight(self, problem: BundleProblem, config: SolveConfig | None = None) -> dict:
+        """``NativeBundleAdjuster::preflight`` (native/mod.rs:184-230): the translation-only
+        observability probe on the prepared problem, or PROCEED with no counts for other problems."""
+        config = config or SolveConfig()
+        mp = abi.MarshalledProblem(problem)
+        cfg = config.to_struct()
+        out, err = abi.Preflight(), abi.Error()
+        code = lib().omvgba_preflight_check(self._ctx, C.byref(mp.struct), C.byref(cfg), C.byref(out), C.byref(err))
+        raise_for(code, err)
+        return out.to_dict()
+
+    def probe_fixed_rotation(self, problem, options=None) -> dict:
+        """``probe_fixed_rotation_observability`` (kernel/fixed_rotation/observability.rs:24-262) of a
+        ``fixed_rotation.FixedRotationProblem``."""
+        from .fixed_rotation import ProbeOptions
+        opts = (options or ProbeOptions()).to_struct()
+        fp = problem.to_struct()
+        out, err = abi.ProbeReport(), abi.Error()
+        code = lib().omvgba_probe_fixed_rotation(self._ctx, C.byref(fp), C.byref(opts), C.byref(out), C.byref(err))
+        raise_for(code, err)
+        return out.to_dict()
+
     def debug_linearize(self, problem: BundleProblem, config: SolveConfig | None = None) -> dict:
         config = config or SolveConfig()
         mp = abi.MarshalledProblem(problem)

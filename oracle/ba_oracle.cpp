@@ -31,6 +31,7 @@
 
 #include "../include/ba_cuda.h"
 #include "oracle_core.hpp"
+#include "fixed_rotation_probe.hpp"
 
 // Phase timer printed to stderr when OMVGBA_ORACLE_TIMES is set (diagnostics only).
 static double oracle_now() {
@@ -67,6 +68,14 @@ struct Native {
   std::vector<Vec3> points;
   std::vector<uint8_t> fixed_points;
   std::vector<uint8_t> fixed_poses;  // native camera order
+  // Calibrated solves carry explicit per-camera pose masks (native camera order; bit 0 rotation, bit 1
+  // translation, 0 fixed): the block of camera c has 3 rotation and 3 (2 on the baseline camera)
+  // translation coordinates as its mask allows, camera 0 included
+  // (workspace/topology.rs:305-347). Self-calibration keeps the legacy layout: camera 0 fixed, every
+  // other camera full or fixed (topology.rs:364-380).
+  bool explicit_masks = false;
+  std::vector<uint8_t> pose_mask;
+  bool translation_only = false;  // CameraPoseVariables::TranslationOnly (calibrated)
   std::vector<uint32_t> obs_cam;
   std::vector<Vec2> obs_px;
   std::vector<uint64_t> obs_src;
@@ -120,7 +129,13 @@ static Layout make_layout(const Native& n) {
   L.pose_dim.resize(n.ncam);
   int off = 0;
   for (int c = 0; c < n.ncam; ++c) {
-    int d = (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+    int d;
+    if (n.explicit_masks) {
+      const int m = n.pose_mask[c];
+      d = (n.fixed_poses[c] || m == 0) ? 0 : 3 * (m & 1) + ((m & 2) ? (c == n.gauge_cam ? 2 : 3) : 0);
+    } else {
+      d = (c == 0 || n.fixed_poses[c]) ? 0 : (c == n.gauge_cam ? 5 : 6);
+    }
     L.pose_off[c] = off;
     L.pose_dim[c] = d;
     off += d;
@@ -321,6 +336,35 @@ static void pose_motion(const Vec3& r, int cam, const GaugeState& g, double m[3]
   }
 }
 
+// The pose columns of one observation's camera Jacobian (schur/point.rs:286-313): a block without
+// rotation moves only its translation (translation_motion, point.rs:764-786); a block with rotation
+// uses pose_motion at the rotated point RX, or, when the translation is held, at the camera point
+// RX + t, since then the camera turns about its fixed centre. J is the 2 x 3 projection Jacobian.
+static int pose_columns(const Native& n, const Layout& L, const GaugeState& g, int cam, const Vec3& rot,
+                        const Vec3& xc, const Mat23& J, double Jc[2][9]) {
+  const int pd = L.pose_dim[cam];
+  if (pd == 0) return 0;
+  const int mask = n.explicit_masks ? n.pose_mask[cam] : 3;
+  double m[3][6];
+  if (!(mask & 1)) {
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 6; ++c) m[r][c] = 0.0;
+    if (g.fixed_camera == cam) {
+      for (int c = 0; c < 3; ++c) {
+        m[c][0] = g.baseline * g.basis[0][c];
+        m[c][1] = g.baseline * g.basis[1][c];
+      }
+    } else {
+      for (int c = 0; c < 3; ++c) m[c][c] = g.scene_scale;
+    }
+  } else {
+    pose_motion((mask & 2) ? rot : xc, cam, g, m);
+  }
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < pd; ++c) Jc[r][c] = J[r][0] * m[0][c] + J[r][1] * m[1][c] + J[r][2] * m[2][c];
+  return pd;
+}
+
 // Shard-local assembly output, combined in shard order (retained/parallel.rs:15-31).
 struct ShardOut {
   std::vector<double> grad, full_grad, diag;
@@ -380,11 +424,7 @@ static void assemble_range(const Native& n, const std::vector<NPose>& poses, con
       double Jc[2][9] = {};
       int params[9];
       if (pd > 0) {
-        double m[3][6];
-        pose_motion(rot, cam, g, m);
-        for (int r = 0; r < 2; ++r)
-          for (int c = 0; c < pd; ++c)
-            Jc[r][c] = ol.p.jacobian[r][0] * m[0][c] + ol.p.jacobian[r][1] * m[1][c] + ol.p.jacobian[r][2] * m[2][c];
+        pose_columns(n, L, g, cam, rot, xc, ol.p.jacobian, Jc);
         for (int k = 0; k < pd; ++k) params[k] = L.pose_off[cam] + k;
       }
       if (id > 0) {
@@ -1053,11 +1093,7 @@ static void band_point_terms(const Native& n, const Layout& L, const std::vector
     ObsRows orow{};
     double Jc[2][9] = {};
     if (pd > 0) {
-      double m[3][6];
-      pose_motion(rot, cam, g, m);
-      for (int r = 0; r < 2; ++r)
-        for (int c = 0; c < pd; ++c)
-          Jc[r][c] = ol.p.jacobian[r][0] * m[0][c] + ol.p.jacobian[r][1] * m[1][c] + ol.p.jacobian[r][2] * m[2][c];
+      pose_columns(n, L, g, cam, rot, xc, ol.p.jacobian, Jc);
       for (int k = 0; k < pd; ++k) orow.params[k] = L.pose_off[cam] + k;
     }
     for (int r = 0; r < 2; ++r)
@@ -1446,21 +1482,32 @@ static NativeReport refine(const Native& n, std::vector<NPose>& poses, std::vect
           for (auto& v : step) v *= sc;
         }
       }
-      for (int c = 0; c < n.ncam; ++c) {  // retract_poses (optimizer.rs:376-424)
+      // retract_poses_with_masks (optimizer.rs:442-510); with every mask full it is retract_poses
+      // (optimizer.rs:376-424)
+      for (int c = 0; c < n.ncam; ++c) {
         int d = L.pose_dim[c], o = L.pose_off[c];
         if (d == 0) {
           cand_poses[c] = poses[c];
           continue;
         }
-        Mat3 up = exp_so3({step[o], step[o + 1], step[o + 2]});
+        const int mask = n.explicit_masks ? n.pose_mask[c] : 3;
+        Mat3 R = poses[c].R, up{};
+        int ts = 0;
+        if (mask & 1) {
+          up = exp_so3({step[o], step[o + 1], step[o + 2]});
+          R = mat_mul(up, poses[c].R);
+          ts = 3;
+        }
         Vec3 t;
-        if (g.fixed_camera == c) {
-          Vec3 dir = retract_s2(g.direction, g.basis, step[o + 3], step[o + 4]);
+        if (!(mask & 2)) {  // t' = Exp(w) t keeps the centre -R^T t
+          t = (mask & 1) ? rotate(up, poses[c].t) : poses[c].t;
+        } else if (g.fixed_camera == c) {
+          Vec3 dir = retract_s2(g.direction, g.basis, step[o + ts], step[o + ts + 1]);
           t = {g.baseline * dir[0], g.baseline * dir[1], g.baseline * dir[2]};
         } else {
-          for (int k = 0; k < 3; ++k) t[k] = poses[c].t[k] + g.scene_scale * step[o + 3 + k];
+          for (int k = 0; k < 3; ++k) t[k] = poses[c].t[k] + g.scene_scale * step[o + ts + k];
         }
-        cand_poses[c] = {mat_mul(up, poses[c].R), t};
+        cand_poses[c] = {R, t};
       }
       if (n.self_cal)
         for (size_t gi = 0; gi < groups.size(); ++gi) {  // retract_cameras (self_calibration/optimizer.rs:565-587)
@@ -1987,19 +2034,15 @@ static Native lower_calibrated(const omvgba_problem& pr) {
   }
   GaugePlan plan = calibrated_gauge_plan(pr);
   auto observed = observed_cameras(pr);
-  bool any_free = false, translation_only = true;
-  for (size_t i = 0; i < pr.pose_count; ++i) {
-    uint32_t m = plan.masks[i];
-    if (m == 0) continue;
-    any_free = true;
-    if (m != OMVGBA_POSE_FREE)
-      fail(OMVGBA_UNSUPPORTED, "partial pose-variable masks (rotation-only or translation-only) are not supported by this adjuster");
-    if (m & OMVGBA_POSE_ROTATION) translation_only = false;
-  }
-  (void)any_free;
-  (void)translation_only;
+  // CameraPoseVariables of the prepared problem (native/calibrated.rs:226-234): translation-only when
+  // no free mask moves a rotation (vacuously so when every pose is fixed)
+  bool translation_only = true;
+  for (size_t i = 0; i < pr.pose_count; ++i)
+    if (plan.masks[i] != 0 && (plan.masks[i] & OMVGBA_POSE_ROTATION)) translation_only = false;
   Native n;
   n.self_cal = false;
+  n.explicit_masks = true;
+  n.translation_only = translation_only;
   set_anchor(pr, n, plan.anchor, plan.scale);
   n.ncam = (int)pr.pose_count;
   std::vector<size_t> dest(pr.pose_count);
@@ -2008,6 +2051,8 @@ static Native lower_calibrated(const omvgba_problem& pr) {
     size_t s = n.camera_source_order[d];
     n.poses.push_back(observed[s] ? pose_to_native(n, pr.poses[s]) : NPose{{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, {0, 0, 0}});
     n.fixed_poses.push_back(plan.masks[s] == 0);
+    n.pose_mask.push_back((uint8_t)((plan.masks[s] & OMVGBA_POSE_ROTATION ? 1 : 0) |
+                                    (plan.masks[s] & OMVGBA_POSE_TRANSLATION ? 2 : 0)));
   }
   std::vector<uint8_t> pobs(pr.point_count, 0);
   for (size_t o = 0; o < pr.observation_count; ++o) pobs[pr.observation_point[o]] = 1;
@@ -2484,6 +2529,9 @@ static bool auto_prefers_direct(const Native& n, const Layout& L, uint64_t budge
 static bool choose_iterative(const omvgba_config& cfg, const Native& n, const Layout& L) {
   if (cfg.linear_solver == OMVGBA_SOLVER_DIRECT) return false;
   if (cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE) return true;
+  // a translation-only solve resolves Auto to the direct solver, so its final rank is exact
+  // (native/mod.rs:398-407)
+  if (!n.self_cal && n.translation_only) return false;
   uint64_t de = 0, ce = 0;
   return !auto_prefers_direct(n, L, cfg.has_workspace_budget ? cfg.workspace_budget_bytes : 0, &de, &ce);
 }
@@ -2502,6 +2550,153 @@ static void check_workspace_budget(const omvgba_config& cfg, const Native& n, co
   if (bytes > cfg.workspace_budget_bytes)
     fail(OMVGBA_RESOURCE_EXHAUSTED, "workspace " + std::to_string(bytes) + " bytes exceeds the workspace budget " +
                                         std::to_string(cfg.workspace_budget_bytes));
+}
+
+// ---- translation-only observability (native/fixed_rotation.rs, native/mod.rs:184-230, 435-447,
+// native/reporting.rs:24-134) ----------------------------------------------------------------------
+struct Preflight {
+  int status = OMVGBA_PREFLIGHT_PROCEED;
+  bool has_counts = false;
+  uint64_t pose_dimension = 0, covered = 0, weak = 0;
+  bool escalation = false;
+};
+
+// common_pose_variables (native/gauge.rs:9-40): 1 translation-only, 0 rotation and translation, -1
+// an unsupported mixture
+static int common_pose_variables(const omvgba_problem& pr) {
+  auto observed = observed_cameras(pr);
+  int selected = -1;
+  for (size_t i = 0; i < pr.pose_count; ++i) {
+    uint32_t v = pr.poses[i].variables;
+    if (!observed[i] || v == 0) continue;
+    if (!(v & OMVGBA_POSE_TRANSLATION)) return -1;
+    int cand = (v & OMVGBA_POSE_ROTATION) ? 0 : 1;
+    if (selected >= 0 && selected != cand) return -1;
+    selected = cand;
+  }
+  return selected < 0 ? 0 : selected;
+}
+
+// can_probe_scale_representative (native/mod.rs:510-521)
+static bool can_probe_scale_representative(const omvgba_problem& pr) {
+  if (pr.gauge_kind != OMVGBA_GAUGE_FIXED_BASELINE) return true;
+  auto observed = observed_cameras(pr);
+  Vec3 f = pose_C(pr.poses[pr.gauge_first]);
+  for (size_t c = 0; c < pr.pose_count; ++c)
+    if (c != pr.gauge_first && observed[c] && !(pr.poses[c].variables & OMVGBA_POSE_TRANSLATION) &&
+        pose_C(pr.poses[c]) != f)
+      return false;
+  return true;
+}
+
+// probe_prepared (native/fixed_rotation.rs:50-165) on the native state poses / points
+static Preflight probe_prepared(const omvgba_problem& pr, const Native& n, const std::vector<NPose>& poses,
+                                const std::vector<Vec3>& points) {
+  FrProblem q;
+  std::vector<size_t> pose_intr;
+  single_pose_intrinsics(pr, &pose_intr);
+  auto observed = observed_cameras(pr);
+  const size_t fallback = pr.observation_count ? pr.observation_intrinsic[0] : 0;
+  for (int c = 0; c < n.ncam; ++c) {
+    const NPose& P = poses[c];
+    q.rotations.push_back(P.R);
+    Vec3 C = rotate_transposed(P.R, P.t);
+    q.centers.push_back({-C[0], -C[1], -C[2]});
+    q.fixed_cameras.push_back(n.fixed_poses[c]);
+    const size_t src = n.camera_source_order[c];
+    FrIntrinsics k{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (!observed[src] && n.pixel_model) {
+      k.fx = k.fy = 1.0;
+    } else {
+      const omvgba_intrinsic& in = pr.intrinsics[observed[src] ? pose_intr[src] : fallback];
+      k.fx = in.fx;
+      k.fy = in.fy;
+      k.cx = in.cx;
+      k.cy = in.cy;
+      if (!n.pixel_model && in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+        k.k1 = in.radial_kind >= 1 ? in.k1 : 0.0;
+        k.k2 = in.radial_kind >= 2 ? in.k2 : 0.0;
+        k.k3 = in.radial_kind >= 3 ? in.k3 : 0.0;
+        k.p1 = in.tangential_kind >= 1 ? in.p1 : 0.0;
+        k.p2 = in.tangential_kind >= 2 ? in.p2 : 0.0;
+      }
+    }
+    q.intrinsics.push_back(k);
+  }
+  q.points = points;
+  q.tracks.resize(points.size());
+  for (size_t p = 0; p < points.size(); ++p)
+    for (uint64_t o = n.pt_off[p]; o < n.pt_off[p + 1]; ++o) q.tracks[p].push_back({n.obs_cam[o], n.obs_px[o][0], n.obs_px[o][1]});
+  q.anchor = 0;
+  q.scale_camera = (size_t)std::max(n.gauge_cam, 0);
+  q.fixed_baseline = pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE;
+  if (q.fixed_baseline) {
+    const Vec3& a = q.centers[0];
+    const Vec3& b = q.centers[q.scale_camera];
+    q.distance = std::sqrt(sqdist(b, a));
+  }
+  FrReport rep;
+  try {
+    rep = fr_probe(q, problem_loss(pr), FrOptions{});
+  } catch (const FrError& e) {
+    fail(OMVGBA_NUMERICAL, e.message);
+  }
+  uint64_t required = 0;
+  for (int c = 1; c < n.ncam; ++c) required += n.fixed_poses[c] ? 0 : 1;
+  Preflight out;
+  out.has_counts = true;
+  out.pose_dimension = rep.pose_dimension;
+  out.covered = rep.covered_free_cameras;
+  out.weak = rep.weak_point_count;
+  switch (rep.status) {  // native_preflight_from_probe (native/fixed_rotation.rs:167-202)
+    case kFrCertified: out.status = OMVGBA_PREFLIGHT_PROCEED; break;
+    case kFrCoverage: out.status = OMVGBA_PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE; break;
+    case kFrResource: out.status = OMVGBA_PREFLIGHT_RESOURCE_LIMIT; break;
+    case kFrWeak: out.status = OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY; break;
+    default:
+      if (rep.weak_point_count == 0 && rep.covered_free_cameras >= required) {
+        out.status = OMVGBA_PREFLIGHT_PROCEED;
+        out.escalation = true;
+      } else {
+        out.status = OMVGBA_PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED;
+      }
+  }
+  return out;
+}
+
+// certified_observability and the probe's details (native/reporting.rs:24-134)
+static void apply_preflight(const omvgba_problem& pr, const Preflight& pf, omvgba_report& r) {
+  if (r.observability == OMVGBA_OBS_NOT_ASSESSED && pf.status == OMVGBA_PREFLIGHT_PROCEED && !pf.escalation &&
+      pf.weak == 0)
+    r.observability = pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE ? OMVGBA_OBS_FULL_RANK : OMVGBA_OBS_ONLY_EXPECTED_GAUGE;
+  const bool ranked = pf.status == OMVGBA_PREFLIGHT_PROCEED &&
+                      (!pf.escalation || r.observability == OMVGBA_OBS_FULL_RANK ||
+                       r.observability == OMVGBA_OBS_ONLY_EXPECTED_GAUGE);
+  if (pf.pose_dimension == 0) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  r.has_observability_details = 1;
+  r.details_pose_rank = ranked ? pf.pose_dimension : 0;
+  r.details_pose_dimension = pf.pose_dimension;
+  r.details_weak_point_count = pf.weak;
+}
+
+static bool wants_post_solve_probe(const omvgba_problem& pr, const Native& n) {
+  bool fixed_points = false;
+  for (size_t i = 0; i < pr.point_count; ++i) fixed_points = fixed_points || point_fixed(pr, i);
+  return !n.self_cal && n.translation_only && !fixed_points && n.pixel_model && can_probe_scale_representative(pr) &&
+         n.gauge_cam >= 0;
+}
+
+// NativeBundleAdjuster::preflight (native/mod.rs:184-230)
+static Preflight preflight(const omvgba_problem& pr, const omvgba_config& cfg) {
+  validate_config(cfg);
+  bool fixed_points = false;
+  for (size_t i = 0; i < pr.point_count; ++i) fixed_points = fixed_points || point_fixed(pr, i);
+  if (common_pose_variables(pr) != 1 || pr.residual_space == OMVGBA_RESIDUAL_ANGULAR || fixed_points) return {};
+  if (has_free_intrinsics(pr)) fail(OMVGBA_UNSUPPORTED, "direct native lowering does not support self-calibration");
+  Native n = lower_calibrated(pr);
+  std::vector<size_t> pose_intr;
+  if (n.gauge_cam < 0 || !single_pose_intrinsics(pr, &pose_intr) || !can_probe_scale_representative(pr)) return {};
+  return probe_prepared(pr, n, n.poses, n.points);
 }
 
 static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
@@ -2548,6 +2743,7 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   Result res = raise(pr, n, poses, points, groups, nr, opt.iterative);
   res.unconstrained = held;
   res.report.unconstrained_intrinsic_count = held.size();
+  if (wants_post_solve_probe(pr, n)) apply_preflight(pr, probe_prepared(pr, n, poses, points), res.report);
   finish_solution(pr, res);
   canonicalize(pr, res);
   oracle_phase("report", t0);
@@ -2876,6 +3072,82 @@ int omvgba_oracle_iteration_seconds(double* out, int cap) {
   return n;
 }
 
+// The oracle's preflight (NativeBundleAdjuster::preflight) and its kernel-level probe.
+int omvgba_oracle_preflight(const omvgba_problem* problem, const omvgba_config* config, omvgba_preflight* out,
+                            omvgba_error* error) {
+  try {
+    oracle::validate_problem(*problem);
+    oracle::Preflight pf = oracle::preflight(*problem, *config);
+    std::memset(out, 0, sizeof(*out));
+    out->status = pf.status;
+    out->has_counts = pf.has_counts ? 1 : 0;
+    out->pose_dimension = pf.pose_dimension;
+    out->covered_free_pose_count = pf.covered;
+    out->weak_point_count = pf.weak;
+    out->dense_observability_escalation = pf.escalation ? 1 : 0;
+    return OMVGBA_OK;
+  } catch (const oracle::SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
+}
+
+int omvgba_oracle_probe_fixed_rotation(const omvgba_fixed_rotation_problem* fp, const omvgba_probe_options* opt,
+                                       omvgba_probe_report* out, omvgba_error* error) {
+  try {
+    oracle::FrProblem q;
+    for (uint64_t c = 0; c < fp->camera_count; ++c) {
+      oracle::Mat3 R;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R[i][j] = fp->rotations[9 * c + 3 * i + j];
+      q.rotations.push_back(R);
+      q.centers.push_back({fp->centers[3 * c], fp->centers[3 * c + 1], fp->centers[3 * c + 2]});
+      const double* k = fp->intrinsics + 9 * c;
+      q.intrinsics.push_back({k[0], k[1], k[2], k[3], k[4], k[5], k[6], k[7], k[8]});
+      q.fixed_cameras.push_back(fp->fixed_cameras[c] ? 1 : 0);
+    }
+    for (uint64_t p = 0; p < fp->point_count; ++p) {
+      q.points.push_back({fp->points[3 * p], fp->points[3 * p + 1], fp->points[3 * p + 2]});
+      std::vector<oracle::FrObservation> t;
+      for (uint64_t o = fp->track_offsets[p]; o < fp->track_offsets[p + 1]; ++o)
+        t.push_back({fp->observation_camera[o], fp->observation_pixel[2 * o], fp->observation_pixel[2 * o + 1]});
+      q.tracks.push_back(t);
+    }
+    q.fixed_baseline = fp->gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE;
+    q.anchor = fp->anchor;
+    q.scale_camera = fp->scale_camera;
+    q.distance = fp->distance;
+    oracle::Loss loss;
+    loss.kind = fp->loss_kind == OMVGBA_LOSS_HUBER ? oracle::LossKind::Huber
+                                                    : (fp->loss_kind == OMVGBA_LOSS_CAUCHY ? oracle::LossKind::Cauchy
+                                                                                            : oracle::LossKind::L2);
+    loss.scale = fp->loss_scale;
+    oracle::FrOptions o;
+    o.max_tracks = opt->max_tracks;
+    o.max_observations = opt->max_observations;
+    o.max_observations_per_track = opt->max_observations_per_track;
+    o.max_coverage_observations_per_track = opt->max_coverage_observations_per_track;
+    o.max_reduced_nonzeros = opt->max_reduced_nonzeros;
+    o.max_factor_nonzeros = opt->max_factor_nonzeros;
+    o.max_symbolic_dense_nonzeros = opt->max_symbolic_dense_nonzeros;
+    o.minimum_normalized_eigenvalue = opt->minimum_normalized_eigenvalue;
+    oracle::FrReport r = oracle::fr_probe(q, loss, o);
+    std::memset(out, 0, sizeof(*out));
+    out->status = r.status;
+    out->pose_dimension = r.pose_dimension;
+    out->selected_tracks = r.selected_tracks;
+    out->selected_observations = r.selected_observations;
+    out->covered_free_cameras = r.covered_free_cameras;
+    out->weak_point_count = r.weak_point_count;
+    out->reduced_nonzeros = r.reduced_nonzeros;
+    out->factor_nonzeros = r.factor_nonzeros;
+    return OMVGBA_OK;
+  } catch (const oracle::FrError& e) {
+    return write_error(error, e.code, e.message);
+  } catch (const oracle::SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  }
+}
+
 // The oracle's execution plan: the linear solver it would use (Auto resolved) and its estimates.
 int omvgba_oracle_execution_plan(const omvgba_problem* problem, const omvgba_config* config, int32_t* iterative,
                                  uint64_t* direct_estimate, uint64_t* cached_estimate, omvgba_error* error) {
@@ -2903,8 +3175,8 @@ int omvgba_oracle_execution_plan(const omvgba_problem* problem, const omvgba_con
     oracle::Layout L = oracle::make_layout(n);
     const bool direct = oracle::auto_prefers_direct(
         n, L, config->has_workspace_budget ? config->workspace_budget_bytes : 0, direct_estimate, cached_estimate);
-    *iterative = config->linear_solver == OMVGBA_SOLVER_AUTO ? !direct
-                                                             : config->linear_solver == OMVGBA_SOLVER_ITERATIVE;
+    *iterative = oracle::choose_iterative(*config, n, L) ? 1 : 0;
+    (void)direct;
     return OMVGBA_OK;
   } catch (const oracle::SolveFailure& f) {
     return write_error(error, f.code, f.message);
@@ -2984,12 +3256,10 @@ int32_t omvgba_oracle_debug_linearize(const omvgba_problem* problem, const omvgb
                 g.scene_scale;
         int pd = L.pose_dim[cam];
         if (pd > 0) {
-          double m[3][6];
-          pose_motion(rot, cam, g, m);
+          double Jc[2][9] = {};
+          pose_columns(n, L, g, cam, rot, xc, ol.p.jacobian, Jc);
           for (int r = 0; r < 2; ++r)
-            for (int c = 0; c < pd; ++c)
-              camera_jacobian[18 * o + 9 * r + c] =
-                  ol.p.jacobian[r][0] * m[0][c] + ol.p.jacobian[r][1] * m[1][c] + ol.p.jacobian[r][2] * m[2][c];
+            for (int c = 0; c < pd; ++c) camera_jacobian[18 * o + 9 * r + c] = Jc[r][c];
         }
         if (n.self_cal) {
           int grp = n.cam_group[cam];

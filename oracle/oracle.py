@@ -60,6 +60,13 @@ def lib():
         L.omvgba_oracle_point_block_inverse.argtypes = [dp, C.c_double, dp, dp]
         L.omvgba_oracle_point_block_inverse.restype = C.c_int
         L.omvgba_oracle_stages.argtypes = [C.c_int, C.c_uint64, C.POINTER(C.c_uint64), ip]
+        L.omvgba_oracle_preflight.argtypes = [C.POINTER(abi.Problem), C.POINTER(abi.Config), C.POINTER(abi.Preflight),
+                                              C.POINTER(abi.Error)]
+        L.omvgba_oracle_preflight.restype = C.c_int
+        L.omvgba_oracle_probe_fixed_rotation.argtypes = [C.POINTER(abi.FixedRotationProblem),
+                                                         C.POINTER(abi.ProbeOptions), C.POINTER(abi.ProbeReport),
+                                                         C.POINTER(abi.Error)]
+        L.omvgba_oracle_probe_fixed_rotation.restype = C.c_int
         u32p = C.POINTER(C.c_uint32)
         L.omvgba_oracle_residual_vjp.argtypes = [C.c_uint64, u32p, u32p, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
         _lib = L
@@ -150,3 +157,26 @@ def execution_plan(problem, config):
                                               C.byref(ce), C.byref(err))
     raise_for(code, err)
     return bool(it.value), int(de.value), int(ce.value)
+
+
+def preflight(problem, config):
+    """The oracle's NativeBundleAdjuster::preflight (dict of the NativePreflight fields)."""
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.problem import raise_for
+    mp = abi.MarshalledProblem(problem)
+    cfg = config.to_struct()
+    out, err = abi.Preflight(), abi.Error()
+    raise_for(lib().omvgba_oracle_preflight(C.byref(mp.struct), C.byref(cfg), C.byref(out), C.byref(err)), err)
+    return out.to_dict()
+
+
+def probe_fixed_rotation(problem, options=None):
+    """The oracle's probe_fixed_rotation_observability of a fixed_rotation.FixedRotationProblem."""
+    from openmvg_ba_cuda import abi
+    from openmvg_ba_cuda.fixed_rotation import ProbeOptions
+    from openmvg_ba_cuda.problem import raise_for
+    opts = (options or ProbeOptions()).to_struct()
+    fp = problem.to_struct()
+    out, err = abi.ProbeReport(), abi.Error()
+    raise_for(lib().omvgba_oracle_probe_fixed_rotation(C.byref(fp), C.byref(opts), C.byref(out), C.byref(err)), err)
+    return out.to_dict()

@@ -336,6 +336,26 @@ def kernel_roofline(plan, info: dict, stream, flush, workload: str, launches: in
             "algorithmic_bytes_per_launch": algorithmic, "avg_launch_us": avg_s * 1e6, "launches_timed": launches}
 
 
+def rows_timing(plan, info: dict, stream, flush, launches: int = 20) -> dict:
+    """Average duration of k_block_rows, the block-row build of the explicit reduced camera system
+    from the current linearization (CUDA events on the plan's stream, L2 flushed before each launch)."""
+    import torch
+    D = int(info["reduced_dimension"])
+    x = torch.zeros(D, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(launches):
+        with torch.cuda.stream(stream):
+            flush.fill_(3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.schur_product(x.data_ptr(), x.data_ptr(), 0.1, fp32=True, stage=2)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return {"kernel": "k_block_rows", "avg_launch_us": total / launches * 1e3, "launches_timed": launches}
+
+
 def run_batched(args) -> int:
     """windows256: LM iterations/s summed over the windows of one omvgba_solve_batched call, timed
     on the host clock around the synchronous call (its workers run on their own streams), with the
@@ -536,13 +556,14 @@ def run_ours(args) -> int:
     # value: mixed precision, problem resident in device memory
     plan = adjuster.plan(problem, mixed_cfg)
     info = plan.info()
-    if args.legs == "kernel":  # the product kernel's timing alone, no solve (for a small ncu capture)
+    if args.legs == "kernel":  # the kernels' timings alone, no solve (for a small ncu capture)
         roofline = kernel_roofline(plan, info, stream, flush, args.workload, launches=max(args.steps, 3))
+        rows = rows_timing(plan, info, stream, flush, launches=max(args.steps, 3))
         plan.close()
         adjuster.close()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "legs": "kernel", "n_gpus": world, "roofline": roofline,
-                              "observations": int(info["observation_count"])}), flush=True)
+                              "explicit_rows": rows, "observations": int(info["observation_count"])}), flush=True)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

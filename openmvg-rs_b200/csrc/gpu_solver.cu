@@ -3637,6 +3637,8 @@ void resident_schur_product(Resident* r, double lambda, bool fp32, int stage, co
   }
   if (stage == 1)
     s.matvec_tiles(x, nullptr, fp32);
+  else if (stage == 2)
+    s.build_rows();
   else
     s.matvec(x, y, lambda, nullptr, fp32);
   s.check_launch();

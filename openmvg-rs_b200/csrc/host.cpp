@@ -2145,7 +2145,7 @@ int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32
                                   double* y, omvgba_error* error) {
   clear_error(error);
   if (!plan || !x || (stage == 0 && !y)) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
-  if (stage != 0 && stage != 1) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0 or 1");
+  if (stage < 0 || stage > 2) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0, 1 or 2");
   if (!(std::isfinite(lambda) && lambda >= 0.0))
     return write_error(error, OMVGBA_INVALID_ARGUMENT, "lambda must be finite and non-negative");
   try {

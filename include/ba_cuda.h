@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OMVGBA_ABI_VERSION 2u
+#define OMVGBA_ABI_VERSION 3u
 
 /* ---- return codes (SolveError, solver.rs:1474-1493; ProblemError, problem.rs:731) ---- */
 enum omvgba_code {
@@ -57,7 +57,14 @@ enum omvgba_camera_model {
   OMVGBA_CAMERA_SPHERICAL = 3  /* idem */
 };
 /* RadialDistortion discriminant: None, K1, K1K2, K1K2K3 (distortion.rs:183-241) */
-enum omvgba_radial_kind { OMVGBA_RADIAL_NONE = 0, OMVGBA_RADIAL_K1 = 1, OMVGBA_RADIAL_K1K2 = 2, OMVGBA_RADIAL_K1K2K3 = 3 };
+/* Brown-Conrady RadialDistortion, or the fisheye's FisheyeDistortion (K1K2K3K4 is fisheye only). */
+enum omvgba_radial_kind {
+  OMVGBA_RADIAL_NONE = 0,
+  OMVGBA_RADIAL_K1 = 1,
+  OMVGBA_RADIAL_K1K2 = 2,
+  OMVGBA_RADIAL_K1K2K3 = 3,
+  OMVGBA_RADIAL_K1K2K3K4 = 4
+};
 /* TangentialDistortion discriminant: None, P1, P1P2 (distortion.rs:459-527) */
 enum omvgba_tangential_kind { OMVGBA_TANGENTIAL_NONE = 0, OMVGBA_TANGENTIAL_P1 = 1, OMVGBA_TANGENTIAL_P1P2 = 2 };
 
@@ -82,14 +89,15 @@ typedef struct omvgba_pose {
 /* BundleIntrinsic: CameraIntrinsics + IntrinsicVariables + IntrinsicCertification. */
 typedef struct omvgba_intrinsic {
   int32_t model;            /* omvgba_camera_model */
-  int32_t radial_kind;      /* omvgba_radial_kind (Brown-Conrady only) */
+  int32_t radial_kind;      /* omvgba_radial_kind (Brown-Conrady and fisheye) */
   int32_t tangential_kind;  /* omvgba_tangential_kind (Brown-Conrady only) */
   uint32_t variables;       /* OMVGBA_INTRINSIC_* bits */
   int32_t certification;    /* 0 Required, 1 Waived */
   int32_t fixed_model;      /* CameraIntrinsics::is_fixed(): 1 forbids variable coordinates */
   double fx, fy, cx, cy;
   double k1, k2, k3, p1, p2;
-  uint32_t width, height;
+  uint32_t width, height;   /* spherical: width (even), height = width / 2 */
+  double k4;                /* fisheye K1K2K3K4 only */
 } omvgba_intrinsic;
 
 enum omvgba_residual_space { OMVGBA_RESIDUAL_PIXELS = 0, OMVGBA_RESIDUAL_ANGULAR = 1 };

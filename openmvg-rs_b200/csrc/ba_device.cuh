@@ -179,15 +179,28 @@ struct FixedCameraDev {
   }
   // remove_validated_distortion (distortion.rs:637-720): damped Newton, used for invertibility counts
   BA_HD bool remove_distortion(double xd, double yd) const {
+    double x, y;
+    return remove_distortion(xd, yd, &x, &y);
+  }
+  BA_HD bool remove_distortion(double xd, double yd, double* xo, double* yo) const {
     if (!isfinite(xd) || !isfinite(yd)) return false;
-    if (!has_distortion()) return true;
+    if (!has_distortion()) {
+      *xo = xd;
+      *yo = yd;
+      return true;
+    }
     double x = xd, y = yd;
     for (int it = 1; it <= 30; ++it) {
       double dxx, dyy;
       apply_distortion(x, y, &dxx, &dyy);
       double dx = xd - dxx, dy = yd - dyy;
       double e2 = fma(dx, dx, dy * dy);
-      if (e2 <= 1e-24) return invertible_at(x, y);
+      if (e2 <= 1e-24) {
+        if (!invertible_at(x, y)) return false;
+        *xo = x;
+        *yo = y;
+        return true;
+      }
       double j11, j12, j22, det;
       if (!distortion_jacobian(x, y, &j11, &j12, &j22, &det)) return false;
       if (fabs(det) <= 1e-15) return false;
@@ -213,6 +226,87 @@ struct FixedCameraDev {
     return false;
   }
 };
+
+// ---- angular residuals (kernel/projection.rs:89-195) -------------------------------------------
+BA_HD double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+BA_HD void cross3(const double a[3], const double b[3], double out[3]) {
+  out[0] = a[1] * b[2] - a[2] * b[1];
+  out[1] = a[2] * b[0] - a[0] * b[2];
+  out[2] = a[0] * b[1] - a[1] * b[0];
+}
+// normalize (projection.rs:156-169): vectors already of unit length to 8 eps stay as they are
+BA_HD bool normalize3(const double v[3], double out[3]) {
+  const double n2 = dot3(v, v);
+  if (!finite3(v[0], v[1], v[2]) || !(isfinite(n2) && n2 > kMinPositive)) return false;
+  if (fabs(n2 - 1.0) <= 8.0 * kEps) {
+    out[0] = v[0];
+    out[1] = v[1];
+    out[2] = v[2];
+    return true;
+  }
+  const double inv = 1.0 / sqrt(n2);
+  for (int k = 0; k < 3; ++k) out[k] = v[k] * inv;
+  return true;
+}
+// tangent_basis (projection.rs:171-186)
+BA_HD void tangent_basis3(const double u[3], double b0[3], double b1[3]) {
+  double ref[3] = {0.0, 0.0, 0.0};
+  if (fabs(u[0]) <= fabs(u[1]) && fabs(u[0]) <= fabs(u[2]))
+    ref[0] = 1.0;
+  else if (fabs(u[1]) <= fabs(u[2]))
+    ref[1] = 1.0;
+  else
+    ref[2] = 1.0;
+  cross3(u, ref, b0);
+  const double inv = 1.0 / sqrt(dot3(b0, b0));
+  for (int k = 0; k < 3; ++k) b0[k] *= inv;
+  cross3(u, b0, b1);
+}
+// angular_projection (projection.rs:89-149): the residual angle(observation, prediction) times the
+// unit direction in the observation's tangent plane, and its Jacobian d r / d X in the camera frame.
+BA_HD bool angular_linearize(const double raw_obs[3], const double X[3], double r[2], double J[2][3]) {
+  double obs[3], pred[3], b0[3], b1[3];
+  if (!normalize3(raw_obs, obs) || !normalize3(X, pred)) return false;
+  tangent_basis3(obs, b0, b1);
+  const double a = dot3(b0, pred), b = dot3(b1, pred), c = dot3(obs, pred);
+  const double s2 = a * a + b * b, s = sqrt(s2);
+  if (c < 0.0 && s < 1e-6) return false;  // near the antipode
+  double factor, fscale = 0.0, angle = 0.0;
+  if (s < 1e-6) {
+    const double s4 = s2 * s2;
+    factor = 1.0 + s2 / 6.0 + 3.0 * s4 / 40.0;
+    fscale = 1.0 / 3.0 + 3.0 * s2 / 10.0;
+  } else {
+    angle = atan2(s, c);
+    factor = angle / s;
+  }
+  double dp[2][3];
+  for (int k = 0; k < 3; ++k) {
+    const double da = b0[k], db = b1[k], dc = obs[k];
+    double fd;
+    if (s < 1e-6) {
+      fd = fscale * (a * da + b * db);
+    } else {
+      const double ds = (a * da + b * db) / s;
+      const double ad = (c * ds - s * dc) / (s2 + c * c);
+      fd = (ad * s - angle * ds) / s2;
+    }
+    dp[0][k] = factor * da + a * fd;
+    dp[1][k] = factor * db + b * fd;
+  }
+  const double pn = sqrt(dot3(X, X));
+  for (int row = 0; row < 2; ++row)
+    for (int col = 0; col < 3; ++col) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += dp[row][k] * (((col == k) ? 1.0 : 0.0) - pred[col] * pred[k]) / pn;
+      J[row][col] = acc;
+    }
+  r[0] = factor * a;
+  r[1] = factor * b;
+  for (int i = 0; i < 2; ++i)
+    if (!finite3(J[i][0], J[i][1], J[i][2])) return false;
+  return isfinite(r[0]) && isfinite(r[1]);
+}
 
 // Pinhole pixel projection with the 64-eps depth floor (kernel/projection.rs:47-87), skew 0.
 BA_HD bool pixel_linearize(const FixedCameraDev& c, double X, double Y, double Z, double ox, double oy, double r[2],

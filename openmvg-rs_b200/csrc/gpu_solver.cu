@@ -255,6 +255,8 @@ struct DevView {
   const int* pose_off;         // ncam
   const int* pose_dim;         // ncam
   const uint8_t* pose_mask;    // ncam: bit 0 rotation, bit 1 translation (3 when the layout is legacy)
+  int angular;                 // angular residuals: obs_bearing holds each observation's unit bearing
+  const double* obs_bearing;   // N x 3 (angular only)
   const int* intr_off;         // ng
   const int* intr_dim;         // ng
   const uint8_t* fixed_points; // P
@@ -280,6 +282,7 @@ __device__ __forceinline__ RadialDev make_radial(const double* g) {
 // Projection of observation o for camera point xc; Ji is filled for self-calibration.
 __device__ __forceinline__ bool project_obs(const DevView& v, const double* groups, int o, const double xc[3],
                                             double r[2], double J[2][3], double Ji[2][3]) {
+  if (v.angular) return angular_linearize(v.obs_bearing + 3 * (size_t)o, xc, r, J);
   double ox = v.obs_px[2 * o], oy = v.obs_px[2 * o + 1];
   if (v.self_cal) {
     RadialDev c = make_radial(groups + 3 * v.cam_group[v.obs_cam[o]]);
@@ -2153,7 +2156,8 @@ ExecutionPlan execution_plan(const NativeProblem& n, const LmOptions& opt) {
   const bool direct = auto_prefers_direct(n.self_cal, n.obs_cam.size(), L.D, n.points.size() / 3, nnz, rows,
                                           opt.workspace_budget, &plan.direct_estimate, &plan.cached_estimate);
   // a translation-only solve resolves Auto to the direct solver (native/mod.rs:398-407)
-  plan.iterative = opt.linear_solver == 0 ? (!direct && !(!n.self_cal && n.translation_only)) : opt.iterative;
+  plan.iterative =
+      opt.linear_solver == 0 ? (!direct && !(!n.self_cal && !n.angular && n.translation_only)) : opt.iterative;
   return plan;
 }
 
@@ -2257,6 +2261,7 @@ struct Solver {
   DBuf<FixedCameraDev> d_models;
   DBuf<int> d_pose_off, d_pose_dim, d_intr_off, d_intr_dim;
   DBuf<uint8_t> d_pose_mask;
+  DBuf<double> d_obs_bearing;
   DBuf<uint8_t> d_fixed_points;
   DBuf<double> d_pose[2], d_points[2], d_groups[2];
   int cur = 0;
@@ -2316,7 +2321,7 @@ struct Solver {
                                            &de, &ce);
       // a translation-only solve resolves Auto to the direct solver, so its final rank is exact
       // (native/mod.rs:398-407)
-      if (!n.self_cal && n.translation_only) opt.iterative = false;
+      if (!n.self_cal && !n.angular && n.translation_only) opt.iterative = false;
     }
     direct = !opt.iterative;
     // the PCG operator: the explicit S by block rows (rebuilt every assembly, a block-sparse product
@@ -2361,6 +2366,8 @@ struct Solver {
     v.pose_off = d_pose_off.p;
     v.pose_dim = d_pose_dim.p;
     v.pose_mask = d_pose_mask.p;
+    v.angular = n.angular ? 1 : 0;
+    v.obs_bearing = d_obs_bearing.p;
     v.intr_off = d_intr_off.p;
     v.intr_dim = d_intr_dim.p;
     v.fixed_points = d_fixed_points.p;
@@ -2432,6 +2439,7 @@ struct Solver {
     d_pt_off.upload(pt_off.data(), pt_off.size(), st);
     d_obs_cam.upload(n.obs_cam.data(), n.obs_cam.size(), st);
     d_obs_px.upload(n.obs_px.data(), n.obs_px.size(), st);
+    if (n.angular) d_obs_bearing.upload(n.obs_bearing.data(), n.obs_bearing.size(), st);
     upload_padded(d_obs_model, n.obs_model, 1, st);
     std::vector<FixedCameraDev> models = n.models;
     if (models.empty()) models.resize(1);

@@ -71,6 +71,10 @@ struct NativeProblem {
   bool explicit_masks = false;
   std::vector<uint8_t> pose_mask;   // per native camera
   bool translation_only = false;    // no free mask moves a rotation (CameraPoseVariables)
+  // Angular residuals (kernel/projection.rs:89-149): each observation's unit bearing in the camera
+  // frame, point-major like obs_px
+  bool angular = false;
+  FillVector<double> obs_bearing;   // N x 3
 };
 
 // Free pose coordinates of native camera c (ReducedLayout, workspace/topology.rs:263-347).

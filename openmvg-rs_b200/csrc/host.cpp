@@ -429,13 +429,171 @@ struct Lowered {
   Rebase rb;
 };
 
-Lowered lower_calibrated(const omvgba_problem& pr) {
-  for (size_t o = 0; o < pr.observation_count; ++o) {
-    int m = pr.intrinsics[pr.observation_intrinsic[o]].model;
-    if (m == OMVGBA_CAMERA_FISHEYE || m == OMVGBA_CAMERA_SPHERICAL)
-      fail(OMVGBA_UNSUPPORTED,
-           "pixel BA supports fixed pinhole and Brown-Conrady cameras; use angular residuals for wide-angle cameras");
+// ---- bearings of measured pixels (Camera::bearing, openmvg-core camera/camera_enum.rs:128-132) ----
+// FisheyeDistortion (camera/distortion.rs:244-460): theta_d = theta (1 + k1 t^2 + k2 t^4 + k3 t^6 + k4 t^8)
+struct FisheyePoly {
+  int kind;  // 0 None .. 4 K1K2K3K4
+  double k1, k2, k3, k4;
+  double apply(double t) const {
+    const double t2 = t * t, t4 = t2 * t2;
+    switch (kind) {
+      case 0: return t;
+      case 1: return t * (1.0 + k1 * t2);
+      case 2: return t * (1.0 + k1 * t2 + k2 * t4);
+      case 3: return t * (1.0 + k1 * t2 + k2 * t4 + k3 * (t4 * t2));
+      default: return t * (1.0 + k1 * t2 + k2 * t4 + k3 * (t4 * t2) + k4 * (t4 * t4));
+    }
   }
+  double derivative(double t) const {
+    const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t8 = t4 * t4;
+    return 1.0 + 3.0 * k1 * t2 + 5.0 * k2 * t4 + 7.0 * k3 * t6 + 9.0 * k4 * t8;
+  }
+  // max_invertible_angle (distortion.rs:416-455)
+  bool max_invertible_angle(double max_theta, double* out) const {
+    if (!(std::isfinite(k1) && std::isfinite(k2) && std::isfinite(k3) && std::isfinite(k4))) return false;
+    if (k3 == 0.0 && k4 == 0.0) {
+      double q;
+      *out = first_radial_turn_squared(k1, k2, &q) ? std::min(std::sqrt(q), max_theta) : max_theta;
+      return true;
+    }
+    if (k1 >= 0.0 && k2 >= 0.0 && k3 >= 0.0 && k4 >= 0.0) {
+      *out = max_theta;
+      return true;
+    }
+    double previous = 0.0;
+    for (int i = 1; i <= 1024; ++i) {
+      const double t = max_theta * i / 1024.0;
+      if (derivative(t) <= 0.0) {
+        double lo = previous, hi = t;
+        for (int k = 0; k < 64; ++k) {
+          const double mid = 0.5 * (lo + hi);
+          if (derivative(mid) > 0.0)
+            lo = mid;
+          else
+            hi = mid;
+        }
+        *out = lo;
+        return true;
+      }
+      previous = t;
+    }
+    *out = max_theta;
+    return true;
+  }
+  // invert_on_validated_interval (distortion.rs:359-409)
+  bool invert(double td, double upper, double* out) const {
+    if (!std::isfinite(td) || !std::isfinite(upper) || td < 0.0 || upper <= 0.0) return false;
+    const double mapped = apply(upper);
+    if (!std::isfinite(mapped) || td > mapped + 1e-12) return false;
+    double lo = 0.0, hi = upper, t = std::min(td, upper);
+    for (int i = 0; i < 48; ++i) {
+      const double r = apply(t) - td;
+      if (std::fabs(r) <= 1e-13) {
+        *out = t;
+        return true;
+      }
+      if (r < 0.0)
+        lo = t;
+      else
+        hi = t;
+      const double d = derivative(t), nt = t - r / d;
+      t = (std::isfinite(d) && d > 1e-15 && nt > lo && nt < hi) ? nt : 0.5 * (lo + hi);
+    }
+    if (std::fabs(apply(t) - td) <= 1e-12) {
+      *out = t;
+      return true;
+    }
+    return false;
+  }
+};
+
+// try_normalize_bearing (camera/camera_model.rs:91-109)
+bool normalize_bearing(const double d[3], double b[3]) {
+  if (!all_finite(d, 3)) return false;
+  const double s = std::max({0.0, std::fabs(d[0]), std::fabs(d[1]), std::fabs(d[2])});
+  if (s == 0.0) return false;
+  const double x[3] = {d[0] / s, d[1] / s, d[2] / s};
+  const double n = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  if (!std::isfinite(n) || n == 0.0) return false;
+  for (int k = 0; k < 3; ++k) b[k] = x[k] / n;
+  return true;
+}
+
+// The unit bearing of pixel (u, v): CameraModel::unproject of the pinhole (pinhole.rs:324-340),
+// Brown-Conrady (brown_conrady.rs:365-383), fisheye (fisheye.rs:271-299) and spherical
+// (spherical.rs:113-257) models, then normalized.
+bool camera_bearing(const omvgba_intrinsic& in, double u, double v, double b[3]) {
+  if (!std::isfinite(u) || !std::isfinite(v)) return false;
+  double d[3];
+  switch (in.model) {
+    case OMVGBA_CAMERA_PINHOLE:
+    case OMVGBA_CAMERA_BROWN_CONRADY: {
+      d[0] = (u - in.cx) / in.fx;
+      d[1] = (v - in.cy) / in.fy;
+      d[2] = 1.0;
+      if (!all_finite(d, 3)) return false;
+      if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+        double x, y;
+        if (!make_fixed_camera(in).remove_distortion(d[0] / d[2], d[1] / d[2], &x, &y)) return false;
+        d[0] = x;
+        d[1] = y;
+        d[2] = 1.0;
+      }
+      break;
+    }
+    case OMVGBA_CAMERA_FISHEYE: {
+      const double xd = (u - in.cx) / in.fx, yd = (v - in.cy) / in.fy;
+      if (!std::isfinite(xd) || !std::isfinite(yd)) return false;
+      const double td = std::hypot(xd, yd);
+      if (td <= kEps) {
+        d[0] = 0.0;
+        d[1] = 0.0;
+        d[2] = 1.0;
+        break;
+      }
+      const FisheyePoly f{in.radial_kind, in.radial_kind >= 1 ? in.k1 : 0.0, in.radial_kind >= 2 ? in.k2 : 0.0,
+                          in.radial_kind >= 3 ? in.k3 : 0.0, in.radial_kind >= 4 ? in.k4 : 0.0};
+      double max_angle, theta;
+      if (!f.max_invertible_angle(3.141592653589793 - 1e-10, &max_angle)) return false;
+      if (!f.invert(td, max_angle, &theta)) return false;
+      const double sc = std::sin(theta) / td;
+      d[0] = xd * sc;
+      d[1] = yd * sc;
+      d[2] = std::cos(theta);
+      if (!all_finite(d, 3)) return false;
+      break;
+    }
+    case OMVGBA_CAMERA_SPHERICAL: {
+      const double w = (double)in.width, h = (double)(in.width / 2);
+      if (v < -0.5 || v > h - 0.5) return false;
+      double x = std::fmod(u + 0.5, w);
+      if (x < 0.0) x += w;
+      x -= 0.5;
+      const double pi = 3.141592653589793;
+      const double lon = (x + 0.5) * (2.0 * pi) / w - pi, lat = (v + 0.5) * pi / h - pi / 2.0;
+      if (!std::isfinite(lon) || !std::isfinite(lat) || lat < -pi / 2.0 || lat > pi / 2.0) return false;
+      const double cl = std::cos(lat);
+      d[0] = cl * std::sin(lon);
+      d[1] = std::sin(lat);
+      d[2] = cl * std::cos(lon);
+      break;
+    }
+    default:
+      return false;
+  }
+  return normalize_bearing(d, b);
+}
+
+// The calibrated lowering (native/calibrated.rs:200-494). Angular residuals (PreparedAngularProblem,
+// calibrated.rs:27-123) keep the same frame, gauge and masks and carry each observation's unit bearing.
+Lowered lower_calibrated(const omvgba_problem& pr, bool angular = false) {
+  if (!angular)
+    for (size_t o = 0; o < pr.observation_count; ++o) {
+      int m = pr.intrinsics[pr.observation_intrinsic[o]].model;
+      if (m == OMVGBA_CAMERA_FISHEYE || m == OMVGBA_CAMERA_SPHERICAL)
+        fail(OMVGBA_UNSUPPORTED,
+             "pixel BA supports fixed pinhole and Brown-Conrady cameras; use angular residuals for wide-angle cameras");
+    }
   GaugePlan plan = calibrated_gauge_plan(pr);
   auto observed = observed_cameras(pr);
   Lowered L;
@@ -491,6 +649,22 @@ Lowered lower_calibrated(const omvgba_problem& pr) {
     n.obs_px[2 * i] = pr.observation_pixel[2 * order[i]];
     n.obs_px[2 * i + 1] = pr.observation_pixel[2 * order[i] + 1];
     n.obs_model[i] = pr.observation_intrinsic[order[i]];
+  }
+  if (angular) {
+    n.angular = true;
+    n.obs_bearing.resize(3 * order.size());
+    std::atomic<size_t> bad{SIZE_MAX};
+    for_fixed_chunks(order.size(), 64, [&](size_t, size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i)
+        if (!camera_bearing(pr.intrinsics[n.obs_model[i]], n.obs_px[2 * i], n.obs_px[2 * i + 1], &n.obs_bearing[3 * i])) {
+          size_t cur = bad.load();
+          while (i < cur && !bad.compare_exchange_weak(cur, i)) {
+          }
+        }
+    });
+    if (bad.load() != SIZE_MAX)
+      fail(OMVGBA_NUMERICAL, "observation " + std::to_string(order[bad.load()]) +
+                                 ": the measured pixel does not define a bearing of its camera model");
   }
   return L;
 }
@@ -608,7 +782,7 @@ void reorder_points_for_locality(NativeProblem& n) {
   FillVector<uint64_t> off(P + 1, 0);
   for (size_t q = 0; q < P; ++q) off[q + 1] = off[q] + (n.pt_off[order[q] + 1] - n.pt_off[order[q]]);
   FillVector<uint32_t> cam(N), model(n.obs_model.empty() ? 0 : N);
-  FillVector<double> px(2 * N);
+  FillVector<double> px(2 * N), bearing(n.angular ? 3 * N : 0);
   FillVector<uint64_t> src(N);
   for_fixed_chunks(P, 64, [&](size_t, size_t b, size_t e) {
     for (size_t q = b; q < e; ++q) {
@@ -621,6 +795,8 @@ void reorder_points_for_locality(NativeProblem& n) {
         if (!model.empty()) model[w] = n.obs_model[o];
         px[2 * w] = n.obs_px[2 * o];
         px[2 * w + 1] = n.obs_px[2 * o + 1];
+        if (n.angular)
+          for (int k = 0; k < 3; ++k) bearing[3 * w + k] = n.obs_bearing[3 * o + k];
         src[w] = n.obs_src[o];
       }
     }
@@ -631,14 +807,17 @@ void reorder_points_for_locality(NativeProblem& n) {
   n.obs_cam.swap(cam);
   if (!model.empty()) n.obs_model.swap(model);
   n.obs_px.swap(px);
+  if (n.angular) n.obs_bearing.swap(bearing);
   n.obs_src.swap(src);
   n.point_source = std::move(order);
 }
 
 Lowered lower(const omvgba_problem& pr) {
-  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR)
-    fail(OMVGBA_UNSUPPORTED, "angular residuals are not supported by this adjuster");
-  Lowered L = has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(pr))
+    fail(OMVGBA_UNSUPPORTED, "angular BA requires fixed intrinsics");
+  Lowered L = pr.residual_space == OMVGBA_RESIDUAL_ANGULAR ? lower_calibrated(pr, true)
+              : has_free_intrinsics(pr)                    ? lower_self_calibrating(pr)
+                                                           : lower_calibrated(pr);
   reorder_points_for_locality(L.n);
   return L;
 }
@@ -731,8 +910,11 @@ struct StateView {
   std::vector<Vec3> C;
   std::vector<FixedCameraDev> model;
   std::vector<uint8_t> supported;
+  bool angular = false;
+  const omvgba_intrinsic* intrinsics = nullptr;
   StateView(const omvgba_problem& pr, const omvgba_pose* poses, const omvgba_intrinsic* intrinsics)
-      : R(pr.pose_count), C(pr.pose_count), model(pr.intrinsic_count), supported(pr.intrinsic_count) {
+      : R(pr.pose_count), C(pr.pose_count), model(pr.intrinsic_count), supported(pr.intrinsic_count),
+        angular(pr.residual_space == OMVGBA_RESIDUAL_ANGULAR), intrinsics(intrinsics) {
     for (size_t i = 0; i < pr.pose_count; ++i) {
       R[i] = pose_R(poses[i]);
       C[i] = pose_C(poses[i]);
@@ -745,12 +927,22 @@ struct StateView {
   }
 };
 
-// Pixel residual norm of observation o with the point at X.
+// Residual norm of observation o with the point at X (solver.rs:1405-1432): pixels, or the angle
+// between the measured bearing and the camera point.
 bool residual_norm(const omvgba_problem& pr, const StateView& sv, size_t o, const double* X, double* out) {
   const size_t pi = pr.observation_pose[o], ii = pr.observation_intrinsic[o];
-  if (!sv.supported[ii]) return false;
   const Vec3& C = sv.C[pi];
   Vec3 xc = rotate(sv.R[pi], {X[0] - C[0], X[1] - C[1], X[2] - C[2]});
+  if (sv.angular) {
+    double b[3], r[2], J[2][3];
+    if (!camera_bearing(sv.intrinsics[ii], pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1], b)) return false;
+    if (!angular_linearize(b, xc.data(), r, J)) return false;
+    const double nrm = std::hypot(r[0], r[1]);
+    if (!std::isfinite(nrm)) return false;
+    *out = nrm;
+    return true;
+  }
+  if (!sv.supported[ii]) return false;
   double u, v;
   if (!sv.model[ii].project(xc[0], xc[1], xc[2], &u, &v)) return false;
   double nrm = std::hypot(u - pr.observation_pixel[2 * o], v - pr.observation_pixel[2 * o + 1]);
@@ -1238,8 +1430,8 @@ omvgba_preflight preflight_from_prepared(Context* ctx, const omvgba_problem& pr,
 bool wants_post_solve_probe(const omvgba_problem& pr, const NativeProblem& n) {
   bool fixed_points = false;
   for (size_t i = 0; i < pr.point_count && !fixed_points; ++i) fixed_points = point_fixed(pr, i);
-  return !n.self_cal && n.translation_only && !fixed_points && n.pixel_model && can_probe_scale_representative(pr) &&
-         n.gauge_cam >= 0;
+  return !n.self_cal && !n.angular && n.translation_only && !fixed_points && n.pixel_model &&
+         can_probe_scale_representative(pr) && n.gauge_cam >= 0;
 }
 
 // certified_observability and the probe's observability details (native/reporting.rs:24-134).
@@ -1469,9 +1661,17 @@ std::vector<size_t> weak_points(const omvgba_problem& pr, const Result& sol) {
     Mat3 R = pose_R(pose);
     Vec3 C = pose_C(pose);
     Vec3 xc = rotate(R, {sol.points[3 * p] - C[0], sol.points[3 * p + 1] - C[1], sol.points[3 * p + 2] - C[2]});
-    FixedCameraDev m = make_fixed_camera(sol.intrinsics[pr.observation_intrinsic[o]]);
     double r[2], J[2][3];
-    bool good = m.linearize(xc[0], xc[1], xc[2], pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1], r, J);
+    bool good;
+    if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) {  // Solution::weak_points (solver.rs:1149-1226)
+      double b[3];
+      good = camera_bearing(sol.intrinsics[pr.observation_intrinsic[o]], pr.observation_pixel[2 * o],
+                            pr.observation_pixel[2 * o + 1], b) &&
+             angular_linearize(b, xc.data(), r, J);
+    } else {
+      FixedCameraDev m = make_fixed_camera(sol.intrinsics[pr.observation_intrinsic[o]]);
+      good = m.linearize(xc[0], xc[1], xc[2], pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1], r, J);
+    }
     double rn = good ? std::hypot(r[0], r[1]) : INFINITY;
     if (!good || !std::isfinite(rn)) {
       ok[p] = 0;

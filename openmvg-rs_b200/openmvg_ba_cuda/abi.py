@@ -20,7 +20,7 @@ OMVGBA_INVALID_ARGUMENT = 7
 OMVGBA_CUDA_ERROR = 8
 
 CAMERA_PINHOLE, CAMERA_BROWN_CONRADY, CAMERA_FISHEYE, CAMERA_SPHERICAL = 0, 1, 2, 3
-RADIAL_NONE, RADIAL_K1, RADIAL_K1K2, RADIAL_K1K2K3 = 0, 1, 2, 3
+RADIAL_NONE, RADIAL_K1, RADIAL_K1K2, RADIAL_K1K2K3, RADIAL_K1K2K3K4 = 0, 1, 2, 3, 4
 TANGENTIAL_NONE, TANGENTIAL_P1, TANGENTIAL_P1P2 = 0, 1, 2
 INTRINSIC_FOCAL, INTRINSIC_PRINCIPAL_POINT, INTRINSIC_RADIAL, INTRINSIC_TANGENTIAL = 1, 2, 4, 8
 POSE_ROTATION, POSE_TRANSLATION = 1, 2
@@ -68,6 +68,7 @@ class Intrinsic(C.Structure):
         ("p2", C.c_double),
         ("width", C.c_uint32),
         ("height", C.c_uint32),
+        ("k4", C.c_double),
     ]
 
 

@@ -88,13 +88,14 @@ class CameraIntrinsics:
     p2: float = 0.0
     width: int = 640
     height: int = 480
+    k4: float = 0.0  # fisheye K1K2K3K4 only
     variables: int = 0
     certification: int = 0
     fixed_model: int = 0
 
     def fill(self, s: abi.Intrinsic) -> None:
         for name in ("model", "radial_kind", "tangential_kind", "variables", "certification", "fixed_model",
-                     "fx", "fy", "cx", "cy", "k1", "k2", "k3", "p1", "p2", "width", "height"):
+                     "fx", "fy", "cx", "cy", "k1", "k2", "k3", "p1", "p2", "width", "height", "k4"):
             setattr(s, name, getattr(self, name))
 
     @classmethod

@@ -6,7 +6,7 @@
 
 use std::ffi::{c_char, c_void};
 
-pub const OMVGBA_ABI_VERSION: u32 = 2;
+pub const OMVGBA_ABI_VERSION: u32 = 3;
 
 // omvgba_code
 pub const OMVGBA_OK: i32 = 0;
@@ -28,6 +28,7 @@ pub const OMVGBA_RADIAL_NONE: i32 = 0;
 pub const OMVGBA_RADIAL_K1: i32 = 1;
 pub const OMVGBA_RADIAL_K1K2: i32 = 2;
 pub const OMVGBA_RADIAL_K1K2K3: i32 = 3;
+pub const OMVGBA_RADIAL_K1K2K3K4: i32 = 4;
 pub const OMVGBA_TANGENTIAL_NONE: i32 = 0;
 pub const OMVGBA_TANGENTIAL_P1: i32 = 1;
 pub const OMVGBA_TANGENTIAL_P1P2: i32 = 2;
@@ -117,6 +118,7 @@ pub struct omvgba_intrinsic {
     pub p2: f64,
     pub width: u32,
     pub height: u32,
+    pub k4: f64,
 }
 
 #[repr(C)]

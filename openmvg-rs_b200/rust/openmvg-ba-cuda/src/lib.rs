@@ -26,7 +26,7 @@ use openmvg_ba::{
     LinearSolver, Observability, ObservabilityDiagnostics, ResidualSpace, RobustLoss, Solution, SolveConfig,
     SolveDiagnostics, SolveError, SolveReport, SolveStatus, StationarityAudit, StepRejections,
 };
-use openmvg_core::camera::{Camera, RadialDistortion, TangentialDistortion};
+use openmvg_core::camera::{Camera, FisheyeDistortion, RadialDistortion, TangentialDistortion};
 use openmvg_core::model::{CameraIntrinsics, WorldToCameraPose};
 
 /// Execution options of the GPU solver that `SolveConfig` does not carry.
@@ -134,6 +134,7 @@ fn intrinsic_to_ffi(block: &BundleIntrinsic) -> ffi::omvgba_intrinsic {
         p2: 0.0,
         width,
         height,
+        k4: 0.0,
     };
     match data.camera() {
         Camera::Pinhole(camera) => {
@@ -171,12 +172,31 @@ fn intrinsic_to_ffi(block: &BundleIntrinsic) -> ffi::omvgba_intrinsic {
                 }
             }
         }
-        // wide-angle models are carried unchanged; the GPU solver answers Unsupported for them in
-        // pixel residuals
+        // wide-angle models serve angular residuals (their bearings); the GPU solver answers
+        // Unsupported for them in pixel residuals
         Camera::Fisheye(camera) => {
             out.model = ffi::OMVGBA_CAMERA_FISHEYE;
             out.fx = camera.focal_x();
             out.fy = camera.focal_y();
+            match *camera.fisheye_distortion() {
+                FisheyeDistortion::None => {}
+                FisheyeDistortion::K1(k1) => {
+                    out.radial_kind = ffi::OMVGBA_RADIAL_K1;
+                    out.k1 = k1;
+                }
+                FisheyeDistortion::K1K2(k1, k2) => {
+                    out.radial_kind = ffi::OMVGBA_RADIAL_K1K2;
+                    (out.k1, out.k2) = (k1, k2);
+                }
+                FisheyeDistortion::K1K2K3(k1, k2, k3) => {
+                    out.radial_kind = ffi::OMVGBA_RADIAL_K1K2K3;
+                    (out.k1, out.k2, out.k3) = (k1, k2, k3);
+                }
+                FisheyeDistortion::K1K2K3K4(k1, k2, k3, k4) => {
+                    out.radial_kind = ffi::OMVGBA_RADIAL_K1K2K3K4;
+                    (out.k1, out.k2, out.k3, out.k4) = (k1, k2, k3, k4);
+                }
+            }
         }
         Camera::Spherical(_) => out.model = ffi::OMVGBA_CAMERA_SPHERICAL,
     }

@@ -76,6 +76,8 @@ struct Native {
   bool explicit_masks = false;
   std::vector<uint8_t> pose_mask;
   bool translation_only = false;  // CameraPoseVariables::TranslationOnly (calibrated)
+  bool angular = false;           // angular residuals (native/calibrated.rs:27-123)
+  std::vector<Vec3> obs_bearing;  // per observation: the measured pixel's bearing
   std::vector<uint32_t> obs_cam;
   std::vector<Vec2> obs_px;
   std::vector<uint64_t> obs_src;
@@ -193,6 +195,13 @@ static bool project_obs(const Native& n, const std::vector<Radial>& groups, size
     out->p = *pr;
     out->has_intr = true;
     out->jint = *ji;
+    return true;
+  }
+  if (n.angular) {  // ObservationModel::project, Angular (kernel/multi_view/model.rs:287-292)
+    auto pr = angular_projection(n.obs_bearing[o], xc);
+    if (!pr) return false;
+    out->p = *pr;
+    out->has_intr = false;
     return true;
   }
   const BrownConrady& m = n.models[n.obs_model[o]];
@@ -2025,8 +2034,114 @@ static void set_anchor(const omvgba_problem& pr, Native& n, size_t anchor, doubl
 }
 
 // PreparedCalibratedProblem::try_new (native/calibrated.rs:200-391), full-pose masks only.
-static Native lower_calibrated(const omvgba_problem& pr) {
-  for (size_t o = 0; o < pr.observation_count; ++o) {
+// Camera::bearing (openmvg-core camera/camera_enum.rs:128-132): unproject (pinhole.rs:324-340,
+// brown_conrady.rs:365-383, fisheye.rs:271-299 with distortion.rs:319-455, spherical.rs:113-257),
+// then try_normalize_bearing (camera_model.rs:91-109).
+static double fisheye_apply(int kind, const double k[4], double t) {
+  const double t2 = t * t, t4 = t2 * t2;
+  switch (kind) {
+    case 0: return t;
+    case 1: return t * (1.0 + k[0] * t2);
+    case 2: return t * (1.0 + k[0] * t2 + k[1] * t4);
+    case 3: return t * (1.0 + k[0] * t2 + k[1] * t4 + k[2] * (t4 * t2));
+    default: return t * (1.0 + k[0] * t2 + k[1] * t4 + k[2] * (t4 * t2) + k[3] * (t4 * t4));
+  }
+}
+static double fisheye_derivative(const double k[4], double t) {
+  const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t8 = t4 * t4;
+  return 1.0 + 3.0 * k[0] * t2 + 5.0 * k[1] * t4 + 7.0 * k[2] * t6 + 9.0 * k[3] * t8;
+}
+static std::optional<Vec3> camera_bearing(const omvgba_intrinsic& in, double u, double v) {
+  if (!std::isfinite(u) || !std::isfinite(v)) return std::nullopt;
+  Vec3 d;
+  if (in.model == OMVGBA_CAMERA_PINHOLE || in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+    d = {(u - in.cx) / in.fx, (v - in.cy) / in.fy, 1.0};
+    if (!all_finite(d.data(), 3)) return std::nullopt;
+    if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
+      double x, y;
+      if (!to_model(in).remove_distortion(d[0] / d[2], d[1] / d[2], &x, &y)) return std::nullopt;
+      d = {x, y, 1.0};
+    }
+  } else if (in.model == OMVGBA_CAMERA_FISHEYE) {
+    const double xd = (u - in.cx) / in.fx, yd = (v - in.cy) / in.fy;
+    if (!std::isfinite(xd) || !std::isfinite(yd)) return std::nullopt;
+    const double td = std::hypot(xd, yd);
+    if (td <= kEps) {
+      d = {0.0, 0.0, 1.0};
+    } else {
+      const int kind = in.radial_kind;
+      const double k[4] = {kind >= 1 ? in.k1 : 0.0, kind >= 2 ? in.k2 : 0.0, kind >= 3 ? in.k3 : 0.0,
+                           kind >= 4 ? in.k4 : 0.0};
+      if (!all_finite(k, 4)) return std::nullopt;
+      // FisheyeCamera::try_new: the end of the positive-derivative branch up to pi - 1e-10
+      const double cap = 3.141592653589793 - 1e-10;
+      double upper = cap;
+      if (k[2] == 0.0 && k[3] == 0.0) {
+        auto q = first_radial_turn_squared(k[0], k[1]);
+        upper = q ? std::min(std::sqrt(*q), cap) : cap;
+      } else if (!(k[0] >= 0.0 && k[1] >= 0.0 && k[2] >= 0.0 && k[3] >= 0.0)) {
+        double prev = 0.0;
+        for (int i = 1; i <= 1024; ++i) {
+          const double t = cap * i / 1024.0;
+          if (fisheye_derivative(k, t) <= 0.0) {
+            double lo = prev, hi = t;
+            for (int it = 0; it < 64; ++it) {
+              const double mid = 0.5 * (lo + hi);
+              (fisheye_derivative(k, mid) > 0.0 ? lo : hi) = mid;
+            }
+            upper = lo;
+            break;
+          }
+          prev = t;
+        }
+      }
+      // invert_on_validated_interval: safeguarded Newton, 48 steps
+      const double mapped = fisheye_apply(kind, k, upper);
+      if (!std::isfinite(mapped) || td > mapped + 1e-12) return std::nullopt;
+      double lo = 0.0, hi = upper, t = std::min(td, upper);
+      bool done = false;
+      for (int it = 0; it < 48 && !done; ++it) {
+        const double r = fisheye_apply(kind, k, t) - td;
+        if (std::fabs(r) <= 1e-13) {
+          done = true;
+          break;
+        }
+        if (r < 0.0)
+          lo = t;
+        else
+          hi = t;
+        const double dv = fisheye_derivative(k, t), nt = t - r / dv;
+        t = (std::isfinite(dv) && dv > 1e-15 && nt > lo && nt < hi) ? nt : 0.5 * (lo + hi);
+      }
+      if (!done && !(std::fabs(fisheye_apply(kind, k, t) - td) <= 1e-12)) return std::nullopt;
+      const double sc = std::sin(t) / td;
+      d = {xd * sc, yd * sc, std::cos(t)};
+      if (!all_finite(d.data(), 3)) return std::nullopt;
+    }
+  } else if (in.model == OMVGBA_CAMERA_SPHERICAL) {
+    const double w = (double)in.width, h = (double)(in.width / 2);
+    if (v < -0.5 || v > h - 0.5) return std::nullopt;
+    double x = std::fmod(u + 0.5, w);
+    if (x < 0.0) x += w;
+    x -= 0.5;
+    const double pi = 3.141592653589793;
+    const double lon = (x + 0.5) * (2.0 * pi) / w - pi, lat = (v + 0.5) * pi / h - pi / 2.0;
+    if (!std::isfinite(lon) || !std::isfinite(lat) || lat < -pi / 2.0 || lat > pi / 2.0) return std::nullopt;
+    d = {std::cos(lat) * std::sin(lon), std::sin(lat), std::cos(lat) * std::cos(lon)};
+  } else {
+    return std::nullopt;
+  }
+  if (!all_finite(d.data(), 3)) return std::nullopt;
+  const double sc = std::max({0.0, std::fabs(d[0]), std::fabs(d[1]), std::fabs(d[2])});
+  if (sc == 0.0) return std::nullopt;
+  const Vec3 x = {d[0] / sc, d[1] / sc, d[2] / sc};
+  const double nrm = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  if (!std::isfinite(nrm) || nrm == 0.0) return std::nullopt;
+  return Vec3{x[0] / nrm, x[1] / nrm, x[2] / nrm};
+}
+
+static Native lower_calibrated(const omvgba_problem& pr, bool angular = false) {
+  for (size_t o = 0; o < pr.observation_count && !angular; ++o) {
     int m = pr.intrinsics[pr.observation_intrinsic[o]].model;
     if (m == OMVGBA_CAMERA_FISHEYE || m == OMVGBA_CAMERA_SPHERICAL)
       fail(OMVGBA_UNSUPPORTED,
@@ -2083,6 +2198,17 @@ static Native lower_calibrated(const omvgba_problem& pr) {
   for (size_t i = 0; i < order.size(); ++i) {
     n.obs_px[i] = {pr.observation_pixel[2 * order[i]], pr.observation_pixel[2 * order[i] + 1]};
     n.obs_model[i] = pr.observation_intrinsic[order[i]];
+  }
+  if (angular) {  // bearings in the sorted order; the first failure is the error
+    n.angular = true;
+    n.obs_bearing.resize(order.size());
+    for (size_t i = 0; i < order.size(); ++i) {
+      auto b = camera_bearing(pr.intrinsics[n.obs_model[i]], n.obs_px[i][0], n.obs_px[i][1]);
+      if (!b)
+        fail(OMVGBA_NUMERICAL, "observation " + std::to_string(order[i]) +
+                                   ": the measured pixel does not define a bearing of its camera model");
+      n.obs_bearing[i] = *b;
+    }
   }
   return n;
 }
@@ -2229,12 +2355,22 @@ static bool camera_project_pixel(const omvgba_intrinsic& in, const Vec3& xc, Vec
   return true;
 }
 
-// residual_norm (solver.rs:1135-1160), pixel residuals
+// residual_norm (solver.rs:1405-1432): pixels, or the angle to the measured bearing
 static bool residual_norm(const omvgba_problem& pr, size_t o, const omvgba_pose& pose, const omvgba_intrinsic& in,
                           const double* X, double* out) {
   Mat3 R = pose_R(pose);
   Vec3 C = pose_C(pose);
   Vec3 xc = rotate(R, {X[0] - C[0], X[1] - C[1], X[2] - C[2]});
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) {
+    auto b = camera_bearing(in, pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1]);
+    if (!b) return false;
+    auto p = angular_projection(*b, xc);
+    if (!p) return false;
+    double n = std::hypot(p->residual[0], p->residual[1]);
+    if (!std::isfinite(n)) return false;
+    *out = n;
+    return true;
+  }
   Vec2 px;
   if (!camera_project_pixel(in, xc, &px)) return false;
   double n = std::hypot(px[0] - pr.observation_pixel[2 * o], px[1] - pr.observation_pixel[2 * o + 1]);
@@ -2531,7 +2667,7 @@ static bool choose_iterative(const omvgba_config& cfg, const Native& n, const La
   if (cfg.linear_solver == OMVGBA_SOLVER_ITERATIVE) return true;
   // a translation-only solve resolves Auto to the direct solver, so its final rank is exact
   // (native/mod.rs:398-407)
-  if (!n.self_cal && n.translation_only) return false;
+  if (!n.self_cal && !n.angular && n.translation_only) return false;
   uint64_t de = 0, ce = 0;
   return !auto_prefers_direct(n, L, cfg.has_workspace_budget ? cfg.workspace_budget_bytes : 0, &de, &ce);
 }
@@ -2550,6 +2686,16 @@ static void check_workspace_budget(const omvgba_config& cfg, const Native& n, co
   if (bytes > cfg.workspace_budget_bytes)
     fail(OMVGBA_RESOURCE_EXHAUSTED, "workspace " + std::to_string(bytes) + " bytes exceeds the workspace budget " +
                                         std::to_string(cfg.workspace_budget_bytes));
+}
+
+// The lowering solve_once chooses (native/mod.rs:352-367): angular residuals (fixed intrinsics
+// only), self-calibration, or the calibrated pixel problem.
+static Native lower_native(const omvgba_problem& pr) {
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) {
+    if (has_free_intrinsics(pr)) fail(OMVGBA_UNSUPPORTED, "angular BA requires fixed intrinsics");
+    return lower_calibrated(pr, true);
+  }
+  return has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
 }
 
 // ---- translation-only observability (native/fixed_rotation.rs, native/mod.rs:184-230, 435-447,
@@ -2682,8 +2828,8 @@ static void apply_preflight(const omvgba_problem& pr, const Preflight& pf, omvgb
 static bool wants_post_solve_probe(const omvgba_problem& pr, const Native& n) {
   bool fixed_points = false;
   for (size_t i = 0; i < pr.point_count; ++i) fixed_points = fixed_points || point_fixed(pr, i);
-  return !n.self_cal && n.translation_only && !fixed_points && n.pixel_model && can_probe_scale_representative(pr) &&
-         n.gauge_cam >= 0;
+  return !n.self_cal && !n.angular && n.translation_only && !fixed_points && n.pixel_model &&
+         can_probe_scale_representative(pr) && n.gauge_cam >= 0;
 }
 
 // NativeBundleAdjuster::preflight (native/mod.rs:184-230)
@@ -2701,10 +2847,8 @@ static Preflight preflight(const omvgba_problem& pr, const omvgba_config& cfg) {
 
 static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
-  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR)
-    fail(OMVGBA_UNSUPPORTED, "angular residuals are not supported by this adjuster");
   double t0 = oracle_now();
-  Native n = has_free_intrinsics(pr) ? lower_self_calibrating(pr) : lower_calibrated(pr);
+  Native n = lower_native(pr);
   oracle_phase("lowering", t0);
   Layout L = make_layout(n);
   Options opt;
@@ -2855,9 +2999,14 @@ static std::vector<size_t> weak_points(const omvgba_problem& pr, const Result& s
     Mat3 R = pose_R(pose);
     Vec3 C = pose_C(pose);
     Vec3 xc = rotate(R, {sol.points[3 * p] - C[0], sol.points[3 * p + 1] - C[1], sol.points[3 * p + 2] - C[2]});
-    BrownConrady m = to_model(sol.intrinsics[pr.observation_intrinsic[o]]);
     Vec2 obs = {pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1]};
-    auto pj = m.project_with_jacobian(obs, xc);
+    std::optional<Projection> pj;
+    if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) {
+      auto b = camera_bearing(sol.intrinsics[pr.observation_intrinsic[o]], obs[0], obs[1]);
+      if (b) pj = angular_projection(*b, xc);
+    } else {
+      pj = to_model(sol.intrinsics[pr.observation_intrinsic[o]]).project_with_jacobian(obs, xc);
+    }
     double rn = pj ? std::hypot(pj->residual[0], pj->residual[1]) : kInf;
     if (!pj || !std::isfinite(rn)) {
       ok[p] = 0;
@@ -3170,8 +3319,7 @@ int omvgba_oracle_execution_plan(const omvgba_problem* problem, const omvgba_con
       oracle::without_points(pr, nullptr, held, first);
       working = &first.view;
     }
-    oracle::Native n = oracle::has_free_intrinsics(*working) ? oracle::lower_self_calibrating(*working)
-                                                             : oracle::lower_calibrated(*working);
+    oracle::Native n = oracle::lower_native(*working);
     oracle::Layout L = oracle::make_layout(n);
     const bool direct = oracle::auto_prefers_direct(
         n, L, config->has_workspace_budget ? config->workspace_budget_bytes : 0, direct_estimate, cached_estimate);
@@ -3226,7 +3374,7 @@ int32_t omvgba_oracle_debug_linearize(const omvgba_problem* problem, const omvgb
   try {
     validate_problem(*problem);
     validate_config(*config);
-    Native n = has_free_intrinsics(*problem) ? lower_self_calibrating(*problem) : lower_calibrated(*problem);
+    Native n = lower_native(*problem);
     Layout L = make_layout(n);
     double scene = n.self_cal ? scene_scale_plain(n, n.poses, n.points) : scene_scale_observed(n, n.poses, n.points);
     GaugeState g = make_gauge(n, n.poses, scene);
@@ -3303,6 +3451,21 @@ int omvgba_oracle_radial_linearize(double f, double k1, double k2, const double*
 int omvgba_oracle_bc_project(const omvgba_intrinsic* in, const double* X, double* out) {
   BrownConrady m = to_model(*in);
   auto p = m.project_with_jacobian({0.0, 0.0}, {X[0], X[1], X[2]});
+  if (!p) return 0;
+  out[0] = p->residual[0];
+  out[1] = p->residual[1];
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 3; ++c) out[2 + 3 * r + c] = p->jacobian[r][c];
+  return 1;
+}
+int omvgba_oracle_camera_bearing(const omvgba_intrinsic* in, double u, double v, double* out) {
+  auto b = camera_bearing(*in, u, v);
+  if (!b) return 0;
+  for (int k = 0; k < 3; ++k) out[k] = (*b)[k];
+  return 1;
+}
+int omvgba_oracle_angular_projection(const double* bearing, const double* X, double* out) {
+  auto p = angular_projection({bearing[0], bearing[1], bearing[2]}, {X[0], X[1], X[2]});
   if (!p) return 0;
   out[0] = p->residual[0];
   out[1] = p->residual[1];

@@ -52,6 +52,10 @@ def lib():
         L.omvgba_oracle_radial_linearize.restype = C.c_int
         L.omvgba_oracle_bc_project.argtypes = [C.POINTER(abi.Intrinsic), dp, dp]
         L.omvgba_oracle_bc_project.restype = C.c_int
+        L.omvgba_oracle_camera_bearing.argtypes = [C.POINTER(abi.Intrinsic), C.c_double, C.c_double, dp]
+        L.omvgba_oracle_camera_bearing.restype = C.c_int
+        L.omvgba_oracle_angular_projection.argtypes = [dp, dp, dp]
+        L.omvgba_oracle_angular_projection.restype = C.c_int
         L.omvgba_oracle_bc_remove_distortion.argtypes = [C.POINTER(abi.Intrinsic), C.c_double, C.c_double, dp]
         L.omvgba_oracle_bc_remove_distortion.restype = C.c_int
         ip = C.POINTER(C.c_int)
@@ -180,3 +184,23 @@ def probe_fixed_rotation(problem, options=None):
     out, err = abi.ProbeReport(), abi.Error()
     raise_for(lib().omvgba_oracle_probe_fixed_rotation(C.byref(fp), C.byref(opts), C.byref(out), C.byref(err)), err)
     return out.to_dict()
+
+
+def camera_bearing(intrinsic, u: float, v: float):
+    """The oracle's Camera::bearing of pixel (u, v) (unit vector) or None outside the model's domain."""
+    from openmvg_ba_cuda import abi
+    st = abi.Intrinsic()
+    intrinsic.fill(st)
+    out = np.zeros(3)
+    ok = lib().omvgba_oracle_camera_bearing(C.byref(st), float(u), float(v), out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out if ok else None
+
+
+def angular_projection(bearing, X):
+    """(residual (2,), jacobian (2, 3)) of angular_projection, or None."""
+    b = np.ascontiguousarray(bearing, dtype=np.float64)
+    x = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.zeros(8)
+    dp = C.POINTER(C.c_double)
+    ok = lib().omvgba_oracle_angular_projection(b.ctypes.data_as(dp), x.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    return (out[:2], out[2:].reshape(2, 3)) if ok else None

@@ -553,6 +553,80 @@ inline double point_rcond(const PointBlockFactor& f, const Mat3& m) {
   double den = inf_norm(m) * inf_norm(inv);
   return (std::isfinite(den) && den > 0.0) ? 1.0 / den : 0.0;
 }
+// ---------------------------------------------------------------------------------------------
+// Angular residuals: kernel/projection.rs:89-195.
+// ---------------------------------------------------------------------------------------------
+inline double odot(const Vec3& a, const Vec3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline Vec3 ocross(const Vec3& a, const Vec3& b) {
+  return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+// normalize (projection.rs:156-169)
+inline std::optional<Vec3> unit_or_none(const Vec3& v) {
+  const double n2 = odot(v, v);
+  if (!all_finite(v.data(), 3) || !(std::isfinite(n2) && n2 > kMinPositive)) return std::nullopt;
+  if (std::fabs(n2 - 1.0) <= 8.0 * kEps) return v;
+  const double inv = 1.0 / std::sqrt(n2);
+  return Vec3{v[0] * inv, v[1] * inv, v[2] * inv};
+}
+// tangent_basis (projection.rs:171-186)
+inline std::array<Vec3, 2> angular_tangent_basis(const Vec3& u) {
+  Vec3 ref{0.0, 0.0, 0.0};
+  if (std::fabs(u[0]) <= std::fabs(u[1]) && std::fabs(u[0]) <= std::fabs(u[2]))
+    ref[0] = 1.0;
+  else if (std::fabs(u[1]) <= std::fabs(u[2]))
+    ref[1] = 1.0;
+  else
+    ref[2] = 1.0;
+  Vec3 first = ocross(u, ref);
+  const double inv = 1.0 / std::sqrt(odot(first, first));
+  for (double& x : first) x *= inv;
+  return {first, ocross(u, first)};
+}
+// angular_projection (projection.rs:89-149)
+inline std::optional<Projection> angular_projection(const Vec3& raw_obs, const Vec3& point) {
+  auto obs = unit_or_none(raw_obs);
+  auto pred = unit_or_none(point);
+  if (!obs || !pred) return std::nullopt;
+  const auto basis = angular_tangent_basis(*obs);
+  const double a = odot(basis[0], *pred), b = odot(basis[1], *pred), c = odot(*obs, *pred);
+  const double s2 = a * a + b * b, s = std::sqrt(s2);
+  if (c < 0.0 && s < 1e-6) return std::nullopt;
+  double factor, fscale = 0.0;
+  if (s < 1e-6) {
+    const double s4 = s2 * s2;
+    factor = 1.0 + s2 / 6.0 + 3.0 * s4 / 40.0;
+    fscale = 1.0 / 3.0 + 3.0 * s2 / 10.0;
+  } else {
+    factor = std::atan2(s, c) / s;
+  }
+  double dp[2][3];
+  for (int k = 0; k < 3; ++k) {
+    const double da = basis[0][k], db = basis[1][k], dc = (*obs)[k];
+    double fd;
+    if (s < 1e-6) {
+      fd = fscale * (a * da + b * db);
+    } else {
+      const double ds = (a * da + b * db) / s;
+      const double angle = std::atan2(s, c);
+      const double ad = (c * ds - s * dc) / (s2 + c * c);
+      fd = (ad * s - angle * ds) / s2;
+    }
+    dp[0][k] = factor * da + a * fd;
+    dp[1][k] = factor * db + b * fd;
+  }
+  const double pn = std::sqrt(odot(point, point));
+  Projection pr;
+  for (int row = 0; row < 2; ++row)
+    for (int col = 0; col < 3; ++col) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += dp[row][k] * (((col == k) ? 1.0 : 0.0) - (*pred)[col] * (*pred)[k]) / pn;
+      pr.jacobian[row][col] = acc;
+    }
+  pr.residual = {factor * a, factor * b};
+  if (!projection_finite(pr)) return std::nullopt;
+  return pr;
+}
+
 constexpr double kPointBlockRcondThreshold = 64.0 * kEps * 3.0;  // point_block.rs:10
 constexpr double kPointBlockQuarantineRcond = 1.0e-5;             // point_block.rs:20
 

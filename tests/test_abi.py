@@ -20,7 +20,7 @@ def declared_functions():
 
 def test_library_loads_and_reports_version():
     L = _lib.lib()
-    assert L.omvgba_abi_version() == 2
+    assert L.omvgba_abi_version() == 3
     assert L.omvgba_adjuster_name().decode() == "openmvg-ba-cuda-b200"
 
 

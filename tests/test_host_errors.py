@@ -83,9 +83,14 @@ CASES = {
     "loss units differ from residuals": (
         lambda p: _copy(p, residual_space=abi.RESIDUAL_ANGULAR, robust_loss=P.RobustLoss.huber(1.0)),
         abi.OMVGBA_INVALID_PROBLEM),
-    "angular residuals": (
-        lambda p: _copy(p, residual_space=abi.RESIDUAL_ANGULAR, robust_loss=P.RobustLoss.squared()),
+    "angular residuals with free intrinsics": (
+        lambda p: _copy(p, residual_space=abi.RESIDUAL_ANGULAR, robust_loss=P.RobustLoss.squared(),
+                        intrinsics=[dataclasses.replace(p.intrinsics[0], variables=abi.INTRINSIC_FOCAL)]),
         abi.OMVGBA_UNSUPPORTED),
+    "angular residuals of a pixel outside a spherical camera": (
+        lambda p: _copy(p, residual_space=abi.RESIDUAL_ANGULAR, robust_loss=P.RobustLoss.squared(),
+                        intrinsics=[P.CameraIntrinsics(model=abi.CAMERA_SPHERICAL, width=64, height=32)]),
+        abi.OMVGBA_NUMERICAL),
     "every track a single observation": (_single_observation_tracks, abi.OMVGBA_UNSUPPORTED),
     "no observations": (_no_observations, abi.OMVGBA_INVALID_PROBLEM),
 }

@@ -996,6 +996,7 @@ __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const
 }  // namespace omvgba
 #include "mv_tiles.cuh"
 #include "explicit_s.cuh"
+#include "two_view.cuh"
 namespace omvgba {
 
 // ----------------------------------------------------------------------------------------------
@@ -1268,7 +1269,7 @@ __global__ void k_step_block_norm(int ncam, const int* pose_off, const int* pose
   out[c] = fmax(sqrt(s1), sqrt(s2));
 }
 
-__device__ __forceinline__ void exp_so3_dev(const double w[3], double R[9]) {
+__host__ __device__ __forceinline__ void exp_so3_dev(const double w[3], double R[9]) {
   // numerics/manifold/so3.rs:254-265 with matrix_polynomial (:420-423)
   double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
   double th = sqrt(th2);
@@ -3552,6 +3553,359 @@ struct Solver {
   }
 
 };
+
+// ---- two-view LM (kernel/two_view/optimizer.rs:16-240) -----------------------------------------
+namespace {
+// solve_positive_definite (numerics/refine/solver.rs:281-335) on the 5 x 5 reduced camera system
+bool tv_solve_spd(const double A[25], const double b[5], double x[5]) {
+  for (int i = 0; i < 25; ++i)
+    if (!std::isfinite(A[i])) return false;
+  for (int i = 0; i < 5; ++i)
+    if (!std::isfinite(b[i])) return false;
+  double L[5][5] = {};
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < j; ++k) acc += L[i][k] * L[j][k];
+      const double sum = A[5 * i + j] - acc;
+      if (!std::isfinite(sum)) return false;
+      if (i == j) {
+        if (sum <= 0.0) return false;
+        L[i][j] = std::sqrt(sum);
+      } else {
+        L[i][j] = sum / L[j][j];
+      }
+    }
+  double y[5];
+  for (int i = 0; i < 5; ++i) {
+    double sum = b[i];
+    for (int j = 0; j < i; ++j) sum -= L[i][j] * y[j];
+    y[i] = sum / L[i][i];
+  }
+  for (int i = 4; i >= 0; --i) {
+    double sum = y[i];
+    for (int j = i + 1; j < 5; ++j) sum -= L[j][i] * x[j];
+    x[i] = sum / L[i][i];
+  }
+  for (int i = 0; i < 5; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+// the camera rank of the final system (schur.rs:338-370): eigenvalues of the symmetrized 5 x 5 by
+// cyclic Jacobi rotations, counted above 64 eps n lambda_max
+int tv_rank(const double H[25]) {
+  double A[25];
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) A[5 * i + j] = 0.5 * (H[5 * i + j] + H[5 * j + i]);
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, scale = 0.0;
+    for (int i = 0; i < 5; ++i) {
+      scale = std::max(scale, std::fabs(A[6 * i]));
+      for (int j = i + 1; j < 5; ++j) off += A[5 * i + j] * A[5 * i + j];
+    }
+    if (!(off > 1e-32 * scale * scale)) break;
+    for (int p = 0; p < 5; ++p)
+      for (int q = p + 1; q < 5; ++q) {
+        const double apq = A[5 * p + q];
+        if (apq == 0.0) continue;
+        const double theta = (A[5 * q + q] - A[5 * p + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < 5; ++k) {
+          const double akp = A[5 * k + p], akq = A[5 * k + q];
+          A[5 * k + p] = c * akp - sn * akq;
+          A[5 * k + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < 5; ++k) {
+          const double apk = A[5 * p + k], aqk = A[5 * q + k];
+          A[5 * p + k] = c * apk - sn * aqk;
+          A[5 * q + k] = sn * apk + c * aqk;
+        }
+      }
+  }
+  double largest = 0.0;
+  for (int i = 0; i < 5; ++i) largest = std::max(largest, std::fabs(A[6 * i]));
+  if (!(std::isfinite(largest) && largest > 0.0)) return 0;
+  const double tol = 64.0 * kEps * 5.0 * largest;
+  int rank = 0;
+  for (int i = 0; i < 5; ++i) rank += (std::isfinite(A[6 * i]) && A[6 * i] > tol) ? 1 : 0;
+  return rank;
+}
+void tv_basis(const double t[3], double baseline, double dir[3], double b0[3], double b1[3]) {
+  for (int k = 0; k < 3; ++k) dir[k] = t[k] / baseline;
+  // s2_tangent_basis (numerics/manifold.rs:118-131)
+  const double nv = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  const double u[3] = {dir[0] / nv, dir[1] / nv, dir[2] / nv};
+  double ref[3] = {0, 0, 0};
+  if (std::fabs(u[0]) <= std::fabs(u[1]) && std::fabs(u[0]) <= std::fabs(u[2]))
+    ref[0] = 1;
+  else if (std::fabs(u[1]) <= std::fabs(u[2]))
+    ref[1] = 1;
+  else
+    ref[2] = 1;
+  double a[3] = {u[1] * ref[2] - u[2] * ref[1], u[2] * ref[0] - u[0] * ref[2], u[0] * ref[1] - u[1] * ref[0]};
+  const double na = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  for (int k = 0; k < 3; ++k) b0[k] = a[k] / na;
+  b1[0] = u[1] * b0[2] - u[2] * b0[1];
+  b1[1] = u[2] * b0[0] - u[0] * b0[2];
+  b1[2] = u[0] * b0[1] - u[1] * b0[0];
+}
+}  // namespace
+
+TwoViewReport gpu_two_view(Context* ctx, TwoViewProblem& pr, const LmOptions& opt) {
+  CUDA_OK(cudaSetDevice(ctx->device));
+  cudaStream_t st = opt.stream ? static_cast<cudaStream_t>(opt.stream) : ctx->stream;
+  const int P = (int)(pr.points.size() / 3);
+  if (P < 5) throw SolveFailure{OMVGBA_NUMERICAL, "two-view bundle adjustment needs at least 5 points"};
+  double baseline = std::sqrt(pr.t[0] * pr.t[0] + pr.t[1] * pr.t[1] + pr.t[2] * pr.t[2]);
+  if (!(std::isfinite(pr.t[0]) && std::isfinite(pr.t[1]) && std::isfinite(pr.t[2])) ||
+      !(std::isfinite(baseline) && baseline > 64.0 * kEps))
+    throw SolveFailure{OMVGBA_NUMERICAL, "two-view bundle adjustment translation is invalid"};
+  DBuf<double> d_points, d_moved, d_obs, d_bearing, d_out, d_local, d_cand, d_sum, d_step;
+  d_points.upload(pr.points.data(), pr.points.size(), st);
+  d_moved.alloc(pr.points.size(), st);
+  if (pr.angular)
+    d_bearing.upload(pr.bearing.data(), pr.bearing.size(), st);
+  else
+    d_obs.upload(pr.obs.data(), pr.obs.size(), st);
+  d_out.alloc((size_t)kTvOut * P, st);
+  d_local.alloc((size_t)kTvLocal * P, st);
+  d_cand.alloc((size_t)4 * P, st);
+  d_sum.alloc(kTvOut, st);
+  d_step.alloc(5, st);
+  TvDev dev{};
+  dev.P = P;
+  dev.angular = pr.angular ? 1 : 0;
+  std::memcpy(dev.cam, pr.cam, sizeof(dev.cam));
+  dev.obs = d_obs.p;
+  dev.bearing = d_bearing.p;
+  TvPose pose{};
+  std::memcpy(pose.R, pr.R, sizeof(pose.R));
+  std::memcpy(pose.t, pr.t, sizeof(pose.t));
+  const int grid = grid_for(P, 128);
+  // one linearization + reduction: sums[0..42], max point gradient, min rcond, weak, invalid, failed
+  auto system = [&](const TvPose& ps, const LossDev& loss, double lambda, double sums[kTvOut]) {
+    double dir[3], b0[3], b1[3];
+    tv_basis(ps.t, baseline, dir, b0, b1);
+    OMVGBA_LAUNCH(k_tv_linearize, grid, 128, 0, st, dev, (const double*)d_points.p, ps, b0[0], b0[1], b0[2], b1[0],
+                  b1[1], b1[2], baseline, loss, lambda, d_out.p, d_local.p);
+    OMVGBA_LAUNCH(k_tv_reduce, 1, 1024, 0, st, (const double*)d_out.p, P, kTvOut, kTvSums, d_sum.p);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(copy_async(sums, d_sum.p, sizeof(double) * kTvOut, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    return sums[kTvSums + 4] == 0.0;  // every point projected in both views
+  };
+  auto floor_of = [](const double* diag) {
+    double sc = 0.0;
+    for (int k = 0; k < 5; ++k) sc = std::max(sc, diag[k]);
+    return 64.0 * kEps * std::max(sc, kMinPositive);
+  };
+  auto scaled_ginf5 = [](const double* g, const double* diag) {
+    double scale = 0.0;
+    for (int i = 0; i < 5; ++i) scale = std::max(scale, diag[i]);
+    if (!(std::isfinite(scale) && scale > 0.0)) {
+      for (int i = 0; i < 5; ++i)
+        if (g[i] != 0.0) return (double)INFINITY;
+      return 0.0;
+    }
+    const double fl = 64.0 * kEps * scale;
+    double best = 0.0;
+    for (int i = 0; i < 5; ++i) best = std::max(best, std::fabs(g[i]) / std::sqrt(std::max(diag[i], fl)));
+    return best;
+  };
+  auto valid_system = [](const double* s) {  // ReducedSystem::is_valid (schur.rs:151-155)
+    if (s[kTvSums + 3] != 0.0) return false;
+    for (int k = 0; k < 30; ++k)
+      if (!std::isfinite(s[k])) return false;
+    return true;
+  };
+  TwoViewReport rep;
+  double sums[kTvOut];
+  if (!system(pose, opt.loss, 0.0, sums))  // validate_projection_domain (optimizer.rs:396-415)
+    throw SolveFailure{OMVGBA_NUMERICAL, "two-view bundle adjustment: a point is not projectable in both views"};
+  rep.initial_cost = sums[40];
+  rep.initial_rmse = std::sqrt(sums[41] / double(4 * (size_t)P));
+  // stages (continuation.rs:18-74)
+  struct StageLoss {
+    LossDev loss;
+    uint64_t iters;
+  } stages[3];
+  const LossDev l2{kLossL2, 0.0};
+  if (opt.loss.kind == kLossCauchy) {
+    const uint64_t w = std::min<uint64_t>(opt.max_iterations / 4, 5);
+    stages[0] = {l2, w};
+    stages[1] = {opt.loss, opt.max_iterations - w};
+    stages[2] = {l2, 0};
+  } else {
+    stages[0] = {opt.loss, opt.max_iterations};
+    stages[1] = {l2, 0};
+    stages[2] = {l2, 0};
+  }
+  int target = 0;
+  for (int i = 2; i >= 0; --i)
+    if (stages[i].iters > 0) {
+      target = i;
+      break;
+    }
+  // LM run state (run_state.rs) with Nielsen damping (controller.rs:63-90), initial 1e-4
+  double lambda = 1e-4, nu = 2.0;
+  auto increase = [&]() {
+    lambda = std::min(lambda * nu, 1e12);
+    nu = std::min(nu * 2.0, 1e12);
+  };
+  uint64_t target_accepted = 0;
+  int convergence = -1;
+  bool done = false;
+  for (int si = 0; si < 3 && !done; ++si) {
+    for (uint64_t it = 0; it < stages[si].iters; ++it) {
+      rep.iterations++;
+      const double trial = lambda;
+      if (!system(pose, stages[si].loss, trial, sums) || !valid_system(sums)) {
+        rep.rej[0]++;
+        increase();
+        continue;
+      }
+      double H[25], g[5];
+      std::memcpy(H, sums, sizeof(H));
+      std::memcpy(g, sums + 25, sizeof(g));
+      const double* full_g = sums + 30;
+      const double* diag = sums + 35;
+      const double fl = floor_of(diag);
+      for (int k = 0; k < 5; ++k) H[6 * k] += trial * std::max(diag[k], fl);  // finish_damping
+      const double current = sums[40];
+      const double gnorm = std::max(sums[kTvSums], scaled_ginf5(full_g, diag));
+      if (si == target && convergence < 0 && std::isfinite(gnorm) && gnorm >= 0.0 && std::isfinite(current) &&
+          gnorm <= opt.gradient_tolerance * (1.0 + std::fabs(current))) {
+        convergence = 1;
+        done = true;
+        break;
+      }
+      double raw[5], step[5];
+      if (!tv_solve_spd(H, g, raw)) {
+        rep.rej[1]++;
+        increase();
+        continue;
+      }
+      for (int k = 0; k < 5; ++k) step[k] = -raw[k];
+      {  // limit_pose_step (optimizer.rs:432-443)
+        const double rn = std::sqrt(step[0] * step[0] + step[1] * step[1] + step[2] * step[2]);
+        const double tn = std::sqrt(step[3] * step[3] + step[4] * step[4]);
+        const double len = std::max(rn, tn);
+        if (len > 0.5)
+          for (double& v : step) v *= 0.5 / len;
+      }
+      // retract_pose (optimizer.rs:365-381)
+      double dir[3], b0[3], b1[3];
+      tv_basis(pose.t, baseline, dir, b0, b1);
+      TvPose cand{};
+      {
+        double w[3] = {step[0], step[1], step[2]}, U[9];
+        exp_so3_dev(w, U);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; ++k) acc += U[3 * i + k] * pose.R[3 * k + j];
+            cand.R[3 * i + j] = acc;
+          }
+        // retract_s2 (numerics/manifold.rs:133-147)
+        const double vv[3] = {b0[0] * step[3] + b1[0] * step[4], b0[1] * step[3] + b1[1] * step[4],
+                              b0[2] * step[3] + b1[2] * step[4]};
+        const double th = std::sqrt(vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]);
+        const double tn = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+        const double tv[3] = {dir[0] / tn, dir[1] / tn, dir[2] / tn};
+        double nd[3];
+        if (th < 1e-10) {
+          const double sv[3] = {tv[0] + vv[0], tv[1] + vv[1], tv[2] + vv[2]};
+          const double nn = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+          for (int k = 0; k < 3; ++k) nd[k] = sv[k] / nn;
+        } else {
+          const double cs = std::cos(th), sn = std::sin(th) / th;
+          for (int k = 0; k < 3; ++k) nd[k] = tv[k] * cs + vv[k] * sn;
+        }
+        for (int k = 0; k < 3; ++k) cand.t[k] = baseline * nd[k];
+      }
+      CUDA_OK(copy_async(d_step.p, step, sizeof(step), cudaMemcpyHostToDevice, st));
+      OMVGBA_LAUNCH(k_tv_candidate, grid, 128, 0, st, dev, (const double*)d_points.p, (const double*)d_local.p, trial,
+                    (const double*)d_step.p, cand, baseline, stages[si].loss, d_moved.p, d_cand.p);
+      OMVGBA_LAUNCH(k_tv_reduce, 1, 1024, 0, st, (const double*)d_cand.p, P, 4, 4, d_sum.p);
+      CUDA_OK(cudaGetLastError());
+      double cs[4];
+      CUDA_OK(copy_async(cs, d_sum.p, sizeof(cs), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      if (cs[3] != 0.0) {
+        rep.rej[2]++;
+        increase();
+        continue;
+      }
+      const double point_rms = std::sqrt(cs[1] / double(P));
+      const double reduction = current - cs[0];
+      // ReducedSystem::predicted_reduction (schur.rs:161-196), with the damped camera system
+      double quad = 0.0, gs = 0.0, pdn = 0.0;
+      for (int r = 0; r < 5; ++r) {
+        double hs = 0.0;
+        for (int c = 0; c < 5; ++c) hs += H[5 * r + c] * step[c];
+        quad += step[r] * hs;
+      }
+      for (int r = 0; r < 5; ++r) gs += g[r] * step[r];
+      for (int r = 0; r < 5; ++r) pdn += std::max(diag[r], fl) * step[r] * step[r];
+      const double predicted = (sums[42] - gs - 0.5 * quad) + 0.5 * trial * (pdn + cs[2]);
+      // NielsenController::accept (controller.rs:63-90)
+      const double gain = (std::isfinite(reduction) && std::isfinite(predicted) && predicted > 0.0)
+                              ? reduction / predicted
+                              : std::nan("");
+      if (!(std::isfinite(gain) && gain > 0.0)) {
+        rep.rej[3]++;
+        increase();
+        continue;
+      }
+      const double c3 = 2.0 * gain - 1.0;
+      lambda = std::max(lambda * std::max(1.0 - c3 * c3 * c3, 1.0 / 3.0), 1e-12);
+      nu = 2.0;
+      // commit_points: the moved points of this step (the same back-substitution at the same state)
+      CUDA_OK(cudaMemcpyAsync(d_points.p, d_moved.p, sizeof(double) * 3 * (size_t)P, cudaMemcpyDeviceToDevice, st));
+      pose = cand;
+      rep.accepted++;
+      double ss = 0.0;
+      for (double v : step) ss += v * v;
+      const double prms = std::sqrt(ss / 5.0);
+      const double sn = std::sqrt(prms * prms + point_rms * point_rms);
+      if (si == target) {
+        target_accepted++;
+        const double rel = reduction / (1.0 + std::fabs(current));
+        const int cc = sn <= opt.step_tolerance ? 2 : (rel <= opt.relative_cost_tolerance ? 0 : -1);
+        convergence = cc;
+        if (cc >= 0) {
+          done = true;
+          break;
+        }
+      }
+    }
+  }
+  // the final undamped system
+  const bool have = system(pose, opt.loss, 0.0, sums);
+  double Hf[25];
+  std::memcpy(Hf, sums, sizeof(Hf));
+  const bool valid = have && valid_system(sums);
+  rep.rank = valid ? tv_rank(Hf) : 0;
+  rep.weak = have ? (uint64_t)sums[kTvSums + 2] : (uint64_t)P;
+  const bool well = rep.rank == 5 && rep.weak == 0;
+  rep.status = !well ? 3 : (convergence >= 0 ? 0 : (rep.iterations > 0 && target_accepted == 0 ? 2 : 1));
+  rep.reason = convergence;
+  rep.grad_norm = valid ? std::max(sums[kTvSums], scaled_ginf5(sums + 30, sums + 35)) : INFINITY;
+  if (have) {
+    rep.final_cost = sums[40];
+    rep.final_rmse = std::sqrt(sums[41] / double(4 * (size_t)P));
+  } else {  // metrics (schur.rs:303-330): a point that no longer projects makes both infinite
+    rep.final_cost = INFINITY;
+    rep.final_rmse = INFINITY;
+  }
+  rep.final_damping = lambda;
+  std::memcpy(rep.R, pose.R, sizeof(rep.R));
+  std::memcpy(rep.t, pose.t, sizeof(rep.t));
+  CUDA_OK(copy_async(pr.points.data(), d_points.p, sizeof(double) * 3 * (size_t)P, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  return rep;
+}
 
 NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOptions& options,
                         std::vector<double>& rotation, std::vector<double>& translation, std::vector<double>& points,

@@ -132,6 +132,25 @@ struct ExecutionPlan {
 };
 ExecutionPlan execution_plan(const NativeProblem& problem, const LmOptions& options);
 
+// Two-view bundle adjustment (native/two_view.rs, kernel/two_view/*): the first camera is the frame,
+// the second's native pose and the points (native frame) are refined; pixel or angular measurements.
+struct TwoViewProblem {
+  bool angular = false;
+  double cam[2][4] = {};          // pixel: fx, fy, cx, cy per view
+  std::vector<double> obs;        // pixel: [view][point][2]
+  std::vector<double> bearing;    // angular: [view][point][3]
+  double R[9] = {}, t[3] = {};    // the second camera's native pose
+  std::vector<double> points;     // P x 3, native frame
+};
+struct TwoViewReport {
+  double R[9] = {}, t[3] = {};
+  int status = 1, reason = -1;    // as NativeReport
+  uint64_t iterations = 0, accepted = 0, rej[4] = {0, 0, 0, 0};
+  double initial_cost = 0, final_cost = 0, initial_rmse = 0, final_rmse = 0, grad_norm = 0, final_damping = 0;
+  int rank = 0;                   // of the final 5 x 5 reduced camera system
+  uint64_t weak = 0;
+};
+
 struct Context;  // device, stream, pinned scratch
 
 int device_count();
@@ -141,6 +160,10 @@ void context_destroy(Context* ctx);
 
 // Runs the LM refinement on the GPU; on return points/rotation/translation/groups hold the refined
 // native state. Throws SolveFailure.
+// refine_ba_2view on the device; on return `problem.points` holds the refined points. Throws
+// SolveFailure (OMVGBA_NUMERICAL for the kernel's own input errors).
+TwoViewReport gpu_two_view(Context* ctx, TwoViewProblem& problem, const LmOptions& options);
+
 NativeReport gpu_refine(Context* ctx, const NativeProblem& problem, const LmOptions& options,
                         std::vector<double>& rotation, std::vector<double>& translation,
                         std::vector<double>& points, std::vector<double>& groups);

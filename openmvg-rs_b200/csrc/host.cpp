@@ -1467,8 +1467,161 @@ omvgba_preflight preflight_check(Context* ctx, const omvgba_problem& pr, const o
   return preflight_from_prepared(ctx, pr, L, L.n.rotation, L.n.translation, pts);
 }
 
+// ---- two-view solves (native/two_view.rs) --------------------------------------------------------
+// unobserved_free_intrinsics (native/mod.rs:465-478): free intrinsic blocks no observation uses; the
+// calibrated, angular and two-view solutions report them unconstrained
+std::vector<uint64_t> unobserved_free_intrinsics(const omvgba_problem& pr) {
+  std::vector<uint8_t> seen(pr.intrinsic_count, 0);
+  for (size_t o = 0; o < pr.observation_count; ++o) seen[pr.observation_intrinsic[o]] = 1;
+  std::vector<uint64_t> out;
+  for (size_t i = 0; i < pr.intrinsic_count; ++i)
+    if (!seen[i] && pr.intrinsics[i].variables != 0) out.push_back(i);
+  return out;
+}
+
+// can_use_two_view (native/two_view.rs:14-48): two poses, the anchor fixed and the other fully
+// free, every point seen exactly once by each (no fixed point, no repeated pose-point pair), one
+// calibration per pose, and undistorted perspective cameras unless the residuals are angular.
+bool can_use_two_view(const omvgba_problem& pr) {
+  if (pr.pose_count != 2 || pr.observation_count != 2 * pr.point_count || has_free_intrinsics(pr)) return false;
+  for (size_t i = 0; i < pr.point_count; ++i)
+    if (point_fixed(pr, i)) return false;
+  std::vector<uint8_t> seen(2 * pr.point_count, 0);
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    uint8_t& s = seen[2 * pr.observation_point[o] + pr.observation_pose[o]];
+    if (s) return false;  // has_repeated_pose_points (native/mod.rs:500-506)
+    s = 1;
+  }
+  std::vector<size_t> intr;
+  if (!single_pose_intrinsics(pr, &intr)) return false;
+  size_t anchor;
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) {
+    anchor = pr.gauge_first;
+  } else if (pr.poses[0].variables == 0) {
+    anchor = 0;
+  } else if (pr.poses[1].variables == 0) {
+    anchor = 1;
+  } else {
+    return false;
+  }
+  if (pr.poses[anchor].variables != 0 || pr.poses[1 - anchor].variables != OMVGBA_POSE_FREE) return false;
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) return true;
+  for (size_t k : intr) {
+    const omvgba_intrinsic& in = pr.intrinsics[k];
+    const bool undistorted = in.model == OMVGBA_CAMERA_PINHOLE ||
+                             (in.model == OMVGBA_CAMERA_BROWN_CONRADY && in.radial_kind == 0 && in.tangential_kind == 0);
+    if (!undistorted) return false;
+  }
+  return true;
+}
+
+// solve_two_view (native/two_view.rs:50-185): rebase on the anchor, refine on the device, raise,
+// and the two-view report (native/reporting.rs:143-182).
+Result solve_two_view(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+  std::vector<size_t> intr;
+  if (!single_pose_intrinsics(pr, &intr)) fail(OMVGBA_UNSUPPORTED, "two-view lowering requires one calibration per pose");
+  GaugePlan plan = gauge_plan(pr);
+  const size_t var = plan.anchor == 0 ? 1 : 0;
+  if (pr.poses[var].variables != OMVGBA_POSE_FREE || pr.poses[plan.anchor].variables != 0)
+    fail(OMVGBA_UNSUPPORTED, "direct two-view lowering requires one fixed anchor and one full-pose camera");
+  Rebase rb;
+  set_anchor(pr, rb, plan.anchor, plan.scale);
+  TwoViewProblem tv;
+  tv.angular = pr.residual_space == OMVGBA_RESIDUAL_ANGULAR;
+  pose_to_native(rb, pr.poses[var], tv.R, tv.t);
+  const size_t P = pr.point_count;
+  tv.points.resize(3 * P);
+  for (size_t i = 0; i < P; ++i) {
+    const Vec3 X = point_to_native(rb, point_at(pr, i));
+    for (int k = 0; k < 3; ++k) tv.points[3 * i + k] = X[k];
+  }
+  std::vector<int64_t> at(2 * P, -1);
+  for (size_t o = 0; o < pr.observation_count; ++o)
+    at[(pr.observation_pose[o] == plan.anchor ? 0 : P) + pr.observation_point[o]] = (int64_t)o;
+  if (tv.angular)
+    tv.bearing.resize(2 * 3 * P);
+  else
+    tv.obs.resize(2 * 2 * P);
+  for (int v = 0; v < 2; ++v) {
+    const omvgba_intrinsic& in = pr.intrinsics[intr[v == 0 ? plan.anchor : var]];
+    tv.cam[v][0] = in.fx;
+    tv.cam[v][1] = in.fy;
+    tv.cam[v][2] = in.cx;
+    tv.cam[v][3] = in.cy;
+    if (!tv.angular && !(std::isfinite(in.fx) && std::isfinite(in.fy) && std::isfinite(in.cx) && std::isfinite(in.cy) &&
+                         in.fx > 0.0 && in.fy > 0.0))
+      fail(OMVGBA_NUMERICAL, "two-view bundle adjustment intrinsics are invalid");
+    for (size_t i = 0; i < P; ++i) {
+      const int64_t o = at[v * P + i];
+      if (o < 0) fail(OMVGBA_UNSUPPORTED, "direct two-view lowering requires complete two-view tracks");
+      const double u = pr.observation_pixel[2 * o], w = pr.observation_pixel[2 * o + 1];
+      if (tv.angular) {
+        if (!camera_bearing(in, u, w, &tv.bearing[3 * (v * P + i)]))
+          fail(OMVGBA_NUMERICAL, "a measured pixel does not define a bearing of its camera model");
+      } else {
+        tv.obs[2 * (v * P + i)] = u;
+        tv.obs[2 * (v * P + i) + 1] = w;
+      }
+    }
+  }
+  LmOptions opt = lm_options(pr, cfg, NativeProblem{});
+  TwoViewReport tr = gpu_two_view(ctx, tv, opt);
+  Result res;
+  res.poses.assign(pr.poses, pr.poses + pr.pose_count);
+  pose_from_native(rb, tr.R, tr.t, res.poses[var].rotation, res.poses[var].center);
+  res.points.resize(3 * P);
+  for (size_t i = 0; i < P; ++i) {
+    const Vec3 X = point_from_native(rb, &tv.points[3 * i]);
+    if (!all_finite(X.data(), 3)) fail(OMVGBA_NUMERICAL, "native BA returned a non-finite point");
+    for (int k = 0; k < 3; ++k) res.points[3 * i + k] = X[k];
+  }
+  res.intrinsics.assign(pr.intrinsics, pr.intrinsics + pr.intrinsic_count);
+  omvgba_report& r = res.report;
+  std::memset(&r, 0, sizeof(r));
+  r.status = tr.status == 0 ? OMVGBA_STATUS_CONVERGED
+                            : (tr.status == 1 ? OMVGBA_STATUS_MAX_ITERATIONS
+                                              : (tr.status == 2 ? OMVGBA_STATUS_STALLED : OMVGBA_STATUS_DEGENERATE));
+  r.convergence_reason = tr.status == 0 ? tr.reason : OMVGBA_REASON_NONE;
+  r.iteration_count = tr.iterations;
+  r.initial_objective = tr.initial_cost;
+  r.final_objective = tr.final_cost;
+  r.initial_rmse = tr.initial_rmse * std::sqrt(2.0);
+  r.final_rmse = tr.final_rmse * std::sqrt(2.0);
+  r.accepted_step_count = tr.accepted;
+  r.rejected_step_count = tr.rej[0] + tr.rej[1] + tr.rej[2] + tr.rej[3];
+  r.rejected_linearization = tr.rej[0];
+  r.rejected_step_solve = tr.rej[1];
+  r.rejected_candidate = tr.rej[2];
+  r.rejected_insufficient_reduction = tr.rej[3];
+  if (!std::isfinite(tr.grad_norm) || tr.grad_norm < 0.0)
+    fail(OMVGBA_NUMERICAL, "stationarity audit requires a finite non-negative gradient norm");
+  r.has_stationarity = 1;
+  r.scaled_gradient_inf_norm = tr.grad_norm;
+  r.observability = tr.rank == 5 ? OMVGBA_OBS_FULL_RANK : OMVGBA_OBS_RANK_DEFICIENT;
+  r.has_weak_point_count = 1;
+  r.weak_point_count = tr.weak;
+  r.has_noninvertible_observation_count = 1;
+  r.noninvertible_observation_count = 0;
+  r.has_linear_solver = 1;
+  r.linear_solver = OMVGBA_SOLVER_DIRECT;
+  r.reduced_dimension = 5;
+  r.final_damping = tr.final_damping;
+  const double vals[4] = {r.initial_objective, r.final_objective, r.initial_rmse, r.final_rmse};
+  for (double v : vals)
+    if (!std::isfinite(v) || v < 0.0) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  res.unconstrained = unobserved_free_intrinsics(pr);
+  r.unconstrained_intrinsic_count = res.unconstrained.size();
+  return res;
+}
+
 Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
+  if (!(pr.residual_space != OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(pr)) && can_use_two_view(pr)) {
+    Result res = solve_two_view(ctx, pr, cfg);
+    finish_solution(pr, res);
+    canonicalize(pr, res);
+    return res;
+  }
   const auto t0 = std::chrono::steady_clock::now();
   Lowered L = lower(pr);
   const double t_lower = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1489,8 +1642,8 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
   }
   const double t_gpu = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_lower;
   Result res = raise(pr, L, rot, tr, pts, grp, nr, nr.iterative != 0);
-  res.unconstrained = held;
-  res.report.unconstrained_intrinsic_count = held.size();
+  res.unconstrained = L.n.self_cal ? held : unobserved_free_intrinsics(pr);
+  res.report.unconstrained_intrinsic_count = res.unconstrained.size();
   if (wants_post_solve_probe(pr, L.n)) apply_preflight(pr, preflight_from_prepared(ctx, pr, L, rot, tr, pts), res.report);
   finish_solution(pr, res);
   canonicalize(pr, res);
@@ -1870,6 +2023,7 @@ using namespace omvgba;
 
 struct omvgba_plan {
   Context* ctx = nullptr;
+  bool two_view = false;  // solved by the two-view path (no resident multi-view solver)
   const omvgba_problem* problem = nullptr;
   omvgba_config config{};
   Prepared prep;
@@ -2253,9 +2407,15 @@ int32_t omvgba_plan_create(omvgba_context* context, const omvgba_problem* proble
     p->problem = problem;
     p->config = *config;
     prepare_quarantine(*problem, p->config, p->prep);
-    p->lowered = lower(*p->prep.working);
-    p->options = lm_options(*p->prep.working, p->config, p->lowered.n);
-    p->resident = resident_create(p->ctx, p->lowered.n, p->options);
+    const omvgba_problem& working = *p->prep.working;
+    // a problem omvgba_solve would hand to the two-view solver keeps that route
+    p->two_view = !(working.residual_space != OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(working)) &&
+                  can_use_two_view(working);
+    if (!p->two_view) {
+      p->lowered = lower(working);
+      p->options = lm_options(working, p->config, p->lowered.n);
+      p->resident = resident_create(p->ctx, p->lowered.n, p->options);
+    }
     *plan = p.release();
     return OMVGBA_OK;
   } catch (const SolveFailure& f) {
@@ -2273,6 +2433,15 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
   try {
     const Telemetry before = telemetry_now();
     const omvgba_problem& working = *plan->prep.working;
+    if (plan->two_view) {
+      Result first = solve_two_view(plan->ctx, working, plan->config);
+      finish_solution(working, first);
+      canonicalize(working, first);
+      Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first));
+      write_solution(*plan->problem, r, solution);
+      stamp_telemetry(solution->report, before, t0);
+      return OMVGBA_OK;
+    }
     std::vector<double> rot, tr, pts, grp;
     double laps[6];
     NativeReport nr = resident_refine(plan->resident, rot, tr, pts, grp);
@@ -2292,8 +2461,8 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     }
     laps[0] = seconds_since(t0);
     Result first = raise(working, *lowered, rot, tr, pts, grp, nr, nr.iterative != 0);
-    first.unconstrained = held;
-    first.report.unconstrained_intrinsic_count = held.size();
+    first.unconstrained = lowered->n.self_cal ? held : unobserved_free_intrinsics(working);
+    first.report.unconstrained_intrinsic_count = first.unconstrained.size();
     if (wants_post_solve_probe(working, lowered->n))
       apply_preflight(working, preflight_from_prepared(plan->ctx, working, *lowered, rot, tr, pts), first.report);
     laps[1] = seconds_since(t0);
@@ -2323,6 +2492,14 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
 int32_t omvgba_plan_info_get(const omvgba_plan* plan, omvgba_plan_info* info, omvgba_error* error) {
   clear_error(error);
   if (!plan || !info) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  if (plan->two_view) {  // the two-view path keeps no resident multi-view solver
+    std::memset(info, 0, sizeof(*info));
+    info->observation_count = plan->prep.working->observation_count;
+    info->point_count = plan->prep.working->point_count;
+    info->camera_count = 2;
+    info->reduced_dimension = 5;
+    return OMVGBA_OK;
+  }
   ResidentInfo r = resident_info(plan->resident);
   std::memset(info, 0, sizeof(*info));
   info->observation_count = r.observations;
@@ -2344,6 +2521,8 @@ int32_t omvgba_plan_info_get(const omvgba_plan* plan, omvgba_plan_info* info, om
 int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32, int32_t stage, const double* x,
                                   double* y, omvgba_error* error) {
   clear_error(error);
+  if (plan && plan->two_view)
+    return write_error(error, OMVGBA_UNSUPPORTED, "a two-view plan has no reduced camera product");
   if (!plan || !x || (stage == 0 && !y)) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
   if (stage < 0 || stage > 2) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0, 1 or 2");
   if (!(std::isfinite(lambda) && lambda >= 0.0))

@@ -2688,6 +2688,582 @@ static void check_workspace_budget(const omvgba_config& cfg, const Native& n, co
                                         std::to_string(cfg.workspace_budget_bytes));
 }
 
+// Eigenvalues of a small symmetric matrix (row-major D x D) by cyclic Jacobi rotations.
+static std::vector<double> jacobi_eigenvalues(std::vector<double> A, int D) {
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, scale = 0.0;
+    for (int i = 0; i < D; ++i) {
+      scale = std::max(scale, std::fabs(A[(size_t)i * D + i]));
+      for (int j = i + 1; j < D; ++j) off += A[(size_t)i * D + j] * A[(size_t)i * D + j];
+    }
+    if (!(off > 1e-32 * scale * scale)) break;
+    for (int p = 0; p < D; ++p)
+      for (int q = p + 1; q < D; ++q) {
+        const double apq = A[(size_t)p * D + q];
+        if (apq == 0.0) continue;
+        const double app = A[(size_t)p * D + p], aqq = A[(size_t)q * D + q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < D; ++k) {
+          const double akp = A[(size_t)k * D + p], akq = A[(size_t)k * D + q];
+          A[(size_t)k * D + p] = c * akp - sn * akq;
+          A[(size_t)k * D + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < D; ++k) {
+          const double apk = A[(size_t)p * D + k], aqk = A[(size_t)q * D + k];
+          A[(size_t)p * D + k] = c * apk - sn * aqk;
+          A[(size_t)q * D + k] = sn * apk + c * aqk;
+        }
+      }
+  }
+  std::vector<double> ev(D);
+  for (int i = 0; i < D; ++i) ev[i] = A[(size_t)i * D + i];
+  return ev;
+}
+
+// unobserved_free_intrinsics (native/mod.rs:465-478): intrinsic blocks with free variables that no
+// observation uses; the calibrated, angular and two-view solutions report them unconstrained
+static std::vector<uint64_t> unobserved_free_intrinsics(const omvgba_problem& pr) {
+  std::vector<uint8_t> seen(pr.intrinsic_count, 0);
+  for (size_t o = 0; o < pr.observation_count; ++o) seen[pr.observation_intrinsic[o]] = 1;
+  std::vector<uint64_t> out;
+  for (size_t i = 0; i < pr.intrinsic_count; ++i)
+    if (!seen[i] && pr.intrinsics[i].variables != 0) out.push_back(i);
+  return out;
+}
+
+// ---- two-view bundle adjustment (native/two_view.rs, kernel/two_view/{optimizer,schur,residual}.rs) ----
+// Two cameras, the anchor fixed and the other free, every point seen once by each: the free pose
+// has 5 coordinates (rotation and the S^2 direction of a translation of fixed length, the baseline)
+// and points move in baseline units. A dense LM over the 5 x 5 reduced camera system.
+
+// has_repeated_pose_points (native/mod.rs:500-506)
+static bool has_repeated_pose_points(const omvgba_problem& pr) {
+  std::set<std::pair<uint32_t, uint32_t>> seen;
+  for (size_t o = 0; o < pr.observation_count; ++o)
+    if (!seen.insert({pr.observation_pose[o], pr.observation_point[o]}).second) return true;
+  return false;
+}
+static bool undistorted_perspective(const omvgba_intrinsic& in) {  // pinhole() (native/mod.rs:523-541)
+  return in.model == OMVGBA_CAMERA_PINHOLE || (in.model == OMVGBA_CAMERA_BROWN_CONRADY && in.radial_kind == 0 &&
+                                               in.tangential_kind == 0);
+}
+// can_use_two_view (native/two_view.rs:14-48)
+static bool can_use_two_view(const omvgba_problem& pr) {
+  if (pr.pose_count != 2 || pr.observation_count != 2 * pr.point_count || has_free_intrinsics(pr) ||
+      has_repeated_pose_points(pr))
+    return false;
+  for (size_t i = 0; i < pr.point_count; ++i)
+    if (point_fixed(pr, i)) return false;
+  std::vector<size_t> intr;
+  if (!single_pose_intrinsics(pr, &intr)) return false;
+  size_t anchor;
+  if (pr.gauge_kind == OMVGBA_GAUGE_FIXED_BASELINE) {
+    anchor = pr.gauge_first;
+  } else {
+    anchor = pr.poses[0].variables == 0 ? 0 : (pr.poses[1].variables == 0 ? 1 : 2);
+    if (anchor == 2) return false;
+  }
+  if (pr.poses[anchor].variables != 0 || pr.poses[1 - anchor].variables != OMVGBA_POSE_FREE) return false;
+  if (pr.residual_space == OMVGBA_RESIDUAL_ANGULAR) return true;
+  for (size_t k : intr)
+    if (!undistorted_perspective(pr.intrinsics[k])) return false;
+  return true;
+}
+
+struct TwoView {
+  bool angular = false;
+  double cam[2][4];                      // pixel: fx, fy, cx, cy per view
+  std::vector<Vec2> obs[2];              // pixel measurements per view
+  std::vector<Vec3> bearing[2];          // angular measurements per view
+  std::optional<Projection> project(int view, size_t index, const Vec3& X) const {
+    if (angular) return angular_projection(bearing[view][index], X);
+    const double* c = cam[view];
+    return pixel_projection(c[0], c[1], c[2], c[3], obs[view][index], X);
+  }
+};
+struct TvLocal {  // LocalLinearization (schur.rs:15-72)
+  double Hpp[5][5] = {}, Hpx[5][3] = {}, Hxx[3][3] = {}, gp[5] = {}, gx[3] = {}, cost = 0.0, sq = 0.0;
+  void accumulate(const double r[2], const double Jp[2][5], const double Jx[2][3], double sw) {
+    for (int k = 0; k < 2; ++k) {
+      const double wr = sw * r[k];
+      double wp[5], wx[3];
+      for (int a = 0; a < 5; ++a) wp[a] = sw * Jp[k][a];
+      for (int a = 0; a < 3; ++a) wx[a] = sw * Jx[k][a];
+      for (int a = 0; a < 5; ++a) {
+        gp[a] += wp[a] * wr;
+        for (int b = 0; b < 5; ++b) Hpp[a][b] += wp[a] * wp[b];
+        for (int b = 0; b < 3; ++b) Hpx[a][b] += wp[a] * wx[b];
+      }
+      for (int a = 0; a < 3; ++a) {
+        gx[a] += wx[a] * wr;
+        for (int b = 0; b < 3; ++b) Hxx[a][b] += wx[a] * wx[b];
+      }
+    }
+  }
+};
+static double tv_scaled_ginf(const double* g, const double* d, int n) {  // scaled_gradient_inf_norm (schur.rs:414-430)
+  double scale = 0.0;
+  for (int i = 0; i < n; ++i) scale = std::max(scale, d[i]);
+  if (!(std::isfinite(scale) && scale > 0.0)) {
+    for (int i = 0; i < n; ++i)
+      if (g[i] != 0.0) return kInf;
+    return 0.0;
+  }
+  const double floor = 64.0 * kEps * scale;
+  double best = 0.0;
+  for (int i = 0; i < n; ++i) best = std::max(best, std::fabs(g[i]) / std::sqrt(std::max(d[i], floor)));
+  return best;
+}
+// linearize_point (schur.rs:223-271)
+static bool tv_linearize(const TwoView& tv, const NPose& pose, const std::array<Vec3, 2>& basis, double baseline,
+                         const Vec3& X, size_t index, const Loss& loss, TvLocal* out) {
+  *out = TvLocal{};
+  auto first = tv.project(0, index, X);
+  if (!first) return false;
+  const double n1 = std::sqrt(first->residual[0] * first->residual[0] + first->residual[1] * first->residual[1]);
+  out->cost += loss.cost(n1);
+  out->sq += n1 * n1;
+  double Jp0[2][5] = {}, Jx0[2][3];
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 3; ++c) Jx0[r][c] = first->jacobian[r][c] * baseline;
+  out->accumulate(first->residual.data(), Jp0, Jx0, loss.sqrt_weight(n1));
+  const Vec3 rot = rotate(pose.R, X);
+  const Vec3 xc = {rot[0] + pose.t[0], rot[1] + pose.t[1], rot[2] + pose.t[2]};
+  auto second = tv.project(1, index, xc);
+  if (!second) return false;
+  const double n2 = std::sqrt(second->residual[0] * second->residual[0] + second->residual[1] * second->residual[1]);
+  out->cost += loss.cost(n2);
+  out->sq += n2 * n2;
+  double Jx1[2][3], Jp1[2][5];
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 3; ++c)
+      Jx1[r][c] = (second->jacobian[r][0] * pose.R[0][c] + second->jacobian[r][1] * pose.R[1][c] +
+                   second->jacobian[r][2] * pose.R[2][c]) *
+                  baseline;
+  const double m[3][5] = {{0.0, rot[2], -rot[1], baseline * basis[0][0], baseline * basis[1][0]},
+                          {-rot[2], 0.0, rot[0], baseline * basis[0][1], baseline * basis[1][1]},
+                          {rot[1], -rot[0], 0.0, baseline * basis[0][2], baseline * basis[1][2]}};
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 5; ++c)
+      Jp1[r][c] = second->jacobian[r][0] * m[0][c] + second->jacobian[r][1] * m[1][c] + second->jacobian[r][2] * m[2][c];
+  out->accumulate(second->residual.data(), Jp1, Jx1, loss.sqrt_weight(n2));
+  return true;
+}
+struct TvSystem {  // ReducedSystem (schur.rs:74-221)
+  double H[5][5] = {}, g[5] = {}, cost = 0.0, sq = 0.0, full_g[5] = {}, diag[5] = {}, point_red = 0.0,
+         point_ginf = 0.0, min_rcond = 1.0;
+  uint64_t weak = 0;
+  bool valid = true;
+  void add(const TvLocal& l, double damping) {
+    cost += l.cost;
+    sq += l.sq;
+    for (int r = 0; r < 5; ++r) {
+      full_g[r] += l.gp[r];
+      diag[r] += l.Hpp[r][r];
+    }
+    const double dx[3] = {l.Hxx[0][0], l.Hxx[1][1], l.Hxx[2][2]};
+    point_ginf = std::max(point_ginf, tv_scaled_ginf(l.gx, dx, 3));
+    Mat3 V;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) V[a][b] = l.Hxx[a][b];
+    auto f = point_block_factor(V, damping);
+    if (!f) {
+      valid = false;
+      if (damping == 0.0) {
+        weak++;
+        min_rcond = 0.0;
+      }
+      return;
+    }
+    if (damping == 0.0) {
+      const double rc = point_rcond(*f, V);
+      min_rcond = std::min(min_rcond, rc);
+      if (rc <= kPointBlockRcondThreshold) weak++;
+    }
+    const Vec3 ig = f->solve({l.gx[0], l.gx[1], l.gx[2]});
+    point_red += 0.5 * (l.gx[0] * ig[0] + l.gx[1] * ig[1] + l.gx[2] * ig[2]);
+    Vec3 ic[5];
+    for (int r = 0; r < 5; ++r) ic[r] = f->solve({l.Hpx[r][0], l.Hpx[r][1], l.Hpx[r][2]});
+    for (int r = 0; r < 5; ++r) {
+      g[r] += l.gp[r] - (l.Hpx[r][0] * ig[0] + l.Hpx[r][1] * ig[1] + l.Hpx[r][2] * ig[2]);
+      for (int c = 0; c < 5; ++c)
+        H[r][c] += l.Hpp[r][c] - (l.Hpx[r][0] * ic[c][0] + l.Hpx[r][1] * ic[c][1] + l.Hpx[r][2] * ic[c][2]);
+    }
+  }
+  double floor_() const {
+    double sc = 0.0;
+    for (double d : diag) sc = std::max(sc, d);
+    return 64.0 * kEps * std::max(sc, kMinPositive);
+  }
+  void finish_damping(double damping) {
+    const double fl = floor_();
+    for (int i = 0; i < 5; ++i) H[i][i] += damping * std::max(diag[i], fl);
+  }
+  bool is_valid() const {
+    if (!valid) return false;
+    for (int i = 0; i < 5; ++i) {
+      if (!std::isfinite(g[i])) return false;
+      for (int j = 0; j < 5; ++j)
+        if (!std::isfinite(H[i][j])) return false;
+    }
+    return true;
+  }
+  double scaled_ginf() const { return std::max(point_ginf, tv_scaled_ginf(full_g, diag, 5)); }
+  double predicted(const double step[5], double damping, double point_dn) const {
+    double quad = 0.0;
+    for (int r = 0; r < 5; ++r) {
+      double hs = 0.0;
+      for (int c = 0; c < 5; ++c) hs += H[r][c] * step[c];
+      quad += step[r] * hs;
+    }
+    double gs = 0.0;
+    for (int r = 0; r < 5; ++r) gs += g[r] * step[r];
+    const double damped = point_red - gs - 0.5 * quad;
+    const double fl = floor_();
+    double pdn = 0.0;
+    for (int r = 0; r < 5; ++r) pdn += std::max(diag[r], fl) * step[r] * step[r];
+    return damped + 0.5 * damping * (pdn + point_dn);
+  }
+  int rank() const {  // camera_hessian_diagnostics (schur.rs:338-370): spectral rank, tol 64 eps n lambda_max
+    if (!is_valid()) return 0;
+    std::vector<double> A(25);
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) A[5 * i + j] = 0.5 * (H[i][j] + H[j][i]);
+    std::vector<double> ev = jacobi_eigenvalues(A, 5);
+    double largest = 0.0;
+    for (double e : ev) largest = std::max(largest, std::fabs(e));
+    if (!(std::isfinite(largest) && largest > 0.0)) return 0;
+    const double tol = 64.0 * kEps * 5.0 * largest;
+    int r = 0;
+    for (double e : ev) r += (std::isfinite(e) && e > tol) ? 1 : 0;
+    return r;
+  }
+};
+// point_step_with_damping_norm (schur.rs:278-301)
+static bool tv_point_step(const TvLocal& l, double damping, const double ps[5], Vec3* step, double* dn) {
+  Mat3 V;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) V[a][b] = l.Hxx[a][b];
+  auto f = point_block_factor(V, damping);
+  if (!f) return false;
+  Vec3 rhs;
+  for (int c = 0; c < 3; ++c) {
+    double s = 0.0;
+    for (int p = 0; p < 5; ++p) s += l.Hpx[p][c] * ps[p];
+    rhs[c] = l.gx[c] + s;
+  }
+  const Vec3 x = f->solve(rhs);
+  *step = {-x[0], -x[1], -x[2]};
+  auto d = damping_diagonal(V);
+  if (!d) return false;
+  *dn = (*d)[0] * (*step)[0] * (*step)[0] + (*d)[1] * (*step)[1] * (*step)[1] + (*d)[2] * (*step)[2] * (*step)[2];
+  return true;
+}
+// solve_positive_definite (numerics/refine/solver.rs:281-335) for the 5 x 5 camera system
+static bool tv_solve_spd(const double A[5][5], const double b[5], double x[5]) {
+  for (int i = 0; i < 5; ++i) {
+    if (!std::isfinite(b[i])) return false;
+    for (int j = 0; j < 5; ++j)
+      if (!std::isfinite(A[i][j])) return false;
+  }
+  double L[5][5] = {};
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < j; ++k) acc += L[i][k] * L[j][k];
+      double sum = A[i][j] - acc;
+      if (!std::isfinite(sum)) return false;
+      if (i == j) {
+        if (sum <= 0.0) return false;
+        L[i][j] = std::sqrt(sum);
+      } else {
+        L[i][j] = sum / L[j][j];
+      }
+    }
+  double y[5];
+  for (int i = 0; i < 5; ++i) {
+    double sum = b[i];
+    for (int j = 0; j < i; ++j) sum -= L[i][j] * y[j];
+    y[i] = sum / L[i][i];
+  }
+  for (int i = 4; i >= 0; --i) {
+    double sum = y[i];
+    for (int j = i + 1; j < 5; ++j) sum -= L[j][i] * x[j];
+    x[i] = sum / L[i][i];
+  }
+  for (int i = 0; i < 5; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+static bool tv_metrics(const TwoView& tv, const NPose& pose, const std::vector<Vec3>& points, const Loss& loss,
+                       double* cost, double* rmse) {  // metrics (schur.rs:303-330)
+  double total = 0.0, sq = 0.0;
+  for (size_t i = 0; i < points.size(); ++i) {
+    const Vec3 rot = rotate(pose.R, points[i]);
+    const Vec3 xc = {rot[0] + pose.t[0], rot[1] + pose.t[1], rot[2] + pose.t[2]};
+    for (int v = 0; v < 2; ++v) {
+      auto p = tv.project(v, i, v == 0 ? points[i] : xc);
+      if (!p) {
+        *cost = *rmse = kInf;
+        return false;
+      }
+      const double nrm = std::sqrt(p->residual[0] * p->residual[0] + p->residual[1] * p->residual[1]);
+      total += loss.cost(nrm);
+      sq += nrm * nrm;
+    }
+  }
+  *cost = total;
+  *rmse = std::sqrt(sq / double(4 * points.size()));
+  return true;
+}
+static bool tv_reduced(const TwoView& tv, const NPose& pose, const std::array<Vec3, 2>& basis, double baseline,
+                       const std::vector<Vec3>& points, const Loss& loss, double damping, TvSystem* sys) {
+  *sys = TvSystem{};
+  for (size_t i = 0; i < points.size(); ++i) {
+    TvLocal l;
+    if (!tv_linearize(tv, pose, basis, baseline, points[i], i, loss, &l)) return false;
+    sys->add(l, damping);
+  }
+  sys->finish_damping(damping);
+  return true;
+}
+
+struct TvReport {
+  NPose pose;
+  int status;
+  int reason;
+  uint64_t iterations, accepted, rej[4];
+  double initial_cost, final_cost, initial_rmse, final_rmse, grad_norm, final_damping;
+  int rank;
+  uint64_t weak;
+};
+
+// refine_ba_2view (kernel/two_view/optimizer.rs:16-240)
+static TvReport refine_two_view(NPose pose, std::vector<Vec3>& points, const TwoView& tv, const Options& opt) {
+  if (points.size() < 5) fail(OMVGBA_NUMERICAL, "two-view bundle adjustment needs at least 5 points");
+  const double baseline = norm3(pose.t);
+  if (!all_finite(pose.t.data(), 3) || !(std::isfinite(baseline) && baseline > 64.0 * kEps))
+    fail(OMVGBA_NUMERICAL, "two-view bundle adjustment translation is invalid");
+  for (size_t i = 0; i < points.size(); ++i) {  // validate_projection_domain (optimizer.rs:396-415)
+    const Vec3 rot = rotate(pose.R, points[i]);
+    const Vec3 xc = {rot[0] + pose.t[0], rot[1] + pose.t[1], rot[2] + pose.t[2]};
+    if (!tv.project(0, i, points[i]) || !tv.project(1, i, xc))
+      fail(OMVGBA_NUMERICAL, "two-view bundle adjustment point " + std::to_string(i) + " is not projectable");
+  }
+  TvReport rep{};
+  tv_metrics(tv, pose, points, opt.loss, &rep.initial_cost, &rep.initial_rmse);
+  const auto st = stages(opt.loss, opt.max_iterations);
+  const int target = final_stage_index(st);
+  RunState run(1e-4);
+  bool done = false;
+  for (int si = 0; si < 3 && !done; ++si) {
+    for (uint64_t it = 0; it < st[si].max_iterations; ++it) {
+      run.iterations++;
+      const double lambda = run.damping.value;
+      const Vec3 dir = {pose.t[0] / baseline, pose.t[1] / baseline, pose.t[2] / baseline};
+      const auto basis = s2_tangent_basis(dir);
+      TvSystem sys;
+      if (!tv_reduced(tv, pose, basis, baseline, points, st[si].loss, lambda, &sys) || !sys.is_valid()) {
+        run.rej_lin++;
+        run.damping.reject();
+        continue;
+      }
+      const double current = sys.cost;
+      if (si == target && run.gradient_converged(sys.scaled_ginf(), current, opt.criteria)) {
+        done = true;
+        break;
+      }
+      double raw[5], step[5];
+      if (!tv_solve_spd(sys.H, sys.g, raw)) {
+        run.rej_solve++;
+        run.damping.reject();
+        continue;
+      }
+      for (int k = 0; k < 5; ++k) step[k] = -raw[k];
+      {  // limit_pose_step (optimizer.rs:432-443)
+        const double rn = std::sqrt(step[0] * step[0] + step[1] * step[1] + step[2] * step[2]);
+        const double tn = std::sqrt(step[3] * step[3] + step[4] * step[4]);
+        const double len = std::max(rn, tn);
+        if (len > 0.5)
+          for (double& v : step) v *= 0.5 / len;
+      }
+      NPose cand;  // retract_pose (optimizer.rs:365-381)
+      cand.R = mat_mul(exp_so3({step[0], step[1], step[2]}), pose.R);
+      const Vec3 nd = retract_s2(dir, basis, step[3], step[4]);
+      cand.t = {baseline * nd[0], baseline * nd[1], baseline * nd[2]};
+      // candidate_cost (optimizer.rs:270-305)
+      double cand_cost = 0.0, pss = 0.0, pdn = 0.0;
+      bool ok = true;
+      std::vector<Vec3> moved(points.size());
+      for (size_t i = 0; i < points.size() && ok; ++i) {
+        TvLocal l;
+        Vec3 dx;
+        double dn;
+        if (!tv_linearize(tv, pose, basis, baseline, points[i], i, st[si].loss, &l) ||
+            !tv_point_step(l, lambda, step, &dx, &dn)) {
+          ok = false;
+          break;
+        }
+        moved[i] = {points[i][0] + baseline * dx[0], points[i][1] + baseline * dx[1], points[i][2] + baseline * dx[2]};
+        const Vec3 rot = rotate(cand.R, moved[i]);
+        const Vec3 xc = {rot[0] + cand.t[0], rot[1] + cand.t[1], rot[2] + cand.t[2]};
+        auto p0 = tv.project(0, i, moved[i]);
+        auto p1 = tv.project(1, i, xc);
+        if (!p0 || !p1) {
+          ok = false;
+          break;
+        }
+        cand_cost += st[si].loss.cost(std::sqrt(p0->residual[0] * p0->residual[0] + p0->residual[1] * p0->residual[1]));
+        cand_cost += st[si].loss.cost(std::sqrt(p1->residual[0] * p1->residual[0] + p1->residual[1] * p1->residual[1]));
+        pss += dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+        pdn += dn;
+      }
+      if (!ok) {
+        run.rej_cand++;
+        run.damping.reject();
+        continue;
+      }
+      const double point_rms = std::sqrt(pss / double(points.size()));
+      const double reduction = current - cand_cost;
+      const double predicted = sys.predicted(step, lambda, pdn);
+      if (run.accept_gain(reduction, predicted)) {
+        points = moved;  // commit_points: the same back-substitution at the same state
+        pose = cand;
+        double ss = 0.0;
+        for (double v : step) ss += v * v;
+        const double prms = std::sqrt(ss / 5.0);
+        const double sn = std::sqrt(prms * prms + point_rms * point_rms);
+        const bool is_target = si == target;
+        Criterion cc = run.record_accepted(sn, reduction, current, is_target, opt.criteria);
+        if (is_target && run.certify(cc)) {
+          done = true;
+          break;
+        }
+      }
+    }
+  }
+  const double baseline2 = baseline;
+  const Vec3 dir = {pose.t[0] / baseline2, pose.t[1] / baseline2, pose.t[2] / baseline2};
+  TvSystem fin;
+  const bool have = tv_reduced(tv, pose, s2_tangent_basis(dir), baseline, points, opt.loss, 0.0, &fin);
+  rep.rank = have ? fin.rank() : 0;
+  rep.weak = have ? fin.weak : points.size();
+  rep.status = run.status(rep.rank == 5 && rep.weak == 0);
+  rep.reason = (int)run.convergence;
+  rep.grad_norm = (have && fin.is_valid()) ? fin.scaled_ginf() : kInf;
+  if (have) {
+    rep.final_cost = fin.cost;
+    rep.final_rmse = std::sqrt(fin.sq / double(4 * points.size()));
+  } else {
+    tv_metrics(tv, pose, points, opt.loss, &rep.final_cost, &rep.final_rmse);
+  }
+  rep.pose = pose;
+  rep.iterations = run.iterations;
+  rep.accepted = run.accepted;
+  rep.rej[0] = run.rej_lin;
+  rep.rej[1] = run.rej_solve;
+  rep.rej[2] = run.rej_cand;
+  rep.rej[3] = run.rej_insuff;
+  rep.final_damping = run.damping.value;
+  return rep;
+}
+
+// solve_two_view (native/two_view.rs:50-185)
+static Result solve_two_view(const omvgba_problem& pr, const omvgba_config& cfg) {
+  std::vector<size_t> intr;
+  if (!single_pose_intrinsics(pr, &intr))
+    fail(OMVGBA_UNSUPPORTED, "two-view lowering requires one calibration per pose");
+  GaugePlan plan = gauge_plan(pr);
+  const size_t var = plan.anchor == 0 ? 1 : 0;
+  if (pr.poses[var].variables != OMVGBA_POSE_FREE || pr.poses[plan.anchor].variables != 0)
+    fail(OMVGBA_UNSUPPORTED, "direct two-view lowering requires one fixed anchor and one full-pose camera");
+  Native n;
+  set_anchor(pr, n, plan.anchor, plan.scale);
+  NPose pose = pose_to_native(n, pr.poses[var]);
+  std::vector<Vec3> points(pr.point_count);
+  for (size_t i = 0; i < pr.point_count; ++i) points[i] = point_to_native(n, point_at(pr, i));
+  TwoView tv;
+  tv.angular = pr.residual_space == OMVGBA_RESIDUAL_ANGULAR;
+  std::vector<int> have[2] = {std::vector<int>(pr.point_count, -1), std::vector<int>(pr.point_count, -1)};
+  for (size_t o = 0; o < pr.observation_count; ++o) {
+    const int view = pr.observation_pose[o] == plan.anchor ? 0 : 1;
+    have[view][pr.observation_point[o]] = (int)o;
+  }
+  for (int v = 0; v < 2; ++v) {
+    const omvgba_intrinsic& in = pr.intrinsics[intr[v == 0 ? plan.anchor : var]];
+    tv.cam[v][0] = in.fx;
+    tv.cam[v][1] = in.fy;
+    tv.cam[v][2] = in.cx;
+    tv.cam[v][3] = in.cy;
+    if (!tv.angular && !(std::isfinite(in.fx) && std::isfinite(in.fy) && std::isfinite(in.cx) && std::isfinite(in.cy) &&
+                         in.fx > 0.0 && in.fy > 0.0))
+      fail(OMVGBA_NUMERICAL, "two-view bundle adjustment intrinsics are invalid");
+    for (size_t i = 0; i < pr.point_count; ++i) {
+      const int o = have[v][i];
+      if (o < 0) fail(OMVGBA_UNSUPPORTED, "direct two-view lowering requires complete two-view tracks");
+      const Vec2 px = {pr.observation_pixel[2 * o], pr.observation_pixel[2 * o + 1]};
+      tv.obs[v].push_back(px);
+      if (tv.angular) {
+        auto b = camera_bearing(in, px[0], px[1]);
+        if (!b) fail(OMVGBA_NUMERICAL, "a measured pixel does not define a bearing of its camera model");
+        tv.bearing[v].push_back(*b);
+      }
+    }
+  }
+  Options opt;
+  opt.max_iterations = cfg.max_iterations;
+  opt.loss = problem_loss(pr);
+  opt.criteria = {cfg.gradient_tolerance, cfg.parameter_tolerance, cfg.function_tolerance};
+  TvReport tr = refine_two_view(pose, points, tv, opt);
+  Result res;
+  res.poses.assign(pr.poses, pr.poses + pr.pose_count);
+  pose_from_native(n, tr.pose, res.poses[var].rotation, res.poses[var].center);
+  res.points.resize(3 * pr.point_count);
+  for (size_t i = 0; i < pr.point_count; ++i) {
+    const Vec3 X = point_from_native(n, points[i]);
+    for (int k = 0; k < 3; ++k) res.points[3 * i + k] = X[k];
+  }
+  res.intrinsics.assign(pr.intrinsics, pr.intrinsics + pr.intrinsic_count);
+  omvgba_report& r = res.report;  // two_view_solve_report (native/reporting.rs:143-182)
+  std::memset(&r, 0, sizeof(r));
+  r.status = tr.status == 0 ? OMVGBA_STATUS_CONVERGED
+                            : (tr.status == 1 ? OMVGBA_STATUS_MAX_ITERATIONS
+                                              : (tr.status == 2 ? OMVGBA_STATUS_STALLED : OMVGBA_STATUS_DEGENERATE));
+  r.convergence_reason = tr.status == 0 ? tr.reason : OMVGBA_REASON_NONE;
+  r.iteration_count = tr.iterations;
+  r.initial_objective = tr.initial_cost;
+  r.final_objective = tr.final_cost;
+  r.initial_rmse = tr.initial_rmse * std::sqrt(2.0);
+  r.final_rmse = tr.final_rmse * std::sqrt(2.0);
+  r.accepted_step_count = tr.accepted;
+  r.rejected_step_count = tr.rej[0] + tr.rej[1] + tr.rej[2] + tr.rej[3];
+  r.rejected_linearization = tr.rej[0];
+  r.rejected_step_solve = tr.rej[1];
+  r.rejected_candidate = tr.rej[2];
+  r.rejected_insufficient_reduction = tr.rej[3];
+  if (!std::isfinite(tr.grad_norm) || tr.grad_norm < 0.0)
+    fail(OMVGBA_NUMERICAL, "stationarity audit requires a finite non-negative gradient norm");
+  r.has_stationarity = 1;
+  r.scaled_gradient_inf_norm = tr.grad_norm;
+  r.observability = tr.rank == 5 ? OMVGBA_OBS_FULL_RANK : OMVGBA_OBS_RANK_DEFICIENT;
+  r.has_weak_point_count = 1;
+  r.weak_point_count = tr.weak;
+  r.has_noninvertible_observation_count = 1;
+  r.noninvertible_observation_count = 0;
+  r.has_linear_solver = 1;
+  r.linear_solver = OMVGBA_SOLVER_DIRECT;
+  r.reduced_dimension = 5;
+  r.final_damping = tr.final_damping;
+  double vals[4] = {r.initial_objective, r.final_objective, r.initial_rmse, r.final_rmse};
+  for (double v : vals)
+    if (!std::isfinite(v) || v < 0.0) fail(OMVGBA_INTERNAL, "bundle-adjustment report is invalid");
+  res.unconstrained = unobserved_free_intrinsics(pr);
+  r.unconstrained_intrinsic_count = res.unconstrained.size();
+  return res;
+}
+
 // The lowering solve_once chooses (native/mod.rs:352-367): angular residuals (fixed intrinsics
 // only), self-calibration, or the calibrated pixel problem.
 static Native lower_native(const omvgba_problem& pr) {
@@ -2847,6 +3423,12 @@ static Preflight preflight(const omvgba_problem& pr, const omvgba_config& cfg) {
 
 static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   validate_config(cfg);
+  if (!(pr.residual_space != OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(pr)) && can_use_two_view(pr)) {
+    Result res = solve_two_view(pr, cfg);
+    finish_solution(pr, res);
+    canonicalize(pr, res);
+    return res;
+  }
   double t0 = oracle_now();
   Native n = lower_native(pr);
   oracle_phase("lowering", t0);
@@ -2885,8 +3467,8 @@ static Result solve_once(const omvgba_problem& pr, const omvgba_config& cfg) {
   }
   t0 = oracle_now();
   Result res = raise(pr, n, poses, points, groups, nr, opt.iterative);
-  res.unconstrained = held;
-  res.report.unconstrained_intrinsic_count = held.size();
+  res.unconstrained = n.self_cal ? held : unobserved_free_intrinsics(pr);
+  res.report.unconstrained_intrinsic_count = res.unconstrained.size();
   if (wants_post_solve_probe(pr, n)) apply_preflight(pr, probe_prepared(pr, n, poses, points), res.report);
   finish_solution(pr, res);
   canonicalize(pr, res);

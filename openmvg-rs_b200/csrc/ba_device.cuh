@@ -468,7 +468,12 @@ BA_HD bool point_damping_diagonal(const double V[6], double d[3]) {
   d[2] = fmax(V[5], fl);
   return true;
 }
-BA_HD bool point_factor(const double V[6], double lambda, double damped[6], double inv[6]) {
+// With fac non-null it also receives N = (S L)^-1 (S the scaling, L the factor of the scaled block),
+// lower packed like inv: Vhat^-1 = N^T N. Applying N and then N^T to a vector is linear and
+// symmetric to rounding even for a badly conditioned block, where a product with the explicit
+// inverse is not: a track-2 point close to a camera centre (cond 1e9) gives that product rounding
+// noise near 1e-5 of its size, which changes from one vector to the next.
+BA_HD bool point_factor(const double V[6], double lambda, double damped[6], double inv[6], double* fac = nullptr) {
   double d[3];
   if (!point_damping_diagonal(V, d)) return false;
   double a[3][3] = {{V[0] + lambda * d[0], V[1], V[3]}, {V[1], V[2] + lambda * d[1], V[4]}, {V[3], V[4], V[5] + lambda * d[2]}};
@@ -504,6 +509,14 @@ BA_HD bool point_factor(const double V[6], double lambda, double damped[6], doub
   inv[3] = (m22 * m20) * (d2 * d0);
   inv[4] = (m22 * m21) * (d2 * d1);
   inv[5] = (m22 * m22) * (d2 * d2);
+  if (fac) {
+    fac[0] = m00 * d0;
+    fac[1] = m10 * d0;
+    fac[2] = m11 * d1;
+    fac[3] = m20 * d0;
+    fac[4] = m21 * d1;
+    fac[5] = m22 * d2;
+  }
   return true;
 }
 BA_HD void sym3_apply(const double P[6], const double x[3], double y[3]) {

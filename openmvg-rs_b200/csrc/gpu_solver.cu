@@ -436,6 +436,7 @@ struct LinOut {
   int rs32;
   double* rw;      // N x 2, sqrt-weighted residual
   double* vinv;    // P x 6: damped point-block inverse (zero for fixed points)
+  double* vfac;    // P x 6: its factor N, Vhat^-1 = N^T N (zero for fixed points), for the tile product
   double* ig;      // P x 3: Vhat^-1 g_p (zero for fixed points)
   double* gp;      // P x 3: point gradient
   double* ddiag;   // P x 3: damping diagonal
@@ -487,8 +488,9 @@ __device__ __forceinline__ void point_epilogue(const DevView& v, uint32_t p, con
                                                double cost, double sq, bool ok, double lambda, LinOut<T>& out) {
   PointSummary sm{0, 0, 0, 0, 1.0, 0, 0, 0};
   double* vi = out.vinv + 6 * (size_t)p;
+  double* vf = out.vfac + 6 * (size_t)p;
   double* ig = out.ig + 3 * (size_t)p;
-  for (int k = 0; k < 6; ++k) vi[k] = 0.0;
+  for (int k = 0; k < 6; ++k) vi[k] = vf[k] = 0.0;
   ig[0] = ig[1] = ig[2] = 0.0;
   out.gp[3 * (size_t)p] = gp[0];
   out.gp[3 * (size_t)p + 1] = gp[1];
@@ -517,8 +519,8 @@ __device__ __forceinline__ void point_epilogue(const DevView& v, uint32_t p, con
     }
     sm.grad_norm = gn;
   }
-  double damped[6], inv[6];
-  if (!point_factor(V, lambda, damped, inv)) {
+  double damped[6], inv[6], fac[6];
+  if (!point_factor(V, lambda, damped, inv, fac)) {
     sm.invalid = 1;
     if (lambda == 0.0) {
       sm.weak = 1;
@@ -540,7 +542,10 @@ __device__ __forceinline__ void point_epilogue(const DevView& v, uint32_t p, con
   double igv[3];
   sym3_apply(inv, gp, igv);
   sm.point_red = 0.5 * (gp[0] * igv[0] + gp[1] * igv[1] + gp[2] * igv[2]);
-  for (int k = 0; k < 6; ++k) vi[k] = inv[k];
+  for (int k = 0; k < 6; ++k) {
+    vi[k] = inv[k];
+    vf[k] = fac[k];
+  }
   ig[0] = igv[0];
   ig[1] = igv[1];
   ig[2] = igv[2];
@@ -2271,7 +2276,7 @@ struct Solver {
   TileSet T64, T32;
   TileSetDev dT64, dT32;
   bool mixed = false;
-  DBuf<double> d_rw, d_vinv, d_ig, d_gp, d_ddiag;
+  DBuf<double> d_rw, d_vinv, d_vfac, d_ig, d_gp, d_ddiag;
   DBuf<PointSummary> d_summary, d_summary_part;
   DBuf<int> d_blk_off, d_blk_dim, d_blk_col, d_blk_edge, d_chunk_block, d_chunk_col, d_blk_chunk_begin, d_blk_chunk_end;
   DBuf<uint32_t> d_ent, d_ent_point, d_chunk_begin, d_chunk_end;
@@ -2377,12 +2382,12 @@ struct Solver {
   DevState state(int which) const { return {d_pose[which].p, d_points[which].p, d_groups[which].p}; }
   // the FP32 records of mixed precision (assembly, pairs and candidate read them, computing in FP64)
   LinOut<float> lin32() const {
-    return {d_rec32.p, dT32.obs_rec.p, mv_tile_obs<float>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_ig.p, d_gp.p,
-            d_ddiag.p, d_summary.p, nullptr};
+    return {d_rec32.p, dT32.obs_rec.p, mv_tile_obs<float>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_vfac.p, d_ig.p,
+            d_gp.p, d_ddiag.p, d_summary.p, nullptr};
   }
   LinOut<T> lin() const {
-    return {d_rec.p, dT64.obs_rec.p, mv_tile_obs<T>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_ig.p, d_gp.p,
-            d_ddiag.p, d_summary.p, nullptr};
+    return {d_rec.p, dT64.obs_rec.p, mv_tile_obs<T>(), nullptr, nullptr, 0, d_rw.p, d_vinv.p, d_vfac.p, d_ig.p,
+            d_gp.p, d_ddiag.p, d_summary.p, nullptr};
   }
   BlockTables tables() const {
     BlockTables b;
@@ -2484,6 +2489,7 @@ struct Solver {
     }
     d_rw.alloc((size_t)2 * N, st);
     d_vinv.alloc((size_t)6 * P, st);
+    d_vfac.alloc((size_t)6 * P, st);
     d_ig.alloc((size_t)3 * P, st);
     d_gp.alloc((size_t)3 * P, st);
     d_ddiag.alloc((size_t)3 * P, st);
@@ -2917,13 +2923,13 @@ struct Solver {
     MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
     if (mt.ntiles > 0) {
       if (fp32)
-        launch_pdl(pdl, k_mv_tiles<float, float>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vinv.p, x,
+        launch_pdl(pdl, k_mv_tiles<float, float>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vfac.p, x,
                    ts.partial.p, ctl);
       else if (mixed)  // FP64 arithmetic on the FP32 records: the refinement's residual product
-        launch_pdl(pdl, k_mv_tiles<float, double>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vinv.p, x,
+        launch_pdl(pdl, k_mv_tiles<float, double>, mt.ntiles, mv_tile_obs<float>(), st, mt, d_rec32.p, d_vfac.p, x,
                    ts.partial.p, ctl);
       else
-        launch_pdl(pdl, k_mv_tiles<T, T>, mt.ntiles, mv_tile_obs<T>(), st, mt, d_rec.p, d_vinv.p, x, ts.partial.p,
+        launch_pdl(pdl, k_mv_tiles<T, T>, mt.ntiles, mv_tile_obs<T>(), st, mt, d_rec.p, d_vfac.p, x, ts.partial.p,
                    ctl);
     }
   }

@@ -99,7 +99,7 @@ __device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
 // R = float is the FP64 product of FP32-stored Jacobians that mixed-precision refinement uses).
 template <typename R, typename T = R>
 __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 : 2)
-    k_mv_tiles(MvTiles mt, const R* __restrict__ rec, const double* __restrict__ vinv, const double* __restrict__ x,
+    k_mv_tiles(MvTiles mt, const R* __restrict__ rec, const double* __restrict__ vfac, const double* __restrict__ x,
                double* __restrict__ partial, const PcgCtl* ctl) {
   constexpr int TILE = mv_tile_obs<R>();
   constexpr int TS = TILE + 1;  // padded row stride: the 9 parameter rows of one column use 9 banks
@@ -137,12 +137,15 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
   const uint32_t my_pt = __ldg(reinterpret_cast<const uint16_t*>(slot + MvSlot::lpt(TILE)) + tid);
   const uint32_t my_pos = __ldg(reinterpret_cast<const uint16_t*>(slot + MvSlot::pos(TILE)) + tid);
   const uint32_t nobs = hdr.x, npt = hdr.y, nseg = hdr.z, p0 = hdr.w;
-  // P2's inverse rows for the first TILE / 4 points, requested as soon as the header is in
+  // P2's factor entries for the first TILE / 4 points, requested as soon as the header is in. Lane
+  // kq of a point's quad loads entries i0, i1, i2 of the packed lower factor N (Vhat^-1 = N^T N):
+  // row kq of N is (v0, 0, 0), (v0, v1, 0), (v0, v1, v2) and column kq is (v0, v1, v2), (0, v1, v2),
+  // (0, 0, v2) for kq = 0, 1, 2.
   const uint32_t lp0 = tid >> 2, kq = tid & 3;
   const int i0 = kq == 0 ? 0 : (kq == 1 ? 1 : 3), i1 = kq == 0 ? 1 : (kq == 1 ? 2 : 4), i2 = kq == 0 ? 3 : (kq == 1 ? 4 : 5);
   double v0 = 0.0, v1 = 0.0, v2 = 0.0;
   if (lp0 < npt && kq < 3) {
-    const double* vi = vinv + 6 * (size_t)(p0 + lp0);
+    const double* vi = vfac + 6 * (size_t)(p0 + lp0);
     v0 = __ldg(vi + i0);
     v1 = __ldg(vi + i1);
     v2 = __ldg(vi + i2);
@@ -199,8 +202,9 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
     terms[2 * TS + tid] = jp[2] * e0 + jp[5] * e1;
   }
   __syncthreads();
-  // P2: z_p = Vhat_p^-1 sum_o Jp_o^T e_o; lanes 4q..4q+2 of a warp sum the three components of
-  // point q's track (in track order), lane 4q+3 idles; the sums are exchanged by shuffles.
+  // P2: z_p = Vhat_p^-1 sum_o Jp_o^T e_o = N^T (N b); lanes 4q..4q+2 of a warp sum the three
+  // components of point q's track (in track order), lane 4q+3 idles; b and then u = N b are exchanged
+  // by shuffles.
   for (uint32_t base = 0; base < npt; base += TILE / 4) {
     const uint32_t lp = base + lp0;
     const bool active = lp < npt && kq < 3;
@@ -209,8 +213,8 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
       const T* row = terms + kq * TS;
       const uint32_t e = pt_begin[lp + 1];
       for (uint32_t i = pt_begin[lp]; i < e; ++i) bk += row[i];
-      if (base > 0) {  // points past the first TILE / 4: their inverse rows load here
-        const double* vi = vinv + 6 * (size_t)(p0 + lp);
+      if (base > 0) {  // points past the first TILE / 4: their factor entries load here
+        const double* vi = vfac + 6 * (size_t)(p0 + lp);
         v0 = __ldg(vi + i0);
         v1 = __ldg(vi + i1);
         v2 = __ldg(vi + i2);
@@ -219,8 +223,11 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
     const int lead = (tid & 31) & ~3;
     const T b0 = __shfl_sync(0xffffffffu, bk, lead), b1 = __shfl_sync(0xffffffffu, bk, lead + 1),
             b2 = __shfl_sync(0xffffffffu, bk, lead + 2);
-    // row kq of the packed symmetric inverse (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
-    if (active) zz[kq * TILE + lp] = (T)v0 * b0 + (T)v1 * b1 + (T)v2 * b2;
+    const T n0 = (T)v0, n1 = (T)v1, n2 = (T)v2;
+    const T uk = n0 * b0 + (kq >= 1 ? n1 * b1 : (T)0) + (kq == 2 ? n2 * b2 : (T)0);  // (N b)_kq
+    const T u0 = __shfl_sync(0xffffffffu, uk, lead), u1 = __shfl_sync(0xffffffffu, uk, lead + 1),
+            u2 = __shfl_sync(0xffffffffu, uk, lead + 2);
+    if (active) zz[kq * TILE + lp] = (kq == 0 ? n0 * u0 : (T)0) + (kq <= 1 ? n1 * u1 : (T)0) + n2 * u2;
   }
   __syncthreads();
   // P3: f = e - Jp z and the camera terms Jc^T f in segment order (the point terms are dead)

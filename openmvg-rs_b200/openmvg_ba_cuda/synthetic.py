@@ -86,7 +86,8 @@ def _perturb(rng, R, C, X, rot=0.01, trans=0.05, pts=0.02):
 
 
 def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_calibrating: bool = False,
-                 loss: RobustLoss | None = None, radius: float = 10.0) -> BundleProblem:
+                 loss: RobustLoss | None = None, radius: float = 10.0,
+                 pose_variables: np.ndarray | None = None) -> BundleProblem:
     """20 radial3 cameras on a ring of radius 10 looking at points uniform in [-1, 1]^3.
 
     At radius 10 the cube spans about +-50 px, where radial distortion is barely observable; a
@@ -95,6 +96,10 @@ def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_cali
     ``self_calibrating=False``: fixed Brown-Conrady (k1, k2, k3) intrinsics.
     ``self_calibrating=True``: one shared Brown-Conrady K1K2 group with free (f, k1, k2) and a fixed
     principal point (the reference rejects free cx, cy or k3).
+
+    ``pose_variables``: per-pose ``POSE_*`` bits; the parts of a pose that a mask holds (the rotation
+    without ``POSE_ROTATION``, the centre without ``POSE_TRANSLATION``) keep their true values, so a
+    masked solve is consistent with the observations.
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     ang = 2 * np.pi * np.arange(cameras) / cameras
@@ -110,6 +115,11 @@ def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_cali
     pix, _ = _project(R[obs_pose], C[obs_pose], X[obs_point], f, cx, cy, k1, k2, k3)
     obs = _noisy(rng, pix)
     Rp, Cp, Xp = _perturb(rng, R, C, X)
+    masks = np.full(cameras, abi.POSE_FREE, dtype=np.uint32)
+    if pose_variables is not None:
+        masks = np.asarray(pose_variables, dtype=np.uint32)
+        Rp = np.where(((masks & abi.POSE_ROTATION) == 0)[:, None, None], R, Rp)
+        Cp = np.where(((masks & abi.POSE_TRANSLATION) == 0)[:, None], C, Cp)
     if self_calibrating:
         intr = CameraIntrinsics(model=abi.CAMERA_BROWN_CONRADY, fx=505.0, fy=505.0, cx=cx, cy=cy,
                                 radial_kind=abi.RADIAL_K1K2, k1=-0.09, k2=0.0,
@@ -118,8 +128,8 @@ def ring_problem(seed: int = 7, cameras: int = 20, points: int = 2000, self_cali
         intr = CameraIntrinsics(model=abi.CAMERA_BROWN_CONRADY, fx=f, fy=f, cx=cx, cy=cy,
                                 radial_kind=abi.RADIAL_K1K2K3, k1=k1, k2=k2, k3=k3)
     return BundleProblem(
-        rotations=Rp, centers=Cp, pose_variables=np.full(cameras, abi.POSE_FREE, dtype=np.uint32),
-        intrinsics=[intr], points=Xp, point_fixed=np.zeros(points, dtype=np.uint8),
+        rotations=Rp, centers=Cp, pose_variables=masks, intrinsics=[intr], points=Xp,
+        point_fixed=np.zeros(points, dtype=np.uint8),
         observation_pose=obs_pose, observation_intrinsic=np.zeros(len(obs_pose), dtype=np.uint32),
         observation_point=obs_point, observation_pixel=obs,
         robust_loss=loss if loss is not None else RobustLoss.huber(1.0), gauge=Gauge(),

@@ -219,6 +219,25 @@ pub struct omvgba_solution {
     pub report: omvgba_report,
 }
 
+#[repr(C)]
+#[derive(Clone, Copy)]
+pub struct omvgba_preflight {
+    pub status: i32,
+    pub has_counts: i32,
+    pub pose_dimension: u64,
+    pub covered_free_pose_count: u64,
+    pub weak_point_count: u64,
+    pub dense_observability_escalation: i32,
+    pub reserved: i32,
+}
+
+// omvgba_preflight_status
+pub const OMVGBA_PREFLIGHT_PROCEED: i32 = 0;
+pub const OMVGBA_PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE: i32 = 1;
+pub const OMVGBA_PREFLIGHT_RESOURCE_LIMIT: i32 = 2;
+pub const OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY: i32 = 3;
+pub const OMVGBA_PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED: i32 = 4;
+
 /// Opaque per-thread solver context.
 #[repr(C)]
 pub struct omvgba_context {
@@ -238,6 +257,13 @@ unsafe extern "C" {
         problem: *const omvgba_problem,
         config: *const omvgba_config,
         solution: *mut omvgba_solution,
+        error: *mut omvgba_error,
+    ) -> i32;
+    pub fn omvgba_preflight_check(
+        context: *mut omvgba_context,
+        problem: *const omvgba_problem,
+        config: *const omvgba_config,
+        preflight: *mut omvgba_preflight,
         error: *mut omvgba_error,
     ) -> i32;
 }

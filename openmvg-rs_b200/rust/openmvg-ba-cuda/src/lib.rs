@@ -46,6 +46,27 @@ impl Default for CudaOptions {
     }
 }
 
+/// `NativePreflightStatus` (crates/openmvg-ba/src/native/mod.rs:120-141).
+#[derive(Clone, Copy, Debug, PartialEq, Eq)]
+pub enum CudaPreflightStatus {
+    Proceed,
+    InsufficientCameraCoverage,
+    ResourceLimit,
+    WeakPointGeometry,
+    ObservabilityNotCertified,
+}
+
+/// `NativePreflight` (crates/openmvg-ba/src/native/mod.rs:143-165); the counts are `None` when the
+/// check did not run.
+#[derive(Clone, Copy, Debug, PartialEq, Eq)]
+pub struct CudaPreflight {
+    pub status: CudaPreflightStatus,
+    pub pose_dimension: Option<usize>,
+    pub covered_free_pose_count: Option<usize>,
+    pub weak_point_count: Option<usize>,
+    pub dense_observability_escalation: bool,
+}
+
 /// One solver context on one CUDA device. `Send` but not `Sync`: the context is used through
 /// `&mut self` only, one solve at a time, as the trait requires.
 pub struct CudaBundleAdjuster {
@@ -74,6 +95,40 @@ impl CudaBundleAdjuster {
             return Err(SolveError::Internal(format!("CUDA context on device {device}: {}", error.text())));
         }
         Ok(Self { context, device, options })
+    }
+
+    /// The translation-only observability check openmvg-sfm runs before a bundle adjustment of
+    /// camera positions with fixed rotations (`NativeBundleAdjuster::preflight`,
+    /// crates/openmvg-ba/src/native/mod.rs:184-230). `NativePreflight` cannot be built outside
+    /// openmvg-ba, so the outcome comes back as this crate's `CudaPreflight` with the same fields.
+    pub fn preflight(&mut self, problem: &BundleProblem, config: &SolveConfig) -> Result<CudaPreflight, SolveError> {
+        config.validate()?;
+        let marshalled = marshal(problem)?;
+        let view = problem_view(problem, &marshalled);
+        let cfg = config_view(config, self.device, &self.options);
+        // SAFETY: an all-zero preflight is a valid value of this plain C struct; the call overwrites it.
+        let mut out: ffi::omvgba_preflight = unsafe { std::mem::zeroed() };
+        let mut error = ffi::omvgba_error::zeroed();
+        // SAFETY: `view` points into `marshalled`, which outlives the call; `out` and `error` are
+        // valid out-pointers; the context is ours.
+        let code = unsafe { ffi::omvgba_preflight_check(self.context, &view, &cfg, &mut out, &mut error) };
+        if code != ffi::OMVGBA_OK {
+            return Err(to_solve_error(code, &error));
+        }
+        let count = |value: u64| (out.has_counts != 0).then_some(value as usize);
+        Ok(CudaPreflight {
+            status: match out.status {
+                ffi::OMVGBA_PREFLIGHT_PROCEED => CudaPreflightStatus::Proceed,
+                ffi::OMVGBA_PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE => CudaPreflightStatus::InsufficientCameraCoverage,
+                ffi::OMVGBA_PREFLIGHT_RESOURCE_LIMIT => CudaPreflightStatus::ResourceLimit,
+                ffi::OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY => CudaPreflightStatus::WeakPointGeometry,
+                _ => CudaPreflightStatus::ObservabilityNotCertified,
+            },
+            pose_dimension: count(out.pose_dimension),
+            covered_free_pose_count: count(out.covered_free_pose_count),
+            weak_point_count: count(out.weak_point_count),
+            dense_observability_escalation: out.dense_observability_escalation != 0,
+        })
     }
 
     /// CUDA devices visible to this process.

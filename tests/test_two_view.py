@@ -153,7 +153,12 @@ def test_gpu_two_view_matches_oracle(adjuster, case):
     for k in ("status", "iteration_count", "accepted_step_count", "observability", "weak_point_count",
               "linear_solver", "reduced_dimension", "inlier_count"):
         assert g.report[k] == o.report[k], k
-    assert abs(g.report["final_objective"] - o.report["final_objective"]) <= 1e-9 * max(o.report["final_objective"], 1e-12)
+    # 1e-9 relative, with a rounding floor for a cost near zero (noise-free pixels): residuals
+    # computed a few ulps apart (1e-13 px on 640-px coordinates) move the cost by at most
+    # sqrt(2 f m) * 1e-13 for m residual components
+    f = o.report["final_objective"]
+    floor = np.sqrt(2.0 * f * 2 * p.observation_count) * 1e-13
+    assert abs(g.report["final_objective"] - f) <= 1e-9 * f + floor
     assert np.max(np.abs(g.rotations - o.rotations)) < 1e-9
     assert np.max(np.abs(g.centers - o.centers)) < 1e-9
     assert np.max(np.abs(g.points - o.points)) < 1e-8

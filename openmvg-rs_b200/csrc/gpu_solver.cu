@@ -3314,6 +3314,7 @@ struct Solver {
     uint64_t pcg_terms = 0;
     double iter_tol = std::min(std::sqrt(opt.relative_cost_tolerance), 1e-6);
     bool done = false;
+    bool switch_pending = false;  // the Auto switch takes effect at the next assembly
     int cand = 1 - cur;
     size_t free_points = 0;
     for (int p = 0; p < P; ++p) free_points += n.fixed_points[p] ? 0 : 1;
@@ -3322,6 +3323,10 @@ struct Solver {
       for (uint64_t it = 0; it < stages[si].iters; ++it) {
         iterations++;
         double t0 = now();
+        if (switch_pending) {
+          explicit_op = true;
+          switch_pending = false;
+        }
         Gauge g = gauge_for(cur, scene);
         Assembly a = assemble(cur, g, stages[si].loss, lambda, direct || explicit_op);
         double t1 = now();
@@ -3360,8 +3365,9 @@ struct Solver {
             iterative_step = true;
             rel_res = r.rel;
             // Auto operator: once a PCG run needs many products, rebuilding the explicit S every
-            // assembly costs less than the tile products it replaces
-            if (opt.matvec == 0 && !explicit_op && r.terms >= kExplicitSwitchTerms) explicit_op = true;
+            // assembly costs less than the tile products it replaces. The switch waits for the next
+            // assembly: this step's model reduction still needs the operator it was solved with.
+            if (opt.matvec == 0 && !explicit_op && r.terms >= kExplicitSwitchTerms) switch_pending = true;
           }
         }
         double t2 = now();

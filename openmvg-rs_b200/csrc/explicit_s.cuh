@@ -448,60 +448,123 @@ __device__ __forceinline__ void acc_store(const double acc[4][4], double* g) {
     for (int a = 0; a < 4; ++a) g[(size_t)(4 * tx + b) * kCT + 4 * ty + a] = acc[a][b];
 }
 
-// POTRF of diagonal tile k (right-looking inside the tile) and the inverse W_k = L_kk^-1 of its factor
-// (column by column, forward substitution). status[0] = 0 when a pivot is not finite and positive;
-// later launches of the factorization then return at once.
+// POTRF of diagonal tile k and the inverse W_k = L_kk^-1 of its factor, both right-looking with the
+// tile in registers: thread (ty, tx) of 16 x 16 holds elements (4 ty + a, 4 tx + b). Step j of the
+// factorization publishes column j (its owners write it to shared memory, one barrier), and every
+// thread scales it by 1 / sqrt(pivot) and updates its elements right of the column; step j of the
+// inverse publishes the finished row j of W and every thread updates its rows below. The published
+// buffers alternate, so each step takes one barrier. status[0] = 0 when a pivot is not finite and
+// positive; later launches of the factorization then return at once.
 __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* status) {
-  __shared__ double A[kCT * (kCT + 1)];
-  __shared__ int fail;
+  __shared__ double Ls[kCT * (kCT + 1)];  // the tile in, then L (column-major, padded)
+  __shared__ double pub[2][kCT];
+  __shared__ double rdiag[kCT];
   if (status[0] == 0) return;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   double* g = tb.t + tile_at(tb, k, k);
   for (int w = tid; w < kCTT; w += blockDim.x) {
     const int c = w / kCT, r = w - c * kCT;
-    A[c * (kCT + 1) + r] = g[w];
-  }
-  if (tid == 0) fail = 0;
-  for (int j = 0; j < kCT; ++j) {
-    __syncthreads();
-    if (tid == 0) {
-      const double d = A[j * (kCT + 1) + j];
-      if (!(isfinite(d) && d > 0.0))
-        fail = 1;
-      else
-        A[j * (kCT + 1) + j] = sqrt(d);
-    }
-    __syncthreads();
-    if (fail) break;
-    const double piv = A[j * (kCT + 1) + j];
-    for (int i = j + 1 + tid; i < kCT; i += blockDim.x) A[j * (kCT + 1) + i] /= piv;
-    __syncthreads();
-    const int m = kCT - j - 1;
-    for (int w = tid; w < m * m; w += blockDim.x) {
-      const int c = j + 1 + w / m, i = j + 1 + w % m;
-      if (c <= i) A[c * (kCT + 1) + i] -= A[j * (kCT + 1) + i] * A[j * (kCT + 1) + c];
-    }
+    Ls[c * (kCT + 1) + r] = g[w];
   }
   __syncthreads();
-  if (fail) {
-    if (tid == 0) status[0] = 0;
-    return;
+  double a[4][4];
+#pragma unroll
+  for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) a[ai][bi] = Ls[(4 * tx + bi) * (kCT + 1) + 4 * ty + ai];
+  for (int j = 0; j < kCT; ++j) {
+    double* cj = pub[j & 1];
+    if (tx == (j >> 2)) {  // static register indices: the column is picked by selects
+      const int bj = j & 3;
+#pragma unroll
+      for (int ai = 0; ai < 4; ++ai)
+        cj[4 * ty + ai] = bj == 0 ? a[ai][0] : (bj == 1 ? a[ai][1] : (bj == 2 ? a[ai][2] : a[ai][3]));
+    }
+    __syncthreads();
+    const double d = cj[j];  // the same value in every thread: all leave together
+    if (!(isfinite(d) && d > 0.0)) {
+      if (tid == 0) status[0] = 0;
+      return;
+    }
+    const double sd = sqrt(d), rs = 1.0 / sd;
+    double li[4], lc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      li[q] = cj[4 * ty + q] * rs;
+      lc[q] = cj[4 * tx + q] * rs;
+    }
+#pragma unroll
+    for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+      for (int bi = 0; bi < 4; ++bi) {
+        const int i = 4 * ty + ai, c = 4 * tx + bi;
+        if (c == j && i >= j)
+          a[ai][bi] = i == j ? sd : li[ai];
+        else if (c > j && c <= i)
+          a[ai][bi] -= li[ai] * lc[bi];
+      }
   }
+  __syncthreads();  // every thread has read the last published column before Ls is rewritten
+#pragma unroll
+  for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) {
+      const int i = 4 * ty + ai, c = 4 * tx + bi;
+      Ls[c * (kCT + 1) + i] = i >= c ? a[ai][bi] : 0.0;
+    }
+  __syncthreads();
   for (int w = tid; w < kCTT; w += blockDim.x) {
     const int c = w / kCT, r = w - c * kCT;
-    g[w] = r >= c ? A[c * (kCT + 1) + r] : 0.0;
+    g[w] = Ls[c * (kCT + 1) + r];
   }
-  if (tid < kCT) {  // column c of W: L w = e_c, rows c..63
-    const int c = tid;
-    double* wc = tb.w + (size_t)k * kCTT + (size_t)c * kCT;
-    for (int r = 0; r < c; ++r) wc[r] = 0.0;
-    double x[kCT];
-    for (int r = c; r < kCT; ++r) {
-      double v = r == c ? 1.0 : 0.0;
-      for (int m = c; m < r; ++m) v -= A[m * (kCT + 1) + r] * x[m];
-      x[r] = v / A[r * (kCT + 1) + r];
-      wc[r] = x[r];
+  if (tid < kCT) rdiag[tid] = 1.0 / Ls[tid * (kCT + 1) + tid];
+  // W = L^-1: row j of W is final once rows above it have been eliminated; it is published and the
+  // rows below subtract L(i, j) times it
+#pragma unroll
+  for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) a[ai][bi] = (4 * ty + ai == 4 * tx + bi) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int j = 0; j < kCT; ++j) {
+    double* xj = pub[j & 1];
+    if (ty == (j >> 2)) {
+      const int aj = j & 3;
+      const double rd = rdiag[j];
+#pragma unroll
+      for (int ai = 0; ai < 4; ++ai)
+        if (ai == aj) {
+#pragma unroll
+          for (int bi = 0; bi < 4; ++bi) {
+            const double v = 4 * tx + bi <= j ? a[ai][bi] * rd : 0.0;
+            a[ai][bi] = v;
+            xj[4 * tx + bi] = v;
+          }
+        }
     }
+    __syncthreads();
+#pragma unroll
+    for (int ai = 0; ai < 4; ++ai) {
+      const int i = 4 * ty + ai;
+      if (i <= j) continue;
+      const double lij = Ls[j * (kCT + 1) + i];
+#pragma unroll
+      for (int bi = 0; bi < 4; ++bi)
+        if (4 * tx + bi <= j) a[ai][bi] -= lij * xj[4 * tx + bi];
+    }
+  }
+  __syncthreads();  // Ls is reused to stage W for coalesced stores
+#pragma unroll
+  for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) {
+      const int i = 4 * ty + ai, c = 4 * tx + bi;
+      Ls[c * (kCT + 1) + i] = i >= c ? a[ai][bi] : 0.0;
+    }
+  __syncthreads();
+  double* wk = tb.w + (size_t)k * kCTT;
+  for (int w = tid; w < kCTT; w += blockDim.x) {
+    const int c = w / kCT, r = w - c * kCT;
+    wk[w] = Ls[c * (kCT + 1) + r];
   }
 }
 
@@ -655,19 +718,45 @@ __global__ void k_perm_scatter(int n, const int* __restrict__ perm_to_orig, cons
 // group is the block of Z at its parameters' positions (sparse/covariance.rs:564-587 gets the same
 // block by solving S x = e_p column by column).
 //
-// Off-diagonal tiles of Z in column j: CTA per i in (j, min(j + bwt, nt - 1)]: acc = sum_k Z_ik L_kj,
-// then Z_ij = -acc W_j. Dynamic shared memory: kTakahashiSmem (two staged operands).
+// Column j runs as three launches, so that the column's 64 x 64 products spread over the GPU:
+//  k_takahashi_partial  CTA (b, s): part(b, s) = sum over k in chunk s of Z_ik L_kj, i = j + 1 + b,
+//                       chunks of kTakahashiChunk consecutive k in order
+//  k_takahashi_offdiag  CTA b: Z_ij = -(sum_s part(b, s)) W_j, and its share of the diagonal sum,
+//                       q(b) = Z_ij^T L_ij
+//  k_takahashi_diag     one CTA: Z_jj = (W_j^T - sum_b q(b)) W_j
+// Every sum runs in a fixed order, so Z does not depend on scheduling. Dynamic shared memory:
+// kTakahashiSmem (two staged operands).
 constexpr size_t kTakahashiSmem = 2 * kStagedTile;
-__global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand Z, int j, const int* status) {
+constexpr int kTakahashiChunk = 4;
+
+__device__ __forceinline__ void acc_add_tile(double acc[4][4], const double* __restrict__ g) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int a = 0; a < 4; ++a) acc[a][b] += g[(size_t)(4 * tx + b) * kCT + 4 * ty + a];
+}
+// acc (output tile element (4 ty + a, 4 tx + b)) transposed into a staged A operand: A(c, r) = acc(r, c)
+__device__ __forceinline__ void acc_to_at(const double acc[4][4], double* T) {
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) T[(4 * ty + a) * kTS + 4 * tx + b] = acc[a][b];
+}
+
+__global__ void __launch_bounds__(256) k_takahashi_partial(TileBand L, TileBand Z, int j, double* part,
+                                                           const int* status) {
   extern __shared__ double sh[];
   if (status[0] == 0) return;
   double* Ta = sh;
   double* Tb = sh + kCT * kTS;
   const int i = j + 1 + blockIdx.x;
   const int kmax = min(L.nt - 1, j + L.bwt);
+  const int k0 = j + 1 + kTakahashiChunk * blockIdx.y, k1 = min(kmax, k0 + kTakahashiChunk - 1);
   double acc[4][4];
   zero_acc(acc);
-  for (int k = j + 1; k <= kmax; ++k) {
+  for (int k = k0; k <= k1; ++k) {
     __syncthreads();
     if (i >= k)
       stage_tile(Z.t + tile_at(Z, i, k), Ta, false, false);  // Z_ik
@@ -677,33 +766,44 @@ __global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand 
     __syncthreads();
     tile_mma_acc(Ta, Tb, acc);
   }
-  __syncthreads();
+  acc_store(acc, part + ((size_t)blockIdx.x * gridDim.y + blockIdx.y) * kCTT);
+}
+
+__global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand Z, int j, int nsplit,
+                                                           const double* __restrict__ part, double* q,
+                                                           const int* status) {
+  extern __shared__ double sh[];
+  if (status[0] == 0) return;
+  double* Ta = sh;
+  double* Tb = sh + kCT * kTS;
+  const int i = j + 1 + blockIdx.x;
+  double acc[4][4];
+  zero_acc(acc);
+  for (int s = 0; s < nsplit; ++s) acc_add_tile(acc, part + ((size_t)blockIdx.x * nsplit + s) * kCTT);
   acc_to_a(acc, -1.0, Ta);
   stage_tile(L.w + (size_t)j * kCTT, Tb, true, false);  // W_j
   __syncthreads();
   zero_acc(acc);
   tile_mma_acc(Ta, Tb, acc);
   acc_store(acc, Z.t + tile_at(Z, i, j));
+  __syncthreads();
+  acc_to_at(acc, Ta);                                    // Z_ij^T
+  stage_tile(L.t + tile_at(L, i, j), Tb, true, false);  // L_ij
+  __syncthreads();
+  zero_acc(acc);
+  tile_mma_acc(Ta, Tb, acc);
+  acc_store(acc, q + (size_t)blockIdx.x * kCTT);
 }
 
-// Diagonal tile of Z in column j (after its off-diagonal tiles): acc = sum_k Z_kj^T L_kj, then
-// Z_jj = (W_j^T - acc) W_j. One CTA.
-__global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, int j, const int* status) {
+__global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, int j, int m,
+                                                        const double* __restrict__ q, const int* status) {
   extern __shared__ double sh[];
   if (status[0] == 0) return;
   double* Ta = sh;
   double* Tb = sh + kCT * kTS;
-  const int kmax = min(L.nt - 1, j + L.bwt);
   double acc[4][4];
   zero_acc(acc);
-  for (int k = j + 1; k <= kmax; ++k) {
-    __syncthreads();
-    stage_tile(Z.t + tile_at(Z, k, j), Ta, false, true);  // Z_kj^T
-    stage_tile(L.t + tile_at(L, k, j), Tb, true, false);  // L_kj
-    __syncthreads();
-    tile_mma_acc(Ta, Tb, acc);
-  }
-  __syncthreads();
+  for (int b = 0; b < m; ++b) acc_add_tile(acc, q + (size_t)b * kCTT);
   acc_to_a(acc, -1.0, Ta);  // -acc
   const double* wj = L.w + (size_t)j * kCTT;
   __syncthreads();

@@ -2852,14 +2852,25 @@ struct Solver {
     // selected inverse of S inside the band (Takahashi recurrence), last tile column first
     const size_t count = (size_t)S.nt * (S.bwt + 1) * kCTT;
     d_ztiles.alloc(count, st);
+    CUDA_OK(cudaFuncSetAttribute(k_takahashi_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
     CUDA_OK(cudaFuncSetAttribute(k_takahashi_offdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
     CUDA_OK(cudaFuncSetAttribute(k_takahashi_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTakahashiSmem));
     const TileBand tl = tile_band();
     const TileBand tz{D, S.nt, S.bwt, d_ztiles.p, nullptr};
+    // scratch: the split partial sums of one column and the diagonal shares of its tiles
+    const int max_split = (S.bwt + kTakahashiChunk - 1) / kTakahashiChunk;
+    DBuf<double> d_zpart, d_zq;
+    d_zpart.alloc((size_t)std::max(S.bwt, 1) * std::max(max_split, 1) * kCTT, st);
+    d_zq.alloc((size_t)std::max(S.bwt, 1) * kCTT, st);
     for (int j = S.nt - 1; j >= 0; --j) {
       const int m = std::min(S.bwt, S.nt - 1 - j);
-      if (m > 0) OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, d_status.p);
-      OMVGBA_LAUNCH(k_takahashi_diag, 1, 256, kTakahashiSmem, st, tl, tz, j, d_status.p);
+      if (m > 0) {
+        const int nsplit = (m + kTakahashiChunk - 1) / kTakahashiChunk;
+        OMVGBA_LAUNCH(k_takahashi_partial, dim3(m, nsplit), 256, kTakahashiSmem, st, tl, tz, j, d_zpart.p, d_status.p);
+        OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, nsplit, d_zpart.p, d_zq.p,
+                      d_status.p);
+      }
+      OMVGBA_LAUNCH(k_takahashi_diag, 1, 256, kTakahashiSmem, st, tl, tz, j, m, d_zq.p, d_status.p);
     }
     DBuf<int> d_pos, d_dims;
     d_pos.upload(pos.data(), pos.size(), st);

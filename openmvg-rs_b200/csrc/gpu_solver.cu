@@ -2989,19 +2989,21 @@ struct Solver {
     double t_start = now();
     int launches = 0, restarts = 0;
     PcgResult res;
+    double t_ready = 0.0;  // host clock when the graph is instantiated
     struct Report {
       double t0;
+      const double* t_ready;
       int* launches;
       int* restarts;
       PcgResult* res;
       bool fp32;
       ~Report() {
         if (std::getenv("OMVGBA_PCG_TRACE"))
-          std::fprintf(stderr, "[pcg%s] %.3f ms terms %llu accepted %d rel %.3e launches %d restarts %d\n",
+          std::fprintf(stderr, "[pcg%s] %.3f ms terms %llu accepted %d rel %.3e launches %d restarts %d setup %.3f ms\n",
                        fp32 ? "32" : "64", (now() - t0) * 1e3, (unsigned long long)res->terms, (int)res->accepted,
-                       res->rel, *launches, *restarts);
+                       res->rel, *launches, *restarts, *t_ready > 0.0 ? (*t_ready - t0) * 1e3 : 0.0);
       }
-    } rpt{t_start, &launches, &restarts, &res, fp32};
+    } rpt{t_start, &t_ready, &launches, &restarts, &res, fp32};
     CUDA_OK(cudaMemsetAsync(x, 0, sizeof(double) * D, st));
     CUDA_OK(copy_async(d_r.p, b, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
     double h[4];
@@ -3049,6 +3051,7 @@ struct Solver {
     const uint64_t kernels_per_graph = tl_telemetry.launches - launches_before;  // counted at capture
     tl_telemetry.launches = launches_before;
     CUDA_OK(cudaGraphInstantiate(&exec, graph, 0));
+    t_ready = now();
     struct GraphGuard {
       cudaGraph_t g;
       cudaGraphExec_t e;

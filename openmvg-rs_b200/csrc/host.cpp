@@ -1159,10 +1159,19 @@ Result raise(const omvgba_problem& pr, const Lowered& L, const std::vector<doubl
 // count and RMSE of the solution. One pass over the observations: each quantity is accumulated per
 // chunk as active_metrics and refresh_inliers accumulate it and combined in the same chunk order, and
 // the solution's residual norm, which both use, is evaluated once.
-void finish_solution(const omvgba_problem& pr, Result& res) {
+// The input-state metrics of a problem with held-out points (the report's initial objective and RMSE)
+// depend only on the input and on the held-out set, so a plan keeps them from one solve to the next.
+struct InputMetrics {
+  bool valid = false;
+  std::vector<uint64_t> quarantined;
+  std::vector<MetricPart> parts;
+};
+
+void finish_solution(const omvgba_problem& pr, Result& res, InputMetrics* cache = nullptr) {
   std::vector<uint8_t> active(pr.point_count, 1);
   for (auto q : res.quarantined) active[q] = 0;
   const bool held_out = !res.quarantined.empty();
+  const bool reuse_input = held_out && cache && cache->valid && cache->quarantined == res.quarantined;
   const LossDev loss = problem_loss(pr);
   const double limit = pr.loss_kind == OMVGBA_LOSS_SQUARED ? INFINITY : pr.loss_scale;
   constexpr size_t kChunks = 64;
@@ -1194,7 +1203,7 @@ void finish_solution(const omvgba_problem& pr, Result& res) {
           }
         }
       }
-      if (held_out && m0.ok) {
+      if (held_out && !reuse_input && m0.ok) {
         double nrm;
         if (!residual_norm(pr, *sv_input, o, pr.points + 3 * p, &nrm))
           m0.ok = false;
@@ -1208,6 +1217,13 @@ void finish_solution(const omvgba_problem& pr, Result& res) {
     inliers[c] = n_in;
     inlier_ss[c] = ss;
   });
+  if (reuse_input) {
+    at_input = cache->parts;
+  } else if (held_out && cache) {
+    cache->valid = true;
+    cache->quarantined = res.quarantined;
+    cache->parts = at_input;
+  }
   uint64_t cnt = 0;
   for (uint64_t k : seen) cnt += k;
   res.report.has_observation_count = 1;
@@ -1614,11 +1630,13 @@ Result solve_two_view(Context* ctx, const omvgba_problem& pr, const omvgba_confi
   return res;
 }
 
-Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg) {
+// finish = false leaves the report's observation and inlier metrics to the caller: the quarantine
+// protocol evaluates them once more over the original problem whenever points are held out.
+Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg, bool finish = true) {
   validate_config(cfg);
   if (!(pr.residual_space != OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(pr)) && can_use_two_view(pr)) {
     Result res = solve_two_view(ctx, pr, cfg);
-    finish_solution(pr, res);
+    if (finish) finish_solution(pr, res);
     canonicalize(pr, res);
     return res;
   }
@@ -1645,7 +1663,7 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
   res.unconstrained = L.n.self_cal ? held : unobserved_free_intrinsics(pr);
   res.report.unconstrained_intrinsic_count = res.unconstrained.size();
   if (wants_post_solve_probe(pr, L.n)) apply_preflight(pr, preflight_from_prepared(ctx, pr, L, rot, tr, pts), res.report);
-  finish_solution(pr, res);
+  if (finish) finish_solution(pr, res);
   canonicalize(pr, res);
   if (std::getenv("OMVGBA_PHASE_TIMES"))
     std::fprintf(stderr, "[omvgba] solve_once: lower %.3fs gpu %.3fs raise+finish %.3fs\n", t_lower, t_gpu,
@@ -1920,7 +1938,7 @@ void prepare_quarantine(const omvgba_problem& pr, const omvgba_config& cfg, Prep
 // The rest of the protocol after the first solve `sol` of prep.working: up to four re-solves
 // without the weak points of the previous solution, then the solution in the input's indexing.
 Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg, const Prepared& prep,
-                         Result sol) {
+                         Result sol, InputMetrics* input_cache = nullptr) {
   std::vector<size_t> kept = prep.kept;
   size_t quarantined = prep.quarantined;
   const bool changes_scale = prep.changes_scale;
@@ -1947,7 +1965,7 @@ Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_co
     }
     Result resolved;
     try {
-      resolved = solve_once(ctx, next.view, retry);
+      resolved = solve_once(ctx, next.view, retry, false);  // held-out points: finished below
     } catch (const SolveFailure& f) {
       if (f.code == OMVGBA_CUDA_ERROR) throw;
       chain.pop_back();
@@ -1981,7 +1999,7 @@ Result finish_quarantine(Context* ctx, const omvgba_problem& pr, const omvgba_co
   out.unconstrained = sol.unconstrained;
   out.report = sol.report;
   if (have_origin) add_origin(out.report, origin);
-  finish_solution(pr, out);
+  finish_solution(pr, out, input_cache);
   return out;
 }
 
@@ -1994,7 +2012,7 @@ Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgb
   Prepared prep;
   prepare_quarantine(pr, cfg, prep);
   const double t_prep = seconds_since(t0);
-  Result sol = solve_once(ctx, *prep.working, cfg);
+  Result sol = solve_once(ctx, *prep.working, cfg, prep.quarantined == 0);
   const double t_solve = seconds_since(t0) - t_prep;
   Result out = finish_quarantine(ctx, pr, cfg, prep, std::move(sol));
   if (std::getenv("OMVGBA_PHASE_TIMES"))
@@ -2030,6 +2048,7 @@ struct omvgba_plan {
   Lowered lowered;
   LmOptions options;
   Resident* resident = nullptr;
+  InputMetrics input_metrics;  // the held-out report's input-state metrics, kept across solves
   ~omvgba_plan() { resident_destroy(resident); }
 };
 
@@ -2435,9 +2454,10 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     const omvgba_problem& working = *plan->prep.working;
     if (plan->two_view) {
       Result first = solve_two_view(plan->ctx, working, plan->config);
-      finish_solution(working, first);
+      if (plan->prep.quarantined == 0) finish_solution(working, first);
       canonicalize(working, first);
-      Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first));
+      Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first),
+                                   &plan->input_metrics);
       write_solution(*plan->problem, r, solution);
       stamp_telemetry(solution->report, before, t0);
       return OMVGBA_OK;
@@ -2466,11 +2486,14 @@ int32_t omvgba_plan_solve(omvgba_plan* plan, omvgba_solution* solution, omvgba_e
     if (wants_post_solve_probe(working, lowered->n))
       apply_preflight(working, preflight_from_prepared(plan->ctx, working, *lowered, rot, tr, pts), first.report);
     laps[1] = seconds_since(t0);
-    finish_solution(working, first);
+    // with points held out, the quarantine protocol evaluates the report's metrics over the original
+    // problem, so the working problem's pass would be discarded
+    if (plan->prep.quarantined == 0) finish_solution(working, first);
     laps[2] = seconds_since(t0);
     canonicalize(working, first);
     laps[3] = seconds_since(t0);
-    Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first));
+    Result r = finish_quarantine(plan->ctx, *plan->problem, plan->config, plan->prep, std::move(first),
+                                 &plan->input_metrics);
     laps[4] = seconds_since(t0);
     write_solution(*plan->problem, r, solution);
     laps[5] = seconds_since(t0);

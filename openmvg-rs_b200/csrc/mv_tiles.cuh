@@ -110,6 +110,10 @@ __global__ void __launch_bounds__(mv_tile_obs<R>(), sizeof(T) == sizeof(R) ? 4 :
   __shared__ uint16_t seg_begin[TILE + 1];
   __shared__ uint16_t pt_begin[TILE + 1];
   const int t = blockIdx.x, tid = threadIdx.x;
+  // Within one graph launch a PCG run that has stopped stays stopped (the host resets the control
+  // block only between launches), so a stop seen before the wait is final: the iterations enqueued
+  // past the end of the run then skip their record loads too, not just their arithmetic.
+  if (ctl && *reinterpret_cast<const volatile int*>(&ctl->status) != kRunning) return;
   // The CTA that starts about one resident wave later finds its records in L2.
   const uint64_t stream_pol = l2_evict_first();
   if (tid == 0 && mt.prefetch_ahead > 0 && t + mt.prefetch_ahead < mt.ntiles)

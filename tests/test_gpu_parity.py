@@ -173,3 +173,38 @@ def test_explicit_schur_pcg_matches_matrix_free_pcg_and_oracle(adjuster, case):
             assert g.report[k] == o.report[k], (k, g.report[k], o.report[k])
         assert _rel(g.report["final_objective"], o.report["final_objective"]) < 1e-9
     assert _param_diff(explicit, implicit) < 1e-7
+
+
+def _with_single_view_points(p, count=5, seed=0):
+    """p plus `count` points seen by one camera each: the quarantine protocol holds them out before the
+    solve (quarantine.rs:34-96) and reports them."""
+    rng = np.random.default_rng(seed)
+    P = p.points.shape[0]
+    extra = rng.uniform(-0.5, 0.5, size=(count, 3))
+    p.points = np.vstack([p.points, extra])
+    p.point_fixed = np.concatenate([p.point_fixed, np.zeros(count, dtype=np.uint8)])
+    p.observation_pose = np.concatenate([p.observation_pose, np.arange(count, dtype=np.uint32)])
+    p.observation_intrinsic = np.concatenate([p.observation_intrinsic, np.zeros(count, dtype=np.uint32)])
+    p.observation_point = np.concatenate([p.observation_point, np.arange(P, P + count, dtype=np.uint32)])
+    p.observation_pixel = np.vstack([p.observation_pixel, rng.uniform(200.0, 300.0, size=(count, 2))])
+    return p
+
+
+def test_plan_solves_with_held_out_points_equal_one_shot_solves(adjuster):
+    """A plan reports the same solution and report as omvgba_solve on its first and on later solves,
+    with points held out (the plan keeps their input-state metrics from one solve to the next)."""
+    p = _with_single_view_points(synthetic.ring_problem(seed=3))
+    cfg = SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, max_iterations=10)
+    one = adjuster.solve(p, cfg)
+    assert one.report["quarantined_point_count"] == 5
+    with adjuster.plan(p, cfg) as plan:
+        first, second = plan.solve(), plan.solve()
+    for s in (first, second):
+        assert np.array_equal(s.points, one.points) and np.array_equal(s.centers, one.centers)
+        assert np.array_equal(s.quarantined_points, one.quarantined_points)
+        for k in ("initial_objective", "final_objective", "initial_rmse", "final_rmse", "inlier_count",
+                  "final_inlier_rmse", "observation_count", "quarantined_point_count", "iteration_count"):
+            assert s.report[k] == one.report[k], k
+    o = O.solve(p, cfg)
+    assert np.array_equal(np.sort(one.quarantined_points), np.sort(o.quarantined_points))
+    assert abs(one.report["initial_objective"] - o.report["initial_objective"]) <= 1e-12 * o.report["initial_objective"]

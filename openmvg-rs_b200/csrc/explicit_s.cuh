@@ -46,6 +46,14 @@ struct RowTables {
 };
 
 
+// D = A B + C for 8 x 8 FP64 tiles with k = 4 (mma.sync.m8n8k4 f64): each lane passes one element
+// of A, one of B and two of C, updated in place.
+__device__ __forceinline__ void dmma_m8n8k4(double a, double b, double& c0, double& c1) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n0, uint32_t n1, int Y) {
   uint32_t lo = n0, hi = n1;
   while (lo < hi) {
@@ -70,7 +78,7 @@ __device__ __forceinline__ int find_slot(const int* __restrict__ nbr, uint32_t n
 // kRowStage observations per round; longer tracks take several rounds) into shared memory, and the
 // slot of each target. After a barrier every warp adds the batch's contributions to the slots it
 // owns (slot index mod kRowWarps), entity by entity in batch order and target by target in track
-// order, lanes over the dX x dY elements. Each element therefore has one writer and a fixed
+// order, one tensor-pipe product per target. Each element therefore has one writer and a fixed
 // summation order: the row is the same bits run to run, without atomics. The row accumulates in
 // shared memory when it has at most row_smem doubles (else in place in global memory) and is
 // stored once at the end. Each warp fetches the indices of its next entity a batch ahead.
@@ -214,33 +222,38 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_block_rows(RowTables rt, Lin
       }
       __syncthreads();
       // ---- every warp adds the batch's contributions to the slots it owns ----
+      // One target is one FP64 m8n8k4 product on the tensor pipe, C (the slot, 8 x 8 with rows >= dX
+      // and columns >= dY masked) += (-E) W_k,Y^T, plus A_o,X^T A_o,Y for the entity's own
+      // observation. Fragments: lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and C(l / 4, 2 (l % 4)
+      // + i), i = 0, 1.
+      const int fg = lane >> 2, ft = lane & 3;
       for (int b = 0; b < kRowWarps; ++b) {
         const int nt = item_n[b];
         if (nt == 0) continue;
         const int sl = lane < nt ? tsl[b][lane] : -1;
         unsigned mask = __ballot_sync(0xffffffffu, sl >= 0 && sl % kRowWarps == w);
+        if (mask == 0u) continue;
         const int cxb = item_cx[b];
         const double* A = Osh[b];
-        const double* E = Esh[b];
+        const double aE = (fg < dX && ft < 3) ? -Esh[b][3 * fg + ft] : 0.0;  // -E (dX x 3)
+        const double aU = (fg < dX && ft < 2) ? A[9 * ft + cxb + fg] : 0.0;  // A_o,X^T (dX x 2)
         while (mask) {
           const int t = __ffs(mask) - 1;
           mask &= mask - 1;
           const uint32_t inf = tinf[b][t];
           const int cd = tcd[b][t], cY = cd & 0xff, own = (cd >> 8) & 1, dY = (int)(inf & 7);
           const double* Wk = Wsh[b][cd >> 9];
-          double* out = row + (inf >> 3);
-          // lanes over a fixed 6 x 6 grid of (m, n): element l of the grid is (l / 6, l % 6)
-#pragma unroll
-          for (int pass = 0; pass < 2; ++pass) {
-            const int l = lane + 32 * pass;
-            const int m = l / 6, n = l - 6 * (l / 6);
-            if (l < 36 && m < dX && n < dY) {
-              const double* wn = Wk + 3 * (cY + n);
-              double acc = -(E[3 * m] * wn[0] + E[3 * m + 1] * wn[1] + E[3 * m + 2] * wn[2]);
-              if (own) acc += A[cxb + m] * A[cY + n] + A[9 + cxb + m] * A[9 + cY + n];
-              out[m * dY + n] += acc;
-            }
+          double* out = row + (inf >> 3) + fg * dY;
+          const double bW = (fg < dY && ft < 3) ? Wk[3 * (cY + fg) + ft] : 0.0;  // W_k,Y^T (3 x dY)
+          const bool in0 = fg < dX && 2 * ft < dY, in1 = fg < dX && 2 * ft + 1 < dY;
+          double c0 = in0 ? out[2 * ft] : 0.0, c1 = in1 ? out[2 * ft + 1] : 0.0;
+          dmma_m8n8k4(aE, bW, c0, c1);
+          if (own) {  // the same target in every lane
+            const double bU = (fg < dY && ft < 2) ? A[9 * ft + cY + fg] : 0.0;  // A_o,Y (2 x dY)
+            dmma_m8n8k4(aU, bU, c0, c1);
           }
+          if (in0) out[2 * ft] = c0;
+          if (in1) out[2 * ft + 1] = c1;
         }
       }
     }

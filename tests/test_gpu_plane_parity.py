@@ -43,6 +43,12 @@ def _compare(g, o, tag):
     assert np.quantile(dp, 0.999) < 1e-7 and dp.max() < 1e-6, (tag, np.quantile(dp, 0.999), dp.max())
 
 
+def _check_pcg_count(g, o):
+    """PCG products within one per LM iteration: a run whose relative residual lands at the tolerance
+    on some iteration can stop one product earlier or later under a different summation order."""
+    assert abs(g.report["pcg_iteration_count"] - o.report["pcg_iteration_count"]) <= o.report["iteration_count"]
+
+
 def test_plane500_fp64_matches_oracle(adjuster):
     p = synthetic.plane_problem()
     cfg = SolveConfig(max_iterations=4, linear_solver=abi.SOLVER_ITERATIVE, precision=abi.PRECISION_FP64,
@@ -50,7 +56,7 @@ def test_plane500_fp64_matches_oracle(adjuster):
     g, o = adjuster.solve(p, cfg), O.solve(p, cfg)
     _compare(g, o, "plane500")
     assert g.report["observability"] == o.report["observability"]
-    assert g.report["pcg_iteration_count"] == o.report["pcg_iteration_count"]
+    _check_pcg_count(g, o)
 
 
 def test_plane3000_geometry_fp64_matches_oracle(adjuster):
@@ -61,7 +67,7 @@ def test_plane3000_geometry_fp64_matches_oracle(adjuster):
     g, o = adjuster.solve(p, cfg), O.solve(p, cfg)
     _compare(g, o, "plane3000_200k")
     assert g.report["observability"] == o.report["observability"]
-    assert g.report["pcg_iteration_count"] == o.report["pcg_iteration_count"]
+    _check_pcg_count(g, o)
 
 
 def _rot_y(a):

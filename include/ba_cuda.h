@@ -483,6 +483,116 @@ typedef struct omvgba_preflight {      /* NativePreflight (native/mod.rs:143-165
 int32_t omvgba_preflight_check(omvgba_context* context, const omvgba_problem* problem, const omvgba_config* config,
                                omvgba_preflight* preflight, omvgba_error* error);
 
+/* ---- the SfM side of a bundle adjustment: refreshing the landmarks' reprojection errors ----------
+ *
+ * After openmvg-sfm commits a bundle adjustment it measures every supporting observation of every
+ * active landmark again (refresh_landmark_reprojection_errors_for, crates/openmvg-sfm/src/ops/
+ * reconstruction/bundle.rs:510-637): the observation's pixel-equivalent residual under the camera
+ * residual policy with no limit (ops/reconstruction/residual.rs:37-90) -- the pixel distance of the
+ * projection for pinhole and Brown-Conrady cameras, the bearing angle times the nominal pixels per
+ * radian for fisheye and spherical ones -- is kept when it exists and is finite; the landmark's
+ * reprojection error becomes the mean of the kept residuals in track order; a landmark with fewer
+ * than two is rejected, one that lost some has its support pruned to the kept observations. */
+#define OMVGBA_NO_POSE 0xFFFFFFFFu
+typedef struct omvgba_landmark_tracks {
+  uint64_t landmark_count;
+  const double* points;            /* 3 per landmark, world frame */
+  const uint8_t* active;           /* 1 for LandmarkStatus::Active; other landmarks are left as they are */
+  const uint64_t* track_offset;    /* landmark_count + 1: each landmark's track observations below */
+  const uint32_t* track_pose;      /* pose of the observing view, or OMVGBA_NO_POSE when it has none */
+  const uint32_t* track_intrinsic; /* intrinsic of the observing view */
+  const double* track_pixel;       /* 2 per track observation */
+  const uint8_t* track_support;    /* 1 when the observation is in the landmark's support */
+} omvgba_landmark_tracks;
+
+typedef enum omvgba_refresh_update {
+  OMVGBA_REFRESH_SKIPPED = 0,   /* not active: nothing changes */
+  OMVGBA_REFRESH_REJECTED = 1,  /* fewer than two supporting residuals: LandmarkStatus::Rejected */
+  OMVGBA_REFRESH_UNCHANGED = 2, /* every supporting residual kept: new reprojection error only */
+  OMVGBA_REFRESH_PRUNED = 3     /* some dropped: new support and reprojection error */
+} omvgba_refresh_update;
+
+typedef struct omvgba_refresh_result {
+  uint8_t* landmark_update;     /* landmark_count: omvgba_refresh_update */
+  double* reprojection_error;   /* landmark_count: mean residual (pixels) of kept landmarks, else untouched */
+  uint8_t* track_support;       /* track observations: the support after the refresh */
+  uint64_t rejected_landmarks;  /* LandmarkSupportCleanupReport */
+  uint64_t removed_observations;
+} omvgba_refresh_result;
+
+/* Refresh of refresh_landmark_reprojection_errors_for (bundle.rs:510-637) on the context's device:
+ * one thread per landmark evaluates its track in order. Poses are world-to-camera rotations with
+ * camera centres (as omvgba_pose); intrinsics as omvgba_intrinsic. Returns OMVGBA_INVALID_PROBLEM
+ * for an index out of range or a fisheye or spherical camera without a positive finite pixel scale
+ * (the residual policy's own error), before any device work. */
+int32_t omvgba_sfm_refresh_reprojection(omvgba_context* context, uint64_t pose_count, const omvgba_pose* poses,
+                                        uint64_t intrinsic_count, const omvgba_intrinsic* intrinsics,
+                                        const omvgba_landmark_tracks* tracks, omvgba_refresh_result* result,
+                                        omvgba_error* error);
+
+/* ---- the SfM side of a bundle adjustment: building the problem from a reconstruction -----------
+ *
+ * prepare_bundle_adjustment_problem (crates/openmvg-sfm/src/ops/reconstruction/bundle.rs:707-989):
+ * the poses of the registered views (ascending pose id; fixed when a fixed view maps to them, or by
+ * the scope), the intrinsic groups those views use (ascending id; free focal and radial terms only
+ * under self-calibration and never for fisheye or spherical cameras; certification waived for a
+ * placeholder focal), the active landmarks not excluded (fixed when listed or under the poses-only
+ * scope) and, landmark by landmark in track order, their supporting observations seen from a
+ * registered view. The residuals are angular when any group is fisheye or spherical, and a pixel
+ * loss scale is then converted with the mean angle one pixel subtends (canonical_robust_loss,
+ * :1006-1032). Unlike the reference this works on flat tables, so the caller resolves view and
+ * landmark ids to table rows, and one reconstruction component per problem is the caller's check. */
+typedef enum omvgba_scope {
+  OMVGBA_SCOPE_FULL = 0,                 /* poses and points */
+  OMVGBA_SCOPE_POINTS_ONLY = 1,
+  OMVGBA_SCOPE_POSES_ONLY = 2,
+  OMVGBA_SCOPE_TRANSLATIONS_AND_POINTS = 3,
+  OMVGBA_SCOPE_SELF_CALIBRATION = 4
+} omvgba_scope;
+
+typedef struct omvgba_sfm_workspace {
+  uint64_t view_count;
+  const uint32_t* view_pose;        /* pose row of each view, OMVGBA_NO_POSE when it is not registered */
+  const uint32_t* view_intrinsic;   /* intrinsic row of each view */
+  const uint32_t* view_size;        /* width, height of each view's image */
+  uint64_t pose_count;
+  const omvgba_pose* poses;         /* rotation and centre; variables are set by the preparation */
+  uint64_t intrinsic_count;
+  const omvgba_intrinsic* intrinsics;
+  const uint8_t* intrinsic_guess;   /* 1 when the group's focal is a placeholder (IntrinsicPrior::Guess) */
+  omvgba_landmark_tracks landmarks; /* track_pose holds the observing VIEW row here */
+} omvgba_sfm_workspace;
+
+typedef struct omvgba_sfm_prepare_config {
+  int32_t scope;                    /* omvgba_scope */
+  uint64_t fixed_view_count;
+  const uint32_t* fixed_views;      /* view rows whose poses stay fixed */
+  uint64_t fixed_landmark_count;
+  const uint32_t* fixed_landmarks;  /* landmark rows held fixed */
+  uint64_t excluded_landmark_count;
+  const uint32_t* excluded_landmarks;
+  int32_t loss_kind;                /* omvgba_loss_kind, scale and its space as in omvgba_problem */
+  double loss_scale;
+  int32_t loss_scale_space;
+  int32_t gauge_kind;               /* omvgba_gauge_kind; the fixed baseline's ends are view rows */
+  uint32_t gauge_first_view, gauge_second_view;
+  double gauge_distance;
+} omvgba_sfm_prepare_config;
+
+typedef struct omvgba_sfm_prepared {
+  omvgba_problem problem;           /* arrays caller-allocated with the counts of the sizing call */
+  uint32_t* pose_rows;              /* pose_count: workspace pose row of each problem pose */
+  uint32_t* intrinsic_rows;         /* intrinsic_count */
+  uint32_t* landmark_rows;          /* point_count */
+} omvgba_sfm_prepared;
+
+/* Call once with prepared->problem's array pointers null to receive the counts (pose, intrinsic,
+ * point and observation), allocate, then call again to fill. OMVGBA_INVALID_PROBLEM for a row out of
+ * range, an intrinsic shared by images of different sizes, a missing fixed-baseline view or a loss
+ * scale whose units cannot be converted; OMVGBA_INVALID_CONFIG for an invalid scope or loss. */
+int32_t omvgba_sfm_prepare_problem(const omvgba_sfm_workspace* workspace, const omvgba_sfm_prepare_config* config,
+                                   omvgba_sfm_prepared* prepared, omvgba_error* error);
+
 #ifdef __cplusplus
 }
 #endif

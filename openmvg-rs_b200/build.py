@@ -15,8 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "openmvg_ba_cuda", "_lib")
 LIB = os.path.join(OUT_DIR, "libomvgba_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["gpu_solver.cu", "residual.cu", "residual_static.cu"]
-CPP_SOURCES = ["host.cpp", "fixed_rotation.cpp"]
+CU_SOURCES = ["gpu_solver.cu", "residual.cu", "residual_static.cu", "sfm_refresh.cu"]
+CPP_SOURCES = ["host.cpp", "fixed_rotation.cpp", "sfm_prepare.cpp"]
 
 
 def nvcc() -> str:

@@ -173,6 +173,7 @@ Context* context_create(int device, std::string* error) {
 }
 
 int context_device(const Context* c) { return c->device; }
+void* context_stream(const Context* c) { return (void*)c->stream; }
 
 void context_destroy(Context* c) {
   if (!c) return;

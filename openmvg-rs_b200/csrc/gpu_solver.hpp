@@ -156,6 +156,30 @@ struct Context;  // device, stream, pinned scratch
 int device_count();
 Context* context_create(int device, std::string* error);
 int context_device(const Context* ctx);
+void* context_stream(const Context* ctx);  // the context's cudaStream_t
+
+// refresh_landmark_reprojection_errors_for (openmvg-sfm ops/reconstruction/bundle.rs:510-637) on the
+// context's device, inputs and outputs in host memory (see omvgba_sfm_refresh_reprojection). The
+// caller has checked every index. Throws SolveFailure on a CUDA error.
+struct SfmRefreshInput {
+  uint64_t pose_count, intrinsic_count, landmark_count, track_count;
+  const double* rotation;      // 9 per pose, world to camera, row-major
+  const double* center;        // 3 per pose
+  const void* intrinsics;      // omvgba_intrinsic[intrinsic_count]
+  const double* points;        // 3 per landmark
+  const uint8_t* active;
+  const uint64_t* track_offset;
+  const uint32_t* track_pose, * track_intrinsic;
+  const double* track_pixel;
+  const uint8_t* track_support;
+};
+struct SfmRefreshOutput {
+  uint8_t* landmark_update;
+  double* reprojection_error;
+  uint8_t* track_support;
+  uint64_t rejected_landmarks = 0, removed_observations = 0;
+};
+void gpu_sfm_refresh(Context* ctx, const SfmRefreshInput& in, SfmRefreshOutput& out);
 void context_destroy(Context* ctx);
 
 // Runs the LM refinement on the GPU; on return points/rotation/translation/groups hold the refined

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/ba_cuda.h"
+#include "camera_models.cuh"
 #include "gpu_solver.hpp"
 #include "fixed_rotation.hpp"
 
@@ -72,31 +73,6 @@ double sqdist(const Vec3& a, const Vec3& b) {
   return dx * dx + dy * dy + dz * dz;
 }
 
-FixedCameraDev make_fixed_camera(const omvgba_intrinsic& in) {
-  FixedCameraDev m{};
-  m.fx = in.fx;
-  m.fy = in.fy;
-  m.cx = in.cx;
-  m.cy = in.cy;
-  if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
-    m.radial_kind = in.radial_kind;
-    m.tangential_kind = in.tangential_kind;
-    m.k1 = in.radial_kind >= 1 ? in.k1 : 0.0;
-    m.k2 = in.radial_kind >= 2 ? in.k2 : 0.0;
-    m.k3 = in.radial_kind >= 3 ? in.k3 : 0.0;
-    m.p1 = in.tangential_kind >= 1 ? in.p1 : 0.0;
-    m.p2 = in.tangential_kind >= 2 ? in.p2 : 0.0;
-    double t;
-    m.has_turn = first_radial_turn_squared(m.k1, m.k2, &t) ? 1 : 0;
-    m.turn_squared = m.has_turn ? t : INFINITY;
-  } else {
-    m.radial_kind = 0;
-    m.tangential_kind = 0;
-    m.has_turn = 0;
-    m.turn_squared = INFINITY;
-  }
-  return m;
-}
 
 LossDev problem_loss(const omvgba_problem& pr) {
   if (pr.loss_kind == OMVGBA_LOSS_HUBER) return {kLossHuber, pr.loss_scale};
@@ -430,158 +406,8 @@ struct Lowered {
 };
 
 // ---- bearings of measured pixels (Camera::bearing, openmvg-core camera/camera_enum.rs:128-132) ----
-// FisheyeDistortion (camera/distortion.rs:244-460): theta_d = theta (1 + k1 t^2 + k2 t^4 + k3 t^6 + k4 t^8)
-struct FisheyePoly {
-  int kind;  // 0 None .. 4 K1K2K3K4
-  double k1, k2, k3, k4;
-  double apply(double t) const {
-    const double t2 = t * t, t4 = t2 * t2;
-    switch (kind) {
-      case 0: return t;
-      case 1: return t * (1.0 + k1 * t2);
-      case 2: return t * (1.0 + k1 * t2 + k2 * t4);
-      case 3: return t * (1.0 + k1 * t2 + k2 * t4 + k3 * (t4 * t2));
-      default: return t * (1.0 + k1 * t2 + k2 * t4 + k3 * (t4 * t2) + k4 * (t4 * t4));
-    }
-  }
-  double derivative(double t) const {
-    const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t8 = t4 * t4;
-    return 1.0 + 3.0 * k1 * t2 + 5.0 * k2 * t4 + 7.0 * k3 * t6 + 9.0 * k4 * t8;
-  }
-  // max_invertible_angle (distortion.rs:416-455)
-  bool max_invertible_angle(double max_theta, double* out) const {
-    if (!(std::isfinite(k1) && std::isfinite(k2) && std::isfinite(k3) && std::isfinite(k4))) return false;
-    if (k3 == 0.0 && k4 == 0.0) {
-      double q;
-      *out = first_radial_turn_squared(k1, k2, &q) ? std::min(std::sqrt(q), max_theta) : max_theta;
-      return true;
-    }
-    if (k1 >= 0.0 && k2 >= 0.0 && k3 >= 0.0 && k4 >= 0.0) {
-      *out = max_theta;
-      return true;
-    }
-    double previous = 0.0;
-    for (int i = 1; i <= 1024; ++i) {
-      const double t = max_theta * i / 1024.0;
-      if (derivative(t) <= 0.0) {
-        double lo = previous, hi = t;
-        for (int k = 0; k < 64; ++k) {
-          const double mid = 0.5 * (lo + hi);
-          if (derivative(mid) > 0.0)
-            lo = mid;
-          else
-            hi = mid;
-        }
-        *out = lo;
-        return true;
-      }
-      previous = t;
-    }
-    *out = max_theta;
-    return true;
-  }
-  // invert_on_validated_interval (distortion.rs:359-409)
-  bool invert(double td, double upper, double* out) const {
-    if (!std::isfinite(td) || !std::isfinite(upper) || td < 0.0 || upper <= 0.0) return false;
-    const double mapped = apply(upper);
-    if (!std::isfinite(mapped) || td > mapped + 1e-12) return false;
-    double lo = 0.0, hi = upper, t = std::min(td, upper);
-    for (int i = 0; i < 48; ++i) {
-      const double r = apply(t) - td;
-      if (std::fabs(r) <= 1e-13) {
-        *out = t;
-        return true;
-      }
-      if (r < 0.0)
-        lo = t;
-      else
-        hi = t;
-      const double d = derivative(t), nt = t - r / d;
-      t = (std::isfinite(d) && d > 1e-15 && nt > lo && nt < hi) ? nt : 0.5 * (lo + hi);
-    }
-    if (std::fabs(apply(t) - td) <= 1e-12) {
-      *out = t;
-      return true;
-    }
-    return false;
-  }
-};
-
-// try_normalize_bearing (camera/camera_model.rs:91-109)
-bool normalize_bearing(const double d[3], double b[3]) {
-  if (!all_finite(d, 3)) return false;
-  const double s = std::max({0.0, std::fabs(d[0]), std::fabs(d[1]), std::fabs(d[2])});
-  if (s == 0.0) return false;
-  const double x[3] = {d[0] / s, d[1] / s, d[2] / s};
-  const double n = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-  if (!std::isfinite(n) || n == 0.0) return false;
-  for (int k = 0; k < 3; ++k) b[k] = x[k] / n;
-  return true;
-}
-
-// The unit bearing of pixel (u, v): CameraModel::unproject of the pinhole (pinhole.rs:324-340),
-// Brown-Conrady (brown_conrady.rs:365-383), fisheye (fisheye.rs:271-299) and spherical
-// (spherical.rs:113-257) models, then normalized.
 bool camera_bearing(const omvgba_intrinsic& in, double u, double v, double b[3]) {
-  if (!std::isfinite(u) || !std::isfinite(v)) return false;
-  double d[3];
-  switch (in.model) {
-    case OMVGBA_CAMERA_PINHOLE:
-    case OMVGBA_CAMERA_BROWN_CONRADY: {
-      d[0] = (u - in.cx) / in.fx;
-      d[1] = (v - in.cy) / in.fy;
-      d[2] = 1.0;
-      if (!all_finite(d, 3)) return false;
-      if (in.model == OMVGBA_CAMERA_BROWN_CONRADY) {
-        double x, y;
-        if (!make_fixed_camera(in).remove_distortion(d[0] / d[2], d[1] / d[2], &x, &y)) return false;
-        d[0] = x;
-        d[1] = y;
-        d[2] = 1.0;
-      }
-      break;
-    }
-    case OMVGBA_CAMERA_FISHEYE: {
-      const double xd = (u - in.cx) / in.fx, yd = (v - in.cy) / in.fy;
-      if (!std::isfinite(xd) || !std::isfinite(yd)) return false;
-      const double td = std::hypot(xd, yd);
-      if (td <= kEps) {
-        d[0] = 0.0;
-        d[1] = 0.0;
-        d[2] = 1.0;
-        break;
-      }
-      const FisheyePoly f{in.radial_kind, in.radial_kind >= 1 ? in.k1 : 0.0, in.radial_kind >= 2 ? in.k2 : 0.0,
-                          in.radial_kind >= 3 ? in.k3 : 0.0, in.radial_kind >= 4 ? in.k4 : 0.0};
-      double max_angle, theta;
-      if (!f.max_invertible_angle(3.141592653589793 - 1e-10, &max_angle)) return false;
-      if (!f.invert(td, max_angle, &theta)) return false;
-      const double sc = std::sin(theta) / td;
-      d[0] = xd * sc;
-      d[1] = yd * sc;
-      d[2] = std::cos(theta);
-      if (!all_finite(d, 3)) return false;
-      break;
-    }
-    case OMVGBA_CAMERA_SPHERICAL: {
-      const double w = (double)in.width, h = (double)(in.width / 2);
-      if (v < -0.5 || v > h - 0.5) return false;
-      double x = std::fmod(u + 0.5, w);
-      if (x < 0.0) x += w;
-      x -= 0.5;
-      const double pi = 3.141592653589793;
-      const double lon = (x + 0.5) * (2.0 * pi) / w - pi, lat = (v + 0.5) * pi / h - pi / 2.0;
-      if (!std::isfinite(lon) || !std::isfinite(lat) || lat < -pi / 2.0 || lat > pi / 2.0) return false;
-      const double cl = std::cos(lat);
-      d[0] = cl * std::sin(lon);
-      d[1] = std::sin(lat);
-      d[2] = cl * std::cos(lon);
-      break;
-    }
-    default:
-      return false;
-  }
-  return normalize_bearing(d, b);
+  return camera_unproject_bearing(make_camera_dev(in), u, v, b);
 }
 
 // The calibrated lowering (native/calibrated.rs:200-494). Angular residuals (PreparedAngularProblem,
@@ -2563,3 +2389,58 @@ int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32
 void omvgba_plan_destroy(omvgba_plan* plan) { delete plan; }
 
 }  // extern "C"
+
+extern "C" int32_t omvgba_sfm_refresh_reprojection(omvgba_context* context, uint64_t pose_count,
+                                                   const omvgba_pose* poses, uint64_t intrinsic_count,
+                                                   const omvgba_intrinsic* intrinsics,
+                                                   const omvgba_landmark_tracks* tracks,
+                                                   omvgba_refresh_result* result, omvgba_error* error) {
+  clear_error(error);
+  if (!context || !tracks || !result || (pose_count && !poses) || (intrinsic_count && !intrinsics))
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
+  const uint64_t L = tracks->landmark_count;
+  if (!tracks->track_offset || (L && (!tracks->points || !tracks->active || !result->landmark_update ||
+                                      !result->reprojection_error)))
+    return write_error(error, OMVGBA_INVALID_ARGUMENT, "null landmark array");
+  try {
+    if (tracks->track_offset[0] != 0) fail(OMVGBA_INVALID_PROBLEM, "track offsets must start at zero");
+    for (uint64_t l = 0; l < L; ++l)
+      if (tracks->track_offset[l + 1] < tracks->track_offset[l])
+        fail(OMVGBA_INVALID_PROBLEM, "track offsets must not decrease");
+    const uint64_t N = tracks->track_offset[L];
+    if (N && (!tracks->track_pose || !tracks->track_intrinsic || !tracks->track_pixel || !tracks->track_support ||
+              !result->track_support))
+      return write_error(error, OMVGBA_INVALID_ARGUMENT, "null track array");
+    std::vector<uint8_t> used(intrinsic_count, 0);
+    for (uint64_t o = 0; o < N; ++o) {
+      const uint32_t p = tracks->track_pose[o], i = tracks->track_intrinsic[o];
+      if (p != OMVGBA_NO_POSE && p >= pose_count) fail(OMVGBA_INVALID_PROBLEM, "track pose index out of range");
+      if (i >= intrinsic_count) fail(OMVGBA_INVALID_PROBLEM, "track intrinsic index out of range");
+      if (p != OMVGBA_NO_POSE && tracks->track_support[o]) used[i] = 1;
+    }
+    // CameraResidualPolicy::from_pixel_limit (residual.rs:37-55) fails for a wide-angle camera
+    // without a positive finite pixel-to-angle scale
+    for (uint64_t i = 0; i < intrinsic_count; ++i) {
+      const CameraDev c = make_camera_dev(intrinsics[i]);
+      if (used[i] && camera_is_generalized(c) && !std::isfinite(camera_pixels_per_radian(c)))
+        fail(OMVGBA_INVALID_PROBLEM, "camera residual policy requires a positive finite pixel-to-angle scale");
+    }
+    std::vector<double> rot(9 * pose_count), cen(3 * pose_count);
+    for (uint64_t p = 0; p < pose_count; ++p) {
+      for (int k = 0; k < 9; ++k) rot[9 * p + k] = poses[p].rotation[k];
+      for (int k = 0; k < 3; ++k) cen[3 * p + k] = poses[p].center[k];
+    }
+    SfmRefreshInput in{pose_count, intrinsic_count, L, N, rot.data(), cen.data(), intrinsics, tracks->points,
+                       tracks->active, tracks->track_offset, tracks->track_pose, tracks->track_intrinsic,
+                       tracks->track_pixel, tracks->track_support};
+    SfmRefreshOutput out{result->landmark_update, result->reprojection_error, result->track_support};
+    gpu_sfm_refresh(context->ctx, in, out);
+    result->rejected_landmarks = out.rejected_landmarks;
+    result->removed_observations = out.removed_observations;
+    return OMVGBA_OK;
+  } catch (const SolveFailure& f) {
+    return write_error(error, f.code, f.message);
+  } catch (const std::exception& ex) {
+    return write_error(error, OMVGBA_INTERNAL, ex.what());
+  }
+}

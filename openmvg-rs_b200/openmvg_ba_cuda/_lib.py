@@ -69,6 +69,13 @@ def lib():
     L.omvgba_preflight_check.argtypes = [C.c_void_p, C.POINTER(abi.Problem), C.POINTER(abi.Config),
                                          C.POINTER(abi.Preflight), C.POINTER(abi.Error)]
     L.omvgba_preflight_check.restype = C.c_int32
+    L.omvgba_sfm_refresh_reprojection.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(abi.Pose), C.c_uint64,
+                                                  C.POINTER(abi.Intrinsic), C.POINTER(abi.LandmarkTracks),
+                                                  C.POINTER(abi.RefreshResult), C.POINTER(abi.Error)]
+    L.omvgba_sfm_refresh_reprojection.restype = C.c_int32
+    L.omvgba_sfm_prepare_problem.argtypes = [C.POINTER(abi.SfmWorkspace), C.POINTER(abi.SfmPrepareConfig),
+                                             C.POINTER(abi.SfmPrepared), C.POINTER(abi.Error)]
+    L.omvgba_sfm_prepare_problem.restype = C.c_int32
     vp, u64 = C.c_void_p, C.c_uint64
     L.omvgba_residual_forward_f32.argtypes = [vp, u64, vp, vp, vp, u64, vp, vp, vp, u64, vp, vp, C.POINTER(abi.Error)]
     L.omvgba_residual_forward_f32.restype = C.c_int32

@@ -355,3 +355,90 @@ PROBE_FULL_RANK_CERTIFIED, PROBE_INSUFFICIENT_CAMERA_COVERAGE, PROBE_RESOURCE_LI
 PROBE_WEAK_POINT_GEOMETRY, PROBE_SPARSE_FACTORIZATION_FAILED = 3, 4
 PREFLIGHT_PROCEED, PREFLIGHT_INSUFFICIENT_CAMERA_COVERAGE, PREFLIGHT_RESOURCE_LIMIT = 0, 1, 2
 PREFLIGHT_WEAK_POINT_GEOMETRY, PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED = 3, 4
+
+
+# ---- the SfM-side reprojection-error refresh (omvgba_sfm_refresh_reprojection) ----
+NO_POSE = 0xFFFFFFFF
+REFRESH_SKIPPED, REFRESH_REJECTED, REFRESH_UNCHANGED, REFRESH_PRUNED = 0, 1, 2, 3
+
+
+class LandmarkTracks(C.Structure):
+    _fields_ = [
+        ("landmark_count", C.c_uint64),
+        ("points", C.POINTER(C.c_double)),
+        ("active", C.POINTER(C.c_uint8)),
+        ("track_offset", C.POINTER(C.c_uint64)),
+        ("track_pose", C.POINTER(C.c_uint32)),
+        ("track_intrinsic", C.POINTER(C.c_uint32)),
+        ("track_pixel", C.POINTER(C.c_double)),
+        ("track_support", C.POINTER(C.c_uint8)),
+    ]
+
+
+class RefreshResult(C.Structure):
+    _fields_ = [
+        ("landmark_update", C.POINTER(C.c_uint8)),
+        ("reprojection_error", C.POINTER(C.c_double)),
+        ("track_support", C.POINTER(C.c_uint8)),
+        ("rejected_landmarks", C.c_uint64),
+        ("removed_observations", C.c_uint64),
+    ]
+
+
+def marshal_poses(rotations, centers):
+    """(Pose array, keep-alive) for world-to-camera rotations (n, 3, 3) and camera centres (n, 3)."""
+    n = len(rotations)
+    poses = (Pose * n)()
+    raw = np.frombuffer(poses, dtype=np.uint8).reshape(n, C.sizeof(Pose)) if n else None
+    if n:
+        view = raw.view(np.dtype([("rotation", "<f8", 9), ("center", "<f8", 3), ("variables", "<u4"), ("reserved", "<u4")]))
+        view["rotation"][:, 0] = np.ascontiguousarray(rotations, dtype=np.float64).reshape(n, 9)
+        view["center"][:, 0] = np.ascontiguousarray(centers, dtype=np.float64).reshape(n, 3)
+    return poses
+
+
+# ---- building the problem from a reconstruction (omvgba_sfm_prepare_problem) ----
+SCOPE_FULL, SCOPE_POINTS_ONLY, SCOPE_POSES_ONLY, SCOPE_TRANSLATIONS_AND_POINTS, SCOPE_SELF_CALIBRATION = 0, 1, 2, 3, 4
+
+
+class SfmWorkspace(C.Structure):
+    _fields_ = [
+        ("view_count", C.c_uint64),
+        ("view_pose", C.POINTER(C.c_uint32)),
+        ("view_intrinsic", C.POINTER(C.c_uint32)),
+        ("view_size", C.POINTER(C.c_uint32)),
+        ("pose_count", C.c_uint64),
+        ("poses", C.POINTER(Pose)),
+        ("intrinsic_count", C.c_uint64),
+        ("intrinsics", C.POINTER(Intrinsic)),
+        ("intrinsic_guess", C.POINTER(C.c_uint8)),
+        ("landmarks", LandmarkTracks),
+    ]
+
+
+class SfmPrepareConfig(C.Structure):
+    _fields_ = [
+        ("scope", C.c_int32),
+        ("fixed_view_count", C.c_uint64),
+        ("fixed_views", C.POINTER(C.c_uint32)),
+        ("fixed_landmark_count", C.c_uint64),
+        ("fixed_landmarks", C.POINTER(C.c_uint32)),
+        ("excluded_landmark_count", C.c_uint64),
+        ("excluded_landmarks", C.POINTER(C.c_uint32)),
+        ("loss_kind", C.c_int32),
+        ("loss_scale", C.c_double),
+        ("loss_scale_space", C.c_int32),
+        ("gauge_kind", C.c_int32),
+        ("gauge_first_view", C.c_uint32),
+        ("gauge_second_view", C.c_uint32),
+        ("gauge_distance", C.c_double),
+    ]
+
+
+class SfmPrepared(C.Structure):
+    _fields_ = [
+        ("problem", Problem),
+        ("pose_rows", C.POINTER(C.c_uint32)),
+        ("intrinsic_rows", C.POINTER(C.c_uint32)),
+        ("landmark_rows", C.POINTER(C.c_uint32)),
+    ]

@@ -83,6 +83,44 @@ def problem_for(rank: int, workload: str = DEFAULT_WORKLOAD):
     return synthetic.plane_problem(seed=11 + rank, **WORKLOADS[workload]["kwargs"])
 
 
+def sfm_refresh_leg(problem, steps: int, sample: int = 3000) -> dict:
+    """The landmark reprojection-error refresh openmvg-sfm runs after a solve, over the workload's
+    landmarks (every observation supporting, every view posed): end to end from host arrays through
+    omvgba_sfm_refresh_reprojection (upload, kernel, download), against the oracle's restatement on
+    the first `sample` landmarks on one host thread."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sfm_oracle  # the CPU baseline's restatement only
+    from openmvg_ba_cuda.adjuster import CudaBundleAdjuster
+    from openmvg_ba_cuda.sfm import LandmarkTracks, refresh_reprojection
+    P = len(problem.points)
+    order = np.argsort(problem.observation_point, kind="stable")
+    offset = np.concatenate([[0], np.cumsum(np.bincount(problem.observation_point, minlength=P))]).astype(np.uint64)
+    tracks = LandmarkTracks(points=problem.points, active=np.ones(P, np.uint8), track_offset=offset,
+                            track_pose=problem.observation_pose[order].astype(np.uint32),
+                            track_intrinsic=problem.observation_intrinsic[order].astype(np.uint32),
+                            track_pixel=np.ascontiguousarray(problem.observation_pixel[order]),
+                            track_support=np.ones(len(order), np.uint8))
+    with CudaBundleAdjuster(0) as ba:
+        refresh_reprojection(ba, problem.rotations, problem.centers, problem.intrinsics, tracks)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            out = refresh_reprojection(ba, problem.rotations, problem.centers, problem.intrinsics, tracks)
+        gpu_s = (time.perf_counter() - t0) / steps
+    n = min(sample, P)
+    sub = LandmarkTracks(points=tracks.points[:n], active=tracks.active[:n], track_offset=offset[:n + 1],
+                         track_pose=tracks.track_pose, track_intrinsic=tracks.track_intrinsic,
+                         track_pixel=tracks.track_pixel, track_support=tracks.track_support)
+    t0 = time.perf_counter()
+    sfm_oracle.refresh(problem.rotations, problem.centers, problem.intrinsics, sub, np.zeros(n))
+    cpu_s = time.perf_counter() - t0
+    obs = int(offset[-1])
+    return {"kernel": "k_sfm_refresh", "landmarks": P, "observations": obs,
+            "e2e_seconds": gpu_s, "e2e_observations_per_s": obs / gpu_s,
+            "rejected_landmarks": out.rejected_landmarks, "removed_observations": out.removed_observations,
+            "cpu_oracle_observations_per_s": int(offset[n]) / cpu_s, "cpu_sample": f"first {n} landmarks, 1 thread, pure Python"}
+
+
 def solve_config(precision: int, max_iterations: int = 50, stream: int = 0):
     from openmvg_ba_cuda import SolveConfig, abi
     return SolveConfig(linear_solver=abi.SOLVER_ITERATIVE, precision=precision, pcg_relative_tolerance=1e-6,
@@ -553,6 +591,12 @@ def run_ours(args) -> int:
     adjuster = CudaBundleAdjuster(local)
     mixed_cfg = solve_config(abi.PRECISION_MIXED, max_iterations=args.max_iterations, stream=stream.cuda_stream)
 
+    if args.legs == "sfm":  # the SfM-side refresh around the solve, on the workload's landmarks
+        adjuster.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "legs": "sfm", "workload": args.workload,
+                              "sfm_refresh": sfm_refresh_leg(problem, max(args.steps, 3))}), flush=True)
+        return 0
     # value: mixed precision, problem resident in device memory
     plan = adjuster.plan(problem, mixed_cfg)
     info = plan.info()
@@ -690,9 +734,10 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--max-iterations", type=int, default=MAX_ITERATIONS, help="LM iteration budget of every solve")
-    ap.add_argument("--legs", choices=["all", "gpu", "value", "kernel"], default="all",
+    ap.add_argument("--legs", choices=["all", "gpu", "value", "kernel", "sfm"], default="all",
                     help="gpu: every leg but the CPU baseline; value: only the resident mixed solve and the kernel "
-                         "timing (for profiler runs); kernel: only the product kernel's timing, no solve")
+                         "timing (for profiler runs); kernel: only the product kernel's timing, no solve; sfm: the "
+                         "SfM-side reprojection-error refresh over the workload's landmarks")
     ap.add_argument("--no-second-leg", dest="second_leg", action="store_false",
                     help="skip the 500-camera mixed/FP64 leg of the headline line")
     args = ap.parse_args(argv)

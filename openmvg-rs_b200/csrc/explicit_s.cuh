@@ -471,6 +471,7 @@ __device__ __forceinline__ void acc_store(const double acc[4][4], double* g) {
 __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* status) {
   __shared__ double Ls[kCT * (kCT + 1)];  // the tile in, then L (column-major, padded)
   __shared__ double pub[2][kCT];
+  __shared__ double piv[2][3];  // pivot, its square root and the root's reciprocal
   __shared__ double rdiag[kCT];
   if (status[0] == 0) return;
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
@@ -490,32 +491,47 @@ __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* sta
     if (tx == (j >> 2)) {  // static register indices: the column is picked by selects
       const int bj = j & 3;
 #pragma unroll
-      for (int ai = 0; ai < 4; ++ai)
-        cj[4 * ty + ai] = bj == 0 ? a[ai][0] : (bj == 1 ? a[ai][1] : (bj == 2 ? a[ai][2] : a[ai][3]));
+      for (int ai = 0; ai < 4; ++ai) {
+        const double v = bj == 0 ? a[ai][0] : (bj == 1 ? a[ai][1] : (bj == 2 ? a[ai][2] : a[ai][3]));
+        cj[4 * ty + ai] = v;
+        if (4 * ty + ai == j) {  // the diagonal's owner takes the root once for every thread
+          const double r = sqrt(v);
+          piv[j & 1][0] = v;
+          piv[j & 1][1] = r;
+          piv[j & 1][2] = 1.0 / r;
+        }
+      }
     }
     __syncthreads();
-    const double d = cj[j];  // the same value in every thread: all leave together
+    const double d = piv[j & 1][0];  // the same value in every thread: all leave together
     if (!(isfinite(d) && d > 0.0)) {
       if (tid == 0) status[0] = 0;
       return;
     }
-    const double sd = sqrt(d), rs = 1.0 / sd;
+    const double sd = piv[j & 1][1], rs = piv[j & 1][2];
+    // branch-free update: the multipliers of columns at or left of j are zero, so those columns keep
+    // their values; elements above the diagonal take values that are never read (zeroed on output)
     double li[4], lc[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       li[q] = cj[4 * ty + q] * rs;
-      lc[q] = cj[4 * tx + q] * rs;
+      lc[q] = 4 * tx + q > j ? cj[4 * tx + q] * rs : 0.0;
     }
 #pragma unroll
     for (int ai = 0; ai < 4; ++ai)
 #pragma unroll
-      for (int bi = 0; bi < 4; ++bi) {
-        const int i = 4 * ty + ai, c = 4 * tx + bi;
-        if (c == j && i >= j)
-          a[ai][bi] = i == j ? sd : li[ai];
-        else if (c > j && c <= i)
-          a[ai][bi] -= li[ai] * lc[bi];
-      }
+      for (int bi = 0; bi < 4; ++bi) a[ai][bi] -= li[ai] * lc[bi];
+    if (tx == (j >> 2)) {  // column j becomes the factor's column
+#pragma unroll
+      for (int bi = 0; bi < 4; ++bi)
+        if (4 * tx + bi == j) {
+#pragma unroll
+          for (int ai = 0; ai < 4; ++ai) {
+            const int i = 4 * ty + ai;
+            if (i >= j) a[ai][bi] = i == j ? sd : li[ai];
+          }
+        }
+    }
   }
   __syncthreads();  // every thread has read the last published column before Ls is rewritten
 #pragma unroll
@@ -555,14 +571,14 @@ __global__ void __launch_bounds__(256) k_tile_potrf(TileBand tb, int k, int* sta
         }
     }
     __syncthreads();
+    // branch-free: the published row is zero right of column j and the multipliers are zero at or
+    // above row j, so only the rows below j change, in the columns up to j
 #pragma unroll
     for (int ai = 0; ai < 4; ++ai) {
       const int i = 4 * ty + ai;
-      if (i <= j) continue;
-      const double lij = Ls[j * (kCT + 1) + i];
+      const double lij = i > j ? Ls[j * (kCT + 1) + i] : 0.0;
 #pragma unroll
-      for (int bi = 0; bi < 4; ++bi)
-        if (4 * tx + bi <= j) a[ai][bi] -= lij * xj[4 * tx + bi];
+      for (int bi = 0; bi < 4; ++bi) a[ai][bi] -= lij * xj[4 * tx + bi];
     }
   }
   __syncthreads();  // Ls is reused to stage W for coalesced stores

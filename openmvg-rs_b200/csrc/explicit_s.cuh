@@ -758,13 +758,6 @@ __global__ void k_perm_scatter(int n, const int* __restrict__ perm_to_orig, cons
 constexpr size_t kTakahashiSmem = 2 * kStagedTile;
 constexpr int kTakahashiChunk = 4;
 
-__device__ __forceinline__ void acc_add_tile(double acc[4][4], const double* __restrict__ g) {
-  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-#pragma unroll
-  for (int b = 0; b < 4; ++b)
-#pragma unroll
-    for (int a = 0; a < 4; ++a) acc[a][b] += g[(size_t)(4 * tx + b) * kCT + 4 * ty + a];
-}
 // acc (output tile element (4 ty + a, 4 tx + b)) transposed into a staged A operand: A(c, r) = acc(r, c)
 __device__ __forceinline__ void acc_to_at(const double acc[4][4], double* T) {
   const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
@@ -806,12 +799,16 @@ __global__ void __launch_bounds__(256) k_takahashi_offdiag(TileBand L, TileBand 
   double* Ta = sh;
   double* Tb = sh + kCT * kTS;
   const int i = j + 1 + blockIdx.x;
-  double acc[4][4];
-  zero_acc(acc);
-  for (int s = 0; s < nsplit; ++s) acc_add_tile(acc, part + ((size_t)blockIdx.x * nsplit + s) * kCTT);
-  acc_to_a(acc, -1.0, Ta);
+  // -(sum of the partial tiles, in order) into the A operand, read along the tiles' storage
+  const double* pb = part + (size_t)blockIdx.x * nsplit * kCTT;
+  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {
+    double v = 0.0;
+    for (int s = 0; s < nsplit; ++s) v += pb[(size_t)s * kCTT + w];
+    Ta[(w / kCT) * kTS + (w % kCT)] = -v;
+  }
   stage_tile(L.w + (size_t)j * kCTT, Tb, true, false);  // W_j
   __syncthreads();
+  double acc[4][4];
   zero_acc(acc);
   tile_mma_acc(Ta, Tb, acc);
   acc_store(acc, Z.t + tile_at(Z, i, j));
@@ -830,16 +827,19 @@ __global__ void __launch_bounds__(256) k_takahashi_diag(TileBand L, TileBand Z, 
   if (status[0] == 0) return;
   double* Ta = sh;
   double* Tb = sh + kCT * kTS;
-  double acc[4][4];
-  zero_acc(acc);
-  for (int b = 0; b < m; ++b) acc_add_tile(acc, q + (size_t)b * kCTT);
-  acc_to_a(acc, -1.0, Ta);  // -acc
+  // -(sum of the tiles' shares, in order) into the A operand, read along the tiles' storage
+  for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {
+    double v = 0.0;
+    for (int b = 0; b < m; ++b) v += q[(size_t)b * kCTT + w];
+    Ta[(w / kCT) * kTS + (w % kCT)] = -v;
+  }
   const double* wj = L.w + (size_t)j * kCTT;
   __syncthreads();
   for (int w = threadIdx.x; w < kCTT; w += blockDim.x) {  // + W_j^T: A(r, q) += W(q, r)
     const int c = w / kCT, r = w - c * kCT;                // W(r, c) at wj[w]
     Ta[r * kTS + c] += wj[w];                              // A element (c, r) of the operand
   }
+  double acc[4][4];
   stage_tile(wj, Tb, true, false);  // W_j
   __syncthreads();
   zero_acc(acc);

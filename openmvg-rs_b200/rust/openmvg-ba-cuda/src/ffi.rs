@@ -238,6 +238,84 @@ pub const OMVGBA_PREFLIGHT_RESOURCE_LIMIT: i32 = 2;
 pub const OMVGBA_PREFLIGHT_WEAK_POINT_GEOMETRY: i32 = 3;
 pub const OMVGBA_PREFLIGHT_OBSERVABILITY_NOT_CERTIFIED: i32 = 4;
 
+// ---- the SfM side of a bundle adjustment (openmvg-sfm ops/reconstruction/bundle.rs) ----
+pub const OMVGBA_NO_POSE: u32 = 0xFFFF_FFFF;
+
+#[repr(C)]
+#[derive(Clone, Copy)]
+pub struct omvgba_landmark_tracks {
+    pub landmark_count: u64,
+    pub points: *const f64,
+    pub active: *const u8,
+    pub track_offset: *const u64,
+    pub track_pose: *const u32,
+    pub track_intrinsic: *const u32,
+    pub track_pixel: *const f64,
+    pub track_support: *const u8,
+}
+
+// omvgba_refresh_update
+pub const OMVGBA_REFRESH_SKIPPED: u8 = 0;
+pub const OMVGBA_REFRESH_REJECTED: u8 = 1;
+pub const OMVGBA_REFRESH_UNCHANGED: u8 = 2;
+pub const OMVGBA_REFRESH_PRUNED: u8 = 3;
+
+#[repr(C)]
+pub struct omvgba_refresh_result {
+    pub landmark_update: *mut u8,
+    pub reprojection_error: *mut f64,
+    pub track_support: *mut u8,
+    pub rejected_landmarks: u64,
+    pub removed_observations: u64,
+}
+
+// omvgba_scope
+pub const OMVGBA_SCOPE_FULL: i32 = 0;
+pub const OMVGBA_SCOPE_POINTS_ONLY: i32 = 1;
+pub const OMVGBA_SCOPE_POSES_ONLY: i32 = 2;
+pub const OMVGBA_SCOPE_TRANSLATIONS_AND_POINTS: i32 = 3;
+pub const OMVGBA_SCOPE_SELF_CALIBRATION: i32 = 4;
+
+#[repr(C)]
+pub struct omvgba_sfm_workspace {
+    pub view_count: u64,
+    pub view_pose: *const u32,
+    pub view_intrinsic: *const u32,
+    pub view_size: *const u32,
+    pub pose_count: u64,
+    pub poses: *const omvgba_pose,
+    pub intrinsic_count: u64,
+    pub intrinsics: *const omvgba_intrinsic,
+    pub intrinsic_guess: *const u8,
+    pub landmarks: omvgba_landmark_tracks,
+}
+
+#[repr(C)]
+pub struct omvgba_sfm_prepare_config {
+    pub scope: i32,
+    pub fixed_view_count: u64,
+    pub fixed_views: *const u32,
+    pub fixed_landmark_count: u64,
+    pub fixed_landmarks: *const u32,
+    pub excluded_landmark_count: u64,
+    pub excluded_landmarks: *const u32,
+    pub loss_kind: i32,
+    pub loss_scale: f64,
+    pub loss_scale_space: i32,
+    pub gauge_kind: i32,
+    pub gauge_first_view: u32,
+    pub gauge_second_view: u32,
+    pub gauge_distance: f64,
+}
+
+#[repr(C)]
+pub struct omvgba_sfm_prepared {
+    pub problem: omvgba_problem,
+    pub pose_rows: *mut u32,
+    pub intrinsic_rows: *mut u32,
+    pub landmark_rows: *mut u32,
+}
+
 /// Opaque per-thread solver context.
 #[repr(C)]
 pub struct omvgba_context {
@@ -264,6 +342,22 @@ unsafe extern "C" {
         problem: *const omvgba_problem,
         config: *const omvgba_config,
         preflight: *mut omvgba_preflight,
+        error: *mut omvgba_error,
+    ) -> i32;
+    pub fn omvgba_sfm_prepare_problem(
+        workspace: *const omvgba_sfm_workspace,
+        config: *const omvgba_sfm_prepare_config,
+        prepared: *mut omvgba_sfm_prepared,
+        error: *mut omvgba_error,
+    ) -> i32;
+    pub fn omvgba_sfm_refresh_reprojection(
+        context: *mut omvgba_context,
+        pose_count: u64,
+        poses: *const omvgba_pose,
+        intrinsic_count: u64,
+        intrinsics: *const omvgba_intrinsic,
+        tracks: *const omvgba_landmark_tracks,
+        result: *mut omvgba_refresh_result,
         error: *mut omvgba_error,
     ) -> i32;
 }

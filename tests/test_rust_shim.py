@@ -48,7 +48,8 @@ def test_shim_structs_mirror_the_header():
     c = c_structs(open(HEADER).read())
     rust = rust_structs(open(FFI).read())
     mirrored = ["omvgba_error", "omvgba_pose", "omvgba_intrinsic", "omvgba_problem", "omvgba_config",
-                "omvgba_report", "omvgba_solution", "omvgba_preflight"]
+                "omvgba_report", "omvgba_solution", "omvgba_preflight", "omvgba_landmark_tracks",
+                "omvgba_refresh_result", "omvgba_sfm_workspace", "omvgba_sfm_prepare_config", "omvgba_sfm_prepared"]
     for name in mirrored:
         assert name in c and name in rust, name
         cf, rf = c[name], rust[name]

@@ -374,9 +374,10 @@ def kernel_roofline(plan, info: dict, stream, flush, workload: str, launches: in
             "algorithmic_bytes_per_launch": algorithmic, "avg_launch_us": avg_s * 1e6, "launches_timed": launches}
 
 
-def rows_timing(plan, info: dict, stream, flush, launches: int = 20) -> dict:
-    """Average duration of k_block_rows, the block-row build of the explicit reduced camera system
-    from the current linearization (CUDA events on the plan's stream, L2 flushed before each launch)."""
+def stage_timing(plan, info: dict, stream, flush, stage: int, kernel: str, launches: int = 20) -> dict:
+    """Average duration of one product stage of the plan by itself (CUDA events on the plan's stream,
+    L2 flushed before each launch): stage 2 is k_block_rows, the block-row build of the explicit
+    reduced camera system; stage 3 the camera-side assembly sums, k_block_tiles then k_block_records."""
     import torch
     D = int(info["reduced_dimension"])
     x = torch.zeros(D, dtype=torch.float64, device="cuda")
@@ -387,11 +388,15 @@ def rows_timing(plan, info: dict, stream, flush, launches: int = 20) -> dict:
             flush.fill_(3)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        plan.schur_product(x.data_ptr(), x.data_ptr(), 0.1, fp32=True, stage=2)
+        plan.schur_product(x.data_ptr(), x.data_ptr(), 0.1, fp32=True, stage=stage)
         e1.record(stream)
         e1.synchronize()
         total += e0.elapsed_time(e1)
-    return {"kernel": "k_block_rows", "avg_launch_us": total / launches * 1e3, "launches_timed": launches}
+    avg_us = total / launches * 1e3
+    out = {"kernel": kernel, "avg_launch_us": avg_us, "launches_timed": launches}
+    if stage == 3:  # the FP32 records each observation's sums read, per second
+        out["observations_per_s"] = int(info["observation_count"]) / (avg_us * 1e-6)
+    return out
 
 
 def run_batched(args) -> int:
@@ -602,12 +607,14 @@ def run_ours(args) -> int:
     info = plan.info()
     if args.legs == "kernel":  # the kernels' timings alone, no solve (for a small ncu capture)
         roofline = kernel_roofline(plan, info, stream, flush, args.workload, launches=max(args.steps, 3))
-        rows = rows_timing(plan, info, stream, flush, launches=max(args.steps, 3))
+        rows = stage_timing(plan, info, stream, flush, 2, "k_block_rows", launches=max(args.steps, 3))
+        sums = stage_timing(plan, info, stream, flush, 3, "k_block_tiles + k_block_records",
+                            launches=max(args.steps, 3))
         plan.close()
         adjuster.close()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "legs": "kernel", "n_gpus": world, "roofline": roofline,
-                              "explicit_rows": rows, "observations": int(info["observation_count"])}), flush=True)
+                              "explicit_rows": rows, "camera_sums": sums, "observations": int(info["observation_count"])}), flush=True)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -630,6 +637,8 @@ def run_ours(args) -> int:
     value = total_its / total_s
     launches = sum(r["kernel_launches"] for r in reports)
     roofline = kernel_roofline(plan, info, stream, flush, args.workload)
+    kernels = {"camera_sums": stage_timing(plan, info, stream, flush, 3, "k_block_tiles + k_block_records"),
+               "explicit_rows": stage_timing(plan, info, stream, flush, 2, "k_block_rows")}
     plan.close()
 
     if args.legs == "value":  # profiling runs: the resident mixed solve and the kernel timing only
@@ -715,6 +724,7 @@ def run_ours(args) -> int:
                     "host_buffers": "numpy arrays passed to omvgba_solve (lowering on the host inside the step)"},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "kernel_timings": kernels,
             "cpu_baseline": cpu,
             "cpu_baseline_single_thread": cpu1,
             "wall_s_timed_region": wall,

@@ -278,7 +278,9 @@ int32_t omvgba_plan_info_get(const omvgba_plan* plan, omvgba_plan_info* info, om
  * x and y are DEVICE pointers of reduced_dimension doubles. fp32 selects the FP32 records of a
  * mixed plan. stage 0 computes the whole product; stage 1 launches only the tile pass (the
  * per-point coupling partials, y untouched), for timing the kernel by itself; stage 2 builds only the
- * explicit S of the linearization by block rows (x and y untouched), for timing that kernel. Runs on
+ * explicit S of the linearization by block rows (x and y untouched), for timing that kernel; stage 3
+ * runs only the camera-side sums of the linearization's assembly (U blocks, gradients, damping
+ * diagonal, pose/intrinsic edges and point coupling per block; x and y untouched). Runs on
  * the plan's stream without synchronizing. Operator: retained/operator.rs:137-227.
  */
 int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32, int32_t stage, const double* x,

@@ -5,8 +5,9 @@
 //                            Jacobians (one CTA per tile of whole points) and the per-point 3x3
 //                            Gram + FP64 damped inverse
 //                            (schur/point.rs:176-448, schur/assembly.rs:893-1040, point_block.rs:78-184)
-//   K2  k_block_chunks ..... camera-side deterministic segmented reductions: U blocks, g, reduced g,
-//                            damping diagonal, pose/intrinsic edges, diagonal point coupling
+//   K2  k_block_tiles ...... camera-side deterministic segmented sums over the record tiles: U blocks,
+//       k_block_records      g, reduced g, damping diagonal, pose/intrinsic edges, diagonal point
+//                            coupling (asm_tiles.cuh)
 //       k_pairs ............ explicit Schur blocks S_bb' -= W V^-1 W^T (schur/assembly.rs:999-1038)
 //   K3  k_block_rows ....... explicit S by block rows (BSR), banded tiled FP64 Cholesky and solves
 //                            (explicit_s.cuh; stands in for faer's sparse LLT)
@@ -574,123 +575,8 @@ struct BlockTables {
   const int* blk_chunk_end;
 };
 
-// Assembly record per chunk: U lower (21), g (6), reduced g (6), diag (6), edge (18), coupling lower (21)
+// Assembly record per block: U lower (21), g (6), reduced g (6), diag (6), edge (18), coupling lower (21)
 constexpr int kAsmRec = 21 + 6 + 6 + 6 + 18 + 21;
-
-template <typename T>
-__global__ void __launch_bounds__(32) k_block_chunks(BlockTables bt, LinOut<T> lin, const int* obs_intr_col,
-                                                     double* chunk_out) {
-  int c = blockIdx.x;
-  if (c >= bt.nchunks) return;
-  int lane = threadIdx.x;
-  int b = bt.chunk_block[c];
-  int d = bt.blk_dim[b];
-  int col = bt.chunk_col[c];
-  bool has_edge = bt.blk_edge[b] >= 0;
-  double U[21], gfull[6], gred[6], dg[6], E[18], Cpl[21];
-#pragma unroll
-  for (int k = 0; k < 21; ++k) {
-    U[k] = 0.0;
-    Cpl[k] = 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) gfull[k] = gred[k] = dg[k] = 0.0;
-#pragma unroll
-  for (int k = 0; k < 18; ++k) E[k] = 0.0;
-  for (uint32_t i = bt.chunk_begin[c] + lane; i < bt.chunk_end[c]; i += 32) {
-    uint32_t e = bt.ent[i];
-    uint32_t o = e >> 1;
-    uint32_t p = bt.ent_point[i];
-    const T* jc = lin.rec + lin.obs_rec[o];
-    const int rs = lin.rs;
-    double a0[6], a1[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      a0[k] = k < d ? (double)jc[(col + k) * rs] : 0.0;
-      a1[k] = k < d ? (double)jc[(9 + col + k) * rs] : 0.0;
-    }
-    double r0 = lin.rw[2 * o], r1 = lin.rw[2 * o + 1];
-    const T* jp = jc + kJp * rs;
-    double p0[3] = {(double)jp[0], (double)jp[rs], (double)jp[2 * rs]};
-    double p1[3] = {(double)jp[3 * rs], (double)jp[4 * rs], (double)jp[5 * rs]};
-    const double* ig = lin.ig + 3 * (size_t)p;
-    // reduced residual: r_w - Jp (Vhat^-1 g_p)
-    double q0 = r0 - (p0[0] * ig[0] + p0[1] * ig[1] + p0[2] * ig[2]);
-    double q1 = r1 - (p1[0] * ig[0] + p1[1] * ig[1] + p1[2] * ig[2]);
-    // A = Jp Vhat^-1 Jp^T (2x2)
-    const double* vi = lin.vinv + 6 * (size_t)p;
-    double t0[3], t1[3];
-    sym3_apply(vi, p0, t0);
-    sym3_apply(vi, p1, t1);
-    double A00 = p0[0] * t0[0] + p0[1] * t0[1] + p0[2] * t0[2];
-    double A01 = p0[0] * t1[0] + p0[1] * t1[1] + p0[2] * t1[2];
-    double A11 = p1[0] * t1[0] + p1[1] * t1[1] + p1[2] * t1[2];
-    int idx = 0;
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      gfull[r] += a0[r] * r0 + a1[r] * r1;
-      gred[r] += a0[r] * q0 + a1[r] * q1;
-      dg[r] += a0[r] * a0[r] + a1[r] * a1[r];
-      // (A a)_r terms for coupling: c_r = [a0_r a1_r] A
-      double c0 = a0[r] * A00 + a1[r] * A01;
-      double c1 = a0[r] * A01 + a1[r] * A11;
-#pragma unroll
-      for (int s2 = 0; s2 <= r; ++s2) {
-        U[idx] += a0[r] * a0[s2] + a1[r] * a1[s2];
-        Cpl[idx] += c0 * a0[s2] + c1 * a1[s2];
-        ++idx;
-      }
-    }
-    if (has_edge) {
-      int icol = obs_intr_col[o];  // column of the intrinsic segment (pose dim), idim in upper bits
-      int id = icol >> 8;
-      icol &= 0xff;
-#pragma unroll
-      for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-          if (k < id) E[3 * r + k] += a0[r] * (double)jc[(icol + k) * rs] + a1[r] * (double)jc[(9 + icol + k) * rs];
-    }
-  }
-  double* rec = chunk_out + (size_t)kAsmRec * c;
-#pragma unroll
-  for (int k = 0; k < 21; ++k) {
-    double s = warp_sum(U[k]);
-    double t = warp_sum(Cpl[k]);
-    if (lane == 0) {
-      rec[k] = s;
-      rec[57 + k] = t;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    double a = warp_sum(gfull[k]), bb = warp_sum(gred[k]), cc = warp_sum(dg[k]);
-    if (lane == 0) {
-      rec[21 + k] = a;
-      rec[27 + k] = bb;
-      rec[33 + k] = cc;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 18; ++k) {
-    double s = warp_sum(E[k]);
-    if (lane == 0) rec[39 + k] = s;
-  }
-}
-
-// Per block: sum its chunk records in chunk order -> block assembly record.
-__global__ void k_block_finalize(BlockTables bt, const double* chunk_out, double* blk_out) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= bt.nblocks) return;
-  double acc[kAsmRec];
-  for (int k = 0; k < kAsmRec; ++k) acc[k] = 0.0;
-  for (int c = bt.blk_chunk_begin[b]; c < bt.blk_chunk_end[b]; ++c) {
-    const double* rec = chunk_out + (size_t)kAsmRec * c;
-    for (int k = 0; k < kAsmRec; ++k) acc[k] += rec[k];
-  }
-  double* out = blk_out + (size_t)kAsmRec * b;
-  for (int k = 0; k < kAsmRec; ++k) out[k] = acc[k];
-}
 
 // Scatter block records into the D-vectors (g, reduced g, diag) — one thread per block.
 __global__ void k_block_vectors(BlockTables bt, const double* blk_out, double* gfull, double* gred, double* diag,
@@ -1001,6 +887,7 @@ __global__ void k_pcg_direction(int n, const double* __restrict__ rr_part, const
 // ----------------------------------------------------------------------------------------------
 }  // namespace omvgba
 #include "mv_tiles.cuh"
+#include "asm_tiles.cuh"
 #include "explicit_s.cuh"
 #include "two_view.cuh"
 namespace omvgba {
@@ -2281,8 +2168,8 @@ struct Solver {
   DBuf<PointSummary> d_summary, d_summary_part;
   DBuf<int> d_blk_off, d_blk_dim, d_blk_col, d_blk_edge, d_chunk_block, d_chunk_col, d_blk_chunk_begin, d_blk_chunk_end;
   DBuf<uint32_t> d_ent, d_ent_point, d_chunk_begin, d_chunk_end;
-  DBuf<int> d_obs_intr_col, d_seg_col;
-  DBuf<double> d_chunk_out, d_blk_out;
+  DBuf<int> d_seg_col;
+  DBuf<double> d_blk_out;
   DBuf<double> d_gfull, d_gred, d_diag, d_diag_minmax;
   DBuf<int> d_clamp;
   // pairs
@@ -2297,6 +2184,8 @@ struct Solver {
   DBuf<double> d_rows, d_tiles, d_winv, d_ztiles, d_perm_vec, d_marg_out, d_power;
   bool rows_valid = false;  // the rows hold S of the current assembly
   bool rows_attr = false;   // k_block_rows may take kRowSmemDoubles of dynamic shared memory
+  bool asm_attr = false;    // k_block_tiles stages kAsmComp (TILE + 1) doubles in dynamic shared memory
+  DBuf<double> d_asm_rec;   // per (block, segment) assembly records, kAsmRecordScale per partial element
   // PCG vectors
   DBuf<double> d_step, d_r, d_z, d_dir, d_q, d_factor, d_tmp, d_rhs, d_r64, d_e, d_dq, d_rr_part, d_rz_part;
   DBuf<int> d_fail;
@@ -2513,7 +2402,6 @@ struct Solver {
     up_u(d_chunk_end, S.chunk_end);
     up_i(d_blk_chunk_begin, S.blk_chunk_begin);
     up_i(d_blk_chunk_end, S.blk_chunk_end);
-    up_i(d_obs_intr_col, S.obs_intr_col);
     up_i(d_seg_col, S.seg_col);
     up_i(d_xgrp_row, S.xgrp_row);
     up_i(d_xgrp_col, S.xgrp_col);
@@ -2524,7 +2412,6 @@ struct Solver {
     up_u(d_xpair_p, S.xpair_p);
     up_i(d_blk_cross_begin, S.blk_cross_begin);
     up_i(d_blk_cross_end, S.blk_cross_end);
-    d_chunk_out.alloc((size_t)kAsmRec * std::max<size_t>(1, S.chunk_block.size()), st);
     d_blk_out.alloc((size_t)kAsmRec * std::max(1, nb), st);
     d_gfull.alloc(std::max(1, D), st);
     d_gred.alloc(std::max(1, D), st);
@@ -2652,11 +2539,7 @@ struct Solver {
     check_launch();
     BlockTables bt = tables();
     if (bt.nchunks > 0) {
-      if (mixed)
-        OMVGBA_LAUNCH(k_block_chunks<float>, bt.nchunks, 32, 0, st, bt, lin32(), d_obs_intr_col.p, d_chunk_out.p);
-      else
-        OMVGBA_LAUNCH(k_block_chunks<T>, bt.nchunks, 32, 0, st, bt, lin(), d_obs_intr_col.p, d_chunk_out.p);
-      OMVGBA_LAUNCH(k_block_finalize, grid_for(nb, 64), 64, 0, st, bt, d_chunk_out.p, d_blk_out.p);
+      camera_sums();
       CUDA_OK(cudaMemsetAsync(d_gfull.p, 0, sizeof(double) * std::max(1, D), st));
       CUDA_OK(cudaMemsetAsync(d_gred.p, 0, sizeof(double) * std::max(1, D), st));
       CUDA_OK(cudaMemsetAsync(d_diag.p, 0, sizeof(double) * std::max(1, D), st));
@@ -2724,6 +2607,36 @@ struct Solver {
   }
 
   // S of the current linearization (no damping) by block rows, from the FP64 or FP32 records.
+  // The camera-side sums of the current linearization into the block assembly records (d_blk_out):
+  // a pass over the record tiles, then each block's records in tile order.
+  void camera_sums() {
+    const int nb = (int)S.blk_off.size();
+    BlockTables bt = tables();
+    const TileSetDev& ts = mixed ? dT32 : dT64;
+    MvTiles mt = ts.view(d_blk_dim.p, d_blk_off.p, nb);
+    if (d_asm_rec.n != (size_t)kAsmRecordScale * ts.partial.n) {
+      d_asm_rec.alloc((size_t)kAsmRecordScale * ts.partial.n, st);
+      d_asm_rec.zero();  // record entries past a block's columns stay zero
+    }
+    if (!asm_attr) {
+      CUDA_OK(cudaFuncSetAttribute(k_block_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)asm_smem_bytes<float>()));
+      CUDA_OK(cudaFuncSetAttribute(k_block_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)asm_smem_bytes<T>()));
+      asm_attr = true;
+    }
+    const uint32_t* pt_off = view().pt_off;
+    if (mt.ntiles > 0) {
+      if (mixed)
+        OMVGBA_LAUNCH(k_block_tiles<float>, mt.ntiles, mv_tile_obs<float>(),
+                      asm_smem_bytes<float>(), st, mt, lin32(), pt_off, d_asm_rec.p);
+      else
+        OMVGBA_LAUNCH(k_block_tiles<T>, mt.ntiles, mv_tile_obs<T>(),
+                      asm_smem_bytes<T>(), st, mt, lin(), pt_off, d_asm_rec.p);
+    }
+    OMVGBA_LAUNCH(k_block_records, nb, 128, 0, st, mt, bt.blk_edge, d_asm_rec.p, d_blk_out.p);
+  }
+
   void build_rows() {
     const int row_smem = (int)std::min<uint64_t>(S.max_row, (uint64_t)kRowSmemDoubles);
     const size_t smem = (size_t)row_smem * sizeof(double);
@@ -4028,6 +3941,8 @@ void resident_schur_product(Resident* r, double lambda, bool fp32, int stage, co
     s.matvec_tiles(x, nullptr, fp32);
   else if (stage == 2)
     s.build_rows();
+  else if (stage == 3)
+    s.camera_sums();
   else
     s.matvec(x, y, lambda, nullptr, fp32);
   s.check_launch();

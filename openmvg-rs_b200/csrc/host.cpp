@@ -2373,7 +2373,7 @@ int32_t omvgba_plan_schur_product(omvgba_plan* plan, double lambda, int32_t fp32
   if (plan && plan->two_view)
     return write_error(error, OMVGBA_UNSUPPORTED, "a two-view plan has no reduced camera product");
   if (!plan || !x || (stage == 0 && !y)) return write_error(error, OMVGBA_INVALID_ARGUMENT, "null argument");
-  if (stage < 0 || stage > 2) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0, 1 or 2");
+  if (stage < 0 || stage > 3) return write_error(error, OMVGBA_INVALID_ARGUMENT, "stage must be 0, 1, 2 or 3");
   if (!(std::isfinite(lambda) && lambda >= 0.0))
     return write_error(error, OMVGBA_INVALID_ARGUMENT, "lambda must be finite and non-negative");
   try {

@@ -165,7 +165,7 @@ class Plan:
 
     def schur_product(self, x_ptr: int, y_ptr: int, damping: float, fp32: bool = False, stage: int = 0) -> None:
         """y = S_lambda x on device pointers (stage 1: the tile pass alone; stage 2: the explicit S
-        rows alone), on the plan's stream."""
+        rows alone; stage 3: the camera-side assembly sums alone), on the plan's stream."""
         err = abi.Error()
         code = lib().omvgba_plan_schur_product(self._plan, damping, int(fp32), stage, C.c_void_p(x_ptr),
                                                C.c_void_p(y_ptr), C.byref(err))

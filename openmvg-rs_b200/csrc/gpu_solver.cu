@@ -115,6 +115,77 @@ thread_local PinnedStage tl_pinned;
 thread_local PinnedStage tl_poll;  // the PCG loop's status mirrors (read while the next batch runs)
 constexpr size_t kStagedCopyMax = 1u << 20;
 
+// Large host->device copies from pageable memory: the source is copied by several host threads into
+// one of two pinned chunks while the other chunk's DMA runs (an event per chunk guards its reuse).
+// Returns when every chunk has reached the device, as a pageable copy would.
+constexpr size_t kPipelinedCopyMin = 32u << 20;
+constexpr size_t kPipelineChunk = 16u << 20;
+struct PinnedRing {
+  void* p[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int device = -1;
+  bool ready = false;
+  ~PinnedRing() {
+    for (int i = 0; i < 2; ++i) {
+      if (p[i]) cudaFreeHost(p[i]);
+      if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+  }
+  bool ensure() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (ready && dev == device) return true;
+    for (int i = 0; i < 2; ++i) {  // events belong to a device: rebuild them for this one
+      if (ev[i]) cudaEventDestroy(ev[i]);
+      ev[i] = nullptr;
+      if (!p[i] && cudaMallocHost(&p[i], kPipelineChunk) != cudaSuccess) {
+        cudaGetLastError();
+        p[i] = nullptr;
+        return false;
+      }
+      if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        ev[i] = nullptr;
+        return false;
+      }
+    }
+    device = dev;
+    ready = true;
+    return true;
+  }
+};
+thread_local PinnedRing tl_ring;
+
+inline void parallel_memcpy(void* dst, const void* src, size_t bytes) {
+  const size_t nt = std::max<size_t>(1, std::min<size_t>(host_thread_limit(), 8));
+  const size_t per = ((bytes + nt - 1) / nt + 63) & ~size_t(63);
+  std::vector<std::thread> pool;
+  for (size_t i = 1; i < nt && i * per < bytes; ++i)
+    pool.emplace_back([=] {
+      std::memcpy(static_cast<char*>(dst) + i * per, static_cast<const char*>(src) + i * per,
+                  std::min(per, bytes - i * per));
+    });
+  std::memcpy(dst, src, std::min(per, bytes));
+  for (auto& t : pool) t.join();
+}
+
+inline cudaError_t upload_pipelined(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!tl_ring.ensure()) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaSuccess;
+  size_t i = 0;
+  for (size_t off = 0; off < bytes && e == cudaSuccess; off += kPipelineChunk, ++i) {
+    const int b = (int)(i & 1);
+    const size_t n = std::min(kPipelineChunk, bytes - off);
+    if (i >= 2) e = cudaEventSynchronize(tl_ring.ev[b]);  // this chunk's previous copy has landed
+    if (e != cudaSuccess) break;
+    parallel_memcpy(tl_ring.p[b], static_cast<const char*>(src) + off, n);
+    e = cudaMemcpyAsync(static_cast<char*>(dst) + off, tl_ring.p[b], n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(tl_ring.ev[b], st);
+  }
+  const cudaError_t w = cudaStreamSynchronize(st);
+  return e != cudaSuccess ? e : w;
+}
+
 // Host<->device copy on `st`, counted in the telemetry. Copies of at most kStagedCopyMax bytes go
 // through the thread's pinned stage and have completed when the call returns (callers read the
 // host side right after their next synchronize, so nothing relies on them staying asynchronous).
@@ -135,6 +206,7 @@ inline cudaError_t copy_async(void* dst, const void* src, size_t bytes, cudaMemc
       return e;
     }
   }
+  if (kind == cudaMemcpyHostToDevice && bytes >= kPipelinedCopyMin) return upload_pipelined(dst, src, bytes, st);
   return cudaMemcpyAsync(dst, src, bytes, kind, st);
 }
 

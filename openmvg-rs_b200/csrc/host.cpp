@@ -1498,6 +1498,48 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
 }
 
 // ---- quarantine --------------------------------------------------------------------------------
+// The k-th smallest of v (k < v.size()), as std::nth_element would place it; v is reordered. Values
+// that are all non-negative and not NaN (distances) order like their bit patterns, so a histogram
+// of the top 16 bits, taken in parallel, finds the bucket that holds the k-th value, and only that
+// bucket is selected from. Anything else takes std::nth_element over the whole vector.
+double kth_smallest(std::vector<double>& v, size_t k) {
+  const size_t n = v.size();
+  constexpr size_t kChunks = 64, kBins = 1 << 16;
+  std::vector<uint32_t> hist(kChunks * kBins, 0);
+  std::atomic<bool> plain{true};
+  for_fixed_chunks(n, kChunks, [&](size_t c, size_t b, size_t e) {
+    uint32_t* h = &hist[c * kBins];
+    for (size_t i = b; i < e; ++i) {
+      if (!(v[i] >= 0.0)) {  // negative or NaN
+        plain = false;
+        return;
+      }
+      uint64_t bits;
+      std::memcpy(&bits, &v[i], 8);
+      h[bits >> 48]++;
+    }
+  });
+  if (!plain || n < (1u << 20)) {
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
+  }
+  size_t below = 0, bucket = 0;
+  for (; bucket < kBins; ++bucket) {
+    size_t cnt = 0;
+    for (size_t c = 0; c < kChunks; ++c) cnt += hist[c * kBins + bucket];
+    if (below + cnt > k) break;
+    below += cnt;
+  }
+  std::vector<double> in_bucket;
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t bits;
+    std::memcpy(&bits, &v[i], 8);
+    if ((bits >> 48) == bucket) in_bucket.push_back(v[i]);
+  }
+  std::nth_element(in_bucket.begin(), in_bucket.begin() + (k - below), in_bucket.end());
+  return in_bucket[k - below];
+}
+
 std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pose* poses, const double* points) {
   size_t N = pr.observation_count;
   // the ray from the camera centre to the point (recomputed where it is used, bit for bit)
@@ -1513,20 +1555,42 @@ std::vector<size_t> degenerate_points(const omvgba_problem& pr, const omvgba_pos
       dist[o] = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     }
   });
-  double scene = 0.0;
-  if (N > 0) {
-    std::nth_element(dist.begin(), dist.begin() + N / 2, dist.end());
-    scene = dist[N / 2];
+  const double scene = N > 0 ? kth_smallest(dist, N / 2) : 0.0;
+  // each point's observations in input order: the input itself when it is grouped by point in
+  // ascending order (a track per point, the usual layout), else a stable counting sort
+  const size_t P = pr.point_count;
+  std::vector<uint64_t> start(P + 1, 0);
+  std::vector<uint64_t> order;
+  std::atomic<bool> grouped{true};
+  for_fixed_chunks(N, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t o = std::max<size_t>(b, 1); o < e; ++o)
+      if (pr.observation_point[o] < pr.observation_point[o - 1]) {
+        grouped = false;
+        return;
+      }
+  });
+  for (size_t o = 0; o < N; ++o) start[pr.observation_point[o] + 1]++;
+  for (size_t p = 0; p < P; ++p) start[p + 1] += start[p];
+  if (!grouped) {
+    order.resize(N);
+    std::vector<uint64_t> next(start.begin(), start.end() - 1);
+    for (size_t o = 0; o < N; ++o) order[next[pr.observation_point[o]]++] = o;
   }
-  std::vector<TrackGeometryDev> geo(pr.point_count);
-  for (auto& g : geo) g.init(scene);
-  for (size_t o = 0; o < N; ++o) {
-    const Vec3 v = offset(o);
-    geo[pr.observation_point[o]].push(v[0], v[1], v[2]);
-  }
+  std::vector<uint8_t> deg(P, 0);
+  for_fixed_chunks(P, 64, [&](size_t, size_t b, size_t e) {
+    for (size_t p = b; p < e; ++p) {
+      TrackGeometryDev g;
+      g.init(scene);
+      for (uint64_t i = start[p]; i < start[p + 1]; ++i) {
+        const Vec3 v = offset(grouped ? i : order[i]);
+        g.push(v[0], v[1], v[2]);
+      }
+      deg[p] = g.degenerate() ? 1 : 0;
+    }
+  });
   std::vector<size_t> out;
-  for (size_t p = 0; p < pr.point_count; ++p)
-    if (geo[p].degenerate()) out.push_back(p);
+  for (size_t p = 0; p < P; ++p)
+    if (deg[p]) out.push_back(p);
   return out;
 }
 

@@ -1528,7 +1528,6 @@ struct Setup {
   FillVector<uint32_t> ent, ent_point;  // written completely by the construction
   std::vector<int> chunk_block, chunk_col, blk_chunk_begin, blk_chunk_end;
   std::vector<uint32_t> chunk_begin, chunk_end;
-  FillVector<int> obs_intr_col;  // (intr dim << 8) | column of intrinsic segment (all written)
   FillVector<int> seg_col;       // per entity id (obs*2+seg): column (all written)
   // cross same-block pairs (preconditioner)
   std::vector<int> xgrp_row, xgrp_col;
@@ -1746,7 +1745,6 @@ static void build_tables(const NativeProblem& n, const Layout& L, Setup& S) {
   // entity lists per block (stable in observation order)
   // every entry is written below (-1: no block, column 0 and no intrinsic when absent)
   S.seg_col.resize(2 * N);
-  S.obs_intr_col.resize(N);
   FillVector<int> ent_block(2 * N);
   host_parallel_chunks(N, 64, [&](size_t, size_t b, size_t e) {
     for (size_t o = b; o < e; ++o) {
@@ -1754,16 +1752,14 @@ static void build_tables(const NativeProblem& n, const Layout& L, Setup& S) {
       int pd = L.pose_dim[c];
       ent_block[2 * o] = cam_block[c];  // -1 when the pose has no block
       S.seg_col[2 * o] = 0;
-      int intr_b = -1, intr_col = 0, intr = 0;
+      int intr_b = -1, intr_col = 0;
       if (n.self_cal) {
         int g = n.cam_group[c];
-        intr = (L.intr_dim[g] << 8) | pd;
         if (grp_block[g] >= 0) {
           intr_b = grp_block[g];
           intr_col = pd;
         }
       }
-      S.obs_intr_col[o] = intr;
       ent_block[2 * o + 1] = intr_b;
       S.seg_col[2 * o + 1] = intr_col;
     }
@@ -1809,10 +1805,9 @@ static void build_tables(const NativeProblem& n, const Layout& L, Setup& S) {
       S.ent_point[at] = obs_point[i >> 1];
     }
   });
-  // intrinsic blocks have a per-observation column: stored via seg_col; blk_col = -1 means "use seg"
-  // For kernels that take blk_col, intrinsic blocks read their column from obs_intr_col. To keep the
-  // chunk kernel simple, split entity lists so every chunk has one column: intrinsic entities of
-  // cameras with different pose dims (0, 5, 6) are grouped by column inside the block.
+  // intrinsic blocks have a per-observation column: stored via seg_col; blk_col = -1 means "use seg".
+  // Inside such a block the entities are grouped by column (cameras with pose dims 0, 5, 6), stably,
+  // so that every chunk has one column.
   host_parallel_for((size_t)nb, [&](size_t b) {
     if (S.blk_col[b] >= 0) return;
     std::stable_sort(S.ent.begin() + counts[b], S.ent.begin() + counts[b + 1],
@@ -2091,7 +2086,6 @@ uint64_t setup_digest(const NativeProblem& n, const LmOptions& opt) {
                         &S.blk_chunk_begin, &S.blk_chunk_end, &S.xgrp_row, &S.xgrp_col,
                         &S.blk_cross_begin, &S.blk_cross_end})
     add(*v);
-  add(S.obs_intr_col);
   add(S.seg_col);
   add(S.ent_block);
   add(S.blk_ent);

@@ -2738,6 +2738,35 @@ struct Solver {
   // Cholesky of (S + lambda diag) -- equilibrated as scale S scale and shifted by -shift I when scale
   // is given -- into the banded tiles; true when every pivot is finite and positive.
   static constexpr size_t kMaxTileBytes = size_t(16) << 30;
+  static constexpr int kGraphColumns = 64;  // tile columns from which a column loop runs as a graph
+  // Runs a long fixed sequence of launches (a tile-column loop) as one CUDA graph: captured on the
+  // solver's stream, instantiated, launched and waited for, so the device runs the columns back to
+  // back whatever the host is doing meanwhile.
+  template <typename Body>
+  void run_as_graph(Body body) {
+    if (S.nt < kGraphColumns) {  // short loops: capture and instantiation would cost more than they save
+      body();
+      return;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    body();
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      CUDA_OK(ce);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CUDA_OK(ie);
+    const cudaError_t le = cudaGraphLaunch(exec, st);
+    const cudaError_t se = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    CUDA_OK(le);
+    CUDA_OK(se);
+  }
+
   bool factor_band(double lambda, const double* scale, double shift) {
     if (D == 0) return true;
     const double t_factor = now();
@@ -2755,14 +2784,16 @@ struct Solver {
     OMVGBA_LAUNCH(k_rows_to_tiles, grid_for(S.nbr.size(), 128), 128, 0, st, row_tables(), d_rows.p, d_perm_off.p,
                   d_diag.p, lambda, scale, shift, tb);
     OMVGBA_LAUNCH(k_tiles_pad, 1, kCT, 0, st, tb);
-    for (int k = 0; k < S.nt; ++k) {
-      OMVGBA_LAUNCH(k_tile_potrf, 1, 256, 0, st, tb, k, d_status.p);
-      const int m = std::min(S.bwt, S.nt - 1 - k);
-      if (m > 0) {
-        OMVGBA_LAUNCH(k_tile_trsm, m, 256, kTrsmSmem, st, tb, k, d_status.p);
-        OMVGBA_LAUNCH(k_tile_update, m * (m + 1) / 2, 256, kUpdateSmem, st, tb, k, d_status.p);
+    run_as_graph([&] {
+      for (int k = 0; k < S.nt; ++k) {
+        OMVGBA_LAUNCH(k_tile_potrf, 1, 256, 0, st, tb, k, d_status.p);
+        const int m = std::min(S.bwt, S.nt - 1 - k);
+        if (m > 0) {
+          OMVGBA_LAUNCH(k_tile_trsm, m, 256, kTrsmSmem, st, tb, k, d_status.p);
+          OMVGBA_LAUNCH(k_tile_update, m * (m + 1) / 2, 256, kUpdateSmem, st, tb, k, d_status.p);
+        }
       }
-    }
+    });
     check_launch();
     int ok = 0;
     CUDA_OK(copy_async(&ok, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -2842,16 +2873,19 @@ struct Solver {
     DBuf<double> d_zpart, d_zq;
     d_zpart.alloc((size_t)std::max(S.bwt, 1) * std::max(max_split, 1) * kCTT, st);
     d_zq.alloc((size_t)std::max(S.bwt, 1) * kCTT, st);
-    for (int j = S.nt - 1; j >= 0; --j) {
-      const int m = std::min(S.bwt, S.nt - 1 - j);
-      if (m > 0) {
-        const int nsplit = (m + kTakahashiChunk - 1) / kTakahashiChunk;
-        OMVGBA_LAUNCH(k_takahashi_partial, dim3(m, nsplit), 256, kTakahashiSmem, st, tl, tz, j, d_zpart.p, d_status.p);
-        OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, nsplit, d_zpart.p, d_zq.p,
-                      d_status.p);
+    run_as_graph([&] {
+      for (int j = S.nt - 1; j >= 0; --j) {
+        const int m = std::min(S.bwt, S.nt - 1 - j);
+        if (m > 0) {
+          const int nsplit = (m + kTakahashiChunk - 1) / kTakahashiChunk;
+          OMVGBA_LAUNCH(k_takahashi_partial, dim3(m, nsplit), 256, kTakahashiSmem, st, tl, tz, j, d_zpart.p,
+                        d_status.p);
+          OMVGBA_LAUNCH(k_takahashi_offdiag, m, 256, kTakahashiSmem, st, tl, tz, j, nsplit, d_zpart.p, d_zq.p,
+                        d_status.p);
+        }
+        OMVGBA_LAUNCH(k_takahashi_diag, 1, 256, kTakahashiSmem, st, tl, tz, j, m, d_zq.p, d_status.p);
       }
-      OMVGBA_LAUNCH(k_takahashi_diag, 1, 256, kTakahashiSmem, st, tl, tz, j, m, d_zq.p, d_status.p);
-    }
+    });
     DBuf<int> d_pos, d_dims;
     d_pos.upload(pos.data(), pos.size(), st);
     d_dims.upload(dims.data(), dims.size(), st);

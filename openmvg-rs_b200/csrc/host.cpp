@@ -14,8 +14,6 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
-#include <functional>
-#include <future>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -995,34 +993,6 @@ struct InputMetrics {
   std::vector<MetricPart> parts;
 };
 
-// The input-state metric parts of the observations of the points not in `quarantined` (ascending),
-// chunk by chunk exactly as finish_solution forms them.
-InputMetrics input_metrics(const omvgba_problem& pr, const std::vector<uint64_t>& quarantined) {
-  std::vector<uint8_t> active(pr.point_count, 1);
-  for (auto q : quarantined) active[q] = 0;
-  const LossDev loss = problem_loss(pr);
-  constexpr size_t kChunks = 64;
-  InputMetrics out;
-  out.parts.assign(kChunks, MetricPart{});
-  const StateView sv(pr, pr.poses, pr.intrinsics);
-  for_fixed_chunks(pr.observation_count, kChunks, [&](size_t c, size_t b, size_t e) {
-    MetricPart m0;
-    for (size_t o = b; o < e; ++o) {
-      const size_t p = pr.observation_point[o];
-      if (!active[p] || !m0.ok) continue;
-      double nrm;
-      if (!residual_norm(pr, sv, o, pr.points + 3 * p, &nrm))
-        m0.ok = false;
-      else
-        m0.add(loss, nrm);
-    }
-    out.parts[c] = m0;
-  });
-  out.quarantined = quarantined;
-  out.valid = true;
-  return out;
-}
-
 void finish_solution(const omvgba_problem& pr, Result& res, InputMetrics* cache = nullptr) {
   std::vector<uint8_t> active(pr.point_count, 1);
   for (auto q : res.quarantined) active[q] = 0;
@@ -1488,8 +1458,7 @@ Result solve_two_view(Context* ctx, const omvgba_problem& pr, const omvgba_confi
 
 // finish = false leaves the report's observation and inlier metrics to the caller: the quarantine
 // protocol evaluates them once more over the original problem whenever points are held out.
-Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg, bool finish = true,
-                  const std::function<void()>& lowered = nullptr) {
+Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& cfg, bool finish = true) {
   validate_config(cfg);
   if (!(pr.residual_space != OMVGBA_RESIDUAL_ANGULAR && has_free_intrinsics(pr)) && can_use_two_view(pr)) {
     Result res = solve_two_view(ctx, pr, cfg);
@@ -1500,7 +1469,6 @@ Result solve_once(Context* ctx, const omvgba_problem& pr, const omvgba_config& c
   const auto t0 = std::chrono::steady_clock::now();
   Lowered L = lower(pr);
   const double t_lower = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  if (lowered) lowered();
   LmOptions opt = lm_options(pr, cfg, L.n);
   std::vector<double> rot, tr, pts, grp;
   NativeReport nr = gpu_refine(ctx, L.n, opt, rot, tr, pts, grp);
@@ -1934,41 +1902,9 @@ Result solve_with_quarantine(Context* ctx, const omvgba_problem& pr, const omvgb
   Prepared prep;
   prepare_quarantine(pr, cfg, prep);
   const double t_prep = seconds_since(t0);
-  // With points held out, the report's input-state metrics over the input problem depend only on
-  // the input and the held-out set: a host thread forms them while the device solves (after the
-  // lowering, whose host threads it would slow). finish_quarantine uses them when the held-out set
-  // is still the same at the end.
-  InputMetrics early;
-  std::promise<void> lowered;
-  std::future<void> metrics;
-  if (prep.quarantined > 0) {
-    std::vector<uint64_t> held;
-    std::vector<uint8_t> kept(pr.point_count, 0);
-    for (size_t k : prep.kept) kept[k] = 1;
-    for (size_t p = 0; p < pr.point_count; ++p)
-      if (!kept[p]) held.push_back(p);
-    const unsigned threads = std::max(1u, host_thread_limit() / 2);  // half: the solver's table setup runs too
-    metrics = std::async(std::launch::async, [&pr, &early, held = std::move(held), threads,
-                                              go = lowered.get_future().share()] {
-      go.wait();
-      set_host_thread_limit(threads);
-      early = input_metrics(pr, held);
-    });
-  }
-  struct Release {  // the metrics thread starts even when the solve fails, and is joined here
-    std::promise<void>* p;
-    bool done = false;
-    void operator()() {
-      if (!done) p->set_value();
-      done = true;
-    }
-    ~Release() { (*this)(); }
-  } release{&lowered};
-  Result sol = solve_once(ctx, *prep.working, cfg, prep.quarantined == 0, [&release] { release(); });
+  Result sol = solve_once(ctx, *prep.working, cfg, prep.quarantined == 0);
   const double t_solve = seconds_since(t0) - t_prep;
-  release();
-  if (metrics.valid()) metrics.get();
-  Result out = finish_quarantine(ctx, pr, cfg, prep, std::move(sol), early.valid ? &early : nullptr);
+  Result out = finish_quarantine(ctx, pr, cfg, prep, std::move(sol));
   if (std::getenv("OMVGBA_PHASE_TIMES"))
     std::fprintf(stderr, "[omvgba] host: prepare %.3fs solve_once %.3fs finish %.3fs\n", t_prep, t_solve,
                  seconds_since(t0) - t_prep - t_solve);
